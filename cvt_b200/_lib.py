@@ -1,0 +1,105 @@
+"""ctypes binding of libcvtpm.so (include/cvtpm.h).
+
+The library is loaded from this package directory.  It is required: there is
+no fallback implementation, and every call below fails loudly if the library
+is missing.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcvtpm.so")
+
+PM_OK, PM_EINVAL_SHAPE, PM_EINVAL_ARG, PM_ENOMEM, PM_ECUDA, PM_ETIMEOUT, PM_ENOTIMPL, PM_ENODEV = range(8)
+PP_NONE, PP_LRCHECK, PP_LRCHECK_FILL = 0, 1, 2
+
+# every exported symbol of include/cvtpm.h
+SYMBOLS = [
+    "pm_options_default", "pm_create", "pm_destroy", "pm_last_error", "pm_status_string",
+    "pm_disparity_map", "pm_disparity_map_device", "pm_set_counting", "pm_get_counters",
+    "pm_disparity_map_batch_device",
+    "pm_k_prep", "pm_k_init", "pm_k_cost", "pm_k_klt", "pm_k_propagate", "pm_k_normal_depth",
+    "pm_rof_scratch_bytes", "pm_k_rof", "pm_k_consistency", "pm_k_to_disparity", "pm_k_fill_depthmap",
+    "pm_k_fill_normalmap", "pm_k_disparity_to_normal",
+    "pm_rng_floats", "pm_expf_host", "pm_sinf_host", "pm_cosf_host", "pm_acospif_host",
+    "pm_exit_threshold_host", "pm_scene_generate",
+]
+
+
+class Options(C.Structure):
+    _fields_ = [("views", C.c_int), ("fused", C.c_int), ("thetamin", C.c_float), ("maxdispdiff", C.c_float),
+                ("maxanglediff", C.c_float), ("rof_iters", C.c_int), ("device", C.c_int), ("use_graph", C.c_int)]
+
+
+class StereoError(RuntimeError):
+    """Raised for a non-zero status of the native library (the reference throws cvt::Exception)."""
+
+    def __init__(self, status, message):
+        super().__init__("%s (status %d)" % (message, status))
+        self.status = status
+
+
+_lib = None
+
+vp = C.c_void_p
+i32 = C.c_int
+f32 = C.c_float
+sz = C.c_size_t
+
+
+def lib():
+    """Load libcvtpm.so (built by cvt_b200/build.py) and declare its signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libcvtpm.so is not built: run `python cvt_b200/build.py` (needs nvcc)")
+    L = C.CDLL(LIB_PATH)
+    sig = {
+        "pm_options_default": (i32, [C.POINTER(Options)]),
+        "pm_create": (i32, [C.POINTER(vp), C.POINTER(Options)]),
+        "pm_destroy": (i32, [vp]),
+        "pm_last_error": (C.c_char_p, [vp]),
+        "pm_status_string": (C.c_char_p, [i32]),
+        "pm_disparity_map": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, i32, vp, vp, vp, vp, vp, vp]),
+        "pm_disparity_map_device": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, i32, vp, vp, vp, vp, vp, vp, vp]),
+        "pm_set_counting": (i32, [vp, i32]),
+        "pm_get_counters": (i32, [vp, C.POINTER(C.c_uint64)]),
+        "pm_disparity_map_batch_device": (i32, [vp, i32, vp, vp, vp, vp, vp, vp, vp, i32, i32, vp, vp, vp, vp]),
+        "pm_k_prep": (i32, [vp, i32, i32, sz, i32, i32, vp, vp, vp, vp]),
+        "pm_k_init": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, f32, i32, vp, vp, i32, vp]),
+        "pm_k_cost": (i32, [vp, vp, vp, vp, vp, vp, i32, i32, i32, f32, i32, vp]),
+        "pm_k_klt": (i32, [vp, vp, vp, vp, vp, vp, i32, i32, i32, i32, vp]),
+        "pm_k_propagate": (i32, [vp, vp, vp, vp, vp, vp, vp, f32, i32, i32, i32, f32, i32, i32,
+                                 vp, vp, vp, vp, vp, i32, vp, vp]),
+        "pm_k_normal_depth": (i32, [vp, vp, i32, i32, f32, i32, vp]),
+        "pm_rof_scratch_bytes": (sz, [i32, i32]),
+        "pm_k_rof": (i32, [vp, vp, vp, C.POINTER(C.c_float), i32, i32, i32, vp, vp]),
+        "pm_k_consistency": (i32, [vp, vp, vp, i32, i32, f32, f32, vp]),
+        "pm_k_to_disparity": (i32, [vp, vp, i32, i32, f32, i32, vp]),
+        "pm_k_fill_depthmap": (i32, [vp, vp, i32, i32, f32, vp]),
+        "pm_k_fill_normalmap": (i32, [vp, vp, i32, i32, i32, vp]),
+        "pm_k_disparity_to_normal": (i32, [vp, vp, i32, i32, vp]),
+        "pm_rng_floats": (i32, [C.c_int64, i32, i32, vp]),
+        "pm_expf_host": (f32, [f32]),
+        "pm_sinf_host": (f32, [f32]),
+        "pm_cosf_host": (f32, [f32]),
+        "pm_acospif_host": (f32, [f32]),
+        "pm_exit_threshold_host": (f32, [f32, f32]),
+        "pm_scene_generate": (i32, [C.c_uint64, i32, i32, i32, f32, f32, f32, f32, vp, vp, i32, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status, handle=None):
+    """Raise StereoError for a non-zero status, with the library's message."""
+    if status != PM_OK:
+        L = lib()
+        msg = L.pm_last_error(handle) if handle is not None else L.pm_last_error(None)
+        raise StereoError(status, (msg or L.pm_status_string(status)).decode())
+    return status

@@ -1,0 +1,575 @@
+// C ABI of the library (include/cvtpm.h): handles, device workspaces and the
+// host orchestration of PMHuberStereo::disparityMap / disparityMapAll
+// (cvt/vision/PMHuberStereo.cpp:75-143, :406-581) on one CUDA stream.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cvtpm.h"
+#include "pm_kernels.h"
+
+using namespace pm;
+
+struct pm_handle {
+    pm_options opt;
+    std::string err;
+    int counting = 0;
+    uint64_t counters[4] = {0, 0, 0, 0};
+    // device workspace for one image size
+    int W = 0, H = 0;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    cudaStream_t own = nullptr;
+};
+
+namespace {
+
+thread_local std::string t_err;
+
+int fail(pm_handle* h, int code, const std::string& msg)
+{
+    if (h) h->err = msg;
+    t_err = msg;
+    return code;
+}
+
+int cuda_fail(pm_handle* h, cudaError_t e, const char* what)
+{
+    return fail(h, PM_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PM_CUDA(h, call)                                         \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return cuda_fail((h), e_, #call); \
+    } while (0)
+
+int check_shape(pm_handle* h, int W, int H, int r)
+{
+    if (W <= 0 || H <= 0 || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT)
+        return fail(h, PM_EINVAL_SHAPE, "image size out of range");
+    if (r < 0 || r > PM_MAX_RADIUS) return fail(h, PM_EINVAL_SHAPE, "patch size out of range");
+    return PM_OK;
+}
+
+inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
+
+// workspace layout for a W x H pair (float4 fields unless noted)
+struct Layout {
+    size_t N;
+    size_t off[32];
+    size_t total;
+    enum {
+        Lbw, Rbw, Lg, Rg, LDT, RDT, Ls, Rs, tmp, mL0, mL1, mR0, mR1, chk, nrm,   // float4 x N
+        vb1c, vb2c,                                                             // int x N
+        vb1s, vb2s,                                                             // u64 x N
+        rof,                                                                    // rof scratch
+        ctr, errf,                                                              // counters (4 u64), error int
+        img0, img1, disp, dmap, nmap, initd, initn,                             // staging for host entry
+        COUNT
+    };
+};
+
+Layout layout(int W, int H, size_t stride)
+{
+    Layout L;
+    L.N = (size_t)W * H;
+    size_t o = 0;
+    auto put = [&](int k, size_t bytes) { L.off[k] = o; o += (bytes + 255) / 256 * 256; };
+    for (int k = Layout::Lbw; k <= Layout::nrm; k++) put(k, L.N * 16);
+    put(Layout::vb1c, L.N * 4);
+    put(Layout::vb2c, L.N * 4);
+    put(Layout::vb1s, L.N * 8);
+    put(Layout::vb2s, L.N * 8);
+    put(Layout::rof, rof_scratch_bytes(W, H));
+    put(Layout::ctr, 64);
+    put(Layout::errf, 64);
+    put(Layout::img0, stride * H);
+    put(Layout::img1, stride * H);
+    put(Layout::disp, L.N * 4);
+    put(Layout::dmap, L.N * 4);
+    put(Layout::nmap, L.N * 16);
+    put(Layout::initd, L.N * 4);
+    put(Layout::initn, L.N * 16);
+    L.total = o;
+    return L;
+}
+
+template <class T> T* at(void* base, const Layout& L, int k) { return reinterpret_cast<T*>(static_cast<char*>(base) + L.off[k]); }
+
+int ensure_ws(pm_handle* h, int W, int H, size_t stride)
+{
+    const Layout L = layout(W, H, stride);
+    if (h->ws && h->ws_bytes >= L.total) return PM_OK;
+    if (h->ws) { cudaFree(h->ws); h->ws = nullptr; h->ws_bytes = 0; }
+    cudaError_t e = cudaMalloc(&h->ws, L.total);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(h, PM_ENOMEM, "device workspace allocation failed"); }
+    h->ws_bytes = L.total;
+    return PM_OK;
+}
+
+// one pass of disparityMapAll + disparityMap post-processing on device buffers
+int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int r,
+                 float dmax, int iterations, int pp, float* dmap, float4* normal, const float* initdisp,
+                 const float4* initnormal, float4* planesL, float4* planesR, cudaStream_t st)
+{
+    const pm_options& o = h->opt;
+    const int views = o.views;
+    const int F = o.fused;
+    int rc = ensure_ws(h, W, H, stride);
+    if (rc) return rc;
+    const Layout L = layout(W, H, stride);
+    void* ws = h->ws;
+    const size_t N = L.N;
+    float4 *Lbw = at<float4>(ws, L, Layout::Lbw), *Rbw = at<float4>(ws, L, Layout::Rbw);
+    float4 *Lg = at<float4>(ws, L, Layout::Lg), *Rg = at<float4>(ws, L, Layout::Rg);
+    float4 *LDT = at<float4>(ws, L, Layout::LDT), *RDT = at<float4>(ws, L, Layout::RDT);
+    float4 *Ls = at<float4>(ws, L, Layout::Ls), *Rs = at<float4>(ws, L, Layout::Rs), *tmp = at<float4>(ws, L, Layout::tmp);
+    float4* mL[2] = {at<float4>(ws, L, Layout::mL0), at<float4>(ws, L, Layout::mL1)};
+    float4* mR[2] = {at<float4>(ws, L, Layout::mR0), at<float4>(ws, L, Layout::mR1)};
+    float4* chk = at<float4>(ws, L, Layout::chk);
+    int *vb1c = at<int>(ws, L, Layout::vb1c), *vb2c = at<int>(ws, L, Layout::vb2c);
+    unsigned long long *vb1s = at<unsigned long long>(ws, L, Layout::vb1s), *vb2s = at<unsigned long long>(ws, L, Layout::vb2s);
+    void* rofs = at<void>(ws, L, Layout::rof);
+    unsigned long long* ctr = at<unsigned long long>(ws, L, Layout::ctr);
+    int* errf = at<int>(ws, L, Layout::errf);
+
+    PM_CUDA(h, cudaMemsetAsync(ctr, 0, 64, st));
+    PM_CUDA(h, cudaMemsetAsync(errf, 0, 64, st));
+    // prep (PMHuberStereo.cpp:445-454)
+    launch_prep(left, stride, W, H, r, F, Lbw, Lg, LDT, st);
+    if (views == 2) launch_prep(right, stride, W, H, r, F, Rbw, Rg, RDT, st);
+    else launch_prep(right, stride, W, H, r, F, Rbw, Rg, nullptr, st);
+    // clear the smoothing images (:457-458) and both view buffers (:487)
+    PM_CUDA(h, cudaMemsetAsync(Ls, 0, N * 16, st));
+    PM_CUDA(h, cudaMemsetAsync(Rs, 0, N * 16, st));
+    launch_view_clear(vb1c, vb1s, N, st);
+    launch_view_clear(vb2c, vb2s, N, st);
+    // init (:469-470); the given disparity and normals apply to the left view only (:92-93)
+    const float4* initn = initnormal;
+    if (initdisp && !initnormal) {
+        float4* nrm = at<float4>(ws, L, Layout::nrm);
+        launch_disparity_to_normal(nrm, initdisp, W, H, st);   // :363-365
+        initn = nrm;
+    }
+    const ViewData VL = {Lbw, Rbw, Lg, Rg, W, H, r};
+    const ViewData VR = {Rbw, Lbw, Rg, Lg, W, H, r};
+    launch_init(mL[0], VL, dmax, 1, initdisp, initn, F, st);
+    if (views == 2) launch_init(mR[0], VR, dmax, 0, nullptr, nullptr, F, st);
+    const float thetamin = o.thetamin;
+    float theta = thetamin;
+    if (initdisp) {   // :473-477
+        const float4 lam = make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);
+        launch_normal_depth(tmp, mL[0], W, H, 1.0f / dmax, 1, st);
+        launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
+    }
+    int swap = 0;
+    iterations |= 1;   // :490
+    for (int iter = 0; iter < iterations; iter++) {
+        const float4 lam = make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);   // :532
+        PropParams P;
+        P.V = VL;
+        P.out = mL[1 - swap];
+        P.old = mL[swap];
+        P.smooth = Ls;
+        P.theta = theta * 50.0f;
+        P.dmax = dmax;
+        P.lr = 1;
+        P.iter = iter;
+        P.vin_count = views == 2 ? vb2c : nullptr;
+        P.vin_src = vb2s;
+        P.vin_planes = mR[swap];
+        P.vout_count = views == 2 ? vb1c : nullptr;
+        P.vout_src = vb1s;
+        P.counters = h->counting ? ctr : nullptr;
+        P.error = errf;
+        launch_propagate(P, F, st);   // :536-537
+        if (views == 2) {
+            P.V = VR;
+            P.out = mR[1 - swap];
+            P.old = mR[swap];
+            P.smooth = Rs;
+            P.lr = 0;
+            P.vin_count = vb1c;
+            P.vin_src = vb1s;
+            P.vin_planes = mL[1 - swap];
+            P.vout_count = vb2c;
+            P.vout_src = vb2s;
+            launch_propagate(P, F, st);   // :542-543
+        }
+        launch_normal_depth(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :552-553
+        launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
+        if (views == 2) {
+            launch_normal_depth(tmp, mR[1 - swap], W, H, 1.0f / dmax, 0, st);   // :566-567
+            launch_rof(Rs, tmp, RDT, lam, o.rof_iters, W, H, rofs, st);
+        }
+        theta = (float)iter / (float)iterations;   // :575-576
+        theta = powf(theta, 4.0f) + thetamin;
+        swap = 1 - swap;
+    }
+    float4* ml = mL[1];
+    if (planesL) PM_CUDA(h, cudaMemcpyAsync(planesL, ml, N * 16, cudaMemcpyDeviceToDevice, st));
+    if (planesR && views == 2) PM_CUDA(h, cudaMemcpyAsync(planesR, mR[1], N * 16, cudaMemcpyDeviceToDevice, st));
+    if (pp == PM_PP_NONE) {   // :123-129
+        if (dmap) launch_to_disparity(dmap, ml, W, H, 1.0f, 1, st);
+        if (normal) launch_fill_normalmap(normal, ml, W, H, st);
+    } else {   // :130-141
+        launch_consistency(chk, ml, mR[1], W, H, o.maxdispdiff, o.maxanglediff, st);
+        if (dmap) {
+            if (pp == PM_PP_LRCHECK) launch_to_disparity(dmap, chk, W, H, 1.0f, 1, st);
+            else launch_fill_depthmap(dmap, chk, W, H, 1.0f, st);
+        }
+        if (normal) launch_fill_normalmap(normal, chk, W, H, st);
+    }
+    PM_CUDA(h, cudaGetLastError());
+    return PM_OK;
+}
+
+int check_args(pm_handle* h, const void* left, const void* right, int W, int H, size_t stride, int r, float dmax,
+               int iterations, int pp)
+{
+    if (!h) return fail(h, PM_EINVAL_ARG, "null handle");
+    if (!left || !right) return fail(h, PM_EINVAL_ARG, "null image");
+    int rc = check_shape(h, W, H, r);
+    if (rc) return rc;
+    if (stride < (size_t)W * 4 || stride % 4) return fail(h, PM_EINVAL_SHAPE, "row stride must be >= 4*width and a multiple of 4");
+    if (!(dmax > 0.0f) || !isfinite(dmax)) return fail(h, PM_EINVAL_ARG, "disparity range must be positive");
+    if (iterations < 0) return fail(h, PM_EINVAL_ARG, "negative iteration count");
+    if (pp < PM_PP_NONE || pp > PM_PP_LRCHECK_FILL) return fail(h, PM_EINVAL_ARG, "unknown post-processing mode");
+    if (h->opt.views == 1 && pp != PM_PP_NONE) return fail(h, PM_EINVAL_ARG, "the left-right check needs both views");
+    return PM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pm_status_string(int s)
+{
+    switch (s) {
+        case PM_OK: return "ok";
+        case PM_EINVAL_SHAPE: return "invalid shape";
+        case PM_EINVAL_ARG: return "invalid argument";
+        case PM_ENOMEM: return "out of memory";
+        case PM_ECUDA: return "CUDA error";
+        case PM_ETIMEOUT: return "device wait timed out";
+        case PM_ENOTIMPL: return "not implemented";
+        case PM_ENODEV: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int pm_options_default(pm_options* o)
+{
+    if (!o) return PM_EINVAL_ARG;
+    o->views = 2;
+    o->fused = 1;
+    o->thetamin = 1e-4f;
+    o->maxdispdiff = 1.0f;
+    o->maxanglediff = 5.0f;
+    o->rof_iters = 40;
+    o->device = 0;
+    o->use_graph = 1;
+    return PM_OK;
+}
+
+int pm_create(pm_handle** out, const pm_options* opt)
+{
+    if (!out) return fail(nullptr, PM_EINVAL_ARG, "null handle pointer");
+    *out = nullptr;
+    pm_options o;
+    pm_options_default(&o);
+    if (opt) o = *opt;
+    if (o.views != 1 && o.views != 2) return fail(nullptr, PM_EINVAL_ARG, "views must be 1 or 2");
+    if (o.rof_iters < 0) return fail(nullptr, PM_EINVAL_ARG, "negative smoothing iteration count");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return fail(nullptr, PM_ENODEV, "no CUDA device"); }
+    if (o.device < 0 || o.device >= n) return fail(nullptr, PM_EINVAL_ARG, "device ordinal out of range");
+    pm_handle* h = new pm_handle();
+    h->opt = o;
+    *out = h;
+    return PM_OK;
+}
+
+int pm_destroy(pm_handle* h)
+{
+    if (!h) return PM_OK;
+    if (h->ws) cudaFree(h->ws);
+    delete h;
+    return PM_OK;
+}
+
+const char* pm_last_error(const pm_handle* h) { return h ? h->err.c_str() : t_err.c_str(); }
+
+int pm_set_counting(pm_handle* h, int on)
+{
+    if (!h) return PM_EINVAL_ARG;
+    h->counting = on ? 1 : 0;
+    return PM_OK;
+}
+
+int pm_get_counters(pm_handle* h, uint64_t c[4])
+{
+    if (!h || !c) return PM_EINVAL_ARG;
+    if (!h->ws) { memset(c, 0, 32); return PM_OK; }
+    const Layout L = layout(h->W, h->H, (size_t)h->W * 4);
+    (void)L;
+    memcpy(c, h->counters, 32);
+    return PM_OK;
+}
+
+int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
+                            int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
+                            const float* initdisp, const float* initnormal, float* planes_left, float* planes_right,
+                            void* stream)
+{
+    int rc = check_args(h, left, right, W, H, stride, patchsize, dispmax, iterations, pp);
+    if (rc) return rc;
+    PM_CUDA(h, cudaSetDevice(h->opt.device));
+    h->W = W;
+    h->H = H;
+    rc = run_pipeline(h, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap,
+                      reinterpret_cast<float4*>(normalmap), initdisp, reinterpret_cast<const float4*>(initnormal),
+                      reinterpret_cast<float4*>(planes_left), reinterpret_cast<float4*>(planes_right), S(stream));
+    if (rc) return rc;
+    if (h->counting) {
+        const Layout L = layout(W, H, stride);
+        unsigned long long c[4];
+        PM_CUDA(h, cudaMemcpyAsync(c, at<unsigned long long>(h->ws, L, Layout::ctr), 32, cudaMemcpyDeviceToHost, S(stream)));
+        PM_CUDA(h, cudaStreamSynchronize(S(stream)));
+        for (int k = 0; k < 4; k++) h->counters[k] = c[k];
+    }
+    return PM_OK;
+}
+
+int pm_disparity_map(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
+                     int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
+                     const float* initdisp, const float* initnormal, float* planes_left, float* planes_right)
+{
+    int rc = check_args(h, left, right, W, H, stride, patchsize, dispmax, iterations, pp);
+    if (rc) return rc;
+    PM_CUDA(h, cudaSetDevice(h->opt.device));
+    rc = ensure_ws(h, W, H, stride);
+    if (rc) return rc;
+    h->W = W;
+    h->H = H;
+    const Layout L = layout(W, H, stride);
+    const size_t N = L.N;
+    cudaStream_t st = 0;
+    uint8_t* dl = at<uint8_t>(h->ws, L, Layout::img0);
+    uint8_t* dr = at<uint8_t>(h->ws, L, Layout::img1);
+    float* dd = at<float>(h->ws, L, Layout::dmap);
+    float4* dn = at<float4>(h->ws, L, Layout::nmap);
+    float* di = at<float>(h->ws, L, Layout::initd);
+    float4* dni = at<float4>(h->ws, L, Layout::initn);
+    float4* pl = at<float4>(h->ws, L, Layout::mL0);   // overwritten only after the copy below
+    PM_CUDA(h, cudaMemcpyAsync(dl, left, stride * H, cudaMemcpyHostToDevice, st));
+    PM_CUDA(h, cudaMemcpyAsync(dr, right, stride * H, cudaMemcpyHostToDevice, st));
+    if (initdisp) PM_CUDA(h, cudaMemcpyAsync(di, initdisp, N * 4, cudaMemcpyHostToDevice, st));
+    if (initnormal) PM_CUDA(h, cudaMemcpyAsync(dni, initnormal, N * 16, cudaMemcpyHostToDevice, st));
+    (void)pl;
+    rc = run_pipeline(h, dl, dr, W, H, stride, patchsize, dispmax, iterations, pp, dmap ? dd : nullptr,
+                      normalmap ? dn : nullptr, initdisp ? di : nullptr, initnormal ? dni : nullptr, nullptr, nullptr, st);
+    if (rc) return rc;
+    if (dmap) PM_CUDA(h, cudaMemcpyAsync(dmap, dd, N * 4, cudaMemcpyDeviceToHost, st));
+    if (normalmap) PM_CUDA(h, cudaMemcpyAsync(normalmap, dn, N * 16, cudaMemcpyDeviceToHost, st));
+    if (planes_left) PM_CUDA(h, cudaMemcpyAsync(planes_left, at<float4>(h->ws, L, Layout::mL1), N * 16, cudaMemcpyDeviceToHost, st));
+    if (planes_right && h->opt.views == 2)
+        PM_CUDA(h, cudaMemcpyAsync(planes_right, at<float4>(h->ws, L, Layout::mR1), N * 16, cudaMemcpyDeviceToHost, st));
+    if (h->counting) {
+        unsigned long long c[4];
+        PM_CUDA(h, cudaMemcpyAsync(c, at<unsigned long long>(h->ws, L, Layout::ctr), 32, cudaMemcpyDeviceToHost, st));
+        PM_CUDA(h, cudaStreamSynchronize(st));
+        for (int k = 0; k < 4; k++) h->counters[k] = c[k];
+    }
+    int errv = 0;
+    PM_CUDA(h, cudaMemcpyAsync(&errv, at<int>(h->ws, L, Layout::errf), 4, cudaMemcpyDeviceToHost, st));
+    PM_CUDA(h, cudaStreamSynchronize(st));
+    if (errv) return fail(h, PM_ETIMEOUT, "view-buffer insertion retried too often");
+    return PM_OK;
+}
+
+int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* left, const uint8_t* const* right,
+                                  const int* width, const int* height, const size_t* stride, const int* patchsize,
+                                  const float* dispmax, int iterations, int pp, float* const* dmap,
+                                  float* const* planes_left, float* const* planes_right, void* stream)
+{
+    (void)n; (void)left; (void)right; (void)width; (void)height; (void)stride; (void)patchsize; (void)dispmax;
+    (void)iterations; (void)pp; (void)dmap; (void)planes_left; (void)planes_right; (void)stream;
+    return fail(h, PM_ENOTIMPL, "batched form not built yet");
+}
+
+// ---- per-kernel entry points ------------------------------------------------------------
+
+int pm_k_prep(const uint8_t* img, int W, int H, size_t stride, int r, int fused, float* bw, float* grad, float* dt,
+              void* stream)
+{
+    int rc = check_shape(nullptr, W, H, r);
+    if (rc) return rc;
+    if (!img || stride < (size_t)W * 4 || stride % 4) return fail(nullptr, PM_EINVAL_ARG, "bad image");
+    launch_prep(img, stride, W, H, r, fused, (float4*)bw, (float4*)grad, (float4*)dt, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_init(float* out, const float* bw1, const float* bw2, const float* g1, const float* g2, int W, int H, int r,
+              float dmax, int lr, const float* initdisp, const float* initnormal, int fused, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, r);
+    if (rc) return rc;
+    if (!out || !bw1 || !bw2 || !g1 || !g2 || (initdisp && !initnormal)) return fail(nullptr, PM_EINVAL_ARG, "null argument");
+    const ViewData V = {(const float4*)bw1, (const float4*)bw2, (const float4*)g1, (const float4*)g2, W, H, r};
+    launch_init((float4*)out, V, dmax, lr, initdisp, (const float4*)initnormal, fused, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_cost(float* cost, const float* planes, const float* bw1, const float* bw2, const float* g1, const float* g2,
+              int W, int H, int r, float mincost, int fused, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, r);
+    if (rc) return rc;
+    if (!cost || !planes || !bw1 || !bw2 || !g1 || !g2) return fail(nullptr, PM_EINVAL_ARG, "null argument");
+    const ViewData V = {(const float4*)bw1, (const float4*)bw2, (const float4*)g1, (const float4*)g2, W, H, r};
+    launch_cost(cost, (const float4*)planes, V, mincost, fused, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_klt(float* out, const float* planes, const float* bw1, const float* bw2, const float* g1, const float* g2,
+             int W, int H, int r, int fused, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, r);
+    if (rc) return rc;
+    if (!out || !planes || !bw1 || !bw2 || !g1 || !g2) return fail(nullptr, PM_EINVAL_ARG, "null argument");
+    const ViewData V = {(const float4*)bw1, (const float4*)bw2, (const float4*)g1, (const float4*)g2, W, H, r};
+    launch_klt((float4*)out, (const float4*)planes, V, fused, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_propagate(float* out, const float* old, const float* bw1, const float* bw2, const float* g1, const float* g2,
+                   const float* smooth, float theta, int W, int H, int r, float dmax, int lr, int iter,
+                   int32_t* vin_count, uint64_t* vin_src, const float* vin_planes, int32_t* vout_count,
+                   uint64_t* vout_src, int fused, uint64_t* counters, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, r);
+    if (rc) return rc;
+    if (!out || !old || !bw1 || !bw2 || !g1 || !g2 || !smooth) return fail(nullptr, PM_EINVAL_ARG, "null argument");
+    if (vin_count && (!vin_src || !vin_planes)) return fail(nullptr, PM_EINVAL_ARG, "incomplete input view buffer");
+    if (vout_count && !vout_src) return fail(nullptr, PM_EINVAL_ARG, "incomplete output view buffer");
+    static int* d_err = nullptr;
+    if (!d_err) PM_CUDA(nullptr, cudaMalloc(&d_err, sizeof(int)));
+    PropParams P;
+    P.V = {(const float4*)bw1, (const float4*)bw2, (const float4*)g1, (const float4*)g2, W, H, r};
+    P.out = (float4*)out;
+    P.old = (const float4*)old;
+    P.smooth = (const float4*)smooth;
+    P.theta = theta;
+    P.dmax = dmax;
+    P.lr = lr;
+    P.iter = iter;
+    P.vin_count = vin_count;
+    P.vin_src = (unsigned long long*)vin_src;
+    P.vin_planes = (const float4*)vin_planes;
+    P.vout_count = vout_count;
+    P.vout_src = (unsigned long long*)vout_src;
+    P.counters = (unsigned long long*)counters;
+    P.error = d_err;
+    launch_propagate(P, fused, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_normal_depth(float* out, const float* planes, int W, int H, float dispscale, int lr, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    launch_normal_depth((float4*)out, (const float4*)planes, W, H, dispscale, lr, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+size_t pm_rof_scratch_bytes(int W, int H) { return rof_scratch_bytes(W, H); }
+
+int pm_k_rof(float* out, const float* input, const float* dt, const float lambda[4], int iters, int W, int H,
+             void* scratch, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    if (!out || !input || !dt || !lambda || !scratch || out == input) return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    launch_rof((float4*)out, (const float4*)input, (const float4*)dt,
+               make_float4(lambda[0], lambda[1], lambda[2], lambda[3]), iters, W, H, scratch, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_consistency(float* out, const float* left, const float* right, int W, int H, float maxdd, float maxad,
+                     void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    launch_consistency((float4*)out, (const float4*)left, (const float4*)right, W, H, maxdd, maxad, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_to_disparity(float* out, const float* planes, int W, int H, float scale, int lr, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    launch_to_disparity(out, (const float4*)planes, W, H, scale, lr, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_fill_depthmap(float* out, const float* planes, int W, int H, float scale, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    launch_fill_depthmap(out, (const float4*)planes, W, H, scale, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_fill_normalmap(float* out, const float* planes, int W, int H, int lr, void* stream)
+{
+    (void)lr;
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    launch_fill_normalmap((float4*)out, (const float4*)planes, W, H, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_disparity_to_normal(float* out, const float* disp, int W, int H, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    launch_disparity_to_normal((float4*)out, disp, W, H, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+// ---- host evaluation of the shared arithmetic -----------------------------------------
+
+int pm_rng_floats(int64_t linpos, int nd, int n, float* out)
+{
+    if (!out || n < 0) return PM_EINVAL_ARG;
+    Rng r;
+    r.init_skip((int)linpos * nd);
+    for (int i = 0; i < n; i++) out[i] = r.next();
+    return PM_OK;
+}
+float pm_expf_host(float x) { return expf_(x); }
+float pm_sinf_host(float x) { float s, c; sincosf_(x, &s, &c); return s; }
+float pm_cosf_host(float x) { float s, c; sincosf_(x, &s, &c); return c; }
+float pm_acospif_host(float x) { return acospif_(x); }
+float pm_exit_threshold_host(float m, float b) { return exit_threshold(m, b); }
+
+}  // extern "C"

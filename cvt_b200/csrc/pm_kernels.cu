@@ -1,0 +1,565 @@
+// CUDA kernels of the PatchMatch-Huber stereo path for sm_100a, and their
+// launchers.  One thread handles one pixel; the window loops run in the
+// reference's sample order so that every sum rounds exactly as the reference's
+// does.  Compile with -fmad=false: the only fused operations are the explicit
+// fmaf() of the hot sites (template parameter F).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "pm_device.cuh"
+#include "pm_kernels.h"
+
+namespace pm {
+
+namespace {
+
+__device__ __forceinline__ float u8f(uint8_t v) { return (float)v / 255.0f; }
+
+// RGBA8 texel as read by read_imagef on CL_UNORM_INT8 (value / 255)
+__device__ __forceinline__ float4 rgba_at(const uint8_t* __restrict__ img, size_t stride, int x, int y)
+{
+    const uchar4 c = __ldg(reinterpret_cast<const uchar4*>(img + (size_t)y * stride) + x);
+    return f4(u8f(c.x), u8f(c.y), u8f(c.z), u8f(c.w));
+}
+
+// grey value dot(rgba, (0.2126, 0.7152, 0.0722, 0)) with CLK_ADDRESS_CLAMP's zero border
+// (pmhstereo.cl:1569-1573, PDDiffTensor.cl:41-45)
+__device__ __forceinline__ float gray_zero(const uint8_t* __restrict__ img, size_t stride, int W, int H, int x, int y)
+{
+    if (x < 0 || x >= W || y < 0 || y >= H) return 0.0f;
+    const float4 v = rgba_at(img, stride, x, y);
+    return v.x * PM_GW_R + v.y * PM_GW_G + v.z * PM_GW_B + v.w * 0.0f;
+}
+
+template <bool F>
+__global__ void k_prep(const uint8_t* __restrict__ img, size_t stride, int W, int H, int r, float4* __restrict__ bw,
+                       float4* __restrict__ grad, float4* __restrict__ dt)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const size_t i = (size_t)y * W + x;
+    if (bw) {
+        // pmhstereo_bilateral_weight_to_alpha (pmhstereo.cl:1462-1498)
+        const float4 c = rgba_at(img, stride, x, y);
+        float wsum = 0.0f;
+        for (int dy = max(-r, -y); dy <= min(r, H - 1 - y); dy++)
+            for (int dx = max(-r, -x); dx <= min(r, W - 1 - x); dx++) {
+                const float4 v = rgba_at(img, stride, x + dx, y + dy);
+                wsum += support_weight<F>(v.x - c.x, v.y - c.y, v.z - c.z);
+            }
+        bw[i] = f4(c.x, c.y, c.z, wsum);
+    }
+    const float g = gray_zero(img, stride, W, H, x, y);
+    const float gxp = gray_zero(img, stride, W, H, x + 1, y), gyp = gray_zero(img, stride, W, H, x, y + 1);
+    if (grad) {
+        // pmhstereo_gradxy (:1584-1601)
+        const float gxm = gray_zero(img, stride, W, H, x - 1, y), gym = gray_zero(img, stride, W, H, x, y - 1);
+        grad[i] = f4(gxp - g, gyp - g, gxp - gxm, gyp - gym);
+    }
+    if (dt) {
+        // PDDiffTensorColor (PDDiffTensor.cl:52-72), alpha 24, beta 1 (PMHuberStereo.cpp:416-417)
+        float dx = gxp - g, dy = gyp - g;
+        const float len = sqrtf(dx * dx + dy * dy);
+        const float w = expf_(-24.0f * len);
+        float4 d;
+        if (len <= 0.001f) {
+            d = f4(1.0f, 0.0f, 0.0f, 1.0f);
+        } else {
+            dx = dx / len;
+            dy = dy / len;
+            const float dxo = dy, dyo = -dx;
+            d = f4(w * dx * dx + dxo * dxo, w * dx * dy + dxo * dyo, w * dy * dx + dyo * dxo, w * dy * dy + dyo * dyo);
+        }
+        dt[i] = d;
+    }
+}
+
+template <bool F>
+__global__ void k_init(float4* __restrict__ out, ViewData V, float dmax, int lr, const float* __restrict__ initdisp,
+                       const float4* __restrict__ initnormal)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= V.W || y >= V.H) return;
+    const size_t i = (size_t)y * V.W + x;
+    const float cx = (float)x, cy = (float)y;
+    Rng rng;
+    rng.init_skip((y * V.W + x) * 3);   // RNG_init(&rng, lin, 3), pmhstereo.cl:766
+    float4 ret;
+    const float disparity = initdisp ? initdisp[i] : 0.0f;
+    if (initdisp && disparity > 0 && lr) {
+        const float4 n = initnormal[i];
+        ret = from_disparity_normal(cx, cy, disparity, normalize3(make_float3(n.x, n.y, n.z)));
+    } else if (initdisp && disparity > 0 && !lr) {
+        const float4 n = initnormal[i];
+        ret = from_disparity_normal(cx, cy, -disparity, normalize3(make_float3(n.x, n.y, n.z)));
+    } else {
+        ret = nd_state_init(rng, cx, cy, lr, dmax);
+    }
+    Counters cnt = {0, 0, 0, 0};
+    ret.w = patch_eval<F, false>(V, x, y, ret, 1e10f, cnt);
+    out[i] = ret;
+}
+
+template <bool F>
+__global__ void k_cost(float* __restrict__ cost, const float4* __restrict__ planes, ViewData V, float mincost)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= V.W || y >= V.H) return;
+    const size_t i = (size_t)y * V.W + x;
+    Counters cnt = {0, 0, 0, 0};
+    cost[i] = patch_eval<F, false>(V, x, y, planes[i], mincost, cnt);
+}
+
+template <bool F>
+__global__ void k_klt(float4* __restrict__ out, const float4* __restrict__ planes, ViewData V)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= V.W || y >= V.H) return;
+    const size_t i = (size_t)y * V.W + x;
+    Counters cnt = {0, 0, 0, 0};
+    out[i] = klt2<F, false>(V, x, y, planes[i], cnt);
+}
+
+// keep the two smallest source columns of a view-buffer entry (see pm_kernels.h)
+__device__ __forceinline__ bool view_insert(unsigned long long* slot, unsigned int x)
+{
+    unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(slot);
+    for (int guard = 0; guard < 4096; guard++) {
+        const unsigned int lo = (unsigned int)cur, hi = (unsigned int)(cur >> 32);
+        unsigned long long nv;
+        if (x < lo) nv = ((unsigned long long)lo << 32) | x;
+        else if (x < hi) nv = ((unsigned long long)x << 32) | lo;
+        else return true;
+        const unsigned long long prev = atomicCAS(slot, cur, nv);
+        if (prev == cur) return true;
+        cur = prev;
+    }
+    return false;
+}
+
+template <bool F, bool COUNT>
+__device__ __forceinline__ void try_candidate(const ViewData& V, int px, int py, float4& self, float4 nb, float4 smooth,
+                                              float theta, float dmax, int lr, Counters& cnt)
+{
+    const float cx = (float)px, cy = (float)py;
+    // smoothDistance does not read the cost component, so one evaluation serves both
+    // minimalCost (:873-877) and the acceptance test
+    const float2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
+    const float mincost = self.w + theta * sd.y - theta * sd.x;
+    nb.w = patch_eval<F, COUNT>(V, px, py, nb, mincost, cnt);
+    if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
+}
+
+template <bool F, bool COUNT>
+__global__ void __launch_bounds__(128) k_propagate(PropParams P)
+{
+    const ViewData& V = P.V;
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+    Counters cnt = {0, 0, 0, 0};
+    if (px < V.W && py < V.H) {
+        const int W = V.W;
+        const size_t idx = (size_t)py * W + px;
+        const float cx = (float)px, cy = (float)py;
+        const int lr = P.lr;
+        const float theta = P.theta, dmax = P.dmax;
+        // pmhstereo_propagate_view (pmhstereo.cl:927-940)
+        float4 smooth = P.smooth[idx];
+        smooth.w = clampf(smooth.w, 0.0f, 1.0f) * dmax;
+        float4 self = P.old[idx];
+        self.w = patch_eval<F, COUNT>(V, px, py, self, 1e10f, cnt);
+
+        // cross-view candidates of this pixel; the entry is emptied for the next writer
+        int nview = 0;
+        unsigned long long vsrc = ~0ULL;
+        if (P.vin_count) {
+            nview = P.vin_count[idx];
+            vsrc = P.vin_src[idx];
+            P.vin_count[idx] = 0;
+            P.vin_src[idx] = ~0ULL;
+            nview = min(nview, 2);
+        }
+
+        Rng rng;
+        // RNG_init(&rng, lin, ((1*1 - 1) + NUMRNDTRIES) * 3 + 2 * NUMRNDSAMPLE) (:942) expands to
+        // (lin) * ((1*1 - 1) + 2) * 3 + 2 * 4 = 6 * lin + 8
+        rng.init_skip((py * W + px + P.iter) * 6 + 8);
+
+        // smooth candidate (:968-976)
+        float4 nb = from_disparity_normal(cx, cy, smooth.w * (lr ? -1.0f : 1.0f),
+                                          normalize3(make_float3(smooth.x, smooth.y, smooth.z)));
+        if (!lr) nb = viewprop(nb);
+        try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+
+        // random neighbourhood (:982-991), offsets drawn x first, in [-4, 5]
+        for (int i = 0; i < 4; i++) {
+            const int ox = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
+            const int oy = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
+            const int nx = min(max(px + ox, 0), W - 1), ny = min(max(py + oy, 0), V.H - 1);
+            nb = P.old[(size_t)ny * W + nx];
+            try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+        }
+
+        // random plane (:996-1002)
+        nb = nd_state_init(rng, cx, cy, lr, dmax);
+        try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+
+        // other view (:1007-1016): planes of the kept source columns, mapped into this view
+        for (int i = 0; i < nview; i++) {
+            const unsigned int sx = i == 0 ? (unsigned int)vsrc : (unsigned int)(vsrc >> 32);
+            nb = viewprop(P.vin_planes[(size_t)py * W + sx]);
+            try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+        }
+
+        // randomized refinement (:1021-1028)
+        nb = nd_state_refine(rng, self, cx, cy, dmax, lr);
+        try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+
+        // Gauss-Newton plane steps (:1034-1053)
+        nb = klt2<F, COUNT>(V, px, py, self, cnt);
+        for (int k = 0; k < 5; k++) nb = klt2<F, COUNT>(V, px, py, nb, cnt);
+        try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+
+        // view scatter (:1060-1067)
+        if (P.vout_count) {
+            const float sidesign = lr ? -1.0f : 1.0f;
+            const float tx = transform_x(self, cx, cy);
+            const int xpv = __float2int_rn(tx);
+            const int disp = (int)((tx - cx) * sidesign);
+            if (xpv >= 0 && xpv < W && disp > 0) {
+                const size_t t = (size_t)py * W + xpv;
+                atomicAdd(P.vout_count + t, 1);
+                if (!view_insert(P.vout_src + t, (unsigned int)px)) atomicAdd(P.error, 1);
+            }
+        }
+        P.out[idx] = self;
+    }
+    if (COUNT) {
+        unsigned long long v[4] = {cnt.eval, cnt.klt, cnt.calls, cnt.exits};
+        for (int k = 0; k < 4; k++) {
+            unsigned long long s = v[k];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) == 0 && s) atomicAdd(P.counters + k, s);
+        }
+    }
+}
+
+__global__ void k_normal_depth(float4* __restrict__ out, const float4* __restrict__ planes, int W, int H,
+                               float dispscale, int lr)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const size_t i = (size_t)y * W + x;
+    float4 v = to_ref_normal_depth(planes[i], (float)x, (float)y, lr);   // pmhstereo.cl:1397-1399
+    v.w = v.w * dispscale;
+    out[i] = v;
+}
+
+// tensor-weighted, projected dual of PDDROFDiffTensor (PDDROFDiffTensor.cl:72-100) at
+// pixel (x, y); outside the image the tensor and the previous dual read as 0
+struct Dual { float4 lo, hi; };
+__device__ __forceinline__ Dual rof_dual(const float4* __restrict__ u, const float4* __restrict__ p,
+                                         const float4* __restrict__ dt, int W, int H, int x, int y, bool first)
+{
+    const int xc = min(max(x, 0), W - 1), yc = min(max(y, 0), H - 1);
+    const int xp = min(max(x + 1, 0), W - 1), yp = min(max(y + 1, 0), H - 1);
+    const float4 uc = u[(size_t)yc * W + xc], ux = u[(size_t)yc * W + xp], uy = u[(size_t)yp * W + xc];
+    const bool inside = x >= 0 && x < W && y >= 0 && y < H;
+    const float4 D = inside ? dt[(size_t)y * W + x] : f4(0, 0, 0, 0);
+    float4 plo = f4(0, 0, 0, 0), phi = f4(0, 0, 0, 0);
+    if (inside && !first) { plo = p[(size_t)y * 2 * W + 2 * x]; phi = p[(size_t)y * 2 * W + 2 * x + 1]; }
+    const float dxv[4] = {uc.x - ux.x, uc.y - ux.y, uc.z - ux.z, uc.w - ux.w};
+    const float dyv[4] = {uc.x - uy.x, uc.y - uy.y, uc.z - uy.z, uc.w - uy.w};
+    const float pl[4] = {plo.x, plo.y, plo.z, plo.w}, ph[4] = {phi.x, phi.y, phi.z, phi.w};
+    float a[4], b[4], nrm[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const float DTdx = D.x * dxv[c] + D.z * dyv[c];
+        const float DTdy = D.y * dxv[c] + D.w * dyv[c];
+        a[c] = pl[c] + 4.0f * DTdx;   // SIGMA
+        b[c] = ph[c] + 4.0f * DTdy;
+        nrm[c] = a[c] * a[c] + b[c] * b[c];
+    }
+    const float n3 = sqrtf(nrm[0] * 1.0f + nrm[1] * 1.0f + nrm[2] * 1.0f);
+    const float n4 = sqrtf(nrm[3]);
+    const float pr[4] = {fmaxf(1.0f, n3), fmaxf(1.0f, n3), fmaxf(1.0f, n3), fmaxf(1.0f, n4)};
+    float l[4], h[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        a[c] = a[c] / pr[c];
+        b[c] = b[c] / pr[c];
+        l[c] = D.x * a[c] + D.z * b[c];
+        h[c] = D.y * a[c] + D.w * b[c];
+    }
+    Dual d;
+    d.lo = f4(l[0], l[1], l[2], l[3]);
+    d.hi = f4(h[0], h[1], h[2], h[3]);
+    return d;
+}
+
+// one primal-dual step (PDDROFDiffTensor.cl:102-126); first: p = q = 0
+__global__ void k_rof_step(float4* __restrict__ unew, float4* __restrict__ pnew, float4* __restrict__ qnew,
+                           const float4* __restrict__ u, const float4* __restrict__ p, const float4* __restrict__ q,
+                           const float4* __restrict__ img, const float4* __restrict__ dt, float4 lam, int W, int H,
+                           int first)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const Dual c = rof_dual(u, p, dt, W, H, x, y, first);
+    const Dual l = rof_dual(u, p, dt, W, H, x - 1, y, first);
+    const Dual t = rof_dual(u, p, dt, W, H, x, y - 1, first);
+    const size_t i = (size_t)y * W + x;
+    const float4 im = img[i], uu = u[i];
+    const float4 qq = first ? f4(0, 0, 0, 0) : q[i];
+    const float div[4] = {c.lo.x - l.lo.x + c.hi.x - t.hi.x, c.lo.y - l.lo.y + c.hi.y - t.hi.y,
+                          c.lo.z - l.lo.z + c.hi.z - t.hi.z, c.lo.w - l.lo.w + c.hi.w - t.hi.w};
+    const float imv[4] = {im.x, im.y, im.z, im.w}, qv[4] = {qq.x, qq.y, qq.z, qq.w}, uv[4] = {uu.x, uu.y, uu.z, uu.w};
+    const float lm[4] = {lam.x, lam.y, lam.z, lam.w};
+    float on[4], qn[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float o = (uv[k] + 0.05f * (lm[k] * imv[k] - div[k] - qv[k])) / (1.0f + 0.05f * lm[k]);   // TAU
+        o = o + 0.5f * (o - uv[k]);                                                               // THETA
+        float qn_ = (qv[k] + 8.0f * (o - imv[k])) / (1.0f + 4.0f * 8.0f / lm[k]);                 // ETA
+        qn_ = qn_ + 0.5f * (qn_ - qv[k]);
+        on[k] = o;
+        qn[k] = qn_;
+    }
+    unew[i] = f4(on[0], on[1], on[2], on[3]);
+    qnew[i] = f4(qn[0], qn[1], qn[2], qn[3]);
+    pnew[(size_t)y * 2 * W + 2 * x] = c.lo;
+    pnew[(size_t)y * 2 * W + 2 * x + 1] = c.hi;
+}
+
+__global__ void k_consistency(float4* __restrict__ out, const float4* __restrict__ L, const float4* __restrict__ R,
+                              int W, int H, float maxdd, float maxad)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const size_t i = (size_t)y * W + x;
+    // pmhstereo_consistency (pmhstereo.cl:1107-1128)
+    const float4 sl = L[i];
+    const float c2x = transform_x(sl, (float)x, (float)y), c2y = (float)y;
+    float4 val = f4(0.0f, 0.0f, 0.0f, -1.0f);
+    if (ceilf(c2x) >= 0 && floorf(c2x) < (float)W) {
+        const int x1 = min(max(__float2int_rn(floorf(c2x)), 0), W - 1);
+        const int x2 = min(max(__float2int_rn(ceilf(c2x)), 0), W - 1);
+        const float4 sr = R[(size_t)y * W + x1], sr2 = R[(size_t)y * W + x2];
+        const float3 nl = to_normal(sl), n1 = to_normal(viewprop(sr)), n2 = to_normal(viewprop(sr2));
+        const float nd = nl.x * n1.x + nl.y * n1.y + nl.z * n1.z;
+        const float nd2 = nl.x * n2.x + nl.y * n2.y + nl.z * n2.z;
+        const float d1 = fabsf((float)x - transform_x(sr, c2x, c2y));
+        const float d2 = fabsf((float)x - transform_x(sr2, c2x, c2y));
+        const float lim = maxad / 180.0f;
+        if (!(d1 >= maxdd || acospif_(clampf(nd, -1.0f, 1.0f)) >= lim) ||
+            !(d2 >= maxdd || acospif_(clampf(nd2, -1.0f, 1.0f)) >= lim))
+            val = sl;
+    }
+    out[i] = val;
+}
+
+__device__ __forceinline__ float length3(float4 v) { return sqrtf(v.x * v.x + v.y * v.y + v.z * v.z); }
+
+__global__ void k_to_disparity(float* __restrict__ out, const float4* __restrict__ planes, int W, int H, float scale,
+                               int lr)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const size_t i = (size_t)y * W + x;
+    // pmhstereo_to_disparity (pmhstereo.cl:1243-1256)
+    const float4 s = planes[i];
+    const float disp = (transform_x(s, (float)x, (float)y) - (float)x) * (lr ? -1.0f : 1.0f);
+    float v;
+    if (length3(s) < 1e-4f || disp < 0 || disp > (float)W) v = 0.0f;
+    else v = fmaxf(disp, 0.0f);
+    out[i] = v * scale;
+}
+
+// the row search of pmhstereo_fill_depthmap / pmhstereo_fill_normalmap (:1199-1218, :1271-1290)
+__device__ __forceinline__ void fill_neighbours(const float4* __restrict__ row, int W, int x, float cx, float cy,
+                                                float4& l, float4& r)
+{
+    l = f4(0, 0, 0, 0);
+    for (int xx = x - 1; length3(l) < 1e-1f && xx >= 0; xx--) l = row[xx];
+    r = f4(0, 0, 0, 0);
+    for (int xx = x + 1; length3(r) < 1e-1f && xx < W; xx++) r = row[xx];
+    if (length3(l) < 1e-1f) { l.x = l.y = l.z = -1e5f; }
+    if (length3(r) < 1e-1f) { r.x = r.y = r.z = -1e5f; }
+    l.w = -(transform_x(l, cx, cy) - cx);
+    r.w = -(transform_x(r, cx, cy) - cx);
+}
+
+__global__ void k_fill_depthmap(float* __restrict__ out, const float4* __restrict__ planes, int W, int H, float scale)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const float4* row = planes + (size_t)y * W;
+    const float4 s = row[x];
+    const float cx = (float)x, cy = (float)y;
+    float v;
+    if (length3(s) < 1e-4f) {
+        float4 l, r;
+        fill_neighbours(row, W, x, cx, cy, l, r);
+        v = fminf(l.w, r.w);
+    } else {
+        v = fabsf(transform_x(s, cx, cy) - cx);
+    }
+    out[(size_t)y * W + x] = v * scale;
+}
+
+__global__ void k_fill_normalmap(float4* __restrict__ out, const float4* __restrict__ planes, int W, int H)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const float4* row = planes + (size_t)y * W;
+    const float4 s = row[x];
+    const float cx = (float)x, cy = (float)y;
+    float3 n;
+    if (length3(s) < 1e-1f) {
+        float4 l, r;
+        fill_neighbours(row, W, x, cx, cy, l, r);
+        n = (l.w < r.w) ? to_normal(l) : to_normal(r);
+    } else {
+        n = to_normal(s);
+    }
+    out[(size_t)y * W + x] = f4(n.x, n.y, n.z, 0.0f);
+}
+
+__global__ void k_disparity_to_normal(float4* __restrict__ out, const float* __restrict__ d, int W, int H)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    // pmhstereo_disparity_to_normal (pmhstereo.cl:1619-1636), zero border
+    auto at = [&](int xx, int yy) { return (xx < 0 || xx >= W || yy < 0 || yy >= H) ? 0.0f : d[(size_t)yy * W + xx]; };
+    const float dx = at(x + 1, y) - at(x, y);
+    const float dy = at(x, y + 1) - at(x, y);
+    const float3 n = normalize3(make_float3(0.0f * dy - dx * 1.0f, dx * 0.0f - 1.0f * dy, 1.0f * 1.0f - 0.0f * 0.0f));
+    out[(size_t)y * W + x] = f4(n.x, n.y, n.z, 0.0f);
+}
+
+__global__ void k_view_clear(int* __restrict__ count, unsigned long long* __restrict__ src, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        count[i] = 0;
+        src[i] = ~0ULL;
+    }
+}
+
+inline dim3 grid2d(int W, int H, dim3 b) { return dim3((W + b.x - 1) / b.x, (H + b.y - 1) / b.y); }
+
+}  // namespace
+
+// ---- launchers ----------------------------------------------------------------------
+
+void launch_prep(const uint8_t* img, size_t stride, int W, int H, int r, int fused, float4* bw, float4* grad,
+                 float4* dt, cudaStream_t st)
+{
+    const dim3 b(32, 4);
+    if (fused) k_prep<true><<<grid2d(W, H, b), b, 0, st>>>(img, stride, W, H, r, bw, grad, dt);
+    else k_prep<false><<<grid2d(W, H, b), b, 0, st>>>(img, stride, W, H, r, bw, grad, dt);
+}
+
+void launch_init(float4* out, const ViewData& V, float dmax, int lr, const float* initdisp, const float4* initnormal,
+                 int fused, cudaStream_t st)
+{
+    const dim3 b(32, 4);
+    if (fused) k_init<true><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal);
+    else k_init<false><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal);
+}
+
+void launch_cost(float* cost, const float4* planes, const ViewData& V, float mincost, int fused, cudaStream_t st)
+{
+    const dim3 b(32, 4);
+    if (fused) k_cost<true><<<grid2d(V.W, V.H, b), b, 0, st>>>(cost, planes, V, mincost);
+    else k_cost<false><<<grid2d(V.W, V.H, b), b, 0, st>>>(cost, planes, V, mincost);
+}
+
+void launch_klt(float4* out, const float4* planes, const ViewData& V, int fused, cudaStream_t st)
+{
+    const dim3 b(32, 4);
+    if (fused) k_klt<true><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, planes, V);
+    else k_klt<false><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, planes, V);
+}
+
+void launch_propagate(const PropParams& P, int fused, cudaStream_t st)
+{
+    const dim3 b(32, 4);
+    const dim3 g = grid2d(P.V.W, P.V.H, b);
+    const bool count = P.counters != nullptr;
+    if (fused) {
+        if (count) k_propagate<true, true><<<g, b, 0, st>>>(P);
+        else k_propagate<true, false><<<g, b, 0, st>>>(P);
+    } else {
+        if (count) k_propagate<false, true><<<g, b, 0, st>>>(P);
+        else k_propagate<false, false><<<g, b, 0, st>>>(P);
+    }
+}
+
+void launch_normal_depth(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    k_normal_depth<<<grid2d(W, H, b), b, 0, st>>>(out, planes, W, H, dispscale, lr);
+}
+
+size_t rof_scratch_bytes(int W, int H) { return (size_t)W * H * sizeof(float4) * (1 + 2 + 2 + 1 + 1); }
+
+void launch_rof(float4* out, const float4* input, const float4* dt, float4 lam, int iters, int W, int H, void* scratch,
+                cudaStream_t st)
+{
+    const size_t N = (size_t)W * H;
+    float4* ut = static_cast<float4*>(scratch);
+    float4* p[2] = {ut + N, ut + 3 * N};
+    float4* q[2] = {ut + 5 * N, ut + 6 * N};
+    // PDOptCL.cpp:1137-1166: `iters` steps, plus one when the last left the result in the scratch image
+    const int steps = (iters > 0 && iters % 2 == 0) ? iters : iters + 1;
+    // step k writes `out` when (steps - 1 - k) is even, so that the last step lands in `out`
+    const dim3 b(32, 8), g = grid2d(W, H, b);
+    const float4* ucur = input;
+    for (int k = 0; k < steps; k++) {
+        float4* unew = ((steps - 1 - k) % 2 == 0) ? out : ut;
+        const int pi = k & 1;
+        k_rof_step<<<g, b, 0, st>>>(unew, p[pi], q[pi], ucur, p[1 - pi], q[1 - pi], input, dt, lam, W, H, k == 0);
+        ucur = unew;
+    }
+}
+
+void launch_consistency(float4* out, const float4* L, const float4* R, int W, int H, float maxdd, float maxad,
+                        cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    k_consistency<<<grid2d(W, H, b), b, 0, st>>>(out, L, R, W, H, maxdd, maxad);
+}
+
+void launch_to_disparity(float* out, const float4* planes, int W, int H, float scale, int lr, cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    k_to_disparity<<<grid2d(W, H, b), b, 0, st>>>(out, planes, W, H, scale, lr);
+}
+
+void launch_fill_depthmap(float* out, const float4* planes, int W, int H, float scale, cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    k_fill_depthmap<<<grid2d(W, H, b), b, 0, st>>>(out, planes, W, H, scale);
+}
+
+void launch_fill_normalmap(float4* out, const float4* planes, int W, int H, cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    k_fill_normalmap<<<grid2d(W, H, b), b, 0, st>>>(out, planes, W, H);
+}
+
+void launch_disparity_to_normal(float4* out, const float* d, int W, int H, cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    k_disparity_to_normal<<<grid2d(W, H, b), b, 0, st>>>(out, d, W, H);
+}
+
+void launch_view_clear(int* count, unsigned long long* src, size_t n, cudaStream_t st)
+{
+    const int threads = 256;
+    const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 8);
+    k_view_clear<<<blocks > 0 ? blocks : 1, threads, 0, st>>>(count, src, n);
+}
+
+}  // namespace pm

@@ -1,0 +1,58 @@
+// Launchers of the PatchMatch-Huber kernels (pm_kernels.cu).  All pointers are
+// device pointers; every launcher only enqueues work on the given stream.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "pm_device.cuh"
+
+namespace pm {
+
+// Arguments of one pmhstereo_propagate_view launch (pmhstereo.cl:880-884).
+// View buffer (VIEWPROP_t, :830-833): per pixel a count of appended candidates and
+// the two smallest source columns appended so far (low / high 32 bits, 0xffffffff
+// when absent).  Keeping the two smallest columns reproduces the sequential
+// executor's append order (sources of one target share its row, and a sequential
+// executor appends them in ascending column order); the candidate plane itself is
+// read back from the source view's output field, which holds the same `self` the
+// reference stores (:1066).
+struct PropParams {
+    float4* out;
+    const float4* old;
+    ViewData V;
+    const float4* smooth;
+    float theta;
+    float dmax;
+    int lr;
+    int iter;
+    int* vin_count;                 // may be null: no cross-view candidates
+    unsigned long long* vin_src;
+    const float4* vin_planes;       // the other view's plane field that vin refers to
+    int* vout_count;                // may be null: no scatter
+    unsigned long long* vout_src;
+    unsigned long long* counters;   // null: not counted
+    int* error;                     // incremented if a view-buffer insert gave up
+};
+
+void launch_prep(const uint8_t* img, size_t stride, int W, int H, int r, int fused, float4* bw, float4* grad,
+                 float4* dt, cudaStream_t st);
+void launch_init(float4* out, const ViewData& V, float dmax, int lr, const float* initdisp, const float4* initnormal,
+                 int fused, cudaStream_t st);
+void launch_cost(float* cost, const float4* planes, const ViewData& V, float mincost, int fused, cudaStream_t st);
+void launch_klt(float4* out, const float4* planes, const ViewData& V, int fused, cudaStream_t st);
+void launch_propagate(const PropParams& P, int fused, cudaStream_t st);
+void launch_normal_depth(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st);
+size_t rof_scratch_bytes(int W, int H);
+void launch_rof(float4* out, const float4* input, const float4* dt, float4 lam, int iters, int W, int H, void* scratch,
+                cudaStream_t st);
+void launch_consistency(float4* out, const float4* L, const float4* R, int W, int H, float maxdd, float maxad,
+                        cudaStream_t st);
+void launch_to_disparity(float* out, const float4* planes, int W, int H, float scale, int lr, cudaStream_t st);
+void launch_fill_depthmap(float* out, const float4* planes, int W, int H, float scale, cudaStream_t st);
+void launch_fill_normalmap(float4* out, const float4* planes, int W, int H, cudaStream_t st);
+void launch_disparity_to_normal(float4* out, const float* d, int W, int H, cudaStream_t st);
+void launch_view_clear(int* count, unsigned long long* src, size_t n, cudaStream_t st);
+
+}  // namespace pm

@@ -1,0 +1,176 @@
+/*
+ * cvtpm — B200 (sm_100a) PatchMatch-Huber stereo, C ABI.
+ *
+ * Drop-in boundary for cvt::PMHuberStereo (cvt/vision/PMHuberStereo.h:42-110
+ * in phheise/cvt).  The reference exposes a C++ class whose methods run OpenCL
+ * kernels and throw cvt::Exception on error; this library exposes the same
+ * operations as plain C functions over host or device pointers that return a
+ * status code (the C++ header include/cvt/vision/PMHuberStereo.h turns the
+ * codes back into exceptions).
+ *
+ * Data layout (all row-major, channel fastest):
+ *   image     RGBA8, `stride` bytes per row (>= 4*width)
+ *   planes    float4 per pixel (a, b, c, cost): the matched column of pixel
+ *             (x, y) is a*x + b*y + c (pmhstereo.cl:183-186)
+ *   dmap      float per pixel; normalmap float4 per pixel (nx, ny, nz, 0)
+ *   fields    bw (r, g, b, support-weight sum), grad (4 grey differences),
+ *             dt (2x2 diffusion tensor), smooth (nx, ny, nz, d/dmax): float4
+ *   view buffer (cross-view candidates, VIEWPROP_t of pmhstereo.cl:830-833)
+ *             count int32 per pixel + source columns uint64 per pixel
+ *             (lowest kept column in the low 32 bits, next in the high 32 bits,
+ *             0xffffffff = empty); the candidate planes are read from the other
+ *             view's plane field.  An empty buffer is count 0, columns all ones.
+ *
+ * Threading: one handle per host thread (or per stream); handles are
+ * independent.  Every entry point is synchronous unless it takes a stream.
+ */
+#ifndef CVTPM_H
+#define CVTPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum {
+    PM_OK = 0,
+    PM_EINVAL_SHAPE = 1,   /* width/height/stride/patch size out of range; image sizes differ */
+    PM_EINVAL_ARG = 2,     /* null or inconsistent argument */
+    PM_ENOMEM = 3,         /* device or host allocation failed */
+    PM_ECUDA = 4,          /* a CUDA call failed; pm_last_error has the text */
+    PM_ETIMEOUT = 5,       /* a bounded device wait ran out */
+    PM_ENOTIMPL = 6,
+    PM_ENODEV = 7          /* no CUDA device */
+};
+
+/* cvt::DisparityPostProcessing (PMHuberStereo.h:36-40) */
+enum { PM_PP_NONE = 0, PM_PP_LRCHECK = 1, PM_PP_LRCHECK_FILL = 2 };
+
+/* limits: images up to 4096 columns (window coordinates stay exact in FP32
+ * products), window half-width 1..32 */
+enum { PM_MAX_WIDTH = 4096, PM_MAX_HEIGHT = 4096, PM_MAX_RADIUS = 32 };
+
+typedef struct pm_options {
+    int views;           /* 2: both views, as the reference (default); 1: left view only (pp must be NONE) */
+    int fused;           /* 1 (default): window loops contract a*b+c into fma; 0: every op rounds separately */
+    float thetamin;      /* 1e-4 (PMHuberStereo.cpp:92) */
+    float maxdispdiff;   /* 1.0 px (PMHuberStereo.cpp:79) */
+    float maxanglediff;  /* 5.0 degrees (PMHuberStereo.cpp:80) */
+    int rof_iters;       /* 40 (PMHuberStereo.cpp:427) */
+    int device;          /* CUDA device ordinal, default 0 */
+    int use_graph;       /* 1 (default): replay the iteration schedule as one CUDA graph */
+} pm_options;
+
+typedef struct pm_handle pm_handle;
+
+int pm_options_default(pm_options* opt);
+int pm_create(pm_handle** h, const pm_options* opt);
+int pm_destroy(pm_handle* h);
+const char* pm_last_error(const pm_handle* h);
+const char* pm_status_string(int status);
+
+/* PMHuberStereo::disparityMap (PMHuberStereo.cpp:75-143) with host buffers.
+ * patchsize is the window half-width r (the window is (2r+1)^2, pmhstereo.cl:685-687);
+ * iterations is rounded up to odd as in the reference (:490).  normalmap,
+ * initdisp (left-view disparity, > 0 where valid), initnormal (float4),
+ * planes_left and planes_right may be NULL. */
+int pm_disparity_map(pm_handle* h, const uint8_t* left, const uint8_t* right, int width, int height,
+                     size_t stride, int patchsize, float dispmax, int iterations, int pp, float* dmap,
+                     float* normalmap, const float* initdisp, const float* initnormal, float* planes_left,
+                     float* planes_right);
+
+/* The same with device pointers, enqueued on `stream` (cudaStream_t; NULL = legacy default stream).
+ * Returns once the work is enqueued; synchronise the stream before reading the outputs. */
+int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int width, int height,
+                            size_t stride, int patchsize, float dispmax, int iterations, int pp, float* dmap,
+                            float* normalmap, const float* initdisp, const float* initnormal, float* planes_left,
+                            float* planes_right, void* stream);
+
+/* Window-sample counters of the last pm_disparity_map* call on this handle when
+ * counting was requested with pm_set_counting(h, 1): [0] cost-window samples,
+ * [1] Gauss-Newton window samples, [2] cost evaluations that entered the window,
+ * [3] early exits.  Counting adds atomics; it is off by default. */
+int pm_set_counting(pm_handle* h, int on);
+int pm_get_counters(pm_handle* h, uint64_t counters[4]);
+
+/* Batched form: n independent pairs, each with its own size, patch size and
+ * disparity range, processed together (one launch per stage for all pairs).
+ * Arrays are indexed by pair; device pointers; outputs as in pm_disparity_map_device. */
+int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* left, const uint8_t* const* right,
+                                  const int* width, const int* height, const size_t* stride,
+                                  const int* patchsize, const float* dispmax, int iterations, int pp,
+                                  float* const* dmap, float* const* planes_left, float* const* planes_right,
+                                  void* stream);
+
+/* ---- per-kernel entry points (device pointers, enqueued on `stream`) ----------------
+ * These expose each reference kernel on injected state for parity testing. */
+
+/* pmhstereo_bilateral_weight_to_alpha + pmhstereo_gradxy + PDDiffTensorColor(alpha 24, beta 1)
+ * (pmhstereo.cl:1462-1498, :1549-1602; PDDiffTensor.cl:26-75); any output may be NULL */
+int pm_k_prep(const uint8_t* img, int width, int height, size_t stride, int patchsize, int fused, float* bw,
+              float* grad, float* dt, void* stream);
+/* pmhstereo_init / pmhstereo_init_disparity_normal (pmhstereo.cl:755-828) */
+int pm_k_init(float* out, const float* bw1, const float* bw2, const float* g1, const float* g2, int width,
+              int height, int patchsize, float dispmax, int lr, const float* initdisp, const float* initnormal,
+              int fused, void* stream);
+/* patch_eval_census (pmhstereo.cl:661-736) at every pixel for the given planes */
+int pm_k_cost(float* cost, const float* planes, const float* bw1, const float* bw2, const float* g1,
+              const float* g2, int width, int height, int patchsize, float mincost, int fused, void* stream);
+/* patch_census_klt2 (pmhstereo.cl:326-410), one Gauss-Newton step at every pixel */
+int pm_k_klt(float* out, const float* planes, const float* bw1, const float* bw2, const float* g1,
+             const float* g2, int width, int height, int patchsize, int fused, void* stream);
+/* pmhstereo_propagate_view (pmhstereo.cl:880-1071).  Reads and then empties the
+ * input view buffer (vin_*; candidate planes from vin_planes, the other view's
+ * field); appends to the output view buffer (vout_*; must start empty).  vin
+ * and vout may be NULL (no candidates / no scatter).  counters (4 x uint64) may be NULL. */
+int pm_k_propagate(float* out, const float* old, const float* bw1, const float* bw2, const float* g1,
+                   const float* g2, const float* smooth, float theta, int width, int height, int patchsize,
+                   float dispmax, int lr, int iter, int32_t* vin_count, uint64_t* vin_src,
+                   const float* vin_planes, int32_t* vout_count, uint64_t* vout_src, int fused,
+                   uint64_t* counters, void* stream);
+/* pmhstereo_normal_depth (pmhstereo.cl:1384-1402) */
+int pm_k_normal_depth(float* out, const float* planes, int width, int height, float dispscale, int lr,
+                      void* stream);
+/* PDOptCL::denoiseDiffusionTensorROF_PDD (PDOptCL.cpp:1114-1168): `iters` steps of
+ * PDDROFDiffTensor (PDDROFDiffTensor.cl:43-127) from u = input, p = q = 0.
+ * scratch: device buffer of pm_rof_scratch_bytes(width, height) bytes. */
+size_t pm_rof_scratch_bytes(int width, int height);
+int pm_k_rof(float* out, const float* input, const float* dt, const float lambda[4], int iters, int width,
+             int height, void* scratch, void* stream);
+/* pmhstereo_consistency (pmhstereo.cl:1095-1129) */
+int pm_k_consistency(float* out, const float* left, const float* right, int width, int height,
+                     float maxdispdiff, float maxanglediff, void* stream);
+/* pmhstereo_to_disparity (:1232-1257), pmhstereo_fill_depthmap (:1187-1230),
+ * pmhstereo_fill_normalmap (:1259-1305), pmhstereo_disparity_to_normal (:1604-1637) */
+int pm_k_to_disparity(float* out, const float* planes, int width, int height, float scale, int lr, void* stream);
+int pm_k_fill_depthmap(float* out, const float* planes, int width, int height, float scale, void* stream);
+int pm_k_fill_normalmap(float* out, const float* planes, int width, int height, int lr, void* stream);
+int pm_k_disparity_to_normal(float* out, const float* disp, int width, int height, void* stream);
+
+/* ---- host-side helpers ------------------------------------------------------------- */
+
+/* MWC64X stream of RNG_init(linpos, nd) (RNG.cl:54-57): `n` RNG_float draws, computed
+ * by the same code the kernels run, on the host */
+int pm_rng_floats(int64_t linpos, int nd, int n, float* out);
+/* the elementary functions the kernels use, evaluated on the host by the same code */
+float pm_expf_host(float x);
+float pm_sinf_host(float x);
+float pm_cosf_host(float x);
+float pm_acospif_host(float x);
+/* smallest c >= 0 with RN(c / b) >= m (the early-exit threshold of the cost loop) */
+float pm_exit_threshold_host(float m, float b);
+
+/* Procedural stereo pair: `nplanes` slanted planar patches (disparity in [dlo, dhi],
+ * |nx|, |ny| <= nmax) with 4-octave value-noise texture; right = left warped by the
+ * ground-truth disparity + noise of standard deviation sigma.  gt_disp (float per
+ * pixel) and gt_normal (float4 per pixel) may be NULL. */
+int pm_scene_generate(uint64_t seed, int width, int height, int nplanes, float dlo, float dhi, float nmax,
+                      float sigma, uint8_t* left, uint8_t* right, int stride, float* gt_disp, float* gt_normal);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,65 @@
+"""ORACLE — test infrastructure only.
+
+Builds the CPU checkers used by tests/, __graft_entry__.smoke() and bench.py's
+cpu_baseline leg:
+
+* oracle/liboracle.so      the CPU restatement (pm_oracle.cpp), always;
+* oracle/_ref/libpmref.so  the reference's own kernel sources
+                           (cvt/cl/kernel/pmhstereo.cl, PDDiffTensor.cl,
+                           PDDROFDiffTensor.cl) rewritten by translate.py and
+                           compiled against clshim.h, when the reference tree is
+                           present (it is not on GPU machines; the built .so
+                           travels with the checkout instead).
+
+Both are built with -O2 -ffp-contract=off -fno-fast-math: every C operator
+rounds once, so results do not depend on the compiler's contraction choices.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_KERNELS = "/root/reference/cvt/cl/kernel"
+CXXFLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-std=c++17"]
+
+
+def _run(cmd):
+    subprocess.run(cmd, check=True)
+
+
+def _stale(out, deps):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_oracle(force=False):
+    out = os.path.join(HERE, "liboracle.so")
+    srcs = [os.path.join(HERE, f) for f in ("pm_oracle.cpp", "pm_oracle.h", "pm_libm.h", "pm_hostloop.h")]
+    if force or _stale(out, srcs):
+        _run(["g++"] + CXXFLAGS + ["-o", out, srcs[0]])
+    return out
+
+
+def build_ref(force=False, kernel_dir=REF_KERNELS):
+    refdir = os.path.join(HERE, "_ref")
+    out = os.path.join(refdir, "libpmref.so")
+    if not os.path.isdir(kernel_dir):
+        return out if os.path.exists(out) else None
+    os.makedirs(refdir, exist_ok=True)
+    cls = ["pmhstereo.cl", "PDDiffTensor.cl", "PDDROFDiffTensor.cl"]
+    deps = [os.path.join(kernel_dir, f) for f in cls + ["RNG.cl", "MWC64X.cl", "Matrix3.cl"]]
+    glue = [os.path.join(HERE, f) for f in ("ref_pmh.cpp", "ref_pd.cpp", "ref_driver.cpp")]
+    hdrs = [os.path.join(HERE, f) for f in ("clshim.h", "ref_exec.h", "pm_hostloop.h", "pm_libm.h", "translate.py")]
+    if not (force or _stale(out, deps + glue + hdrs)):
+        return out
+    for f in cls:
+        _run([sys.executable, os.path.join(HERE, "translate.py"), kernel_dir, f, os.path.join(refdir, f + ".cpp")])
+    _run(["g++"] + CXXFLAGS + ["-w", "-Wno-narrowing", "-I", HERE, "-o", out] + glue)
+    return out
+
+
+if __name__ == "__main__":
+    print(build_oracle(force="-f" in sys.argv))
+    print(build_ref(force="-f" in sys.argv))

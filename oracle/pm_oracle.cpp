@@ -1,0 +1,924 @@
+/*
+ * ORACLE — test infrastructure only (see pm_oracle.h).  Built by
+ * oracle/Makefile into oracle/liboracle.so; never linked into the product.
+ *
+ * A plain CPU restatement of the PatchMatch-Huber stereo path of phheise/cvt.
+ * Citations are file:line within the reference project.  Build flags:
+ * -O2 -ffp-contract=off -fno-fast-math, so every C operator below rounds once.
+ */
+#include "pm_oracle.h"
+#include "pm_libm.h"
+#include "pm_hostloop.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+namespace {
+
+struct F2 { float x, y; };
+struct F3 { float x, y, z; };
+struct F4 { float x, y, z, w; };
+
+inline F4 f4(float x, float y, float z, float w) { F4 r = {x, y, z, w}; return r; }
+inline F3 f3(float x, float y, float z) { F3 r = {x, y, z}; return r; }
+inline F3 xyz(const F4& v) { return f3(v.x, v.y, v.z); }
+
+/* ---- arithmetic-mode helpers -------------------------------------------------- */
+
+/* a*b + c, contracted in fused mode (used only at the hot sites named ORC_HOT) */
+inline float orc_mad(int fused, float a, float b, float c) { return fused ? fmaf(a, b, c) : a * b + c; }
+
+/* OpenCL dot(float3, float3), left to right (ORC_HOT: contracted in fused mode) */
+inline float dot3_hot(int fused, F3 a, F3 b)
+{
+    if (fused) return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x));
+    return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+inline float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline float dot4(F4 a, F4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+
+inline bool isfin(float v) { return isfinite(v) != 0; }
+inline bool allfinite3(F3 v) { return isfin(v.x) && isfin(v.y) && isfin(v.z); }
+
+/* OpenCL clamp = fmin(fmax(x, lo), hi) */
+inline float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+
+/* OpenCL 1.2 normalize: zero vector returned unchanged, NaN propagated, otherwise
+ * v / |v| with the squared length rescaled away from under/overflow. */
+F3 normalize3(F3 v)
+{
+    if (v.x == 0.0f && v.y == 0.0f && v.z == 0.0f) return v;
+    if (v.x != v.x || v.y != v.y || v.z != v.z) { float n = NAN; return f3(n, n, n); }
+    if (isinf(v.x) || isinf(v.y) || isinf(v.z)) {
+        v.x = isinf(v.x) ? copysignf(1.0f, v.x) : 0.0f * v.x;
+        v.y = isinf(v.y) ? copysignf(1.0f, v.y) : 0.0f * v.y;
+        v.z = isinf(v.z) ? copysignf(1.0f, v.z) : 0.0f * v.z;
+    }
+    float d = dot3(v, v);
+    if (d < 7.8886090522101181e-31f) {            /* 2^-100: rescale by 2^64 */
+        v.x *= 1.8446744073709552e19f; v.y *= 1.8446744073709552e19f; v.z *= 1.8446744073709552e19f;
+        d = dot3(v, v);
+    } else if (d > 1.2676506002282294e30f) {      /* 2^100: rescale by 2^-64 */
+        v.x *= 5.4210108624275222e-20f; v.y *= 5.4210108624275222e-20f; v.z *= 5.4210108624275222e-20f;
+        d = dot3(v, v);
+    }
+    const float l = sqrtf(d);
+    return f3(v.x / l, v.y / l, v.z / l);
+}
+
+/* native_rsqrt: 1/sqrt, both correctly rounded */
+inline float rsqrt_(float x) { return 1.0f / sqrtf(x); }
+
+/* convert_int_rte / convert_int: NaN -> 0, saturating */
+inline int cvt_int_sat(float f)
+{
+    if (f != f) return 0;
+    if (f >= 2147483648.0f) return 2147483647;
+    if (f < -2147483648.0f) return (-2147483647 - 1);
+    return (int)f;
+}
+inline int convert_int_rte(float x) { return cvt_int_sat(rintf(x)); }
+inline int convert_int_rtz(float x) { return cvt_int_sat(x); }
+
+inline uint32_t signbits4(F4 v)
+{
+    return (orc_f2bits(v.x) >> 31) | ((orc_f2bits(v.y) >> 31) << 1) | ((orc_f2bits(v.z) >> 31) << 2) |
+           ((orc_f2bits(v.w) >> 31) << 3);
+}
+inline int popc4(uint32_t m) { return (int)((m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1) + ((m >> 3) & 1)); }
+
+/* ---- images ------------------------------------------------------------------ */
+
+struct Img4 {
+    const float* p; int W, H;
+    F4 at(int x, int y) const { const float* q = p + 4 * ((size_t)y * W + x); return f4(q[0], q[1], q[2], q[3]); }
+    /* SAMPLER_NN with CLK_ADDRESS_CLAMP_TO_EDGE (pmhstereo.cl:70) */
+    F4 edge(int x, int y) const {
+        x = x < 0 ? 0 : (x >= W ? W - 1 : x);
+        y = y < 0 ? 0 : (y >= H ? H - 1 : y);
+        return at(x, y);
+    }
+    /* CLK_ADDRESS_CLAMP: border colour (0,0,0,0) */
+    F4 zero(int x, int y) const {
+        if (x < 0 || x >= W || y < 0 || y >= H) return f4(0, 0, 0, 0);
+        return at(x, y);
+    }
+};
+
+/* SAMPLER_BILINEAR (CLK_FILTER_LINEAR, CLK_ADDRESS_CLAMP_TO_EDGE, pmhstereo.cl:71) read
+ * at (u, y + 0.5) with integral y, as every call on the path makes it (OpenCL 1.2 s8.2):
+ * t = u - 0.5, i0 = floor(t), a = t - floor(t); the vertical weight is exactly 0, so the
+ * value is (1-a)*T[i0] + a*T[i0+1] with edge-clamped columns (ORC_HOT: a*T[i0+1] is
+ * contracted in fused mode).  A non-finite u yields the positive quiet NaN. */
+inline F4 lerp_row(int fused, const Img4& im, float u, int y)
+{
+    const float t = u - 0.5f;
+    if (!isfin(t)) { const float n = orc_bits2f(0x7fffffffu); return f4(n, n, n, n); }
+    float fl = floorf(t);
+    const float a = t - fl;
+    fl = fminf(fmaxf(fl, -1.0f), (float)im.W);
+    const int i0 = (int)fl;
+    const F4 T0 = im.edge(i0, y), T1 = im.edge(i0 + 1, y);
+    const float b = 1.0f - a;
+    return f4(orc_mad(fused, a, T1.x, b * T0.x), orc_mad(fused, a, T1.y, b * T0.y),
+              orc_mad(fused, a, T1.z, b * T0.z), orc_mad(fused, a, T1.w, b * T0.w));
+}
+
+/* ---- MWC64X (MWC64X.cl:36-141, RNG.cl:30-59) --------------------------------- */
+
+const uint64_t MWC_A = 4294883355ULL;
+const uint64_t MWC_M = 18446383549859758079ULL;
+const uint64_t MWC_BASEID = 4077358422479273989ULL;
+
+inline uint64_t mulmod(uint64_t a, uint64_t b) { return (uint64_t)(((unsigned __int128)a * b) % MWC_M); }
+uint64_t powmod(uint64_t a, uint64_t e)
+{
+    uint64_t acc = 1, sq = a;
+    while (e) { if (e & 1) acc = mulmod(acc, sq); sq = mulmod(sq, sq); e >>= 1; }
+    return acc;
+}
+
+struct Rng {
+    uint32_t x, c;
+    /* RNG_init(s, linpos, numdraws): MWC64X_SeedStreams(s, 0, 0) starts every stream at
+     * MWC_BASEID (stream gap 0), then MWC64X_Skip(s, (linpos) * numdraws).  The macro
+     * does not parenthesise numdraws (RNG.cl:54-57), so the distance is the int value of
+     * the expanded expression; callers pass it. */
+    void init_skip(int32_t dist32) {
+        const uint64_t dist = (uint64_t)(int64_t)dist32;
+        uint64_t v = mulmod(MWC_BASEID, powmod(MWC_A, dist));
+        x = (uint32_t)(v / MWC_A); c = (uint32_t)(v % MWC_A);
+    }
+    float next() {
+        const uint32_t res = x ^ c;
+        const uint32_t Xn = (uint32_t)MWC_A * x + c;
+        const uint32_t carry = (uint32_t)(Xn < c);
+        const uint32_t Cn = (uint32_t)(((uint64_t)(uint32_t)MWC_A * x) >> 32) + carry;
+        x = Xn; c = Cn;
+        return 2.3283064365386962890625e-10f * (float)res;
+    }
+};
+
+/* ---- plane state algebra (pmhstereo.cl:74-224) -------------------------------- */
+
+const float GW_R = 0.2126f, GW_G = 0.7152f, GW_B = 0.0722f;
+
+/* nd_state_viewprop (:174-181) */
+inline F4 viewprop(F4 n)
+{
+    F4 r = f4(1.0f / n.x, -n.y / n.x, -n.z / n.x, 0.0f);
+    if (fabsf(n.x) < 1e-8f) r = f4(0.0f, -n.y, -n.z, 0.0f);
+    return r;
+}
+/* nd_state_transform (:183-186), x component, strict */
+inline float transform_x(F4 s, float cx, float cy) { return s.x * cx + s.y * cy + s.z; }
+
+/* nd_state_init (:77-97) */
+F4 nd_state_init(Rng& rng, float cx, float cy, int lr, float dmax)
+{
+    const float z = rng.next() * dmax;
+    const float azimuth = (float)(2.0f * M_PI * (double)rng.next());
+    const float u = rng.next() * 0.95f;
+    const float w = sqrtf(1.0f - u * u);
+    float s, c;
+    orc_sincosf(azimuth, &s, &c);
+    F3 n = f3(w * c, w * s, u);
+    n.z = fmaxf(n.z, 1e-4f);
+    n = normalize3(n);
+    const float t0 = -n.x / n.z, t1 = -n.y / n.z, t2 = (n.x * cx + n.y * cy) / n.z + z;
+    F4 ret = f4(1.0f - t0, 0.0f - t1, 0.0f - t2, 0.0f - 0.0f);
+    if (!lr) ret = viewprop(ret);
+    return ret;
+}
+
+/* nd_state_from_disparity_normal (:99-106) */
+F4 from_disparity_normal(float cx, float cy, float disparity, F3 normal)
+{
+    normal.z = fmaxf(normal.z, 1e-4f);
+    normal = normalize3(normal);
+    const float t0 = -normal.x / normal.z, t1 = -normal.y / normal.z;
+    const float t2 = (normal.x * cx + normal.y * cy) / normal.z + disparity;
+    return f4(1.0f - t0, 0.0f - t1, 0.0f - t2, 0.0f - 0.0f);
+}
+
+/* nd_state_to_ref_normal_depth (:108-127) */
+F4 to_ref_normal_depth(F4 state, float cx, float cy, int lr)
+{
+    F4 s = state;
+    const float sidesign = lr ? -1.0f : 1.0f;
+    if (!lr) s = viewprop(state);
+    s = f4(1.0f - s.x, 0.0f - s.y, 0.0f - s.z, 0.0f - s.w);
+    F4 ret;
+    ret.w = (transform_x(state, cx, cy) - cx) * sidesign;
+    ret.z = rsqrt_(s.x * s.x + s.y * s.y + 1.0f);
+    ret.x = -s.x * ret.z;
+    ret.y = -s.y * ret.z;
+    if (!allfinite3(xyz(ret))) return f4(0.0f, 0.0f, 1.0f, 0.0f);
+    return ret;
+}
+
+/* nd_state_refine (:129-172), including the lr == 0 early return at :169-170 */
+F4 nd_state_refine(Rng& rng, F4 in, float cx, float cy, float dmax, int lr)
+{
+    F4 state = in;
+    if (!lr) state = viewprop(state);
+    state = f4(1.0f - state.x, 0.0f - state.y, 0.0f - state.z, 0.0f - state.w);
+    float z = state.x * cx + state.y * cy + state.z;
+    F3 n;
+    n.z = rsqrt_(state.x * state.x + state.y * state.y + 1.0f);
+    n.x = -state.x * n.z;
+    n.y = -state.y * n.z;
+    z += (rng.next() - 0.5f) * 2.0f * 2.0f;
+    z = clampf(z, 0.0f, dmax);
+    const float azimuth = (float)(2.0f * M_PI * (double)rng.next());
+    const float u = rng.next() * (1.0f - 0.05f);
+    const float w = sqrtf(1.0f - u * u);
+    float s, c;
+    orc_sincosf(azimuth, &s, &c);
+    F3 n2 = f3(w * c, w * s, u);
+    n = f3((n.x + n2.x) * 0.5f, (n.y + n2.y) * 0.5f, (n.z + n2.z) * 0.5f);
+    n.z = fmaxf(n.z, 1e-4f);
+    n = normalize3(n);
+    F4 ret = f4(-n.x / n.z, -n.y / n.z, (n.x * cx + n.y * cy) / n.z + z, 0.0f);
+    ret = f4(1.0f - ret.x, 0.0f - ret.y, 0.0f - ret.z, 0.0f - ret.w);
+    if (!lr) return viewprop(state);
+    return ret;
+}
+
+/* nd_state_to_normal (:201-210) */
+F3 to_normal(F4 st)
+{
+    const F4 s = f4(1.0f - st.x, 0.0f - st.y, 0.0f - st.z, 0.0f - st.w);
+    F3 n;
+    n.z = rsqrt_(s.x * s.x + s.y * s.y + 1.0f);
+    n.x = -s.x * n.z;
+    n.y = -s.y * n.z;
+    n.z = sqrtf(1.0f - n.x * n.x - n.y * n.y);
+    return n;
+}
+
+/* smoothDistance (:846-871) */
+F2 smooth_distance(F4 sa, F4 sb, F4 smooth, float cx, float cy, float dmax, int lr)
+{
+    const F4 a = to_ref_normal_depth(sa, cx, cy, lr);
+    const F4 b = to_ref_normal_depth(sb, cx, cy, lr);
+    const float id2 = 1.0f / (dmax * dmax);
+    const float den = id2 + 0.3f;
+    const F4 diag = f4(0.1f / den, 0.1f / den, 0.1f / den, id2 / den);
+    const F4 da = f4(a.x - smooth.x, a.y - smooth.y, a.z - smooth.z, a.w - smooth.w);
+    const F4 db = f4(b.x - smooth.x, b.y - smooth.y, b.z - smooth.z, b.w - smooth.w);
+    F2 r;
+    r.x = dot4(da, f4(diag.x * da.x, diag.y * da.y, diag.z * da.z, diag.w * da.w));
+    r.y = dot4(db, f4(diag.x * db.x, diag.y * db.y, diag.z * db.z, diag.w * db.w));
+    return r;
+}
+
+/* ---- window kernels ----------------------------------------------------------- */
+
+struct Views {
+    Img4 bw1, bw2, g1, g2;  /* first/second: rgb + support-weight sum; gradients */
+    int W, H, r;
+};
+
+/* support weight exp(-|dot(I1(q) - I1(p), gray)| * 12) (pmhstereo.cl:355, :701, :1491) */
+inline float support_weight(int fused, F3 val1)
+{
+    const float d = dot3_hot(fused, val1, f3(GW_R, GW_G, GW_B));
+    return orc_expf(-fabsf(d) * 12.0f);
+}
+
+/* per-sample ASW cost terms of patch_eval_census (:698-716) */
+inline float census_cost(F3 valin, F4 gval1, F4 v2, F4 gval2)
+{
+    const float cx = fminf(fabsf(v2.x - valin.x), 0.05f) / 0.05f;
+    const float cy = fminf(fabsf(v2.y - valin.y), 0.05f) / 0.05f;
+    const float cz = fminf(fabsf(v2.z - valin.z), 0.05f) / 0.05f;
+    const float cad = 0.33f * (cx + cy + cz);
+    float cost = 0.125f * cad;
+    const int cnt = popc4(signbits4(gval1) ^ signbits4(gval2));
+    const float cc = 0.25f * (float)cnt;
+    cost += 0.875f * cc;
+    return cost;
+}
+
+/* patch_eval_census (pmhstereo.cl:661-736) */
+float patch_eval(const Views& V, int fused, int px, int py, F4 state, float mincost, int64_t* cnt)
+{
+    const float cx = (float)px, cy = (float)py;
+    const float c2x = transform_x(state, cx, cy);
+    if (!allfinite3(xyz(state)) || to_normal(state).z < 1e-4f || c2x < 0 || c2x >= (float)V.W) return 1e5f;
+    const F4 in = V.bw1.at(px, py);
+    const float bilw = in.w;
+    const F3 valc1 = xyz(in);
+    float wsum = 0.0f, census = 0.0f;
+    const int r = V.r;
+    if (cnt) cnt[2]++;
+    for (int dy = -r; dy <= r; dy++) {
+        for (int dx = -r; dx <= r; dx++) {
+            const float qx = cx + (float)dx, qy = cy + (float)dy;
+            /* ORC_HOT: the transform's a*x is contracted in fused mode */
+            const float p2x = orc_mad(fused, state.x, qx, state.y * qy) + state.z;
+            if (p2x < 0 || p2x >= (float)V.W || qx < 0 || qx >= (float)V.W || qy < 0 || qy >= (float)V.H) continue;
+            const int ix = px + dx, iy = py + dy;
+            const F3 valin = xyz(V.bw1.at(ix, iy));
+            const F3 val1 = f3(valin.x - valc1.x, valin.y - valc1.y, valin.z - valc1.z);
+            const float w = support_weight(fused, val1);
+            const F4 gval1 = V.g1.at(ix, iy);
+            const F4 gval2 = lerp_row(fused, V.g2, p2x + 0.5f, iy);
+            const F4 val2 = lerp_row(fused, V.bw2, p2x + 0.5f, iy);
+            const float cost = census_cost(valin, gval1, val2, gval2);
+            census = orc_mad(fused, w, cost, census);   /* ORC_HOT */
+            wsum += w;
+            if (cnt) cnt[0]++;
+            if (census / bilw >= mincost) { if (cnt) cnt[3]++; return 1.0f; }
+        }
+    }
+    if (wsum <= 1.0f) return 1.1f;
+    return census / wsum;
+}
+
+/* cost of one KLT tap: patch_census_klt2 (:361-370) with the colour term taken
+ * against the colour difference val1, as the reference does */
+inline float klt_tap(int fused, float w1, F3 val1, uint32_t sg1, F4 v2, F4 gv2)
+{
+    const float cx = fminf(fabsf(v2.x - val1.x), 0.05f) / 0.05f;
+    const float cy = fminf(fabsf(v2.y - val1.y), 0.05f) / 0.05f;
+    const float cz = fminf(fabsf(v2.z - val1.z), 0.05f) / 0.05f;
+    float C = w1 * 0.125f * 0.33f * (cx + cy + cz);
+    const int cnt = popc4(sg1 ^ signbits4(gv2));
+    /* `w1 * (1.0f - alpha) * 0.25 * (float)cnt` has a double literal: the sum is formed in
+     * double and rounded once; fused mode forms the same sum with one fma. */
+    if (fused) C = fmaf(w1 * 0.875f * 0.25f, (float)cnt, C);
+    else C = (float)((double)C + (double)(w1 * 0.875f) * 0.25 * (double)(float)cnt);
+    return C;
+}
+
+/* mat3f_lusolve (Matrix3.cl:286-311) on the symmetric H */
+F3 lusolve(const float Hm[3][3], F3 b)
+{
+    float m[3][3];
+    memcpy(m, Hm, sizeof(m));
+    m[1][0] /= m[0][0];
+    m[2][0] /= m[0][0];
+    m[1][1] -= m[1][0] * m[0][1];
+    m[1][2] -= m[1][0] * m[0][2];
+    m[2][1] -= m[2][0] * m[0][1];
+    m[2][2] -= m[2][0] * m[0][2];
+    m[2][1] /= m[1][1];
+    m[2][2] -= m[2][1] * m[1][2];
+    b.y -= m[1][0] * b.x;
+    b.z -= m[2][0] * b.x + m[2][1] * b.y;
+    F3 ret;
+    ret.z = b.z / m[2][2];
+    ret.y = (b.y - m[1][2] * ret.z) / m[1][1];
+    ret.x = (b.x - (m[0][1] * ret.y + m[0][2] * ret.z)) / m[0][0];
+    return ret;
+}
+
+/* patch_census_klt2 (pmhstereo.cl:326-410), including the in-bounds test on pos rather
+ * than pos2 (:358) */
+F4 klt2(const Views& V, int fused, int px, int py, F4 state, int64_t* cnt)
+{
+    const float cxf = (float)px, cyf = (float)py;
+    float J[3] = {0, 0, 0};
+    float Hm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    const F3 valc1 = xyz(V.bw1.at(px, py));
+    const int r = V.r;
+    for (int dy = -r; dy <= r; dy++) {
+        for (int dx = -r; dx <= r; dx++) {
+            const float qx = cxf + (float)dx, qy = cyf + (float)dy;
+            if (qx < 0 || qx >= (float)V.W || qy < 0 || qy >= (float)V.H) continue;
+            const int ix = px + dx, iy = py + dy;
+            const F3 valin = xyz(V.bw1.at(ix, iy));
+            const F3 val1 = f3(valin.x - valc1.x, valin.y - valc1.y, valin.z - valc1.z);
+            const F4 gval1 = V.g1.at(ix, iy);
+            const float w1 = support_weight(fused, val1);
+            const float p2x = orc_mad(fused, state.x, qx, state.y * qy) + state.z;   /* ORC_HOT */
+            if (qx < 1 || qx >= (float)(V.W - 1)) continue;
+            if (cnt) cnt[1]++;
+            const uint32_t sg1 = signbits4(gval1);
+            const float u0 = p2x + 0.5f;
+            const float up = (p2x + 1.0f) + 0.5f;
+            const float um = (p2x + -1.0f) + 0.5f;
+            const float C = klt_tap(fused, w1, val1, sg1, lerp_row(fused, V.bw2, u0, iy), lerp_row(fused, V.g2, u0, iy));
+            const float Cxp = klt_tap(fused, w1, val1, sg1, lerp_row(fused, V.bw2, up, iy), lerp_row(fused, V.g2, up, iy));
+            const float Cxm = klt_tap(fused, w1, val1, sg1, lerp_row(fused, V.bw2, um, iy), lerp_row(fused, V.g2, um, iy));
+            if ((Cxp + Cxm - 2.0f * C) > 0.0f) {
+                const float p[3] = {qx, qy, 1.0f};
+                const float t = w1 * (Cxm - Cxp) * 0.5f;
+                const float s = w1 * (Cxp + Cxm - 2.0f * C);
+                for (int i = 0; i < 3; i++) J[i] = orc_mad(fused, t, p[i], J[i]);           /* ORC_HOT */
+                for (int i = 0; i < 3; i++)
+                    for (int j = 0; j < 3; j++) Hm[i][j] = orc_mad(fused, s, p[i] * p[j], Hm[i][j]); /* ORC_HOT */
+            }
+        }
+    }
+    const F3 d = lusolve(Hm, f3(J[0], J[1], J[2]));
+    return f4(state.x - d.x, state.y - d.y, state.z - d.z, state.w - 1e5f);
+}
+
+/* minimalCost (:873-877) */
+inline float minimal_cost(F4 nb, F4 self, F4 smooth, float cx, float cy, float theta, float dmax, int lr)
+{
+    const F2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
+    return self.w + theta * sd.y - theta * sd.x;
+}
+
+/* the select at :976 / :990 / :1002 / :1015 / :1027 / :1052 */
+inline void try_candidate(const Views& V, int fused, int px, int py, F4& self, F4 nb, F4 smooth,
+                          float theta, float dmax, int lr, int64_t* cnt)
+{
+    const float cx = (float)px, cy = (float)py;
+    const float mincost = minimal_cost(nb, self, smooth, cx, cy, theta, dmax, lr);
+    nb.w = patch_eval(V, fused, px, py, nb, mincost, cnt);
+    const F2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
+    if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
+}
+
+struct ScatterReq { int target; int src; F4 value; };
+
+/* pmhstereo_propagate_view body for one pixel (:924-1070) */
+F4 propagate_pixel(const Views& V, int fused, const Img4& old, const Img4& smoothimg, float theta,
+                   float dmax, int lr, int iter, const int32_t* vin_n, const float* vin_val,
+                   int px, int py, ScatterReq* req, int64_t* cnt)
+{
+    const int W = V.W;
+    const float cx = (float)px, cy = (float)py;
+    F4 smooth = smoothimg.at(px, py);
+    smooth.w = clampf(smooth.w, 0.0f, 1.0f) * dmax;
+    F4 self = old.at(px, py);
+    self.w = patch_eval(V, fused, px, py, self, 1e10f, cnt);
+
+    Rng rng;
+    /* RNG_init(&rng, lin, (((2*PROPSIZE+1)*(2*PROPSIZE+1)-1) + NUMRNDTRIES)*3 + 2*NUMRNDSAMPLE)
+     * (:942) expands to (lin) * ((1*1 - 1) + 2) * 3 + 2 * 4 = 6 * lin + 8 */
+    const int32_t lin = py * W + px + iter;
+    rng.init_skip(lin * 2 * 3 + 2 * 4);
+
+    /* smooth candidate (:968-976) */
+    F4 nb = from_disparity_normal(cx, cy, smooth.w * (lr ? -1.0f : 1.0f), normalize3(xyz(smooth)));
+    if (!lr) nb = viewprop(nb);
+    try_candidate(V, fused, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+
+    /* random neighbourhood (:982-991); the two offsets are drawn x first */
+    for (int i = 0; i < 4; i++) {
+        const int ox = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
+        const int oy = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
+        nb = old.edge(px + ox, py + oy);
+        try_candidate(V, fused, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+    }
+
+    /* random plane (:996-1002) */
+    nb = nd_state_init(rng, cx, cy, lr, dmax);
+    try_candidate(V, fused, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+
+    /* other view (:1007-1016) */
+    const size_t idx = (size_t)py * W + px;
+    int nview = vin_n ? vin_n[idx] : 0;
+    if (nview > 2) nview = 2;
+    for (int i = 0; i < nview; i++) {
+        const float* v = vin_val + 8 * idx + 4 * i;
+        nb = f4(v[0], v[1], v[2], v[3]);
+        try_candidate(V, fused, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+    }
+
+    /* randomized refinement, NUMRNDTRIES - 1 = 1 (:1021-1028) */
+    nb = nd_state_refine(rng, self, cx, cy, dmax, lr);
+    try_candidate(V, fused, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+
+    /* KLT step (:1034-1053) */
+    nb = klt2(V, fused, px, py, self, cnt);
+    for (int k = 0; k < 5; k++) nb = klt2(V, fused, px, py, nb, cnt);
+    try_candidate(V, fused, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+
+    /* view scatter (:1060-1067) */
+    req->target = -1;
+    const float sidesign = lr ? -1.0f : 1.0f;
+    const float tx = transform_x(self, cx, cy);
+    const int xposview = convert_int_rte(tx);
+    const int disp = convert_int_rtz((tx - cx) * sidesign);
+    if (xposview >= 0 && xposview < W && disp > 0) {
+        req->target = py * W + xposview;
+        req->src = px;
+        req->value = viewprop(self);
+    }
+    return self;
+}
+
+inline void put4(float* dst, size_t i, F4 v) { dst[4 * i] = v.x; dst[4 * i + 1] = v.y; dst[4 * i + 2] = v.z; dst[4 * i + 3] = v.w; }
+
+std::vector<float> rgba8_to_float(const uint8_t* img, int W, int H, int stride)
+{
+    std::vector<float> f((size_t)W * H * 4);
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++)
+            for (int c = 0; c < 4; c++) f[4 * ((size_t)y * W + x) + c] = (float)img[(size_t)y * stride + 4 * x + c] / 255.0f;
+    return f;
+}
+
+void add_counters(int64_t* dst, const int64_t* src) { if (dst) for (int i = 0; i < ORC_NCOUNTERS; i++) dst[i] += src[i]; }
+
+}  // namespace
+
+extern "C" {
+
+int orc_version(void) { return 1; }
+
+float orc_exp(float x) { return orc_expf(x); }
+float orc_sin(float x) { return orc_sinf(x); }
+float orc_cos(float x) { return orc_cosf(x); }
+float orc_acospi(float x) { return orc_acospif(x); }
+
+int orc_rng_floats(int64_t linpos, int nd, int ndraws, float* out)
+{
+    Rng r; r.init_skip((int32_t)linpos * nd);
+    for (int i = 0; i < ndraws; i++) out[i] = r.next();
+    return 0;
+}
+
+int orc_prep(const uint8_t* img, int W, int H, int stride, int r, int fused, float* bw, float* grad, float* dt)
+{
+    const std::vector<float> f = rgba8_to_float(img, W, H, stride);
+    const Img4 src = {f.data(), W, H};
+    /* grey with the zero border of CLK_ADDRESS_CLAMP (:1569-1573, PDDiffTensor.cl:41-45) */
+    auto gray = [&](int x, int y) { return dot4(src.zero(x, y), f4(GW_R, GW_G, GW_B, 0.0f)); };
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++) {
+        for (int x = 0; x < W; x++) {
+            const size_t i = (size_t)y * W + x;
+            if (bw) {
+                /* pmhstereo_bilateral_weight_to_alpha (:1462-1498) */
+                const F3 valc1 = xyz(src.at(x, y));
+                float wsum = 0.0f;
+                for (int dy = -r; dy <= r; dy++)
+                    for (int dx = -r; dx <= r; dx++) {
+                        const int qx = x + dx, qy = y + dy;
+                        if (qx < 0 || qx >= W || qy < 0 || qy >= H) continue;
+                        const F3 v = xyz(src.at(qx, qy));
+                        wsum += support_weight(fused, f3(v.x - valc1.x, v.y - valc1.y, v.z - valc1.z));
+                    }
+                put4(bw, i, f4(valc1.x, valc1.y, valc1.z, wsum));
+            }
+            const float g = gray(x, y);
+            if (grad) {
+                /* pmhstereo_gradxy (:1584-1601) */
+                put4(grad, i, f4(gray(x + 1, y) - g, gray(x, y + 1) - g, gray(x + 1, y) - gray(x - 1, y),
+                                 gray(x, y + 1) - gray(x, y - 1)));
+            }
+            if (dt) {
+                /* PDDiffTensorColor (PDDiffTensor.cl:52-72) with alpha = 24, beta = 1
+                 * (PMHuberStereo.cpp:416-417); pow(len, 1) = len */
+                float dx = gray(x + 1, y) - g;
+                float dy = gray(x, y + 1) - g;
+                const float len = sqrtf(dx * dx + dy * dy);
+                const float w = orc_expf(-24.0f * len);
+                F4 d;
+                if (len <= 0.001f) {
+                    d = f4(1.0f, 0.0f, 0.0f, 1.0f);
+                } else {
+                    dx = dx / len;
+                    dy = dy / len;
+                    const float dxo = dy, dyo = -dx;
+                    d = f4(w * dx * dx + dxo * dxo, w * dx * dy + dxo * dyo, w * dy * dx + dyo * dxo,
+                           w * dy * dy + dyo * dyo);
+                }
+                put4(dt, i, d);
+            }
+        }
+    }
+    return 0;
+}
+
+int orc_init(float* out, const float* bw1, const float* bw2, const float* g1, const float* g2,
+             int W, int H, int r, float dmax, int lr, const float* initdisp, const float* initnormal, int fused)
+{
+    const Views V = {{bw1, W, H}, {bw2, W, H}, {g1, W, H}, {g2, W, H}, W, H, r};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < H; y++) {
+        for (int x = 0; x < W; x++) {
+            const size_t i = (size_t)y * W + x;
+            const float cx = (float)x, cy = (float)y;
+            Rng rng;
+            rng.init_skip((y * W + x) * 3);   /* RNG_init(&rng, lin, 3) (:766) */
+            F4 ret;
+            const float disparity = initdisp ? initdisp[i] : 0.0f;
+            if (initdisp && disparity > 0 && lr) {
+                const F3 n = normalize3(f3(initnormal[4 * i], initnormal[4 * i + 1], initnormal[4 * i + 2]));
+                ret = from_disparity_normal(cx, cy, disparity, n);
+            } else if (initdisp && disparity > 0 && !lr) {
+                const F3 n = normalize3(f3(initnormal[4 * i], initnormal[4 * i + 1], initnormal[4 * i + 2]));
+                ret = from_disparity_normal(cx, cy, -disparity, n);
+            } else {
+                ret = nd_state_init(rng, cx, cy, lr, dmax);
+            }
+            ret.w = patch_eval(V, fused, x, y, ret, 1e10f, nullptr);
+            put4(out, i, ret);
+        }
+    }
+    return 0;
+}
+
+int orc_propagate(float* out, const float* old, const float* bw1, const float* bw2,
+                  const float* g1, const float* g2, const float* smooth, float theta,
+                  int W, int H, int r, float dmax, int lr, int iter,
+                  const int32_t* vin_n, const float* vin_val,
+                  int32_t* vout_n, float* vout_val, int32_t* vout_src,
+                  int fused, int64_t* counters)
+{
+    const Views V = {{bw1, W, H}, {bw2, W, H}, {g1, W, H}, {g2, W, H}, W, H, r};
+    const Img4 oldimg = {old, W, H}, smoothimg = {smooth, W, H};
+    std::vector<ScatterReq> req((size_t)W * H);
+    int64_t total[ORC_NCOUNTERS] = {0, 0, 0, 0};
+#pragma omp parallel
+    {
+        int64_t local[ORC_NCOUNTERS] = {0, 0, 0, 0};
+#pragma omp for schedule(dynamic, 1)
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++) {
+                const size_t i = (size_t)y * W + x;
+                const F4 s = propagate_pixel(V, fused, oldimg, smoothimg, theta, dmax, lr, iter, vin_n, vin_val,
+                                             x, y, &req[i], local);
+                put4(out, i, s);
+            }
+#pragma omp critical
+        add_counters(total, local);
+    }
+    add_counters(counters, total);
+    /* append in the order a sequential executor issues atomic_inc: row-major */
+    if (vout_n) {
+        for (size_t i = 0; i < (size_t)W * H; i++) {
+            const ScatterReq& q = req[i];
+            if (q.target < 0) continue;
+            const int nold = vout_n[q.target]++;
+            if (nold < 2) {
+                put4(vout_val + 4 * nold, 2 * (size_t)q.target, q.value);
+                if (vout_src) vout_src[2 * (size_t)q.target + nold] = q.src;
+            }
+        }
+    }
+    return 0;
+}
+
+int orc_cost(float* cost, const float* planes, const float* bw1, const float* bw2,
+             const float* g1, const float* g2, int W, int H, int r, float mincost, int fused)
+{
+    const Views V = {{bw1, W, H}, {bw2, W, H}, {g1, W, H}, {g2, W, H}, W, H, r};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const size_t i = (size_t)y * W + x;
+            const F4 s = f4(planes[4 * i], planes[4 * i + 1], planes[4 * i + 2], planes[4 * i + 3]);
+            cost[i] = patch_eval(V, fused, x, y, s, mincost, nullptr);
+        }
+    return 0;
+}
+
+int orc_klt(float* out, const float* planes, const float* bw1, const float* bw2,
+            const float* g1, const float* g2, int W, int H, int r, int fused)
+{
+    const Views V = {{bw1, W, H}, {bw2, W, H}, {g1, W, H}, {g2, W, H}, W, H, r};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const size_t i = (size_t)y * W + x;
+            const F4 s = f4(planes[4 * i], planes[4 * i + 1], planes[4 * i + 2], planes[4 * i + 3]);
+            put4(out, i, klt2(V, fused, x, y, s, nullptr));
+        }
+    return 0;
+}
+
+int orc_normal_depth(float* out, const float* planes, int W, int H, float dispscale, int lr)
+{
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const size_t i = (size_t)y * W + x;
+            const F4 s = f4(planes[4 * i], planes[4 * i + 1], planes[4 * i + 2], planes[4 * i + 3]);
+            F4 v = to_ref_normal_depth(s, (float)x, (float)y, lr);
+            v.w = v.w * dispscale;
+            put4(out, i, v);
+        }
+    return 0;
+}
+
+int orc_rof(float* out, const float* input, const float* dt, const float lambda[4], int iters, int W, int H)
+{
+    const float SIGMA = 4.0f, TAU = 0.05f, ETA = 8.0f, THETA = 0.5f;   /* PDDROFDiffTensor.cl:35-41 */
+    const size_t N = (size_t)W * H;
+    std::vector<float> u0(input, input + 4 * N), u1(4 * N);
+    std::vector<float> p0(8 * N, 0.0f), p1(8 * N, 0.0f), q0(4 * N, 0.0f), q1(4 * N, 0.0f);
+    const float lam[4] = {lambda[0], lambda[1], lambda[2], lambda[3]};
+    std::vector<float>* ucur = &u0; std::vector<float>* unew = &u1;
+    std::vector<float>* pcur = &p0; std::vector<float>* pnew = &p1;
+    std::vector<float>* qcur = &q0; std::vector<float>* qnew = &q1;
+    /* the host loop runs iters steps and, when the last one left the result in the
+     * scratch image (iters odd, or 0), one more (PDOptCL.cpp:1137-1166) */
+    const int steps = (iters > 0 && iters % 2 == 0) ? iters : iters + 1;
+    for (int it = 0; it < steps; it++) {
+        const Img4 U = {ucur->data(), W, H}, DT = {dt, W, H}, IMG = {input, W, H}, Q = {qcur->data(), W, H};
+        const Img4 P = {pcur->data(), 2 * W, H};
+        /* projected, tensor-weighted dual at pixel (x, y), zero outside (PDDROFDiffTensor.cl:72-100) */
+        auto dual = [&](int x, int y, F4& lo, F4& hi) {
+            const F4 uc = U.edge(x, y), ux = U.edge(x + 1, y), uy = U.edge(x, y + 1);
+            const F4 D = DT.zero(x, y);
+            const float dxv[4] = {uc.x - ux.x, uc.y - ux.y, uc.z - ux.z, uc.w - ux.w};
+            const float dyv[4] = {uc.x - uy.x, uc.y - uy.y, uc.z - uy.z, uc.w - uy.w};
+            const F4 plo = P.zero(2 * x, y), phi = P.zero(2 * x + 1, y);
+            const float pl[4] = {plo.x, plo.y, plo.z, plo.w}, ph[4] = {phi.x, phi.y, phi.z, phi.w};
+            float a[4], b[4], nrm[4];
+            for (int c = 0; c < 4; c++) {
+                const float DTdx = D.x * dxv[c] + D.z * dyv[c];
+                const float DTdy = D.y * dxv[c] + D.w * dyv[c];
+                a[c] = pl[c] + SIGMA * DTdx;
+                b[c] = ph[c] + SIGMA * DTdy;
+                nrm[c] = a[c] * a[c] + b[c] * b[c];
+            }
+            const float n3 = sqrtf(nrm[0] * 1.0f + nrm[1] * 1.0f + nrm[2] * 1.0f);
+            const float n4 = sqrtf(nrm[3]);
+            const float pr[4] = {fmaxf(1.0f, n3), fmaxf(1.0f, n3), fmaxf(1.0f, n3), fmaxf(1.0f, n4)};
+            float l[4], h[4];
+            for (int c = 0; c < 4; c++) {
+                a[c] = a[c] / pr[c];
+                b[c] = b[c] / pr[c];
+                l[c] = D.x * a[c] + D.z * b[c];
+                h[c] = D.y * a[c] + D.w * b[c];
+            }
+            lo = f4(l[0], l[1], l[2], l[3]);
+            hi = f4(h[0], h[1], h[2], h[3]);
+        };
+#pragma omp parallel for schedule(static)
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++) {
+                F4 lo, hi, llo, lhi, tlo, thi;
+                dual(x, y, lo, hi);
+                dual(x - 1, y, llo, lhi);
+                dual(x, y - 1, tlo, thi);
+                const float div[4] = {lo.x - llo.x + hi.x - thi.x, lo.y - llo.y + hi.y - thi.y,
+                                      lo.z - llo.z + hi.z - thi.z, lo.w - llo.w + hi.w - thi.w};
+                const F4 im = IMG.at(x, y), q = Q.at(x, y), u = U.at(x, y);
+                const float imv[4] = {im.x, im.y, im.z, im.w}, qv[4] = {q.x, q.y, q.z, q.w}, uv[4] = {u.x, u.y, u.z, u.w};
+                float on[4], qn[4];
+                for (int c = 0; c < 4; c++) {
+                    float o = (uv[c] + TAU * (lam[c] * imv[c] - div[c] - qv[c])) / (1.0f + TAU * lam[c]);
+                    o = o + THETA * (o - uv[c]);
+                    float qq = (qv[c] + ETA * (o - imv[c])) / (1.0f + 4.0f * ETA / lam[c]);
+                    qq = qq + THETA * (qq - qv[c]);
+                    on[c] = o; qn[c] = qq;
+                }
+                const size_t i = (size_t)y * W + x;
+                put4(unew->data(), i, f4(on[0], on[1], on[2], on[3]));
+                put4(qnew->data(), i, f4(qn[0], qn[1], qn[2], qn[3]));
+                put4(pnew->data(), (size_t)y * 2 * W + 2 * x, lo);
+                put4(pnew->data(), (size_t)y * 2 * W + 2 * x + 1, hi);
+            }
+        std::swap(ucur, unew); std::swap(pcur, pnew); std::swap(qcur, qnew);
+    }
+    memcpy(out, ucur->data(), 4 * N * sizeof(float));
+    return 0;
+}
+
+int orc_consistency(float* out, const float* left, const float* right, int W, int H, float maxdispdiff, float maxanglediff)
+{
+    const Img4 R = {right, W, H};
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const size_t i = (size_t)y * W + x;
+            const F4 sl = f4(left[4 * i], left[4 * i + 1], left[4 * i + 2], left[4 * i + 3]);
+            const float c2x = transform_x(sl, (float)x, (float)y), c2y = (float)y;
+            F4 val = f4(0.0f, 0.0f, 0.0f, -1.0f);
+            if (ceilf(c2x) >= 0 && floorf(c2x) < (float)W) {
+                const F4 sr = R.edge(convert_int_rte(floorf(c2x)), y);
+                const F4 sr2 = R.edge(convert_int_rte(ceilf(c2x)), y);
+                const F3 nl = to_normal(sl);
+                const float nd = dot3(nl, to_normal(viewprop(sr)));
+                const float nd2 = dot3(nl, to_normal(viewprop(sr2)));
+                const float d1 = fabsf((float)x - transform_x(sr, c2x, c2y));
+                const float d2 = fabsf((float)x - transform_x(sr2, c2x, c2y));
+                const float lim = maxanglediff / 180.0f;
+                if (!(d1 >= maxdispdiff || orc_acospif(clampf(nd, -1.0f, 1.0f)) >= lim) ||
+                    !(d2 >= maxdispdiff || orc_acospif(clampf(nd2, -1.0f, 1.0f)) >= lim))
+                    val = sl;
+            }
+            put4(out, i, val);
+        }
+    return 0;
+}
+
+static inline float length3(F3 v) { return sqrtf(dot3(v, v)); }
+
+int orc_to_disparity(float* out, const float* planes, int W, int H, float scale, int lr)
+{
+    const float sidesign = lr ? -1.0f : 1.0f;
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const size_t i = (size_t)y * W + x;
+            const F4 s = f4(planes[4 * i], planes[4 * i + 1], planes[4 * i + 2], planes[4 * i + 3]);
+            const float disp = (transform_x(s, (float)x, (float)y) - (float)x) * sidesign;
+            float v;
+            if (length3(xyz(s)) < 1e-4f || disp < 0 || disp > (float)W) v = 0.0f;
+            else v = fmaxf(disp, 0.0f);
+            out[i] = v * scale;
+        }
+    return 0;
+}
+
+int orc_fill_depthmap(float* out, const float* planes, int W, int H, float scale)
+{
+    const Img4 P = {planes, W, H};
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const F4 s = P.at(x, y);
+            const float cx = (float)x, cy = (float)y;
+            float v;
+            if (length3(xyz(s)) < 1e-4f) {
+                F4 l = f4(0, 0, 0, 0);
+                for (int xx = x - 1; length3(xyz(l)) < 1e-1f && xx >= 0; xx--) l = P.at(xx, y);
+                F4 rr = f4(0, 0, 0, 0);
+                for (int xx = x + 1; length3(xyz(rr)) < 1e-1f && xx < W; xx++) rr = P.at(xx, y);
+                if (length3(xyz(l)) < 1e-1f) { l.x = l.y = l.z = -1e5f; }
+                if (length3(xyz(rr)) < 1e-1f) { rr.x = rr.y = rr.z = -1e5f; }
+                l.w = -(transform_x(l, cx, cy) - cx);
+                rr.w = -(transform_x(rr, cx, cy) - cx);
+                v = fminf(l.w, rr.w);
+            } else {
+                v = fabsf(transform_x(s, cx, cy) - cx);
+            }
+            out[(size_t)y * W + x] = v * scale;
+        }
+    return 0;
+}
+
+int orc_fill_normalmap(float* out, const float* planes, int W, int H, int lr)
+{
+    (void)lr;
+    const Img4 P = {planes, W, H};
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const F4 s = P.at(x, y);
+            const float cx = (float)x, cy = (float)y;
+            F3 n;
+            if (length3(xyz(s)) < 1e-1f) {
+                F4 l = f4(0, 0, 0, 0);
+                for (int xx = x - 1; length3(xyz(l)) < 1e-1f && xx >= 0; xx--) l = P.at(xx, y);
+                F4 rr = f4(0, 0, 0, 0);
+                for (int xx = x + 1; length3(xyz(rr)) < 1e-1f && xx < W; xx++) rr = P.at(xx, y);
+                if (length3(xyz(l)) < 1e-1f) { l.x = l.y = l.z = -1e5f; }
+                if (length3(xyz(rr)) < 1e-1f) { rr.x = rr.y = rr.z = -1e5f; }
+                l.w = -(transform_x(l, cx, cy) - cx);
+                rr.w = -(transform_x(rr, cx, cy) - cx);
+                n = (l.w < rr.w) ? to_normal(l) : to_normal(rr);
+            } else {
+                n = to_normal(s);
+            }
+            put4(out, (size_t)y * W + x, f4(n.x, n.y, n.z, 0.0f));
+        }
+    return 0;
+}
+
+int orc_disparity_to_normal(float* out, const float* disp, int W, int H)
+{
+    auto d = [&](int x, int y) { return (x < 0 || x >= W || y < 0 || y >= H) ? 0.0f : disp[(size_t)y * W + x]; };
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const float dx = d(x + 1, y) - d(x, y);
+            const float dy = d(x, y + 1) - d(x, y);
+            /* cross((1,0,dx,0), (0,1,dy,0)) */
+            const F3 n = f3(0.0f * dy - dx * 1.0f, dx * 0.0f - 1.0f * dy, 1.0f * 1.0f - 0.0f * 0.0f);
+            const F3 nn = normalize3(n);
+            put4(out, (size_t)y * W + x, f4(nn.x, nn.y, nn.z, 0.0f));
+        }
+    return 0;
+}
+
+static const PmKernels ORC_KERNELS = {orc_prep, orc_init, orc_propagate, orc_normal_depth, orc_rof,
+                                      orc_consistency, orc_to_disparity, orc_fill_depthmap, orc_fill_normalmap,
+                                      orc_disparity_to_normal};
+
+int orc_disparity_map(const uint8_t* left, const uint8_t* right, int W, int H, int stride,
+                      int r, float dmax, int iterations, int pp, int views,
+                      float* dmap, float* normal, const float* initdisp, const float* initnormal,
+                      float* planesL, float* planesR, int fused, int64_t* counters)
+{
+    return pm_host_disparity_map(ORC_KERNELS, left, right, W, H, stride, r, dmax, iterations, pp, views, dmap, normal,
+                                 initdisp, initnormal, planesL, planesR, fused, counters, nullptr, nullptr);
+}
+
+int orc_disparity_map_dump(const uint8_t* left, const uint8_t* right, int W, int H, int stride,
+                           int r, float dmax, int iterations, int pp, int views,
+                           float* dmap, float* normal, const float* initdisp, const float* initnormal,
+                           float* planesL, float* planesR, int fused, int64_t* counters, PmDumpFn dump, void* user)
+{
+    return pm_host_disparity_map(ORC_KERNELS, left, right, W, H, stride, r, dmax, iterations, pp, views, dmap, normal,
+                                 initdisp, initnormal, planesL, planesR, fused, counters, dump, user);
+}
+
+}  // extern "C"

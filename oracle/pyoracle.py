@@ -1,0 +1,200 @@
+"""ORACLE — test infrastructure only (tests/, __graft_entry__.smoke(), bench.py's
+cpu_baseline leg).
+
+numpy front end of the two CPU checkers:
+  Oracle('orc')  the restatement, oracle/liboracle.so
+  Oracle('ref')  the reference's own kernel sources compiled through the
+                 OpenCL-C shim, oracle/_ref/libpmref.so (present where it was
+                 built from the reference tree)
+Both expose the same functions with the same arguments.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libpmref.so")
+
+vp = C.c_void_p
+i32 = C.c_int
+f32 = C.c_float
+DUMP_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_int, C.POINTER(C.c_float), C.c_void_p)
+
+
+def available(kind):
+    return os.path.exists(ORACLE_SO if kind == "orc" else REF_SO)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _f4(shape):
+    return np.zeros(shape + (4,), np.float32)
+
+
+class Oracle:
+    def __init__(self, kind="orc"):
+        self.kind = kind
+        path = ORACLE_SO if kind == "orc" else REF_SO
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.L = C.CDLL(path)
+        p = kind + "_"
+        sig = {
+            "prep": [vp, i32, i32, i32, i32, i32, vp, vp, vp],
+            "init": [vp, vp, vp, vp, vp, i32, i32, i32, f32, i32, vp, vp, i32],
+            "propagate": [vp, vp, vp, vp, vp, vp, vp, f32, i32, i32, i32, f32, i32, i32, vp, vp, vp, vp, vp, i32, vp],
+            "cost": [vp, vp, vp, vp, vp, vp, i32, i32, i32, f32, i32],
+            "klt": [vp, vp, vp, vp, vp, vp, i32, i32, i32, i32],
+            "normal_depth": [vp, vp, i32, i32, f32, i32],
+            "rof": [vp, vp, vp, C.POINTER(C.c_float), i32, i32, i32],
+            "consistency": [vp, vp, vp, i32, i32, f32, f32],
+            "to_disparity": [vp, vp, i32, i32, f32, i32],
+            "fill_depthmap": [vp, vp, i32, i32, f32],
+            "fill_normalmap": [vp, vp, i32, i32, i32],
+            "disparity_to_normal": [vp, vp, i32, i32],
+        }
+        for name, args in sig.items():
+            fn = getattr(self.L, p + name)
+            fn.restype = i32
+            fn.argtypes = args
+            setattr(self, "_" + name, fn)
+        if kind == "orc":
+            self.L.orc_disparity_map_dump.restype = i32
+            self.L.orc_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, vp, vp, vp, vp,
+                                                      vp, vp, i32, vp, DUMP_FN, vp]
+            for fn in ("orc_exp", "orc_sin", "orc_cos", "orc_acospi"):
+                getattr(self.L, fn).restype = f32
+                getattr(self.L, fn).argtypes = [f32]
+            self.L.orc_rng_floats.restype = i32
+            self.L.orc_rng_floats.argtypes = [C.c_int64, i32, i32, vp]
+        else:
+            self.L.ref_disparity_map_dump.restype = i32
+            self.L.ref_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, vp, vp, vp, vp,
+                                                      vp, vp, DUMP_FN, vp]
+
+    # ---- kernels -----------------------------------------------------------------
+    def prep(self, img, r, fused=0):
+        H, W = img.shape[:2]
+        img = np.ascontiguousarray(img)
+        bw, g, dt = _f4((H, W)), _f4((H, W)), _f4((H, W))
+        assert self._prep(img.ctypes.data, W, H, W * 4, r, fused, bw.ctypes.data, g.ctypes.data, dt.ctypes.data) == 0
+        return bw, g, dt
+
+    def init(self, bw1, bw2, g1, g2, r, dmax, lr, initdisp=None, initnormal=None, fused=0):
+        H, W = bw1.shape[:2]
+        out = _f4((H, W))
+        assert self._init(out.ctypes.data, _p(bw1), _p(bw2), _p(g1), _p(g2), W, H, r, dmax, lr, _p(initdisp),
+                          _p(initnormal), fused) == 0
+        return out
+
+    def propagate(self, old, bw1, bw2, g1, g2, smooth, theta, r, dmax, lr, it, vin_n=None, vin_val=None,
+                  scatter=True, fused=0, counters=None):
+        """Returns (planes, vout_n, vout_val, vout_src); vout_src is None for the reference build."""
+        H, W = old.shape[:2]
+        out = _f4((H, W))
+        vn = np.zeros((H, W), np.int32) if scatter else None
+        vv = np.zeros((H, W, 8), np.float32) if scatter else None
+        vs = np.full((H, W, 2), -1, np.int32) if (scatter and self.kind == "orc") else None
+        assert self._propagate(out.ctypes.data, _p(old), _p(bw1), _p(bw2), _p(g1), _p(g2), _p(smooth), theta, W, H, r,
+                               dmax, lr, it, _p(vin_n), _p(vin_val), _p(vn), _p(vv), _p(vs), fused,
+                               _p(counters)) == 0
+        return out, vn, vv, vs
+
+    def cost(self, planes, bw1, bw2, g1, g2, r, mincost, fused=0):
+        H, W = planes.shape[:2]
+        out = np.zeros((H, W), np.float32)
+        assert self._cost(out.ctypes.data, _p(planes), _p(bw1), _p(bw2), _p(g1), _p(g2), W, H, r, mincost, fused) == 0
+        return out
+
+    def klt(self, planes, bw1, bw2, g1, g2, r, fused=0):
+        H, W = planes.shape[:2]
+        out = _f4((H, W))
+        assert self._klt(out.ctypes.data, _p(planes), _p(bw1), _p(bw2), _p(g1), _p(g2), W, H, r, fused) == 0
+        return out
+
+    def normal_depth(self, planes, dispscale, lr):
+        H, W = planes.shape[:2]
+        out = _f4((H, W))
+        assert self._normal_depth(out.ctypes.data, _p(planes), W, H, dispscale, lr) == 0
+        return out
+
+    def rof(self, inp, dt, lam, iters):
+        H, W = inp.shape[:2]
+        out = _f4((H, W))
+        lam_c = (C.c_float * 4)(*lam)
+        assert self._rof(out.ctypes.data, _p(inp), _p(dt), lam_c, iters, W, H) == 0
+        return out
+
+    def consistency(self, left, right, maxdd=1.0, maxad=5.0):
+        H, W = left.shape[:2]
+        out = _f4((H, W))
+        assert self._consistency(out.ctypes.data, _p(left), _p(right), W, H, maxdd, maxad) == 0
+        return out
+
+    def to_disparity(self, planes, scale=1.0, lr=1):
+        H, W = planes.shape[:2]
+        out = np.zeros((H, W), np.float32)
+        assert self._to_disparity(out.ctypes.data, _p(planes), W, H, scale, lr) == 0
+        return out
+
+    def fill_depthmap(self, planes, scale=1.0):
+        H, W = planes.shape[:2]
+        out = np.zeros((H, W), np.float32)
+        assert self._fill_depthmap(out.ctypes.data, _p(planes), W, H, scale) == 0
+        return out
+
+    def fill_normalmap(self, planes, lr=1):
+        H, W = planes.shape[:2]
+        out = _f4((H, W))
+        assert self._fill_normalmap(out.ctypes.data, _p(planes), W, H, lr) == 0
+        return out
+
+    def disparity_to_normal(self, disp):
+        H, W = disp.shape[:2]
+        out = _f4((H, W))
+        assert self._disparity_to_normal(out.ctypes.data, _p(disp), W, H) == 0
+        return out
+
+    # ---- whole pipeline ------------------------------------------------------------
+    def disparity_map(self, left, right, r, dmax, iterations, pp=1, views=2, initdisp=None, initnormal=None,
+                      fused=0, dump=False, counters=None):
+        """PMHuberStereo::disparityMap.  Returns dict with dmap, normal, planesL, planesR
+        and, with dump=True, every intermediate stage keyed (stage, iter)."""
+        H, W = left.shape[:2]
+        left = np.ascontiguousarray(left)
+        right = np.ascontiguousarray(right)
+        res = {"dmap": np.zeros((H, W), np.float32), "normal": _f4((H, W)), "planesL": _f4((H, W)),
+               "planesR": _f4((H, W)), "stages": {}}
+        stages = res["stages"]
+
+        def cb(name, it, ptr, user):
+            stages[(name.decode(), it)] = np.ctypeslib.as_array(ptr, shape=(H, W, 4)).copy()
+
+        fn = DUMP_FN(cb) if dump else DUMP_FN()
+        common = [left.ctypes.data, right.ctypes.data, W, H, W * 4, r, dmax, iterations, pp, views,
+                  res["dmap"].ctypes.data, res["normal"].ctypes.data, _p(initdisp), _p(initnormal),
+                  res["planesL"].ctypes.data, res["planesR"].ctypes.data]
+        if self.kind == "orc":
+            st = self.L.orc_disparity_map_dump(*common, fused, _p(counters), fn, None)
+        else:
+            st = self.L.ref_disparity_map_dump(*common, fn, None)
+        assert st == 0, st
+        return res
+
+    # ---- helpers (restatement only) ------------------------------------------------
+    def rng_floats(self, linpos, nd, n):
+        out = np.zeros(n, np.float32)
+        assert self.L.orc_rng_floats(linpos, nd, n, out.ctypes.data) == 0
+        return out
+
+
+def bits_equal(a, b):
+    """Bitwise equality of float arrays with every NaN treated as equal."""
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    nan = np.isnan(a) & np.isnan(b)
+    return (a.view(np.uint32) == b.view(np.uint32)) | nan
