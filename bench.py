@@ -1,0 +1,303 @@
+"""Benchmark of the PatchMatch-Huber stereo path (cvt::PMHuberStereo::disparityMap).
+
+Workload (default `hd`): one 1280x720 RGBA8 pair from the procedural generator
+(40 slanted planes, disparity 2-120 px), disparity range 0-128, 21x21 window
+(patch half-width 10), 8 iterations (9 executed, the reference rounds up to
+odd), both views with view propagation, left-right check at 1 px / 5 deg.
+A step is one full disparityMap call: prep, init, 9 x (propagate L + R,
+40-step ROF smoothing per view), LR check, disparity conversion.
+
+Metric: Mpixel*iterations/s = width * height * executed iterations / step time.
+  value  device time (CUDA events per step) with inputs resident in HBM; L2 is
+         flushed (256 MiB write) between steps, outside the timed events
+  e2e    the public host API (numpy in, numpy out) including the host->device
+         copy of both images from pinned memory and the device->host copy of the
+         disparity map, timed with CUDA events around the call
+One process per GPU: each rank processes its own pair (weak scaling, no
+collective on the data path); the step time is the maximum over ranks.
+
+`--impl reference` times the reference's CPU implementation instead: the
+reference kernel sources compiled through the OpenCL-C shim (oracle/_ref) when
+built, otherwise the CPU restatement (oracle/), on a bounded crop of the same
+workload, using every host thread.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpixel·iterations/s"
+WORKLOADS = {
+    # name: (W, H, planes, dlo, dhi, patch half-width, dispmax, iterations, views, pp)
+    "hd": (1280, 720, 40, 2.0, 120.0, 10, 128.0, 8, 2, 1),
+    "small": (320, 240, 12, 2.0, 30.0, 7, 32.0, 4, 1, 0),
+}
+# bounded CPU samples (crop of the same scene, same window / range / iterations)
+CPU_CROP = {"hd": (128, 72), "small": (160, 120)}
+REF_CROP = {"hd": (96, 54), "small": (96, 72)}
+
+
+def executed(iters):
+    return iters | 1
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([s.strip() for s in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]
+                          and "Not" not in s[3 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def window_positions(W, H, r):
+    """sum over pixels of in-image window positions (the support weights computed once per pixel)"""
+    def axis(n):
+        i = np.arange(n)
+        return (np.minimum(r, n - 1 - i) + np.minimum(r, i) + 1).sum()
+    return int(axis(W)) * int(axis(H))
+
+
+def cpu_sample(kind_pref, crop, wl, scene_lr):
+    """time the CPU implementation on a crop; returns (Mpx*it/s, seconds, kind, cores)"""
+    from oracle import build as obuild
+    from oracle.pyoracle import Oracle, available
+
+    W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
+    cw, ch = crop
+    L, R = scene_lr
+    L = np.ascontiguousarray(L[:ch, :cw])
+    R = np.ascontiguousarray(R[:ch, :cw])
+    kind = "port"
+    if kind_pref == "reference" and available("ref"):
+        kind = "reference"
+    if kind == "port":
+        obuild.build_oracle()
+    o = Oracle("ref" if kind == "reference" else "orc")
+    t0 = time.perf_counter()
+    if kind == "reference":
+        o.disparity_map(L, R, r, dmax, iters, pp=pp, views=views)
+    else:
+        o.disparity_map(L, R, r, dmax, iters, pp=pp, views=views, fused=0)
+    dt = time.perf_counter() - t0
+    rate = cw * ch * executed(iters) / dt / 1e6
+    return rate, dt, kind, os.cpu_count()
+
+
+def run_reference(args, wl, rank, world):
+    """--impl reference: the reference's CPU implementation, rank 0 only"""
+    if rank != 0:
+        return
+    from cvt_b200 import scene
+
+    W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
+    crop = REF_CROP[args.config]
+    L, R = scene.generate(0, crop[0], crop[1], max(2, npl * crop[0] * crop[1] // (W * H) + 2), dlo, dhi)
+    for _ in range(args.warmup):
+        cpu_sample("reference", crop, wl, (L, R))
+    rates, secs = [], []
+    kind, cores = None, None
+    for _ in range(args.steps):
+        rate, dt, kind, cores = cpu_sample("reference", crop, wl, (L, R))
+        rates.append(rate)
+        secs.append(dt)
+    value = crop[0] * crop[1] * executed(iters) * len(secs) / sum(secs) / 1e6
+    sample = "%dx%d crop, window %dx%d, dispmax %g, %d iterations executed, %s" % (
+        crop[0], crop[1], 2 * r + 1, 2 * r + 1, dmax, executed(iters), "both views, LR check" if views == 2 else
+        "left view")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpixel·iterations/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "Mpixel·iterations/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "Mpixel·iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="hd", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.config]
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference(args, wl, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from cvt_b200 import PMHuberStereo, scene
+    from cvt_b200 import _lib
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
+    L, R = scene.generate(rank, W, H, npl, dlo, dhi)
+    dL, dR = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    pm = PMHuberStereo(views=views, fused=True, device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # counting pass (untimed): window samples of the propagate launches
+    pm.set_counting(True)
+    pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+    torch.cuda.synchronize()
+    ctr = pm.counters()
+    pm.set_counting(False)
+    for _ in range(args.warmup):
+        pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+    torch.cuda.synchronize()
+
+    # timed region
+    pm.set_profiling(True)
+    clocks = Clocks(local).start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    prop_ms, prop_n, launches = 0.0, 0, 0
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        ev[k][0].record()
+        pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+        ev[k][1].record()
+        ph = pm.phase_times()
+        prop_ms += ph["propagate"][0]
+        prop_n += ph["propagate"][1]
+        launches += ph["total"][1]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    pm.set_profiling(False)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(total, op=dist.ReduceOp.MAX)
+    total_ms = float(total.item())
+    px_it = W * H * executed(iters)
+    value = world * px_it * args.steps / (total_ms * 1e-3) / 1e6
+
+    # end to end through the host API: pinned host images in, disparity map out
+    pl = torch.from_numpy(L).pin_memory().numpy()
+    pr = torch.from_numpy(R).pin_memory().numpy()
+    pm.disparity_map(pl, pr, r, dmax, iters, pp=pp)
+    e2e = []
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        pm.disparity_map(pl, pr, r, dmax, iters, pp=pp)
+        b.record()
+        torch.cuda.synchronize()
+        e2e.append(a.elapsed_time(b))
+    e2e_t = torch.tensor([sum(e2e)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * px_it * args.steps / (float(e2e_t.item()) * 1e-3) / 1e6
+
+    # roofline of the propagate kernel (FP32-bound): algorithmic flops per launch
+    # = 10 per hoisted support weight + 41 per cost-window sample + 129 per
+    #   Gauss-Newton window sample, over the launch's measured average duration
+    nlaunch = views * executed(iters)
+    flops_launch = (10.0 * window_positions(W, H, r) * nlaunch + 41.0 * ctr[0] + 129.0 * ctr[1]) / nlaunch
+    avg_launch_s = prop_ms / max(prop_n, 1) * 1e-3
+    peak = C_float = None
+    import ctypes as C
+    pk = C.c_float(0.0)
+    if _lib.lib().pm_measure_fp32_peak(local, 200.0, C.byref(pk)) == 0:
+        peak = float(pk.value)
+    achieved = flops_launch / avg_launch_s / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "propagate_%s_dram.json" % args.config)
+    if os.path.exists(tfile):
+        traffic = json.load(open(tfile)).get("bytes_per_launch")
+    roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if peak else None, "traffic": traffic,
+            "kernel": "k_propagate", "avg_launch_ms": avg_launch_s * 1e3, "flops_per_launch": flops_launch,
+            "peak_source": "FP32 fma probe measured in this run (pm_measure_fp32_peak)"}
+
+    line = {"metric": METRIC, "value": value, "unit": "Mpixel·iterations/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config, "width": W, "height": H, "planes": npl, "dispmax": dmax,
+                       "window": 2 * r + 1, "iterations": iters, "iterations_executed": executed(iters),
+                       "views": views, "pp": "lrcheck" if pp == 1 else "none", "parallelism": "pairs%d" % world,
+                       "l2": "flushed between steps (256 MiB write)"},
+            "e2e": {"value": e2e_value, "unit": "Mpixel·iterations/s", "h2d_bytes_per_step": 2 * W * H * 4,
+                    "d2h_bytes_per_step": W * H * 4},
+            "roofline": roof, "clocks": clk, "gpu_launches": launches,
+            "counters": {"cost_samples": ctr[0], "gn_samples": ctr[1], "cost_evals": ctr[2], "early_exits": ctr[3]},
+            "phase_ms": {k: v[0] for k, v in pm.phase_times().items()}}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, dt, kind, cores = cpu_sample("port", CPU_CROP[args.config], wl, (L, R))
+        cw, ch = CPU_CROP[args.config]
+        line["cpu_baseline"] = {"value": rate, "unit": "Mpixel·iterations/s", "cores": cores, "kind": kind,
+                                "sample": "%dx%d crop of the same pair, same window/range/iterations, %.1f s" % (
+                                    cw, ch, dt)}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -20,6 +20,13 @@ struct pm_handle {
     std::string err;
     int counting = 0;
     uint64_t counters[4] = {0, 0, 0, 0};
+    // phase timing: events recorded at phase boundaries, summed per phase after the call
+    int profiling = 0;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> ev_phase, ev_launches;
+    int ev_used = 0;
+    float phase_ms[PM_NPHASES] = {0, 0, 0, 0, 0, 0};
+    int phase_launches[PM_NPHASES] = {0, 0, 0, 0, 0, 0};
     // device workspace for one image size
     int W = 0, H = 0;
     void* ws = nullptr;
@@ -58,6 +65,41 @@ int check_shape(pm_handle* h, int W, int H, int r)
 }
 
 inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
+
+// record a phase boundary: the interval since the previous mark belongs to `phase`
+// and contained `launches` kernel launches
+void prof_mark(pm_handle* h, cudaStream_t st, int phase, int launches)
+{
+    if (!h->profiling) return;
+    if (h->ev_used == (int)h->ev.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return; }
+        h->ev.push_back(e);
+        h->ev_phase.push_back(0);
+        h->ev_launches.push_back(0);
+    }
+    cudaEventRecord(h->ev[h->ev_used], st);
+    h->ev_phase[h->ev_used] = phase;
+    h->ev_launches[h->ev_used] = launches;
+    h->ev_used++;
+}
+
+int prof_collect(pm_handle* h, cudaStream_t st)
+{
+    if (!h->profiling) return PM_OK;
+    PM_CUDA(h, cudaStreamSynchronize(st));
+    for (int k = 0; k < PM_NPHASES; k++) { h->phase_ms[k] = 0.0f; h->phase_launches[k] = 0; }
+    for (int i = 1; i < h->ev_used; i++) {
+        float ms = 0.0f;
+        PM_CUDA(h, cudaEventElapsedTime(&ms, h->ev[i - 1], h->ev[i]));
+        h->phase_ms[h->ev_phase[i]] += ms;
+        h->phase_launches[h->ev_phase[i]] += h->ev_launches[i];
+        h->phase_ms[PM_PHASE_TOTAL] += ms;
+        h->phase_launches[PM_PHASE_TOTAL] += h->ev_launches[i];
+    }
+    h->ev_used = 0;
+    return PM_OK;
+}
 
 // workspace layout for a W x H pair (float4 fields unless noted)
 struct Layout {
@@ -141,6 +183,8 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
 
     PM_CUDA(h, cudaMemsetAsync(ctr, 0, 64, st));
     PM_CUDA(h, cudaMemsetAsync(errf, 0, 64, st));
+    h->ev_used = 0;
+    prof_mark(h, st, PM_PHASE_PREP, 0);
     // prep (PMHuberStereo.cpp:445-454)
     launch_prep(left, stride, W, H, r, F, Lbw, Lg, LDT, st);
     if (views == 2) launch_prep(right, stride, W, H, r, F, Rbw, Rg, RDT, st);
@@ -150,24 +194,31 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
     PM_CUDA(h, cudaMemsetAsync(Rs, 0, N * 16, st));
     launch_view_clear(vb1c, vb1s, N, st);
     launch_view_clear(vb2c, vb2s, N, st);
+    prof_mark(h, st, PM_PHASE_PREP, 4);
     // init (:469-470); the given disparity and normals apply to the left view only (:92-93)
+    int nl = 0;
     const float4* initn = initnormal;
     if (initdisp && !initnormal) {
         float4* nrm = at<float4>(ws, L, Layout::nrm);
         launch_disparity_to_normal(nrm, initdisp, W, H, st);   // :363-365
         initn = nrm;
+        nl++;
     }
     const ViewData VL = {Lbw, Rbw, Lg, Rg, W, H, r};
     const ViewData VR = {Rbw, Lbw, Rg, Lg, W, H, r};
     launch_init(mL[0], VL, dmax, 1, initdisp, initn, F, st);
-    if (views == 2) launch_init(mR[0], VR, dmax, 0, nullptr, nullptr, F, st);
+    nl++;
+    if (views == 2) { launch_init(mR[0], VR, dmax, 0, nullptr, nullptr, F, st); nl++; }
     const float thetamin = o.thetamin;
     float theta = thetamin;
+    const int rof_launches = (o.rof_iters > 0 && o.rof_iters % 2 == 0) ? o.rof_iters : o.rof_iters + 1;
     if (initdisp) {   // :473-477
         const float4 lam = make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);
         launch_normal_depth(tmp, mL[0], W, H, 1.0f / dmax, 1, st);
         launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
+        nl += 1 + rof_launches;
     }
+    prof_mark(h, st, PM_PHASE_INIT, nl);
     int swap = 0;
     iterations |= 1;   // :490
     for (int iter = 0; iter < iterations; iter++) {
@@ -202,12 +253,14 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
             P.vout_src = vb2s;
             launch_propagate(P, F, st);   // :542-543
         }
+        prof_mark(h, st, PM_PHASE_PROPAGATE, views);
         launch_normal_depth(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :552-553
         launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
         if (views == 2) {
             launch_normal_depth(tmp, mR[1 - swap], W, H, 1.0f / dmax, 0, st);   // :566-567
             launch_rof(Rs, tmp, RDT, lam, o.rof_iters, W, H, rofs, st);
         }
+        prof_mark(h, st, PM_PHASE_SMOOTH, views * (1 + rof_launches));
         theta = (float)iter / (float)iterations;   // :575-576
         theta = powf(theta, 4.0f) + thetamin;
         swap = 1 - swap;
@@ -215,19 +268,23 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
     float4* ml = mL[1];
     if (planesL) PM_CUDA(h, cudaMemcpyAsync(planesL, ml, N * 16, cudaMemcpyDeviceToDevice, st));
     if (planesR && views == 2) PM_CUDA(h, cudaMemcpyAsync(planesR, mR[1], N * 16, cudaMemcpyDeviceToDevice, st));
+    nl = 0;
     if (pp == PM_PP_NONE) {   // :123-129
-        if (dmap) launch_to_disparity(dmap, ml, W, H, 1.0f, 1, st);
-        if (normal) launch_fill_normalmap(normal, ml, W, H, st);
+        if (dmap) { launch_to_disparity(dmap, ml, W, H, 1.0f, 1, st); nl++; }
+        if (normal) { launch_fill_normalmap(normal, ml, W, H, st); nl++; }
     } else {   // :130-141
         launch_consistency(chk, ml, mR[1], W, H, o.maxdispdiff, o.maxanglediff, st);
+        nl++;
         if (dmap) {
             if (pp == PM_PP_LRCHECK) launch_to_disparity(dmap, chk, W, H, 1.0f, 1, st);
             else launch_fill_depthmap(dmap, chk, W, H, 1.0f, st);
+            nl++;
         }
-        if (normal) launch_fill_normalmap(normal, chk, W, H, st);
+        if (normal) { launch_fill_normalmap(normal, chk, W, H, st); nl++; }
     }
+    prof_mark(h, st, PM_PHASE_POST, nl);
     PM_CUDA(h, cudaGetLastError());
-    return PM_OK;
+    return prof_collect(h, st);
 }
 
 int check_args(pm_handle* h, const void* left, const void* right, int W, int H, size_t stride, int r, float dmax,
@@ -300,7 +357,58 @@ int pm_destroy(pm_handle* h)
 {
     if (!h) return PM_OK;
     if (h->ws) cudaFree(h->ws);
+    for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     delete h;
+    return PM_OK;
+}
+
+int pm_set_profiling(pm_handle* h, int on)
+{
+    if (!h) return PM_EINVAL_ARG;
+    h->profiling = on ? 1 : 0;
+    return PM_OK;
+}
+
+int pm_get_phase_times(pm_handle* h, float ms[PM_NPHASES], int launches[PM_NPHASES])
+{
+    if (!h) return PM_EINVAL_ARG;
+    for (int k = 0; k < PM_NPHASES; k++) {
+        if (ms) ms[k] = h->phase_ms[k];
+        if (launches) launches[k] = h->phase_launches[k];
+    }
+    return PM_OK;
+}
+
+int pm_measure_fp32_peak(int device, float ms, float* tflops)
+{
+    if (!tflops || !(ms > 0.0f)) return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    PM_CUDA(nullptr, cudaSetDevice(device));
+    float* buf = nullptr;
+    int sms = 0;
+    PM_CUDA(nullptr, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int blocks = sms * 8, threads = 256;
+    PM_CUDA(nullptr, cudaMalloc(&buf, (size_t)blocks * threads * sizeof(float)));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 0.0f;
+    int iters = 4096;
+    for (int rep = 0; rep < 6; rep++) {
+        cudaEventRecord(a);
+        launch_fma_peak(buf, iters, blocks, threads, 0);
+        cudaEventRecord(b);
+        cudaError_t e = cudaEventSynchronize(b);
+        if (e != cudaSuccess) { cudaFree(buf); return cuda_fail(nullptr, e, "fp32 peak kernel"); }
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, a, b);
+        const double flops = (double)blocks * threads * iters * fma_peak_flops_per_iter();
+        best = fmaxf(best, (float)(flops / (t * 1e-3) / 1e12));
+        if (t < ms && iters < (1 << 24)) iters = (int)(iters * fminf(8.0f, ms / fmaxf(t, 1e-3f)));
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(buf);
+    *tflops = best;
     return PM_OK;
 }
 

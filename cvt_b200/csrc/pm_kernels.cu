@@ -448,7 +448,36 @@ __global__ void k_view_clear(int* __restrict__ count, unsigned long long* __rest
 
 inline dim3 grid2d(int W, int H, dim3 b) { return dim3((W + b.x - 1) / b.x, (H + b.y - 1) / b.y); }
 
+// 8 independent fma chains per thread: enough instruction-level parallelism to keep
+// every FP32 pipe busy; the result is stored so that nothing is optimised away
+constexpr int FMA_CHAINS = 8;
+constexpr int FMA_UNROLL = 16;
+__global__ void k_fma_peak(float* out, int iters)
+{
+    float a[FMA_CHAINS];
+#pragma unroll
+    for (int k = 0; k < FMA_CHAINS; k++) a[k] = (float)(threadIdx.x + k) * 1e-3f;
+    const float m = 0.999f, c = 1e-4f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < FMA_UNROLL; u++) {
+#pragma unroll
+            for (int k = 0; k < FMA_CHAINS; k++) a[k] = fmaf(a[k], m, c);
+        }
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < FMA_CHAINS; k++) s += a[k];
+    out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace
+
+void launch_fma_peak(float* out, int iters, int blocks, int threads, cudaStream_t st)
+{
+    k_fma_peak<<<blocks, threads, 0, st>>>(out, iters);
+}
+double fma_peak_flops_per_iter() { return 2.0 * FMA_CHAINS * FMA_UNROLL; }
 
 // ---- launchers ----------------------------------------------------------------------
 

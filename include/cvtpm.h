@@ -96,6 +96,18 @@ int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* ri
 int pm_set_counting(pm_handle* h, int on);
 int pm_get_counters(pm_handle* h, uint64_t counters[4]);
 
+/* Phase timing of the last pm_disparity_map* call (CUDA events on its stream) when
+ * enabled with pm_set_profiling(h, 1); the call then synchronises its stream before
+ * returning.  ms[PM_PHASE_*] in milliseconds; launches[PM_PHASE_*] kernel launches. */
+enum { PM_PHASE_PREP = 0, PM_PHASE_INIT = 1, PM_PHASE_PROPAGATE = 2, PM_PHASE_SMOOTH = 3, PM_PHASE_POST = 4,
+       PM_PHASE_TOTAL = 5, PM_NPHASES = 6 };
+int pm_set_profiling(pm_handle* h, int on);
+int pm_get_phase_times(pm_handle* h, float ms[6], int launches[6]);
+
+/* FP32 FMA throughput of `device` in TFLOP/s (2 flop per FMA), measured with a
+ * kernel of independent fma chains over every SM for about `ms` milliseconds. */
+int pm_measure_fp32_peak(int device, float ms, float* tflops);
+
 /* Batched form: n independent pairs, each with its own size, patch size and
  * disparity range, processed together (one launch per stage for all pairs).
  * Arrays are indexed by pair; device pointers; outputs as in pm_disparity_map_device. */

@@ -1,0 +1,88 @@
+"""Generate the golden fixtures of tests/golden/ from the reference kernels.
+
+The outputs come from cvt/cl/kernel/pmhstereo.cl, PDDiffTensor.cl and
+PDDROFDiffTensor.cl compiled from their own source through the OpenCL-C shim
+(oracle/build.py -> oracle/_ref/libpmref.so), driven by the restated host loop
+of PMHuberStereo::disparityMap.  Inputs are seeded procedural scenes from
+cvt_b200.scene.  Run from the repository root where the reference tree is
+available:
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from cvt_b200 import scene  # noqa: E402
+from oracle import build as obuild  # noqa: E402
+from oracle.pyoracle import Oracle  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# name: (seed, W, H, nplanes, dlo, dhi, r, dmax, iterations, pp, views, init_from_gt)
+CASES = {
+    "lr_40x28": (3, 40, 28, 5, 2.0, 10.0, 3, 12.0, 3, 1, 2, False),
+    "odd_33x19": (7, 33, 19, 4, 1.0, 8.0, 2, 10.0, 2, 2, 2, False),
+    "left_36x24": (4, 36, 24, 4, 2.0, 8.0, 2, 10.0, 2, 0, 1, False),
+    "init_40x28": (5, 40, 28, 5, 2.0, 10.0, 3, 12.0, 1, 2, 2, True),
+}
+
+
+def make_case(ref, name, spec):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, pp, views, init = spec
+    left, right, gtd, gtn = scene.generate(seed, W, H, npl, dlo, dhi, with_gt=True)
+    initd = gtd.copy() if init else None
+    if init:
+        initd[::5, ::3] = 0.0   # some pixels without a given disparity take the random init
+    res = ref.disparity_map(left, right, r, dmax, iters, pp=pp, views=views, initdisp=initd, dump=True)
+    arrays = {"left": left, "right": right, "dmap": res["dmap"], "normal": res["normal"],
+              "planesL": res["planesL"], "spec": np.array([seed, W, H, npl, dlo, dhi, r, dmax, iters, pp, views,
+                                                           int(init)], np.float64)}
+    if views == 2:
+        arrays["planesR"] = res["planesR"]
+    if init:
+        arrays["initdisp"] = initd
+    for (stage, it), v in res["stages"].items():
+        arrays["stage_%s_%d" % (stage, it)] = v
+    # per-kernel fixtures on the first view
+    bwL, gL, dtL = ref.prep(left, r)
+    bwR, gR, dtR = ref.prep(right, r)
+    arrays.update(bwL=bwL, gL=gL, dtL=dtL, bwR=bwR, gR=gR, dtR=dtR)
+    rng = np.random.default_rng(seed)
+    planes = res["stages"][("init_left", -1)].copy()
+    # a few awkward planes: non-finite, steep, far outside the image
+    planes[0, 0] = [np.nan, 0, 0, 0]
+    planes[1, 1] = [np.inf, 1, 1, 0]
+    planes[2, 2] = [40.0, 3.0, -900.0, 0]
+    planes[3, 3] = [1.0, 0.0, -1e6, 0]
+    arrays["k_planes"] = planes
+    arrays["k_cost_inf"] = ref.cost(planes, bwL, bwR, gL, gR, r, 1e10)
+    arrays["k_cost_02"] = ref.cost(planes, bwL, bwR, gL, gR, r, 0.2)
+    arrays["k_klt"] = ref.klt(planes, bwL, bwR, gL, gR, r)
+    smooth = (rng.random((H, W, 4), np.float32) * np.array([0.2, 0.2, 1.0, 1.0], np.float32)).astype(np.float32)
+    arrays["k_smooth"] = smooth
+    pout, vn, vv, _ = ref.propagate(planes, bwL, bwR, gL, gR, smooth, 0.37, r, dmax, 1, 1)
+    arrays.update(k_prop=pout, k_prop_vn=vn, k_prop_vv=vv)
+    nd = ref.normal_depth(planes, 1.0 / dmax, 1)
+    arrays["k_nd"] = nd
+    arrays["k_rof"] = ref.rof(nd, dtL, [1.3, 1.3, 1.3, 1.0], 40)
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+
+
+def main():
+    so = obuild.build_ref()
+    if so is None:
+        sys.exit("the reference kernels are not available (no reference tree and no prebuilt oracle/_ref)")
+    obuild.build_oracle()
+    ref = Oracle("ref")
+    for name, spec in CASES.items():
+        make_case(ref, name, spec)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()

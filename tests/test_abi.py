@@ -1,0 +1,110 @@
+"""The C-ABI library without a GPU: it loads, exports every declared entry point,
+rejects bad arguments, and its host-evaluated arithmetic (the same code the
+kernels run) equals the oracle's."""
+import ctypes as C
+import hashlib
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "cvtpm.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(pm_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_exports_every_declared_symbol(native):
+    from cvt_b200 import _lib
+
+    names = declared_functions()
+    assert len(names) >= 25
+    for n in names:
+        assert hasattr(native, n), n
+    assert sorted(_lib.SYMBOLS) == names
+
+
+def test_rejects_bad_shapes_without_touching_the_device(native):
+    from cvt_b200 import _lib
+
+    assert native.pm_k_prep(None, 0, 10, 40, 2, 1, None, None, None, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_k_prep(None, 10, 10, 40, 99, 1, None, None, None, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_k_prep(None, 5000, 10, 20000, 2, 1, None, None, None, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_k_prep(None, 10, 10, 40, 2, 1, None, None, None, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_k_init(None, None, None, None, None, 8, 8, 2, 4.0, 1, None, None, 1, None) == _lib.PM_EINVAL_ARG
+    assert b"null" in native.pm_last_error(None)
+
+
+def test_create_fails_loudly_without_device(native):
+    import torch
+
+    from cvt_b200 import _lib
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    h = C.c_void_p()
+    assert native.pm_create(C.byref(h), None) == _lib.PM_ENODEV
+    from cvt_b200 import PMHuberStereo, StereoError
+
+    with pytest.raises(StereoError):
+        PMHuberStereo()
+
+
+def test_rng_matches_oracle(native, orc):
+    for lin, nd in ((0, 3), (1, 3), (1234, 3), (77, 6), (921599 * 6 + 8, 1), (4000000, 6)):
+        a = np.zeros(16, np.float32)
+        assert native.pm_rng_floats(lin, nd, 16, a.ctypes.data) == 0
+        b = orc.rng_floats(lin, nd, 16)
+        assert (a.view(np.uint32) == b.view(np.uint32)).all(), (lin, nd)
+
+
+def test_elementary_functions_match_oracle(native, orc):
+    rng = np.random.default_rng(0)
+    xs = np.concatenate([np.linspace(-40, 0, 4001), rng.uniform(-104, 89, 4000), [0.0, -0.0, 88.7, -103.9]])
+    for x in xs.astype(np.float32):
+        assert np.float32(native.pm_expf_host(float(x))).view(np.uint32) == \
+            np.float32(orc.L.orc_exp(float(x))).view(np.uint32), x
+    for x in np.concatenate([np.linspace(0, 6.3, 4001), rng.uniform(-100, 100, 2000)]).astype(np.float32):
+        assert np.float32(native.pm_sinf_host(float(x))).view(np.uint32) == np.float32(orc.L.orc_sin(float(x))).view(np.uint32)
+        assert np.float32(native.pm_cosf_host(float(x))).view(np.uint32) == np.float32(orc.L.orc_cos(float(x))).view(np.uint32)
+    for x in np.linspace(-1, 1, 4001).astype(np.float32):
+        assert np.float32(native.pm_acospif_host(float(x))).view(np.uint32) == \
+            np.float32(orc.L.orc_acospi(float(x))).view(np.uint32)
+
+
+def test_exit_threshold_is_exact(native):
+    """census >= threshold(m, b)  <=>  RN(census / b) >= m, around the threshold."""
+    rng = np.random.default_rng(1)
+    for _ in range(3000):
+        b = np.float32(rng.uniform(1.0, 450.0))
+        m = np.float32(rng.choice([rng.uniform(0, 1.2), rng.uniform(1e-8, 1e-3), rng.uniform(0.9, 1.1)]))
+        t = np.float32(native.pm_exit_threshold_host(float(m), float(b)))
+        assert np.isfinite(t) and t >= 0
+        below = np.nextafter(t, np.float32(-1))
+        assert np.float32(t / b) >= m
+        if t > 0:
+            assert not (np.float32(below / b) >= m)
+    assert native.pm_exit_threshold_host(0.0, 3.0) == -np.inf
+    assert native.pm_exit_threshold_host(-1.0, 3.0) == -np.inf
+    assert np.isnan(native.pm_exit_threshold_host(float("nan"), 3.0))
+    assert native.pm_exit_threshold_host(float("inf"), 3.0) == np.inf
+
+
+def test_scene_generator_is_deterministic(native):
+    from cvt_b200 import scene
+
+    L1, R1, d1, n1 = scene.generate(1234, 96, 64, 8, 2.0, 30.0, with_gt=True)
+    L2, R2 = scene.generate(1234, 96, 64, 8, 2.0, 30.0)
+    assert (L1 == L2).all() and (R1 == R2).all()
+    assert d1.min() >= 2.0 - 1e-4 and d1.max() <= 30.0 + 1e-4
+    assert np.abs(n1[..., :2]).max() <= 0.3 + 1e-6
+    # the same bytes on every host: pinned digests
+    h = hashlib.sha256(L1.tobytes() + R1.tobytes()).hexdigest()
+    assert h == SCENE_DIGEST, h
+
+
+SCENE_DIGEST = "54e0dc1c90811ccd82790abf7eceef416b3e1e22cc42747722fc6a5d7d1094ca"

@@ -1,0 +1,327 @@
+"""Parity of the sm_100a kernels with the oracle, through the C ABI.
+
+strict mode (fused=0) must reproduce the reference-kernel golden fixtures bit
+for bit; fused mode (the default) must reproduce the oracle's fused
+restatement bit for bit.  NaN payloads are not compared (every NaN equals
+every NaN).  Larger sizes are checked against the oracle where it finishes in
+seconds and through size-independent properties beyond that.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+from oracle.pyoracle import bits_equal
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda(native):
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    import torch
+
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def stream(torch):
+    return torch.cuda.current_stream().cuda_stream
+
+
+def spec_of(g):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, pp, views, init = g["spec"]
+    return int(W), int(H), int(r), float(dmax), int(iters), int(pp), int(views)
+
+
+def viewprop_np(p):
+    p = p.astype(np.float32)
+    with np.errstate(all="ignore"):
+        r = np.stack([np.float32(1.0) / p[..., 0], -p[..., 1] / p[..., 0], -p[..., 2] / p[..., 0],
+                      np.zeros_like(p[..., 0])], -1).astype(np.float32)
+    small = np.abs(p[..., 0]) < np.float32(1e-8)
+    r[small] = np.stack([np.zeros_like(p[..., 0]), -p[..., 1], -p[..., 2], np.zeros_like(p[..., 0])], -1)[small]
+    return r
+
+
+class Dev:
+    """Per-kernel calls through the C ABI on device buffers."""
+
+    def __init__(self, torch, L):
+        self.t, self.L = torch, L
+
+    def f4(self, H, W):
+        return self.t.zeros((H, W, 4), dtype=self.t.float32, device="cuda")
+
+    def prep(self, img, r, fused):
+        H, W = img.shape[:2]
+        d = dev(self.t, img)
+        bw, g, dt = self.f4(H, W), self.f4(H, W), self.f4(H, W)
+        assert self.L.pm_k_prep(d.data_ptr(), W, H, W * 4, r, fused, bw.data_ptr(), g.data_ptr(), dt.data_ptr(),
+                                stream(self.t)) == 0
+        return bw, g, dt
+
+    def init(self, bw1, bw2, g1, g2, r, dmax, lr, fused, initd=None, initn=None):
+        H, W = bw1.shape[:2]
+        out = self.f4(H, W)
+        assert self.L.pm_k_init(out.data_ptr(), bw1.data_ptr(), bw2.data_ptr(), g1.data_ptr(), g2.data_ptr(), W, H, r,
+                                dmax, lr, None if initd is None else initd.data_ptr(),
+                                None if initn is None else initn.data_ptr(), fused, stream(self.t)) == 0
+        return out
+
+    def cost(self, P, bw1, bw2, g1, g2, r, mincost, fused):
+        H, W = P.shape[:2]
+        out = self.t.zeros((H, W), dtype=self.t.float32, device="cuda")
+        assert self.L.pm_k_cost(out.data_ptr(), P.data_ptr(), bw1.data_ptr(), bw2.data_ptr(), g1.data_ptr(),
+                                g2.data_ptr(), W, H, r, mincost, fused, stream(self.t)) == 0
+        return out
+
+    def klt(self, P, bw1, bw2, g1, g2, r, fused):
+        H, W = P.shape[:2]
+        out = self.f4(H, W)
+        assert self.L.pm_k_klt(out.data_ptr(), P.data_ptr(), bw1.data_ptr(), bw2.data_ptr(), g1.data_ptr(),
+                               g2.data_ptr(), W, H, r, fused, stream(self.t)) == 0
+        return out
+
+    def empty_view(self, H, W):
+        return (self.t.zeros((H, W), dtype=self.t.int32, device="cuda"),
+                self.t.full((H, W), -1, dtype=self.t.int64, device="cuda"))
+
+    def propagate(self, old, bw1, bw2, g1, g2, smooth, theta, r, dmax, lr, it, vin=None, vin_planes=None,
+                  vout=None, fused=1, counters=None):
+        H, W = old.shape[:2]
+        out = self.f4(H, W)
+        p = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        vic, vis = vin if vin is not None else (None, None)
+        voc, vos = vout if vout is not None else (None, None)
+        assert self.L.pm_k_propagate(out.data_ptr(), old.data_ptr(), bw1.data_ptr(), bw2.data_ptr(), g1.data_ptr(),
+                                     g2.data_ptr(), smooth.data_ptr(), theta, W, H, r, dmax, lr, it, p(vic), p(vis),
+                                     p(vin_planes), p(voc), p(vos), fused, p(counters), stream(self.t)) == 0
+        return out
+
+
+@pytest.fixture(scope="module")
+def D(torch_cuda, native):
+    return Dev(torch_cuda, native)
+
+
+def src_pairs(vs):
+    """view-buffer source columns (int64 holding two uint32) -> (lo, hi) int arrays, -1 if empty"""
+    u = vs.view(np.uint64) if vs.dtype == np.int64 else vs
+    lo = (u & np.uint64(0xffffffff)).astype(np.int64)
+    hi = (u >> np.uint64(32)).astype(np.int64)
+    lo[lo == 0xffffffff] = -1
+    hi[hi == 0xffffffff] = -1
+    return lo, hi
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_kernels_strict_match_reference_golden(D, case):
+    g = load_golden(case)
+    W, H, r, dmax, iters, pp, views = spec_of(g)
+    bwL, gL, dtL = D.prep(g["left"], r, 0)
+    bwR, gR, dtR = D.prep(g["right"], r, 0)
+    for t, k in ((bwL, "bwL"), (gL, "gL"), (dtL, "dtL"), (bwR, "bwR"), (gR, "gR"), (dtR, "dtR")):
+        assert bits_equal(host(t), g[k]).all(), k
+    P = dev(D.t, g["k_planes"])
+    assert bits_equal(host(D.cost(P, bwL, bwR, gL, gR, r, 1e10, 0)), g["k_cost_inf"]).all()
+    assert bits_equal(host(D.cost(P, bwL, bwR, gL, gR, r, 0.2, 0)), g["k_cost_02"]).all()
+    assert bits_equal(host(D.klt(P, bwL, bwR, gL, gR, r, 0)), g["k_klt"]).all()
+    vout = D.empty_view(H, W)
+    out = D.propagate(P, bwL, bwR, gL, gR, dev(D.t, g["k_smooth"]), 0.37, r, dmax, 1, 1, vout=vout, fused=0)
+    out_h = host(out)
+    assert bits_equal(out_h, g["k_prop"]).all()
+    vn = host(vout[0])
+    assert (vn == g["k_prop_vn"]).all()
+    lo, hi = src_pairs(host(vout[1]))
+    ys = np.arange(H)[:, None].repeat(W, 1)
+    for k, src in enumerate((lo, hi)):
+        m = np.minimum(vn, 2) > k
+        vals = viewprop_np(out_h[ys[m], src[m]])
+        assert bits_equal(vals, g["k_prop_vv"][..., 4 * k:4 * k + 4][m]).all()
+    nd = D.f4(H, W)
+    assert D.L.pm_k_normal_depth(nd.data_ptr(), P.data_ptr(), W, H, 1.0 / dmax, 1, stream(D.t)) == 0
+    assert bits_equal(host(nd), g["k_nd"]).all()
+    scratch = D.t.zeros(D.L.pm_rof_scratch_bytes(W, H), dtype=D.t.uint8, device="cuda")
+    ro = D.f4(H, W)
+    lam = (C.c_float * 4)(1.3, 1.3, 1.3, 1.0)
+    assert D.L.pm_k_rof(ro.data_ptr(), nd.data_ptr(), dtL.data_ptr(), lam, 40, W, H, scratch.data_ptr(),
+                        stream(D.t)) == 0
+    assert bits_equal(host(ro), g["k_rof"]).all()
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_kernels_fused_match_oracle(D, orc, case):
+    g = load_golden(case)
+    W, H, r, dmax, iters, pp, views = spec_of(g)
+    bwL, gL, dtL = D.prep(g["left"], r, 1)
+    bwR, gR, dtR = D.prep(g["right"], r, 1)
+    obwL, ogL, odtL = orc.prep(g["left"], r, fused=1)
+    obwR, ogR, _ = orc.prep(g["right"], r, fused=1)
+    assert bits_equal(host(bwL), obwL).all() and bits_equal(host(gL), ogL).all() and bits_equal(host(dtL), odtL).all()
+    P = dev(D.t, g["k_planes"])
+    for m in (1e10, 0.2, 0.05):
+        assert bits_equal(host(D.cost(P, bwL, bwR, gL, gR, r, m, 1)),
+                          orc.cost(g["k_planes"], obwL, obwR, ogL, ogR, r, m, fused=1)).all(), m
+    assert bits_equal(host(D.klt(P, bwL, bwR, gL, gR, r, 1)),
+                      orc.klt(g["k_planes"], obwL, obwR, ogL, ogR, r, fused=1)).all()
+    init = host(D.init(bwL, bwR, gL, gR, r, dmax, 1, 1))
+    assert bits_equal(init, orc.init(obwL, obwR, ogL, ogR, r, dmax, 1, fused=1)).all()
+
+
+def test_propagate_view_exchange_matches_oracle(D, orc):
+    """Left propagate scatters into the view buffer, right propagate consumes it."""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(21, 64, 40, 6, 2.0, 14.0)
+    r, dmax = 3, 16.0
+    for fused in (0, 1):
+        bwL, gL, _ = D.prep(L, r, fused)
+        bwR, gR, _ = D.prep(R, r, fused)
+        obwL, ogL, _ = orc.prep(L, r, fused=fused)
+        obwR, ogR, _ = orc.prep(R, r, fused=fused)
+        iL = orc.init(obwL, obwR, ogL, ogR, r, dmax, 1, fused=fused)
+        iR = orc.init(obwR, obwL, ogR, ogL, r, dmax, 0, fused=fused)
+        sm = np.zeros((40, 64, 4), np.float32)
+        # oracle: left then right
+        oL, vn1, vv1, vs1 = orc.propagate(iL, obwL, obwR, ogL, ogR, sm, 0.3, r, dmax, 1, 2, fused=fused)
+        oR, vn2, vv2, vs2 = orc.propagate(iR, obwR, obwL, ogR, ogL, sm, 0.3, r, dmax, 0, 2, vin_n=vn1, vin_val=vv1,
+                                          fused=fused)
+        # device
+        vb1, vb2 = D.empty_view(40, 64), D.empty_view(40, 64)
+        smd = dev(D.t, sm)
+        dL = D.propagate(dev(D.t, iL), bwL, bwR, gL, gR, smd, 0.3, r, dmax, 1, 2, vout=vb1, fused=fused)
+        assert bits_equal(host(dL), oL).all()
+        assert (host(vb1[0]) == vn1).all()
+        lo, hi = src_pairs(host(vb1[1]))
+        assert (lo == vs1[..., 0]).all() and (hi == vs1[..., 1]).all()
+        dR = D.propagate(dev(D.t, iR), bwR, bwL, gR, gL, smd, 0.3, r, dmax, 0, 2, vin=vb1, vin_planes=dL, vout=vb2,
+                         fused=fused)
+        assert bits_equal(host(dR), oR).all()
+        assert (host(vb1[0]) == 0).all(), "the consumed view buffer is left empty"
+        assert (host(vb2[0]) == vn2).all()
+
+
+def test_post_kernels_match_oracle(D, orc):
+    g = load_golden("lr_40x28")
+    W, H = 40, 28
+    Lp, Rp = g["planesL"], g["planesR"]
+    dL, dR = dev(D.t, Lp), dev(D.t, Rp)
+    chk = D.f4(H, W)
+    assert D.L.pm_k_consistency(chk.data_ptr(), dL.data_ptr(), dR.data_ptr(), W, H, 1.0, 5.0, stream(D.t)) == 0
+    ochk = orc.consistency(Lp, Rp)
+    assert bits_equal(host(chk), ochk).all()
+    out = D.t.zeros((H, W), dtype=D.t.float32, device="cuda")
+    assert D.L.pm_k_to_disparity(out.data_ptr(), chk.data_ptr(), W, H, 1.0, 1, stream(D.t)) == 0
+    assert bits_equal(host(out), orc.to_disparity(ochk)).all()
+    assert D.L.pm_k_fill_depthmap(out.data_ptr(), chk.data_ptr(), W, H, 1.0, stream(D.t)) == 0
+    assert bits_equal(host(out), orc.fill_depthmap(ochk)).all()
+    nm = D.f4(H, W)
+    assert D.L.pm_k_fill_normalmap(nm.data_ptr(), chk.data_ptr(), W, H, 1, stream(D.t)) == 0
+    assert bits_equal(host(nm), orc.fill_normalmap(ochk)).all()
+    disp = orc.to_disparity(Lp)
+    assert D.L.pm_k_disparity_to_normal(nm.data_ptr(), dev(D.t, disp).data_ptr(), W, H, stream(D.t)) == 0
+    assert bits_equal(host(nm), orc.disparity_to_normal(disp)).all()
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_pipeline_strict_matches_reference_golden(native, torch_cuda, case):
+    from cvt_b200 import PMHuberStereo
+
+    g = load_golden(case)
+    W, H, r, dmax, iters, pp, views = spec_of(g)
+    pm = PMHuberStereo(views=views, fused=False)
+    res = pm.disparity_map(g["left"], g["right"], r, dmax, iters, pp=pp, normalmap=True, planes=True,
+                           initdisparity=g.get("initdisp"))
+    assert bits_equal(res["planes_left"], g["planesL"]).all()
+    if views == 2:
+        assert bits_equal(res["planes_right"], g["planesR"]).all()
+    assert bits_equal(res["dmap"], g["dmap"]).all()
+    assert bits_equal(res["normal"], g["normal"]).all()
+
+
+@pytest.mark.parametrize("W,H,r,dmax,iters,seed", [(96, 64, 5, 24.0, 3, 1), (150, 101, 7, 32.0, 2, 2)])
+def test_pipeline_fused_matches_oracle(native, torch_cuda, orc, W, H, r, dmax, iters, seed):
+    from cvt_b200 import PMHuberStereo, scene
+
+    L, R = scene.generate(seed, W, H, 8, 2.0, dmax - 2.0)
+    ctr = np.zeros(4, np.int64)
+    o = orc.disparity_map(L, R, r, dmax, iters, pp=1, fused=1, counters=ctr)
+    pm = PMHuberStereo(fused=True)
+    pm.set_counting(True)
+    res = pm.disparity_map(L, R, r, dmax, iters, pp=1, normalmap=True, planes=True)
+    assert bits_equal(res["planes_left"], o["planesL"]).all()
+    assert bits_equal(res["planes_right"], o["planesR"]).all()
+    assert bits_equal(res["dmap"], o["dmap"]).all()
+    assert bits_equal(res["normal"], o["normal"]).all()
+    assert pm.counters() == [int(v) for v in ctr], "window-sample counts equal the oracle's"
+
+
+def test_device_entry_matches_host_entry(native, torch_cuda):
+    from cvt_b200 import PMHuberStereo, scene
+
+    torch = torch_cuda
+    L, R = scene.generate(5, 128, 72, 6, 2.0, 20.0)
+    pm = PMHuberStereo()
+    a = pm.disparity_map(L, R, 4, 24.0, 2, normalmap=True)
+    b = pm.disparity_map(dev(torch, L), dev(torch, R), 4, 24.0, 2, normalmap=True)
+    assert bits_equal(host(b["dmap"]), a["dmap"]).all()
+    assert bits_equal(host(b["normal"]), a["normal"]).all()
+
+
+def test_errors_raise(native, torch_cuda):
+    from cvt_b200 import PMHuberStereo, StereoError, scene
+
+    L, R = scene.generate(5, 32, 24, 3, 2.0, 8.0)
+    pm = PMHuberStereo()
+    with pytest.raises(StereoError):
+        pm.disparity_map(L, R[:, :16], 2, 8.0, 1)
+    with pytest.raises(StereoError):
+        pm.disparity_map(L, R, 99, 8.0, 1)
+    with pytest.raises(StereoError):
+        pm.disparity_map(L, R, 2, -1.0, 1)
+    with pytest.raises(StereoError):
+        PMHuberStereo(views=1).disparity_map(L, R, 2, 8.0, 1, pp=1)
+    # the handle stays usable after an error
+    assert pm.disparity_map(L, R, 2, 8.0, 1).shape == (24, 32)
+
+
+def test_left_view_small_config_matches_oracle(native, torch_cuda, orc):
+    """The 320x240, 15x15-window, 4(->5)-iteration left-view configuration, at full size."""
+    from cvt_b200 import PMHuberStereo, scene
+
+    L, R = scene.workload("small", seed=0)
+    o = orc.disparity_map(L, R, 7, 32.0, 4, pp=0, views=1, fused=1)
+    pm = PMHuberStereo(views=1, fused=True)
+    res = pm.disparity_map(L, R, 7, 32.0, 4, pp=0, planes=True)
+    assert bits_equal(res["planes_left"], o["planesL"]).all()
+    assert bits_equal(res["dmap"], o["dmap"]).all()
+
+
+def test_hd_config_is_deterministic_and_accurate(native, torch_cuda):
+    """1280x720, disparity 0-128, 21x21, 8 iterations, both views: size-independent checks."""
+    from cvt_b200 import PMHuberStereo, scene
+
+    torch = torch_cuda
+    L, R, gt, _ = scene.generate(0, 1280, 720, 40, 2.0, 120.0, with_gt=True)
+    pm = PMHuberStereo()
+    a = pm.disparity_map(dev(torch, L), dev(torch, R), 10, 128.0, 8, pp=1, planes=True)
+    b = pm.disparity_map(dev(torch, L), dev(torch, R), 10, 128.0, 8, pp=1, planes=True)
+    for k in ("dmap", "planes_left", "planes_right"):
+        assert bits_equal(host(a[k]), host(b[k])).all(), k
+    d = host(a["dmap"])
+    valid = d > 0
+    assert valid.mean() > 0.5
+    good = np.abs(d - gt)[valid] < 1.0
+    assert good.mean() > 0.8, good.mean()

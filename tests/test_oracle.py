@@ -1,0 +1,137 @@
+"""The CPU oracle: pinned against the reference kernels (golden fixtures and, where
+the reference tree is present, a live build of its own source), plus known-answer
+tests for the arithmetic it fixes."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+from oracle.pyoracle import bits_equal
+
+
+def spec_of(g):
+    s = g["spec"]
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, pp, views, init = s
+    return dict(W=int(W), H=int(H), r=int(r), dmax=float(dmax), iters=int(iters), pp=int(pp), views=int(views),
+                init=bool(init))
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_restatement_matches_reference_golden(orc, case):
+    """Every stage of PMHuberStereo::disparityMap, bit for bit (strict arithmetic)."""
+    g = load_golden(case)
+    s = spec_of(g)
+    res = orc.disparity_map(g["left"], g["right"], s["r"], s["dmax"], s["iters"], pp=s["pp"], views=s["views"],
+                            initdisp=g.get("initdisp"), dump=True, fused=0)
+    for (stage, it), v in res["stages"].items():
+        ok = bits_equal(v, g["stage_%s_%d" % (stage, it)])
+        assert ok.all(), (case, stage, it, ok.mean())
+    for k in ("dmap", "normal", "planesL") + (("planesR",) if s["views"] == 2 else ()):
+        assert bits_equal(res[k], g[k]).all(), (case, k)
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_restatement_kernels_match_reference_golden(orc, case):
+    g = load_golden(case)
+    s = spec_of(g)
+    r, dmax = s["r"], s["dmax"]
+    bwL, gL, dtL = orc.prep(g["left"], r)
+    bwR, gR, dtR = orc.prep(g["right"], r)
+    for a, k in ((bwL, "bwL"), (gL, "gL"), (dtL, "dtL"), (bwR, "bwR"), (gR, "gR"), (dtR, "dtR")):
+        assert bits_equal(a, g[k]).all(), k
+    P = g["k_planes"]
+    assert bits_equal(orc.cost(P, bwL, bwR, gL, gR, r, 1e10), g["k_cost_inf"]).all()
+    assert bits_equal(orc.cost(P, bwL, bwR, gL, gR, r, 0.2), g["k_cost_02"]).all()
+    assert bits_equal(orc.klt(P, bwL, bwR, gL, gR, r), g["k_klt"]).all()
+    out, vn, vv, vs = orc.propagate(P, bwL, bwR, gL, gR, g["k_smooth"], 0.37, r, dmax, 1, 1)
+    assert bits_equal(out, g["k_prop"]).all()
+    assert (vn == g["k_prop_vn"]).all()
+    keep = np.minimum(vn, 2)
+    for k in range(2):
+        m = keep > k
+        assert bits_equal(vv[..., 4 * k:4 * k + 4][m], g["k_prop_vv"][..., 4 * k:4 * k + 4][m]).all()
+    nd = orc.normal_depth(P, 1.0 / dmax, 1)
+    assert bits_equal(nd, g["k_nd"]).all()
+    assert bits_equal(orc.rof(nd, dtL, [1.3, 1.3, 1.3, 1.0], 40), g["k_rof"]).all()
+
+
+def test_restatement_matches_reference_live(orc, ref):
+    """A fresh seed through both CPU builds (needs the reference tree or a prebuilt oracle/_ref)."""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(11, 37, 23, 5, 1.0, 9.0)
+    a = orc.disparity_map(L, R, 2, 11.0, 2, pp=1, dump=True)
+    b = ref.disparity_map(L, R, 2, 11.0, 2, pp=1, dump=True)
+    for k in a["stages"]:
+        assert bits_equal(a["stages"][k], b["stages"][k]).all(), k
+    assert bits_equal(a["dmap"], b["dmap"]).all()
+
+
+@pytest.mark.parametrize("W,H,r", [(1, 1, 2), (3, 2, 1), (5, 7, 4), (17, 3, 3)])
+def test_tiny_images_match_reference(orc, ref, W, H, r):
+    """Images smaller than the window and than a 16x16 work-group."""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(W * 100 + H, W, H, 2, 1.0, 3.0)
+    a = orc.disparity_map(L, R, r, 4.0, 1, pp=2, dump=True)
+    b = ref.disparity_map(L, R, r, 4.0, 1, pp=2, dump=True)
+    for k in a["stages"]:
+        assert bits_equal(a["stages"][k], b["stages"][k]).all(), k
+    assert bits_equal(a["dmap"], b["dmap"]).all()
+    assert bits_equal(a["normal"], b["normal"]).all()
+
+
+def _mwc_step(x, c):
+    A = 4294883355
+    xn = (A * x + c) & 0xffffffff
+    carry = 1 if xn < c else 0
+    cn = ((A * x) >> 32) + carry
+    return xn, cn & 0xffffffff
+
+
+def test_mwc64x_skip_equals_stepping(orc):
+    """MWC64X skip-ahead (MWC64X.cl:104-141) against plain stepping from the common seed."""
+    A, BASE = 4294883355, 4077358422479273989
+    x, c = BASE // A, BASE % A
+    states = []
+    for _ in range(64):
+        states.append((x, c))
+        x, c = _mwc_step(x, c)
+    for d in (0, 1, 2, 3, 17, 63):
+        sx, sc = states[d]
+        expect = np.float32(np.float32(sx ^ sc) * np.float32(2.3283064365386962890625e-10))
+        got = orc.rng_floats(d, 1, 1)[0]
+        assert got == expect, d
+
+
+def test_libm_within_opencl_bounds(orc):
+    """exp <= 3 ulp, sin/cos <= 4 ulp, acospi <= 5 ulp (OpenCL 1.2 s7.4), in fact ~1-2.5."""
+    L = orc.L
+    xs = np.linspace(-40, 0, 20001, dtype=np.float32)
+    got = np.array([L.orc_exp(float(x)) for x in xs], np.float32)
+    want = np.exp(xs.astype(np.float64))
+    ulp = np.spacing(want.astype(np.float32)).astype(np.float64)
+    assert (np.abs(got - want) / ulp).max() <= 1.0
+    assert L.orc_exp(0.0) == 1.0
+    xs = np.linspace(0, 6.3, 20001, dtype=np.float32)
+    for fn, ref_fn in ((L.orc_sin, np.sin), (L.orc_cos, np.cos)):
+        got = np.array([fn(float(x)) for x in xs], np.float32)
+        want = ref_fn(xs.astype(np.float64))
+        ulp = np.spacing(np.abs(want).astype(np.float32)).astype(np.float64)
+        m = np.abs(want) > 1e-6
+        assert (np.abs(got - want)[m] / ulp[m]).max() <= 2.0
+    xs = np.linspace(-1, 1, 20001, dtype=np.float32)
+    got = np.array([L.orc_acospi(float(x)) for x in xs], np.float32)
+    want = np.arccos(xs.astype(np.float64)) / np.pi
+    ulp = np.spacing(want.astype(np.float32)).astype(np.float64)
+    m = want > 1e-6
+    assert (np.abs(got - want)[m] / ulp[m]).max() <= 3.0
+
+
+def test_fused_mode_differs_only_by_rounding(orc):
+    """Fused arithmetic changes last bits, not the method: final disparities stay close."""
+    from cvt_b200 import scene
+
+    L, R, gt, _ = scene.generate(2, 48, 32, 4, 2.0, 10.0, with_gt=True)
+    a = orc.disparity_map(L, R, 3, 12.0, 3, pp=0, fused=0)
+    b = orc.disparity_map(L, R, 3, 12.0, 3, pp=0, fused=1)
+    assert np.mean(np.abs(a["dmap"] - b["dmap"]) < 1.0) > 0.9
