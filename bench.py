@@ -173,6 +173,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="hd", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="only run warmup + steps of the device pipeline (for ncu captures) and print the step times")
     args = ap.parse_args()
     wl = WORKLOADS[args.config]
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
@@ -195,6 +197,14 @@ def main():
     dL, dR = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
     pm = PMHuberStereo(views=views, fused=True, device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    if args.profile_run:
+        for _ in range(args.warmup):
+            pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+        pm.set_profiling(True)
+        for k in range(args.steps):
+            pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+            print(json.dumps({"step": k, "phase_ms": pm.phase_times()}))
+        return
 
     # counting pass (untimed): window samples of the propagate launches
     pm.set_counting(True)

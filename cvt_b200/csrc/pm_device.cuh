@@ -1,5 +1,5 @@
-// Device functions of the PatchMatch-Huber path: plane-state algebra and the
-// per-pixel window work.  Each function names the reference lines it computes
+// Device functions of the PatchMatch-Huber path: plane-state algebra, support
+// weights and the bilinear row read.  Each function names the reference lines it computes
 // (cvt/cl/kernel/pmhstereo.cl, Matrix3.cl).  Arithmetic is FP32 with the
 // reference's operation order; the file must be compiled with -fmad=false so
 // that only the explicit fmaf() calls (the "hot" sites, enabled by the template
@@ -201,170 +201,5 @@ __device__ __forceinline__ float4 lerp_row(const float4* __restrict__ row, int W
     return f4(b * T0.x + a * T1.x, b * T0.y + a * T1.y, b * T0.z + a * T1.z, b * T0.w + a * T1.w);
 }
 
-// per-sample cost of patch_eval_census (:707-716)
-__device__ __forceinline__ float census_cost(float3 valin, uint32_t sg1, float4 v2, float4 gv2)
-{
-    const float cx = div005(fminf(fabsf(v2.x - valin.x), 0.05f));
-    const float cy = div005(fminf(fabsf(v2.y - valin.y), 0.05f));
-    const float cz = div005(fminf(fabsf(v2.z - valin.z), 0.05f));
-    const float cad = 0.33f * (cx + cy + cz);
-    float cost = 0.125f * cad;
-    const float cc = 0.25f * (float)__popc(sg1 ^ signbits4(gv2));
-    cost = cost + 0.875f * cc;
-    return cost;
-}
-
-struct ViewData {
-    const float4* __restrict__ bw1;   // first view: rgb + support-weight sum
-    const float4* __restrict__ bw2;   // second view
-    const float4* __restrict__ g1;
-    const float4* __restrict__ g2;
-    int W, H, r;
-};
-
-struct Counters {
-    unsigned long long eval, klt, calls, exits;
-};
-
-// patch_eval_census (:661-736).  The early exit `census / bilw >= mincost` is tested as
-// census >= exit_threshold(mincost, bilw), which is the same predicate.
-template <bool F, bool COUNT>
-__device__ float patch_eval(const ViewData& V, int px, int py, float4 s, float mincost, Counters& cnt)
-{
-    const float cx = (float)px, cy = (float)py;
-    const float c2x = transform_x(s, cx, cy);
-    if (!(fin(s.x) && fin(s.y) && fin(s.z)) || to_normal(s).z < 1e-4f || c2x < 0 || c2x >= (float)V.W) return 1e5f;
-    const float4 in = __ldg(V.bw1 + (size_t)py * V.W + px);
-    const float thr = exit_threshold(mincost, in.w);
-    float wsum = 0.0f, census = 0.0f;
-    if (COUNT) cnt.calls++;
-    const int r = V.r;
-    const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
-    const int dx0 = max(-r, -px), dx1 = min(r, V.W - 1 - px);
-    // rows and columns outside the image are skipped by the source's own test
-    for (int dy = -r; dy <= r; dy++) {
-        if (dy < dy0 || dy > dy1) continue;
-        const int iy = py + dy;
-        const float qy = cy + (float)dy;
-        const float byq = s.y * qy;
-        const float4* __restrict__ row1 = V.bw1 + (size_t)iy * V.W;
-        const float4* __restrict__ rowg1 = V.g1 + (size_t)iy * V.W;
-        const float4* __restrict__ row2 = V.bw2 + (size_t)iy * V.W;
-        const float4* __restrict__ rowg2 = V.g2 + (size_t)iy * V.W;
-        for (int dx = dx0; dx <= dx1; dx++) {
-            const float qx = cx + (float)dx;
-            const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
-            if (p2x < 0 || p2x >= (float)V.W) continue;
-            const int ix = px + dx;
-            const float4 vin = __ldg(row1 + ix);
-            const float w = support_weight<F>(vin.x - in.x, vin.y - in.y, vin.z - in.z);
-            const float4 gv1 = __ldg(rowg1 + ix);
-            const float4 gv2 = lerp_row<F>(rowg2, V.W, p2x + 0.5f);
-            const float4 v2 = lerp_row<F>(row2, V.W, p2x + 0.5f);
-            const float cost = census_cost(make_float3(vin.x, vin.y, vin.z), signbits4(gv1), v2, gv2);
-            census = F ? fmaf(w, cost, census) : census + w * cost;
-            wsum += w;
-            if (COUNT) cnt.eval++;
-            if (census >= thr) { if (COUNT) cnt.exits++; return 1.0f; }
-        }
-    }
-    if (wsum <= 1.0f) return 1.1f;
-    return census / wsum;
-}
-
-// one tap of patch_census_klt2 (:361-370); the colour term compares against the
-// colour difference val1, as in the source.  The double literal in
-// `w1 * (1.0f - alpha) * 0.25 * (float)cnt` makes the sum a double-precision one,
-// rounded once: formed exactly in double (strict) or with one fma (fused).
-template <bool F>
-__device__ __forceinline__ float klt_tap(float w1, float3 val1, uint32_t sg1, float4 v2, float4 gv2)
-{
-    const float cx = div005(fminf(fabsf(v2.x - val1.x), 0.05f));
-    const float cy = div005(fminf(fabsf(v2.y - val1.y), 0.05f));
-    const float cz = div005(fminf(fabsf(v2.z - val1.z), 0.05f));
-    float C = w1 * 0.125f * 0.33f * (cx + cy + cz);
-    const int n = __popc(sg1 ^ signbits4(gv2));
-    if (F) C = fmaf(w1 * 0.875f * 0.25f, (float)n, C);
-    else C = (float)((double)C + (double)(w1 * 0.875f) * 0.25 * (double)(float)n);
-    return C;
-}
-
-// mat3f_lusolve (Matrix3.cl:286-311) on the symmetric 3x3 H = [h00 h01 h02; h01 h11 h12; h02 h12 h22]
-__device__ __forceinline__ float3 lusolve(float h00, float h01, float h02, float h11, float h12, float h22, float3 b)
-{
-    float m10 = h01, m20 = h02, m11 = h11, m12 = h12, m21 = h12, m22 = h22;
-    const float m00 = h00, m01 = h01, m02 = h02;
-    m10 /= m00;
-    m20 /= m00;
-    m11 -= m10 * m01;
-    m12 -= m10 * m02;
-    m21 -= m20 * m01;
-    m22 -= m20 * m02;
-    m21 /= m11;
-    m22 -= m21 * m12;
-    b.y -= m10 * b.x;
-    b.z -= m20 * b.x + m21 * b.y;
-    float3 ret;
-    ret.z = b.z / m22;
-    ret.y = (b.y - m12 * ret.z) / m11;
-    ret.x = (b.x - (m01 * ret.y + m02 * ret.z)) / m00;
-    return ret;
-}
-
-// patch_census_klt2 (:326-410), with the in-bounds test on the window position rather
-// than the matched one (:358)
-template <bool F, bool COUNT>
-__device__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cnt)
-{
-    const float cxf = (float)px, cyf = (float)py;
-    float J0 = 0.0f, J1 = 0.0f, J2 = 0.0f;
-    float h00 = 0.0f, h01 = 0.0f, h02 = 0.0f, h11 = 0.0f, h12 = 0.0f, h22 = 0.0f;
-    const float4 c1 = __ldg(V.bw1 + (size_t)py * V.W + px);
-    const int r = V.r;
-    const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
-    // the 3-point cost needs 1 <= qx < W - 1
-    const int dx0 = max(-r, 1 - px), dx1 = min(r, V.W - 2 - px);
-    for (int dy = dy0; dy <= dy1; dy++) {
-        const int iy = py + dy;
-        const float qy = cyf + (float)dy;
-        const float byq = s.y * qy;
-        const float4* __restrict__ row1 = V.bw1 + (size_t)iy * V.W;
-        const float4* __restrict__ rowg1 = V.g1 + (size_t)iy * V.W;
-        const float4* __restrict__ row2 = V.bw2 + (size_t)iy * V.W;
-        const float4* __restrict__ rowg2 = V.g2 + (size_t)iy * V.W;
-        for (int dx = dx0; dx <= dx1; dx++) {
-            const float qx = cxf + (float)dx;
-            const int ix = px + dx;
-            const float4 vin = __ldg(row1 + ix);
-            const float3 val1 = make_float3(vin.x - c1.x, vin.y - c1.y, vin.z - c1.z);
-            const float w1 = support_weight<F>(val1.x, val1.y, val1.z);
-            const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
-            const uint32_t sg1 = signbits4(__ldg(rowg1 + ix));
-            const float u0 = p2x + 0.5f;
-            const float up = (p2x + 1.0f) + 0.5f;
-            const float um = (p2x + -1.0f) + 0.5f;
-            const float C = klt_tap<F>(w1, val1, sg1, lerp_row<F>(row2, V.W, u0), lerp_row<F>(rowg2, V.W, u0));
-            const float Cxp = klt_tap<F>(w1, val1, sg1, lerp_row<F>(row2, V.W, up), lerp_row<F>(rowg2, V.W, up));
-            const float Cxm = klt_tap<F>(w1, val1, sg1, lerp_row<F>(row2, V.W, um), lerp_row<F>(rowg2, V.W, um));
-            if (COUNT) cnt.klt++;
-            if ((Cxp + Cxm - 2.0f * C) > 0.0f) {
-                const float t = w1 * (Cxm - Cxp) * 0.5f;
-                const float sc = w1 * (Cxp + Cxm - 2.0f * C);
-                const float xx = qx * qx, xy = qx * qy, yy = qy * qy;
-                if (F) {
-                    J0 = fmaf(t, qx, J0); J1 = fmaf(t, qy, J1); J2 = fmaf(t, 1.0f, J2);
-                    h00 = fmaf(sc, xx, h00); h01 = fmaf(sc, xy, h01); h02 = fmaf(sc, qx, h02);
-                    h11 = fmaf(sc, yy, h11); h12 = fmaf(sc, qy, h12); h22 = fmaf(sc, 1.0f, h22);
-                } else {
-                    J0 = J0 + t * qx; J1 = J1 + t * qy; J2 = J2 + t * 1.0f;
-                    h00 = h00 + sc * xx; h01 = h01 + sc * xy; h02 = h02 + sc * qx;
-                    h11 = h11 + sc * yy; h12 = h12 + sc * qy; h22 = h22 + sc * 1.0f;
-                }
-            }
-        }
-    }
-    const float3 d = lusolve(h00, h01, h02, h11, h12, h22, make_float3(J0, J1, J2));
-    return f4(s.x - d.x, s.y - d.y, s.z - d.z, s.w - 1e5f);
-}
-
 }  // namespace pm
+

@@ -6,7 +6,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
-#include "pm_device.cuh"
+#include "pm_window.cuh"
 
 namespace pm {
 

@@ -1,0 +1,294 @@
+// Window loops of the PatchMatch-Huber path: the adaptive-support-weight cost
+// (patch_eval_census, pmhstereo.cl:661-736) and the Gauss-Newton plane step
+// (patch_census_klt2, :326-410), one thread per pixel, samples in the
+// reference's order.
+//
+// Blackwell specifics: the 7-channel bilinear reads of the second view and the
+// truncated absolute differences run as packed FP32 pairs (FFMA2 / FMUL2 /
+// FADD2, sm_100), the sign census packs the four gradient sign bits with byte
+// permutes, and the three Gauss-Newton taps at x'-1, x', x'+1 share four texels
+// when their fractional parts agree (checked exactly; otherwise each tap is
+// read on its own).  Every packed operation rounds per element exactly like its
+// scalar form, so results equal the scalar restatement bit for bit.
+#pragma once
+
+#include "pm_device.cuh"
+
+namespace pm {
+
+struct ViewData {
+    const float4* __restrict__ bw1;   // first view: rgb + support-weight sum
+    const float4* __restrict__ bw2;   // second view
+    const float4* __restrict__ g1;    // gradients (pmhstereo_gradxy)
+    const float4* __restrict__ g2;
+    int W, H, r;
+};
+
+struct Counters {
+    unsigned long long eval, klt, calls, exits;
+};
+
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+
+// bilinear pair: (1-a)*T0 + a*T1 per element; fused contracts a*T1
+template <bool F>
+__device__ __forceinline__ float2 lerp2(float2 a2, float2 b2, float2 t0, float2 t1)
+{
+    if (F) return __ffma2_rn(a2, t1, __fmul2_rn(b2, t0));
+    return __fadd2_rn(__fmul2_rn(b2, t0), __fmul2_rn(a2, t1));
+}
+
+// one texel of the second view: colour (r, g, b, w) and gradient (4 components)
+struct Texel {
+    float4 c, g;
+};
+
+__device__ __forceinline__ Texel fetch(const float4* __restrict__ row2, const float4* __restrict__ rowg2, int j)
+{
+    Texel t;
+    t.c = __ldg(row2 + j);
+    t.g = __ldg(rowg2 + j);
+    return t;
+}
+
+template <bool F>
+__device__ __forceinline__ Texel lerp_texel(float a, float b, const Texel& t0, const Texel& t1)
+{
+    const float2 a2 = f2(a, a), b2 = f2(b, b);
+    const float2 c01 = lerp2<F>(a2, b2, f2(t0.c.x, t0.c.y), f2(t1.c.x, t1.c.y));
+    const float2 c23 = lerp2<F>(a2, b2, f2(t0.c.z, t0.c.w), f2(t1.c.z, t1.c.w));
+    const float2 g01 = lerp2<F>(a2, b2, f2(t0.g.x, t0.g.y), f2(t1.g.x, t1.g.y));
+    const float2 g23 = lerp2<F>(a2, b2, f2(t0.g.z, t0.g.w), f2(t1.g.z, t1.g.w));
+    Texel r;
+    r.c = make_float4(c01.x, c01.y, c23.x, c23.y);
+    r.g = make_float4(g01.x, g01.y, g23.x, g23.y);
+    return r;
+}
+
+// byte k holds the top byte of component k, so bit 7 of byte k is its sign bit
+__device__ __forceinline__ uint32_t sign_bytes(float4 g)
+{
+    const uint32_t lo = __byte_perm(__float_as_uint(g.x), __float_as_uint(g.y), 0x0073);
+    const uint32_t hi = __byte_perm(__float_as_uint(g.z), __float_as_uint(g.w), 0x0073);
+    return __byte_perm(lo, hi, 0x5410);
+}
+
+// number of gradient components whose signs differ (the census term, :712-715, :367-370)
+__device__ __forceinline__ int sign_mismatch(uint32_t a, uint32_t b) { return __popc((a ^ b) & 0x80808080u); }
+
+// sum over r, g, b of fmin(|v2 - ref|, 0.05) / 0.05 (:707-709, :364-365), divisions exact
+__device__ __forceinline__ float ad_sum(float4 v2, float4 ref)
+{
+    const float2 d01 = __ffma2_rn(f2(ref.x, ref.y), f2(-1.0f, -1.0f), f2(v2.x, v2.y));   // v2 - ref, exact
+    const float d2 = v2.z - ref.z;
+    const float m0 = fminf(fabsf(d01.x), 0.05f), m1 = fminf(fabsf(d01.y), 0.05f), m2 = fminf(fabsf(d2), 0.05f);
+    const float2 m01 = f2(m0, m1);
+    const float2 q01 = __fmul2_rn(m01, f2(20.0f, 20.0f));
+    const float2 r01 = __ffma2_rn(q01, f2(-0.05f, -0.05f), m01);
+    float2 c01 = __ffma2_rn(r01, f2(20.0f, 20.0f), q01);
+    const float q2 = m2 * 20.0f;
+    const float r2 = fmaf(q2, -0.05f, m2);
+    float c2 = fmaf(r2, 20.0f, q2);
+    if (fminf(fminf(m0, m1), m2) < 7.88860905e-31f) {   // below 2^-100 the fma correction is not exact
+        c01 = f2(m0 / 0.05f, m1 / 0.05f);
+        c2 = m2 / 0.05f;
+    }
+    return c01.x + c01.y + c2;
+}
+
+// ---- slow path: one bilinear tap at a time, exactly as the source reads it -------------
+
+// one tap of patch_census_klt2 (:361-370)
+template <bool F>
+__device__ __forceinline__ float klt_tap(float w1, float3 val1, uint32_t sg1, float4 v2, float4 gv2)
+{
+    const float cx = div005(fminf(fabsf(v2.x - val1.x), 0.05f));
+    const float cy = div005(fminf(fabsf(v2.y - val1.y), 0.05f));
+    const float cz = div005(fminf(fabsf(v2.z - val1.z), 0.05f));
+    float C = w1 * 0.125f * 0.33f * (cx + cy + cz);
+    const int n = sign_mismatch(sg1, sign_bytes(gv2));
+    if (F) C = fmaf(w1 * 0.875f * 0.25f, (float)n, C);
+    else C = (float)((double)C + (double)(w1 * 0.875f) * 0.25 * (double)(float)n);
+    return C;
+}
+
+// the cost of one Gauss-Newton tap from its interpolated texel (same arithmetic as klt_tap).
+// `w1 * (1.0f - alpha) * 0.25 * (float)cnt` (:370) carries a double literal, so the sum is a
+// double-precision one rounded once: formed exactly in double (strict) or with one fma (fused).
+template <bool F>
+__device__ __forceinline__ float klt_cost(float k1, float w1, float4 val1, uint32_t sb1, const Texel& t)
+{
+    float C = k1 * ad_sum(t.c, val1);
+    const int n = sign_mismatch(sb1, sign_bytes(t.g));
+    if (F) C = fmaf(w1 * 0.875f * 0.25f, (float)n, C);
+    else C = (float)((double)C + (double)(w1 * 0.875f) * 0.25 * (double)(float)n);
+    return C;
+}
+
+// mat3f_lusolve (Matrix3.cl:286-311) on the symmetric 3x3 H = [h00 h01 h02; h01 h11 h12; h02 h12 h22]
+__device__ __forceinline__ float3 lusolve(float h00, float h01, float h02, float h11, float h12, float h22, float3 b)
+{
+    float m10 = h01, m20 = h02, m11 = h11, m12 = h12, m21 = h12, m22 = h22;
+    const float m00 = h00, m01 = h01, m02 = h02;
+    m10 /= m00;
+    m20 /= m00;
+    m11 -= m10 * m01;
+    m12 -= m10 * m02;
+    m21 -= m20 * m01;
+    m22 -= m20 * m02;
+    m21 /= m11;
+    m22 -= m21 * m12;
+    b.y -= m10 * b.x;
+    b.z -= m20 * b.x + m21 * b.y;
+    float3 ret;
+    ret.z = b.z / m22;
+    ret.y = (b.y - m12 * ret.z) / m11;
+    ret.x = (b.x - (m01 * ret.y + m02 * ret.z)) / m00;
+    return ret;
+}
+
+// patch_eval_census (:661-736).  The early exit `census / bilw >= mincost` (:724) is tested
+// as census >= exit_threshold(mincost, bilw), the same predicate without a division.
+template <bool F, bool COUNT>
+__device__ float patch_eval(const ViewData& V, int px, int py, float4 s, float mincost, Counters& cnt)
+{
+    const float cx = (float)px, cy = (float)py;
+    const float c2x = transform_x(s, cx, cy);
+    if (!(fin(s.x) && fin(s.y) && fin(s.z)) || to_normal(s).z < 1e-4f || c2x < 0 || c2x >= (float)V.W) return 1e5f;
+    const int W = V.W;
+    const float4 in = __ldg(V.bw1 + (size_t)py * W + px);
+    const float thr = exit_threshold(mincost, in.w);
+    float wsum = 0.0f, census = 0.0f;
+    if (COUNT) cnt.calls++;
+    const int r = V.r;
+    const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
+    const int dx0 = max(-r, -px), dx1 = min(r, W - 1 - px);
+    const float fW = (float)W;
+    for (int dy = dy0; dy <= dy1; dy++) {
+        const int iy = py + dy;
+        const float qy = cy + (float)dy;
+        const float byq = s.y * qy;
+        const float4* __restrict__ row1 = V.bw1 + (size_t)iy * W;
+        const float4* __restrict__ rowg1 = V.g1 + (size_t)iy * W;
+        const float4* __restrict__ row2 = V.bw2 + (size_t)iy * W;
+        const float4* __restrict__ rowg2 = V.g2 + (size_t)iy * W;
+        for (int dx = dx0; dx <= dx1; dx++) {
+            const float qx = cx + (float)dx;
+            const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
+            if (p2x < 0 || p2x >= fW) continue;
+            const int ix = px + dx;
+            const float4 vin = __ldg(row1 + ix);
+            const float4 gin = __ldg(rowg1 + ix);
+            const float w = support_weight<F>(vin.x - in.x, vin.y - in.y, vin.z - in.z);
+            const float t = (p2x + 0.5f) - 0.5f;
+            Texel tx;
+            if (fin(t)) {
+                const float fl = floorf(t);
+                const float a = t - fl;
+                const int i0 = (int)fl;   // p2x in [0, W) gives t in [0, W]: i0 in [0, W]
+                tx = lerp_texel<F>(a, 1.0f - a, fetch(row2, rowg2, min(i0, W - 1)), fetch(row2, rowg2, min(i0 + 1, W - 1)));
+            } else {
+                tx.c = lerp_row<F>(row2, W, p2x + 0.5f);
+                tx.g = lerp_row<F>(rowg2, W, p2x + 0.5f);
+            }
+            const float cad = 0.33f * ad_sum(tx.c, vin);
+            float cost = 0.125f * cad;
+            // cost + 0.875f * (0.25f * n): the product 0.21875 n is exact, so one fma rounds the same
+            cost = fmaf(0.21875f, (float)sign_mismatch(sign_bytes(gin), sign_bytes(tx.g)), cost);
+            census = F ? fmaf(w, cost, census) : census + w * cost;
+            wsum += w;
+            if (COUNT) cnt.eval++;
+            if (census >= thr) {
+                if (COUNT) cnt.exits++;
+                return 1.0f;
+            }
+        }
+    }
+    if (wsum <= 1.0f) return 1.1f;
+    return census / wsum;
+}
+
+// patch_census_klt2 (:326-410), with the in-bounds test on the window position rather than
+// the matched one (:358) and the colour term against the colour difference (:352, :364)
+template <bool F, bool COUNT>
+__device__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cnt)
+{
+    const float cxf = (float)px, cyf = (float)py;
+    const int W = V.W;
+    float2 J01 = f2(0.0f, 0.0f);
+    float J2 = 0.0f;
+    float2 h00_01 = f2(0.0f, 0.0f), h02_11 = f2(0.0f, 0.0f), h12_22 = f2(0.0f, 0.0f);
+    const float4 c1 = __ldg(V.bw1 + (size_t)py * W + px);
+    const int r = V.r;
+    const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
+    const int dx0 = max(-r, 1 - px), dx1 = min(r, W - 2 - px);   // the 3-point cost needs 1 <= qx < W - 1
+    for (int dy = dy0; dy <= dy1; dy++) {
+        const int iy = py + dy;
+        const float qy = cyf + (float)dy;
+        const float byq = s.y * qy;
+        const float yy = qy * qy;
+        const float4* __restrict__ row1 = V.bw1 + (size_t)iy * W;
+        const float4* __restrict__ rowg1 = V.g1 + (size_t)iy * W;
+        const float4* __restrict__ row2 = V.bw2 + (size_t)iy * W;
+        const float4* __restrict__ rowg2 = V.g2 + (size_t)iy * W;
+        for (int dx = dx0; dx <= dx1; dx++) {
+            const float qx = cxf + (float)dx;
+            const int ix = px + dx;
+            const float4 vin = __ldg(row1 + ix);
+            const float4 val1 = make_float4(vin.x - c1.x, vin.y - c1.y, vin.z - c1.z, 0.0f);
+            const float w1 = support_weight<F>(val1.x, val1.y, val1.z);
+            const uint32_t sb1 = sign_bytes(__ldg(rowg1 + ix));
+            const float k1 = w1 * 0.125f * 0.33f;
+            const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
+            const float t0 = (p2x + 0.5f) - 0.5f;
+            const float tp = ((p2x + 1.0f) + 0.5f) - 0.5f;
+            const float tm = ((p2x + -1.0f) + 0.5f) - 0.5f;
+            const float f0 = floorf(t0), fp = floorf(tp), fm = floorf(tm);
+            const float a0 = t0 - f0;
+            float C, Cxp, Cxm;
+            if (fp == f0 + 1.0f && fm == f0 - 1.0f && tp - fp == a0 && tm - fm == a0) {
+                // the three taps read texels f0-1 .. f0+2 with one weight
+                const int i0 = (int)fminf(fmaxf(f0, -2.0f), (float)W + 1.0f);
+                const Texel tA = fetch(row2, rowg2, min(max(i0 - 1, 0), W - 1));
+                const Texel tB = fetch(row2, rowg2, min(max(i0, 0), W - 1));
+                const Texel tC = fetch(row2, rowg2, min(max(i0 + 1, 0), W - 1));
+                const Texel tD = fetch(row2, rowg2, min(max(i0 + 2, 0), W - 1));
+                const float b0 = 1.0f - a0;
+                Cxm = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tA, tB));
+                C = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tB, tC));
+                Cxp = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tC, tD));
+            } else {
+                const float3 v1 = make_float3(val1.x, val1.y, val1.z);
+                const uint32_t sg1 = sb1;
+                const float u0 = p2x + 0.5f, up = (p2x + 1.0f) + 0.5f, um = (p2x + -1.0f) + 0.5f;
+                C = klt_tap<F>(w1, v1, sg1, lerp_row<F>(row2, W, u0), lerp_row<F>(rowg2, W, u0));
+                Cxp = klt_tap<F>(w1, v1, sg1, lerp_row<F>(row2, W, up), lerp_row<F>(rowg2, W, up));
+                Cxm = klt_tap<F>(w1, v1, sg1, lerp_row<F>(row2, W, um), lerp_row<F>(rowg2, W, um));
+            }
+            if (COUNT) cnt.klt++;
+            const float curv = Cxp + Cxm - 2.0f * C;
+            if (curv > 0.0f) {
+                const float t = w1 * (Cxm - Cxp) * 0.5f;
+                const float sc = w1 * curv;
+                const float2 t2 = f2(t, t), s2 = f2(sc, sc);
+                if (F) {
+                    J01 = __ffma2_rn(t2, f2(qx, qy), J01);
+                    J2 = fmaf(t, 1.0f, J2);
+                    h00_01 = __ffma2_rn(s2, f2(qx * qx, qx * qy), h00_01);
+                    h02_11 = __ffma2_rn(s2, f2(qx, yy), h02_11);
+                    h12_22 = __ffma2_rn(s2, f2(qy, 1.0f), h12_22);
+                } else {
+                    J01 = __fadd2_rn(J01, __fmul2_rn(t2, f2(qx, qy)));
+                    J2 = J2 + t * 1.0f;
+                    h00_01 = __fadd2_rn(h00_01, __fmul2_rn(s2, f2(qx * qx, qx * qy)));
+                    h02_11 = __fadd2_rn(h02_11, __fmul2_rn(s2, f2(qx, yy)));
+                    h12_22 = __fadd2_rn(h12_22, __fmul2_rn(s2, f2(qy, 1.0f)));
+                }
+            }
+        }
+    }
+    const float3 d = lusolve(h00_01.x, h00_01.y, h02_11.x, h02_11.y, h12_22.x, h12_22.y, make_float3(J01.x, J01.y, J2));
+    return f4(s.x - d.x, s.y - d.y, s.z - d.z, s.w - 1e5f);
+}
+
+}  // namespace pm
