@@ -30,12 +30,15 @@ struct Counters {
 
 __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
 
-// bilinear pair: (1-a)*T0 + a*T1 per element; fused contracts a*T1
+// bilinear pair: (1-a)*T0 + a*T1 per element; fused contracts a*T1.  The strict form
+// stays scalar: nvcc contracts a packed multiply feeding a packed add into FFMA2 even
+// under -fmad=false, which would change the rounding.
 template <bool F>
 __device__ __forceinline__ float2 lerp2(float2 a2, float2 b2, float2 t0, float2 t1)
 {
     if (F) return __ffma2_rn(a2, t1, __fmul2_rn(b2, t0));
-    return __fadd2_rn(__fmul2_rn(b2, t0), __fmul2_rn(a2, t1));
+    return make_float2(__fadd_rn(__fmul_rn(b2.x, t0.x), __fmul_rn(a2.x, t1.x)),
+                       __fadd_rn(__fmul_rn(b2.y, t0.y), __fmul_rn(a2.y, t1.y)));
 }
 
 // one texel of the second view: colour (r, g, b, w) and gradient (4 components)
@@ -277,12 +280,12 @@ __device__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cn
                     h00_01 = __ffma2_rn(s2, f2(qx * qx, qx * qy), h00_01);
                     h02_11 = __ffma2_rn(s2, f2(qx, yy), h02_11);
                     h12_22 = __ffma2_rn(s2, f2(qy, 1.0f), h12_22);
-                } else {
-                    J01 = __fadd2_rn(J01, __fmul2_rn(t2, f2(qx, qy)));
+                } else {   // scalar: see lerp2
+                    J01 = f2(__fadd_rn(J01.x, __fmul_rn(t, qx)), __fadd_rn(J01.y, __fmul_rn(t, qy)));
                     J2 = J2 + t * 1.0f;
-                    h00_01 = __fadd2_rn(h00_01, __fmul2_rn(s2, f2(qx * qx, qx * qy)));
-                    h02_11 = __fadd2_rn(h02_11, __fmul2_rn(s2, f2(qx, yy)));
-                    h12_22 = __fadd2_rn(h12_22, __fmul2_rn(s2, f2(qy, 1.0f)));
+                    h00_01 = f2(__fadd_rn(h00_01.x, __fmul_rn(sc, qx * qx)), __fadd_rn(h00_01.y, __fmul_rn(sc, qx * qy)));
+                    h02_11 = f2(__fadd_rn(h02_11.x, __fmul_rn(sc, qx)), __fadd_rn(h02_11.y, __fmul_rn(sc, yy)));
+                    h12_22 = f2(__fadd_rn(h12_22.x, __fmul_rn(sc, qy)), __fadd_rn(h12_22.y, __fmul_rn(sc, 1.0f)));
                 }
             }
         }

@@ -1,0 +1,38 @@
+// A user of cvt::PMHuberStereo switching to this library: the reference's call,
+// unchanged, on a procedural pair.  Writes the disparity map (float32, W*H) to argv[1].
+#include <cstdio>
+#include <cstring>
+
+#include "cvt/vision/PMHuberStereo.h"
+
+int main(int argc, char** argv)
+{
+    if (argc < 2) return 2;
+    const int W = 96, H = 64;
+    cvt::Image left(W, H, cvt::IFormat::RGBA_UINT8), right(W, H, cvt::IFormat::RGBA_UINT8);
+    size_t sl, sr;
+    uint8_t* pl = left.map(&sl);
+    uint8_t* pr = right.map(&sr);
+    if (pm_scene_generate(7, W, H, 6, 2.0f, 20.0f, 0.3f, 2.0f, pl, pr, (int)sl, NULL, NULL) != PM_OK) return 3;
+    try {
+        cvt::PMHuberStereo pmh;
+        cvt::Image dmap, normals;
+        pmh.disparityMap(dmap, left, right, 4, 24.0f, 3, cvt::DISPARITY_PP_LRCHECK, &normals);
+        size_t sd;
+        const uint8_t* pd = dmap.map(&sd);
+        FILE* f = fopen(argv[1], "wb");
+        for (int y = 0; y < H; y++) fwrite(pd + y * sd, 4, W, f);
+        fclose(f);
+        // inconsistent inputs throw, as in the reference (PMHuberStereo.cpp:412-414)
+        cvt::Image small(W / 2, H, cvt::IFormat::RGBA_UINT8);
+        try {
+            pmh.disparityMap(dmap, left, small, 4, 24.0f, 3);
+            return 4;
+        } catch (const cvt::Exception&) {
+        }
+    } catch (const cvt::Exception& e) {
+        fprintf(stderr, "%s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -108,3 +108,26 @@ def test_scene_generator_is_deterministic(native):
 
 
 SCENE_DIGEST = "54e0dc1c90811ccd82790abf7eceef416b3e1e22cc42747722fc6a5d7d1094ca"
+
+
+def build_drop_in(tmp_path):
+    import subprocess
+
+    exe = str(tmp_path / "drop_in")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "drop_in.cpp"), "-L", os.path.join(ROOT, "cvt_b200"), "-lcvtpm",
+                    "-Wl,-rpath," + os.path.join(ROOT, "cvt_b200"), "-o", exe], check=True)
+    return exe
+
+
+def test_cpp_drop_in_header_compiles_and_fails_loudly(native, tmp_path):
+    """The C++ class with the reference's signatures builds against the library; without a
+    device it throws (no CPU fallback)."""
+    import subprocess
+
+    import torch
+
+    exe = build_drop_in(tmp_path)
+    if not torch.cuda.is_available():
+        p = subprocess.run([exe, str(tmp_path / "d.raw")], capture_output=True, text=True)
+        assert p.returncode == 1 and "no CUDA device" in p.stderr

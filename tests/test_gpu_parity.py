@@ -325,3 +325,19 @@ def test_hd_config_is_deterministic_and_accurate(native, torch_cuda):
     assert valid.mean() > 0.5
     good = np.abs(d - gt)[valid] < 1.0
     assert good.mean() > 0.8, good.mean()
+
+
+def test_cpp_drop_in_matches_python(native, torch_cuda, tmp_path):
+    """The reference-shaped C++ call (tests/cpp/drop_in.cpp) gives the same disparity map."""
+    import subprocess
+
+    from cvt_b200 import PMHuberStereo, scene
+    from test_abi import build_drop_in
+
+    exe = build_drop_in(tmp_path)
+    out = tmp_path / "d.raw"
+    subprocess.run([exe, str(out)], check=True)
+    d = np.fromfile(str(out), np.float32).reshape(64, 96)
+    L, R = scene.generate(7, 96, 64, 6, 2.0, 20.0)
+    ref = PMHuberStereo().disparity_map(L, R, 4, 24.0, 3, pp=1)
+    assert bits_equal(d, ref).all()
