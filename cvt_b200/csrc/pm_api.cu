@@ -110,6 +110,7 @@ struct Layout {
         Lbw, Rbw, Lg, Rg, LDT, RDT, Ls, Rs, tmp, mL0, mL1, mR0, mR1, chk, nrm,   // float4 x N
         vb1c, vb2c,                                                             // int x N
         vb1s, vb2s,                                                             // u64 x N
+        texL, texR,                                                             // texel rows
         rof,                                                                    // rof scratch
         ctr, errf,                                                              // counters (4 u64), error int
         img0, img1, disp, dmap, nmap, initd, initn,                             // staging for host entry
@@ -128,6 +129,8 @@ Layout layout(int W, int H, size_t stride)
     put(Layout::vb2c, L.N * 4);
     put(Layout::vb1s, L.N * 8);
     put(Layout::vb2s, L.N * 8);
+    put(Layout::texL, tex_bytes(W, H));
+    put(Layout::texR, tex_bytes(W, H));
     put(Layout::rof, rof_scratch_bytes(W, H));
     put(Layout::ctr, 64);
     put(Layout::errf, 64);
@@ -194,7 +197,11 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
     PM_CUDA(h, cudaMemsetAsync(Rs, 0, N * 16, st));
     launch_view_clear(vb1c, vb1s, N, st);
     launch_view_clear(vb2c, vb2s, N, st);
-    prof_mark(h, st, PM_PHASE_PREP, 4);
+    float4* texL = at<float4>(ws, L, Layout::texL);
+    float4* texR = at<float4>(ws, L, Layout::texR);
+    launch_pack_tex(texL, Lbw, Lg, W, H, st);
+    launch_pack_tex(texR, Rbw, Rg, W, H, st);
+    prof_mark(h, st, PM_PHASE_PREP, 6);
     // init (:469-470); the given disparity and normals apply to the left view only (:92-93)
     int nl = 0;
     const float4* initn = initnormal;
@@ -204,8 +211,8 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
         initn = nrm;
         nl++;
     }
-    const ViewData VL = {Lbw, Rbw, Lg, Rg, W, H, r};
-    const ViewData VR = {Rbw, Lbw, Rg, Lg, W, H, r};
+    const ViewData VL = {texL, texR, W, H, r, tex_pitch(W)};
+    const ViewData VR = {texR, texL, W, H, r, tex_pitch(W)};
     launch_init(mL[0], VL, dmax, 1, initdisp, initn, F, st);
     nl++;
     if (views == 2) { launch_init(mR[0], VR, dmax, 0, nullptr, nullptr, F, st); nl++; }
@@ -286,6 +293,29 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
     PM_CUDA(h, cudaGetLastError());
     return prof_collect(h, st);
 }
+
+// texel rows (pm_window.cuh) of both views for the per-kernel entry points, in
+// stream-ordered scratch released once the stream has used it
+struct TexPair {
+    float4* t1 = nullptr;
+    float4* t2 = nullptr;
+    cudaStream_t st = nullptr;
+    int make(const float* bw1, const float* g1, const float* bw2, const float* g2, int W, int H, cudaStream_t s)
+    {
+        st = s;
+        PM_CUDA(nullptr, cudaMallocAsync((void**)&t1, tex_bytes(W, H), s));
+        PM_CUDA(nullptr, cudaMallocAsync((void**)&t2, tex_bytes(W, H), s));
+        launch_pack_tex(t1, (const float4*)bw1, (const float4*)g1, W, H, s);
+        launch_pack_tex(t2, (const float4*)bw2, (const float4*)g2, W, H, s);
+        return PM_OK;
+    }
+    ViewData view(int W, int H, int r) const { return ViewData{t1, t2, W, H, r, tex_pitch(W)}; }
+    ~TexPair()
+    {
+        if (t1) cudaFreeAsync(t1, st);
+        if (t2) cudaFreeAsync(t2, st);
+    }
+};
 
 int check_args(pm_handle* h, const void* left, const void* right, int W, int H, size_t stride, int r, float dmax,
                int iterations, int pp)
@@ -531,7 +561,9 @@ int pm_k_init(float* out, const float* bw1, const float* bw2, const float* g1, c
     int rc = check_shape(nullptr, W, H, r);
     if (rc) return rc;
     if (!out || !bw1 || !bw2 || !g1 || !g2 || (initdisp && !initnormal)) return fail(nullptr, PM_EINVAL_ARG, "null argument");
-    const ViewData V = {(const float4*)bw1, (const float4*)bw2, (const float4*)g1, (const float4*)g2, W, H, r};
+    TexPair tp;
+    if ((rc = tp.make(bw1, g1, bw2, g2, W, H, S(stream)))) return rc;
+    const ViewData V = tp.view(W, H, r);
     launch_init((float4*)out, V, dmax, lr, initdisp, (const float4*)initnormal, fused, S(stream));
     PM_CUDA(nullptr, cudaGetLastError());
     return PM_OK;
@@ -543,7 +575,9 @@ int pm_k_cost(float* cost, const float* planes, const float* bw1, const float* b
     int rc = check_shape(nullptr, W, H, r);
     if (rc) return rc;
     if (!cost || !planes || !bw1 || !bw2 || !g1 || !g2) return fail(nullptr, PM_EINVAL_ARG, "null argument");
-    const ViewData V = {(const float4*)bw1, (const float4*)bw2, (const float4*)g1, (const float4*)g2, W, H, r};
+    TexPair tp;
+    if ((rc = tp.make(bw1, g1, bw2, g2, W, H, S(stream)))) return rc;
+    const ViewData V = tp.view(W, H, r);
     launch_cost(cost, (const float4*)planes, V, mincost, fused, S(stream));
     PM_CUDA(nullptr, cudaGetLastError());
     return PM_OK;
@@ -555,7 +589,9 @@ int pm_k_klt(float* out, const float* planes, const float* bw1, const float* bw2
     int rc = check_shape(nullptr, W, H, r);
     if (rc) return rc;
     if (!out || !planes || !bw1 || !bw2 || !g1 || !g2) return fail(nullptr, PM_EINVAL_ARG, "null argument");
-    const ViewData V = {(const float4*)bw1, (const float4*)bw2, (const float4*)g1, (const float4*)g2, W, H, r};
+    TexPair tp;
+    if ((rc = tp.make(bw1, g1, bw2, g2, W, H, S(stream)))) return rc;
+    const ViewData V = tp.view(W, H, r);
     launch_klt((float4*)out, (const float4*)planes, V, fused, S(stream));
     PM_CUDA(nullptr, cudaGetLastError());
     return PM_OK;
@@ -574,7 +610,9 @@ int pm_k_propagate(float* out, const float* old, const float* bw1, const float* 
     static int* d_err = nullptr;
     if (!d_err) PM_CUDA(nullptr, cudaMalloc(&d_err, sizeof(int)));
     PropParams P;
-    P.V = {(const float4*)bw1, (const float4*)bw2, (const float4*)g1, (const float4*)g2, W, H, r};
+    TexPair tp;
+    if ((rc = tp.make(bw1, g1, bw2, g2, W, H, S(stream)))) return rc;
+    P.V = tp.view(W, H, r);
     P.out = (float4*)out;
     P.old = (const float4*)old;
     P.smooth = (const float4*)smooth;

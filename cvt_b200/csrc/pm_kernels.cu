@@ -438,6 +438,19 @@ __global__ void k_disparity_to_normal(float4* __restrict__ out, const float* __r
     out[(size_t)y * W + x] = f4(n.x, n.y, n.z, 0.0f);
 }
 
+// texel rows of one view (pm_window.cuh): column c in [-2, W+1] holds bw and grad of
+// column clamp(c, 0, W-1)
+__global__ void k_pack_tex(float4* __restrict__ tex, const float4* __restrict__ bw, const float4* __restrict__ grad,
+                           int W, int H, int P)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x - TEX_PAD, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c > W + TEX_PAD - 1 || y >= H) return;
+    const int s = min(max(c, 0), W - 1);
+    const size_t o = 2 * ((size_t)y * P + c + TEX_PAD);
+    tex[o] = bw[(size_t)y * W + s];
+    tex[o + 1] = grad[(size_t)y * W + s];
+}
+
 __global__ void k_view_clear(int* __restrict__ count, unsigned long long* __restrict__ src, size_t n)
 {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -582,6 +595,15 @@ void launch_disparity_to_normal(float4* out, const float* d, int W, int H, cudaS
 {
     const dim3 b(32, 8);
     k_disparity_to_normal<<<grid2d(W, H, b), b, 0, st>>>(out, d, W, H);
+}
+
+int tex_pitch(int W) { return W + 2 * TEX_PAD; }
+size_t tex_bytes(int W, int H) { return (size_t)tex_pitch(W) * H * 2 * sizeof(float4); }
+
+void launch_pack_tex(float4* tex, const float4* bw, const float4* grad, int W, int H, cudaStream_t st)
+{
+    const dim3 b(64, 4);
+    k_pack_tex<<<grid2d(tex_pitch(W), H, b), b, 0, st>>>(tex, bw, grad, W, H, tex_pitch(W));
 }
 
 void launch_view_clear(int* count, unsigned long long* src, size_t n, cudaStream_t st)

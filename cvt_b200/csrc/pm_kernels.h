@@ -54,6 +54,10 @@ void launch_fill_depthmap(float* out, const float4* planes, int W, int H, float 
 void launch_fill_normalmap(float4* out, const float4* planes, int W, int H, cudaStream_t st);
 void launch_disparity_to_normal(float4* out, const float* d, int W, int H, cudaStream_t st);
 void launch_view_clear(int* count, unsigned long long* src, size_t n, cudaStream_t st);
+// texel rows of a view (pm_window.cuh) from its bw and grad fields
+int tex_pitch(int W);
+size_t tex_bytes(int W, int H);
+void launch_pack_tex(float4* tex, const float4* bw, const float4* grad, int W, int H, cudaStream_t st);
 // FP32 peak probe: `iters` rounds of independent fma chains per thread
 void launch_fma_peak(float* out, int iters, int blocks, int threads, cudaStream_t st);
 double fma_peak_flops_per_iter();

@@ -3,9 +3,15 @@
 // (patch_census_klt2, :326-410), one thread per pixel, samples in the
 // reference's order.
 //
+// Texel layout.  Each view is stored as 32-byte texels {colour (r, g, b, Σw),
+// gradient (4 components)} in rows of W + 4 texels: columns -2 .. W+1, the four
+// outside ones replicating the edge texel (CLK_ADDRESS_CLAMP_TO_EDGE).  A
+// bilinear tap pair therefore needs no clamping inside that range and all
+// loads of a sample come from one base address.
+//
 // Blackwell specifics: the 7-channel bilinear reads of the second view and the
-// truncated absolute differences run as packed FP32 pairs (FFMA2 / FMUL2 /
-// FADD2, sm_100), the sign census packs the four gradient sign bits with byte
+// truncated absolute differences run as packed FP32 pairs (FFMA2 / FMUL2,
+// sm_100), the sign census packs the four gradient sign bits with byte
 // permutes, and the three Gauss-Newton taps at x'-1, x', x'+1 share four texels
 // when their fractional parts agree (checked exactly; otherwise each tap is
 // read on its own).  Every packed operation rounds per element exactly like its
@@ -16,12 +22,15 @@
 
 namespace pm {
 
+constexpr int TEX_PAD = 2;   // replicated columns on each side of a texel row
+
 struct ViewData {
-    const float4* __restrict__ bw1;   // first view: rgb + support-weight sum
-    const float4* __restrict__ bw2;   // second view
-    const float4* __restrict__ g1;    // gradients (pmhstereo_gradxy)
-    const float4* __restrict__ g2;
-    int W, H, r;
+    const float4* __restrict__ t1;   // first view texels (row pitch P texels)
+    const float4* __restrict__ t2;   // second view texels
+    int W, H, r, P;
+    // pointer to texel column 0 of row y
+    __device__ __forceinline__ const float4* row1(int y) const { return t1 + 2 * ((size_t)y * P + TEX_PAD); }
+    __device__ __forceinline__ const float4* row2(int y) const { return t2 + 2 * ((size_t)y * P + TEX_PAD); }
 };
 
 struct Counters {
@@ -41,16 +50,16 @@ __device__ __forceinline__ float2 lerp2(float2 a2, float2 b2, float2 t0, float2 
                        __fadd_rn(__fmul_rn(b2.y, t0.y), __fmul_rn(a2.y, t1.y)));
 }
 
-// one texel of the second view: colour (r, g, b, w) and gradient (4 components)
+// one texel: colour (r, g, b, w) and gradient (4 components)
 struct Texel {
     float4 c, g;
 };
 
-__device__ __forceinline__ Texel fetch(const float4* __restrict__ row2, const float4* __restrict__ rowg2, int j)
+__device__ __forceinline__ Texel texel_at(const float4* __restrict__ p)
 {
     Texel t;
-    t.c = __ldg(row2 + j);
-    t.g = __ldg(rowg2 + j);
+    t.c = __ldg(p);
+    t.g = __ldg(p + 1);
     return t;
 }
 
@@ -66,6 +75,29 @@ __device__ __forceinline__ Texel lerp_texel(float a, float b, const Texel& t0, c
     r.c = make_float4(c01.x, c01.y, c23.x, c23.y);
     r.g = make_float4(g01.x, g01.y, g23.x, g23.y);
     return r;
+}
+
+// SAMPLER_BILINEAR (:71) read at (u, row + 0.5), OpenCL 1.2 s8.2 with the vertical weight
+// exactly 0: (1-a)*T[i0] + a*T[i0+1], columns clamped to the edge; a non-finite
+// coordinate reads the positive quiet NaN.  General form, for the rare taps the fast
+// paths below do not cover.
+template <bool F>
+__device__ __forceinline__ Texel lerp_texel_at(const float4* __restrict__ row, int W, float u)
+{
+    const float t = u - 0.5f;
+    if (!fin(t)) {
+        const float n = qnan();
+        Texel r;
+        r.c = f4(n, n, n, n);
+        r.g = r.c;
+        return r;
+    }
+    float fl = floorf(t);
+    const float a = t - fl;
+    fl = fminf(fmaxf(fl, -1.0f), (float)W);
+    const int i0 = (int)fl;
+    const int j0 = min(max(i0, 0), W - 1), j1 = min(max(i0 + 1, 0), W - 1);
+    return lerp_texel<F>(a, 1.0f - a, texel_at(row + 2 * j0), texel_at(row + 2 * j1));
 }
 
 // byte k holds the top byte of component k, so bit 7 of byte k is its sign bit
@@ -99,31 +131,20 @@ __device__ __forceinline__ float ad_sum(float4 v2, float4 ref)
     return c01.x + c01.y + c2;
 }
 
-// ---- slow path: one bilinear tap at a time, exactly as the source reads it -------------
+// (w1 * 0.125f) * 0.33f and 0.125f * (0.33f * S) as one multiply: the product of 0.125 and
+// 0.33f is exact, and scaling by a power of two commutes with rounding
+#define PM_K033_8 0.04125000163912773f
 
-// one tap of patch_census_klt2 (:361-370)
-template <bool F>
-__device__ __forceinline__ float klt_tap(float w1, float3 val1, uint32_t sg1, float4 v2, float4 gv2)
-{
-    const float cx = div005(fminf(fabsf(v2.x - val1.x), 0.05f));
-    const float cy = div005(fminf(fabsf(v2.y - val1.y), 0.05f));
-    const float cz = div005(fminf(fabsf(v2.z - val1.z), 0.05f));
-    float C = w1 * 0.125f * 0.33f * (cx + cy + cz);
-    const int n = sign_mismatch(sg1, sign_bytes(gv2));
-    if (F) C = fmaf(w1 * 0.875f * 0.25f, (float)n, C);
-    else C = (float)((double)C + (double)(w1 * 0.875f) * 0.25 * (double)(float)n);
-    return C;
-}
-
-// the cost of one Gauss-Newton tap from its interpolated texel (same arithmetic as klt_tap).
+// the cost of one Gauss-Newton tap from its interpolated texel (:361-370).
 // `w1 * (1.0f - alpha) * 0.25 * (float)cnt` (:370) carries a double literal, so the sum is a
-// double-precision one rounded once: formed exactly in double (strict) or with one fma (fused).
+// double-precision one rounded once: formed exactly in double (strict) or with one fma
+// (fused); w1 * 0.875f * 0.25f is one multiply by 0.21875 for the same reason as above.
 template <bool F>
 __device__ __forceinline__ float klt_cost(float k1, float w1, float4 val1, uint32_t sb1, const Texel& t)
 {
     float C = k1 * ad_sum(t.c, val1);
     const int n = sign_mismatch(sb1, sign_bytes(t.g));
-    if (F) C = fmaf(w1 * 0.875f * 0.25f, (float)n, C);
+    if (F) C = fmaf(w1 * 0.21875f, (float)n, C);
     else C = (float)((double)C + (double)(w1 * 0.875f) * 0.25 * (double)(float)n);
     return C;
 }
@@ -159,7 +180,7 @@ __device__ float patch_eval(const ViewData& V, int px, int py, float4 s, float m
     const float c2x = transform_x(s, cx, cy);
     if (!(fin(s.x) && fin(s.y) && fin(s.z)) || to_normal(s).z < 1e-4f || c2x < 0 || c2x >= (float)V.W) return 1e5f;
     const int W = V.W;
-    const float4 in = __ldg(V.bw1 + (size_t)py * W + px);
+    const float4 in = __ldg(V.row1(py) + 2 * px);
     const float thr = exit_threshold(mincost, in.w);
     float wsum = 0.0f, census = 0.0f;
     if (COUNT) cnt.calls++;
@@ -171,33 +192,28 @@ __device__ float patch_eval(const ViewData& V, int px, int py, float4 s, float m
         const int iy = py + dy;
         const float qy = cy + (float)dy;
         const float byq = s.y * qy;
-        const float4* __restrict__ row1 = V.bw1 + (size_t)iy * W;
-        const float4* __restrict__ rowg1 = V.g1 + (size_t)iy * W;
-        const float4* __restrict__ row2 = V.bw2 + (size_t)iy * W;
-        const float4* __restrict__ rowg2 = V.g2 + (size_t)iy * W;
+        const float4* __restrict__ row1 = V.row1(iy);
+        const float4* __restrict__ row2 = V.row2(iy);
         for (int dx = dx0; dx <= dx1; dx++) {
             const float qx = cx + (float)dx;
             const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
             if (p2x < 0 || p2x >= fW) continue;
-            const int ix = px + dx;
-            const float4 vin = __ldg(row1 + ix);
-            const float4 gin = __ldg(rowg1 + ix);
-            const float w = support_weight<F>(vin.x - in.x, vin.y - in.y, vin.z - in.z);
+            const Texel q = texel_at(row1 + 2 * (px + dx));
+            const float w = support_weight<F>(q.c.x - in.x, q.c.y - in.y, q.c.z - in.z);
             const float t = (p2x + 0.5f) - 0.5f;
             Texel tx;
             if (fin(t)) {
+                // p2x in [0, W) gives t in [0, W]: texels i0, i0 + 1 lie in the padded row
                 const float fl = floorf(t);
                 const float a = t - fl;
-                const int i0 = (int)fl;   // p2x in [0, W) gives t in [0, W]: i0 in [0, W]
-                tx = lerp_texel<F>(a, 1.0f - a, fetch(row2, rowg2, min(i0, W - 1)), fetch(row2, rowg2, min(i0 + 1, W - 1)));
+                const float4* __restrict__ b = row2 + 2 * (int)fl;
+                tx = lerp_texel<F>(a, 1.0f - a, texel_at(b), texel_at(b + 2));
             } else {
-                tx.c = lerp_row<F>(row2, W, p2x + 0.5f);
-                tx.g = lerp_row<F>(rowg2, W, p2x + 0.5f);
+                tx = lerp_texel_at<F>(row2, W, p2x + 0.5f);
             }
-            const float cad = 0.33f * ad_sum(tx.c, vin);
-            float cost = 0.125f * cad;
+            float cost = PM_K033_8 * ad_sum(tx.c, q.c);
             // cost + 0.875f * (0.25f * n): the product 0.21875 n is exact, so one fma rounds the same
-            cost = fmaf(0.21875f, (float)sign_mismatch(sign_bytes(gin), sign_bytes(tx.g)), cost);
+            cost = fmaf(0.21875f, (float)sign_mismatch(sign_bytes(q.g), sign_bytes(tx.g)), cost);
             census = F ? fmaf(w, cost, census) : census + w * cost;
             wsum += w;
             if (COUNT) cnt.eval++;
@@ -221,7 +237,7 @@ __device__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cn
     float2 J01 = f2(0.0f, 0.0f);
     float J2 = 0.0f;
     float2 h00_01 = f2(0.0f, 0.0f), h02_11 = f2(0.0f, 0.0f), h12_22 = f2(0.0f, 0.0f);
-    const float4 c1 = __ldg(V.bw1 + (size_t)py * W + px);
+    const float4 c1 = __ldg(V.row1(py) + 2 * px);
     const int r = V.r;
     const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
     const int dx0 = max(-r, 1 - px), dx1 = min(r, W - 2 - px);   // the 3-point cost needs 1 <= qx < W - 1
@@ -230,18 +246,15 @@ __device__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cn
         const float qy = cyf + (float)dy;
         const float byq = s.y * qy;
         const float yy = qy * qy;
-        const float4* __restrict__ row1 = V.bw1 + (size_t)iy * W;
-        const float4* __restrict__ rowg1 = V.g1 + (size_t)iy * W;
-        const float4* __restrict__ row2 = V.bw2 + (size_t)iy * W;
-        const float4* __restrict__ rowg2 = V.g2 + (size_t)iy * W;
+        const float4* __restrict__ row1 = V.row1(iy);
+        const float4* __restrict__ row2 = V.row2(iy);
         for (int dx = dx0; dx <= dx1; dx++) {
             const float qx = cxf + (float)dx;
-            const int ix = px + dx;
-            const float4 vin = __ldg(row1 + ix);
-            const float4 val1 = make_float4(vin.x - c1.x, vin.y - c1.y, vin.z - c1.z, 0.0f);
+            const Texel q = texel_at(row1 + 2 * (px + dx));
+            const float4 val1 = make_float4(q.c.x - c1.x, q.c.y - c1.y, q.c.z - c1.z, 0.0f);
             const float w1 = support_weight<F>(val1.x, val1.y, val1.z);
-            const uint32_t sb1 = sign_bytes(__ldg(rowg1 + ix));
-            const float k1 = w1 * 0.125f * 0.33f;
+            const uint32_t sb1 = sign_bytes(q.g);
+            const float k1 = w1 * PM_K033_8;
             const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
             const float t0 = (p2x + 0.5f) - 0.5f;
             const float tp = ((p2x + 1.0f) + 0.5f) - 0.5f;
@@ -249,44 +262,40 @@ __device__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cn
             const float f0 = floorf(t0), fp = floorf(tp), fm = floorf(tm);
             const float a0 = t0 - f0;
             float C, Cxp, Cxm;
-            if (fp == f0 + 1.0f && fm == f0 - 1.0f && tp - fp == a0 && tm - fm == a0) {
-                // the three taps read texels f0-1 .. f0+2 with one weight
-                const int i0 = (int)fminf(fmaxf(f0, -2.0f), (float)W + 1.0f);
-                const Texel tA = fetch(row2, rowg2, min(max(i0 - 1, 0), W - 1));
-                const Texel tB = fetch(row2, rowg2, min(max(i0, 0), W - 1));
-                const Texel tC = fetch(row2, rowg2, min(max(i0 + 1, 0), W - 1));
-                const Texel tD = fetch(row2, rowg2, min(max(i0 + 2, 0), W - 1));
+            if (fp == f0 + 1.0f && fm == f0 - 1.0f && tp - fp == a0 && tm - fm == a0 && f0 >= -1.0f &&
+                f0 <= (float)(W - 2)) {
+                // the three taps read texels f0-1 .. f0+2 (inside the padded row) with one weight
+                const float4* __restrict__ b = row2 + 2 * ((int)f0 - 1);
+                const Texel tA = texel_at(b), tB = texel_at(b + 2), tC = texel_at(b + 4), tD = texel_at(b + 6);
                 const float b0 = 1.0f - a0;
                 Cxm = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tA, tB));
                 C = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tB, tC));
                 Cxp = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tC, tD));
             } else {
-                const float3 v1 = make_float3(val1.x, val1.y, val1.z);
-                const uint32_t sg1 = sb1;
-                const float u0 = p2x + 0.5f, up = (p2x + 1.0f) + 0.5f, um = (p2x + -1.0f) + 0.5f;
-                C = klt_tap<F>(w1, v1, sg1, lerp_row<F>(row2, W, u0), lerp_row<F>(rowg2, W, u0));
-                Cxp = klt_tap<F>(w1, v1, sg1, lerp_row<F>(row2, W, up), lerp_row<F>(rowg2, W, up));
-                Cxm = klt_tap<F>(w1, v1, sg1, lerp_row<F>(row2, W, um), lerp_row<F>(rowg2, W, um));
+                Cxm = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, W, (p2x + -1.0f) + 0.5f));
+                C = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, W, p2x + 0.5f));
+                Cxp = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, W, (p2x + 1.0f) + 0.5f));
             }
             if (COUNT) cnt.klt++;
+            // the update of :394-402 without a branch: a rejected sample adds exact zeros, and
+            // no accumulator can be -0, so adding +0 or -0 leaves it unchanged
             const float curv = Cxp + Cxm - 2.0f * C;
-            if (curv > 0.0f) {
-                const float t = w1 * (Cxm - Cxp) * 0.5f;
-                const float sc = w1 * curv;
+            const bool take = curv > 0.0f;
+            const float t = take ? w1 * (Cxm - Cxp) * 0.5f : 0.0f;
+            const float sc = take ? w1 * curv : 0.0f;
+            if (F) {
                 const float2 t2 = f2(t, t), s2 = f2(sc, sc);
-                if (F) {
-                    J01 = __ffma2_rn(t2, f2(qx, qy), J01);
-                    J2 = fmaf(t, 1.0f, J2);
-                    h00_01 = __ffma2_rn(s2, f2(qx * qx, qx * qy), h00_01);
-                    h02_11 = __ffma2_rn(s2, f2(qx, yy), h02_11);
-                    h12_22 = __ffma2_rn(s2, f2(qy, 1.0f), h12_22);
-                } else {   // scalar: see lerp2
-                    J01 = f2(__fadd_rn(J01.x, __fmul_rn(t, qx)), __fadd_rn(J01.y, __fmul_rn(t, qy)));
-                    J2 = J2 + t * 1.0f;
-                    h00_01 = f2(__fadd_rn(h00_01.x, __fmul_rn(sc, qx * qx)), __fadd_rn(h00_01.y, __fmul_rn(sc, qx * qy)));
-                    h02_11 = f2(__fadd_rn(h02_11.x, __fmul_rn(sc, qx)), __fadd_rn(h02_11.y, __fmul_rn(sc, yy)));
-                    h12_22 = f2(__fadd_rn(h12_22.x, __fmul_rn(sc, qy)), __fadd_rn(h12_22.y, __fmul_rn(sc, 1.0f)));
-                }
+                J01 = __ffma2_rn(t2, f2(qx, qy), J01);
+                J2 = fmaf(t, 1.0f, J2);
+                h00_01 = __ffma2_rn(s2, f2(qx * qx, qx * qy), h00_01);
+                h02_11 = __ffma2_rn(s2, f2(qx, yy), h02_11);
+                h12_22 = __ffma2_rn(s2, f2(qy, 1.0f), h12_22);
+            } else {   // scalar: see lerp2
+                J01 = f2(__fadd_rn(J01.x, __fmul_rn(t, qx)), __fadd_rn(J01.y, __fmul_rn(t, qy)));
+                J2 = J2 + t * 1.0f;
+                h00_01 = f2(__fadd_rn(h00_01.x, __fmul_rn(sc, qx * qx)), __fadd_rn(h00_01.y, __fmul_rn(sc, qx * qy)));
+                h02_11 = f2(__fadd_rn(h02_11.x, __fmul_rn(sc, qx)), __fadd_rn(h02_11.y, __fmul_rn(sc, yy)));
+                h12_22 = f2(__fadd_rn(h12_22.x, __fmul_rn(sc, qy)), __fadd_rn(h12_22.y, __fmul_rn(sc, 1.0f)));
             }
         }
     }
