@@ -108,6 +108,7 @@ struct Layout {
     size_t total;
     enum {
         Lbw, Rbw, Lg, Rg, LDT, RDT, Ls, Rs, tmp, mL0, mL1, mR0, mR1, chk, nrm,   // float4 x N
+        pself, pnb,                                                             // float4 x N
         vb1c, vb2c,                                                             // int x N
         vb1s, vb2s,                                                             // u64 x N
         texL, texR,                                                             // texel rows
@@ -129,6 +130,8 @@ Layout layout(int W, int H, size_t stride)
     put(Layout::vb2c, L.N * 4);
     put(Layout::vb1s, L.N * 8);
     put(Layout::vb2s, L.N * 8);
+    put(Layout::pself, L.N * 16);
+    put(Layout::pnb, L.N * 16);
     put(Layout::texL, tex_bytes(W, H));
     put(Layout::texR, tex_bytes(W, H));
     put(Layout::rof, rof_scratch_bytes(W, H));
@@ -211,8 +214,8 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
         initn = nrm;
         nl++;
     }
-    const ViewData VL = {texL, texR, W, H, r, tex_pitch(W)};
-    const ViewData VR = {texR, texL, W, H, r, tex_pitch(W)};
+    const ViewData VL = make_view(texL, texR, W, H, r);
+    const ViewData VR = make_view(texR, texL, W, H, r);
     launch_init(mL[0], VL, dmax, 1, initdisp, initn, F, st);
     nl++;
     if (views == 2) { launch_init(mR[0], VR, dmax, 0, nullptr, nullptr, F, st); nl++; }
@@ -246,6 +249,8 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
         P.vout_src = vb1s;
         P.counters = h->counting ? ctr : nullptr;
         P.error = errf;
+        P.tmp_self = at<float4>(ws, L, Layout::pself);
+        P.tmp_nb = at<float4>(ws, L, Layout::pnb);
         launch_propagate(P, F, st);   // :536-537
         if (views == 2) {
             P.V = VR;
@@ -309,7 +314,7 @@ struct TexPair {
         launch_pack_tex(t2, (const float4*)bw2, (const float4*)g2, W, H, s);
         return PM_OK;
     }
-    ViewData view(int W, int H, int r) const { return ViewData{t1, t2, W, H, r, tex_pitch(W)}; }
+    ViewData view(int W, int H, int r) const { return make_view(t1, t2, W, H, r); }
     ~TexPair()
     {
         if (t1) cudaFreeAsync(t1, st);
@@ -627,7 +632,12 @@ int pm_k_propagate(float* out, const float* old, const float* bw1, const float* 
     P.vout_src = (unsigned long long*)vout_src;
     P.counters = (unsigned long long*)counters;
     P.error = d_err;
+    float4* tmp = nullptr;
+    PM_CUDA(nullptr, cudaMallocAsync((void**)&tmp, (size_t)W * H * 2 * sizeof(float4), S(stream)));
+    P.tmp_self = tmp;
+    P.tmp_nb = tmp + (size_t)W * H;
     launch_propagate(P, fused, S(stream));
+    PM_CUDA(nullptr, cudaFreeAsync(tmp, S(stream)));
     PM_CUDA(nullptr, cudaGetLastError());
     return PM_OK;
 }

@@ -152,8 +152,27 @@ __device__ __forceinline__ void try_candidate(const ViewData& V, int px, int py,
     if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
 }
 
+template <bool COUNT>
+__device__ __forceinline__ void flush_counters(const Counters& cnt, unsigned long long* out)
+{
+    if (!COUNT) return;
+    unsigned long long v[4] = {cnt.eval, cnt.klt, cnt.calls, cnt.exits};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        unsigned long long s = v[k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0 && s) atomicAdd(out + k, s);
+    }
+}
+
+// pmhstereo_propagate_view (pmhstereo.cl:880-1071) runs as three kernels over the same
+// pixels: the candidate chain up to the randomized refinement (k_prop_eval), the six
+// Gauss-Newton steps (k_prop_klt) and the evaluation of their result with the view
+// scatter (k_prop_final).  The per-pixel state between them is `self` and the
+// Gauss-Newton result, kept in two float4 fields; splitting keeps each kernel's register
+// footprint to its own phase.
 template <bool F, bool COUNT>
-__global__ void __launch_bounds__(128) k_propagate(PropParams P)
+__global__ void __launch_bounds__(128) k_prop_eval(PropParams P)
 {
     const ViewData& V = P.V;
     const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
@@ -168,7 +187,6 @@ __global__ void __launch_bounds__(128) k_propagate(PropParams P)
         float4 smooth = P.smooth[idx];
         smooth.w = clampf(smooth.w, 0.0f, 1.0f) * dmax;
         float4 self = P.old[idx];
-        self.w = patch_eval<F, COUNT>(V, px, py, self, 1e10f, cnt);
 
         // cross-view candidates of this pixel; the entry is emptied for the next writer
         int nview = 0;
@@ -186,40 +204,82 @@ __global__ void __launch_bounds__(128) k_propagate(PropParams P)
         // (lin) * ((1*1 - 1) + 2) * 3 + 2 * 4 = 6 * lin + 8
         rng.init_skip((py * W + px + P.iter) * 6 + 8);
 
-        // smooth candidate (:968-976)
-        float4 nb = from_disparity_normal(cx, cy, smooth.w * (lr ? -1.0f : 1.0f),
-                                          normalize3(make_float3(smooth.x, smooth.y, smooth.z)));
-        if (!lr) nb = viewprop(nb);
-        try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
-
-        // random neighbourhood (:982-991), offsets drawn x first, in [-4, 5]
-        for (int i = 0; i < 4; i++) {
-            const int ox = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
-            const int oy = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
-            const int nx = min(max(px + ox, 0), W - 1), ny = min(max(py + oy, 0), V.H - 1);
-            nb = P.old[(size_t)ny * W + nx];
-            try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+        // The candidate sequence as one loop, so that the window evaluation has a single call
+        // site: k = 0 re-evaluates the current plane (:939-940), 1 the smooth plane (:968-976),
+        // 2-5 random neighbours with offsets drawn x first, in [-4, 5] (:982-991), 6 a random
+        // plane (:996-1002), 7-8 the cross-view planes of the kept source columns
+        // (:1007-1016) and 9 the randomized refinement (:1021-1028).
+        for (int k = 0; k < 10; k++) {
+            float4 nb;
+            if (k == 0) {
+                nb = self;
+            } else if (k == 1) {
+                nb = from_disparity_normal(cx, cy, smooth.w * (lr ? -1.0f : 1.0f),
+                                           normalize3(make_float3(smooth.x, smooth.y, smooth.z)));
+                if (!lr) nb = viewprop(nb);
+            } else if (k <= 5) {
+                const int ox = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
+                const int oy = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
+                const int nx = min(max(px + ox, 0), W - 1), ny = min(max(py + oy, 0), V.H - 1);
+                nb = P.old[(size_t)ny * W + nx];
+            } else if (k == 6) {
+                nb = nd_state_init(rng, cx, cy, lr, dmax);
+            } else if (k <= 8) {
+                if (k - 7 >= nview) continue;
+                const unsigned int sx = k == 7 ? (unsigned int)vsrc : (unsigned int)(vsrc >> 32);
+                nb = viewprop(P.vin_planes[(size_t)py * W + sx]);
+            } else {
+                nb = nd_state_refine(rng, self, cx, cy, dmax, lr);
+            }
+            if (k == 0) {
+                self.w = patch_eval<F, COUNT>(V, px, py, nb, 1e10f, cnt);
+            } else {
+                // smoothDistance does not read the cost component, so one evaluation serves
+                // both minimalCost (:873-877) and the acceptance test
+                const float2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
+                const float mincost = self.w + theta * sd.y - theta * sd.x;
+                nb.w = patch_eval<F, COUNT>(V, px, py, nb, mincost, cnt);
+                if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
+            }
         }
+        P.tmp_self[idx] = self;
+    }
+    flush_counters<COUNT>(cnt, P.counters);
+}
 
-        // random plane (:996-1002)
-        nb = nd_state_init(rng, cx, cy, lr, dmax);
-        try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+// Gauss-Newton plane steps (:1034-1038)
+template <bool F, bool COUNT>
+__global__ void __launch_bounds__(128) k_prop_klt(PropParams P)
+{
+    const ViewData& V = P.V;
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+    Counters cnt = {0, 0, 0, 0};
+    if (px < V.W && py < V.H) {
+        const size_t idx = (size_t)py * V.W + px;
+        float4 nb = P.tmp_self[idx];
+        for (int k = 0; k < 6; k++) nb = klt2<F, COUNT>(V, px, py, nb, cnt);
+        P.tmp_nb[idx] = nb;
+    }
+    flush_counters<COUNT>(cnt, P.counters);
+}
 
-        // other view (:1007-1016): planes of the kept source columns, mapped into this view
-        for (int i = 0; i < nview; i++) {
-            const unsigned int sx = i == 0 ? (unsigned int)vsrc : (unsigned int)(vsrc >> 32);
-            nb = viewprop(P.vin_planes[(size_t)py * W + sx]);
-            try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
-        }
-
-        // randomized refinement (:1021-1028)
-        nb = nd_state_refine(rng, self, cx, cy, dmax, lr);
-        try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
-
-        // Gauss-Newton plane steps (:1034-1053)
-        nb = klt2<F, COUNT>(V, px, py, self, cnt);
-        for (int k = 0; k < 5; k++) nb = klt2<F, COUNT>(V, px, py, nb, cnt);
-        try_candidate<F, COUNT>(V, px, py, self, nb, smooth, theta, dmax, lr, cnt);
+// evaluation of the Gauss-Newton result (:1039-1052), view scatter (:1060-1067), output
+template <bool F, bool COUNT>
+__global__ void __launch_bounds__(128) k_prop_final(PropParams P)
+{
+    const ViewData& V = P.V;
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+    Counters cnt = {0, 0, 0, 0};
+    if (px < V.W && py < V.H) {
+        const int W = V.W;
+        const size_t idx = (size_t)py * W + px;
+        const float cx = (float)px, cy = (float)py;
+        const int lr = P.lr;
+        const float dmax = P.dmax;
+        float4 smooth = P.smooth[idx];
+        smooth.w = clampf(smooth.w, 0.0f, 1.0f) * dmax;
+        float4 self = P.tmp_self[idx];
+        try_candidate<F, COUNT>(V, px, py, self, P.tmp_nb[idx], smooth, P.theta, dmax, lr, cnt);
 
         // view scatter (:1060-1067)
         if (P.vout_count) {
@@ -235,14 +295,7 @@ __global__ void __launch_bounds__(128) k_propagate(PropParams P)
         }
         P.out[idx] = self;
     }
-    if (COUNT) {
-        unsigned long long v[4] = {cnt.eval, cnt.klt, cnt.calls, cnt.exits};
-        for (int k = 0; k < 4; k++) {
-            unsigned long long s = v[k];
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-            if ((threadIdx.x & 31) == 0 && s) atomicAdd(P.counters + k, s);
-        }
-    }
+    flush_counters<COUNT>(cnt, P.counters);
 }
 
 __global__ void k_normal_depth(float4* __restrict__ out, const float4* __restrict__ planes, int W, int H,
@@ -438,17 +491,17 @@ __global__ void k_disparity_to_normal(float4* __restrict__ out, const float* __r
     out[(size_t)y * W + x] = f4(n.x, n.y, n.z, 0.0f);
 }
 
-// texel rows of one view (pm_window.cuh): column c in [-2, W+1] holds bw and grad of
-// column clamp(c, 0, W-1)
+// texel planes of one view (pm_window.cuh): column c in [-2, W+1] of the colour plane
+// holds bw, of the gradient plane grad, both of column clamp(c, 0, W-1)
 __global__ void k_pack_tex(float4* __restrict__ tex, const float4* __restrict__ bw, const float4* __restrict__ grad,
                            int W, int H, int P)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x - TEX_PAD, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (c > W + TEX_PAD - 1 || y >= H) return;
     const int s = min(max(c, 0), W - 1);
-    const size_t o = 2 * ((size_t)y * P + c + TEX_PAD);
+    const size_t o = (size_t)y * P + c + TEX_PAD;
     tex[o] = bw[(size_t)y * W + s];
-    tex[o + 1] = grad[(size_t)y * W + s];
+    tex[(size_t)H * P + o] = grad[(size_t)y * W + s];
 }
 
 __global__ void k_view_clear(int* __restrict__ count, unsigned long long* __restrict__ src, size_t n)
@@ -529,13 +582,20 @@ void launch_propagate(const PropParams& P, int fused, cudaStream_t st)
     const dim3 b(32, 4);
     const dim3 g = grid2d(P.V.W, P.V.H, b);
     const bool count = P.counters != nullptr;
+#define PM_PROP_LAUNCH(FF, CC)                          \
+    do {                                                \
+        k_prop_eval<FF, CC><<<g, b, 0, st>>>(P);        \
+        k_prop_klt<FF, CC><<<g, b, 0, st>>>(P);         \
+        k_prop_final<FF, CC><<<g, b, 0, st>>>(P);       \
+    } while (0)
     if (fused) {
-        if (count) k_propagate<true, true><<<g, b, 0, st>>>(P);
-        else k_propagate<true, false><<<g, b, 0, st>>>(P);
+        if (count) PM_PROP_LAUNCH(true, true);
+        else PM_PROP_LAUNCH(true, false);
     } else {
-        if (count) k_propagate<false, true><<<g, b, 0, st>>>(P);
-        else k_propagate<false, false><<<g, b, 0, st>>>(P);
+        if (count) PM_PROP_LAUNCH(false, true);
+        else PM_PROP_LAUNCH(false, false);
     }
+#undef PM_PROP_LAUNCH
 }
 
 void launch_normal_depth(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st)

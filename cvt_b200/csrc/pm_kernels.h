@@ -34,6 +34,8 @@ struct PropParams {
     unsigned long long* vout_src;
     unsigned long long* counters;   // null: not counted
     int* error;                     // incremented if a view-buffer insert gave up
+    float4* tmp_self;               // per-pixel state between the three propagate kernels
+    float4* tmp_nb;
 };
 
 void launch_prep(const uint8_t* img, size_t stride, int W, int H, int r, int fused, float4* bw, float4* grad,
@@ -54,9 +56,13 @@ void launch_fill_depthmap(float* out, const float4* planes, int W, int H, float 
 void launch_fill_normalmap(float4* out, const float4* planes, int W, int H, cudaStream_t st);
 void launch_disparity_to_normal(float4* out, const float* d, int W, int H, cudaStream_t st);
 void launch_view_clear(int* count, unsigned long long* src, size_t n, cudaStream_t st);
-// texel rows of a view (pm_window.cuh) from its bw and grad fields
+// texel planes of a view (pm_window.cuh) from its bw and grad fields
 int tex_pitch(int W);
 size_t tex_bytes(int W, int H);
+inline ViewData make_view(const float4* t1, const float4* t2, int W, int H, int r)
+{
+    return ViewData{t1, t2, W, H, r, tex_pitch(W), tex_pitch(W) * H};
+}
 void launch_pack_tex(float4* tex, const float4* bw, const float4* grad, int W, int H, cudaStream_t st);
 // FP32 peak probe: `iters` rounds of independent fma chains per thread
 void launch_fma_peak(float* out, int iters, int blocks, int threads, cudaStream_t st);

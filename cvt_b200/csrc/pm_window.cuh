@@ -3,11 +3,13 @@
 // (patch_census_klt2, :326-410), one thread per pixel, samples in the
 // reference's order.
 //
-// Texel layout.  Each view is stored as 32-byte texels {colour (r, g, b, Σw),
-// gradient (4 components)} in rows of W + 4 texels: columns -2 .. W+1, the four
-// outside ones replicating the edge texel (CLK_ADDRESS_CLAMP_TO_EDGE).  A
-// bilinear tap pair therefore needs no clamping inside that range and all
-// loads of a sample come from one base address.
+// Texel layout.  Each view is stored as two planes of float4, colour (r, g, b, Σw)
+// and gradient (4 components), the gradient plane `plane` float4 after the
+// colour plane, in rows of W + 4 texels: columns -2 .. W+1, the four outside
+// ones replicating the edge texel (CLK_ADDRESS_CLAMP_TO_EDGE).  A bilinear tap
+// pair therefore needs no clamping inside that range, all loads of a sample
+// come from one index, and the lanes of a warp gathering neighbouring texels
+// read 16-byte strided addresses.
 //
 // Blackwell specifics: the 7-channel bilinear reads of the second view and the
 // truncated absolute differences run as packed FP32 pairs (FFMA2 / FMUL2,
@@ -25,12 +27,13 @@ namespace pm {
 constexpr int TEX_PAD = 2;   // replicated columns on each side of a texel row
 
 struct ViewData {
-    const float4* __restrict__ t1;   // first view texels (row pitch P texels)
-    const float4* __restrict__ t2;   // second view texels
-    int W, H, r, P;
-    // pointer to texel column 0 of row y
-    __device__ __forceinline__ const float4* row1(int y) const { return t1 + 2 * ((size_t)y * P + TEX_PAD); }
-    __device__ __forceinline__ const float4* row2(int y) const { return t2 + 2 * ((size_t)y * P + TEX_PAD); }
+    const float4* __restrict__ t1;   // first view: colour plane, gradient plane at + plane
+    const float4* __restrict__ t2;   // second view
+    int W, H, r, P;                  // P = W + 2 * TEX_PAD texels per row
+    int plane;                       // H * P
+    // colour texel column 0 of row y
+    __device__ __forceinline__ const float4* row1(int y) const { return t1 + (size_t)y * P + TEX_PAD; }
+    __device__ __forceinline__ const float4* row2(int y) const { return t2 + (size_t)y * P + TEX_PAD; }
 };
 
 struct Counters {
@@ -55,11 +58,11 @@ struct Texel {
     float4 c, g;
 };
 
-__device__ __forceinline__ Texel texel_at(const float4* __restrict__ p)
+__device__ __forceinline__ Texel texel_at(const float4* __restrict__ p, int plane)
 {
     Texel t;
     t.c = __ldg(p);
-    t.g = __ldg(p + 1);
+    t.g = __ldg(p + plane);
     return t;
 }
 
@@ -82,7 +85,7 @@ __device__ __forceinline__ Texel lerp_texel(float a, float b, const Texel& t0, c
 // coordinate reads the positive quiet NaN.  General form, for the rare taps the fast
 // paths below do not cover.
 template <bool F>
-__device__ __forceinline__ Texel lerp_texel_at(const float4* __restrict__ row, int W, float u)
+__device__ __forceinline__ Texel lerp_texel_at(const float4* __restrict__ row, int plane, int W, float u)
 {
     const float t = u - 0.5f;
     if (!fin(t)) {
@@ -97,7 +100,7 @@ __device__ __forceinline__ Texel lerp_texel_at(const float4* __restrict__ row, i
     fl = fminf(fmaxf(fl, -1.0f), (float)W);
     const int i0 = (int)fl;
     const int j0 = min(max(i0, 0), W - 1), j1 = min(max(i0 + 1, 0), W - 1);
-    return lerp_texel<F>(a, 1.0f - a, texel_at(row + 2 * j0), texel_at(row + 2 * j1));
+    return lerp_texel<F>(a, 1.0f - a, texel_at(row + j0, plane), texel_at(row + j1, plane));
 }
 
 // byte k holds the top byte of component k, so bit 7 of byte k is its sign bit
@@ -173,14 +176,16 @@ __device__ __forceinline__ float3 lusolve(float h00, float h01, float h02, float
 
 // patch_eval_census (:661-736).  The early exit `census / bilw >= mincost` (:724) is tested
 // as census >= exit_threshold(mincost, bilw), the same predicate without a division.
+// Window coordinates run as floats (integers below 2^24 are exact) instead of being
+// converted from the loop counters.
 template <bool F, bool COUNT>
-__device__ float patch_eval(const ViewData& V, int px, int py, float4 s, float mincost, Counters& cnt)
+__device__ __forceinline__ float patch_eval(const ViewData& V, int px, int py, float4 s, float mincost, Counters& cnt)
 {
     const float cx = (float)px, cy = (float)py;
     const float c2x = transform_x(s, cx, cy);
     if (!(fin(s.x) && fin(s.y) && fin(s.z)) || to_normal(s).z < 1e-4f || c2x < 0 || c2x >= (float)V.W) return 1e5f;
-    const int W = V.W;
-    const float4 in = __ldg(V.row1(py) + 2 * px);
+    const int W = V.W, plane = V.plane;
+    const float4 in = __ldg(V.row1(py) + px);
     const float thr = exit_threshold(mincost, in.w);
     float wsum = 0.0f, census = 0.0f;
     if (COUNT) cnt.calls++;
@@ -188,17 +193,17 @@ __device__ float patch_eval(const ViewData& V, int px, int py, float4 s, float m
     const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
     const int dx0 = max(-r, -px), dx1 = min(r, W - 1 - px);
     const float fW = (float)W;
-    for (int dy = dy0; dy <= dy1; dy++) {
-        const int iy = py + dy;
-        const float qy = cy + (float)dy;
+    const float qx0 = cx + (float)dx0;
+    float qy = cy + (float)dy0;
+    for (int iy = py + dy0; iy <= py + dy1; iy++, qy += 1.0f) {
         const float byq = s.y * qy;
-        const float4* __restrict__ row1 = V.row1(iy);
+        const float4* __restrict__ q1 = V.row1(iy) + px + dx0;
         const float4* __restrict__ row2 = V.row2(iy);
-        for (int dx = dx0; dx <= dx1; dx++) {
-            const float qx = cx + (float)dx;
+        float qx = qx0;
+        for (int n = dx1 - dx0; n >= 0; n--, q1++, qx += 1.0f) {
             const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
             if (p2x < 0 || p2x >= fW) continue;
-            const Texel q = texel_at(row1 + 2 * (px + dx));
+            const Texel q = texel_at(q1, plane);
             const float w = support_weight<F>(q.c.x - in.x, q.c.y - in.y, q.c.z - in.z);
             const float t = (p2x + 0.5f) - 0.5f;
             Texel tx;
@@ -206,10 +211,10 @@ __device__ float patch_eval(const ViewData& V, int px, int py, float4 s, float m
                 // p2x in [0, W) gives t in [0, W]: texels i0, i0 + 1 lie in the padded row
                 const float fl = floorf(t);
                 const float a = t - fl;
-                const float4* __restrict__ b = row2 + 2 * (int)fl;
-                tx = lerp_texel<F>(a, 1.0f - a, texel_at(b), texel_at(b + 2));
+                const float4* __restrict__ b = row2 + (int)fl;
+                tx = lerp_texel<F>(a, 1.0f - a, texel_at(b, plane), texel_at(b + 1, plane));
             } else {
-                tx = lerp_texel_at<F>(row2, W, p2x + 0.5f);
+                tx = lerp_texel_at<F>(row2, plane, W, p2x + 0.5f);
             }
             float cost = PM_K033_8 * ad_sum(tx.c, q.c);
             // cost + 0.875f * (0.25f * n): the product 0.21875 n is exact, so one fma rounds the same
@@ -230,27 +235,28 @@ __device__ float patch_eval(const ViewData& V, int px, int py, float4 s, float m
 // patch_census_klt2 (:326-410), with the in-bounds test on the window position rather than
 // the matched one (:358) and the colour term against the colour difference (:352, :364)
 template <bool F, bool COUNT>
-__device__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cnt)
+__device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cnt)
 {
     const float cxf = (float)px, cyf = (float)py;
-    const int W = V.W;
+    const int W = V.W, plane = V.plane;
     float2 J01 = f2(0.0f, 0.0f);
     float J2 = 0.0f;
     float2 h00_01 = f2(0.0f, 0.0f), h02_11 = f2(0.0f, 0.0f), h12_22 = f2(0.0f, 0.0f);
-    const float4 c1 = __ldg(V.row1(py) + 2 * px);
+    const float4 c1 = __ldg(V.row1(py) + px);
     const int r = V.r;
     const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
     const int dx0 = max(-r, 1 - px), dx1 = min(r, W - 2 - px);   // the 3-point cost needs 1 <= qx < W - 1
-    for (int dy = dy0; dy <= dy1; dy++) {
-        const int iy = py + dy;
-        const float qy = cyf + (float)dy;
+    const float qx0 = cxf + (float)dx0;
+    const float fWm2 = (float)(W - 2);
+    float qy = cyf + (float)dy0;
+    for (int iy = py + dy0; iy <= py + dy1; iy++, qy += 1.0f) {
         const float byq = s.y * qy;
         const float yy = qy * qy;
-        const float4* __restrict__ row1 = V.row1(iy);
+        const float4* __restrict__ q1 = V.row1(iy) + px + dx0;
         const float4* __restrict__ row2 = V.row2(iy);
-        for (int dx = dx0; dx <= dx1; dx++) {
-            const float qx = cxf + (float)dx;
-            const Texel q = texel_at(row1 + 2 * (px + dx));
+        float qx = qx0;
+        for (int n = dx1 - dx0; n >= 0; n--, q1++, qx += 1.0f) {
+            const Texel q = texel_at(q1, plane);
             const float4 val1 = make_float4(q.c.x - c1.x, q.c.y - c1.y, q.c.z - c1.z, 0.0f);
             const float w1 = support_weight<F>(val1.x, val1.y, val1.z);
             const uint32_t sb1 = sign_bytes(q.g);
@@ -262,19 +268,19 @@ __device__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cn
             const float f0 = floorf(t0), fp = floorf(tp), fm = floorf(tm);
             const float a0 = t0 - f0;
             float C, Cxp, Cxm;
-            if (fp == f0 + 1.0f && fm == f0 - 1.0f && tp - fp == a0 && tm - fm == a0 && f0 >= -1.0f &&
-                f0 <= (float)(W - 2)) {
+            if (fp == f0 + 1.0f && fm == f0 - 1.0f && tp - fp == a0 && tm - fm == a0 && f0 >= -1.0f && f0 <= fWm2) {
                 // the three taps read texels f0-1 .. f0+2 (inside the padded row) with one weight
-                const float4* __restrict__ b = row2 + 2 * ((int)f0 - 1);
-                const Texel tA = texel_at(b), tB = texel_at(b + 2), tC = texel_at(b + 4), tD = texel_at(b + 6);
+                const float4* __restrict__ b = row2 + ((int)f0 - 1);
+                const Texel tA = texel_at(b, plane), tB = texel_at(b + 1, plane);
+                const Texel tC = texel_at(b + 2, plane), tD = texel_at(b + 3, plane);
                 const float b0 = 1.0f - a0;
                 Cxm = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tA, tB));
                 C = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tB, tC));
                 Cxp = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tC, tD));
             } else {
-                Cxm = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, W, (p2x + -1.0f) + 0.5f));
-                C = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, W, p2x + 0.5f));
-                Cxp = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, W, (p2x + 1.0f) + 0.5f));
+                Cxm = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + -1.0f) + 0.5f));
+                C = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, p2x + 0.5f));
+                Cxp = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + 1.0f) + 0.5f));
             }
             if (COUNT) cnt.klt++;
             // the update of :394-402 without a branch: a rejected sample adds exact zeros, and
