@@ -267,10 +267,11 @@ def main():
     # roofline of the propagate kernel (FP32-bound): algorithmic flops per launch
     # = 10 per hoisted support weight + 41 per cost-window sample + 129 per
     #   Gauss-Newton window sample, over the launch's measured average duration
+    # one propagate pass = the three kernels of one view and iteration (pm_propagate.cu)
     nlaunch = views * executed(iters)
     flops_launch = (10.0 * window_positions(W, H, r) * nlaunch + 41.0 * ctr[0] + 129.0 * ctr[1]) / nlaunch
-    avg_launch_s = prop_ms / max(prop_n, 1) * 1e-3
-    peak = C_float = None
+    avg_launch_s = prop_ms / (nlaunch * args.steps) * 1e-3
+    peak = None
     import ctypes as C
     pk = C.c_float(0.0)
     if _lib.lib().pm_measure_fp32_peak(local, 200.0, C.byref(pk)) == 0:
@@ -282,7 +283,7 @@ def main():
         traffic = json.load(open(tfile)).get("bytes_per_launch")
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": (achieved / peak) if peak else None, "traffic": traffic,
-            "kernel": "k_propagate", "avg_launch_ms": avg_launch_s * 1e3, "flops_per_launch": flops_launch,
+            "kernel": "propagate pass (k_prop_chain + k_prop_klt + k_prop_final)", "avg_launch_ms": avg_launch_s * 1e3, "flops_per_launch": flops_launch,
             "peak_source": "FP32 fma probe measured in this run (pm_measure_fp32_peak)"}
 
     line = {"metric": METRIC, "value": value, "unit": "Mpixel·iterations/s", "n_gpus": world, "steps": args.steps,

@@ -265,7 +265,7 @@ int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
             P.vout_src = vb2s;
             launch_propagate(P, F, st);   // :542-543
         }
-        prof_mark(h, st, PM_PHASE_PROPAGATE, views);
+        prof_mark(h, st, PM_PHASE_PROPAGATE, 3 * views);   // three kernels per view (pm_propagate.cu)
         launch_normal_depth(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :552-553
         launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
         if (views == 2) {

@@ -140,21 +140,23 @@ __device__ __forceinline__ float3 to_normal(float4 st)
     return n;
 }
 
-// smoothDistance (:846-871): returns (distance of a, distance of b)
-__device__ __forceinline__ float2 smooth_distance(float4 sa, float4 sb, float4 smooth, float cx, float cy,
-                                                  float dmax, int lr)
+// one component of smoothDistance (:846-871): the diagonal-weighted squared distance of a
+// plane's (normal, depth) to the smoothed field; it does not read the plane's cost
+__device__ __forceinline__ float smooth_dist1(float4 s, float4 smooth, float cx, float cy, float dmax, int lr)
 {
-    const float4 a = to_ref_normal_depth(sa, cx, cy, lr);
-    const float4 b = to_ref_normal_depth(sb, cx, cy, lr);
+    const float4 a = to_ref_normal_depth(s, cx, cy, lr);
     const float id2 = 1.0f / (dmax * dmax);
     const float den = id2 + 0.3f;
     const float4 dg = f4(0.1f / den, 0.1f / den, 0.1f / den, id2 / den);
     const float4 da = f4(a.x - smooth.x, a.y - smooth.y, a.z - smooth.z, a.w - smooth.w);
-    const float4 db = f4(b.x - smooth.x, b.y - smooth.y, b.z - smooth.z, b.w - smooth.w);
-    float2 r;
-    r.x = da.x * (dg.x * da.x) + da.y * (dg.y * da.y) + da.z * (dg.z * da.z) + da.w * (dg.w * da.w);
-    r.y = db.x * (dg.x * db.x) + db.y * (dg.y * db.y) + db.z * (dg.z * db.z) + db.w * (dg.w * db.w);
-    return r;
+    return da.x * (dg.x * da.x) + da.y * (dg.y * da.y) + da.z * (dg.z * da.z) + da.w * (dg.w * da.w);
+}
+
+// smoothDistance (:846-871): returns (distance of a, distance of b)
+__device__ __forceinline__ float2 smooth_distance(float4 sa, float4 sb, float4 smooth, float cx, float cy,
+                                                  float dmax, int lr)
+{
+    return make_float2(smooth_dist1(sa, smooth, cx, cy, dmax, lr), smooth_dist1(sb, smooth, cx, cy, dmax, lr));
 }
 
 __device__ __forceinline__ uint32_t signbits4(float4 v)
@@ -176,11 +178,35 @@ __device__ __forceinline__ float gray_dot(float dx, float dy, float dz)
     return dx * PM_GW_R + dy * PM_GW_G + dz * PM_GW_B;
 }
 
-// support weight exp(-|dot(I1(q) - I1(p), gray)| * 12) (:355, :701, :1491)
+// expf_ for x in [-87, 0]: the same operations as expf_ on that range, without its NaN /
+// overflow / underflow branches, and with rint(x * log2 e) taken by adding 1.5 * 2^23
+// (the sum rounds to the nearest integer, ties to even, exactly as rintf) so that the
+// integer part comes from the float's bits rather than from two conversions
+__device__ __forceinline__ float expf_neg(float x)
+{
+    const float M = 12582912.0f;   // 1.5 * 2^23
+    const float t = __fadd_rn(__fmul_rn(x, 1.44269502162933349609375f), M);
+    const float n = __fsub_rn(t, M);
+    float r = fmaf(n, -0.693145751953125f, x);
+    r = fmaf(n, -1.428606765330187045e-06f, r);
+    float p = 1.9841270113829523e-4f;
+    p = fmaf(p, r, 1.3888889e-3f);
+    p = fmaf(p, r, 8.3333338e-3f);
+    p = fmaf(p, r, 4.1666668e-2f);
+    p = fmaf(p, r, 1.6666667e-1f);
+    p = fmaf(p, r, 0.5f);
+    p = fmaf(p, r, 1.0f);
+    p = fmaf(p, r, 1.0f);
+    const int ni = __float_as_int(t) - __float_as_int(M);   // n as an integer, in [-126, 0]
+    return p * __int_as_float((ni + 127) << 23);
+}
+
+// support weight exp(-|dot(I1(q) - I1(p), gray)| * 12) (:355, :701, :1491).  Colours are
+// in [0, 1], so |dot| <= 1 and the argument lies in [-12.0001, 0], inside expf_neg's range.
 template <bool F>
 __device__ __forceinline__ float support_weight(float dx, float dy, float dz)
 {
-    return expf_(-fabsf(gray_dot<F>(dx, dy, dz)) * 12.0f);
+    return expf_neg(-fabsf(gray_dot<F>(dx, dy, dz)) * 12.0f);
 }
 
 // SAMPLER_BILINEAR (:71) read at (u, row + 0.5): OpenCL 1.2 s8.2 with the vertical

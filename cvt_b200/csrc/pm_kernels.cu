@@ -122,182 +122,6 @@ __global__ void k_klt(float4* __restrict__ out, const float4* __restrict__ plane
     out[i] = klt2<F, false>(V, x, y, planes[i], cnt);
 }
 
-// keep the two smallest source columns of a view-buffer entry (see pm_kernels.h)
-__device__ __forceinline__ bool view_insert(unsigned long long* slot, unsigned int x)
-{
-    unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(slot);
-    for (int guard = 0; guard < 4096; guard++) {
-        const unsigned int lo = (unsigned int)cur, hi = (unsigned int)(cur >> 32);
-        unsigned long long nv;
-        if (x < lo) nv = ((unsigned long long)lo << 32) | x;
-        else if (x < hi) nv = ((unsigned long long)x << 32) | lo;
-        else return true;
-        const unsigned long long prev = atomicCAS(slot, cur, nv);
-        if (prev == cur) return true;
-        cur = prev;
-    }
-    return false;
-}
-
-template <bool F, bool COUNT>
-__device__ __forceinline__ void try_candidate(const ViewData& V, int px, int py, float4& self, float4 nb, float4 smooth,
-                                              float theta, float dmax, int lr, Counters& cnt)
-{
-    const float cx = (float)px, cy = (float)py;
-    // smoothDistance does not read the cost component, so one evaluation serves both
-    // minimalCost (:873-877) and the acceptance test
-    const float2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
-    const float mincost = self.w + theta * sd.y - theta * sd.x;
-    nb.w = patch_eval<F, COUNT>(V, px, py, nb, mincost, cnt);
-    if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
-}
-
-template <bool COUNT>
-__device__ __forceinline__ void flush_counters(const Counters& cnt, unsigned long long* out)
-{
-    if (!COUNT) return;
-    unsigned long long v[4] = {cnt.eval, cnt.klt, cnt.calls, cnt.exits};
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        unsigned long long s = v[k];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if ((threadIdx.x & 31) == 0 && s) atomicAdd(out + k, s);
-    }
-}
-
-// pmhstereo_propagate_view (pmhstereo.cl:880-1071) runs as three kernels over the same
-// pixels: the candidate chain up to the randomized refinement (k_prop_eval), the six
-// Gauss-Newton steps (k_prop_klt) and the evaluation of their result with the view
-// scatter (k_prop_final).  The per-pixel state between them is `self` and the
-// Gauss-Newton result, kept in two float4 fields; splitting keeps each kernel's register
-// footprint to its own phase.
-template <bool F, bool COUNT>
-__global__ void __launch_bounds__(128) k_prop_eval(PropParams P)
-{
-    const ViewData& V = P.V;
-    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
-    Counters cnt = {0, 0, 0, 0};
-    if (px < V.W && py < V.H) {
-        const int W = V.W;
-        const size_t idx = (size_t)py * W + px;
-        const float cx = (float)px, cy = (float)py;
-        const int lr = P.lr;
-        const float theta = P.theta, dmax = P.dmax;
-        // pmhstereo_propagate_view (pmhstereo.cl:927-940)
-        float4 smooth = P.smooth[idx];
-        smooth.w = clampf(smooth.w, 0.0f, 1.0f) * dmax;
-        float4 self = P.old[idx];
-
-        // cross-view candidates of this pixel; the entry is emptied for the next writer
-        int nview = 0;
-        unsigned long long vsrc = ~0ULL;
-        if (P.vin_count) {
-            nview = P.vin_count[idx];
-            vsrc = P.vin_src[idx];
-            P.vin_count[idx] = 0;
-            P.vin_src[idx] = ~0ULL;
-            nview = min(nview, 2);
-        }
-
-        Rng rng;
-        // RNG_init(&rng, lin, ((1*1 - 1) + NUMRNDTRIES) * 3 + 2 * NUMRNDSAMPLE) (:942) expands to
-        // (lin) * ((1*1 - 1) + 2) * 3 + 2 * 4 = 6 * lin + 8
-        rng.init_skip((py * W + px + P.iter) * 6 + 8);
-
-        // The candidate sequence as one loop, so that the window evaluation has a single call
-        // site: k = 0 re-evaluates the current plane (:939-940), 1 the smooth plane (:968-976),
-        // 2-5 random neighbours with offsets drawn x first, in [-4, 5] (:982-991), 6 a random
-        // plane (:996-1002), 7-8 the cross-view planes of the kept source columns
-        // (:1007-1016) and 9 the randomized refinement (:1021-1028).
-        for (int k = 0; k < 10; k++) {
-            float4 nb;
-            if (k == 0) {
-                nb = self;
-            } else if (k == 1) {
-                nb = from_disparity_normal(cx, cy, smooth.w * (lr ? -1.0f : 1.0f),
-                                           normalize3(make_float3(smooth.x, smooth.y, smooth.z)));
-                if (!lr) nb = viewprop(nb);
-            } else if (k <= 5) {
-                const int ox = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
-                const int oy = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
-                const int nx = min(max(px + ox, 0), W - 1), ny = min(max(py + oy, 0), V.H - 1);
-                nb = P.old[(size_t)ny * W + nx];
-            } else if (k == 6) {
-                nb = nd_state_init(rng, cx, cy, lr, dmax);
-            } else if (k <= 8) {
-                if (k - 7 >= nview) continue;
-                const unsigned int sx = k == 7 ? (unsigned int)vsrc : (unsigned int)(vsrc >> 32);
-                nb = viewprop(P.vin_planes[(size_t)py * W + sx]);
-            } else {
-                nb = nd_state_refine(rng, self, cx, cy, dmax, lr);
-            }
-            if (k == 0) {
-                self.w = patch_eval<F, COUNT>(V, px, py, nb, 1e10f, cnt);
-            } else {
-                // smoothDistance does not read the cost component, so one evaluation serves
-                // both minimalCost (:873-877) and the acceptance test
-                const float2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
-                const float mincost = self.w + theta * sd.y - theta * sd.x;
-                nb.w = patch_eval<F, COUNT>(V, px, py, nb, mincost, cnt);
-                if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
-            }
-        }
-        P.tmp_self[idx] = self;
-    }
-    flush_counters<COUNT>(cnt, P.counters);
-}
-
-// Gauss-Newton plane steps (:1034-1038)
-template <bool F, bool COUNT>
-__global__ void __launch_bounds__(128) k_prop_klt(PropParams P)
-{
-    const ViewData& V = P.V;
-    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
-    Counters cnt = {0, 0, 0, 0};
-    if (px < V.W && py < V.H) {
-        const size_t idx = (size_t)py * V.W + px;
-        float4 nb = P.tmp_self[idx];
-        for (int k = 0; k < 6; k++) nb = klt2<F, COUNT>(V, px, py, nb, cnt);
-        P.tmp_nb[idx] = nb;
-    }
-    flush_counters<COUNT>(cnt, P.counters);
-}
-
-// evaluation of the Gauss-Newton result (:1039-1052), view scatter (:1060-1067), output
-template <bool F, bool COUNT>
-__global__ void __launch_bounds__(128) k_prop_final(PropParams P)
-{
-    const ViewData& V = P.V;
-    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
-    Counters cnt = {0, 0, 0, 0};
-    if (px < V.W && py < V.H) {
-        const int W = V.W;
-        const size_t idx = (size_t)py * W + px;
-        const float cx = (float)px, cy = (float)py;
-        const int lr = P.lr;
-        const float dmax = P.dmax;
-        float4 smooth = P.smooth[idx];
-        smooth.w = clampf(smooth.w, 0.0f, 1.0f) * dmax;
-        float4 self = P.tmp_self[idx];
-        try_candidate<F, COUNT>(V, px, py, self, P.tmp_nb[idx], smooth, P.theta, dmax, lr, cnt);
-
-        // view scatter (:1060-1067)
-        if (P.vout_count) {
-            const float sidesign = lr ? -1.0f : 1.0f;
-            const float tx = transform_x(self, cx, cy);
-            const int xpv = __float2int_rn(tx);
-            const int disp = (int)((tx - cx) * sidesign);
-            if (xpv >= 0 && xpv < W && disp > 0) {
-                const size_t t = (size_t)py * W + xpv;
-                atomicAdd(P.vout_count + t, 1);
-                if (!view_insert(P.vout_src + t, (unsigned int)px)) atomicAdd(P.error, 1);
-            }
-        }
-        P.out[idx] = self;
-    }
-    flush_counters<COUNT>(cnt, P.counters);
-}
-
 __global__ void k_normal_depth(float4* __restrict__ out, const float4* __restrict__ planes, int W, int H,
                                float dispscale, int lr)
 {
@@ -575,27 +399,6 @@ void launch_klt(float4* out, const float4* planes, const ViewData& V, int fused,
     const dim3 b(32, 4);
     if (fused) k_klt<true><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, planes, V);
     else k_klt<false><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, planes, V);
-}
-
-void launch_propagate(const PropParams& P, int fused, cudaStream_t st)
-{
-    const dim3 b(32, 4);
-    const dim3 g = grid2d(P.V.W, P.V.H, b);
-    const bool count = P.counters != nullptr;
-#define PM_PROP_LAUNCH(FF, CC)                          \
-    do {                                                \
-        k_prop_eval<FF, CC><<<g, b, 0, st>>>(P);        \
-        k_prop_klt<FF, CC><<<g, b, 0, st>>>(P);         \
-        k_prop_final<FF, CC><<<g, b, 0, st>>>(P);       \
-    } while (0)
-    if (fused) {
-        if (count) PM_PROP_LAUNCH(true, true);
-        else PM_PROP_LAUNCH(true, false);
-    } else {
-        if (count) PM_PROP_LAUNCH(false, true);
-        else PM_PROP_LAUNCH(false, false);
-    }
-#undef PM_PROP_LAUNCH
 }
 
 void launch_normal_depth(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st)

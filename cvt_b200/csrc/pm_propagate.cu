@@ -1,0 +1,306 @@
+// pmhstereo_propagate_view (cvt/cl/kernel/pmhstereo.cl:880-1071) on sm_100a, as three
+// kernels over the same pixels:
+//   k_prop_chain  the candidate chain up to the randomized refinement (:927-1028)
+//   k_prop_klt    the six Gauss-Newton steps (:1034-1038)
+//   k_prop_final  the evaluation of their result, the view scatter and the output (:1039-1070)
+// The state between them is `self` and the Gauss-Newton result (two float4 fields).
+//
+// The candidate chain runs as a per-lane state machine.  Each lane evaluates its pixel's
+// candidates in the source's order, but a lane whose window evaluation ends (early exit,
+// :724-726, or the last sample) closes that candidate and opens its next one at once,
+// instead of idling until every lane of the warp has finished the same candidate.  The
+// candidate planes that do not depend on the evolving best plane (smooth, the four random
+// neighbours, the random plane, the cross-view planes) are generated up front in the
+// source's RNG order and parked in shared memory with their smoothing distance; the
+// refinement, which depends on the best plane, is generated when it is reached.  Per lane
+// the sequence of operations, and therefore every result, is unchanged.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pm_kernels.h"
+
+namespace pm {
+
+namespace {
+
+constexpr int PROP_BX = 32, PROP_BY = 4, PROP_THREADS = PROP_BX * PROP_BY;
+
+inline dim3 grid2d(int W, int H, dim3 b) { return dim3((W + b.x - 1) / b.x, (H + b.y - 1) / b.y); }
+
+template <bool COUNT>
+__device__ __forceinline__ void flush_counters(const Counters& cnt, unsigned long long* out)
+{
+    if (!COUNT) return;
+    unsigned long long v[4] = {cnt.eval, cnt.klt, cnt.calls, cnt.exits};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        unsigned long long s = v[k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0 && s) atomicAdd(out + k, s);
+    }
+}
+
+// keep the two smallest source columns of a view-buffer entry (see pm_kernels.h)
+__device__ __forceinline__ bool view_insert(unsigned long long* slot, unsigned int x)
+{
+    unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(slot);
+    for (int guard = 0; guard < 4096; guard++) {
+        const unsigned int lo = (unsigned int)cur, hi = (unsigned int)(cur >> 32);
+        unsigned long long nv;
+        if (x < lo) nv = ((unsigned long long)lo << 32) | x;
+        else if (x < hi) nv = ((unsigned long long)x << 32) | lo;
+        else return true;
+        const unsigned long long prev = atomicCAS(slot, cur, nv);
+        if (prev == cur) return true;
+        cur = prev;
+    }
+    return false;
+}
+
+// pmhstereo_propagate_view (:927-1028): candidates k = 0 (the current plane, re-evaluated,
+// :939-940), 1 smooth (:968-976), 2-5 random neighbours with offsets drawn x first, in
+// [-4, 5] (:982-991), 6 a random plane (:996-1002), 7-8 cross-view planes (:1007-1016),
+// 9 the randomized refinement (:1021-1028).
+template <bool F, bool COUNT>
+__global__ void __launch_bounds__(PROP_THREADS) k_prop_chain(PropParams P)
+{
+    __shared__ float4 cand[8][PROP_THREADS];   // candidates 1..8: (a, b, c, smoothing distance)
+    const ViewData& V = P.V;
+    const int tid = threadIdx.y * PROP_BX + threadIdx.x;
+    const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
+    const bool live = px < V.W && py < V.H;
+    const int W = V.W, plane = V.plane;
+    const float fW = (float)W;
+    const float cx = (float)px, cy = (float)py;
+    const int lr = P.lr;
+    const float theta = P.theta, dmax = P.dmax;
+    Counters cnt = {0, 0, 0, 0};
+
+    float4 self = f4(0, 0, 0, 0), smooth = f4(0, 0, 0, 0), in = f4(0, 0, 0, 0);
+    float sd_self = 0.0f;
+    unsigned int absent = 0;   // bit k: candidate k does not exist (view candidates beyond the count)
+    Rng rng;
+    rng.x = rng.c = 0;
+    if (live) {
+        const size_t idx = (size_t)py * W + px;
+        smooth = P.smooth[idx];
+        smooth.w = clampf(smooth.w, 0.0f, 1.0f) * dmax;   // :927-928
+        self = P.old[idx];
+        in = __ldg(V.row1(py) + px);
+        // cross-view candidates of this pixel; the entry is emptied for the next writer
+        int nview = 0;
+        unsigned long long vsrc = ~0ULL;
+        if (P.vin_count) {
+            nview = min(P.vin_count[idx], 2);
+            vsrc = P.vin_src[idx];
+            P.vin_count[idx] = 0;
+            P.vin_src[idx] = ~0ULL;
+        }
+        // RNG_init(&rng, lin, ((1*1 - 1) + NUMRNDTRIES) * 3 + 2 * NUMRNDSAMPLE) (:942) expands to
+        // (lin) * ((1*1 - 1) + 2) * 3 + 2 * 4 = 6 * lin + 8
+        rng.init_skip((py * W + px + P.iter) * 6 + 8);
+        for (int k = 1; k <= 8; k++) {
+            float4 nb;
+            if (k == 1) {
+                nb = from_disparity_normal(cx, cy, smooth.w * (lr ? -1.0f : 1.0f),
+                                           normalize3(make_float3(smooth.x, smooth.y, smooth.z)));
+                if (!lr) nb = viewprop(nb);
+            } else if (k <= 5) {
+                const int ox = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
+                const int oy = (int)((rng.next() - 0.5f) * 2.0f * 5.0f + 0.5f);
+                nb = P.old[(size_t)min(max(py + oy, 0), V.H - 1) * W + min(max(px + ox, 0), W - 1)];
+            } else if (k == 6) {
+                nb = nd_state_init(rng, cx, cy, lr, dmax);
+            } else {
+                if (k - 7 >= nview) {
+                    absent |= 1u << k;
+                    continue;
+                }
+                nb = viewprop(P.vin_planes[(size_t)py * W + (k == 7 ? (unsigned int)vsrc : (unsigned int)(vsrc >> 32))]);
+            }
+            nb.w = smooth_dist1(nb, smooth, cx, cy, dmax, lr);
+            cand[k - 1][tid] = nb;
+        }
+        sd_self = smooth_dist1(self, smooth, cx, cy, dmax, lr);
+    }
+
+    // evaluation state of the current candidate
+    int k = live ? -1 : 10;   // 10: chain finished
+    bool active = false;      // a window evaluation is in progress
+    bool exited = false;
+    float4 cur = f4(0, 0, 0, 0);   // candidate plane; .w its smoothing distance
+    float thr = 0.0f, census = 0.0f, wsum = 0.0f;
+    const int r = V.r;
+    const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
+    const int dx0 = max(-r, -px), dx1 = min(r, W - 1 - px);
+    const float qx0 = cx + (float)dx0;
+    int iy = 0, n = 0;
+    float qx = 0.0f, qy = 0.0f, byq = 0.0f;
+    const float4* q1 = nullptr;
+    const float4* row2 = nullptr;
+
+    for (;;) {
+        const bool need = k < 10 && !active;
+        if (__any_sync(0xffffffffu, need)) {
+            if (need) {
+                // close the candidate whose window just ended ...
+                if (k >= 0) {
+                    const float cost = exited ? 1.0f : (wsum <= 1.0f ? 1.1f : census / wsum);
+                    if (k == 0) {
+                        self.w = cost;
+                    } else if (cost + theta * cur.w <= self.w + theta * sd_self) {   // :976 etc.
+                        self = f4(cur.x, cur.y, cur.z, cost);
+                        sd_self = cur.w;
+                    }
+                }
+                // ... and open the next one that needs a window, settling unusable ones here
+                for (;;) {
+                    k++;
+                    while (k >= 7 && k <= 8 && ((absent >> k) & 1u)) k++;
+                    if (k >= 10) break;
+                    if (k == 0) {
+                        cur = self;
+                    } else if (k <= 8) {
+                        cur = cand[k - 1][tid];
+                    } else {
+                        cur = nd_state_refine(rng, self, cx, cy, dmax, lr);
+                        cur.w = smooth_dist1(cur, smooth, cx, cy, dmax, lr);
+                    }
+                    if (!plane_usable(cur, cx, cy, W)) {   // cost 1e5 without a window (:677-678)
+                        if (k == 0) {
+                            self.w = 1e5f;
+                        } else if (1e5f + theta * cur.w <= self.w + theta * sd_self) {
+                            self = f4(cur.x, cur.y, cur.z, 1e5f);
+                            sd_self = cur.w;
+                        }
+                        continue;
+                    }
+                    // minimalCost (:873-877)
+                    const float mincost = k == 0 ? 1e10f : self.w + theta * sd_self - theta * cur.w;
+                    thr = exit_threshold(mincost, in.w);
+                    census = 0.0f;
+                    wsum = 0.0f;
+                    exited = false;
+                    active = true;
+                    iy = py + dy0;
+                    qy = cy + (float)dy0;
+                    byq = cur.y * qy;
+                    n = dx1 - dx0;
+                    qx = qx0;
+                    q1 = V.row1(iy) + px + dx0;
+                    row2 = V.row2(iy);
+                    if (COUNT) cnt.calls++;
+                    break;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, k >= 10)) break;
+        if (active) {
+            if (eval_sample<F>(q1, row2, plane, W, fW, in, cur, qx, byq, census, wsum)) {
+                if (COUNT) cnt.eval++;
+                if (census >= thr) {   // :724-726
+                    if (COUNT) cnt.exits++;
+                    exited = true;
+                    active = false;
+                }
+            }
+            if (active) {
+                q1++;
+                qx += 1.0f;
+                if (--n < 0) {
+                    if (++iy > py + dy1) {
+                        active = false;
+                    } else {
+                        qy += 1.0f;
+                        byq = cur.y * qy;
+                        n = dx1 - dx0;
+                        qx = qx0;
+                        q1 = V.row1(iy) + px + dx0;
+                        row2 = V.row2(iy);
+                    }
+                }
+            }
+        }
+    }
+    if (live) P.tmp_self[(size_t)py * W + px] = self;
+    flush_counters<COUNT>(cnt, P.counters);
+}
+
+// Gauss-Newton plane steps (:1034-1038)
+template <bool F, bool COUNT>
+__global__ void __launch_bounds__(PROP_THREADS) k_prop_klt(PropParams P)
+{
+    const ViewData& V = P.V;
+    const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
+    Counters cnt = {0, 0, 0, 0};
+    if (px < V.W && py < V.H) {
+        const size_t idx = (size_t)py * V.W + px;
+        float4 nb = P.tmp_self[idx];
+        for (int k = 0; k < 6; k++) nb = klt2<F, COUNT>(V, px, py, nb, cnt);
+        P.tmp_nb[idx] = nb;
+    }
+    flush_counters<COUNT>(cnt, P.counters);
+}
+
+// evaluation of the Gauss-Newton result (:1039-1052), view scatter (:1060-1067), output (:1070)
+template <bool F, bool COUNT>
+__global__ void __launch_bounds__(PROP_THREADS) k_prop_final(PropParams P)
+{
+    const ViewData& V = P.V;
+    const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
+    Counters cnt = {0, 0, 0, 0};
+    if (px < V.W && py < V.H) {
+        const int W = V.W;
+        const size_t idx = (size_t)py * W + px;
+        const float cx = (float)px, cy = (float)py;
+        const int lr = P.lr;
+        const float dmax = P.dmax, theta = P.theta;
+        float4 smooth = P.smooth[idx];
+        smooth.w = clampf(smooth.w, 0.0f, 1.0f) * dmax;
+        float4 self = P.tmp_self[idx];
+        float4 nb = P.tmp_nb[idx];
+        const float2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
+        const float mincost = self.w + theta * sd.y - theta * sd.x;
+        nb.w = patch_eval<F, COUNT>(V, px, py, nb, mincost, cnt);
+        if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
+
+        if (P.vout_count) {
+            const float sidesign = lr ? -1.0f : 1.0f;
+            const float tx = transform_x(self, cx, cy);
+            const int xpv = __float2int_rn(tx);           // convert_int_rte
+            const int disp = (int)((tx - cx) * sidesign);  // convert_int
+            if (xpv >= 0 && xpv < W && disp > 0) {
+                const size_t t = (size_t)py * W + xpv;
+                atomicAdd(P.vout_count + t, 1);
+                if (!view_insert(P.vout_src + t, (unsigned int)px)) atomicAdd(P.error, 1);
+            }
+        }
+        P.out[idx] = self;
+    }
+    flush_counters<COUNT>(cnt, P.counters);
+}
+
+}  // namespace
+
+void launch_propagate(const PropParams& P, int fused, cudaStream_t st)
+{
+    const dim3 b(PROP_BX, PROP_BY);
+    const dim3 g = grid2d(P.V.W, P.V.H, b);
+    const bool count = P.counters != nullptr;
+#define PM_PROP_LAUNCH(FF, CC)                      \
+    do {                                            \
+        k_prop_chain<FF, CC><<<g, b, 0, st>>>(P);   \
+        k_prop_klt<FF, CC><<<g, b, 0, st>>>(P);     \
+        k_prop_final<FF, CC><<<g, b, 0, st>>>(P);   \
+    } while (0)
+    if (fused) {
+        if (count) PM_PROP_LAUNCH(true, true);
+        else PM_PROP_LAUNCH(true, false);
+    } else {
+        if (count) PM_PROP_LAUNCH(false, true);
+        else PM_PROP_LAUNCH(false, false);
+    }
+#undef PM_PROP_LAUNCH
+}
+
+}  // namespace pm

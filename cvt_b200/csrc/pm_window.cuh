@@ -174,6 +174,46 @@ __device__ __forceinline__ float3 lusolve(float h00, float h01, float h02, float
     return ret;
 }
 
+// one window sample of patch_eval_census (:690-722) at window position (qx, row of q1) of a
+// pixel with centre texel `in`, for the plane s (byq = s.y * qy): accumulates the weighted
+// cost into census and the weight into wsum, or returns false when the matched column lies
+// outside the image (:693-696)
+template <bool F>
+__device__ __forceinline__ bool eval_sample(const float4* __restrict__ q1, const float4* __restrict__ row2, int plane,
+                                            int W, float fW, float4 in, float4 s, float qx, float byq, float& census,
+                                            float& wsum)
+{
+    const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
+    if (p2x < 0 || p2x >= fW) return false;
+    const Texel q = texel_at(q1, plane);
+    const float w = support_weight<F>(q.c.x - in.x, q.c.y - in.y, q.c.z - in.z);
+    const float t = (p2x + 0.5f) - 0.5f;
+    Texel tx;
+    if (fin(t)) {
+        // p2x in [0, W) gives t in [0, W]: texels i0, i0 + 1 lie in the padded row
+        const float fl = floorf(t);
+        const float a = t - fl;
+        const float4* __restrict__ b = row2 + (int)fl;
+        tx = lerp_texel<F>(a, 1.0f - a, texel_at(b, plane), texel_at(b + 1, plane));
+    } else {
+        tx = lerp_texel_at<F>(row2, plane, W, p2x + 0.5f);
+    }
+    float cost = PM_K033_8 * ad_sum(tx.c, q.c);
+    // cost + 0.875f * (0.25f * n): the product 0.21875 n is exact, so one fma rounds the same
+    cost = fmaf(0.21875f, (float)sign_mismatch(sign_bytes(q.g), sign_bytes(tx.g)), cost);
+    census = F ? fmaf(w, cost, census) : census + w * cost;
+    wsum += w;
+    return true;
+}
+
+// validity test at the top of patch_eval_census (:675-678): a plane that is not finite,
+// too steep, or whose centre matches outside the image costs 1e5 without a window
+__device__ __forceinline__ bool plane_usable(float4 s, float cx, float cy, int W)
+{
+    const float c2x = transform_x(s, cx, cy);
+    return fin(s.x) && fin(s.y) && fin(s.z) && !(to_normal(s).z < 1e-4f) && !(c2x < 0) && !(c2x >= (float)W);
+}
+
 // patch_eval_census (:661-736).  The early exit `census / bilw >= mincost` (:724) is tested
 // as census >= exit_threshold(mincost, bilw), the same predicate without a division.
 // Window coordinates run as floats (integers below 2^24 are exact) instead of being
@@ -182,8 +222,7 @@ template <bool F, bool COUNT>
 __device__ __forceinline__ float patch_eval(const ViewData& V, int px, int py, float4 s, float mincost, Counters& cnt)
 {
     const float cx = (float)px, cy = (float)py;
-    const float c2x = transform_x(s, cx, cy);
-    if (!(fin(s.x) && fin(s.y) && fin(s.z)) || to_normal(s).z < 1e-4f || c2x < 0 || c2x >= (float)V.W) return 1e5f;
+    if (!plane_usable(s, cx, cy, V.W)) return 1e5f;
     const int W = V.W, plane = V.plane;
     const float4 in = __ldg(V.row1(py) + px);
     const float thr = exit_threshold(mincost, in.w);
@@ -201,26 +240,7 @@ __device__ __forceinline__ float patch_eval(const ViewData& V, int px, int py, f
         const float4* __restrict__ row2 = V.row2(iy);
         float qx = qx0;
         for (int n = dx1 - dx0; n >= 0; n--, q1++, qx += 1.0f) {
-            const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
-            if (p2x < 0 || p2x >= fW) continue;
-            const Texel q = texel_at(q1, plane);
-            const float w = support_weight<F>(q.c.x - in.x, q.c.y - in.y, q.c.z - in.z);
-            const float t = (p2x + 0.5f) - 0.5f;
-            Texel tx;
-            if (fin(t)) {
-                // p2x in [0, W) gives t in [0, W]: texels i0, i0 + 1 lie in the padded row
-                const float fl = floorf(t);
-                const float a = t - fl;
-                const float4* __restrict__ b = row2 + (int)fl;
-                tx = lerp_texel<F>(a, 1.0f - a, texel_at(b, plane), texel_at(b + 1, plane));
-            } else {
-                tx = lerp_texel_at<F>(row2, plane, W, p2x + 0.5f);
-            }
-            float cost = PM_K033_8 * ad_sum(tx.c, q.c);
-            // cost + 0.875f * (0.25f * n): the product 0.21875 n is exact, so one fma rounds the same
-            cost = fmaf(0.21875f, (float)sign_mismatch(sign_bytes(q.g), sign_bytes(tx.g)), cost);
-            census = F ? fmaf(w, cost, census) : census + w * cost;
-            wsum += w;
+            if (!eval_sample<F>(q1, row2, plane, W, fW, in, s, qx, byq, census, wsum)) continue;
             if (COUNT) cnt.eval++;
             if (census >= thr) {
                 if (COUNT) cnt.exits++;
@@ -247,7 +267,7 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
     const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
     const int dx0 = max(-r, 1 - px), dx1 = min(r, W - 2 - px);   // the 3-point cost needs 1 <= qx < W - 1
     const float qx0 = cxf + (float)dx0;
-    const float fWm2 = (float)(W - 2);
+    const float fWm2 = (float)(W - 2), fWm1 = (float)(W - 1);
     float qy = cyf + (float)dy0;
     for (int iy = py + dy0; iy <= py + dy1; iy++, qy += 1.0f) {
         const float byq = s.y * qy;
@@ -262,13 +282,28 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
             const uint32_t sb1 = sign_bytes(q.g);
             const float k1 = w1 * PM_K033_8;
             const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
-            const float t0 = (p2x + 0.5f) - 0.5f;
-            const float tp = ((p2x + 1.0f) + 0.5f) - 0.5f;
-            const float tm = ((p2x + -1.0f) + 0.5f) - 0.5f;
-            const float f0 = floorf(t0), fp = floorf(tp), fm = floorf(tm);
-            const float a0 = t0 - f0;
+            // Common case: 1 <= p2x < W - 1 and p2x + 1.5 in the binade of p2x.  Then p2x is a
+            // multiple of its ulp (<= 0.5), every +-1 and +-0.5 below is exact, the three taps'
+            // coordinates are p2x - 1, p2x, p2x + 1 and they share the weight p2x - floor(p2x).
+            // Otherwise the coordinates are formed as the source forms them and compared.
+            float f0, a0;
+            bool shared = p2x >= 1.0f && p2x < fWm1 &&
+                          ((__float_as_uint(p2x + 1.5f) ^ __float_as_uint(p2x)) < 0x00800000u);
+            if (shared) {
+                f0 = floorf(p2x);
+                a0 = p2x - f0;
+            } else {
+                const float t0 = (p2x + 0.5f) - 0.5f;
+                const float tp = ((p2x + 1.0f) + 0.5f) - 0.5f;
+                const float tm = ((p2x + -1.0f) + 0.5f) - 0.5f;
+                f0 = floorf(t0);
+                const float fp = floorf(tp), fm = floorf(tm);
+                a0 = t0 - f0;
+                shared = fp == f0 + 1.0f && fm == f0 - 1.0f && tp - fp == a0 && tm - fm == a0 && f0 >= -1.0f &&
+                         f0 <= fWm2;
+            }
             float C, Cxp, Cxm;
-            if (fp == f0 + 1.0f && fm == f0 - 1.0f && tp - fp == a0 && tm - fm == a0 && f0 >= -1.0f && f0 <= fWm2) {
+            if (shared) {
                 // the three taps read texels f0-1 .. f0+2 (inside the padded row) with one weight
                 const float4* __restrict__ b = row2 + ((int)f0 - 1);
                 const Texel tA = texel_at(b, plane), tB = texel_at(b + 1, plane);
