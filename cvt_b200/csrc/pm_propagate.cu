@@ -5,15 +5,11 @@
 //   k_prop_final  the evaluation of their result, the view scatter and the output (:1039-1070)
 // The state between them is `self` and the Gauss-Newton result (two float4 fields).
 //
-// The candidate chain runs as a per-lane state machine.  Each lane evaluates its pixel's
-// candidates in the source's order, but a lane whose window evaluation ends (early exit,
-// :724-726, or the last sample) closes that candidate and opens its next one at once,
-// instead of idling until every lane of the warp has finished the same candidate.  The
-// candidate planes that do not depend on the evolving best plane (smooth, the four random
-// neighbours, the random plane, the cross-view planes) are generated up front in the
-// source's RNG order and parked in shared memory with their smoothing distance; the
-// refinement, which depends on the best plane, is generated when it is reached.  Per lane
-// the sequence of operations, and therefore every result, is unchanged.
+// The candidate chain keeps the source's structure: the lanes of a warp evaluate their
+// pixels' k-th candidates together, so that neighbouring lanes read neighbouring texels of
+// both views (a per-lane schedule, where each lane moves on to its next candidate as soon as
+// its window ends, measured slower: the lanes' windows then diverge in rows and planes and
+// the L1 hit rate halves).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -24,6 +20,14 @@ namespace pm {
 namespace {
 
 constexpr int PROP_BX = 32, PROP_BY = 4, PROP_THREADS = PROP_BX * PROP_BY;
+// resident blocks per SM asked of the register allocator for each kernel (at 128 threads,
+// 6 blocks = 80 registers, 5 = 96; measured best at 6 for both)
+#ifndef PM_CHAIN_BLOCKS
+#define PM_CHAIN_BLOCKS 6
+#endif
+#ifndef PM_KLT_BLOCKS
+#define PM_KLT_BLOCKS 6
+#endif
 
 inline dim3 grid2d(int W, int H, dim3 b) { return dim3((W + b.x - 1) / b.x, (H + b.y - 1) / b.y); }
 
@@ -60,33 +64,24 @@ __device__ __forceinline__ bool view_insert(unsigned long long* slot, unsigned i
 // pmhstereo_propagate_view (:927-1028): candidates k = 0 (the current plane, re-evaluated,
 // :939-940), 1 smooth (:968-976), 2-5 random neighbours with offsets drawn x first, in
 // [-4, 5] (:982-991), 6 a random plane (:996-1002), 7-8 cross-view planes (:1007-1016),
-// 9 the randomized refinement (:1021-1028).
+// 9 the randomized refinement (:1021-1028).  One loop, so that the window evaluation has a
+// single call site.
 template <bool F, bool COUNT>
-__global__ void __launch_bounds__(PROP_THREADS) k_prop_chain(PropParams P)
+__global__ void __launch_bounds__(PROP_THREADS, PM_CHAIN_BLOCKS) k_prop_chain(PropParams P)
 {
-    __shared__ float4 cand[8][PROP_THREADS];   // candidates 1..8: (a, b, c, smoothing distance)
     const ViewData& V = P.V;
-    const int tid = threadIdx.y * PROP_BX + threadIdx.x;
     const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
-    const bool live = px < V.W && py < V.H;
-    const int W = V.W, plane = V.plane;
-    const float fW = (float)W;
-    const float cx = (float)px, cy = (float)py;
-    const int lr = P.lr;
-    const float theta = P.theta, dmax = P.dmax;
     Counters cnt = {0, 0, 0, 0};
-
-    float4 self = f4(0, 0, 0, 0), smooth = f4(0, 0, 0, 0), in = f4(0, 0, 0, 0);
-    float sd_self = 0.0f;
-    unsigned int absent = 0;   // bit k: candidate k does not exist (view candidates beyond the count)
-    Rng rng;
-    rng.x = rng.c = 0;
-    if (live) {
+    if (px < V.W && py < V.H) {
+        const int W = V.W;
         const size_t idx = (size_t)py * W + px;
-        smooth = P.smooth[idx];
+        const float cx = (float)px, cy = (float)py;
+        const int lr = P.lr;
+        const float theta = P.theta, dmax = P.dmax;
+        float4 smooth = P.smooth[idx];
         smooth.w = clampf(smooth.w, 0.0f, 1.0f) * dmax;   // :927-928
-        self = P.old[idx];
-        in = __ldg(V.row1(py) + px);
+        float4 self = P.old[idx];
+
         // cross-view candidates of this pixel; the entry is emptied for the next writer
         int nview = 0;
         unsigned long long vsrc = ~0ULL;
@@ -96,12 +91,18 @@ __global__ void __launch_bounds__(PROP_THREADS) k_prop_chain(PropParams P)
             P.vin_count[idx] = 0;
             P.vin_src[idx] = ~0ULL;
         }
+
+        Rng rng;
         // RNG_init(&rng, lin, ((1*1 - 1) + NUMRNDTRIES) * 3 + 2 * NUMRNDSAMPLE) (:942) expands to
         // (lin) * ((1*1 - 1) + 2) * 3 + 2 * 4 = 6 * lin + 8
         rng.init_skip((py * W + px + P.iter) * 6 + 8);
-        for (int k = 1; k <= 8; k++) {
+
+        float sd_self = 0.0f;   // smoothing distance of `self` (smoothDistance does not read the cost)
+        for (int k = 0; k < 10; k++) {
             float4 nb;
-            if (k == 1) {
+            if (k == 0) {
+                nb = self;
+            } else if (k == 1) {
                 nb = from_disparity_normal(cx, cy, smooth.w * (lr ? -1.0f : 1.0f),
                                            normalize3(make_float3(smooth.x, smooth.y, smooth.z)));
                 if (!lr) nb = viewprop(nb);
@@ -111,124 +112,34 @@ __global__ void __launch_bounds__(PROP_THREADS) k_prop_chain(PropParams P)
                 nb = P.old[(size_t)min(max(py + oy, 0), V.H - 1) * W + min(max(px + ox, 0), W - 1)];
             } else if (k == 6) {
                 nb = nd_state_init(rng, cx, cy, lr, dmax);
-            } else {
-                if (k - 7 >= nview) {
-                    absent |= 1u << k;
-                    continue;
-                }
+            } else if (k <= 8) {
+                if (k - 7 >= nview) continue;
                 nb = viewprop(P.vin_planes[(size_t)py * W + (k == 7 ? (unsigned int)vsrc : (unsigned int)(vsrc >> 32))]);
+            } else {
+                nb = nd_state_refine(rng, self, cx, cy, dmax, lr);
             }
-            nb.w = smooth_dist1(nb, smooth, cx, cy, dmax, lr);
-            cand[k - 1][tid] = nb;
+            if (k == 0) {
+                self.w = patch_eval<F, COUNT>(V, px, py, nb, 1e10f, cnt);
+                sd_self = smooth_dist1(self, smooth, cx, cy, dmax, lr);
+            } else {
+                const float sd = smooth_dist1(nb, smooth, cx, cy, dmax, lr);
+                // minimalCost (:873-877)
+                const float mincost = self.w + theta * sd_self - theta * sd;
+                nb.w = patch_eval<F, COUNT>(V, px, py, nb, mincost, cnt);
+                if (nb.w + theta * sd <= self.w + theta * sd_self) {   // :976 etc.
+                    self = nb;
+                    sd_self = sd;
+                }
+            }
         }
-        sd_self = smooth_dist1(self, smooth, cx, cy, dmax, lr);
+        P.tmp_self[idx] = self;
     }
-
-    // evaluation state of the current candidate
-    int k = live ? -1 : 10;   // 10: chain finished
-    bool active = false;      // a window evaluation is in progress
-    bool exited = false;
-    float4 cur = f4(0, 0, 0, 0);   // candidate plane; .w its smoothing distance
-    float thr = 0.0f, census = 0.0f, wsum = 0.0f;
-    const int r = V.r;
-    const int dy0 = max(-r, -py), dy1 = min(r, V.H - 1 - py);
-    const int dx0 = max(-r, -px), dx1 = min(r, W - 1 - px);
-    const float qx0 = cx + (float)dx0;
-    int iy = 0, n = 0;
-    float qx = 0.0f, qy = 0.0f, byq = 0.0f;
-    const float4* q1 = nullptr;
-    const float4* row2 = nullptr;
-
-    for (;;) {
-        const bool need = k < 10 && !active;
-        if (__any_sync(0xffffffffu, need)) {
-            if (need) {
-                // close the candidate whose window just ended ...
-                if (k >= 0) {
-                    const float cost = exited ? 1.0f : (wsum <= 1.0f ? 1.1f : census / wsum);
-                    if (k == 0) {
-                        self.w = cost;
-                    } else if (cost + theta * cur.w <= self.w + theta * sd_self) {   // :976 etc.
-                        self = f4(cur.x, cur.y, cur.z, cost);
-                        sd_self = cur.w;
-                    }
-                }
-                // ... and open the next one that needs a window, settling unusable ones here
-                for (;;) {
-                    k++;
-                    while (k >= 7 && k <= 8 && ((absent >> k) & 1u)) k++;
-                    if (k >= 10) break;
-                    if (k == 0) {
-                        cur = self;
-                    } else if (k <= 8) {
-                        cur = cand[k - 1][tid];
-                    } else {
-                        cur = nd_state_refine(rng, self, cx, cy, dmax, lr);
-                        cur.w = smooth_dist1(cur, smooth, cx, cy, dmax, lr);
-                    }
-                    if (!plane_usable(cur, cx, cy, W)) {   // cost 1e5 without a window (:677-678)
-                        if (k == 0) {
-                            self.w = 1e5f;
-                        } else if (1e5f + theta * cur.w <= self.w + theta * sd_self) {
-                            self = f4(cur.x, cur.y, cur.z, 1e5f);
-                            sd_self = cur.w;
-                        }
-                        continue;
-                    }
-                    // minimalCost (:873-877)
-                    const float mincost = k == 0 ? 1e10f : self.w + theta * sd_self - theta * cur.w;
-                    thr = exit_threshold(mincost, in.w);
-                    census = 0.0f;
-                    wsum = 0.0f;
-                    exited = false;
-                    active = true;
-                    iy = py + dy0;
-                    qy = cy + (float)dy0;
-                    byq = cur.y * qy;
-                    n = dx1 - dx0;
-                    qx = qx0;
-                    q1 = V.row1(iy) + px + dx0;
-                    row2 = V.row2(iy);
-                    if (COUNT) cnt.calls++;
-                    break;
-                }
-            }
-        }
-        if (__all_sync(0xffffffffu, k >= 10)) break;
-        if (active) {
-            if (eval_sample<F>(q1, row2, plane, W, fW, in, cur, qx, byq, census, wsum)) {
-                if (COUNT) cnt.eval++;
-                if (census >= thr) {   // :724-726
-                    if (COUNT) cnt.exits++;
-                    exited = true;
-                    active = false;
-                }
-            }
-            if (active) {
-                q1++;
-                qx += 1.0f;
-                if (--n < 0) {
-                    if (++iy > py + dy1) {
-                        active = false;
-                    } else {
-                        qy += 1.0f;
-                        byq = cur.y * qy;
-                        n = dx1 - dx0;
-                        qx = qx0;
-                        q1 = V.row1(iy) + px + dx0;
-                        row2 = V.row2(iy);
-                    }
-                }
-            }
-        }
-    }
-    if (live) P.tmp_self[(size_t)py * W + px] = self;
     flush_counters<COUNT>(cnt, P.counters);
 }
 
 // Gauss-Newton plane steps (:1034-1038)
 template <bool F, bool COUNT>
-__global__ void __launch_bounds__(PROP_THREADS) k_prop_klt(PropParams P)
+__global__ void __launch_bounds__(PROP_THREADS, PM_KLT_BLOCKS) k_prop_klt(PropParams P)
 {
     const ViewData& V = P.V;
     const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
