@@ -20,7 +20,7 @@ SYMBOLS = [
     "pm_set_profiling", "pm_get_phase_times", "pm_measure_fp32_peak",
     "pm_disparity_map_batch_device",
     "pm_k_prep", "pm_k_init", "pm_k_cost", "pm_k_klt", "pm_k_propagate", "pm_k_normal_depth",
-    "pm_rof_scratch_bytes", "pm_k_rof", "pm_k_consistency", "pm_k_to_disparity", "pm_k_fill_depthmap",
+    "pm_rof_scratch_bytes", "pm_k_rof", "pm_k_rof_static", "pm_k_consistency", "pm_k_to_disparity", "pm_k_fill_depthmap",
     "pm_k_fill_normalmap", "pm_k_disparity_to_normal",
     "pm_rng_floats", "pm_expf_host", "pm_sinf_host", "pm_cosf_host", "pm_acospif_host",
     "pm_exit_threshold_host", "pm_scene_generate",
@@ -79,6 +79,7 @@ def lib():
         "pm_k_normal_depth": (i32, [vp, vp, i32, i32, f32, i32, vp]),
         "pm_rof_scratch_bytes": (sz, [i32, i32]),
         "pm_k_rof": (i32, [vp, vp, vp, C.POINTER(C.c_float), i32, i32, i32, vp, vp]),
+        "pm_k_rof_static": (i32, [vp, vp, vp, C.POINTER(C.c_float), i32, i32, i32, vp]),
         "pm_k_consistency": (i32, [vp, vp, vp, i32, i32, f32, f32, vp]),
         "pm_k_to_disparity": (i32, [vp, vp, i32, i32, f32, i32, vp]),
         "pm_k_fill_depthmap": (i32, [vp, vp, i32, i32, f32, vp]),

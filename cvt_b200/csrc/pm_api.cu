@@ -7,6 +7,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -55,6 +56,32 @@ int cuda_fail(pm_handle* h, cudaError_t e, const char* what)
         cudaError_t e_ = (call);                                 \
         if (e_ != cudaSuccess) return cuda_fail((h), e_, #call); \
     } while (0)
+
+// Scratch of pm_k_rof_static: a file-scope device array, so that the entry point
+// allocates nothing.  It holds the ROF intermediates of launch_rof (7 float4 per
+// pixel: u, two dual images p of 2 float4, two q) for up to
+// PM_ROF_STATIC_MAX_PIXELS pixels = 28 MiB of every context that loads this
+// library.  Its device address is looked up once per device, under a lock.
+constexpr size_t kRofStaticBytes = (size_t)PM_ROF_STATIC_MAX_PIXELS * 7 * sizeof(float4);
+__device__ __align__(256) unsigned char g_rof_static[kRofStaticBytes];
+constexpr int kMaxDevices = 64;
+std::mutex g_rof_static_mu;
+void* g_rof_static_ptr[kMaxDevices] = {};
+
+int rof_static_scratch(void** out)
+{
+    int dev = 0;
+    PM_CUDA(nullptr, cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(nullptr, PM_EINVAL_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_rof_static_mu);
+    if (!g_rof_static_ptr[dev]) {
+        void* p = nullptr;
+        PM_CUDA(nullptr, cudaGetSymbolAddress(&p, g_rof_static));
+        g_rof_static_ptr[dev] = p;
+    }
+    *out = g_rof_static_ptr[dev];
+    return PM_OK;
+}
 
 int check_shape(pm_handle* h, int W, int H, int r)
 {
@@ -659,6 +686,31 @@ int pm_k_rof(float* out, const float* input, const float* dt, const float lambda
     int rc = check_shape(nullptr, W, H, 0);
     if (rc) return rc;
     if (!out || !input || !dt || !lambda || !scratch || out == input) return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    launch_rof((float4*)out, (const float4*)input, (const float4*)dt,
+               make_float4(lambda[0], lambda[1], lambda[2], lambda[3]), iters, W, H, scratch, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+// Same steps as pm_k_rof on the library's static scratch.  Nothing in the scratch has
+// to start at zero: the first step takes p = q = 0 and u = input without reading it,
+// and every later step reads only what the step before wrote, so the contents left by
+// the previous call never reach the result.  Two calls in flight at once (two streams,
+// two host threads, two handles) share the scratch and race.
+int pm_k_rof_static(float* out, const float* input, const float* dt, const float lambda[4], int iters, int W, int H,
+                    void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    if ((int64_t)W * H > PM_ROF_STATIC_MAX_PIXELS)
+        return fail(nullptr, PM_EINVAL_SHAPE,
+                    "pm_k_rof_static: " + std::to_string(W) + " x " + std::to_string(H) +
+                        " pixels exceed the static scratch of PM_ROF_STATIC_MAX_PIXELS = " +
+                        std::to_string(PM_ROF_STATIC_MAX_PIXELS) + "; use pm_k_rof with a caller buffer");
+    if (!out || !input || !dt || !lambda || out == input) return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    void* scratch = nullptr;
+    rc = rof_static_scratch(&scratch);
+    if (rc) return rc;
     launch_rof((float4*)out, (const float4*)input, (const float4*)dt,
                make_float4(lambda[0], lambda[1], lambda[2], lambda[3]), iters, W, H, scratch, S(stream));
     PM_CUDA(nullptr, cudaGetLastError());

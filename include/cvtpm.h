@@ -152,6 +152,22 @@ int pm_k_normal_depth(float* out, const float* planes, int width, int height, fl
 size_t pm_rof_scratch_bytes(int width, int height);
 int pm_k_rof(float* out, const float* input, const float* dt, const float lambda[4], int iters, int width,
              int height, void* scratch, void* stream);
+/* No counterpart in the reference (whose PDOptCL::denoiseDiffusionTensorROF_PDD,
+ * PDOptCL.cpp:1114-1168, allocates its temporaries on every call).  pm_k_rof without
+ * a scratch argument and without any allocation: the intermediates live in a
+ * library-owned static device array of PM_ROF_STATIC_MAX_PIXELS pixels (28 MiB per
+ * context).  For callers that cannot allocate device memory on this path: a binding
+ * that only passes image pointers and has no device allocator to make a scratch
+ * buffer, or a loop under a fixed device-memory budget that must not stall other
+ * streams behind cudaMalloc/cudaFree.  Results equal pm_k_rof's.
+ * - The first call on each device (the device current at the call) looks up the
+ *   array's address; make that first call before any stream capture begins.
+ * - width*height > PM_ROF_STATIC_MAX_PIXELS returns PM_EINVAL_SHAPE with a message.
+ * - All calls share one array: calls in flight at the same time (two streams, two
+ *   host threads) race; serialise them. */
+#define PM_ROF_STATIC_MAX_PIXELS 262144
+int pm_k_rof_static(float* out, const float* input, const float* dt, const float lambda[4], int iters,
+                    int width, int height, void* stream);
 /* pmhstereo_consistency (pmhstereo.cl:1095-1129) */
 int pm_k_consistency(float* out, const float* left, const float* right, int width, int height,
                      float maxdispdiff, float maxanglediff, void* stream);
