@@ -42,7 +42,7 @@ WORKLOADS = {
     "small": (320, 240, 12, 2.0, 30.0, 7, 32.0, 4, 1, 0),
 }
 # bounded CPU samples (crop of the same scene, same window / range / iterations)
-CPU_CROP = {"hd": (128, 72), "small": (160, 120)}
+CPU_CROP = {"hd": (256, 144), "small": (320, 240)}
 REF_CROP = {"hd": (96, 54), "small": (96, 72)}
 
 
@@ -165,19 +165,97 @@ def run_reference(args, wl, rank, world):
     print(json.dumps(line))
 
 
+def run_batch(args, rank, world, local):
+    """--config batch: 64 pairs of uneven sizes (batch_specs: W x H uniform in [320,1920] x
+    [240,1080], 8-60 planes, disparity range max(32, W/10)), 21x21 window, 8 (9) iterations,
+    both views, LR check, as one graph launch (pm_disparity_map_batch_device), against the
+    same 64 pairs as 64 eager single-pair calls.  Each rank runs the whole batch of its own
+    seed (weak scaling)."""
+    import torch
+    import torch.distributed as dist
+
+    from cvt_b200 import PMHuberStereo, scene
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    specs = scene.batch_specs(seed=1234 + 1000 * rank)
+    pairs = scene.batch(specs)
+    dl = [torch.from_numpy(a).cuda() for a, _ in pairs]
+    dr = [torch.from_numpy(b).cuda() for _, b in pairs]
+    rs = [10] * len(specs)
+    dm = [s["dispmax"] for s in specs]
+    iters = 8
+    px_it = sum(s["width"] * s["height"] for s in specs) * executed(iters)
+    pm = PMHuberStereo(views=2, fused=True, device=local)
+    seq = PMHuberStereo(views=2, fused=True, device=local, use_graph=False)
+
+    def timed(fn, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(steps):
+            ev[k][0].record()
+            fn()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        t = torch.tensor([sum(a.elapsed_time(b) for a, b in ev)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def batched():
+        pm.disparity_map_batch(dl, dr, rs, dm, iters, pp=1)
+
+    def sequential():
+        for a, b, r, d in zip(dl, dr, rs, dm):
+            seq.disparity_map(a, b, r, d, iters, pp=1)
+
+    for _ in range(args.warmup):
+        batched()
+    clocks = Clocks(local).start()
+    tb = timed(batched, args.steps)
+    clk = clocks.stop()
+    sequential()
+    ts = timed(sequential, args.steps)
+    value = world * px_it * args.steps / (tb * 1e-3) / 1e6
+    line = {"metric": METRIC, "value": value, "unit": "Mpixel·iterations/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tb / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batch", "pairs": len(specs), "megapixels": px_it / executed(iters) / 1e6,
+                       "window": 21, "iterations": iters, "iterations_executed": executed(iters), "views": 2,
+                       "pp": "lrcheck", "parallelism": "pairs%d" % world, "schedule": "one graph launch",
+                       "l2": "inputs and workspaces (~25 GB) far larger than L2"},
+            "sequential": {"value": world * px_it * args.steps / (ts * 1e-3) / 1e6, "ms_per_step": ts / args.steps,
+                           "schedule": "64 eager single-pair calls"},
+            "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="hd", choices=sorted(WORKLOADS))
+    ap.add_argument("--config", default="hd", choices=sorted(WORKLOADS) + ["batch"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run warmup + steps of the device pipeline (for ncu captures) and print the step times")
     args = ap.parse_args()
-    wl = WORKLOADS[args.config]
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    if args.config == "batch":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the batched workload is timed on the GPU only"}))
+            return
+        run_batch(args, rank, world, local)
+        return
+    wl = WORKLOADS[args.config]
     if args.impl == "reference":
         run_reference(args, wl, rank, world)
         return
@@ -216,28 +294,21 @@ def main():
         pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
     torch.cuda.synchronize()
 
-    # timed region
-    pm.set_profiling(True)
+    # timed region: the product path (each call one CUDA graph launch, enqueued back to back)
     clocks = Clocks(local).start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    prop_ms, prop_n, launches = 0.0, 0, 0
     for k in range(args.steps):
         flush.fill_(k & 0xff)
         ev[k][0].record()
         pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
         ev[k][1].record()
-        ph = pm.phase_times()
-        prop_ms += ph["propagate"][0]
-        prop_n += ph["propagate"][1]
-        launches += ph["total"][1]
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    pm.set_profiling(False)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -245,6 +316,16 @@ def main():
     total_ms = float(total.item())
     px_it = W * H * executed(iters)
     value = world * px_it * args.steps / (total_ms * 1e-3) / 1e6
+
+    # one more step with per-phase events (eager launches), outside the timed region: the
+    # propagate kernels' device time for the roofline and the launch count per step
+    flush.fill_(0x5a)
+    pm.set_profiling(True)
+    pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+    ph = pm.phase_times()
+    pm.set_profiling(False)
+    prop_ms = ph["propagate"][0]
+    launches = ph["total"][1] * args.steps
 
     # end to end through the host API: pinned host images in, disparity map out
     pl = torch.from_numpy(L).pin_memory().numpy()
@@ -270,7 +351,7 @@ def main():
     # one propagate pass = the three kernels of one view and iteration (pm_propagate.cu)
     nlaunch = views * executed(iters)
     flops_launch = (10.0 * window_positions(W, H, r) * nlaunch + 41.0 * ctr[0] + 129.0 * ctr[1]) / nlaunch
-    avg_launch_s = prop_ms / (nlaunch * args.steps) * 1e-3
+    avg_launch_s = prop_ms / nlaunch * 1e-3
     peak = None
     import ctypes as C
     pk = C.c_float(0.0)
@@ -297,7 +378,7 @@ def main():
                     "d2h_bytes_per_step": W * H * 4},
             "roofline": roof, "clocks": clk, "gpu_launches": launches,
             "counters": {"cost_samples": ctr[0], "gn_samples": ctr[1], "cost_evals": ctr[2], "early_exits": ctr[3]},
-            "phase_ms": {k: v[0] for k, v in pm.phase_times().items()}}
+            "phase_ms": {k: v[0] for k, v in ph.items()}}
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, dt, kind, cores = cpu_sample("port", CPU_CROP[args.config], wl, (L, R))
         cw, ch = CPU_CROP[args.config]

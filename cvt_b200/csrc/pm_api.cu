@@ -7,6 +7,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -32,7 +33,17 @@ struct pm_handle {
     int W = 0, H = 0;
     void* ws = nullptr;
     size_t ws_bytes = 0;
-    cudaStream_t own = nullptr;
+    cudaStream_t own = nullptr;   // blocking stream for calls made on the legacy default stream
+    // CUDA graphs of the last single-pair and batched calls, replayed while the call's
+    // arguments (buffers, sizes, parameters) are unchanged
+    int capturing = 0;
+    std::vector<uint64_t> key1, keyb;
+    cudaGraphExec_t exec1 = nullptr, execb = nullptr;
+    // batched calls: one workspace per pair, branch streams and their fork/join events
+    std::vector<void*> bws;
+    std::vector<size_t> bws_bytes;
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> bev;
 };
 
 namespace {
@@ -97,7 +108,7 @@ inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
 // and contained `launches` kernel launches
 void prof_mark(pm_handle* h, cudaStream_t st, int phase, int launches)
 {
-    if (!h->profiling) return;
+    if (!h->profiling || h->capturing) return;
     if (h->ev_used == (int)h->ev.size()) {
         cudaEvent_t e;
         if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return; }
@@ -113,7 +124,7 @@ void prof_mark(pm_handle* h, cudaStream_t st, int phase, int launches)
 
 int prof_collect(pm_handle* h, cudaStream_t st)
 {
-    if (!h->profiling) return PM_OK;
+    if (!h->profiling || h->capturing) return PM_OK;
     PM_CUDA(h, cudaStreamSynchronize(st));
     for (int k = 0; k < PM_NPHASES; k++) { h->phase_ms[k] = 0.0f; h->phase_launches[k] = 0; }
     for (int i = 1; i < h->ev_used; i++) {
@@ -177,29 +188,33 @@ Layout layout(int W, int H, size_t stride)
 
 template <class T> T* at(void* base, const Layout& L, int k) { return reinterpret_cast<T*>(static_cast<char*>(base) + L.off[k]); }
 
-int ensure_ws(pm_handle* h, int W, int H, size_t stride)
+// grow a workspace to `bytes` (contents are not kept); a replayable graph that holds the
+// old address is dropped by the caller through the argument key
+int grow(pm_handle* h, void*& ws, size_t& have, size_t bytes)
 {
-    const Layout L = layout(W, H, stride);
-    if (h->ws && h->ws_bytes >= L.total) return PM_OK;
-    if (h->ws) { cudaFree(h->ws); h->ws = nullptr; h->ws_bytes = 0; }
-    cudaError_t e = cudaMalloc(&h->ws, L.total);
+    if (ws && have >= bytes) return PM_OK;
+    if (ws) { cudaFree(ws); ws = nullptr; have = 0; }
+    cudaError_t e = cudaMalloc(&ws, bytes);
     if (e != cudaSuccess) { cudaGetLastError(); return fail(h, PM_ENOMEM, "device workspace allocation failed"); }
-    h->ws_bytes = L.total;
+    have = bytes;
     return PM_OK;
 }
 
-// one pass of disparityMapAll + disparityMap post-processing on device buffers
-int run_pipeline(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int r,
-                 float dmax, int iterations, int pp, float* dmap, float4* normal, const float* initdisp,
+int ensure_ws(pm_handle* h, int W, int H, size_t stride)
+{
+    return grow(h, h->ws, h->ws_bytes, layout(W, H, stride).total);
+}
+
+// one pass of disparityMapAll + disparityMap post-processing on device buffers, in the
+// workspace `ws` (at least layout(W, H, stride).total bytes)
+int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
+                 int r, float dmax, int iterations, int pp, float* dmap, float4* normal, const float* initdisp,
                  const float4* initnormal, float4* planesL, float4* planesR, cudaStream_t st)
 {
     const pm_options& o = h->opt;
     const int views = o.views;
     const int F = o.fused;
-    int rc = ensure_ws(h, W, H, stride);
-    if (rc) return rc;
     const Layout L = layout(W, H, stride);
-    void* ws = h->ws;
     const size_t N = L.N;
     float4 *Lbw = at<float4>(ws, L, Layout::Lbw), *Rbw = at<float4>(ws, L, Layout::Rbw);
     float4 *Lg = at<float4>(ws, L, Layout::Lg), *Rg = at<float4>(ws, L, Layout::Rg);
@@ -364,6 +379,90 @@ int check_args(pm_handle* h, const void* left, const void* right, int W, int H, 
     return PM_OK;
 }
 
+// the handle's own blocking stream: graphs are captured on it (capture is not possible on
+// the legacy default stream) and launched on the caller's stream
+int own_stream(pm_handle* h, cudaStream_t* out)
+{
+    if (!h->own) PM_CUDA(h, cudaStreamCreate(&h->own));
+    *out = h->own;
+    return PM_OK;
+}
+
+uint64_t fbits(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return u;
+}
+
+// Run `body(cs)` as a CUDA graph on `st`: captured on the handle's own stream `cs` the first
+// time, replayed while `key` (every argument the captured work depends on) is unchanged.
+template <class Fn>
+int run_graph(pm_handle* h, std::vector<uint64_t>& cached, cudaGraphExec_t& exec, const std::vector<uint64_t>& key,
+              cudaStream_t st, Fn body)
+{
+    if (!(exec && cached == key)) {
+        if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+        cached.clear();
+        cudaStream_t cs;
+        int rc = own_stream(h, &cs);
+        if (rc) return rc;
+        PM_CUDA(h, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        h->capturing = 1;
+        rc = body(cs);
+        h->capturing = 0;
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(cs, &g);
+        if (rc) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return rc; }
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+        const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) { exec = nullptr; return cuda_fail(h, ei, "cudaGraphInstantiate"); }
+        cached = key;
+    }
+    PM_CUDA(h, cudaGraphLaunch(exec, st));
+    return PM_OK;
+}
+
+// graphs are used unless disabled, while profiling (per-phase events need eager launches),
+// or when the caller is itself capturing `st` (the launches then go into the caller's graph)
+int use_graph(pm_handle* h, cudaStream_t st, bool* yes)
+{
+    *yes = false;
+    if (!h->opt.use_graph || h->profiling) return PM_OK;
+    if (st) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        PM_CUDA(h, cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return PM_OK;
+    }
+    *yes = true;
+    return PM_OK;
+}
+
+// the single-pair pipeline on `st`, through the handle's graph when graphs are in use
+int pipeline_on(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int r,
+                float dmax, int iterations, int pp, float* dmap, float4* normal, const float* initdisp,
+                const float4* initnormal, float4* planesL, float4* planesR, cudaStream_t st)
+{
+    bool graph = false;
+    int rc = use_graph(h, st, &graph);
+    if (rc) return rc;
+    if (!graph)
+        return run_pipeline(h, ws, left, right, W, H, stride, r, dmax, iterations, pp, dmap, normal, initdisp,
+                            initnormal, planesL, planesR, st);
+    const pm_options& o = h->opt;
+    const std::vector<uint64_t> key = {
+        (uint64_t)(uintptr_t)ws, (uint64_t)(uintptr_t)left, (uint64_t)(uintptr_t)right, (uint64_t)W, (uint64_t)H,
+        (uint64_t)stride, (uint64_t)r, fbits(dmax), (uint64_t)iterations, (uint64_t)pp, (uint64_t)(uintptr_t)dmap,
+        (uint64_t)(uintptr_t)normal, (uint64_t)(uintptr_t)initdisp, (uint64_t)(uintptr_t)initnormal,
+        (uint64_t)(uintptr_t)planesL, (uint64_t)(uintptr_t)planesR, (uint64_t)o.views, (uint64_t)o.fused,
+        fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff), (uint64_t)o.rof_iters, (uint64_t)h->counting};
+    return run_graph(h, h->key1, h->exec1, key, st, [&](cudaStream_t cs) {
+        return run_pipeline(h, ws, left, right, W, H, stride, r, dmax, iterations, pp, dmap, normal, initdisp,
+                            initnormal, planesL, planesR, cs);
+    });
+}
+
 }  // namespace
 
 extern "C" {
@@ -420,6 +519,13 @@ int pm_destroy(pm_handle* h)
     if (!h) return PM_OK;
     if (h->ws) cudaFree(h->ws);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+    if (h->exec1) cudaGraphExecDestroy(h->exec1);
+    if (h->execb) cudaGraphExecDestroy(h->execb);
+    for (void* p : h->bws)
+        if (p) cudaFree(p);
+    for (cudaStream_t b : h->branch) cudaStreamDestroy(b);
+    for (cudaEvent_t e : h->bev) cudaEventDestroy(e);
+    if (h->own) cudaStreamDestroy(h->own);
     delete h;
     return PM_OK;
 }
@@ -503,9 +609,11 @@ int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* ri
     PM_CUDA(h, cudaSetDevice(h->opt.device));
     h->W = W;
     h->H = H;
-    rc = run_pipeline(h, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap,
-                      reinterpret_cast<float4*>(normalmap), initdisp, reinterpret_cast<const float4*>(initnormal),
-                      reinterpret_cast<float4*>(planes_left), reinterpret_cast<float4*>(planes_right), S(stream));
+    rc = ensure_ws(h, W, H, stride);
+    if (rc) return rc;
+    rc = pipeline_on(h, h->ws, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap,
+                     reinterpret_cast<float4*>(normalmap), initdisp, reinterpret_cast<const float4*>(initnormal),
+                     reinterpret_cast<float4*>(planes_left), reinterpret_cast<float4*>(planes_right), S(stream));
     if (rc) return rc;
     if (h->counting) {
         const Layout L = layout(W, H, stride);
@@ -543,8 +651,8 @@ int pm_disparity_map(pm_handle* h, const uint8_t* left, const uint8_t* right, in
     if (initdisp) PM_CUDA(h, cudaMemcpyAsync(di, initdisp, N * 4, cudaMemcpyHostToDevice, st));
     if (initnormal) PM_CUDA(h, cudaMemcpyAsync(dni, initnormal, N * 16, cudaMemcpyHostToDevice, st));
     (void)pl;
-    rc = run_pipeline(h, dl, dr, W, H, stride, patchsize, dispmax, iterations, pp, dmap ? dd : nullptr,
-                      normalmap ? dn : nullptr, initdisp ? di : nullptr, initnormal ? dni : nullptr, nullptr, nullptr, st);
+    rc = pipeline_on(h, h->ws, dl, dr, W, H, stride, patchsize, dispmax, iterations, pp, dmap ? dd : nullptr,
+                     normalmap ? dn : nullptr, initdisp ? di : nullptr, initnormal ? dni : nullptr, nullptr, nullptr, st);
     if (rc) return rc;
     if (dmap) PM_CUDA(h, cudaMemcpyAsync(dmap, dd, N * 4, cudaMemcpyDeviceToHost, st));
     if (normalmap) PM_CUDA(h, cudaMemcpyAsync(normalmap, dn, N * 16, cudaMemcpyDeviceToHost, st));
@@ -569,9 +677,94 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
                                   const float* dispmax, int iterations, int pp, float* const* dmap,
                                   float* const* planes_left, float* const* planes_right, void* stream)
 {
-    (void)n; (void)left; (void)right; (void)width; (void)height; (void)stride; (void)patchsize; (void)dispmax;
-    (void)iterations; (void)pp; (void)dmap; (void)planes_left; (void)planes_right; (void)stream;
-    return fail(h, PM_ENOTIMPL, "batched form not built yet");
+    if (!h) return fail(h, PM_EINVAL_ARG, "null handle");
+    if (n < 0 || n > PM_MAX_BATCH) return fail(h, PM_EINVAL_ARG, "batch size out of range");
+    if (n == 0) return PM_OK;
+    if (!left || !right || !width || !height || !stride || !patchsize || !dispmax)
+        return fail(h, PM_EINVAL_ARG, "null per-pair array");
+    for (int i = 0; i < n; i++) {
+        const int rc = check_args(h, left[i], right[i], width[i], height[i], stride[i], patchsize[i], dispmax[i],
+                                  iterations, pp);
+        if (rc) return rc;
+    }
+    PM_CUDA(h, cudaSetDevice(h->opt.device));
+    // one workspace per pair
+    if ((int)h->bws.size() < n) { h->bws.resize(n, nullptr); h->bws_bytes.resize(n, 0); }
+    for (int i = 0; i < n; i++) {
+        const int rc = grow(h, h->bws[i], h->bws_bytes[i], layout(width[i], height[i], stride[i]).total);
+        if (rc) return rc;
+    }
+    // pairs in decreasing window work, each to the least loaded branch (longest processing
+    // time first); the branches run concurrently inside one graph
+    const int nb = n < PM_BATCH_BRANCHES ? n : PM_BATCH_BRANCHES;
+    while ((int)h->branch.size() < nb) {
+        cudaStream_t b;
+        PM_CUDA(h, cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+        h->branch.push_back(b);
+    }
+    while ((int)h->bev.size() < nb + 1) {
+        cudaEvent_t e;
+        PM_CUDA(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h->bev.push_back(e);
+    }
+    std::vector<int> order(n), owner(n);
+    std::vector<double> work(n), load(nb, 0.0);
+    for (int i = 0; i < n; i++) {
+        order[i] = i;
+        work[i] = (double)width[i] * height[i] * (2.0 * patchsize[i] + 1.0) * (2.0 * patchsize[i] + 1.0);
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+    for (int i : order) {
+        int best = 0;
+        for (int b = 1; b < nb; b++)
+            if (load[b] < load[best]) best = b;
+        owner[i] = best;
+        load[best] += work[i];
+    }
+    auto body = [&](cudaStream_t cs) -> int {
+        PM_CUDA(h, cudaEventRecord(h->bev[nb], cs));
+        for (int b = 0; b < nb; b++) PM_CUDA(h, cudaStreamWaitEvent(h->branch[b], h->bev[nb], 0));
+        for (int i : order) {
+            const int rc = run_pipeline(h, h->bws[i], left[i], right[i], width[i], height[i], stride[i], patchsize[i],
+                                        dispmax[i], iterations, pp, dmap ? dmap[i] : nullptr, nullptr, nullptr,
+                                        nullptr, planes_left ? reinterpret_cast<float4*>(planes_left[i]) : nullptr,
+                                        planes_right ? reinterpret_cast<float4*>(planes_right[i]) : nullptr,
+                                        h->branch[owner[i]]);
+            if (rc) return rc;
+        }
+        for (int b = 0; b < nb; b++) {
+            PM_CUDA(h, cudaEventRecord(h->bev[b], h->branch[b]));
+            PM_CUDA(h, cudaStreamWaitEvent(cs, h->bev[b], 0));
+        }
+        return PM_OK;
+    };
+    const cudaStream_t st = S(stream);
+    bool graph = false;
+    int rc = use_graph(h, st, &graph);
+    if (rc) return rc;
+    const int saved = h->profiling;
+    h->profiling = 0;   // per-phase timing covers single-pair calls only
+    if (!graph) {
+        // eager: the same fork / join on the caller's stream
+        rc = body(st);
+        h->profiling = saved;
+        return rc;
+    }
+    const pm_options& o = h->opt;
+    std::vector<uint64_t> key = {(uint64_t)n, (uint64_t)iterations, (uint64_t)pp, (uint64_t)o.views, (uint64_t)o.fused,
+                                 fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff), (uint64_t)o.rof_iters,
+                                 (uint64_t)h->counting};
+    for (int i = 0; i < n; i++) {
+        const uint64_t v[] = {(uint64_t)(uintptr_t)h->bws[i], (uint64_t)(uintptr_t)left[i], (uint64_t)(uintptr_t)right[i],
+                              (uint64_t)width[i], (uint64_t)height[i], (uint64_t)stride[i], (uint64_t)patchsize[i],
+                              fbits(dispmax[i]), (uint64_t)(uintptr_t)(dmap ? dmap[i] : nullptr),
+                              (uint64_t)(uintptr_t)(planes_left ? planes_left[i] : nullptr),
+                              (uint64_t)(uintptr_t)(planes_right ? planes_right[i] : nullptr)};
+        key.insert(key.end(), v, v + 11);
+    }
+    rc = run_graph(h, h->keyb, h->execb, key, st, body);
+    h->profiling = saved;
+    return rc;
 }
 
 // ---- per-kernel entry points ------------------------------------------------------------

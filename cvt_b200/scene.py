@@ -36,3 +36,25 @@ def workload(name, seed=0):
     if name == "hd":
         return generate(seed, 1280, 720, 40, 2.0, 120.0)
     raise ValueError(name)
+
+
+def batch_specs(n=64, seed=1234, wmin=320, wmax=1920, hmin=240, hmax=1080):
+    """Pair specifications of the uneven batched workload: width and height uniform in
+    [wmin, wmax] x [hmin, hmax], 8-60 planes, disparity range 0..max(32, width / 10)
+    (scene disparities 2..0.9 of that range).  Pair i is generated with seed + i.
+    Returns a list of dicts {seed, width, height, planes, dispmax, dlo, dhi}."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        w = int(rng.integers(wmin, wmax + 1))
+        h = int(rng.integers(hmin, hmax + 1))
+        npl = int(rng.integers(8, 61))
+        dmax = float(max(32, w // 10))
+        out.append({"seed": seed + i, "width": w, "height": h, "planes": npl, "dispmax": dmax, "dlo": 2.0,
+                    "dhi": 0.9 * dmax})
+    return out
+
+
+def batch(specs):
+    """(left, right) arrays for each spec of batch_specs."""
+    return [generate(s["seed"], s["width"], s["height"], s["planes"], s["dlo"], s["dhi"]) for s in specs]

@@ -108,6 +108,43 @@ class PMHuberStereo:
             out["planes_left"], out["planes_right"] = pl, pr
         return out
 
+    def disparity_map_batch(self, lefts, rights, patchsizes, disparitymaxs, iterations, pp=PP_LRCHECK, planes=False,
+                            stream=None):
+        """n pairs of CUDA uint8 tensors (H_i, W_i, 4), each with its own patch size and disparity
+        range, run as one graph launch (pm_disparity_map_batch_device).  Returns a list of
+        dmaps, or of dicts {dmap, planes_left, planes_right} when planes is requested."""
+        import torch
+
+        L = _lib.lib()
+        n = len(lefts)
+        if len(rights) != n or len(patchsizes) != n or len(disparitymaxs) != n:
+            raise StereoError(_lib.PM_EINVAL_ARG, "per-pair lists differ in length")
+        ls, rs, outs = [], [], []
+        for a, b in zip(lefts, rights):
+            if a.shape != b.shape or a.dim() != 3 or a.shape[2] != 4 or a.dtype != torch.uint8 or not a.is_cuda:
+                raise StereoError(_lib.PM_EINVAL_SHAPE, "Left/Right stereo images inconsistent")
+            ls.append(a.contiguous())
+            rs.append(b.contiguous())
+        dm = [torch.empty(a.shape[:2], dtype=torch.float32, device=a.device) for a in ls]
+        pl = [torch.empty(a.shape, dtype=torch.float32, device=a.device) for a in ls] if planes else None
+        pr = [torch.empty(a.shape, dtype=torch.float32, device=a.device) for a in ls] if planes else None
+
+        def arr(ctype, vals):
+            return (ctype * max(n, 1))(*vals)
+
+        st = stream if stream is not None else torch.cuda.current_stream(ls[0].device if n else None).cuda_stream
+        ptr = C.c_void_p
+        _lib.check(L.pm_disparity_map_batch_device(
+            self._h, n, arr(ptr, [t.data_ptr() for t in ls]), arr(ptr, [t.data_ptr() for t in rs]),
+            arr(C.c_int, [t.shape[1] for t in ls]), arr(C.c_int, [t.shape[0] for t in ls]),
+            arr(C.c_size_t, [t.shape[1] * 4 for t in ls]), arr(C.c_int, [int(r) for r in patchsizes]),
+            arr(C.c_float, [float(d) for d in disparitymaxs]), int(iterations), int(pp),
+            arr(ptr, [t.data_ptr() for t in dm]), arr(ptr, [t.data_ptr() for t in pl]) if planes else None,
+            arr(ptr, [t.data_ptr() for t in pr]) if planes else None, st), self._h)
+        if not planes:
+            return dm
+        return [{"dmap": d, "planes_left": a, "planes_right": b} for d, a, b in zip(dm, pl, pr)]
+
     def _device(self, left, right, patchsize, dmax, iterations, pp, normalmap, initd, initn, planes, stream):
         import torch
 

@@ -61,7 +61,8 @@ typedef struct pm_options {
     float maxanglediff;  /* 5.0 degrees (PMHuberStereo.cpp:80) */
     int rof_iters;       /* 40 (PMHuberStereo.cpp:427) */
     int device;          /* CUDA device ordinal, default 0 */
-    int use_graph;       /* 1 (default): replay the iteration schedule as one CUDA graph */
+    int use_graph;       /* 1 (default): run each call as a CUDA graph, captured once and replayed while the
+                            call's arguments are unchanged; 0: launch eagerly */
 } pm_options;
 
 typedef struct pm_handle pm_handle;
@@ -109,8 +110,16 @@ int pm_get_phase_times(pm_handle* h, float ms[6], int launches[6]);
 int pm_measure_fp32_peak(int device, float ms, float* tflops);
 
 /* Batched form: n independent pairs, each with its own size, patch size and
- * disparity range, processed together (one launch per stage for all pairs).
- * Arrays are indexed by pair; device pointers; outputs as in pm_disparity_map_device. */
+ * disparity range, enqueued on `stream` as one CUDA graph launch.  Each pair's pipeline
+ * is a branch of the graph; pairs go longest-first (by W*H*window) to the least loaded of
+ * up to PM_BATCH_BRANCHES concurrent branches, so small pairs fill the GPU beside large
+ * ones.  The graph is captured on the first call and replayed while every argument is the
+ * same.  Arrays are indexed by pair; device pointers; outputs as in
+ * pm_disparity_map_device (dmap, planes_left, planes_right may be NULL, or hold NULL
+ * entries).  Results equal n calls of pm_disparity_map_device.  Every pair has its own
+ * workspace, kept by the handle for the next call.  Counting and phase timing apply
+ * to single-pair calls only. */
+enum { PM_MAX_BATCH = 4096, PM_BATCH_BRANCHES = 16 };
 int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* left, const uint8_t* const* right,
                                   const int* width, const int* height, const size_t* stride,
                                   const int* patchsize, const float* dispmax, int iterations, int pp,

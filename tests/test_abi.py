@@ -131,3 +131,24 @@ def test_cpp_drop_in_header_compiles_and_fails_loudly(native, tmp_path):
     if not torch.cuda.is_available():
         p = subprocess.run([exe, str(tmp_path / "d.raw")], capture_output=True, text=True)
         assert p.returncode == 1 and "no CUDA device" in p.stderr
+
+
+def test_batch_specs_seeded_and_in_range():
+    from cvt_b200 import scene
+
+    a, b = scene.batch_specs(), scene.batch_specs()
+    assert a == b and len(a) == 64
+    for i, s in enumerate(a):
+        assert s["seed"] == 1234 + i
+        assert 320 <= s["width"] <= 1920 and 240 <= s["height"] <= 1080
+        assert 8 <= s["planes"] <= 60
+        assert s["dispmax"] == max(32, s["width"] // 10)
+    assert len({(s["width"], s["height"]) for s in a}) > 60
+
+
+def test_batch_null_handle(native):
+    from cvt_b200 import _lib
+
+    # argument checks come before any device work
+    assert native.pm_disparity_map_batch_device(None, 1, None, None, None, None, None, None, None, 3, 1,
+                                                None, None, None, None) == _lib.PM_EINVAL_ARG

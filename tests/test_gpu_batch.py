@@ -1,0 +1,81 @@
+"""Batched pairs of uneven sizes in one graph launch (pm_disparity_map_batch_device) and the
+graph replay of single-pair calls, against eager single-pair calls through the C ABI.
+
+All three run the same kernels on the same inputs, so the results must be bit-identical
+(tolerance 0); the single-pair device path itself is pinned to the oracle in
+test_gpu_parity.py.
+"""
+import numpy as np
+import pytest
+
+from oracle.pyoracle import bits_equal
+
+pytestmark = pytest.mark.gpu
+
+# (width, height, patch half-width, disparity range, planes)
+PAIRS = [(72, 40, 3, 16.0, 5), (40, 56, 2, 12.0, 4), (96, 33, 4, 24.0, 6), (33, 17, 1, 8.0, 3)]
+
+
+@pytest.fixture(scope="module")
+def torch_cuda(native):
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+def _pairs(torch):
+    from cvt_b200 import scene
+
+    out = []
+    for i, (w, h, r, d, npl) in enumerate(PAIRS):
+        L, R = scene.generate(100 + i, w, h, npl, 1.0, 0.9 * d)
+        out.append((torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda(), r, d))
+    return out
+
+
+def _host(t):
+    return t.cpu().numpy()
+
+
+def test_batch_equals_single_pair_calls(torch_cuda):
+    from cvt_b200 import PMHuberStereo
+
+    pairs = _pairs(torch_cuda)
+    eager = PMHuberStereo(views=2, fused=True, use_graph=False)
+    ref = [eager.disparity_map(a, b, r, d, 3, planes=True) for a, b, r, d in pairs]
+    pm = PMHuberStereo(views=2, fused=True)
+    for rep in range(2):   # capture, then replay
+        out = pm.disparity_map_batch([p[0] for p in pairs], [p[1] for p in pairs], [p[2] for p in pairs],
+                                     [p[3] for p in pairs], 3, planes=True)
+        torch_cuda.cuda.synchronize()
+        for o, e in zip(out, ref):
+            for k in ("dmap", "planes_left", "planes_right"):
+                assert bits_equal(_host(o[k]), _host(e[k])).all(), (rep, k)
+
+
+def test_graph_replay_equals_eager(torch_cuda):
+    from cvt_b200 import PMHuberStereo
+
+    a, b, r, d = _pairs(torch_cuda)[0]
+    eager = PMHuberStereo(views=2, fused=True, use_graph=False)
+    e = eager.disparity_map(a, b, r, d, 3, planes=True)
+    pm = PMHuberStereo(views=2, fused=True)
+    for rep in range(3):
+        o = pm.disparity_map(a, b, r, d, 3, planes=True)
+        torch_cuda.cuda.synchronize()
+        for k in ("dmap", "planes_left", "planes_right"):
+            assert bits_equal(_host(o[k]), _host(e[k])).all(), (rep, k)
+    # host entry (legacy default stream) through the graph as well
+    h = pm.disparity_map(_host(a), _host(b), r, d, 3)
+    assert bits_equal(h, _host(e["dmap"])).all()
+
+
+def test_batch_rejects_bad_pair(torch_cuda):
+    from cvt_b200 import PMHuberStereo, StereoError
+
+    pairs = _pairs(torch_cuda)
+    pm = PMHuberStereo(views=2)
+    with pytest.raises(StereoError):
+        pm.disparity_map_batch([pairs[0][0], pairs[1][0]], [pairs[0][1], pairs[1][1]], [3, 99], [16.0, 12.0], 3)
+    assert pm.disparity_map_batch([], [], [], [], 3) == []
