@@ -100,6 +100,29 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def max_over_ranks(ms, world):
+    """Maximum over ranks of a per-rank elapsed time in ms (one all-reduce, made outside the
+    timed region; the tensor lives where the process group's backend wants it)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def pair_seed(rank):
+    """scene seed of a rank's pair: every rank works on its own pair"""
+    return rank
+
+
+def batch_seed(rank):
+    return 1234 + 1000 * rank
+
+
 def window_positions(W, H, r):
     """sum over pixels of in-image window positions (the support weights computed once per pixel)"""
     def axis(n):
@@ -180,7 +203,7 @@ def run_batch(args, rank, world, local):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    specs = scene.batch_specs(seed=1234 + 1000 * rank)
+    specs = scene.batch_specs(seed=batch_seed(rank))
     pairs = scene.batch(specs)
     dl = [torch.from_numpy(a).cuda() for a, _ in pairs]
     dr = [torch.from_numpy(b).cuda() for _, b in pairs]
@@ -201,10 +224,7 @@ def run_batch(args, rank, world, local):
             fn()
             ev[k][1].record()
         torch.cuda.synchronize()
-        t = torch.tensor([sum(a.elapsed_time(b) for a, b in ev)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world)
 
     def batched():
         pm.disparity_map_batch(dl, dr, rs, dm, iters, pp=1)
@@ -271,7 +291,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
-    L, R = scene.generate(rank, W, H, npl, dlo, dhi)
+    L, R = scene.generate(pair_seed(rank), W, H, npl, dlo, dhi)
     dL, dR = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
     pm = PMHuberStereo(views=views, fused=True, device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -310,10 +330,7 @@ def main():
         dist.barrier()
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    total = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(total, op=dist.ReduceOp.MAX)
-    total_ms = float(total.item())
+    total_ms = max_over_ranks(sum(step_ms), world)
     px_it = W * H * executed(iters)
     value = world * px_it * args.steps / (total_ms * 1e-3) / 1e6
 
@@ -340,10 +357,7 @@ def main():
         b.record()
         torch.cuda.synchronize()
         e2e.append(a.elapsed_time(b))
-    e2e_t = torch.tensor([sum(e2e)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * px_it * args.steps / (float(e2e_t.item()) * 1e-3) / 1e6
+    e2e_value = world * px_it * args.steps / (max_over_ranks(sum(e2e), world) * 1e-3) / 1e6
 
     # roofline of the propagate kernel (FP32-bound): algorithmic flops per launch
     # = 10 per hoisted support weight + 41 per cost-window sample + 129 per
