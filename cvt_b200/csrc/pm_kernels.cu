@@ -316,7 +316,8 @@ __global__ void k_disparity_to_normal(float4* __restrict__ out, const float* __r
 }
 
 // texel planes of one view (pm_window.cuh): column c in [-2, W+1] of the colour plane
-// holds bw, of the gradient plane grad, both of column clamp(c, 0, W-1)
+// holds bw, of the gradient plane grad, of the compact plane (bw.rgb, gradient sign
+// bytes), all of column clamp(c, 0, W-1)
 __global__ void k_pack_tex(float4* __restrict__ tex, const float4* __restrict__ bw, const float4* __restrict__ grad,
                            int W, int H, int P)
 {
@@ -324,8 +325,10 @@ __global__ void k_pack_tex(float4* __restrict__ tex, const float4* __restrict__ 
     if (c > W + TEX_PAD - 1 || y >= H) return;
     const int s = min(max(c, 0), W - 1);
     const size_t o = (size_t)y * P + c + TEX_PAD;
-    tex[o] = bw[(size_t)y * W + s];
-    tex[(size_t)H * P + o] = grad[(size_t)y * W + s];
+    const float4 col = bw[(size_t)y * W + s], g = grad[(size_t)y * W + s];
+    tex[o] = col;
+    tex[(size_t)H * P + o] = g;
+    tex[(size_t)2 * H * P + o] = make_float4(col.x, col.y, col.z, __uint_as_float(sign_bytes(g)));
 }
 
 __global__ void k_view_clear(int* __restrict__ count, unsigned long long* __restrict__ src, size_t n)
@@ -461,7 +464,7 @@ void launch_disparity_to_normal(float4* out, const float* d, int W, int H, cudaS
 }
 
 int tex_pitch(int W) { return W + 2 * TEX_PAD; }
-size_t tex_bytes(int W, int H) { return (size_t)tex_pitch(W) * H * 2 * sizeof(float4); }
+size_t tex_bytes(int W, int H) { return (size_t)tex_pitch(W) * H * 3 * sizeof(float4); }
 
 void launch_pack_tex(float4* tex, const float4* bw, const float4* grad, int W, int H, cudaStream_t st)
 {

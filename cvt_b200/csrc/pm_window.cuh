@@ -3,13 +3,17 @@
 // (patch_census_klt2, :326-410), one thread per pixel, samples in the
 // reference's order.
 //
-// Texel layout.  Each view is stored as two planes of float4, colour (r, g, b, Σw)
-// and gradient (4 components), the gradient plane `plane` float4 after the
-// colour plane, in rows of W + 4 texels: columns -2 .. W+1, the four outside
-// ones replicating the edge texel (CLK_ADDRESS_CLAMP_TO_EDGE).  A bilinear tap
-// pair therefore needs no clamping inside that range, all loads of a sample
-// come from one index, and the lanes of a warp gathering neighbouring texels
-// read 16-byte strided addresses.
+// Texel layout.  Each view is stored as three planes of float4 in rows of W + 4
+// texels: columns -2 .. W+1, the four outside ones replicating the edge texel
+// (CLK_ADDRESS_CLAMP_TO_EDGE).  Colour (r, g, b, Σw) and gradient (4 components),
+// the gradient plane `plane` float4 after the colour plane, serve the second
+// view's bilinear taps and the first view's centre texel: a tap pair needs no
+// clamping inside the padded range, all loads of a tap come from one index, and
+// the lanes of a warp gathering neighbouring texels read 16-byte strided
+// addresses.  The compact plane (r, g, b, the four gradient sign bits as bytes),
+// `plane` float4 after the gradient plane, holds all that a first-view window
+// sample needs, in one load.  (Interleaved 32-byte texels read with 256-bit
+// loads measured slower for the Gauss-Newton taps.)
 //
 // Blackwell specifics: the 7-channel bilinear reads of the second view and the
 // truncated absolute differences run as packed FP32 pairs (FFMA2 / FMUL2,
@@ -27,12 +31,13 @@ namespace pm {
 constexpr int TEX_PAD = 2;   // replicated columns on each side of a texel row
 
 struct ViewData {
-    const float4* __restrict__ t1;   // first view: colour plane, gradient plane at + plane
+    const float4* __restrict__ t1;   // first view: colour plane, gradient plane at + plane, compact at + 2 plane
     const float4* __restrict__ t2;   // second view
     int W, H, r, P;                  // P = W + 2 * TEX_PAD texels per row
     int plane;                       // H * P
-    // colour texel column 0 of row y
+    // colour texel (compact texel) of column 0 of row y
     __device__ __forceinline__ const float4* row1(int y) const { return t1 + (size_t)y * P + TEX_PAD; }
+    __device__ __forceinline__ const float4* row1c(int y) const { return t1 + 2 * (size_t)plane + (size_t)y * P + TEX_PAD; }
     __device__ __forceinline__ const float4* row2(int y) const { return t2 + (size_t)y * P + TEX_PAD; }
 };
 
@@ -185,8 +190,8 @@ __device__ __forceinline__ bool eval_sample(const float4* __restrict__ q1, const
 {
     const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
     if (p2x < 0 || p2x >= fW) return false;
-    const Texel q = texel_at(q1, plane);
-    const float w = support_weight<F>(q.c.x - in.x, q.c.y - in.y, q.c.z - in.z);
+    const float4 q = __ldg(q1);   // compact texel
+    const float w = support_weight<F>(q.x - in.x, q.y - in.y, q.z - in.z);
     const float t = (p2x + 0.5f) - 0.5f;
     Texel tx;
     if (fin(t)) {
@@ -198,9 +203,9 @@ __device__ __forceinline__ bool eval_sample(const float4* __restrict__ q1, const
     } else {
         tx = lerp_texel_at<F>(row2, plane, W, p2x + 0.5f);
     }
-    float cost = PM_K033_8 * ad_sum(tx.c, q.c);
+    float cost = PM_K033_8 * ad_sum(tx.c, q);
     // cost + 0.875f * (0.25f * n): the product 0.21875 n is exact, so one fma rounds the same
-    cost = fmaf(0.21875f, (float)sign_mismatch(sign_bytes(q.g), sign_bytes(tx.g)), cost);
+    cost = fmaf(0.21875f, (float)sign_mismatch(__float_as_uint(q.w), sign_bytes(tx.g)), cost);
     census = F ? fmaf(w, cost, census) : census + w * cost;
     wsum += w;
     return true;
@@ -236,7 +241,7 @@ __device__ __forceinline__ float patch_eval(const ViewData& V, int px, int py, f
     float qy = cy + (float)dy0;
     for (int iy = py + dy0; iy <= py + dy1; iy++, qy += 1.0f) {
         const float byq = s.y * qy;
-        const float4* __restrict__ q1 = V.row1(iy) + px + dx0;
+        const float4* __restrict__ q1 = V.row1c(iy) + px + dx0;
         const float4* __restrict__ row2 = V.row2(iy);
         float qx = qx0;
         for (int n = dx1 - dx0; n >= 0; n--, q1++, qx += 1.0f) {
@@ -272,14 +277,14 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
     for (int iy = py + dy0; iy <= py + dy1; iy++, qy += 1.0f) {
         const float byq = s.y * qy;
         const float yy = qy * qy;
-        const float4* __restrict__ q1 = V.row1(iy) + px + dx0;
+        const float4* __restrict__ q1 = V.row1c(iy) + px + dx0;
         const float4* __restrict__ row2 = V.row2(iy);
         float qx = qx0;
         for (int n = dx1 - dx0; n >= 0; n--, q1++, qx += 1.0f) {
-            const Texel q = texel_at(q1, plane);
-            const float4 val1 = make_float4(q.c.x - c1.x, q.c.y - c1.y, q.c.z - c1.z, 0.0f);
+            const float4 q = __ldg(q1);   // compact texel
+            const float4 val1 = make_float4(q.x - c1.x, q.y - c1.y, q.z - c1.z, 0.0f);
             const float w1 = support_weight<F>(val1.x, val1.y, val1.z);
-            const uint32_t sb1 = sign_bytes(q.g);
+            const uint32_t sb1 = __float_as_uint(q.w);
             const float k1 = w1 * PM_K033_8;
             const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
             // Common case: 1 <= p2x < W - 1 and p2x + 1.5 in the binade of p2x.  Then p2x is a
