@@ -259,8 +259,11 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
     const ViewData VL = make_view(texL, texR, W, H, r);
     const ViewData VR = make_view(texR, texL, W, H, r);
     launch_init(mL[0], VL, dmax, 1, initdisp, initn, F, st);
-    nl++;
-    if (views == 2) { launch_init(mR[0], VR, dmax, 0, nullptr, nullptr, F, st); nl++; }
+    nl += window_kernel_launches(F, false);
+    if (views == 2) {
+        launch_init(mR[0], VR, dmax, 0, nullptr, nullptr, F, st);
+        nl += window_kernel_launches(F, false);
+    }
     const float thetamin = o.thetamin;
     float theta = thetamin;
     const int rof_launches = (o.rof_iters > 0 && o.rof_iters % 2 == 0) ? o.rof_iters : o.rof_iters + 1;
@@ -307,7 +310,7 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
             P.vout_src = vb2s;
             launch_propagate(P, F, st);   // :542-543
         }
-        prof_mark(h, st, PM_PHASE_PROPAGATE, 3 * views);   // three kernels per view (pm_propagate.cu)
+        prof_mark(h, st, PM_PHASE_PROPAGATE, 3 * window_kernel_launches(F, h->counting) * views);
         launch_normal_depth(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :552-553
         launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
         if (views == 2) {

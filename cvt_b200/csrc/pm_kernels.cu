@@ -76,10 +76,11 @@ __global__ void k_prep(const uint8_t* __restrict__ img, size_t stride, int W, in
     }
 }
 
-template <bool F>
+template <bool F, bool CHK>
 __global__ void k_init(float4* __restrict__ out, ViewData V, float dmax, int lr, const float* __restrict__ initdisp,
-                       const float4* __restrict__ initnormal)
+                       const float4* __restrict__ initnormal, int dual)
 {
+    if (variant_skips<CHK>(V, dual)) return;
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= V.W || y >= V.H) return;
     const size_t i = (size_t)y * V.W + x;
@@ -98,28 +99,31 @@ __global__ void k_init(float4* __restrict__ out, ViewData V, float dmax, int lr,
         ret = nd_state_init(rng, cx, cy, lr, dmax);
     }
     Counters cnt = {0, 0, 0, 0};
-    ret.w = patch_eval<F, false>(V, x, y, ret, 1e10f, cnt);
+    ret.w = patch_eval<F, false, CHK>(V, x, y, ret, 1e10f, cnt);
     out[i] = ret;
 }
 
-template <bool F>
-__global__ void k_cost(float* __restrict__ cost, const float4* __restrict__ planes, ViewData V, float mincost)
+template <bool F, bool CHK>
+__global__ void k_cost(float* __restrict__ cost, const float4* __restrict__ planes, ViewData V, float mincost,
+                       int dual)
 {
+    if (variant_skips<CHK>(V, dual)) return;
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= V.W || y >= V.H) return;
     const size_t i = (size_t)y * V.W + x;
     Counters cnt = {0, 0, 0, 0};
-    cost[i] = patch_eval<F, false>(V, x, y, planes[i], mincost, cnt);
+    cost[i] = patch_eval<F, false, CHK>(V, x, y, planes[i], mincost, cnt);
 }
 
-template <bool F>
-__global__ void k_klt(float4* __restrict__ out, const float4* __restrict__ planes, ViewData V)
+template <bool F, bool CHK>
+__global__ void k_klt(float4* __restrict__ out, const float4* __restrict__ planes, ViewData V, int dual)
 {
+    if (variant_skips<CHK>(V, dual)) return;
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= V.W || y >= V.H) return;
     const size_t i = (size_t)y * V.W + x;
     Counters cnt = {0, 0, 0, 0};
-    out[i] = klt2<F, false>(V, x, y, planes[i], cnt);
+    out[i] = klt2<F, false, CHK>(V, x, y, planes[i], cnt);
 }
 
 __global__ void k_normal_depth(float4* __restrict__ out, const float4* __restrict__ planes, int W, int H,
@@ -317,6 +321,10 @@ __global__ void k_disparity_to_normal(float4* __restrict__ out, const float* __r
 
 // texel planes of one view (pm_window.cuh): column c in [-2, W+1] of the colour plane
 // holds bw, of the gradient plane grad, of the compact plane (bw.rgb, gradient sign
+// a finite nonzero colour value below 2^-40 in magnitude (the window loops then need the
+// exact-division fallback of ad_sum)
+__device__ __forceinline__ bool tiny_colour(float v) { return v != 0.0f && fabsf(v) < 0x1p-40f; }
+
 // bytes), all of column clamp(c, 0, W-1)
 __global__ void k_pack_tex(float4* __restrict__ tex, const float4* __restrict__ bw, const float4* __restrict__ grad,
                            int W, int H, int P)
@@ -329,6 +337,8 @@ __global__ void k_pack_tex(float4* __restrict__ tex, const float4* __restrict__ 
     tex[o] = col;
     tex[(size_t)H * P + o] = g;
     tex[(size_t)2 * H * P + o] = make_float4(col.x, col.y, col.z, __uint_as_float(sign_bytes(g)));
+    if (c == s && (tiny_colour(col.x) || tiny_colour(col.y) || tiny_colour(col.z)))
+        atomicOr(reinterpret_cast<int*>(tex + (size_t)3 * H * P), 1);
 }
 
 __global__ void k_view_clear(int* __restrict__ count, unsigned long long* __restrict__ src, size_t n)
@@ -386,22 +396,37 @@ void launch_init(float4* out, const ViewData& V, float dmax, int lr, const float
                  int fused, cudaStream_t st)
 {
     const dim3 b(32, 4);
-    if (fused) k_init<true><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal);
-    else k_init<false><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal);
+    const dim3 g = grid2d(V.W, V.H, b);
+    if (fused) {   // both variants; the one that does not apply returns at once (pm_window.cuh)
+        k_init<true, false><<<g, b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal, 1);
+        k_init<true, true><<<g, b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal, 1);
+    } else {
+        k_init<false, true><<<g, b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal, 0);
+    }
 }
 
 void launch_cost(float* cost, const float4* planes, const ViewData& V, float mincost, int fused, cudaStream_t st)
 {
     const dim3 b(32, 4);
-    if (fused) k_cost<true><<<grid2d(V.W, V.H, b), b, 0, st>>>(cost, planes, V, mincost);
-    else k_cost<false><<<grid2d(V.W, V.H, b), b, 0, st>>>(cost, planes, V, mincost);
+    const dim3 g = grid2d(V.W, V.H, b);
+    if (fused) {
+        k_cost<true, false><<<g, b, 0, st>>>(cost, planes, V, mincost, 1);
+        k_cost<true, true><<<g, b, 0, st>>>(cost, planes, V, mincost, 1);
+    } else {
+        k_cost<false, true><<<g, b, 0, st>>>(cost, planes, V, mincost, 0);
+    }
 }
 
 void launch_klt(float4* out, const float4* planes, const ViewData& V, int fused, cudaStream_t st)
 {
     const dim3 b(32, 4);
-    if (fused) k_klt<true><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, planes, V);
-    else k_klt<false><<<grid2d(V.W, V.H, b), b, 0, st>>>(out, planes, V);
+    const dim3 g = grid2d(V.W, V.H, b);
+    if (fused) {
+        k_klt<true, false><<<g, b, 0, st>>>(out, planes, V, 1);
+        k_klt<true, true><<<g, b, 0, st>>>(out, planes, V, 1);
+    } else {
+        k_klt<false, true><<<g, b, 0, st>>>(out, planes, V, 0);
+    }
 }
 
 void launch_normal_depth(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st)
@@ -464,11 +489,12 @@ void launch_disparity_to_normal(float4* out, const float* d, int W, int H, cudaS
 }
 
 int tex_pitch(int W) { return W + 2 * TEX_PAD; }
-size_t tex_bytes(int W, int H) { return (size_t)tex_pitch(W) * H * 3 * sizeof(float4); }
+size_t tex_bytes(int W, int H) { return ((size_t)tex_pitch(W) * H * 3 + 1) * sizeof(float4); }
 
 void launch_pack_tex(float4* tex, const float4* bw, const float4* grad, int W, int H, cudaStream_t st)
 {
     const dim3 b(64, 4);
+    cudaMemsetAsync(tex + (size_t)3 * tex_pitch(W) * H, 0, sizeof(float4), st);   // the tiny-colour flag
     k_pack_tex<<<grid2d(tex_pitch(W), H, b), b, 0, st>>>(tex, bw, grad, W, H, tex_pitch(W));
 }
 

@@ -36,6 +36,7 @@ struct PropParams {
     int* error;                     // incremented if a view-buffer insert gave up
     float4* tmp_self;               // per-pixel state between the three propagate kernels
     float4* tmp_nb;
+    int dual;                       // the window-loop kernels run as two variants (pm_window.cuh)
 };
 
 void launch_prep(const uint8_t* img, size_t stride, int W, int H, int r, int fused, float4* bw, float4* grad,
@@ -45,6 +46,9 @@ void launch_init(float4* out, const ViewData& V, float dmax, int lr, const float
 void launch_cost(float* cost, const float4* planes, const ViewData& V, float mincost, int fused, cudaStream_t st);
 void launch_klt(float4* out, const float4* planes, const ViewData& V, int fused, cudaStream_t st);
 void launch_propagate(const PropParams& P, int fused, cudaStream_t st);
+// launches per window-loop kernel (init, cost, klt, each of the three propagate kernels):
+// fused and uncounted runs launch both variants (pm_window.cuh)
+inline int window_kernel_launches(int fused, bool counting) { return fused && !counting ? 2 : 1; }
 void launch_normal_depth(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st);
 size_t rof_scratch_bytes(int W, int H);
 void launch_rof(float4* out, const float4* input, const float4* dt, float4 lam, int iters, int W, int H, void* scratch,
@@ -61,7 +65,9 @@ int tex_pitch(int W);
 size_t tex_bytes(int W, int H);
 inline ViewData make_view(const float4* t1, const float4* t2, int W, int H, int r)
 {
-    return ViewData{t1, t2, W, H, r, tex_pitch(W), tex_pitch(W) * H};
+    const int plane = tex_pitch(W) * H;
+    return ViewData{t1, t2, W, H, r, tex_pitch(W), plane, reinterpret_cast<const int*>(t1 + (size_t)3 * plane),
+                    reinterpret_cast<const int*>(t2 + (size_t)3 * plane)};
 }
 void launch_pack_tex(float4* tex, const float4* bw, const float4* grad, int W, int H, cudaStream_t st);
 // FP32 peak probe: `iters` rounds of independent fma chains per thread

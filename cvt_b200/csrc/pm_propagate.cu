@@ -19,15 +19,20 @@ namespace pm {
 
 namespace {
 
-constexpr int PROP_BX = 32, PROP_BY = 4, PROP_THREADS = PROP_BX * PROP_BY;
-// resident blocks per SM asked of the register allocator for each kernel (at 128 threads,
-// 6 blocks = 80 registers, 5 = 96; measured best at 6 for both)
-#ifndef PM_CHAIN_BLOCKS
-#define PM_CHAIN_BLOCKS 6
+// block shape: a warp is 32 consecutive pixels of a row, PM_PROP_BY rows per block
+#ifndef PM_PROP_BY
+#define PM_PROP_BY 4
 #endif
-#ifndef PM_KLT_BLOCKS
-#define PM_KLT_BLOCKS 6
+constexpr int PROP_BX = 32, PROP_BY = PM_PROP_BY, PROP_THREADS = PROP_BX * PROP_BY;
+// resident threads per SM asked of the register allocator for each kernel (768 threads =
+// 80 registers, 640 = 96; measured best at 768 for both)
+#ifndef PM_CHAIN_THREADS
+#define PM_CHAIN_THREADS 768
 #endif
+#ifndef PM_KLT_THREADS
+#define PM_KLT_THREADS 768
+#endif
+constexpr int PM_CHAIN_BLOCKS = PM_CHAIN_THREADS / PROP_THREADS, PM_KLT_BLOCKS = PM_KLT_THREADS / PROP_THREADS;
 
 inline dim3 grid2d(int W, int H, dim3 b) { return dim3((W + b.x - 1) / b.x, (H + b.y - 1) / b.y); }
 
@@ -66,9 +71,10 @@ __device__ __forceinline__ bool view_insert(unsigned long long* slot, unsigned i
 // [-4, 5] (:982-991), 6 a random plane (:996-1002), 7-8 cross-view planes (:1007-1016),
 // 9 the randomized refinement (:1021-1028).  One loop, so that the window evaluation has a
 // single call site.
-template <bool F, bool COUNT>
+template <bool F, bool COUNT, bool CHK>
 __global__ void __launch_bounds__(PROP_THREADS, PM_CHAIN_BLOCKS) k_prop_chain(PropParams P)
 {
+    if (variant_skips<CHK>(P.V, P.dual)) return;
     const ViewData& V = P.V;
     const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
     Counters cnt = {0, 0, 0, 0};
@@ -119,13 +125,13 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_CHAIN_BLOCKS) k_prop_chain(Pr
                 nb = nd_state_refine(rng, self, cx, cy, dmax, lr);
             }
             if (k == 0) {
-                self.w = patch_eval<F, COUNT>(V, px, py, nb, 1e10f, cnt);
+                self.w = patch_eval<F, COUNT, CHK>(V, px, py, nb, 1e10f, cnt);
                 sd_self = smooth_dist1(self, smooth, cx, cy, dmax, lr);
             } else {
                 const float sd = smooth_dist1(nb, smooth, cx, cy, dmax, lr);
                 // minimalCost (:873-877)
                 const float mincost = self.w + theta * sd_self - theta * sd;
-                nb.w = patch_eval<F, COUNT>(V, px, py, nb, mincost, cnt);
+                nb.w = patch_eval<F, COUNT, CHK>(V, px, py, nb, mincost, cnt);
                 if (nb.w + theta * sd <= self.w + theta * sd_self) {   // :976 etc.
                     self = nb;
                     sd_self = sd;
@@ -138,25 +144,27 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_CHAIN_BLOCKS) k_prop_chain(Pr
 }
 
 // Gauss-Newton plane steps (:1034-1038)
-template <bool F, bool COUNT>
+template <bool F, bool COUNT, bool CHK>
 __global__ void __launch_bounds__(PROP_THREADS, PM_KLT_BLOCKS) k_prop_klt(PropParams P)
 {
+    if (variant_skips<CHK>(P.V, P.dual)) return;
     const ViewData& V = P.V;
     const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
     Counters cnt = {0, 0, 0, 0};
     if (px < V.W && py < V.H) {
         const size_t idx = (size_t)py * V.W + px;
         float4 nb = P.tmp_self[idx];
-        for (int k = 0; k < 6; k++) nb = klt2<F, COUNT>(V, px, py, nb, cnt);
+        for (int k = 0; k < 6; k++) nb = klt2<F, COUNT, CHK>(V, px, py, nb, cnt);
         P.tmp_nb[idx] = nb;
     }
     flush_counters<COUNT>(cnt, P.counters);
 }
 
 // evaluation of the Gauss-Newton result (:1039-1052), view scatter (:1060-1067), output (:1070)
-template <bool F, bool COUNT>
+template <bool F, bool COUNT, bool CHK>
 __global__ void __launch_bounds__(PROP_THREADS) k_prop_final(PropParams P)
 {
+    if (variant_skips<CHK>(P.V, P.dual)) return;
     const ViewData& V = P.V;
     const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
     Counters cnt = {0, 0, 0, 0};
@@ -172,7 +180,7 @@ __global__ void __launch_bounds__(PROP_THREADS) k_prop_final(PropParams P)
         float4 nb = P.tmp_nb[idx];
         const float2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
         const float mincost = self.w + theta * sd.y - theta * sd.x;
-        nb.w = patch_eval<F, COUNT>(V, px, py, nb, mincost, cnt);
+        nb.w = patch_eval<F, COUNT, CHK>(V, px, py, nb, mincost, cnt);
         if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
 
         if (P.vout_count) {
@@ -198,18 +206,28 @@ void launch_propagate(const PropParams& P, int fused, cudaStream_t st)
     const dim3 b(PROP_BX, PROP_BY);
     const dim3 g = grid2d(P.V.W, P.V.H, b);
     const bool count = P.counters != nullptr;
-#define PM_PROP_LAUNCH(FF, CC)                      \
-    do {                                            \
-        k_prop_chain<FF, CC><<<g, b, 0, st>>>(P);   \
-        k_prop_klt<FF, CC><<<g, b, 0, st>>>(P);     \
-        k_prop_final<FF, CC><<<g, b, 0, st>>>(P);   \
+#define PM_PROP_LAUNCH(FF, CC, KK, PP)                  \
+    do {                                                \
+        k_prop_chain<FF, CC, KK><<<g, b, 0, st>>>(PP);  \
+        k_prop_klt<FF, CC, KK><<<g, b, 0, st>>>(PP);    \
+        k_prop_final<FF, CC, KK><<<g, b, 0, st>>>(PP);  \
     } while (0)
-    if (fused) {
-        if (count) PM_PROP_LAUNCH(true, true);
-        else PM_PROP_LAUNCH(true, false);
+    PropParams Q = P;
+    if (fused && !count) {
+        // both variants; the one that does not apply returns at once (pm_window.cuh).  Each
+        // kernel of the pass finishes before the next starts, for either variant.
+        Q.dual = 1;
+        k_prop_chain<true, false, false><<<g, b, 0, st>>>(Q);
+        k_prop_chain<true, false, true><<<g, b, 0, st>>>(Q);
+        k_prop_klt<true, false, false><<<g, b, 0, st>>>(Q);
+        k_prop_klt<true, false, true><<<g, b, 0, st>>>(Q);
+        k_prop_final<true, false, false><<<g, b, 0, st>>>(Q);
+        k_prop_final<true, false, true><<<g, b, 0, st>>>(Q);
     } else {
-        if (count) PM_PROP_LAUNCH(false, true);
-        else PM_PROP_LAUNCH(false, false);
+        Q.dual = 0;
+        if (fused) PM_PROP_LAUNCH(true, true, true, Q);
+        else if (count) PM_PROP_LAUNCH(false, true, true, Q);
+        else PM_PROP_LAUNCH(false, false, true, Q);
     }
 #undef PM_PROP_LAUNCH
 }

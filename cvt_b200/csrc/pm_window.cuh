@@ -12,8 +12,10 @@
 // the lanes of a warp gathering neighbouring texels read 16-byte strided
 // addresses.  The compact plane (r, g, b, the four gradient sign bits as bytes),
 // `plane` float4 after the gradient plane, holds all that a first-view window
-// sample needs, in one load.  (Interleaved 32-byte texels read with 256-bit
-// loads measured slower for the Gauss-Newton taps.)
+// sample needs, in one load.  (Interleaved 32-byte texels read with 256-bit loads
+// measured slower for the Gauss-Newton taps.)  After the three planes, one int:
+// set when some colour value is finite, nonzero and below 2^-40 in magnitude (see
+// ad_sum).
 //
 // Blackwell specifics: the 7-channel bilinear reads of the second view and the
 // truncated absolute differences run as packed FP32 pairs (FFMA2 / FMUL2,
@@ -35,6 +37,8 @@ struct ViewData {
     const float4* __restrict__ t2;   // second view
     int W, H, r, P;                  // P = W + 2 * TEX_PAD texels per row
     int plane;                       // H * P
+    const int* tiny1;                // the views' tiny-colour flags (after the three planes)
+    const int* tiny2;
     // colour texel (compact texel) of column 0 of row y
     __device__ __forceinline__ const float4* row1(int y) const { return t1 + (size_t)y * P + TEX_PAD; }
     __device__ __forceinline__ const float4* row1c(int y) const { return t1 + 2 * (size_t)plane + (size_t)y * P + TEX_PAD; }
@@ -119,7 +123,17 @@ __device__ __forceinline__ uint32_t sign_bytes(float4 g)
 // number of gradient components whose signs differ (the census term, :712-715, :367-370)
 __device__ __forceinline__ int sign_mismatch(uint32_t a, uint32_t b) { return __popc((a ^ b) & 0x80808080u); }
 
-// sum over r, g, b of fmin(|v2 - ref|, 0.05) / 0.05 (:707-709, :364-365), divisions exact
+// Sum over r, g, b of fmin(|v2 - ref|, 0.05) / 0.05 (:707-709, :364-365), divisions exact.
+// x / 0.05 is formed as q = 20 x corrected by one fma, exact for every x >= 2^-100 (checked
+// exhaustively); below that the division itself is taken (CHK).  The window loops need the
+// fallback only for inputs that can make a nonzero |v2 - ref| that small: v2 is a bilinear
+// mix of colour values with weights that are multiples of 2^-26 (fractions of coordinates
+// formed as (x + 0.5) - 0.5 or x - floor(x)), ref a colour value or a difference of two.
+// When every finite nonzero colour value has magnitude >= 2^-40 (its ulp >= 2^-63), all of
+// these are multiples of 2^-89, so a nonzero difference is >= 2^-89 and the fallback never
+// fires.  k_pack_tex flags any view that breaks this (images read as k/255 never do), and
+// only then do the loops run with CHK.
+template <bool CHK>
 __device__ __forceinline__ float ad_sum(float4 v2, float4 ref)
 {
     const float2 d01 = __ffma2_rn(f2(ref.x, ref.y), f2(-1.0f, -1.0f), f2(v2.x, v2.y));   // v2 - ref, exact
@@ -132,7 +146,7 @@ __device__ __forceinline__ float ad_sum(float4 v2, float4 ref)
     const float q2 = m2 * 20.0f;
     const float r2 = fmaf(q2, -0.05f, m2);
     float c2 = fmaf(r2, 20.0f, q2);
-    if (fminf(fminf(m0, m1), m2) < 7.88860905e-31f) {   // below 2^-100 the fma correction is not exact
+    if (CHK && fminf(fminf(m0, m1), m2) < 7.88860905e-31f) {   // below 2^-100 the fma correction is not exact
         c01 = f2(m0 / 0.05f, m1 / 0.05f);
         c2 = m2 / 0.05f;
     }
@@ -147,10 +161,10 @@ __device__ __forceinline__ float ad_sum(float4 v2, float4 ref)
 // `w1 * (1.0f - alpha) * 0.25 * (float)cnt` (:370) carries a double literal, so the sum is a
 // double-precision one rounded once: formed exactly in double (strict) or with one fma
 // (fused); w1 * 0.875f * 0.25f is one multiply by 0.21875 for the same reason as above.
-template <bool F>
+template <bool F, bool CHK>
 __device__ __forceinline__ float klt_cost(float k1, float w1, float4 val1, uint32_t sb1, const Texel& t)
 {
-    float C = k1 * ad_sum(t.c, val1);
+    float C = k1 * ad_sum<CHK>(t.c, val1);
     const int n = sign_mismatch(sb1, sign_bytes(t.g));
     if (F) C = fmaf(w1 * 0.21875f, (float)n, C);
     else C = (float)((double)C + (double)(w1 * 0.875f) * 0.25 * (double)(float)n);
@@ -179,11 +193,23 @@ __device__ __forceinline__ float3 lusolve(float h00, float h01, float h02, float
     return ret;
 }
 
+// Whether the views carry colour values for which ad_sum needs its fallback.  Kernels that
+// run the window loops come in two variants launched back to back: without the fallback
+// (returns at once when a flag is set) and with it (returns at once when none is, if
+// `dual`); a kernel launched alone has the fallback and dual = 0.
+__device__ __forceinline__ bool views_need_check(const ViewData& V) { return (__ldg(V.tiny1) | __ldg(V.tiny2)) != 0; }
+template <bool CHK>
+__device__ __forceinline__ bool variant_skips(const ViewData& V, int dual)
+{
+    const bool chk = views_need_check(V);
+    return CHK ? (dual && !chk) : chk;
+}
+
 // one window sample of patch_eval_census (:690-722) at window position (qx, row of q1) of a
 // pixel with centre texel `in`, for the plane s (byq = s.y * qy): accumulates the weighted
 // cost into census and the weight into wsum, or returns false when the matched column lies
 // outside the image (:693-696)
-template <bool F>
+template <bool F, bool CHK>
 __device__ __forceinline__ bool eval_sample(const float4* __restrict__ q1, const float4* __restrict__ row2, int plane,
                                             int W, float fW, float4 in, float4 s, float qx, float byq, float& census,
                                             float& wsum)
@@ -203,7 +229,7 @@ __device__ __forceinline__ bool eval_sample(const float4* __restrict__ q1, const
     } else {
         tx = lerp_texel_at<F>(row2, plane, W, p2x + 0.5f);
     }
-    float cost = PM_K033_8 * ad_sum(tx.c, q);
+    float cost = PM_K033_8 * ad_sum<CHK>(tx.c, q);
     // cost + 0.875f * (0.25f * n): the product 0.21875 n is exact, so one fma rounds the same
     cost = fmaf(0.21875f, (float)sign_mismatch(__float_as_uint(q.w), sign_bytes(tx.g)), cost);
     census = F ? fmaf(w, cost, census) : census + w * cost;
@@ -223,7 +249,7 @@ __device__ __forceinline__ bool plane_usable(float4 s, float cx, float cy, int W
 // as census >= exit_threshold(mincost, bilw), the same predicate without a division.
 // Window coordinates run as floats (integers below 2^24 are exact) instead of being
 // converted from the loop counters.
-template <bool F, bool COUNT>
+template <bool F, bool COUNT, bool CHK>
 __device__ __forceinline__ float patch_eval(const ViewData& V, int px, int py, float4 s, float mincost, Counters& cnt)
 {
     const float cx = (float)px, cy = (float)py;
@@ -245,7 +271,7 @@ __device__ __forceinline__ float patch_eval(const ViewData& V, int px, int py, f
         const float4* __restrict__ row2 = V.row2(iy);
         float qx = qx0;
         for (int n = dx1 - dx0; n >= 0; n--, q1++, qx += 1.0f) {
-            if (!eval_sample<F>(q1, row2, plane, W, fW, in, s, qx, byq, census, wsum)) continue;
+            if (!eval_sample<F, CHK>(q1, row2, plane, W, fW, in, s, qx, byq, census, wsum)) continue;
             if (COUNT) cnt.eval++;
             if (census >= thr) {
                 if (COUNT) cnt.exits++;
@@ -259,7 +285,7 @@ __device__ __forceinline__ float patch_eval(const ViewData& V, int px, int py, f
 
 // patch_census_klt2 (:326-410), with the in-bounds test on the window position rather than
 // the matched one (:358) and the colour term against the colour difference (:352, :364)
-template <bool F, bool COUNT>
+template <bool F, bool COUNT, bool CHK>
 __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4 s, Counters& cnt)
 {
     const float cxf = (float)px, cyf = (float)py;
@@ -314,13 +340,13 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
                 const Texel tA = texel_at(b, plane), tB = texel_at(b + 1, plane);
                 const Texel tC = texel_at(b + 2, plane), tD = texel_at(b + 3, plane);
                 const float b0 = 1.0f - a0;
-                Cxm = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tA, tB));
-                C = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tB, tC));
-                Cxp = klt_cost<F>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tC, tD));
+                Cxm = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tA, tB));
+                C = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tB, tC));
+                Cxp = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tC, tD));
             } else {
-                Cxm = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + -1.0f) + 0.5f));
-                C = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, p2x + 0.5f));
-                Cxp = klt_cost<F>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + 1.0f) + 0.5f));
+                Cxm = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + -1.0f) + 0.5f));
+                C = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, p2x + 0.5f));
+                Cxp = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + 1.0f) + 0.5f));
             }
             if (COUNT) cnt.klt++;
             // the update of :394-402 without a branch: a rejected sample adds exact zeros, and

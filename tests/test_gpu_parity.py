@@ -180,6 +180,24 @@ def test_kernels_fused_match_oracle(D, orc, case):
     assert bits_equal(init, orc.init(obwL, obwR, ogL, ogR, r, dmax, 1, fused=1)).all()
 
 
+def test_tiny_colours_take_exact_division(D, orc):
+    """Colour values below 2^-40 make the window loops run their checked variant (exact
+    division for truncated differences below 2^-100); results still equal the oracle's."""
+    g = load_golden("lr_40x28")
+    W, H, r, dmax, iters, pp, views = spec_of(g)
+    bwL, bwR = g["bwL"].copy(), g["bwR"].copy()
+    tiny = np.float32(2.0 ** -110)
+    bwL[5:20, :, :3] *= tiny   # the same band in both views: differences far below 2^-100
+    bwR[5:20, :, :3] *= tiny
+    gL, gR, P = g["gL"], g["gR"], g["k_planes"]
+    dL, dR, dgL, dgR, dP = (dev(D.t, a) for a in (bwL, bwR, gL, gR, P))
+    for m in (1e10, 0.2):
+        assert bits_equal(host(D.cost(dP, dL, dR, dgL, dgR, r, m, 1)), orc.cost(P, bwL, bwR, gL, gR, r, m, fused=1)).all()
+    assert bits_equal(host(D.klt(dP, dL, dR, dgL, dgR, r, 1)), orc.klt(P, bwL, bwR, gL, gR, r, fused=1)).all()
+    init = host(D.init(dL, dR, dgL, dgR, r, dmax, 1, 1))
+    assert bits_equal(init, orc.init(bwL, bwR, gL, gR, r, dmax, 1, fused=1)).all()
+
+
 def test_propagate_view_exchange_matches_oracle(D, orc):
     """Left propagate scatters into the view buffer, right propagate consumes it."""
     from cvt_b200 import scene
