@@ -21,7 +21,7 @@ SYMBOLS = [
     "pm_disparity_map_batch_device",
     "pm_k_prep", "pm_k_init", "pm_k_cost", "pm_k_klt", "pm_k_propagate", "pm_k_normal_depth",
     "pm_rof_scratch_bytes", "pm_k_rof", "pm_k_rof_static", "pm_k_consistency", "pm_k_to_disparity", "pm_k_fill_depthmap",
-    "pm_k_fill_normalmap", "pm_k_disparity_to_normal",
+    "pm_k_fill_normalmap", "pm_k_disparity_to_normal", "pm_k_pyrdown", "pm_k_pyrup_mul", "pm_pyramid_size",
     "pm_rng_floats", "pm_expf_host", "pm_sinf_host", "pm_cosf_host", "pm_acospif_host",
     "pm_exit_threshold_host", "pm_scene_generate",
 ]
@@ -29,7 +29,8 @@ SYMBOLS = [
 
 class Options(C.Structure):
     _fields_ = [("views", C.c_int), ("fused", C.c_int), ("thetamin", C.c_float), ("maxdispdiff", C.c_float),
-                ("maxanglediff", C.c_float), ("rof_iters", C.c_int), ("device", C.c_int), ("use_graph", C.c_int)]
+                ("maxanglediff", C.c_float), ("rof_iters", C.c_int), ("device", C.c_int), ("use_graph", C.c_int),
+                ("levels", C.c_int)]
 
 
 class StereoError(RuntimeError):
@@ -85,6 +86,9 @@ def lib():
         "pm_k_fill_depthmap": (i32, [vp, vp, i32, i32, f32, vp]),
         "pm_k_fill_normalmap": (i32, [vp, vp, i32, i32, i32, vp]),
         "pm_k_disparity_to_normal": (i32, [vp, vp, i32, i32, vp]),
+        "pm_k_pyrdown": (i32, [vp, i32, i32, vp, sz, i32, i32, vp]),
+        "pm_k_pyrup_mul": (i32, [vp, i32, i32, vp, i32, i32, i32, C.POINTER(C.c_float), vp]),
+        "pm_pyramid_size": (i32, [i32, i32]),
         "pm_rng_floats": (i32, [C.c_int64, i32, i32, vp]),
         "pm_expf_host": (f32, [f32]),
         "pm_sinf_host": (f32, [f32]),

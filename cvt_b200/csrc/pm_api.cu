@@ -44,6 +44,9 @@ struct pm_handle {
     std::vector<size_t> bws_bytes;
     std::vector<cudaStream_t> branch;
     std::vector<cudaEvent_t> bev;
+    // pyramid levels 1.. of single-pair calls: one workspace each
+    std::vector<void*> lws;
+    std::vector<size_t> lws_bytes;
 };
 
 namespace {
@@ -141,9 +144,6 @@ int prof_collect(pm_handle* h, cudaStream_t st)
 
 // workspace layout for a W x H pair (float4 fields unless noted)
 struct Layout {
-    size_t N;
-    size_t off[32];
-    size_t total;
     enum {
         Lbw, Rbw, Lg, Rg, LDT, RDT, Ls, Rs, tmp, mL0, mL1, mR0, mR1, chk, nrm,   // float4 x N
         pself, pnb,                                                             // float4 x N
@@ -153,8 +153,12 @@ struct Layout {
         rof,                                                                    // rof scratch
         ctr, errf,                                                              // counters (4 u64), error int
         img0, img1, disp, dmap, nmap, initd, initn,                             // staging for host entry
+        initdR, initnR,                                                         // right-view init (pyramid)
         COUNT
     };
+    size_t N;
+    size_t off[COUNT];
+    size_t total;
 };
 
 Layout layout(int W, int H, size_t stride)
@@ -182,6 +186,8 @@ Layout layout(int W, int H, size_t stride)
     put(Layout::nmap, L.N * 16);
     put(Layout::initd, L.N * 4);
     put(Layout::initn, L.N * 16);
+    put(Layout::initdR, L.N * 4);
+    put(Layout::initnR, L.N * 16);
     L.total = o;
     return L;
 }
@@ -205,16 +211,18 @@ int ensure_ws(pm_handle* h, int W, int H, size_t stride)
     return grow(h, h->ws, h->ws_bytes, layout(W, H, stride).total);
 }
 
-// one pass of disparityMapAll + disparityMap post-processing on device buffers, in the
-// workspace `ws` (at least layout(W, H, stride).total bytes)
-int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
-                 int r, float dmax, int iterations, int pp, float* dmap, float4* normal, const float* initdisp,
-                 const float4* initnormal, float4* planesL, float4* planesR, cudaStream_t st)
+// PMHuberStereo::disparityMapAll (PMHuberStereo.cpp:406-581) on one pyramid level, in the
+// workspace `ws` (layout L): the final plane fields end in mL1 and mR1.  initdL/initnL and
+// initdR/initnR are W x H init fields of the views (NULL: random init); counters and the
+// view-buffer error flag are the caller's.
+int run_level(pm_handle* h, void* ws, const Layout& L, const uint8_t* left, const uint8_t* right, int W, int H,
+              size_t stride, int r, float dmax, int iterations, float thetamin, const float* initdL,
+              const float* initdR, const float4* initnL, const float4* initnR, unsigned long long* ctr, int* errf,
+              cudaStream_t st)
 {
     const pm_options& o = h->opt;
     const int views = o.views;
     const int F = o.fused;
-    const Layout L = layout(W, H, stride);
     const size_t N = L.N;
     float4 *Lbw = at<float4>(ws, L, Layout::Lbw), *Rbw = at<float4>(ws, L, Layout::Rbw);
     float4 *Lg = at<float4>(ws, L, Layout::Lg), *Rg = at<float4>(ws, L, Layout::Rg);
@@ -222,17 +230,10 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
     float4 *Ls = at<float4>(ws, L, Layout::Ls), *Rs = at<float4>(ws, L, Layout::Rs), *tmp = at<float4>(ws, L, Layout::tmp);
     float4* mL[2] = {at<float4>(ws, L, Layout::mL0), at<float4>(ws, L, Layout::mL1)};
     float4* mR[2] = {at<float4>(ws, L, Layout::mR0), at<float4>(ws, L, Layout::mR1)};
-    float4* chk = at<float4>(ws, L, Layout::chk);
     int *vb1c = at<int>(ws, L, Layout::vb1c), *vb2c = at<int>(ws, L, Layout::vb2c);
     unsigned long long *vb1s = at<unsigned long long>(ws, L, Layout::vb1s), *vb2s = at<unsigned long long>(ws, L, Layout::vb2s);
     void* rofs = at<void>(ws, L, Layout::rof);
-    unsigned long long* ctr = at<unsigned long long>(ws, L, Layout::ctr);
-    int* errf = at<int>(ws, L, Layout::errf);
 
-    PM_CUDA(h, cudaMemsetAsync(ctr, 0, 64, st));
-    PM_CUDA(h, cudaMemsetAsync(errf, 0, 64, st));
-    h->ev_used = 0;
-    prof_mark(h, st, PM_PHASE_PREP, 0);
     // prep (PMHuberStereo.cpp:445-454)
     launch_prep(left, stride, W, H, r, F, Lbw, Lg, LDT, st);
     if (views == 2) launch_prep(right, stride, W, H, r, F, Rbw, Rg, RDT, st);
@@ -247,30 +248,39 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
     launch_pack_tex(texL, Lbw, Lg, W, H, st);
     launch_pack_tex(texR, Rbw, Rg, W, H, st);
     prof_mark(h, st, PM_PHASE_PREP, 6);
-    // init (:469-470); the given disparity and normals apply to the left view only (:92-93)
+    // init (:469-470, :349-379): a given disparity without normals gets normals from it
     int nl = 0;
-    const float4* initn = initnormal;
-    if (initdisp && !initnormal) {
+    if (initdL && !initnL) {
         float4* nrm = at<float4>(ws, L, Layout::nrm);
-        launch_disparity_to_normal(nrm, initdisp, W, H, st);   // :363-365
-        initn = nrm;
+        launch_disparity_to_normal(nrm, initdL, W, H, st);   // :363-365
+        initnL = nrm;
+        nl++;
+    }
+    if (initdR && !initnR && views == 2) {
+        float4* nrm = at<float4>(ws, L, Layout::initnR);
+        launch_disparity_to_normal(nrm, initdR, W, H, st);
+        initnR = nrm;
         nl++;
     }
     const ViewData VL = make_view(texL, texR, W, H, r);
     const ViewData VR = make_view(texR, texL, W, H, r);
-    launch_init(mL[0], VL, dmax, 1, initdisp, initn, F, st);
+    launch_init(mL[0], VL, dmax, 1, initdL, initnL, F, st);
     nl += window_kernel_launches(F, false);
     if (views == 2) {
-        launch_init(mR[0], VR, dmax, 0, nullptr, nullptr, F, st);
+        launch_init(mR[0], VR, dmax, 0, initdR, initnR, F, st);
         nl += window_kernel_launches(F, false);
     }
-    const float thetamin = o.thetamin;
     float theta = thetamin;
     const int rof_launches = (o.rof_iters > 0 && o.rof_iters % 2 == 0) ? o.rof_iters : o.rof_iters + 1;
-    if (initdisp) {   // :473-477
-        const float4 lam = make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);
+    const float4 lam0 = make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);
+    if (initdL) {   // :473-477
         launch_normal_depth(tmp, mL[0], W, H, 1.0f / dmax, 1, st);
-        launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
+        launch_rof(Ls, tmp, LDT, lam0, o.rof_iters, W, H, rofs, st);
+        nl += 1 + rof_launches;
+    }
+    if (initdR && views == 2) {   // :479-483
+        launch_normal_depth(tmp, mR[0], W, H, 1.0f / dmax, 0, st);
+        launch_rof(Rs, tmp, RDT, lam0, o.rof_iters, W, H, rofs, st);
         nl += 1 + rof_launches;
     }
     prof_mark(h, st, PM_PHASE_INIT, nl);
@@ -296,6 +306,7 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
         P.error = errf;
         P.tmp_self = at<float4>(ws, L, Layout::pself);
         P.tmp_nb = at<float4>(ws, L, Layout::pnb);
+        P.dual = 0;
         launch_propagate(P, F, st);   // :536-537
         if (views == 2) {
             P.V = VR;
@@ -322,15 +333,165 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
         theta = powf(theta, 4.0f) + thetamin;
         swap = 1 - swap;
     }
-    float4* ml = mL[1];
+    return PM_OK;
+}
+
+// pyramid level sizes of a W x H pair (level 0 first); PM_EINVAL_SHAPE when a level would
+// be empty
+int level_sizes(pm_handle* h, int W, int H, std::vector<int>& Wl, std::vector<int>& Hl)
+{
+    const int levels = h->opt.levels;
+    Wl.assign(levels, W);
+    Hl.assign(levels, H);
+    for (int l = 1; l < levels; l++) {
+        Wl[l] = pyr_next(Wl[l - 1]);
+        Hl[l] = pyr_next(Hl[l - 1]);
+        if (Wl[l] < 1 || Hl[l] < 1) return fail(h, PM_EINVAL_SHAPE, "image too small for the pyramid levels");
+    }
+    return PM_OK;
+}
+
+// workspaces of pyramid levels 1.. (level 0 uses the caller's)
+int ensure_level_ws(pm_handle* h, int W, int H)
+{
+    std::vector<int> Wl, Hl;
+    int rc = level_sizes(h, W, H, Wl, Hl);
+    if (rc) return rc;
+    const int levels = h->opt.levels;
+    if ((int)h->lws.size() < levels) { h->lws.resize(levels, nullptr); h->lws_bytes.resize(levels, 0); }
+    for (int l = 1; l < levels; l++) {
+        rc = grow(h, h->lws[l], h->lws_bytes[l], layout(Wl[l], Hl[l], (size_t)Wl[l] * 4).total);
+        if (rc) return rc;
+    }
+    return PM_OK;
+}
+
+// PMHuberStereo::disparityMap (PMHuberStereo.cpp:75-143) on device buffers: with
+// h->opt.levels = 1 (the reference's setting, :78) one disparityMapAll on the pair; with more
+// levels the coarse-to-fine loop of :83-120 (CLPyramid with scale 0.35, each finer level
+// initialised from the upsampled coarser result).  Level 0 runs in `ws`, levels 1.. in the
+// handle's level workspaces (ensure_level_ws first).
+int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
+                 int r, float dmax, int iterations, int pp, float* dmap, float4* normal, const float* initdisp,
+                 const float4* initnormal, float4* planesL, float4* planesR, cudaStream_t st)
+{
+    const pm_options& o = h->opt;
+    const int views = o.views;
+    const int levels = o.levels;
+    const Layout L = layout(W, H, stride);
+    const size_t N = L.N;
+    float4* chk = at<float4>(ws, L, Layout::chk);
+    unsigned long long* ctr = at<unsigned long long>(ws, L, Layout::ctr);
+    int* errf = at<int>(ws, L, Layout::errf);
+
+    PM_CUDA(h, cudaMemsetAsync(ctr, 0, 64, st));
+    PM_CUDA(h, cudaMemsetAsync(errf, 0, 64, st));
+    h->ev_used = 0;
+    prof_mark(h, st, PM_PHASE_PREP, 0);
+    int rc;
+    if (levels == 1) {
+        rc = run_level(h, ws, L, left, right, W, H, stride, r, dmax, iterations, o.thetamin, initdisp, nullptr,
+                       initnormal, nullptr, ctr, errf, st);   // :92-93
+        if (rc) return rc;
+    } else {
+        std::vector<int> Wl, Hl;
+        rc = level_sizes(h, W, H, Wl, Hl);
+        if (rc) return rc;
+        std::vector<void*> lw(levels);
+        std::vector<Layout> ll(levels);
+        lw[0] = ws;
+        ll[0] = L;
+        for (int l = 1; l < levels; l++) {
+            lw[l] = h->lws[l];
+            ll[l] = layout(Wl[l], Hl[l], (size_t)Wl[l] * 4);
+        }
+        // CLPyramid(0.35f, levels) of both images (:83-87): level l in its workspace's staging
+        std::vector<const uint8_t*> il(levels), ir(levels);
+        std::vector<size_t> is(levels);
+        il[0] = left;
+        ir[0] = right;
+        is[0] = stride;
+        int nl = 0;
+        for (int l = 1; l < levels; l++) {
+            uint8_t* a = at<uint8_t>(lw[l], ll[l], Layout::img0);
+            uint8_t* b = at<uint8_t>(lw[l], ll[l], Layout::img1);
+            launch_pyrdown(a, Wl[l], Hl[l], il[l - 1], is[l - 1], Wl[l - 1], Hl[l - 1], st);
+            launch_pyrdown(b, Wl[l], Hl[l], ir[l - 1], is[l - 1], Wl[l - 1], Hl[l - 1], st);
+            il[l] = a;
+            ir[l] = b;
+            is[l] = (size_t)Wl[l] * 4;
+            nl += 2;
+        }
+        // the coarsest level reads the caller's init fields at its integer coordinates
+        // (SAMPLER_NN, pmhstereo.cl:815-816): their top-left corner; normals missing from
+        // them come from the full-size disparity (:363-365)
+        const int T = levels - 1;
+        const float* id = nullptr;
+        const float4* in = nullptr;
+        if (initdisp) {
+            const float4* nfull = initnormal;
+            if (!nfull) {
+                float4* nrm = at<float4>(ws, L, Layout::nrm);
+                launch_disparity_to_normal(nrm, initdisp, W, H, st);
+                nfull = nrm;
+                nl++;
+            }
+            float* cd = at<float>(lw[T], ll[T], Layout::initd);
+            float4* cn = at<float4>(lw[T], ll[T], Layout::initn);
+            launch_crop(cd, Wl[T], Hl[T], initdisp, W, 1, st);
+            launch_crop((float*)cn, Wl[T], Hl[T], (const float*)nfull, W, 4, st);
+            nl += 2;
+            id = cd;
+            in = cn;
+        }
+        prof_mark(h, st, PM_PHASE_PREP, nl);
+        rc = run_level(h, lw[T], ll[T], il[T], ir[T], Wl[T], Hl[T], is[T], r, dmax * ((float)Wl[T] / (float)Wl[0]),
+                       iterations, o.thetamin, id, nullptr, in, nullptr, ctr, errf, st);   // :91-93
+        if (rc) return rc;
+        for (int l = T - 1; l >= 0; l--) {   // :94-120
+            const int Wc = Wl[l + 1], Hc = Hl[l + 1], Wf = Wl[l], Hf = Hl[l];
+            void* wc = lw[l + 1];
+            const Layout& lc = ll[l + 1];
+            float* t1 = at<float>(wc, lc, Layout::disp);
+            float4* t4 = at<float4>(wc, lc, Layout::nmap);
+            float* dl = at<float>(lw[l], ll[l], Layout::initd);
+            float* dr = at<float>(lw[l], ll[l], Layout::initdR);
+            float4* nlf = at<float4>(lw[l], ll[l], Layout::initn);
+            float4* nrf = at<float4>(lw[l], ll[l], Layout::initnR);
+            const float4* cl = at<float4>(wc, lc, Layout::mL1);
+            const float4* cr = at<float4>(wc, lc, Layout::mR1);
+            const float up = (float)Wf / (float)Wc;
+            const float4 mulD = make_float4(up, up, up, up), mulN = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+            launch_to_disparity(t1, cl, Wc, Hc, 1.0f, 1, st);
+            launch_pyrup_mul(dl, Wf, Hf, t1, Wc, Hc, 1, mulD, st);
+            launch_fill_normalmap(t4, cl, Wc, Hc, st);
+            launch_pyrup_mul((float*)nlf, Wf, Hf, (const float*)t4, Wc, Hc, 4, mulN, st);
+            nl = 4;
+            if (views == 2) {
+                launch_to_disparity(t1, cr, Wc, Hc, 1.0f, 0, st);
+                launch_pyrup_mul(dr, Wf, Hf, t1, Wc, Hc, 1, mulD, st);
+                launch_fill_normalmap(t4, cr, Wc, Hc, st);
+                launch_pyrup_mul((float*)nrf, Wf, Hf, (const float*)t4, Wc, Hc, 4, mulN, st);
+                nl += 4;
+            }
+            prof_mark(h, st, PM_PHASE_INIT, nl);
+            const float mintheta = (float)(levels - l) / (float)levels;
+            rc = run_level(h, lw[l], ll[l], il[l], ir[l], Wf, Hf, is[l], r, dmax * ((float)Wf / (float)Wl[0]),
+                           iterations, 1e-1f * mintheta + o.thetamin, dl, views == 2 ? dr : nullptr, nlf,
+                           views == 2 ? nrf : nullptr, ctr, errf, st);
+            if (rc) return rc;
+        }
+    }
+    float4* ml = at<float4>(ws, L, Layout::mL1);
+    float4* mr = at<float4>(ws, L, Layout::mR1);
     if (planesL) PM_CUDA(h, cudaMemcpyAsync(planesL, ml, N * 16, cudaMemcpyDeviceToDevice, st));
-    if (planesR && views == 2) PM_CUDA(h, cudaMemcpyAsync(planesR, mR[1], N * 16, cudaMemcpyDeviceToDevice, st));
-    nl = 0;
+    if (planesR && views == 2) PM_CUDA(h, cudaMemcpyAsync(planesR, mr, N * 16, cudaMemcpyDeviceToDevice, st));
+    int nl = 0;
     if (pp == PM_PP_NONE) {   // :123-129
         if (dmap) { launch_to_disparity(dmap, ml, W, H, 1.0f, 1, st); nl++; }
         if (normal) { launch_fill_normalmap(normal, ml, W, H, st); nl++; }
     } else {   // :130-141
-        launch_consistency(chk, ml, mR[1], W, H, o.maxdispdiff, o.maxanglediff, st);
+        launch_consistency(chk, ml, mr, W, H, o.maxdispdiff, o.maxanglediff, st);
         nl++;
         if (dmap) {
             if (pp == PM_PP_LRCHECK) launch_to_disparity(dmap, chk, W, H, 1.0f, 1, st);
@@ -367,11 +528,14 @@ struct TexPair {
     }
 };
 
+inline bool aligned(const void* p, size_t n) { return ((uintptr_t)p % n) == 0; }
+
 int check_args(pm_handle* h, const void* left, const void* right, int W, int H, size_t stride, int r, float dmax,
                int iterations, int pp)
 {
     if (!h) return fail(h, PM_EINVAL_ARG, "null handle");
     if (!left || !right) return fail(h, PM_EINVAL_ARG, "null image");
+    if (!aligned(left, 4) || !aligned(right, 4)) return fail(h, PM_EINVAL_ARG, "images must be 4-byte aligned");
     int rc = check_shape(h, W, H, r);
     if (rc) return rc;
     if (stride < (size_t)W * 4 || stride % 4) return fail(h, PM_EINVAL_SHAPE, "row stride must be >= 4*width and a multiple of 4");
@@ -454,12 +618,14 @@ int pipeline_on(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* righ
         return run_pipeline(h, ws, left, right, W, H, stride, r, dmax, iterations, pp, dmap, normal, initdisp,
                             initnormal, planesL, planesR, st);
     const pm_options& o = h->opt;
-    const std::vector<uint64_t> key = {
+    std::vector<uint64_t> key = {
         (uint64_t)(uintptr_t)ws, (uint64_t)(uintptr_t)left, (uint64_t)(uintptr_t)right, (uint64_t)W, (uint64_t)H,
         (uint64_t)stride, (uint64_t)r, fbits(dmax), (uint64_t)iterations, (uint64_t)pp, (uint64_t)(uintptr_t)dmap,
         (uint64_t)(uintptr_t)normal, (uint64_t)(uintptr_t)initdisp, (uint64_t)(uintptr_t)initnormal,
         (uint64_t)(uintptr_t)planesL, (uint64_t)(uintptr_t)planesR, (uint64_t)o.views, (uint64_t)o.fused,
-        fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff), (uint64_t)o.rof_iters, (uint64_t)h->counting};
+        fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff), (uint64_t)o.rof_iters, (uint64_t)h->counting,
+        (uint64_t)o.levels};
+    for (void* p : h->lws) key.push_back((uint64_t)(uintptr_t)p);
     return run_graph(h, h->key1, h->exec1, key, st, [&](cudaStream_t cs) {
         return run_pipeline(h, ws, left, right, W, H, stride, r, dmax, iterations, pp, dmap, normal, initdisp,
                             initnormal, planesL, planesR, cs);
@@ -496,6 +662,7 @@ int pm_options_default(pm_options* o)
     o->rof_iters = 40;
     o->device = 0;
     o->use_graph = 1;
+    o->levels = 1;
     return PM_OK;
 }
 
@@ -508,6 +675,7 @@ int pm_create(pm_handle** out, const pm_options* opt)
     if (opt) o = *opt;
     if (o.views != 1 && o.views != 2) return fail(nullptr, PM_EINVAL_ARG, "views must be 1 or 2");
     if (o.rof_iters < 0) return fail(nullptr, PM_EINVAL_ARG, "negative smoothing iteration count");
+    if (o.levels < 1 || o.levels > PM_MAX_LEVELS) return fail(nullptr, PM_EINVAL_ARG, "pyramid levels out of range");
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return fail(nullptr, PM_ENODEV, "no CUDA device"); }
     if (o.device < 0 || o.device >= n) return fail(nullptr, PM_EINVAL_ARG, "device ordinal out of range");
@@ -525,6 +693,8 @@ int pm_destroy(pm_handle* h)
     if (h->exec1) cudaGraphExecDestroy(h->exec1);
     if (h->execb) cudaGraphExecDestroy(h->execb);
     for (void* p : h->bws)
+        if (p) cudaFree(p);
+    for (void* p : h->lws)
         if (p) cudaFree(p);
     for (cudaStream_t b : h->branch) cudaStreamDestroy(b);
     for (cudaEvent_t e : h->bev) cudaEventDestroy(e);
@@ -609,10 +779,15 @@ int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* ri
 {
     int rc = check_args(h, left, right, W, H, stride, patchsize, dispmax, iterations, pp);
     if (rc) return rc;
+    if (!aligned(dmap, 4) || !aligned(initdisp, 4) || !aligned(normalmap, 16) || !aligned(initnormal, 16) ||
+        !aligned(planes_left, 16) || !aligned(planes_right, 16))
+        return fail(h, PM_EINVAL_ARG, "float fields must be 4-byte aligned, float4 fields 16-byte aligned");
     PM_CUDA(h, cudaSetDevice(h->opt.device));
     h->W = W;
     h->H = H;
     rc = ensure_ws(h, W, H, stride);
+    if (rc) return rc;
+    rc = ensure_level_ws(h, W, H);
     if (rc) return rc;
     rc = pipeline_on(h, h->ws, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap,
                      reinterpret_cast<float4*>(normalmap), initdisp, reinterpret_cast<const float4*>(initnormal),
@@ -636,6 +811,8 @@ int pm_disparity_map(pm_handle* h, const uint8_t* left, const uint8_t* right, in
     if (rc) return rc;
     PM_CUDA(h, cudaSetDevice(h->opt.device));
     rc = ensure_ws(h, W, H, stride);
+    if (rc) return rc;
+    rc = ensure_level_ws(h, W, H);
     if (rc) return rc;
     h->W = W;
     h->H = H;
@@ -682,6 +859,7 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
 {
     if (!h) return fail(h, PM_EINVAL_ARG, "null handle");
     if (n < 0 || n > PM_MAX_BATCH) return fail(h, PM_EINVAL_ARG, "batch size out of range");
+    if (h->opt.levels != 1) return fail(h, PM_EINVAL_ARG, "pyramid levels apply to single-pair calls only");
     if (n == 0) return PM_OK;
     if (!left || !right || !width || !height || !stride || !patchsize || !dispmax)
         return fail(h, PM_EINVAL_ARG, "null per-pair array");
@@ -958,6 +1136,40 @@ int pm_k_disparity_to_normal(float* out, const float* disp, int W, int H, void* 
     launch_disparity_to_normal((float4*)out, disp, W, H, S(stream));
     PM_CUDA(nullptr, cudaGetLastError());
     return PM_OK;
+}
+
+int pm_k_pyrdown(uint8_t* out, int Wo, int Ho, const uint8_t* in, size_t stride, int Wi, int Hi, void* stream)
+{
+    int rc = check_shape(nullptr, Wi, Hi, 0);
+    if (rc) return rc;
+    rc = check_shape(nullptr, Wo, Ho, 0);
+    if (rc) return rc;
+    if (!out || !in || stride < (size_t)Wi * 4 || stride % 4 || !aligned(in, 4) || !aligned(out, 4))
+        return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    launch_pyrdown(out, Wo, Ho, in, stride, Wi, Hi, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, int channels, const float mul[4],
+                   void* stream)
+{
+    int rc = check_shape(nullptr, Wi, Hi, 0);
+    if (rc) return rc;
+    rc = check_shape(nullptr, Wo, Ho, 0);
+    if (rc) return rc;
+    const size_t al = channels == 4 ? 16 : 4;
+    if (!out || !in || !mul || (channels != 1 && channels != 4) || !aligned(in, al) || !aligned(out, al))
+        return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    launch_pyrup_mul(out, Wo, Ho, in, Wi, Hi, channels, make_float4(mul[0], mul[1], mul[2], mul[3]), S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_pyramid_size(int n, int levels)
+{
+    for (int l = 1; l < levels; l++) n = pyr_next(n);
+    return n;
 }
 
 // ---- host evaluation of the shared arithmetic -----------------------------------------

@@ -307,6 +307,83 @@ __global__ void k_fill_normalmap(float4* __restrict__ out, const float4* __restr
     out[(size_t)y * W + x] = f4(n.x, n.y, n.z, 0.0f);
 }
 
+// Linear sampler, CLK_ADDRESS_CLAMP_TO_EDGE, unnormalised coordinates (OpenCL 1.2 s8.2) at a
+// general 2-D point, in FP32 with every product and sum rounded in order: weights
+// (1-a)(1-b), a(1-b), (1-a)b, ab, summed left to right.  fetch(x, y) takes clamped texels.
+template <class Fetch>
+__device__ __forceinline__ float4 sample_linear(Fetch fetch, int w, int h, float cx, float cy)
+{
+    const float tu = cx - 0.5f, tv = cy - 0.5f;
+    const float fu = floorf(tu), fv = floorf(tv);
+    const float a = tu - fu, b = tv - fv;
+    const int i0 = fu < -2.0f ? -2 : (fu > (float)w + 1.0f ? w + 1 : (int)fu);
+    const int j0 = fv < -2.0f ? -2 : (fv > (float)h + 1.0f ? h + 1 : (int)fv);
+    const int x0 = min(max(i0, 0), w - 1), x1 = min(max(i0 + 1, 0), w - 1);
+    const int y0 = min(max(j0, 0), h - 1), y1 = min(max(j0 + 1, 0), h - 1);
+    const float4 T00 = fetch(x0, y0), T10 = fetch(x1, y0), T01 = fetch(x0, y1), T11 = fetch(x1, y1);
+    const float w00 = (1.0f - a) * (1.0f - b), w10 = a * (1.0f - b), w01 = (1.0f - a) * b, w11 = a * b;
+    return f4(w00 * T00.x + w10 * T10.x + w01 * T01.x + w11 * T11.x, w00 * T00.y + w10 * T10.y + w01 * T01.y + w11 * T11.y,
+              w00 * T00.z + w10 * T10.z + w01 * T01.z + w11 * T11.z, w00 * T00.w + w10 * T10.w + w01 * T01.w + w11 * T11.w);
+}
+
+// write_imagef to a CL_UNORM_INT8 channel: convert_uchar_sat_rte(v * 255) (OpenCL 1.2 s8.3.1.1)
+__device__ __forceinline__ unsigned int unorm8(float v)
+{
+    const float x = v * 255.0f;
+    if (!(x > 0.0f)) return 0u;
+    if (x >= 255.0f) return 255u;
+    return (unsigned int)__float2int_rn(x);
+}
+
+// pyrdown (cvt/cl/kernel/pyr/pyrdown.cl:27-46) as CLPyramid::pyrDown runs it
+// (cvt/cl/CLPyramid.cpp:73-78): one output texel per thread, the linear sample of the
+// RGBA8 input at (Wi/Wo * (x + 0.5), Hi/Ho * (y + 0.5)), written back as RGBA8
+__global__ void k_pyrdown(uchar4* __restrict__ out, int Wo, int Ho, const uint8_t* __restrict__ in, size_t stride,
+                          int Wi, int Hi)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wo || y >= Ho) return;
+    const float incx = (float)Wi / (float)Wo, incy = (float)Hi / (float)Ho;
+    auto fetch = [&](int i, int j) {
+        const uchar4 p = *reinterpret_cast<const uchar4*>(in + (size_t)j * stride + 4 * (size_t)i);
+        return f4(__fdiv_rn((float)p.x, 255.0f), __fdiv_rn((float)p.y, 255.0f), __fdiv_rn((float)p.z, 255.0f),
+                  __fdiv_rn((float)p.w, 255.0f));
+    };
+    const float4 v = sample_linear(fetch, Wi, Hi, incx * ((float)x + 0.5f), incy * ((float)y + 0.5f));
+    out[(size_t)y * Wo + x] = make_uchar4(unorm8(v.x), unorm8(v.y), unorm8(v.z), unorm8(v.w));
+}
+
+// pyrup_mul4f (cvt/cl/kernel/pyr/pyrupmul.cl:50-71) as PMHuberStereo::pyrUpMul runs it
+// (PMHuberStereo.cpp:709-721): mul times the linear sample of a float image of 1 or 4
+// channels at (Wi/Wo * (x + 0.5), Hi/Ho * (y + 0.5))
+template <int CH>
+__global__ void k_pyrup_mul(float* __restrict__ out, int Wo, int Ho, const float* __restrict__ in, int Wi, int Hi,
+                            float4 mul)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wo || y >= Ho) return;
+    const float incx = (float)Wi / (float)Wo, incy = (float)Hi / (float)Ho;
+    auto fetch = [&](int i, int j) {
+        const size_t k = (size_t)j * Wi + i;
+        if (CH == 1) return f4(in[k], in[k], in[k], in[k]);
+        return reinterpret_cast<const float4*>(in)[k];
+    };
+    const float4 v = sample_linear(fetch, Wi, Hi, incx * ((float)x + 0.5f), incy * ((float)y + 0.5f));
+    const size_t o = (size_t)y * Wo + x;
+    if (CH == 1) out[o] = mul.x * v.x;
+    else reinterpret_cast<float4*>(out)[o] = f4(mul.x * v.x, mul.y * v.y, mul.z * v.z, mul.w * v.w);
+}
+
+// the top-left Wd x Hd corner of a field with Ws columns (CH floats per texel)
+template <int CH>
+__global__ void k_crop(float* __restrict__ dst, int Wd, int Hd, const float* __restrict__ src, int Ws)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= Wd || y >= Hd) return;
+#pragma unroll
+    for (int c = 0; c < CH; c++) dst[((size_t)y * Wd + x) * CH + c] = src[((size_t)y * Ws + x) * CH + c];
+}
+
 __global__ void k_disparity_to_normal(float4* __restrict__ out, const float* __restrict__ d, int W, int H)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -486,6 +563,27 @@ void launch_disparity_to_normal(float4* out, const float* d, int W, int H, cudaS
 {
     const dim3 b(32, 8);
     k_disparity_to_normal<<<grid2d(W, H, b), b, 0, st>>>(out, d, W, H);
+}
+
+void launch_pyrdown(uint8_t* out, int Wo, int Ho, const uint8_t* in, size_t stride, int Wi, int Hi, cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    k_pyrdown<<<grid2d(Wo, Ho, b), b, 0, st>>>(reinterpret_cast<uchar4*>(out), Wo, Ho, in, stride, Wi, Hi);
+}
+
+void launch_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, int channels, float4 mul,
+                      cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    if (channels == 1) k_pyrup_mul<1><<<grid2d(Wo, Ho, b), b, 0, st>>>(out, Wo, Ho, in, Wi, Hi, mul);
+    else k_pyrup_mul<4><<<grid2d(Wo, Ho, b), b, 0, st>>>(out, Wo, Ho, in, Wi, Hi, mul);
+}
+
+void launch_crop(float* dst, int Wd, int Hd, const float* src, int Ws, int channels, cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    if (channels == 1) k_crop<1><<<grid2d(Wd, Hd, b), b, 0, st>>>(dst, Wd, Hd, src, Ws);
+    else k_crop<4><<<grid2d(Wd, Hd, b), b, 0, st>>>(dst, Wd, Hd, src, Ws);
 }
 
 int tex_pitch(int W) { return W + 2 * TEX_PAD; }

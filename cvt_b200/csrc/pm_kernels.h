@@ -59,6 +59,16 @@ void launch_to_disparity(float* out, const float4* planes, int W, int H, float s
 void launch_fill_depthmap(float* out, const float4* planes, int W, int H, float scale, cudaStream_t st);
 void launch_fill_normalmap(float4* out, const float4* planes, int W, int H, cudaStream_t st);
 void launch_disparity_to_normal(float4* out, const float* d, int W, int H, cudaStream_t st);
+// pyramid steps: RGBA8 downscale (input rows of `stride` bytes, output tight) and the
+// upscale-and-multiply of a float image of 1 or 4 channels (tight rows)
+void launch_pyrdown(uint8_t* out, int Wo, int Ho, const uint8_t* in, size_t stride, int Wi, int Hi, cudaStream_t st);
+void launch_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, int channels, float4 mul,
+                      cudaStream_t st);
+// the top-left Wd x Hd corner of a field of Ws columns, 1 or 4 floats per texel
+void launch_crop(float* dst, int Wd, int Hd, const float* src, int Ws, int channels, cudaStream_t st);
+// size of the next pyramid level: CLPyramid::update (cvt/cl/CLPyramid.cpp:51-57) multiplies
+// the size_t width by the float scale 0.35f and truncates
+inline int pyr_next(int n) { return (int)(size_t)((float)(size_t)n * 0.35f); }
 void launch_view_clear(int* count, unsigned long long* src, size_t n, cudaStream_t st);
 // texel planes of a view (pm_window.cuh) from its bw and grad fields
 int tex_pitch(int W);

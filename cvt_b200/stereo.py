@@ -29,13 +29,14 @@ class PMHuberStereo:
     """Slanted-plane PatchMatch stereo with ROF-coupled smoothing on one B200."""
 
     def __init__(self, views=2, fused=True, device=0, thetamin=1e-4, maxdispdiff=1.0, maxanglediff=5.0,
-                 rof_iters=40, use_graph=True):
+                 rof_iters=40, use_graph=True, levels=1):
         L = _lib.lib()
         opt = _lib.Options()
         _lib.check(L.pm_options_default(C.byref(opt)))
         opt.views, opt.fused, opt.device = int(views), int(bool(fused)), int(device)
         opt.thetamin, opt.maxdispdiff, opt.maxanglediff = thetamin, maxdispdiff, maxanglediff
         opt.rof_iters, opt.use_graph = int(rof_iters), int(bool(use_graph))
+        opt.levels = int(levels)
         h = C.c_void_p()
         _lib.check(L.pm_create(C.byref(h), C.byref(opt)))
         self._h = h

@@ -81,11 +81,14 @@ enum DisparityPostProcessing { DISPARITY_PP_NONE, DISPARITY_PP_LRCHECK, DISPARIT
 
 class PMHuberStereo {
   public:
-    explicit PMHuberStereo(int device = 0) : _h(nullptr)
+    // levels: pyramid levels of disparityMap's coarse-to-fine loop; the reference fixes 1
+    // (PMHuberStereo.cpp:78)
+    explicit PMHuberStereo(int device = 0, int levels = 1) : _h(nullptr)
     {
         pm_options o;
         pm_options_default(&o);
         o.device = device;
+        o.levels = levels;
         check(pm_create(&_h, &o));
     }
     ~PMHuberStereo() { pm_destroy(_h); }

@@ -63,7 +63,14 @@ typedef struct pm_options {
     int device;          /* CUDA device ordinal, default 0 */
     int use_graph;       /* 1 (default): run each call as a CUDA graph, captured once and replayed while the
                             call's arguments are unchanged; 0: launch eagerly */
+    int levels;          /* pyramid levels, 1 (default; the reference fixes levels = 1,
+                            PMHuberStereo.cpp:78) .. PM_MAX_LEVELS: with more, disparityMap's
+                            coarse-to-fine loop (:83-120) over a CLPyramid of scale 0.35, each
+                            level initialised from the upsampled result of the coarser one.
+                            Single-pair calls only. */
 } pm_options;
+
+enum { PM_MAX_LEVELS = 8 };
 
 typedef struct pm_handle pm_handle;
 
@@ -186,6 +193,19 @@ int pm_k_to_disparity(float* out, const float* planes, int width, int height, fl
 int pm_k_fill_depthmap(float* out, const float* planes, int width, int height, float scale, void* stream);
 int pm_k_fill_normalmap(float* out, const float* planes, int width, int height, int lr, void* stream);
 int pm_k_disparity_to_normal(float* out, const float* disp, int width, int height, void* stream);
+/* pyrdown (cvt/cl/kernel/pyr/pyrdown.cl, run by CLPyramid::pyrDown, cvt/cl/CLPyramid.cpp:73-78):
+ * RGBA8 in_width x in_height (rows of `stride` bytes) -> RGBA8 out_width x out_height (tight
+ * rows), each output texel the linear sample at (Wi/Wo (x + 0.5), Hi/Ho (y + 0.5)) */
+int pm_k_pyrdown(uint8_t* out, int out_width, int out_height, const uint8_t* in, size_t stride, int in_width,
+                 int in_height, void* stream);
+/* pyrup_mul4f (cvt/cl/kernel/pyr/pyrupmul.cl, run by PMHuberStereo::pyrUpMul,
+ * PMHuberStereo.cpp:709-721): a float image of `channels` (1 or 4) per texel, tight rows,
+ * resampled the same way and multiplied by mul per component */
+int pm_k_pyrup_mul(float* out, int out_width, int out_height, const float* in, int in_width, int in_height,
+                   int channels, const float mul[4], void* stream);
+/* width (or height) of pyramid level `levels` - 1 of an image of n columns (rows):
+ * CLPyramid::update (cvt/cl/CLPyramid.cpp:51-57), each level (size_t)(n * 0.35f) */
+int pm_pyramid_size(int n, int levels);
 
 /* ---- host-side helpers ------------------------------------------------------------- */
 

@@ -6,7 +6,8 @@ cpu_baseline leg:
 * oracle/liboracle.so      the CPU restatement (pm_oracle.cpp), always;
 * oracle/_ref/libpmref.so  the reference's own kernel sources
                            (cvt/cl/kernel/pmhstereo.cl, PDDiffTensor.cl,
-                           PDDROFDiffTensor.cl) rewritten by translate.py and
+                           PDDROFDiffTensor.cl, pyr/pyrdown.cl, pyr/pyrupmul.cl)
+                           rewritten by translate.py and
                            compiled against clshim.h, when the reference tree is
                            present (it is not on GPU machines; the built .so
                            travels with the checkout instead).
@@ -50,12 +51,17 @@ def build_ref(force=False, kernel_dir=REF_KERNELS):
     os.makedirs(refdir, exist_ok=True)
     cls = ["pmhstereo.cl", "PDDiffTensor.cl", "PDDROFDiffTensor.cl"]
     deps = [os.path.join(kernel_dir, f) for f in cls + ["RNG.cl", "MWC64X.cl", "Matrix3.cl"]]
-    glue = [os.path.join(HERE, f) for f in ("ref_pmh.cpp", "ref_pd.cpp", "ref_driver.cpp")]
+    pyr = ["pyrdown.cl", "pyrupmul.cl"]
+    deps += [os.path.join(kernel_dir, "pyr", f) for f in pyr]
+    glue = [os.path.join(HERE, f) for f in ("ref_pmh.cpp", "ref_pd.cpp", "ref_pyr.cpp", "ref_driver.cpp")]
     hdrs = [os.path.join(HERE, f) for f in ("clshim.h", "ref_exec.h", "pm_hostloop.h", "pm_libm.h", "translate.py")]
     if not (force or _stale(out, deps + glue + hdrs)):
         return out
     for f in cls:
         _run([sys.executable, os.path.join(HERE, "translate.py"), kernel_dir, f, os.path.join(refdir, f + ".cpp")])
+    for f in pyr:
+        _run([sys.executable, os.path.join(HERE, "translate.py"), os.path.join(kernel_dir, "pyr"), f,
+              os.path.join(refdir, f + ".cpp")])
     _run(["g++"] + CXXFLAGS + ["-w", "-Wno-narrowing", "-I", HERE, "-o", out] + glue)
     return out
 

@@ -348,7 +348,14 @@ inline void write_imagef(image2d_t im, int2 c, float4 v)
     const size_t i = (size_t)c.y * im.w + c.x;
     if (im.kind == IMG_RGBA_FLOAT) { float* p = (float*)im.data + 4 * i; p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w; }
     else if (im.kind == IMG_INTENSITY_FLOAT) { ((float*)im.data)[i] = v.x; }
-    else abort();
+    else {   /* CL_UNORM_INT8: convert_uchar_sat_rte(v * 255) (OpenCL 1.2 s8.3.1.1) */
+        unsigned char* p = (unsigned char*)im.data + 4 * i;
+        const float c[4] = {v.x, v.y, v.z, v.w};
+        for (int k = 0; k < 4; k++) {
+            const float x = c[k] * 255.0f;
+            p[k] = !(x > 0.0f) ? 0 : (x >= 255.0f ? 255 : (unsigned char)std::nearbyint(x));
+        }
+    }
 }
 
 }  // namespace clk

@@ -899,26 +899,104 @@ int orc_disparity_to_normal(float* out, const float* disp, int W, int H)
     return 0;
 }
 
+/* Linear sampler, CLK_ADDRESS_CLAMP_TO_EDGE, unnormalised coordinates (OpenCL 1.2 s8.2) in
+ * FP32 at a general 2-D point: t = c - 0.5, i0 = floor(t), a = t - floor(t) per axis;
+ * T = (1-a)(1-b) T00 + a(1-b) T10 + (1-a)b T01 + ab T11, each weight one product, summed
+ * left to right.  fetch(x, y) returns the texel with clamped coordinates. */
+extern "C++" {
+template <class Fetch>
+static F4 sample_linear(Fetch fetch, int w, int h, float cx, float cy)
+{
+    const float tu = cx - 0.5f, tv = cy - 0.5f;
+    const float fu = floorf(tu), fv = floorf(tv);
+    const float a = tu - fu, b = tv - fv;
+    auto ci = [](float f, int n) { return f < -2.0f ? -2 : (f > (float)n + 1.0f ? n + 1 : (int)f); };
+    const int i0 = ci(fu, w), j0 = ci(fv, h);
+    auto cl = [](int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); };
+    const F4 T00 = fetch(cl(i0, w), cl(j0, h)), T10 = fetch(cl(i0 + 1, w), cl(j0, h));
+    const F4 T01 = fetch(cl(i0, w), cl(j0 + 1, h)), T11 = fetch(cl(i0 + 1, w), cl(j0 + 1, h));
+    const float w00 = (1.0f - a) * (1.0f - b), w10 = a * (1.0f - b), w01 = (1.0f - a) * b, w11 = a * b;
+    return f4(w00 * T00.x + w10 * T10.x + w01 * T01.x + w11 * T11.x, w00 * T00.y + w10 * T10.y + w01 * T01.y + w11 * T11.y,
+              w00 * T00.z + w10 * T10.z + w01 * T01.z + w11 * T11.z, w00 * T00.w + w10 * T10.w + w01 * T01.w + w11 * T11.w);
+}
+}  // extern "C++"
+
+/* write_imagef to a CL_UNORM_INT8 channel: convert_uchar_sat_rte(v * 255) (OpenCL 1.2 s8.3.1.1) */
+static uint8_t unorm8(float v)
+{
+    const float x = v * 255.0f;
+    if (!(x > 0.0f)) return 0;
+    if (x >= 255.0f) return 255;
+    return (uint8_t)rintf(x);
+}
+
+/* pyrdown (cvt/cl/kernel/pyr/pyrdown.cl) as CLPyramid::pyrDown runs it (cvt/cl/CLPyramid.cpp:73-78):
+ * RGBA8 in (Wi x Hi, tight rows) -> RGBA8 out (Wo x Ho), each output pixel the linear sample
+ * at (Wi/Wo * (x + 0.5), Hi/Ho * (y + 0.5)) */
+int orc_pyrdown(uint8_t* out, int Wo, int Ho, const uint8_t* in, int Wi, int Hi)
+{
+    const float incx = (float)Wi / (float)Wo, incy = (float)Hi / (float)Ho;
+    auto fetch = [&](int x, int y) {
+        const uint8_t* p = in + 4 * ((size_t)y * Wi + x);
+        return f4((float)p[0] / 255.0f, (float)p[1] / 255.0f, (float)p[2] / 255.0f, (float)p[3] / 255.0f);
+    };
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < Ho; y++)
+        for (int x = 0; x < Wo; x++) {
+            const F4 v = sample_linear(fetch, Wi, Hi, incx * ((float)x + 0.5f), incy * ((float)y + 0.5f));
+            uint8_t* o = out + 4 * ((size_t)y * Wo + x);
+            o[0] = unorm8(v.x); o[1] = unorm8(v.y); o[2] = unorm8(v.z); o[3] = unorm8(v.w);
+        }
+    return 0;
+}
+
+/* pyrup_mul4f (cvt/cl/kernel/pyr/pyrupmul.cl) as PMHuberStereo::pyrUpMul runs it
+ * (PMHuberStereo.cpp:709-721): out = mul * linear sample at (Wi/Wo * (x + 0.5), Hi/Ho * (y + 0.5)),
+ * per component; channels 1 (a grey float image, the sample's .x) or 4 */
+int orc_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, int channels, const float mul[4])
+{
+    if (channels != 1 && channels != 4) return -1;
+    const float incx = (float)Wi / (float)Wo, incy = (float)Hi / (float)Ho;
+    auto fetch = [&](int x, int y) {
+        const size_t i = (size_t)y * Wi + x;
+        if (channels == 1) return f4(in[i], in[i], in[i], in[i]);
+        return f4(in[4 * i], in[4 * i + 1], in[4 * i + 2], in[4 * i + 3]);
+    };
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < Ho; y++)
+        for (int x = 0; x < Wo; x++) {
+            const F4 v = sample_linear(fetch, Wi, Hi, incx * ((float)x + 0.5f), incy * ((float)y + 0.5f));
+            const size_t i = (size_t)y * Wo + x;
+            if (channels == 1) {
+                out[i] = mul[0] * v.x;
+            } else {
+                out[4 * i] = mul[0] * v.x; out[4 * i + 1] = mul[1] * v.y;
+                out[4 * i + 2] = mul[2] * v.z; out[4 * i + 3] = mul[3] * v.w;
+            }
+        }
+    return 0;
+}
+
 static const PmKernels ORC_KERNELS = {orc_prep, orc_init, orc_propagate, orc_normal_depth, orc_rof,
                                       orc_consistency, orc_to_disparity, orc_fill_depthmap, orc_fill_normalmap,
-                                      orc_disparity_to_normal};
+                                      orc_disparity_to_normal, orc_pyrdown, orc_pyrup_mul};
 
 int orc_disparity_map(const uint8_t* left, const uint8_t* right, int W, int H, int stride,
                       int r, float dmax, int iterations, int pp, int views,
                       float* dmap, float* normal, const float* initdisp, const float* initnormal,
                       float* planesL, float* planesR, int fused, int64_t* counters)
 {
-    return pm_host_disparity_map(ORC_KERNELS, left, right, W, H, stride, r, dmax, iterations, pp, views, dmap, normal,
-                                 initdisp, initnormal, planesL, planesR, fused, counters, nullptr, nullptr);
+    return pm_host_disparity_map(ORC_KERNELS, left, right, W, H, stride, r, dmax, iterations, pp, views, 1, dmap,
+                                 normal, initdisp, initnormal, planesL, planesR, fused, counters, nullptr, nullptr);
 }
 
 int orc_disparity_map_dump(const uint8_t* left, const uint8_t* right, int W, int H, int stride,
-                           int r, float dmax, int iterations, int pp, int views,
+                           int r, float dmax, int iterations, int pp, int views, int levels,
                            float* dmap, float* normal, const float* initdisp, const float* initnormal,
                            float* planesL, float* planesR, int fused, int64_t* counters, PmDumpFn dump, void* user)
 {
-    return pm_host_disparity_map(ORC_KERNELS, left, right, W, H, stride, r, dmax, iterations, pp, views, dmap, normal,
-                                 initdisp, initnormal, planesL, planesR, fused, counters, dump, user);
+    return pm_host_disparity_map(ORC_KERNELS, left, right, W, H, stride, r, dmax, iterations, pp, views, levels,
+                                 dmap, normal, initdisp, initnormal, planesL, planesR, fused, counters, dump, user);
 }
 
 }  // extern "C"

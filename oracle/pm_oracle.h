@@ -107,13 +107,19 @@ int orc_disparity_map(const uint8_t* left, const uint8_t* right, int W, int H, i
                       float* dmap, float* normal, const float* initdisp, const float* initnormal,
                       float* planesL, float* planesR, int fused, int64_t* counters);
 
-/* as orc_disparity_map, calling dump(stage, iter, field, user) after init, each propagate
- * pair and each smoothing pair with the W*H*4 float field of that stage */
+/* pyrdown (cvt/cl/kernel/pyr/pyrdown.cl): RGBA8 Wi x Hi -> RGBA8 Wo x Ho, tight rows */
+int orc_pyrdown(uint8_t* out, int Wo, int Ho, const uint8_t* in, int Wi, int Hi);
+/* pyrup_mul4f (cvt/cl/kernel/pyr/pyrupmul.cl): float images of 1 or 4 channels */
+int orc_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, int channels, const float mul[4]);
+
+/* as orc_disparity_map with `levels` pyramid levels (1: the reference's setting), calling
+ * dump(stage, iter, W, H, field, user) after init, each propagate pair and each smoothing
+ * pair with the W*H*4 float field of that stage (NULL: no dumps) */
 int orc_disparity_map_dump(const uint8_t* left, const uint8_t* right, int W, int H, int stride,
-                           int r, float dmax, int iterations, int pp, int views,
+                           int r, float dmax, int iterations, int pp, int views, int levels,
                            float* dmap, float* normal, const float* initdisp, const float* initnormal,
                            float* planesL, float* planesR, int fused, int64_t* counters,
-                           void (*dump)(const char*, int, const float*, void*), void* user);
+                           void (*dump)(const char*, int, int, int, const float*, void*), void* user);
 
 #ifdef __cplusplus
 }

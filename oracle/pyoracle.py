@@ -20,7 +20,7 @@ REF_SO = os.path.join(HERE, "_ref", "libpmref.so")
 vp = C.c_void_p
 i32 = C.c_int
 f32 = C.c_float
-DUMP_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_int, C.POINTER(C.c_float), C.c_void_p)
+DUMP_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float), C.c_void_p)
 
 
 def available(kind):
@@ -56,6 +56,8 @@ class Oracle:
             "fill_depthmap": [vp, vp, i32, i32, f32],
             "fill_normalmap": [vp, vp, i32, i32, i32],
             "disparity_to_normal": [vp, vp, i32, i32],
+            "pyrdown": [vp, i32, i32, vp, i32, i32],
+            "pyrup_mul": [vp, i32, i32, vp, i32, i32, i32, C.POINTER(C.c_float)],
         }
         for name, args in sig.items():
             fn = getattr(self.L, p + name)
@@ -64,8 +66,8 @@ class Oracle:
             setattr(self, "_" + name, fn)
         if kind == "orc":
             self.L.orc_disparity_map_dump.restype = i32
-            self.L.orc_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, vp, vp, vp, vp,
-                                                      vp, vp, i32, vp, DUMP_FN, vp]
+            self.L.orc_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, i32, vp, vp, vp,
+                                                      vp, vp, vp, i32, vp, DUMP_FN, vp]
             for fn in ("orc_exp", "orc_sin", "orc_cos", "orc_acospi"):
                 getattr(self.L, fn).restype = f32
                 getattr(self.L, fn).argtypes = [f32]
@@ -73,8 +75,8 @@ class Oracle:
             self.L.orc_rng_floats.argtypes = [C.c_int64, i32, i32, vp]
         else:
             self.L.ref_disparity_map_dump.restype = i32
-            self.L.ref_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, vp, vp, vp, vp,
-                                                      vp, vp, DUMP_FN, vp]
+            self.L.ref_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, i32, vp, vp, vp,
+                                                      vp, vp, vp, DUMP_FN, vp]
 
     # ---- kernels -----------------------------------------------------------------
     def prep(self, img, r, fused=0):
@@ -159,11 +161,28 @@ class Oracle:
         assert self._disparity_to_normal(out.ctypes.data, _p(disp), W, H) == 0
         return out
 
+    def pyrdown(self, img, Wo, Ho):
+        """one pyramid step of an RGBA8 image (H, W, 4) to (Ho, Wo, 4)"""
+        img = np.ascontiguousarray(img, np.uint8)
+        out = np.zeros((Ho, Wo, 4), np.uint8)
+        assert self._pyrdown(out.ctypes.data, Wo, Ho, img.ctypes.data, img.shape[1], img.shape[0]) == 0
+        return out
+
+    def pyrup_mul(self, img, Wo, Ho, mul):
+        """pyrup_mul4f of a float image (H, W) or (H, W, 4) to (Ho, Wo[, 4]), times mul (4 floats)"""
+        img = np.ascontiguousarray(img, np.float32)
+        ch = 1 if img.ndim == 2 else 4
+        out = np.zeros((Ho, Wo) if ch == 1 else (Ho, Wo, 4), np.float32)
+        m = (C.c_float * 4)(*[float(v) for v in mul])
+        assert self._pyrup_mul(out.ctypes.data, Wo, Ho, img.ctypes.data, img.shape[1], img.shape[0], ch, m) == 0
+        return out
+
     # ---- whole pipeline ------------------------------------------------------------
     def disparity_map(self, left, right, r, dmax, iterations, pp=1, views=2, initdisp=None, initnormal=None,
-                      fused=0, dump=False, counters=None):
+                      fused=0, dump=False, counters=None, levels=1):
         """PMHuberStereo::disparityMap.  Returns dict with dmap, normal, planesL, planesR
-        and, with dump=True, every intermediate stage keyed (stage, iter)."""
+        and, with dump=True, every intermediate stage keyed (stage, iter); stages of pyramid
+        level l > 0 are named "l<l>_<stage>"."""
         H, W = left.shape[:2]
         left = np.ascontiguousarray(left)
         right = np.ascontiguousarray(right)
@@ -171,11 +190,11 @@ class Oracle:
                "planesR": _f4((H, W)), "stages": {}}
         stages = res["stages"]
 
-        def cb(name, it, ptr, user):
-            stages[(name.decode(), it)] = np.ctypeslib.as_array(ptr, shape=(H, W, 4)).copy()
+        def cb(name, it, w, h, ptr, user):
+            stages[(name.decode(), it)] = np.ctypeslib.as_array(ptr, shape=(h, w, 4)).copy()
 
         fn = DUMP_FN(cb) if dump else DUMP_FN()
-        common = [left.ctypes.data, right.ctypes.data, W, H, W * 4, r, dmax, iterations, pp, views,
+        common = [left.ctypes.data, right.ctypes.data, W, H, W * 4, r, dmax, iterations, pp, views, levels,
                   res["dmap"].ctypes.data, res["normal"].ctypes.data, _p(initdisp), _p(initnormal),
                   res["planesL"].ctypes.data, res["planesR"].ctypes.data]
         if self.kind == "orc":

@@ -187,22 +187,31 @@ int ref_fill_normalmap(float* out, const float* planes, int W, int H, int lr)
 int ref_disparity_to_normal(float* out, const float* disp, int W, int H)
 { return ref_k_disparity_to_normal(out, disp, W, H); }
 
+int ref_k_pyrdown(uint8_t* out, int Wo, int Ho, const uint8_t* in, int Wi, int Hi);
+int ref_k_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, int channels, const float* mul);
+int ref_pyrdown(uint8_t* out, int Wo, int Ho, const uint8_t* in, int Wi, int Hi)
+{ return ref_k_pyrdown(out, Wo, Ho, in, Wi, Hi); }
+int ref_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, int channels, const float* mul)
+{ return ref_k_pyrup_mul(out, Wo, Ho, in, Wi, Hi, channels, mul); }
+
 static const PmKernels REF_KERNELS = {ref_prep, ref_init, ref_propagate, ref_normal_depth, ref_rof, ref_consistency,
-                                      ref_to_disparity, ref_fill_depthmap, ref_fill_normalmap, ref_disparity_to_normal};
+                                      ref_to_disparity, ref_fill_depthmap, ref_fill_normalmap, ref_disparity_to_normal,
+                                      ref_pyrdown, ref_pyrup_mul};
 
 int ref_disparity_map_dump(const uint8_t* left, const uint8_t* right, int W, int H, int stride, int r, float dmax,
-                           int iterations, int pp, int views, float* dmap, float* normal, const float* initdisp,
-                           const float* initnormal, float* planesL, float* planesR, PmDumpFn dump, void* user)
+                           int iterations, int pp, int views, int levels, float* dmap, float* normal,
+                           const float* initdisp, const float* initnormal, float* planesL, float* planesR,
+                           PmDumpFn dump, void* user)
 {
-    return pm_host_disparity_map(REF_KERNELS, left, right, W, H, stride, r, dmax, iterations, pp, views, dmap, normal,
-                                 initdisp, initnormal, planesL, planesR, 0, nullptr, dump, user);
+    return pm_host_disparity_map(REF_KERNELS, left, right, W, H, stride, r, dmax, iterations, pp, views, levels, dmap,
+                                 normal, initdisp, initnormal, planesL, planesR, 0, nullptr, dump, user);
 }
 
 int ref_disparity_map(const uint8_t* left, const uint8_t* right, int W, int H, int stride, int r, float dmax,
                       int iterations, int pp, int views, float* dmap, float* normal, const float* initdisp,
                       const float* initnormal, float* planesL, float* planesR)
 {
-    return ref_disparity_map_dump(left, right, W, H, stride, r, dmax, iterations, pp, views, dmap, normal, initdisp,
+    return ref_disparity_map_dump(left, right, W, H, stride, r, dmax, iterations, pp, views, 1, dmap, normal, initdisp,
                                   initnormal, planesL, planesR, nullptr, nullptr);
 }
 

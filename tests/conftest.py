@@ -45,7 +45,13 @@ def ref():
 
 
 def golden_cases():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    """single-level cases (the reference's setting)"""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("pyr"))
+
+
+def pyramid_cases():
+    """coarse-to-fine cases (pyramid levels > 1)"""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("pyr"))
 
 
 def load_golden(name):

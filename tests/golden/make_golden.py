@@ -31,6 +31,13 @@ CASES = {
     "init_40x28": (5, 40, 28, 5, 2.0, 10.0, 3, 12.0, 1, 2, 2, True),
 }
 
+# coarse-to-fine runs (pyramid levels > 1); name: (seed, W, H, nplanes, dlo, dhi, r, dmax,
+# iterations, pp, views, levels, init_from_gt)
+PYR_CASES = {
+    "pyr_96x64": (11, 96, 64, 6, 2.0, 20.0, 2, 24.0, 1, 1, 2, 2, False),
+    "pyr3_100x70": (12, 100, 70, 6, 2.0, 30.0, 1, 32.0, 1, 2, 2, 3, True),
+}
+
 
 def make_case(ref, name, spec):
     seed, W, H, npl, dlo, dhi, r, dmax, iters, pp, views, init = spec
@@ -73,6 +80,35 @@ def make_case(ref, name, spec):
     np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
 
 
+def make_pyr_case(ref, name, spec):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, pp, views, levels, init = spec
+    left, right, gtd, gtn = scene.generate(seed, W, H, npl, dlo, dhi, with_gt=True)
+    initd = gtd.copy() if init else None
+    if init:
+        initd[::4, ::3] = 0.0
+    res = ref.disparity_map(left, right, r, dmax, iters, pp=pp, views=views, initdisp=initd, levels=levels,
+                            dump=True)
+    arrays = {"left": left, "right": right, "dmap": res["dmap"], "normal": res["normal"],
+              "planesL": res["planesL"], "planesR": res["planesR"],
+              "spec": np.array([seed, W, H, npl, dlo, dhi, r, dmax, iters, pp, views, levels, int(init)], np.float64)}
+    if init:
+        arrays["initdisp"] = initd
+    for (stage, it), v in res["stages"].items():
+        if "init" in stage:   # each level's initial planes (the rest is pinned by the outputs)
+            arrays["stage_%s_%d" % (stage, it)] = v
+    # per-kernel fixtures: one pyramid step down of the left image and one step up of a
+    # disparity and a normal field (the sizes of the first level step)
+    W1, H1 = int(np.float32(W) * np.float32(0.35)), int(np.float32(H) * np.float32(0.35))
+    arrays["k_pyrdown"] = ref.pyrdown(left, W1, H1)
+    rng = np.random.default_rng(seed)
+    d1 = (rng.random((H1, W1), np.float32) * 10).astype(np.float32)
+    n1 = rng.standard_normal((H1, W1, 4)).astype(np.float32)
+    up = np.float32(W) / np.float32(W1)
+    arrays.update(k_pyr_d1=d1, k_pyr_n1=n1, k_pyrup_d=ref.pyrup_mul(d1, W, H, [up] * 4),
+                  k_pyrup_n=ref.pyrup_mul(n1, W, H, [1.0] * 4))
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+
+
 def main():
     so = obuild.build_ref()
     if so is None:
@@ -81,6 +117,9 @@ def main():
     ref = Oracle("ref")
     for name, spec in CASES.items():
         make_case(ref, name, spec)
+        print("wrote", name)
+    for name, spec in PYR_CASES.items():
+        make_pyr_case(ref, name, spec)
         print("wrote", name)
 
 

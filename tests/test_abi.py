@@ -152,3 +152,12 @@ def test_batch_null_handle(native):
     # argument checks come before any device work
     assert native.pm_disparity_map_batch_device(None, 1, None, None, None, None, None, None, None, 3, 1,
                                                 None, None, None, None) == _lib.PM_EINVAL_ARG
+
+
+def test_pyramid_sizes_follow_float_scaling(native):
+    # CLPyramid::update: (size_t)(size_t(n) * 0.35f) per level, in float arithmetic
+    for n in (1, 2, 3, 97, 320, 1280, 1920, 4096):
+        m = n
+        for levels in range(1, 5):
+            assert native.pm_pyramid_size(n, levels) == m, (n, levels)
+            m = int(np.float32(m) * np.float32(0.35))

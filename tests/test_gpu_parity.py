@@ -11,7 +11,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from conftest import golden_cases, load_golden
+from conftest import golden_cases, load_golden, pyramid_cases
 from oracle.pyoracle import bits_equal
 
 pytestmark = pytest.mark.gpu
@@ -359,3 +359,70 @@ def test_cpp_drop_in_matches_python(native, torch_cuda, tmp_path):
     L, R = scene.generate(7, 96, 64, 6, 2.0, 20.0)
     ref = PMHuberStereo().disparity_map(L, R, 4, 24.0, 3, pp=1)
     assert bits_equal(d, ref).all()
+
+
+def _pyr_spec(g):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, pp, views, levels, init = g["spec"]
+    return int(W), int(H), int(r), float(dmax), int(iters), int(pp), int(views), int(levels)
+
+
+@pytest.mark.parametrize("case", pyramid_cases())
+def test_pyramid_kernels_match_reference_golden(D, case):
+    g = load_golden(case)
+    W, H = _pyr_spec(g)[:2]
+    H1, W1 = g["k_pyrdown"].shape[:2]
+    src = dev(D.t, g["left"])
+    out = D.t.zeros((H1, W1, 4), dtype=D.t.uint8, device="cuda")
+    assert D.L.pm_k_pyrdown(out.data_ptr(), W1, H1, src.data_ptr(), W * 4, W, H, stream(D.t)) == 0
+    assert (host(out) == g["k_pyrdown"]).all()
+    up = float(np.float32(W) / np.float32(W1))
+    for k_in, k_out, ch, mul in (("k_pyr_d1", "k_pyrup_d", 1, [up] * 4), ("k_pyr_n1", "k_pyrup_n", 4, [1.0] * 4)):
+        a = dev(D.t, g[k_in])
+        o = D.t.zeros(g[k_out].shape, dtype=D.t.float32, device="cuda")
+        m = (C.c_float * 4)(*mul)
+        assert D.L.pm_k_pyrup_mul(o.data_ptr(), W, H, a.data_ptr(), W1, H1, ch, m, stream(D.t)) == 0
+        assert bits_equal(host(o), g[k_out]).all(), k_out
+
+
+@pytest.mark.parametrize("case", pyramid_cases())
+def test_pyramid_pipeline_strict_matches_reference_golden(native, torch_cuda, case):
+    from cvt_b200 import PMHuberStereo
+
+    g = load_golden(case)
+    W, H, r, dmax, iters, pp, views, levels = _pyr_spec(g)
+    pm = PMHuberStereo(views=views, fused=False, levels=levels)
+    for rep in range(2):   # graph capture, then replay
+        res = pm.disparity_map(g["left"], g["right"], r, dmax, iters, pp=pp, normalmap=True, planes=True,
+                               initdisparity=g.get("initdisp"))
+        for k, gk in (("planes_left", "planesL"), ("planes_right", "planesR"), ("dmap", "dmap"), ("normal", "normal")):
+            assert bits_equal(res[k], g[gk]).all(), (rep, k)
+
+
+def test_pyramid_pipeline_fused_matches_oracle(native, torch_cuda, orc):
+    from cvt_b200 import PMHuberStereo, scene
+
+    L, R = scene.generate(21, 150, 101, 8, 2.0, 30.0)
+    o = orc.disparity_map(L, R, 4, 32.0, 3, pp=2, fused=1, levels=3)
+    pm = PMHuberStereo(fused=True, levels=3)
+    dl, dr = torch_cuda.from_numpy(L).cuda(), torch_cuda.from_numpy(R).cuda()
+    res = pm.disparity_map(dl, dr, 4, 32.0, 3, pp=2, normalmap=True, planes=True)
+    torch_cuda.cuda.synchronize()
+    assert bits_equal(host(res["planes_left"]), o["planesL"]).all()
+    assert bits_equal(host(res["planes_right"]), o["planesR"]).all()
+    assert bits_equal(host(res["dmap"]), o["dmap"]).all()
+    assert bits_equal(host(res["normal"]), o["normal"]).all()
+
+
+def test_pipeline_with_given_normals_equals_derived_normals(native, torch_cuda, orc):
+    """initnormal given through the host entry (staged in the workspace) gives the result the
+    reference derives from the disparity alone"""
+    from cvt_b200 import PMHuberStereo
+
+    g = load_golden("init_40x28")
+    W, H, r, dmax, iters, pp, views = spec_of(g)
+    nrm = orc.disparity_to_normal(g["initdisp"])
+    pm = PMHuberStereo(views=views, fused=False)
+    res = pm.disparity_map(g["left"], g["right"], r, dmax, iters, pp=pp, planes=True, initdisparity=g["initdisp"],
+                           initnormalmap=nrm)
+    assert bits_equal(res["planes_left"], g["planesL"]).all()
+    assert bits_equal(res["dmap"], g["dmap"]).all()

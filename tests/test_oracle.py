@@ -4,7 +4,7 @@ tests for the arithmetic it fixes."""
 import numpy as np
 import pytest
 
-from conftest import golden_cases, load_golden
+from conftest import golden_cases, load_golden, pyramid_cases
 from oracle.pyoracle import bits_equal
 
 
@@ -135,3 +135,45 @@ def test_fused_mode_differs_only_by_rounding(orc):
     a = orc.disparity_map(L, R, 3, 12.0, 3, pp=0, fused=0)
     b = orc.disparity_map(L, R, 3, 12.0, 3, pp=0, fused=1)
     assert np.mean(np.abs(a["dmap"] - b["dmap"]) < 1.0) > 0.9
+
+
+def pyr_spec(g):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, pp, views, levels, init = g["spec"]
+    return dict(W=int(W), H=int(H), r=int(r), dmax=float(dmax), iters=int(iters), pp=int(pp), views=int(views),
+                levels=int(levels), init=bool(init))
+
+
+@pytest.mark.parametrize("case", pyramid_cases())
+def test_pyramid_restatement_matches_reference_golden(orc, case):
+    """The coarse-to-fine loop of PMHuberStereo::disparityMap (levels > 1), bit for bit."""
+    g = load_golden(case)
+    s = pyr_spec(g)
+    res = orc.disparity_map(g["left"], g["right"], s["r"], s["dmax"], s["iters"], pp=s["pp"], views=s["views"],
+                            initdisp=g.get("initdisp"), levels=s["levels"], dump=True, fused=0)
+    n = 0
+    for (stage, it), v in res["stages"].items():
+        k = "stage_%s_%d" % (stage, it)
+        if k in g:
+            assert bits_equal(v, g[k]).all(), (case, stage)
+            n += 1
+    assert n == 2 * s["levels"]
+    for k in ("dmap", "normal", "planesL", "planesR"):
+        assert bits_equal(res[k], g[k]).all(), (case, k)
+    W1, H1 = g["k_pyrdown"].shape[1], g["k_pyrdown"].shape[0]
+    assert (orc.pyrdown(g["left"], W1, H1) == g["k_pyrdown"]).all()
+    up = np.float32(s["W"]) / np.float32(W1)
+    assert bits_equal(orc.pyrup_mul(g["k_pyr_d1"], s["W"], s["H"], [up] * 4), g["k_pyrup_d"]).all()
+    assert bits_equal(orc.pyrup_mul(g["k_pyr_n1"], s["W"], s["H"], [1.0] * 4), g["k_pyrup_n"]).all()
+
+
+@pytest.mark.parametrize("Wi,Hi,Wo,Ho", [(37, 23, 12, 8), (5, 3, 1, 1), (8, 6, 19, 13), (64, 1, 22, 1)])
+def test_pyramid_kernels_match_reference_live(orc, ref, Wi, Hi, Wo, Ho):
+    """pyrdown and pyrup_mul4f for down- and upsampling and degenerate sizes"""
+    rng = np.random.default_rng(Wi * 100 + Ho)
+    img = rng.integers(0, 256, (Hi, Wi, 4), dtype=np.uint8)
+    assert (orc.pyrdown(img, Wo, Ho) == ref.pyrdown(img, Wo, Ho)).all()
+    f1 = rng.standard_normal((Hi, Wi)).astype(np.float32)
+    f4 = rng.standard_normal((Hi, Wi, 4)).astype(np.float32)
+    mul = [1.7, -0.5, 3.0, 1.0]
+    assert bits_equal(orc.pyrup_mul(f1, Wo, Ho, mul), ref.pyrup_mul(f1, Wo, Ho, mul)).all()
+    assert bits_equal(orc.pyrup_mul(f4, Wo, Ho, mul), ref.pyrup_mul(f4, Wo, Ho, mul)).all()
