@@ -16,12 +16,13 @@ PP_NONE, PP_LRCHECK, PP_LRCHECK_FILL = 0, 1, 2
 # every exported symbol of include/cvtpm.h
 SYMBOLS = [
     "pm_options_default", "pm_create", "pm_destroy", "pm_last_error", "pm_status_string",
-    "pm_disparity_map", "pm_disparity_map_device", "pm_set_counting", "pm_get_counters",
+    "pm_disparity_map", "pm_disparity_map_device", "pm_depth_map", "pm_depth_map_device", "pm_set_counting", "pm_get_counters",
     "pm_set_profiling", "pm_get_phase_times", "pm_measure_fp32_peak",
     "pm_disparity_map_batch_device",
     "pm_k_prep", "pm_k_init", "pm_k_cost", "pm_k_klt", "pm_k_propagate", "pm_k_normal_depth",
     "pm_rof_scratch_bytes", "pm_k_rof", "pm_k_rof_static", "pm_k_consistency", "pm_k_to_disparity", "pm_k_fill_depthmap",
     "pm_k_fill_normalmap", "pm_k_disparity_to_normal", "pm_k_pyrdown", "pm_k_pyrup_mul", "pm_pyramid_size",
+    "pm_k_fill_state", "pm_k_huber", "pm_k_prep_raw",
     "pm_rng_floats", "pm_expf_host", "pm_sinf_host", "pm_cosf_host", "pm_acospif_host",
     "pm_exit_threshold_host", "pm_scene_generate",
 ]
@@ -65,6 +66,9 @@ def lib():
         "pm_status_string": (C.c_char_p, [i32]),
         "pm_disparity_map": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, i32, vp, vp, vp, vp, vp, vp]),
         "pm_disparity_map_device": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, i32, vp, vp, vp, vp, vp, vp, vp]),
+        "pm_depth_map": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, f32, i32, vp, vp, vp, vp, vp, vp]),
+        "pm_depth_map_device": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, f32, i32, vp, vp, vp, vp, vp, vp,
+                                      vp]),
         "pm_set_counting": (i32, [vp, i32]),
         "pm_get_counters": (i32, [vp, C.POINTER(C.c_uint64)]),
         "pm_set_profiling": (i32, [vp, i32]),
@@ -86,6 +90,9 @@ def lib():
         "pm_k_fill_depthmap": (i32, [vp, vp, i32, i32, f32, vp]),
         "pm_k_fill_normalmap": (i32, [vp, vp, i32, i32, i32, vp]),
         "pm_k_disparity_to_normal": (i32, [vp, vp, i32, i32, vp]),
+        "pm_k_fill_state": (i32, [vp, vp, i32, i32, f32, i32, vp]),
+        "pm_k_huber": (i32, [vp, vp, vp, C.POINTER(C.c_float), f32, i32, i32, i32, vp, vp]),
+        "pm_k_prep_raw": (i32, [vp, i32, i32, sz, f32, vp, vp, vp, vp]),
         "pm_k_pyrdown": (i32, [vp, i32, i32, vp, sz, i32, i32, vp]),
         "pm_k_pyrup_mul": (i32, [vp, i32, i32, vp, i32, i32, i32, C.POINTER(C.c_float), vp]),
         "pm_pyramid_size": (i32, [i32, i32]),

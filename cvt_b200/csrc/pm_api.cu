@@ -154,6 +154,7 @@ struct Layout {
         ctr, errf,                                                              // counters (4 u64), error int
         img0, img1, disp, dmap, nmap, initd, initn,                             // staging for host entry
         initdR, initnR,                                                         // right-view init (pyramid)
+        outpL, outpR,                                                           // plane outputs for host entry
         COUNT
     };
     size_t N;
@@ -188,6 +189,8 @@ Layout layout(int W, int H, size_t stride)
     put(Layout::initn, L.N * 16);
     put(Layout::initdR, L.N * 4);
     put(Layout::initnR, L.N * 16);
+    put(Layout::outpL, L.N * 16);
+    put(Layout::outpR, L.N * 16);
     L.total = o;
     return L;
 }
@@ -334,6 +337,144 @@ int run_level(pm_handle* h, void* ws, const Layout& L, const uint8_t* left, cons
         swap = 1 - swap;
     }
     return PM_OK;
+}
+
+// PMHuberStereo::depthMap (PMHuberStereo.cpp:145-347) on device buffers in `ws`: the kernels read
+// the images themselves as colour (:203-204), the diffusion tensors use alpha 12 (:152), each
+// iteration smooths the gap-filled planes (pmhstereo_fill_state) with the tensor-weighted Huber
+// model (eps 1e-4, 40 steps, :273-296), theta starts at 1e-3 and follows :320-323, the iteration
+// count is not made odd, and outputs are scaled by dscale (1 / dmax when dscale <= 0, :164-165).
+// The occlusion maps of :271 and :289 feed nothing and are not computed.
+int run_depth(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int r,
+              float dmax, int iterations, float dscale, int pp, float* dmap, float4* normal, const float* initdisp,
+              const float4* initnormal, float4* planesL, float4* planesR, cudaStream_t st)
+{
+    const pm_options& o = h->opt;
+    const int views = o.views;
+    const int F = o.fused;
+    const Layout L = layout(W, H, stride);
+    const size_t N = L.N;
+    const float HUBEREPS = 0.0001f, THETASCALE_D = 15.0f, THETABIAS_D = 2.0f, THETASCALE = 10.0f;   // :154-161
+    if (dscale <= 0.0f) dscale = 1.0f / dmax;
+    float4 *Lc = at<float4>(ws, L, Layout::Lbw), *Rc = at<float4>(ws, L, Layout::Rbw);
+    float4 *Lg = at<float4>(ws, L, Layout::Lg), *Rg = at<float4>(ws, L, Layout::Rg);
+    float4 *LDT = at<float4>(ws, L, Layout::LDT), *RDT = at<float4>(ws, L, Layout::RDT);
+    float4 *Ls = at<float4>(ws, L, Layout::Ls), *Rs = at<float4>(ws, L, Layout::Rs), *tmp = at<float4>(ws, L, Layout::tmp);
+    float4* mL[2] = {at<float4>(ws, L, Layout::mL0), at<float4>(ws, L, Layout::mL1)};
+    float4* mR[2] = {at<float4>(ws, L, Layout::mR0), at<float4>(ws, L, Layout::mR1)};
+    float4* chk = at<float4>(ws, L, Layout::chk);
+    int *vb1c = at<int>(ws, L, Layout::vb1c), *vb2c = at<int>(ws, L, Layout::vb2c);
+    unsigned long long *vb1s = at<unsigned long long>(ws, L, Layout::vb1s), *vb2s = at<unsigned long long>(ws, L, Layout::vb2s);
+    void* pds = at<void>(ws, L, Layout::rof);
+    unsigned long long* ctr = at<unsigned long long>(ws, L, Layout::ctr);
+    int* errf = at<int>(ws, L, Layout::errf);
+
+    PM_CUDA(h, cudaMemsetAsync(ctr, 0, 64, st));
+    PM_CUDA(h, cudaMemsetAsync(errf, 0, 64, st));
+    h->ev_used = 0;
+    prof_mark(h, st, PM_PHASE_PREP, 0);
+    launch_prep(left, stride, W, H, r, F, Lc, Lg, LDT, st, 12.0f, 1);   // :184-190
+    launch_prep(right, stride, W, H, r, F, Rc, Rg, views == 2 ? RDT : nullptr, st, 12.0f, 1);
+    PM_CUDA(h, cudaMemsetAsync(Ls, 0, N * 16, st));   // :193-194
+    PM_CUDA(h, cudaMemsetAsync(Rs, 0, N * 16, st));
+    launch_view_clear(vb1c, vb1s, N, st);
+    launch_view_clear(vb2c, vb2s, N, st);   // :212
+    float4* texL = at<float4>(ws, L, Layout::texL);
+    float4* texR = at<float4>(ws, L, Layout::texR);
+    launch_pack_tex(texL, Lc, Lg, W, H, st);
+    launch_pack_tex(texR, Rc, Rg, W, H, st);
+    prof_mark(h, st, PM_PHASE_PREP, 6);
+    int nl = 0;
+    const float4* initn = initnormal;
+    if (initdisp && !initnormal) {
+        float4* nrm = at<float4>(ws, L, Layout::nrm);
+        launch_disparity_to_normal(nrm, initdisp, W, H, st);   // :363-365
+        initn = nrm;
+        nl++;
+    }
+    const ViewData VL = make_view(texL, texR, W, H, r);
+    const ViewData VR = make_view(texR, texL, W, H, r);
+    launch_init(mL[0], VL, dmax, 1, initdisp, initn, F, st);   // :206-207
+    nl += window_kernel_launches(F, false);
+    if (views == 2) {
+        launch_init(mR[0], VR, dmax, 0, nullptr, nullptr, F, st);
+        nl += window_kernel_launches(F, false);
+    }
+    prof_mark(h, st, PM_PHASE_INIT, nl);
+    const int pd_launches = (o.rof_iters > 0 && o.rof_iters % 2 == 0) ? o.rof_iters : o.rof_iters + 1;
+    float theta = 1e-3f;   // :163
+    int swap = 0;
+    for (int iter = 0; iter < iterations; iter++) {
+        const float l = theta * THETASCALE_D + THETABIAS_D;   // :259
+        const float4 lam = make_float4(l, l, l, l);
+        PropParams P;
+        P.V = VL;
+        P.out = mL[1 - swap];
+        P.old = mL[swap];
+        P.smooth = Ls;
+        P.theta = theta * THETASCALE;
+        P.dmax = dmax;
+        P.lr = 1;
+        P.iter = iter;
+        P.vin_count = views == 2 ? vb2c : nullptr;
+        P.vin_src = vb2s;
+        P.vin_planes = mR[swap];
+        P.vout_count = views == 2 ? vb1c : nullptr;
+        P.vout_src = vb1s;
+        P.counters = h->counting ? ctr : nullptr;
+        P.error = errf;
+        P.tmp_self = at<float4>(ws, L, Layout::pself);
+        P.tmp_nb = at<float4>(ws, L, Layout::pnb);
+        P.dual = 0;
+        launch_propagate(P, F, st);   // :263-264
+        if (views == 2) {
+            P.V = VR;
+            P.out = mR[1 - swap];
+            P.old = mR[swap];
+            P.smooth = Rs;
+            P.lr = 0;
+            P.vin_count = vb1c;
+            P.vin_src = vb1s;
+            P.vin_planes = mL[1 - swap];
+            P.vout_count = vb2c;
+            P.vout_src = vb2s;
+            launch_propagate(P, F, st);   // :268-269
+        }
+        prof_mark(h, st, PM_PHASE_PROPAGATE, 3 * window_kernel_launches(F, h->counting) * views);
+        launch_fill_state(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :273-274
+        launch_huber(Ls, tmp, LDT, lam, HUBEREPS, o.rof_iters, W, H, pds, st);
+        if (views == 2) {
+            launch_fill_state(tmp, mR[1 - swap], W, H, 1.0f / dmax, 0, st);   // :295-296
+            launch_huber(Rs, tmp, RDT, lam, HUBEREPS, o.rof_iters, W, H, pds, st);
+        }
+        prof_mark(h, st, PM_PHASE_SMOOTH, views * (1 + pd_launches));
+        if (iter >= 3) {   // :320-323
+            theta = ((float)iter - 3.0f) / ((float)iterations - 4.0f);
+            theta = theta * theta * theta + 1e-3f;
+        }
+        swap = 1 - swap;
+    }
+    float4* ml = mL[swap];
+    float4* mr = mR[swap];
+    if (planesL) PM_CUDA(h, cudaMemcpyAsync(planesL, ml, N * 16, cudaMemcpyDeviceToDevice, st));
+    if (planesR && views == 2) PM_CUDA(h, cudaMemcpyAsync(planesR, mr, N * 16, cudaMemcpyDeviceToDevice, st));
+    nl = 0;
+    if (pp == PM_PP_NONE) {   // :331-337
+        if (dmap) { launch_to_disparity(dmap, ml, W, H, dscale, 1, st); nl++; }
+        if (normal) { launch_fill_normalmap(normal, ml, W, H, st); nl++; }
+    } else {   // :338-345
+        launch_consistency(chk, ml, mr, W, H, o.maxdispdiff, o.maxanglediff, st);
+        nl++;
+        if (dmap) {
+            if (pp == PM_PP_LRCHECK) launch_to_disparity(dmap, chk, W, H, dscale, 1, st);
+            else launch_fill_depthmap(dmap, chk, W, H, dscale, st);
+            nl++;
+        }
+        if (normal) { launch_fill_normalmap(normal, chk, W, H, st); nl++; }
+    }
+    prof_mark(h, st, PM_PHASE_POST, nl);
+    PM_CUDA(h, cudaGetLastError());
+    return prof_collect(h, st);
 }
 
 // pyramid level sizes of a W x H pair (level 0 first); PM_EINVAL_SHAPE when a level would
@@ -609,14 +750,20 @@ int use_graph(pm_handle* h, cudaStream_t st, bool* yes)
 // the single-pair pipeline on `st`, through the handle's graph when graphs are in use
 int pipeline_on(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int r,
                 float dmax, int iterations, int pp, float* dmap, float4* normal, const float* initdisp,
-                const float4* initnormal, float4* planesL, float4* planesR, cudaStream_t st)
+                const float4* initnormal, float4* planesL, float4* planesR, cudaStream_t st, int depth = 0,
+                float dscale = 0.0f)
 {
+    auto run = [&](cudaStream_t s) {
+        if (depth)
+            return run_depth(h, ws, left, right, W, H, stride, r, dmax, iterations, dscale, pp, dmap, normal, initdisp,
+                             initnormal, planesL, planesR, s);
+        return run_pipeline(h, ws, left, right, W, H, stride, r, dmax, iterations, pp, dmap, normal, initdisp,
+                            initnormal, planesL, planesR, s);
+    };
     bool graph = false;
     int rc = use_graph(h, st, &graph);
     if (rc) return rc;
-    if (!graph)
-        return run_pipeline(h, ws, left, right, W, H, stride, r, dmax, iterations, pp, dmap, normal, initdisp,
-                            initnormal, planesL, planesR, st);
+    if (!graph) return run(st);
     const pm_options& o = h->opt;
     std::vector<uint64_t> key = {
         (uint64_t)(uintptr_t)ws, (uint64_t)(uintptr_t)left, (uint64_t)(uintptr_t)right, (uint64_t)W, (uint64_t)H,
@@ -624,12 +771,9 @@ int pipeline_on(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* righ
         (uint64_t)(uintptr_t)normal, (uint64_t)(uintptr_t)initdisp, (uint64_t)(uintptr_t)initnormal,
         (uint64_t)(uintptr_t)planesL, (uint64_t)(uintptr_t)planesR, (uint64_t)o.views, (uint64_t)o.fused,
         fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff), (uint64_t)o.rof_iters, (uint64_t)h->counting,
-        (uint64_t)o.levels};
+        (uint64_t)o.levels, (uint64_t)depth, fbits(dscale)};
     for (void* p : h->lws) key.push_back((uint64_t)(uintptr_t)p);
-    return run_graph(h, h->key1, h->exec1, key, st, [&](cudaStream_t cs) {
-        return run_pipeline(h, ws, left, right, W, H, stride, r, dmax, iterations, pp, dmap, normal, initdisp,
-                            initnormal, planesL, planesR, cs);
-    });
+    return run_graph(h, h->key1, h->exec1, key, st, run);
 }
 
 }  // namespace
@@ -772,10 +916,15 @@ int pm_get_counters(pm_handle* h, uint64_t c[4])
     return PM_OK;
 }
 
-int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
-                            int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
-                            const float* initdisp, const float* initnormal, float* planes_left, float* planes_right,
-                            void* stream)
+}  // extern "C"
+
+namespace {
+
+// single-pair entry with device buffers: disparityMap (depth = 0) or depthMap (depth = 1)
+int entry_device(pm_handle* h, int depth, float dscale, const uint8_t* left, const uint8_t* right, int W, int H,
+                 size_t stride, int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
+                 const float* initdisp, const float* initnormal, float* planes_left, float* planes_right,
+                 cudaStream_t st)
 {
     int rc = check_args(h, left, right, W, H, stride, patchsize, dispmax, iterations, pp);
     if (rc) return rc;
@@ -787,33 +936,39 @@ int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* ri
     h->H = H;
     rc = ensure_ws(h, W, H, stride);
     if (rc) return rc;
-    rc = ensure_level_ws(h, W, H);
-    if (rc) return rc;
+    if (!depth) {
+        rc = ensure_level_ws(h, W, H);
+        if (rc) return rc;
+    }
     rc = pipeline_on(h, h->ws, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap,
                      reinterpret_cast<float4*>(normalmap), initdisp, reinterpret_cast<const float4*>(initnormal),
-                     reinterpret_cast<float4*>(planes_left), reinterpret_cast<float4*>(planes_right), S(stream));
+                     reinterpret_cast<float4*>(planes_left), reinterpret_cast<float4*>(planes_right), st, depth, dscale);
     if (rc) return rc;
     if (h->counting) {
         const Layout L = layout(W, H, stride);
         unsigned long long c[4];
-        PM_CUDA(h, cudaMemcpyAsync(c, at<unsigned long long>(h->ws, L, Layout::ctr), 32, cudaMemcpyDeviceToHost, S(stream)));
-        PM_CUDA(h, cudaStreamSynchronize(S(stream)));
+        PM_CUDA(h, cudaMemcpyAsync(c, at<unsigned long long>(h->ws, L, Layout::ctr), 32, cudaMemcpyDeviceToHost, st));
+        PM_CUDA(h, cudaStreamSynchronize(st));
         for (int k = 0; k < 4; k++) h->counters[k] = c[k];
     }
     return PM_OK;
 }
 
-int pm_disparity_map(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
-                     int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
-                     const float* initdisp, const float* initnormal, float* planes_left, float* planes_right)
+// single-pair entry with host buffers: inputs staged into the workspace, outputs copied back,
+// on the legacy default stream; returns once the outputs are written
+int entry_host(pm_handle* h, int depth, float dscale, const uint8_t* left, const uint8_t* right, int W, int H,
+               size_t stride, int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
+               const float* initdisp, const float* initnormal, float* planes_left, float* planes_right)
 {
     int rc = check_args(h, left, right, W, H, stride, patchsize, dispmax, iterations, pp);
     if (rc) return rc;
     PM_CUDA(h, cudaSetDevice(h->opt.device));
     rc = ensure_ws(h, W, H, stride);
     if (rc) return rc;
-    rc = ensure_level_ws(h, W, H);
-    if (rc) return rc;
+    if (!depth) {
+        rc = ensure_level_ws(h, W, H);
+        if (rc) return rc;
+    }
     h->W = W;
     h->H = H;
     const Layout L = layout(W, H, stride);
@@ -825,20 +980,20 @@ int pm_disparity_map(pm_handle* h, const uint8_t* left, const uint8_t* right, in
     float4* dn = at<float4>(h->ws, L, Layout::nmap);
     float* di = at<float>(h->ws, L, Layout::initd);
     float4* dni = at<float4>(h->ws, L, Layout::initn);
-    float4* pl = at<float4>(h->ws, L, Layout::mL0);   // overwritten only after the copy below
+    float4* dpl = at<float4>(h->ws, L, Layout::outpL);
+    float4* dpr = at<float4>(h->ws, L, Layout::outpR);
     PM_CUDA(h, cudaMemcpyAsync(dl, left, stride * H, cudaMemcpyHostToDevice, st));
     PM_CUDA(h, cudaMemcpyAsync(dr, right, stride * H, cudaMemcpyHostToDevice, st));
     if (initdisp) PM_CUDA(h, cudaMemcpyAsync(di, initdisp, N * 4, cudaMemcpyHostToDevice, st));
     if (initnormal) PM_CUDA(h, cudaMemcpyAsync(dni, initnormal, N * 16, cudaMemcpyHostToDevice, st));
-    (void)pl;
     rc = pipeline_on(h, h->ws, dl, dr, W, H, stride, patchsize, dispmax, iterations, pp, dmap ? dd : nullptr,
-                     normalmap ? dn : nullptr, initdisp ? di : nullptr, initnormal ? dni : nullptr, nullptr, nullptr, st);
+                     normalmap ? dn : nullptr, initdisp ? di : nullptr, initnormal ? dni : nullptr,
+                     planes_left ? dpl : nullptr, planes_right ? dpr : nullptr, st, depth, dscale);
     if (rc) return rc;
     if (dmap) PM_CUDA(h, cudaMemcpyAsync(dmap, dd, N * 4, cudaMemcpyDeviceToHost, st));
     if (normalmap) PM_CUDA(h, cudaMemcpyAsync(normalmap, dn, N * 16, cudaMemcpyDeviceToHost, st));
-    if (planes_left) PM_CUDA(h, cudaMemcpyAsync(planes_left, at<float4>(h->ws, L, Layout::mL1), N * 16, cudaMemcpyDeviceToHost, st));
-    if (planes_right && h->opt.views == 2)
-        PM_CUDA(h, cudaMemcpyAsync(planes_right, at<float4>(h->ws, L, Layout::mR1), N * 16, cudaMemcpyDeviceToHost, st));
+    if (planes_left) PM_CUDA(h, cudaMemcpyAsync(planes_left, dpl, N * 16, cudaMemcpyDeviceToHost, st));
+    if (planes_right && h->opt.views == 2) PM_CUDA(h, cudaMemcpyAsync(planes_right, dpr, N * 16, cudaMemcpyDeviceToHost, st));
     if (h->counting) {
         unsigned long long c[4];
         PM_CUDA(h, cudaMemcpyAsync(c, at<unsigned long long>(h->ws, L, Layout::ctr), 32, cudaMemcpyDeviceToHost, st));
@@ -850,6 +1005,44 @@ int pm_disparity_map(pm_handle* h, const uint8_t* left, const uint8_t* right, in
     PM_CUDA(h, cudaStreamSynchronize(st));
     if (errv) return fail(h, PM_ETIMEOUT, "view-buffer insertion retried too often");
     return PM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
+                            int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
+                            const float* initdisp, const float* initnormal, float* planes_left, float* planes_right,
+                            void* stream)
+{
+    return entry_device(h, 0, 0.0f, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap, normalmap,
+                        initdisp, initnormal, planes_left, planes_right, S(stream));
+}
+
+int pm_disparity_map(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
+                     int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
+                     const float* initdisp, const float* initnormal, float* planes_left, float* planes_right)
+{
+    return entry_host(h, 0, 0.0f, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap, normalmap,
+                      initdisp, initnormal, planes_left, planes_right);
+}
+
+int pm_depth_map_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
+                        int patchsize, float dispmax, int iterations, float dscale, int pp, float* dmap,
+                        float* normalmap, const float* initdisp, const float* initnormal, float* planes_left,
+                        float* planes_right, void* stream)
+{
+    return entry_device(h, 1, dscale, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap, normalmap,
+                        initdisp, initnormal, planes_left, planes_right, S(stream));
+}
+
+int pm_depth_map(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int patchsize,
+                 float dispmax, int iterations, float dscale, int pp, float* dmap, float* normalmap,
+                 const float* initdisp, const float* initnormal, float* planes_left, float* planes_right)
+{
+    return entry_host(h, 1, dscale, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap, normalmap,
+                      initdisp, initnormal, planes_left, planes_right);
 }
 
 int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* left, const uint8_t* const* right,
@@ -1134,6 +1327,40 @@ int pm_k_disparity_to_normal(float* out, const float* disp, int W, int H, void* 
     int rc = check_shape(nullptr, W, H, 0);
     if (rc) return rc;
     launch_disparity_to_normal((float4*)out, disp, W, H, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_fill_state(float* out, const float* planes, int W, int H, float dispscale, int lr, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    if (!out || !planes || !aligned(out, 16) || !aligned(planes, 16)) return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    launch_fill_state((float4*)out, (const float4*)planes, W, H, dispscale, lr, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_huber(float* out, const float* input, const float* dt, const float lambda[4], float eps, int iters, int W,
+               int H, void* scratch, void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    if (!out || !input || !dt || !lambda || !scratch || out == input || iters < 0)
+        return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    launch_huber((float4*)out, (const float4*)input, (const float4*)dt,
+                 make_float4(lambda[0], lambda[1], lambda[2], lambda[3]), eps, iters, W, H, scratch, S(stream));
+    PM_CUDA(nullptr, cudaGetLastError());
+    return PM_OK;
+}
+
+int pm_k_prep_raw(const uint8_t* img, int W, int H, size_t stride, float alpha, float* colour, float* grad, float* dt,
+                  void* stream)
+{
+    int rc = check_shape(nullptr, W, H, 0);
+    if (rc) return rc;
+    if (!img || stride < (size_t)W * 4 || stride % 4 || !aligned(img, 4)) return fail(nullptr, PM_EINVAL_ARG, "bad image");
+    launch_prep(img, stride, W, H, 0, 0, (float4*)colour, (float4*)grad, (float4*)dt, S(stream), alpha, 1);
     PM_CUDA(nullptr, cudaGetLastError());
     return PM_OK;
 }

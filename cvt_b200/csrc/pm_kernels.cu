@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "pm_device.cuh"
 #include "pm_kernels.h"
@@ -33,14 +34,19 @@ __device__ __forceinline__ float gray_zero(const uint8_t* __restrict__ img, size
     return v.x * PM_GW_R + v.y * PM_GW_G + v.z * PM_GW_B + v.w * 0.0f;
 }
 
+// raw: bw receives the image itself (r, g, b, a), as depthMap hands it to its kernels
+// (PMHuberStereo.cpp:203-204), instead of colour and window weight sum; alpha: the diffusion
+// tensor's edge weight (24 in disparityMapAll, :416; 12 in depthMap, :152)
 template <bool F>
 __global__ void k_prep(const uint8_t* __restrict__ img, size_t stride, int W, int H, int r, float4* __restrict__ bw,
-                       float4* __restrict__ grad, float4* __restrict__ dt)
+                       float4* __restrict__ grad, float4* __restrict__ dt, float alpha, int raw)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
     const size_t i = (size_t)y * W + x;
-    if (bw) {
+    if (bw && raw) {
+        bw[i] = rgba_at(img, stride, x, y);
+    } else if (bw) {
         // pmhstereo_bilateral_weight_to_alpha (pmhstereo.cl:1462-1498)
         const float4 c = rgba_at(img, stride, x, y);
         float wsum = 0.0f;
@@ -59,10 +65,10 @@ __global__ void k_prep(const uint8_t* __restrict__ img, size_t stride, int W, in
         grad[i] = f4(gxp - g, gyp - g, gxp - gxm, gyp - gym);
     }
     if (dt) {
-        // PDDiffTensorColor (PDDiffTensor.cl:52-72), alpha 24, beta 1 (PMHuberStereo.cpp:416-417)
+        // PDDiffTensorColor (PDDiffTensor.cl:52-72), beta 1 (PMHuberStereo.cpp:417, :153)
         float dx = gxp - g, dy = gyp - g;
         const float len = sqrtf(dx * dx + dy * dy);
-        const float w = expf_(-24.0f * len);
+        const float w = expf_(-alpha * len);
         float4 d;
         if (len <= 0.001f) {
             d = f4(1.0f, 0.0f, 0.0f, 1.0f);
@@ -140,8 +146,10 @@ __global__ void k_normal_depth(float4* __restrict__ out, const float4* __restric
 // tensor-weighted, projected dual of PDDROFDiffTensor (PDDROFDiffTensor.cl:72-100) at
 // pixel (x, y); outside the image the tensor and the previous dual read as 0
 struct Dual { float4 lo, hi; };
+template <bool HUBER>
 __device__ __forceinline__ Dual rof_dual(const float4* __restrict__ u, const float4* __restrict__ p,
-                                         const float4* __restrict__ dt, int W, int H, int x, int y, bool first)
+                                         const float4* __restrict__ dt, int W, int H, int x, int y, bool first,
+                                         float eps)
 {
     const int xc = min(max(x, 0), W - 1), yc = min(max(y, 0), H - 1);
     const int xp = min(max(x + 1, 0), W - 1), yp = min(max(y + 1, 0), H - 1);
@@ -160,11 +168,22 @@ __device__ __forceinline__ Dual rof_dual(const float4* __restrict__ u, const flo
         const float DTdy = D.y * dxv[c] + D.w * dyv[c];
         a[c] = pl[c] + 4.0f * DTdx;   // SIGMA
         b[c] = ph[c] + 4.0f * DTdy;
+        if (HUBER) {   // PDDHuberDiffTensor.cl:61-63
+            a[c] = a[c] / (1.0f + 4.0f * eps);
+            b[c] = b[c] / (1.0f + 4.0f * eps);
+        }
         nrm[c] = a[c] * a[c] + b[c] * b[c];
     }
-    const float n3 = sqrtf(nrm[0] * 1.0f + nrm[1] * 1.0f + nrm[2] * 1.0f);
-    const float n4 = sqrtf(nrm[3]);
-    const float pr[4] = {fmaxf(1.0f, n3), fmaxf(1.0f, n3), fmaxf(1.0f, n3), fmaxf(1.0f, n4)};
+    float pr[4];
+    if (HUBER) {   // one norm over the four channels (PDDHuberDiffTensor.cl:66-67)
+        const float n = sqrtf(nrm[0] * 1.0f + nrm[1] * 1.0f + nrm[2] * 1.0f + nrm[3] * 1.0f);
+        pr[0] = pr[1] = pr[2] = pr[3] = fmaxf(1.0f, n);
+    } else {
+        const float n3 = sqrtf(nrm[0] * 1.0f + nrm[1] * 1.0f + nrm[2] * 1.0f);
+        const float n4 = sqrtf(nrm[3]);
+        pr[0] = pr[1] = pr[2] = fmaxf(1.0f, n3);
+        pr[3] = fmaxf(1.0f, n4);
+    }
     float l[4], h[4];
 #pragma unroll
     for (int c = 0; c < 4; c++) {
@@ -179,17 +198,19 @@ __device__ __forceinline__ Dual rof_dual(const float4* __restrict__ u, const flo
     return d;
 }
 
-// one primal-dual step (PDDROFDiffTensor.cl:102-126); first: p = q = 0
+// one primal-dual step (PDDROFDiffTensor.cl:102-126; with HUBER PDDHuberDiffTensor.cl:92-106);
+// first: p = q = 0
+template <bool HUBER>
 __global__ void k_rof_step(float4* __restrict__ unew, float4* __restrict__ pnew, float4* __restrict__ qnew,
                            const float4* __restrict__ u, const float4* __restrict__ p, const float4* __restrict__ q,
                            const float4* __restrict__ img, const float4* __restrict__ dt, float4 lam, int W, int H,
-                           int first)
+                           int first, float eps)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
-    const Dual c = rof_dual(u, p, dt, W, H, x, y, first);
-    const Dual l = rof_dual(u, p, dt, W, H, x - 1, y, first);
-    const Dual t = rof_dual(u, p, dt, W, H, x, y - 1, first);
+    const Dual c = rof_dual<HUBER>(u, p, dt, W, H, x, y, first, eps);
+    const Dual l = rof_dual<HUBER>(u, p, dt, W, H, x - 1, y, first, eps);
+    const Dual t = rof_dual<HUBER>(u, p, dt, W, H, x, y - 1, first, eps);
     const size_t i = (size_t)y * W + x;
     const float4 im = img[i], uu = u[i];
     const float4 qq = first ? f4(0, 0, 0, 0) : q[i];
@@ -374,6 +395,52 @@ __global__ void k_pyrup_mul(float* __restrict__ out, int Wo, int Ho, const float
     else reinterpret_cast<float4*>(out)[o] = f4(mul.x * v.x, mul.y * v.y, mul.z * v.z, mul.w * v.w);
 }
 
+// float to int as an x86 truncating conversion does it (cvttss2si), which is what the
+// reference's implicit float-to-int conversions compile to on its host (pmhstereo.cl:1169-1170
+// through the OpenCL-C shim): NaN and values outside the int range give INT_MIN
+__device__ __forceinline__ int f2i_x86(float f)
+{
+    if (!(f > -2147483904.0f && f < 2147483648.0f)) return INT_MIN;
+    return (int)f;
+}
+
+// pmhstereo_fill_state (pmhstereo.cl:1131-1185): a plane with a negative cost or a disparity
+// outside [0, W] takes the valid neighbour of its row (nearest left / right with cost >= 0)
+// that gives the smaller positive disparity; out = (normal, depth * dispscale) of the
+// reference view
+__global__ void k_fill_state(float4* __restrict__ out, const float4* __restrict__ planes, int W, int H,
+                             float dispscale, int lr)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const float4* row = planes + (size_t)y * W;
+    const float4 state = row[x];
+    const float cx = (float)x, cy = (float)y;
+    const int sidesign = lr ? -1 : 1;
+    const float disp = (transform_x(state, cx, cy) - cx) * (float)sidesign;
+    float4 val;
+    if (state.w < 0 || disp < 0 || disp > (float)W) {
+        float4 l = f4(-1.0f, -1.0f, -1.0f, -1.0f), r = l;
+        for (int xx = x - 1; l.w < 0 && xx >= 0; xx--) l = row[xx];
+        for (int xx = x + 1; r.w < 0 && xx < W; xx++) r = row[xx];
+        if (l.w >= 0 && r.w >= 0) {
+            int dl = f2i_x86((float)sidesign * (transform_x(l, cx, cy) - cx));
+            int dr = f2i_x86((float)sidesign * (transform_x(r, cx, cy) - cx));
+            if (dl <= 0) dl = W;
+            if (dr <= 0) dr = W;
+            val = dl <= dr ? l : r;
+        } else {
+            val = r.w < 0 ? l : r;
+        }
+    } else {
+        val = state;
+    }
+    if (!(fin(val.x) && fin(val.y))) { val.x = 0.0f; val.y = 0.0f; }
+    float4 nd = to_ref_normal_depth(val, cx, cy, lr);
+    nd.w = nd.w * dispscale;
+    out[(size_t)y * W + x] = nd;
+}
+
 // the top-left Wd x Hd corner of a field with Ws columns (CH floats per texel)
 template <int CH>
 __global__ void k_crop(float* __restrict__ dst, int Wd, int Hd, const float* __restrict__ src, int Ws)
@@ -462,11 +529,11 @@ double fma_peak_flops_per_iter() { return 2.0 * FMA_CHAINS * FMA_UNROLL; }
 // ---- launchers ----------------------------------------------------------------------
 
 void launch_prep(const uint8_t* img, size_t stride, int W, int H, int r, int fused, float4* bw, float4* grad,
-                 float4* dt, cudaStream_t st)
+                 float4* dt, cudaStream_t st, float alpha, int raw)
 {
     const dim3 b(32, 4);
-    if (fused) k_prep<true><<<grid2d(W, H, b), b, 0, st>>>(img, stride, W, H, r, bw, grad, dt);
-    else k_prep<false><<<grid2d(W, H, b), b, 0, st>>>(img, stride, W, H, r, bw, grad, dt);
+    if (fused) k_prep<true><<<grid2d(W, H, b), b, 0, st>>>(img, stride, W, H, r, bw, grad, dt, alpha, raw);
+    else k_prep<false><<<grid2d(W, H, b), b, 0, st>>>(img, stride, W, H, r, bw, grad, dt, alpha, raw);
 }
 
 void launch_init(float4* out, const ViewData& V, float dmax, int lr, const float* initdisp, const float4* initnormal,
@@ -514,8 +581,10 @@ void launch_normal_depth(float4* out, const float4* planes, int W, int H, float 
 
 size_t rof_scratch_bytes(int W, int H) { return (size_t)W * H * sizeof(float4) * (1 + 2 + 2 + 1 + 1); }
 
-void launch_rof(float4* out, const float4* input, const float4* dt, float4 lam, int iters, int W, int H, void* scratch,
-                cudaStream_t st)
+namespace {
+template <bool HUBER>
+void launch_pd(float4* out, const float4* input, const float4* dt, float4 lam, float eps, int iters, int W, int H,
+               void* scratch, cudaStream_t st)
 {
     const size_t N = (size_t)W * H;
     float4* ut = static_cast<float4*>(scratch);
@@ -529,9 +598,24 @@ void launch_rof(float4* out, const float4* input, const float4* dt, float4 lam, 
     for (int k = 0; k < steps; k++) {
         float4* unew = ((steps - 1 - k) % 2 == 0) ? out : ut;
         const int pi = k & 1;
-        k_rof_step<<<g, b, 0, st>>>(unew, p[pi], q[pi], ucur, p[1 - pi], q[1 - pi], input, dt, lam, W, H, k == 0);
+        k_rof_step<HUBER><<<g, b, 0, st>>>(unew, p[pi], q[pi], ucur, p[1 - pi], q[1 - pi], input, dt, lam, W, H,
+                                           k == 0, eps);
         ucur = unew;
     }
+}
+}  // namespace
+
+void launch_rof(float4* out, const float4* input, const float4* dt, float4 lam, int iters, int W, int H, void* scratch,
+                cudaStream_t st)
+{
+    launch_pd<false>(out, input, dt, lam, 0.0f, iters, W, H, scratch, st);
+}
+
+// PDOptCL::denoiseDiffusionTensorHuber_PDD (PDOptCL.cpp:1170-1226): the same buffer schedule
+void launch_huber(float4* out, const float4* input, const float4* dt, float4 lam, float eps, int iters, int W, int H,
+                  void* scratch, cudaStream_t st)
+{
+    launch_pd<true>(out, input, dt, lam, eps, iters, W, H, scratch, st);
 }
 
 void launch_consistency(float4* out, const float4* L, const float4* R, int W, int H, float maxdd, float maxad,
@@ -577,6 +661,12 @@ void launch_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int H
     const dim3 b(32, 8);
     if (channels == 1) k_pyrup_mul<1><<<grid2d(Wo, Ho, b), b, 0, st>>>(out, Wo, Ho, in, Wi, Hi, mul);
     else k_pyrup_mul<4><<<grid2d(Wo, Ho, b), b, 0, st>>>(out, Wo, Ho, in, Wi, Hi, mul);
+}
+
+void launch_fill_state(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st)
+{
+    const dim3 b(32, 8);
+    k_fill_state<<<grid2d(W, H, b), b, 0, st>>>(out, planes, W, H, dispscale, lr);
 }
 
 void launch_crop(float* dst, int Wd, int Hd, const float* src, int Ws, int channels, cudaStream_t st)

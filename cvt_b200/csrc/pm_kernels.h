@@ -39,8 +39,10 @@ struct PropParams {
     int dual;                       // the window-loop kernels run as two variants (pm_window.cuh)
 };
 
+// prep of disparityMapAll (bw = colour + window weight sum, tensor edge weight alpha = 24) or,
+// with raw, of depthMap (bw = the image as floats, alpha = 12)
 void launch_prep(const uint8_t* img, size_t stride, int W, int H, int r, int fused, float4* bw, float4* grad,
-                 float4* dt, cudaStream_t st);
+                 float4* dt, cudaStream_t st, float alpha = 24.0f, int raw = 0);
 void launch_init(float4* out, const ViewData& V, float dmax, int lr, const float* initdisp, const float4* initnormal,
                  int fused, cudaStream_t st);
 void launch_cost(float* cost, const float4* planes, const ViewData& V, float mincost, int fused, cudaStream_t st);
@@ -51,6 +53,9 @@ void launch_propagate(const PropParams& P, int fused, cudaStream_t st);
 inline int window_kernel_launches(int fused, bool counting) { return fused && !counting ? 2 : 1; }
 void launch_normal_depth(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st);
 size_t rof_scratch_bytes(int W, int H);
+void launch_huber(float4* out, const float4* input, const float4* dt, float4 lam, float eps, int iters, int W, int H,
+                  void* scratch, cudaStream_t st);
+void launch_fill_state(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st);
 void launch_rof(float4* out, const float4* input, const float4* dt, float4 lam, int iters, int W, int H, void* scratch,
                 cudaStream_t st);
 void launch_consistency(float4* out, const float4* L, const float4* R, int W, int H, float maxdd, float maxad,

@@ -78,9 +78,21 @@ class PMHuberStereo:
                       initdisparity=None, initnormalmap=None, planes=False, stream=None):
         """Returns dmap, or a dict {dmap, normal?, planes_left?, planes_right?} when
         normalmap or planes is requested.  left/right: (H, W, 4) uint8."""
+        return self._run(None, left, right, patchsize, disparitymax, iterations, pp, normalmap, initdisparity,
+                         initnormalmap, planes, stream)
+
+    def depth_map(self, left, right, patchsize, depthmax, iterations, dscale=-1.0, pp=PP_LRCHECK, normalmap=False,
+                  initdisparity=None, initnormalmap=None, planes=False, stream=None):
+        """PMHuberStereo::depthMap (PMHuberStereo.cpp:145-347): the Huber-smoothed variant; dmap is
+        the disparity times dscale (dscale <= 0: 1 / depthmax).  Returns as disparity_map."""
+        return self._run(float(dscale), left, right, patchsize, depthmax, iterations, pp, normalmap, initdisparity,
+                         initnormalmap, planes, stream)
+
+    def _run(self, dscale, left, right, patchsize, disparitymax, iterations, pp, normalmap, initdisparity,
+             initnormalmap, planes, stream):
         if _is_torch(left):
             return self._device(left, right, patchsize, disparitymax, iterations, pp, normalmap, initdisparity,
-                                initnormalmap, planes, stream)
+                                initnormalmap, planes, stream, dscale)
         L = _lib.lib()
         left = np.ascontiguousarray(left, np.uint8)
         right = np.ascontiguousarray(right, np.uint8)
@@ -97,8 +109,13 @@ class PMHuberStereo:
         def p(a):
             return None if a is None else a.ctypes.data
 
-        _lib.check(L.pm_disparity_map(self._h, left.ctypes.data, right.ctypes.data, W, H, W * 4, int(patchsize),
-                                      float(disparitymax), int(iterations), int(pp), dmap.ctypes.data, p(nmap),
+        if dscale is None:
+            _lib.check(L.pm_disparity_map(self._h, left.ctypes.data, right.ctypes.data, W, H, W * 4, int(patchsize),
+                                          float(disparitymax), int(iterations), int(pp), dmap.ctypes.data, p(nmap),
+                                          p(idisp), p(inorm), p(pl), p(pr)), self._h)
+        else:
+            _lib.check(L.pm_depth_map(self._h, left.ctypes.data, right.ctypes.data, W, H, W * 4, int(patchsize),
+                                      float(disparitymax), int(iterations), dscale, int(pp), dmap.ctypes.data, p(nmap),
                                       p(idisp), p(inorm), p(pl), p(pr)), self._h)
         if not normalmap and not planes:
             return dmap
@@ -146,7 +163,8 @@ class PMHuberStereo:
             return dm
         return [{"dmap": d, "planes_left": a, "planes_right": b} for d, a, b in zip(dm, pl, pr)]
 
-    def _device(self, left, right, patchsize, dmax, iterations, pp, normalmap, initd, initn, planes, stream):
+    def _device(self, left, right, patchsize, dmax, iterations, pp, normalmap, initd, initn, planes, stream,
+                dscale=None):
         import torch
 
         L = _lib.lib()
@@ -167,9 +185,14 @@ class PMHuberStereo:
         def p(t):
             return None if t is None else t.data_ptr()
 
-        _lib.check(L.pm_disparity_map_device(self._h, p(left), p(right), W, H, W * 4, int(patchsize), float(dmax),
-                                             int(iterations), int(pp), p(dmap), p(nmap), p(initd), p(initn), p(pl),
-                                             p(pr), st), self._h)
+        if dscale is None:
+            _lib.check(L.pm_disparity_map_device(self._h, p(left), p(right), W, H, W * 4, int(patchsize), float(dmax),
+                                                 int(iterations), int(pp), p(dmap), p(nmap), p(initd), p(initn), p(pl),
+                                                 p(pr), st), self._h)
+        else:
+            _lib.check(L.pm_depth_map_device(self._h, p(left), p(right), W, H, W * 4, int(patchsize), float(dmax),
+                                             int(iterations), dscale, int(pp), p(dmap), p(nmap), p(initd), p(initn),
+                                             p(pl), p(pr), st), self._h)
         if not normalmap and not planes:
             return dmap
         out = {"dmap": dmap}

@@ -2,7 +2,9 @@
  * Drop-in replacement for cvt::PMHuberStereo (cvt/vision/PMHuberStereo.h:36-110 in
  * phheise/cvt), header-only, over the C ABI of cvtpm.h (libcvtpm.so).
  *
- * The class keeps the reference's names and signatures:
+ * The class keeps the reference's names and signatures (disparityMap below, and
+ * depthMap(dmap, left, right, patchsize, depthmax, iterations, dscale = -1, pp, normalmap,
+ * initdisparity, initnormalmap), PMHuberStereo.h:50-51):
  *   void disparityMap(Image& dmap, const Image& left, const Image& right, size_t patchsize,
  *                     float disparitymax, size_t iterations,
  *                     DisparityPostProcessing pp = DISPARITY_PP_LRCHECK, Image* normalmap = NULL,
@@ -120,6 +122,35 @@ class PMHuberStereo {
         check(pm_disparity_map(_h, pl, pr, (int)w, (int)h, sl, (int)patchsize, disparitymax, (int)iterations, (int)pp,
                                pd, pn, initdisparity ? idisp.data() : NULL, initnormalmap ? inorm.data() : NULL, NULL,
                                NULL));
+    }
+
+    // PMHuberStereo::depthMap (PMHuberStereo.h:50-51, PMHuberStereo.cpp:145-347): dmap holds the
+    // disparity times dscale (dscale <= 0: 1 / depthmax)
+    void depthMap(Image& dmap, const Image& left, const Image& right, size_t patchsize, float depthmax,
+                  size_t iterations, float dscale = -1.0f, DisparityPostProcessing pp = DISPARITY_PP_LRCHECK,
+                  Image* normalmap = NULL, const Image* initdisparity = NULL, const Image* initnormalmap = NULL)
+    {
+        if (left.width() != right.width() || left.height() != right.height() ||
+            left.format() != IFormat::RGBA_UINT8 || right.format() != IFormat::RGBA_UINT8)
+            throw Exception("Left/Right stereo images inconsistent or incompatible memory type");
+        const size_t w = left.width(), h = left.height();
+        size_t sl, sr, sd, sn = 0;
+        const uint8_t* pl = left.map(&sl);
+        const uint8_t* pr = right.map(&sr);
+        if (sl != sr) throw Exception("Left/Right stereo images have different strides");
+        dmap.reallocate(w, h, IFormat::GRAY_FLOAT);
+        float* pd = reinterpret_cast<float*>(dmap.map(&sd));
+        float* pn = NULL;
+        if (normalmap) {
+            normalmap->reallocate(w, h, IFormat::RGBA_FLOAT);
+            pn = reinterpret_cast<float*>(normalmap->map(&sn));
+        }
+        std::vector<float> idisp, inorm;
+        if (initdisparity) idisp = dense(*initdisparity, IFormat::GRAY_FLOAT, w, h);
+        if (initnormalmap) inorm = dense(*initnormalmap, IFormat::RGBA_FLOAT, w, h);
+        check(pm_depth_map(_h, pl, pr, (int)w, (int)h, sl, (int)patchsize, depthmax, (int)iterations, dscale, (int)pp,
+                           pd, pn, initdisparity ? idisp.data() : NULL, initnormalmap ? inorm.data() : NULL, NULL,
+                           NULL));
     }
 
   private:

@@ -97,6 +97,21 @@ int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* ri
                             float* normalmap, const float* initdisp, const float* initnormal, float* planes_left,
                             float* planes_right, void* stream);
 
+/* PMHuberStereo::depthMap (PMHuberStereo.cpp:145-347), the Huber-smoothed variant: its kernels
+ * read the images themselves as colour, the diffusion tensors use alpha 12, each iteration
+ * smooths the gap-filled planes (pmhstereo_fill_state) with the tensor-weighted Huber model
+ * (PDDHuberDiffTensor, eps 1e-4), theta follows :320-323, the iteration count is used as given
+ * (not made odd), and dmap is the disparity times dscale (dscale <= 0: 1 / dispmax, :164-165).
+ * Arguments otherwise as pm_disparity_map / pm_disparity_map_device; pyramid levels do not
+ * apply. */
+int pm_depth_map(pm_handle* h, const uint8_t* left, const uint8_t* right, int width, int height, size_t stride,
+                 int patchsize, float dispmax, int iterations, float dscale, int pp, float* dmap, float* normalmap,
+                 const float* initdisp, const float* initnormal, float* planes_left, float* planes_right);
+int pm_depth_map_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int width, int height,
+                        size_t stride, int patchsize, float dispmax, int iterations, float dscale, int pp, float* dmap,
+                        float* normalmap, const float* initdisp, const float* initnormal, float* planes_left,
+                        float* planes_right, void* stream);
+
 /* Window-sample counters of the last pm_disparity_map* call on this handle when
  * counting was requested with pm_set_counting(h, 1): [0] cost-window samples,
  * [1] Gauss-Newton window samples, [2] cost evaluations that entered the window,
@@ -193,6 +208,18 @@ int pm_k_to_disparity(float* out, const float* planes, int width, int height, fl
 int pm_k_fill_depthmap(float* out, const float* planes, int width, int height, float scale, void* stream);
 int pm_k_fill_normalmap(float* out, const float* planes, int width, int height, int lr, void* stream);
 int pm_k_disparity_to_normal(float* out, const float* disp, int width, int height, void* stream);
+/* pmhstereo_fill_state (pmhstereo.cl:1131-1185, run by PMHuberStereo::convertFillNormalDisparity,
+ * PMHuberStereo.cpp:606-614): planes -> (normal, depth * dispscale) with gaps filled from the row */
+int pm_k_fill_state(float* out, const float* planes, int width, int height, float dispscale, int lr, void* stream);
+/* PDOptCL::denoiseDiffusionTensorHuber_PDD (PDOptCL.cpp:1170-1226): `iters` steps of
+ * PDDHuberDiffTensor (PDDHuberDiffTensor.cl:38-107) from u = input, p = q = 0.
+ * scratch: device buffer of pm_rof_scratch_bytes(width, height) bytes. */
+int pm_k_huber(float* out, const float* input, const float* dt, const float lambda[4], float eps, int iters,
+               int width, int height, void* scratch, void* stream);
+/* prep of depthMap (PMHuberStereo.cpp:184-190, :203-204): colour = the image as floats
+ * (r, g, b, a), gradients, diffusion tensor with edge weight alpha (beta 1); any output may be NULL */
+int pm_k_prep_raw(const uint8_t* img, int width, int height, size_t stride, float alpha, float* colour, float* grad,
+                  float* dt, void* stream);
 /* pyrdown (cvt/cl/kernel/pyr/pyrdown.cl, run by CLPyramid::pyrDown, cvt/cl/CLPyramid.cpp:73-78):
  * RGBA8 in_width x in_height (rows of `stride` bytes) -> RGBA8 out_width x out_height (tight
  * rows), each output texel the linear sample at (Wi/Wo (x + 0.5), Hi/Ho (y + 0.5)) */

@@ -6,7 +6,8 @@ cpu_baseline leg:
 * oracle/liboracle.so      the CPU restatement (pm_oracle.cpp), always;
 * oracle/_ref/libpmref.so  the reference's own kernel sources
                            (cvt/cl/kernel/pmhstereo.cl, PDDiffTensor.cl,
-                           PDDROFDiffTensor.cl, pyr/pyrdown.cl, pyr/pyrupmul.cl)
+                           PDDROFDiffTensor.cl, PDDHuberDiffTensor.cl,
+                           pyr/pyrdown.cl, pyr/pyrupmul.cl)
                            rewritten by translate.py and
                            compiled against clshim.h, when the reference tree is
                            present (it is not on GPU machines; the built .so
@@ -49,7 +50,7 @@ def build_ref(force=False, kernel_dir=REF_KERNELS):
     if not os.path.isdir(kernel_dir):
         return out if os.path.exists(out) else None
     os.makedirs(refdir, exist_ok=True)
-    cls = ["pmhstereo.cl", "PDDiffTensor.cl", "PDDROFDiffTensor.cl"]
+    cls = ["pmhstereo.cl", "PDDiffTensor.cl", "PDDROFDiffTensor.cl", "PDDHuberDiffTensor.cl"]
     deps = [os.path.join(kernel_dir, f) for f in cls + ["RNG.cl", "MWC64X.cl", "Matrix3.cl"]]
     pyr = ["pyrdown.cl", "pyrupmul.cl"]
     deps += [os.path.join(kernel_dir, "pyr", f) for f in pyr]

@@ -35,6 +35,9 @@ struct PmKernels {
     int (*disparity_to_normal)(float*, const float*, int, int);
     int (*pyrdown)(uint8_t*, int, int, const uint8_t*, int, int);
     int (*pyrup_mul)(float*, int, int, const float*, int, int, int, const float*);
+    int (*prep_raw)(const uint8_t*, int, int, int, float, float*, float*, float*);
+    int (*fill_state)(float*, const float*, int, int, float, int);
+    int (*huber)(float*, const float*, const float*, const float*, float, int, int, int);
 };
 
 /* Optional per-stage dump: called with a stage name and a W*H*4 float field.  Stages of a
@@ -232,6 +235,91 @@ static inline int pm_host_disparity_map(const PmKernels& K, const uint8_t* left,
         if (dmap) {
             if (pp == 1) K.to_disparity(dmap, chk.data(), W, H, 1.0f, 1);
             else K.fill_depthmap(dmap, chk.data(), W, H, 1.0f);
+        }
+        if (normal) K.fill_normalmap(normal, chk.data(), W, H, 1);
+    }
+    return 0;
+}
+
+/* PMHuberStereo::depthMap (PMHuberStereo.cpp:145-347): the Huber-smoothed variant.  Its kernels
+ * read the images themselves as colour (no window weight sum, :203-204), the diffusion tensors use
+ * alpha = 12 (:152), the smoothing is denoiseDiffusionTensorHuber_PDD (eps 1e-4, 40 steps) of the
+ * gap-filled planes (convertFillNormalDisparity, :273, :295), theta starts at 1e-3 and follows
+ * :320-323, the iteration count is not made odd, and the disparity is scaled by dscale (1 / dmax
+ * when dscale <= 0, :164-165).  The occlusion maps of :271 and :289 feed nothing and are left out. */
+static inline int pm_host_depth_map(const PmKernels& K, const uint8_t* left, const uint8_t* right, int W, int H,
+                                    int stride, int r, float dmax, int iterations, float dscale, int pp, int views,
+                                    float* dmap, float* normal, const float* initdisp, const float* initnormal,
+                                    float* planesL, float* planesR, int fused, int64_t* counters, PmDumpFn dump,
+                                    void* user)
+{
+    if (W <= 0 || H <= 0 || r < 0 || iterations < 0) return -1;
+    if (views != 1 && views != 2) return -1;
+    if (views == 1 && pp != 0) return -1;
+    const float HUBEREPS = 0.0001f, THETASCALE_D = 15.0f, THETABIAS_D = 2.0f, THETASCALE = 10.0f;   /* :154-161 */
+    float theta = 1e-3f;                                                                           /* :163 */
+    if (dscale <= 0.0f) dscale = 1.0f / dmax;
+    const size_t N = (size_t)W * H;
+    std::vector<float> Lc(4 * N), Rc(4 * N), Lg(4 * N), Rg(4 * N), LDT(4 * N), RDT(4 * N);
+    std::vector<float> Ls(4 * N, 0.0f), Rs(4 * N, 0.0f), tmp(4 * N);
+    std::vector<float> m1[2] = {std::vector<float>(4 * N), std::vector<float>(4 * N)};
+    std::vector<float> m2[2] = {std::vector<float>(4 * N), std::vector<float>(4 * N)};
+    std::vector<int32_t> vb1n(N, 0), vb2n(N, 0);
+    std::vector<float> vb1v(8 * N, 0.0f), vb2v(8 * N, 0.0f);
+    K.prep_raw(left, W, H, stride, 12.0f, Lc.data(), Lg.data(), LDT.data());    /* :184-190 */
+    K.prep_raw(right, W, H, stride, 12.0f, Rc.data(), Rg.data(), RDT.data());
+    std::vector<float> nrm;
+    const float* initn = initnormal;
+    if (initdisp && !initnormal) {                                             /* :363-365 */
+        nrm.resize(4 * N);
+        K.disparity_to_normal(nrm.data(), initdisp, W, H);
+        initn = nrm.data();
+    }
+    K.init(m1[0].data(), Lc.data(), Rc.data(), Lg.data(), Rg.data(), W, H, r, dmax, 1, initdisp, initn, fused);
+    if (views == 2)
+        K.init(m2[0].data(), Rc.data(), Lc.data(), Rg.data(), Lg.data(), W, H, r, dmax, 0, nullptr, nullptr, fused);
+    if (dump) { dump("init_left", -1, W, H, m1[0].data(), user); if (views == 2) dump("init_right", -1, W, H, m2[0].data(), user); }
+    int swap = 0;
+    for (int iter = 0; iter < iterations; iter++) {
+        const float l = theta * THETASCALE_D + THETABIAS_D;                                               /* :259 */
+        const float lam[4] = {l, l, l, l};
+        std::fill(vb1n.begin(), vb1n.end(), 0);                                                           /* :261 */
+        K.propagate(m1[1 - swap].data(), m1[swap].data(), Lc.data(), Rc.data(), Lg.data(), Rg.data(), Ls.data(),
+                    theta * THETASCALE, W, H, r, dmax, 1, iter, vb2n.data(), vb2v.data(),
+                    views == 2 ? vb1n.data() : nullptr, vb1v.data(), nullptr, fused, counters);
+        if (views == 2) {
+            std::fill(vb2n.begin(), vb2n.end(), 0);                                                       /* :266 */
+            K.propagate(m2[1 - swap].data(), m2[swap].data(), Rc.data(), Lc.data(), Rg.data(), Lg.data(), Rs.data(),
+                        theta * THETASCALE, W, H, r, dmax, 0, iter, vb1n.data(), vb1v.data(), vb2n.data(),
+                        vb2v.data(), nullptr, fused, counters);
+        }
+        if (dump) { dump("prop_left", iter, W, H, m1[1 - swap].data(), user); if (views == 2) dump("prop_right", iter, W, H, m2[1 - swap].data(), user); }
+        K.fill_state(tmp.data(), m1[1 - swap].data(), W, H, 1.0f / dmax, 1);                               /* :273-274 */
+        K.huber(Ls.data(), tmp.data(), LDT.data(), lam, HUBEREPS, 40, W, H);
+        if (views == 2) {
+            K.fill_state(tmp.data(), m2[1 - swap].data(), W, H, 1.0f / dmax, 0);                           /* :295-296 */
+            K.huber(Rs.data(), tmp.data(), RDT.data(), lam, HUBEREPS, 40, W, H);
+        }
+        if (dump) { dump("smooth_left", iter, W, H, Ls.data(), user); if (views == 2) dump("smooth_right", iter, W, H, Rs.data(), user); }
+        if (iter >= 3) {                                                                                 /* :320-323 */
+            theta = ((float)iter - 3.0f) / ((float)iterations - 4.0f);
+            theta = theta * theta * theta + 1e-3f;
+        }
+        swap = 1 - swap;
+    }
+    const std::vector<float>& ml = m1[swap];
+    const std::vector<float>& mr = m2[swap];
+    if (planesL) memcpy(planesL, ml.data(), 4 * N * sizeof(float));
+    if (planesR && views == 2) memcpy(planesR, mr.data(), 4 * N * sizeof(float));
+    if (pp == 0) {                                                             /* :331-337 */
+        if (dmap) K.to_disparity(dmap, ml.data(), W, H, dscale, 1);
+        if (normal) K.fill_normalmap(normal, ml.data(), W, H, 1);
+    } else {                                                                   /* :338-345 */
+        std::vector<float> chk(4 * N);
+        K.consistency(chk.data(), ml.data(), mr.data(), W, H, 1.0f, 5.0f);
+        if (dmap) {
+            if (pp == 1) K.to_disparity(dmap, chk.data(), W, H, dscale, 1);
+            else K.fill_depthmap(dmap, chk.data(), W, H, dscale);
         }
         if (normal) K.fill_normalmap(normal, chk.data(), W, H, 1);
     }

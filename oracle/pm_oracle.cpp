@@ -540,7 +540,11 @@ int orc_rng_floats(int64_t linpos, int nd, int ndraws, float* out)
     return 0;
 }
 
-int orc_prep(const uint8_t* img, int W, int H, int stride, int r, int fused, float* bw, float* grad, float* dt)
+/* raw: bw holds the image itself (r, g, b, a) instead of the colour and its window weight sum
+ * (the images depthMap hands to its kernels, PMHuberStereo.cpp:203-204); alpha: the diffusion
+ * tensor's edge weight (24 in disparityMapAll, :416; 12 in depthMap, :152) */
+static int prep_impl(const uint8_t* img, int W, int H, int stride, int r, int fused, float* bw, float* grad, float* dt,
+                     float alpha, int raw)
 {
     const std::vector<float> f = rgba8_to_float(img, W, H, stride);
     const Img4 src = {f.data(), W, H};
@@ -550,7 +554,9 @@ int orc_prep(const uint8_t* img, int W, int H, int stride, int r, int fused, flo
     for (int y = 0; y < H; y++) {
         for (int x = 0; x < W; x++) {
             const size_t i = (size_t)y * W + x;
-            if (bw) {
+            if (bw && raw) {
+                put4(bw, i, src.at(x, y));
+            } else if (bw) {
                 /* pmhstereo_bilateral_weight_to_alpha (:1462-1498) */
                 const F3 valc1 = xyz(src.at(x, y));
                 float wsum = 0.0f;
@@ -570,12 +576,12 @@ int orc_prep(const uint8_t* img, int W, int H, int stride, int r, int fused, flo
                                  gray(x, y + 1) - gray(x, y - 1)));
             }
             if (dt) {
-                /* PDDiffTensorColor (PDDiffTensor.cl:52-72) with alpha = 24, beta = 1
-                 * (PMHuberStereo.cpp:416-417); pow(len, 1) = len */
+                /* PDDiffTensorColor (PDDiffTensor.cl:52-72) with beta = 1 (PMHuberStereo.cpp:417,
+                 * :153); pow(len, 1) = len */
                 float dx = gray(x + 1, y) - g;
                 float dy = gray(x, y + 1) - g;
                 const float len = sqrtf(dx * dx + dy * dy);
-                const float w = orc_expf(-24.0f * len);
+                const float w = orc_expf(-alpha * len);
                 F4 d;
                 if (len <= 0.001f) {
                     d = f4(1.0f, 0.0f, 0.0f, 1.0f);
@@ -591,6 +597,16 @@ int orc_prep(const uint8_t* img, int W, int H, int stride, int r, int fused, flo
         }
     }
     return 0;
+}
+
+int orc_prep(const uint8_t* img, int W, int H, int stride, int r, int fused, float* bw, float* grad, float* dt)
+{
+    return prep_impl(img, W, H, stride, r, fused, bw, grad, dt, 24.0f, 0);
+}
+
+int orc_prep_raw(const uint8_t* img, int W, int H, int stride, float alpha, float* colour, float* grad, float* dt)
+{
+    return prep_impl(img, W, H, stride, 0, 0, colour, grad, dt, alpha, 1);
 }
 
 int orc_init(float* out, const float* bw1, const float* bw2, const float* g1, const float* g2,
@@ -705,7 +721,12 @@ int orc_normal_depth(float* out, const float* planes, int W, int H, float dispsc
     return 0;
 }
 
-int orc_rof(float* out, const float* input, const float* dt, const float lambda[4], int iters, int W, int H)
+/* The primal-dual steps of PDOptCL::denoiseDiffusionTensorROF_PDD (PDOptCL.cpp:1114-1168, kernel
+ * PDDROFDiffTensor.cl:43-127) or, with huber, denoiseDiffusionTensorHuber_PDD (PDOptCL.cpp:1170-1226,
+ * kernel PDDHuberDiffTensor.cl:38-107): the Huber dual divides p + SIGMA DT du by 1 + SIGMA eps
+ * and projects all four channels with one norm. */
+static int pd_tensor(int huber, float eps, float* out, const float* input, const float* dt, const float lambda[4],
+                     int iters, int W, int H)
 {
     const float SIGMA = 4.0f, TAU = 0.05f, ETA = 8.0f, THETA = 0.5f;   /* PDDROFDiffTensor.cl:35-41 */
     const size_t N = (size_t)W * H;
@@ -730,16 +751,28 @@ int orc_rof(float* out, const float* input, const float* dt, const float lambda[
             const F4 plo = P.zero(2 * x, y), phi = P.zero(2 * x + 1, y);
             const float pl[4] = {plo.x, plo.y, plo.z, plo.w}, ph[4] = {phi.x, phi.y, phi.z, phi.w};
             float a[4], b[4], nrm[4];
+            const float den = 1.0f + SIGMA * eps;
             for (int c = 0; c < 4; c++) {
                 const float DTdx = D.x * dxv[c] + D.z * dyv[c];
                 const float DTdy = D.y * dxv[c] + D.w * dyv[c];
                 a[c] = pl[c] + SIGMA * DTdx;
                 b[c] = ph[c] + SIGMA * DTdy;
+                if (huber) {
+                    a[c] = a[c] / den;
+                    b[c] = b[c] / den;
+                }
                 nrm[c] = a[c] * a[c] + b[c] * b[c];
             }
-            const float n3 = sqrtf(nrm[0] * 1.0f + nrm[1] * 1.0f + nrm[2] * 1.0f);
-            const float n4 = sqrtf(nrm[3]);
-            const float pr[4] = {fmaxf(1.0f, n3), fmaxf(1.0f, n3), fmaxf(1.0f, n3), fmaxf(1.0f, n4)};
+            float pr[4];
+            if (huber) {
+                const float n = sqrtf(nrm[0] * 1.0f + nrm[1] * 1.0f + nrm[2] * 1.0f + nrm[3] * 1.0f);
+                pr[0] = pr[1] = pr[2] = pr[3] = fmaxf(1.0f, n);
+            } else {
+                const float n3 = sqrtf(nrm[0] * 1.0f + nrm[1] * 1.0f + nrm[2] * 1.0f);
+                const float n4 = sqrtf(nrm[3]);
+                pr[0] = pr[1] = pr[2] = fmaxf(1.0f, n3);
+                pr[3] = fmaxf(1.0f, n4);
+            }
             float l[4], h[4];
             for (int c = 0; c < 4; c++) {
                 a[c] = a[c] / pr[c];
@@ -778,6 +811,63 @@ int orc_rof(float* out, const float* input, const float* dt, const float lambda[
         std::swap(ucur, unew); std::swap(pcur, pnew); std::swap(qcur, qnew);
     }
     memcpy(out, ucur->data(), 4 * N * sizeof(float));
+    return 0;
+}
+
+int orc_rof(float* out, const float* input, const float* dt, const float lambda[4], int iters, int W, int H)
+{
+    return pd_tensor(0, 0.0f, out, input, dt, lambda, iters, W, H);
+}
+
+int orc_huber(float* out, const float* input, const float* dt, const float lambda[4], float eps, int iters, int W, int H)
+{
+    return pd_tensor(1, eps, out, input, dt, lambda, iters, W, H);
+}
+
+/* float to int as an x86 truncating conversion does it (cvttss2si), which is what the
+ * reference's implicit conversions compile to on the host: NaN and values outside the int
+ * range give INT_MIN */
+static inline int f2i_x86(float f)
+{
+    if (!(f > -2147483904.0f && f < 2147483648.0f)) return INT32_MIN;
+    return (int)f;
+}
+
+/* pmhstereo_fill_state (pmhstereo.cl:1131-1185): planes with a negative cost, or a disparity
+ * outside [0, W], take the nearer-disparity valid neighbour of their row; the result as
+ * (normal, depth * dispscale) of the reference view */
+int orc_fill_state(float* out, const float* planes, int W, int H, float dispscale, int lr)
+{
+    const Img4 P = {planes, W, H};
+    const int sidesign = lr ? -1 : 1;
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const F4 state = P.at(x, y);
+            const float cx = (float)x, cy = (float)y;
+            const float disp = (transform_x(state, cx, cy) - cx) * (float)sidesign;
+            F4 val;
+            if (state.w < 0 || disp < 0 || disp > (float)W) {
+                F4 l = f4(-1.0f, -1.0f, -1.0f, -1.0f), r = f4(-1.0f, -1.0f, -1.0f, -1.0f);
+                for (int xx = x - 1; l.w < 0 && xx >= 0; xx--) l = P.at(xx, y);
+                for (int xx = x + 1; r.w < 0 && xx < W; xx++) r = P.at(xx, y);
+                if (l.w >= 0 && r.w >= 0) {
+                    int dl = f2i_x86((float)sidesign * (transform_x(l, cx, cy) - cx));
+                    int dr = f2i_x86((float)sidesign * (transform_x(r, cx, cy) - cx));
+                    if (dl <= 0) dl = W;
+                    if (dr <= 0) dr = W;
+                    val = dl <= dr ? l : r;
+                } else {
+                    val = r.w < 0 ? l : r;
+                }
+            } else {
+                val = state;
+            }
+            if (!(isfin(val.x) && isfin(val.y))) { val.x = 0.0f; val.y = 0.0f; }
+            F4 nd = to_ref_normal_depth(val, cx, cy, lr);
+            nd.w = nd.w * dispscale;
+            put4(out, (size_t)y * W + x, nd);
+        }
     return 0;
 }
 
@@ -979,7 +1069,8 @@ int orc_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, i
 
 static const PmKernels ORC_KERNELS = {orc_prep, orc_init, orc_propagate, orc_normal_depth, orc_rof,
                                       orc_consistency, orc_to_disparity, orc_fill_depthmap, orc_fill_normalmap,
-                                      orc_disparity_to_normal, orc_pyrdown, orc_pyrup_mul};
+                                      orc_disparity_to_normal, orc_pyrdown, orc_pyrup_mul, orc_prep_raw,
+                                      orc_fill_state, orc_huber};
 
 int orc_disparity_map(const uint8_t* left, const uint8_t* right, int W, int H, int stride,
                       int r, float dmax, int iterations, int pp, int views,
@@ -997,6 +1088,15 @@ int orc_disparity_map_dump(const uint8_t* left, const uint8_t* right, int W, int
 {
     return pm_host_disparity_map(ORC_KERNELS, left, right, W, H, stride, r, dmax, iterations, pp, views, levels,
                                  dmap, normal, initdisp, initnormal, planesL, planesR, fused, counters, dump, user);
+}
+
+int orc_depth_map_dump(const uint8_t* left, const uint8_t* right, int W, int H, int stride, int r, float dmax,
+                       int iterations, float dscale, int pp, int views, float* dmap, float* normal,
+                       const float* initdisp, const float* initnormal, float* planesL, float* planesR, int fused,
+                       int64_t* counters, PmDumpFn dump, void* user)
+{
+    return pm_host_depth_map(ORC_KERNELS, left, right, W, H, stride, r, dmax, iterations, dscale, pp, views, dmap,
+                             normal, initdisp, initnormal, planesL, planesR, fused, counters, dump, user);
 }
 
 }  // extern "C"

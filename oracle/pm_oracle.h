@@ -107,6 +107,15 @@ int orc_disparity_map(const uint8_t* left, const uint8_t* right, int W, int H, i
                       float* dmap, float* normal, const float* initdisp, const float* initnormal,
                       float* planesL, float* planesR, int fused, int64_t* counters);
 
+/* depthMap's inputs (PMHuberStereo.cpp:184-190, :203-204): the image as floats (r, g, b, a),
+ * pmhstereo_gradxy, and PDDiffTensorColor with edge weight alpha (beta 1) */
+int orc_prep_raw(const uint8_t* img, int W, int H, int stride, float alpha, float* colour, float* grad, float* dt);
+/* pmhstereo_fill_state (pmhstereo.cl:1131-1185) */
+int orc_fill_state(float* out, const float* planes, int W, int H, float dispscale, int lr);
+/* PDOptCL::denoiseDiffusionTensorHuber_PDD (PDOptCL.cpp:1170-1226) over PDDHuberDiffTensor
+ * (PDDHuberDiffTensor.cl:38-107): iters primal-dual steps from u = input, p = q = 0 */
+int orc_huber(float* out, const float* input, const float* dt, const float lambda[4], float eps, int iters, int W, int H);
+
 /* pyrdown (cvt/cl/kernel/pyr/pyrdown.cl): RGBA8 Wi x Hi -> RGBA8 Wo x Ho, tight rows */
 int orc_pyrdown(uint8_t* out, int Wo, int Ho, const uint8_t* in, int Wi, int Hi);
 /* pyrup_mul4f (cvt/cl/kernel/pyr/pyrupmul.cl): float images of 1 or 4 channels */
@@ -120,6 +129,12 @@ int orc_disparity_map_dump(const uint8_t* left, const uint8_t* right, int W, int
                            float* dmap, float* normal, const float* initdisp, const float* initnormal,
                            float* planesL, float* planesR, int fused, int64_t* counters,
                            void (*dump)(const char*, int, int, int, const float*, void*), void* user);
+
+/* PMHuberStereo::depthMap (PMHuberStereo.cpp:145-347); dscale <= 0 means 1 / dmax */
+int orc_depth_map_dump(const uint8_t* left, const uint8_t* right, int W, int H, int stride, int r, float dmax,
+                       int iterations, float dscale, int pp, int views, float* dmap, float* normal,
+                       const float* initdisp, const float* initnormal, float* planesL, float* planesR, int fused,
+                       int64_t* counters, void (*dump)(const char*, int, int, int, const float*, void*), void* user);
 
 #ifdef __cplusplus
 }

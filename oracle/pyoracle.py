@@ -58,6 +58,9 @@ class Oracle:
             "disparity_to_normal": [vp, vp, i32, i32],
             "pyrdown": [vp, i32, i32, vp, i32, i32],
             "pyrup_mul": [vp, i32, i32, vp, i32, i32, i32, C.POINTER(C.c_float)],
+            "prep_raw": [vp, i32, i32, i32, f32, vp, vp, vp],
+            "fill_state": [vp, vp, i32, i32, f32, i32],
+            "huber": [vp, vp, vp, C.POINTER(C.c_float), f32, i32, i32, i32],
         }
         for name, args in sig.items():
             fn = getattr(self.L, p + name)
@@ -68,6 +71,9 @@ class Oracle:
             self.L.orc_disparity_map_dump.restype = i32
             self.L.orc_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, i32, vp, vp, vp,
                                                       vp, vp, vp, i32, vp, DUMP_FN, vp]
+            self.L.orc_depth_map_dump.restype = i32
+            self.L.orc_depth_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, f32, i32, i32, vp, vp, vp,
+                                                  vp, vp, vp, i32, vp, DUMP_FN, vp]
             for fn in ("orc_exp", "orc_sin", "orc_cos", "orc_acospi"):
                 getattr(self.L, fn).restype = f32
                 getattr(self.L, fn).argtypes = [f32]
@@ -77,6 +83,9 @@ class Oracle:
             self.L.ref_disparity_map_dump.restype = i32
             self.L.ref_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, i32, vp, vp, vp,
                                                       vp, vp, vp, DUMP_FN, vp]
+            self.L.ref_depth_map_dump.restype = i32
+            self.L.ref_depth_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, f32, i32, i32, vp, vp, vp,
+                                                  vp, vp, vp, DUMP_FN, vp]
 
     # ---- kernels -----------------------------------------------------------------
     def prep(self, img, r, fused=0):
@@ -203,6 +212,52 @@ class Oracle:
             st = self.L.ref_disparity_map_dump(*common, fn, None)
         assert st == 0, st
         return res
+
+    def depth_map(self, left, right, r, dmax, iterations, dscale=-1.0, pp=1, views=2, initdisp=None,
+                  initnormal=None, fused=0, dump=False, counters=None):
+        """PMHuberStereo::depthMap.  Returns dict with dmap, normal, planesL, planesR (and stages)."""
+        H, W = left.shape[:2]
+        left = np.ascontiguousarray(left)
+        right = np.ascontiguousarray(right)
+        res = {"dmap": np.zeros((H, W), np.float32), "normal": _f4((H, W)), "planesL": _f4((H, W)),
+               "planesR": _f4((H, W)), "stages": {}}
+        stages = res["stages"]
+
+        def cb(name, it, w, h, ptr, user):
+            stages[(name.decode(), it)] = np.ctypeslib.as_array(ptr, shape=(h, w, 4)).copy()
+
+        fn = DUMP_FN(cb) if dump else DUMP_FN()
+        common = [left.ctypes.data, right.ctypes.data, W, H, W * 4, r, dmax, iterations, dscale, pp, views,
+                  res["dmap"].ctypes.data, res["normal"].ctypes.data, _p(initdisp), _p(initnormal),
+                  res["planesL"].ctypes.data, res["planesR"].ctypes.data]
+        if self.kind == "orc":
+            st = self.L.orc_depth_map_dump(*common, fused, _p(counters), fn, None)
+        else:
+            st = self.L.ref_depth_map_dump(*common, fn, None)
+        assert st == 0, st
+        return res
+
+    def prep_raw(self, img, alpha):
+        H, W = img.shape[:2]
+        img = np.ascontiguousarray(img, np.uint8)
+        c, g, d = _f4((H, W)), _f4((H, W)), _f4((H, W))
+        assert self._prep_raw(img.ctypes.data, W, H, W * 4, alpha, c.ctypes.data, g.ctypes.data, d.ctypes.data) == 0
+        return c, g, d
+
+    def fill_state(self, planes, dispscale, lr):
+        H, W = planes.shape[:2]
+        out = _f4((H, W))
+        assert self._fill_state(out.ctypes.data, _p(np.ascontiguousarray(planes, np.float32)), W, H, dispscale,
+                                lr) == 0
+        return out
+
+    def huber(self, inp, dt, lam, eps, iters):
+        H, W = inp.shape[:2]
+        out = _f4((H, W))
+        lm = (C.c_float * 4)(*[float(v) for v in lam])
+        assert self._huber(out.ctypes.data, _p(np.ascontiguousarray(inp, np.float32)),
+                           _p(np.ascontiguousarray(dt, np.float32)), lm, eps, iters, W, H) == 0
+        return out
 
     # ---- helpers (restatement only) ------------------------------------------------
     def rng_floats(self, linpos, nd, n):

@@ -118,8 +118,31 @@ int ref_k_to_disparity(float* out, const float* planes, int W, int H, float scal
 int ref_k_fill_depthmap(float* out, const float* planes, int W, int H, float scale);
 int ref_k_fill_normalmap(float* out, const float* planes, int W, int H, int lr);
 int ref_k_disparity_to_normal(float* out, const float* disp, int W, int H);
+int ref_k_fill_state(float* out, const float* planes, int W, int H, float dispscale, int lr);
+int ref_k_huber(float* out, const float* input, const float* dt, const float lambda[4], float eps, int iters, int W,
+                int H);
 
 int ref_version(void) { return 1; }
+
+/* orc_prep_raw signature: the image as floats (what the kernels read from it), its gradients
+ * (pmhstereo_gradxy) and its diffusion tensor with edge weight alpha (PDDiffTensorColor, beta 1) */
+int ref_prep_raw(const uint8_t* img, int W, int H, int stride, float alpha, float* colour, float* grad, float* dt)
+{
+    std::vector<uint8_t> packed((size_t)W * H * 4);
+    for (int y = 0; y < H; y++) memcpy(&packed[(size_t)y * W * 4], img + (size_t)y * stride, (size_t)W * 4);
+    std::vector<float> b((size_t)W * H * 4), g((size_t)W * H * 4), d((size_t)W * H * 4);
+    ref_k_prep(packed.data(), W, H, 0, b.data(), g.data());
+    ref_k_difftensor(packed.data(), W, H, alpha, 1.0f, d.data());
+    if (colour)
+        for (size_t i = 0; i < packed.size(); i++) colour[i] = (float)packed[i] / 255.0f;
+    if (grad) memcpy(grad, g.data(), g.size() * 4);
+    if (dt) memcpy(dt, d.data(), d.size() * 4);
+    return 0;
+}
+int ref_fill_state(float* out, const float* planes, int W, int H, float dispscale, int lr)
+{ return ref_k_fill_state(out, planes, W, H, dispscale, lr); }
+int ref_huber(float* out, const float* input, const float* dt, const float lambda[4], float eps, int iters, int W, int H)
+{ return ref_k_huber(out, input, dt, lambda, eps, iters, W, H); }
 
 /* orc_prep signature; `fused` must be 0 (the reference source has one arithmetic) */
 int ref_prep(const uint8_t* img, int W, int H, int stride, int r, int fused, float* bw, float* grad, float* dt)
@@ -196,7 +219,7 @@ int ref_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, i
 
 static const PmKernels REF_KERNELS = {ref_prep, ref_init, ref_propagate, ref_normal_depth, ref_rof, ref_consistency,
                                       ref_to_disparity, ref_fill_depthmap, ref_fill_normalmap, ref_disparity_to_normal,
-                                      ref_pyrdown, ref_pyrup_mul};
+                                      ref_pyrdown, ref_pyrup_mul, ref_prep_raw, ref_fill_state, ref_huber};
 
 int ref_disparity_map_dump(const uint8_t* left, const uint8_t* right, int W, int H, int stride, int r, float dmax,
                            int iterations, int pp, int views, int levels, float* dmap, float* normal,
@@ -213,6 +236,15 @@ int ref_disparity_map(const uint8_t* left, const uint8_t* right, int W, int H, i
 {
     return ref_disparity_map_dump(left, right, W, H, stride, r, dmax, iterations, pp, views, 1, dmap, normal, initdisp,
                                   initnormal, planesL, planesR, nullptr, nullptr);
+}
+
+int ref_depth_map_dump(const uint8_t* left, const uint8_t* right, int W, int H, int stride, int r, float dmax,
+                       int iterations, float dscale, int pp, int views, float* dmap, float* normal,
+                       const float* initdisp, const float* initnormal, float* planesL, float* planesR, PmDumpFn dump,
+                       void* user)
+{
+    return pm_host_depth_map(REF_KERNELS, left, right, W, H, stride, r, dmax, iterations, dscale, pp, views, dmap,
+                             normal, initdisp, initnormal, planesL, planesR, 0, nullptr, dump, user);
 }
 
 }  // extern "C"

@@ -156,6 +156,15 @@ int ref_k_fill_normalmap(float* out, const float* planes, int W, int H, int lr)
     return 0;
 }
 
+int ref_k_fill_state(float* out, const float* planes, int W, int H, float dispscale, int lr)
+{
+    /* the `otherimg` argument is read but unused by the kernel (pmhstereo.cl:1144) */
+    image2d_t o = img(out, W, H), in = img(planes, W, H);
+    nd_range(pad16(W), pad16(H), 16, 16, false,
+             [&]() { pmh::pmhstereo_fill_state(o, in, in, dispscale, lr); });
+    return 0;
+}
+
 int ref_k_disparity_to_normal(float* out, const float* disp, int W, int H)
 {
     image2d_t o = img(out, W, H), in = img1(disp, W, H);

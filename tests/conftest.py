@@ -45,13 +45,18 @@ def ref():
 
 
 def golden_cases():
-    """single-level cases (the reference's setting)"""
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("pyr"))
+    """disparityMap, single level (the reference's setting)"""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith(("pyr", "depth")))
 
 
 def pyramid_cases():
     """coarse-to-fine cases (pyramid levels > 1)"""
     return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("pyr"))
+
+
+def depth_cases():
+    """depthMap (the Huber-smoothed variant)"""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("depth"))
 
 
 def load_golden(name):

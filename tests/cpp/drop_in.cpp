@@ -1,5 +1,6 @@
-// A user of cvt::PMHuberStereo switching to this library: the reference's call,
-// unchanged, on a procedural pair.  Writes the disparity map (float32, W*H) to argv[1].
+// A user of cvt::PMHuberStereo switching to this library: the reference's calls,
+// unchanged, on a procedural pair.  Writes the disparity map of disparityMap (float32, W*H)
+// to argv[1] and, given argv[2], the map of depthMap (default dscale 1 / depthmax) there.
 #include <cstdio>
 #include <cstring>
 
@@ -23,6 +24,13 @@ int main(int argc, char** argv)
         FILE* f = fopen(argv[1], "wb");
         for (int y = 0; y < H; y++) fwrite(pd + y * sd, 4, W, f);
         fclose(f);
+        if (argc > 2) {
+            pmh.depthMap(dmap, left, right, 4, 24.0f, 5);
+            pd = dmap.map(&sd);
+            f = fopen(argv[2], "wb");
+            for (int y = 0; y < H; y++) fwrite(pd + y * sd, 4, W, f);
+            fclose(f);
+        }
         // inconsistent inputs throw, as in the reference (PMHuberStereo.cpp:412-414)
         cvt::Image small(W / 2, H, cvt::IFormat::RGBA_UINT8);
         try {

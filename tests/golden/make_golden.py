@@ -109,6 +109,42 @@ def make_pyr_case(ref, name, spec):
     np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
 
 
+# depthMap runs; name: (seed, W, H, nplanes, dlo, dhi, r, dmax, iterations, dscale, pp, init_from_gt)
+DEPTH_CASES = {
+    "depth_48x32": (21, 48, 32, 5, 2.0, 14.0, 2, 16.0, 6, -1.0, 1, False),
+    "depth_init_44x30": (22, 44, 30, 5, 2.0, 12.0, 2, 14.0, 3, 0.5, 2, True),
+}
+
+
+def make_depth_case(ref, name, spec):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, dscale, pp, init = spec
+    left, right, gtd, gtn = scene.generate(seed, W, H, npl, dlo, dhi, with_gt=True)
+    initd = gtd.copy() if init else None
+    if init:
+        initd[::4, ::3] = 0.0
+    res = ref.depth_map(left, right, r, dmax, iters, dscale=dscale, pp=pp, initdisp=initd, dump=True)
+    arrays = {"left": left, "right": right, "dmap": res["dmap"], "normal": res["normal"],
+              "planesL": res["planesL"], "planesR": res["planesR"],
+              "spec": np.array([seed, W, H, npl, dlo, dhi, r, dmax, iters, dscale, pp, int(init)], np.float64)}
+    if init:
+        arrays["initdisp"] = initd
+    for (stage, it), v in res["stages"].items():
+        if stage.startswith("init") or it == 0:
+            arrays["stage_%s_%d" % (stage, it)] = v
+    # per-kernel fixtures: the raw prep, fill_state of a plane field with gaps, the Huber smoother
+    colour, grad, dt = ref.prep_raw(left, 12.0)
+    arrays.update(k_colour=colour, k_grad=grad, k_dt12=dt)
+    planes = res["stages"][("prop_left", 0)].copy()
+    planes[3, :, 3] = -1.0
+    planes[5, 7:20, 3] = -2.0
+    arrays["k_fs_planes"] = planes
+    arrays["k_fill_state_l"] = ref.fill_state(planes, 1.0 / dmax, 1)
+    arrays["k_fill_state_r"] = ref.fill_state(planes, 1.0 / dmax, 0)
+    arrays["k_huber"] = ref.huber(arrays["k_fill_state_l"], dt, [2.3] * 4, 1e-4, 40)
+    arrays["k_huber_odd"] = ref.huber(arrays["k_fill_state_l"], dt, [2.3] * 4, 1e-4, 7)
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+
+
 def main():
     so = obuild.build_ref()
     if so is None:
@@ -120,6 +156,9 @@ def main():
         print("wrote", name)
     for name, spec in PYR_CASES.items():
         make_pyr_case(ref, name, spec)
+        print("wrote", name)
+    for name, spec in DEPTH_CASES.items():
+        make_depth_case(ref, name, spec)
         print("wrote", name)
 
 

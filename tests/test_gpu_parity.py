@@ -11,7 +11,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from conftest import golden_cases, load_golden, pyramid_cases
+from conftest import depth_cases, golden_cases, load_golden, pyramid_cases
 from oracle.pyoracle import bits_equal
 
 pytestmark = pytest.mark.gpu
@@ -353,12 +353,14 @@ def test_cpp_drop_in_matches_python(native, torch_cuda, tmp_path):
     from test_abi import build_drop_in
 
     exe = build_drop_in(tmp_path)
-    out = tmp_path / "d.raw"
-    subprocess.run([exe, str(out)], check=True)
+    out, outd = tmp_path / "d.raw", tmp_path / "depth.raw"
+    subprocess.run([exe, str(out), str(outd)], check=True)
     d = np.fromfile(str(out), np.float32).reshape(64, 96)
     L, R = scene.generate(7, 96, 64, 6, 2.0, 20.0)
-    ref = PMHuberStereo().disparity_map(L, R, 4, 24.0, 3, pp=1)
-    assert bits_equal(d, ref).all()
+    pm = PMHuberStereo()
+    assert bits_equal(d, pm.disparity_map(L, R, 4, 24.0, 3, pp=1)).all()
+    dd = np.fromfile(str(outd), np.float32).reshape(64, 96)
+    assert bits_equal(dd, pm.depth_map(L, R, 4, 24.0, 5)).all()
 
 
 def _pyr_spec(g):
@@ -426,3 +428,60 @@ def test_pipeline_with_given_normals_equals_derived_normals(native, torch_cuda, 
                            initnormalmap=nrm)
     assert bits_equal(res["planes_left"], g["planesL"]).all()
     assert bits_equal(res["dmap"], g["dmap"]).all()
+
+
+def _depth_spec(g):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, dscale, pp, init = g["spec"]
+    return int(W), int(H), int(r), float(dmax), int(iters), float(dscale), int(pp)
+
+
+@pytest.mark.parametrize("case", depth_cases())
+def test_depth_kernels_match_reference_golden(D, case):
+    g = load_golden(case)
+    W, H, r, dmax, iters, dscale, pp = _depth_spec(g)
+    img = dev(D.t, g["left"])
+    c, gr, dt = D.f4(H, W), D.f4(H, W), D.f4(H, W)
+    assert D.L.pm_k_prep_raw(img.data_ptr(), W, H, W * 4, 12.0, c.data_ptr(), gr.data_ptr(), dt.data_ptr(),
+                             stream(D.t)) == 0
+    for t, k in ((c, "k_colour"), (gr, "k_grad"), (dt, "k_dt12")):
+        assert bits_equal(host(t), g[k]).all(), k
+    P = dev(D.t, g["k_fs_planes"])
+    for lr, k in ((1, "k_fill_state_l"), (0, "k_fill_state_r")):
+        o = D.f4(H, W)
+        assert D.L.pm_k_fill_state(o.data_ptr(), P.data_ptr(), W, H, 1.0 / dmax, lr, stream(D.t)) == 0
+        assert bits_equal(host(o), g[k]).all(), k
+    fs = dev(D.t, g["k_fill_state_l"])
+    scratch = D.t.zeros(D.L.pm_rof_scratch_bytes(W, H), dtype=D.t.uint8, device="cuda")
+    lam = (C.c_float * 4)(2.3, 2.3, 2.3, 2.3)
+    for iters_, k in ((40, "k_huber"), (7, "k_huber_odd")):
+        o = D.f4(H, W)
+        assert D.L.pm_k_huber(o.data_ptr(), fs.data_ptr(), dt.data_ptr(), lam, 1e-4, iters_, W, H, scratch.data_ptr(),
+                              stream(D.t)) == 0
+        assert bits_equal(host(o), g[k]).all(), k
+
+
+@pytest.mark.parametrize("case", depth_cases())
+def test_depth_pipeline_strict_matches_reference_golden(native, torch_cuda, case):
+    from cvt_b200 import PMHuberStereo
+
+    g = load_golden(case)
+    W, H, r, dmax, iters, dscale, pp = _depth_spec(g)
+    pm = PMHuberStereo(fused=False)
+    for rep in range(2):   # graph capture, then replay
+        res = pm.depth_map(g["left"], g["right"], r, dmax, iters, dscale=dscale, pp=pp, normalmap=True, planes=True,
+                           initdisparity=g.get("initdisp"))
+        for k, gk in (("planes_left", "planesL"), ("planes_right", "planesR"), ("dmap", "dmap"), ("normal", "normal")):
+            assert bits_equal(res[k], g[gk]).all(), (rep, k)
+
+
+def test_depth_pipeline_fused_matches_oracle(native, torch_cuda, orc):
+    from cvt_b200 import PMHuberStereo, scene
+
+    L, R = scene.generate(23, 120, 80, 8, 2.0, 26.0)
+    o = orc.depth_map(L, R, 4, 32.0, 5, pp=1, fused=1)
+    pm = PMHuberStereo(fused=True)
+    dl, dr = torch_cuda.from_numpy(L).cuda(), torch_cuda.from_numpy(R).cuda()
+    res = pm.depth_map(dl, dr, 4, 32.0, 5, pp=1, normalmap=True, planes=True)
+    torch_cuda.cuda.synchronize()
+    for k, ok in (("planes_left", "planesL"), ("planes_right", "planesR"), ("dmap", "dmap"), ("normal", "normal")):
+        assert bits_equal(host(res[k]), o[ok]).all(), k

@@ -4,7 +4,7 @@ tests for the arithmetic it fixes."""
 import numpy as np
 import pytest
 
-from conftest import golden_cases, load_golden, pyramid_cases
+from conftest import depth_cases, golden_cases, load_golden, pyramid_cases
 from oracle.pyoracle import bits_equal
 
 
@@ -177,3 +177,47 @@ def test_pyramid_kernels_match_reference_live(orc, ref, Wi, Hi, Wo, Ho):
     mul = [1.7, -0.5, 3.0, 1.0]
     assert bits_equal(orc.pyrup_mul(f1, Wo, Ho, mul), ref.pyrup_mul(f1, Wo, Ho, mul)).all()
     assert bits_equal(orc.pyrup_mul(f4, Wo, Ho, mul), ref.pyrup_mul(f4, Wo, Ho, mul)).all()
+
+
+def depth_spec(g):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, dscale, pp, init = g["spec"]
+    return dict(W=int(W), H=int(H), r=int(r), dmax=float(dmax), iters=int(iters), dscale=float(dscale), pp=int(pp),
+                init=bool(init))
+
+
+@pytest.mark.parametrize("case", depth_cases())
+def test_depth_restatement_matches_reference_golden(orc, case):
+    """PMHuberStereo::depthMap, bit for bit (strict arithmetic), and its kernels"""
+    g = load_golden(case)
+    s = depth_spec(g)
+    res = orc.depth_map(g["left"], g["right"], s["r"], s["dmax"], s["iters"], dscale=s["dscale"], pp=s["pp"],
+                        initdisp=g.get("initdisp"), dump=True, fused=0)
+    n = 0
+    for (stage, it), v in res["stages"].items():
+        k = "stage_%s_%d" % (stage, it)
+        if k in g:
+            assert bits_equal(v, g[k]).all(), (case, stage, it)
+            n += 1
+    assert n >= 6
+    for k in ("dmap", "normal", "planesL", "planesR"):
+        assert bits_equal(res[k], g[k]).all(), (case, k)
+    c, gr, dt = orc.prep_raw(g["left"], 12.0)
+    assert bits_equal(c, g["k_colour"]).all() and bits_equal(gr, g["k_grad"]).all() and bits_equal(dt, g["k_dt12"]).all()
+    P = g["k_fs_planes"]
+    assert bits_equal(orc.fill_state(P, 1.0 / s["dmax"], 1), g["k_fill_state_l"]).all()
+    assert bits_equal(orc.fill_state(P, 1.0 / s["dmax"], 0), g["k_fill_state_r"]).all()
+    assert bits_equal(orc.huber(g["k_fill_state_l"], dt, [2.3] * 4, 1e-4, 40), g["k_huber"]).all()
+    assert bits_equal(orc.huber(g["k_fill_state_l"], dt, [2.3] * 4, 1e-4, 7), g["k_huber_odd"]).all()
+
+
+def test_depth_restatement_matches_reference_live(orc, ref):
+    """a fresh seed and a single-view-free edge: 4 iterations (theta's schedule divides by 0 after the last)"""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(31, 41, 27, 5, 1.0, 9.0)
+    for iters in (1, 4):
+        a = orc.depth_map(L, R, 2, 11.0, iters, pp=2, dump=True)
+        b = ref.depth_map(L, R, 2, 11.0, iters, pp=2, dump=True)
+        for k in a["stages"]:
+            assert bits_equal(a["stages"][k], b["stages"][k]).all(), (iters, k)
+        assert bits_equal(a["dmap"], b["dmap"]).all()
