@@ -23,6 +23,7 @@ SYMBOLS = [
     "pm_rof_scratch_bytes", "pm_k_rof", "pm_k_rof_static", "pm_k_consistency", "pm_k_to_disparity", "pm_k_fill_depthmap",
     "pm_k_fill_normalmap", "pm_k_disparity_to_normal", "pm_k_pyrdown", "pm_k_pyrup_mul", "pm_pyramid_size",
     "pm_k_fill_state", "pm_k_huber", "pm_k_prep_raw",
+    "pm_pfm_save", "pm_pfm_load", "pm_cvtraw_save", "pm_cvtraw_load", "pm_io_last_error",
     "pm_rng_floats", "pm_expf_host", "pm_sinf_host", "pm_cosf_host", "pm_acospif_host",
     "pm_exit_threshold_host", "pm_scene_generate",
 ]
@@ -90,6 +91,12 @@ def lib():
         "pm_k_fill_depthmap": (i32, [vp, vp, i32, i32, f32, vp]),
         "pm_k_fill_normalmap": (i32, [vp, vp, i32, i32, i32, vp]),
         "pm_k_disparity_to_normal": (i32, [vp, vp, i32, i32, vp]),
+        "pm_pfm_save": (i32, [C.c_char_p, vp, i32, i32, i32, sz]),
+        "pm_pfm_load": (i32, [C.c_char_p, vp, sz, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]),
+        "pm_cvtraw_save": (i32, [C.c_char_p, vp, i32, i32, sz, i32]),
+        "pm_cvtraw_load": (i32, [C.c_char_p, vp, sz, sz, C.POINTER(i32), C.POINTER(i32), C.POINTER(sz),
+                                 C.POINTER(i32)]),
+        "pm_io_last_error": (C.c_char_p, []),
         "pm_k_fill_state": (i32, [vp, vp, i32, i32, f32, i32, vp]),
         "pm_k_huber": (i32, [vp, vp, vp, C.POINTER(C.c_float), f32, i32, i32, i32, vp, vp]),
         "pm_k_prep_raw": (i32, [vp, i32, i32, sz, f32, vp, vp, vp, vp]),

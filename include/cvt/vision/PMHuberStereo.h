@@ -24,6 +24,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -72,7 +73,59 @@ class Image {
     const uint8_t* map(size_t* stride) const { *stride = _stride; return _data.data(); }
     void unmap(const uint8_t*) const {}
 
+    /* Image::save / Image::load for the formats disparity, normal and plane images are kept in,
+     * chosen by extension as cvt's plugins do: ".pfm" (PFMSaver / PFMLoader: float images; an
+     * RGBA image is saved without alpha and loaded with alpha 1) and ".cvtraw" (CVTRawSaver /
+     * CVTRawLoader: any of the three formats, raw rows). */
+    void save(const std::string& path) const
+    {
+        const int w = (int)_w, h = (int)_h;
+        int rc;
+        if (ends_with(path, ".pfm") || ends_with(path, ".PFM")) {
+            if (_fmt == IFormat::RGBA_UINT8) throw Exception("PFM holds float images");
+            rc = pm_pfm_save(path.c_str(), reinterpret_cast<const float*>(_data.data()), w, h, (int)_fmt.channels,
+                             _stride);
+        } else if (ends_with(path, ".cvtraw")) {
+            rc = pm_cvtraw_save(path.c_str(), _data.data(), w, h, _stride, format_id(_fmt));
+        } else {
+            throw Exception("no saver for " + path);
+        }
+        if (rc != PM_OK) throw Exception(pm_io_last_error());
+    }
+    void load(const std::string& path)
+    {
+        int w = 0, h = 0, c = 0, fid = 0;
+        size_t st = 0;
+        if (ends_with(path, ".pfm") || ends_with(path, ".PFM")) {
+            if (pm_pfm_load(path.c_str(), NULL, 0, &w, &h, &c) != PM_OK) throw Exception(pm_io_last_error());
+            reallocate(w, h, c == 1 ? IFormat::GRAY_FLOAT : IFormat::RGBA_FLOAT);
+            if (pm_pfm_load(path.c_str(), reinterpret_cast<float*>(_data.data()), _data.size() / 4, &w, &h, &c) != PM_OK)
+                throw Exception(pm_io_last_error());
+        } else if (ends_with(path, ".cvtraw")) {
+            if (pm_cvtraw_load(path.c_str(), NULL, 0, 0, &w, &h, &st, &fid) != PM_OK) throw Exception(pm_io_last_error());
+            if (fid == PM_IFORMAT_GRAY_FLOAT) reallocate(w, h, IFormat::GRAY_FLOAT);
+            else if (fid == PM_IFORMAT_RGBA_UINT8) reallocate(w, h, IFormat::RGBA_UINT8);
+            else if (fid == PM_IFORMAT_RGBA_FLOAT) reallocate(w, h, IFormat::RGBA_FLOAT);
+            else throw Exception("CVTRaw: format not supported here");
+            if (pm_cvtraw_load(path.c_str(), _data.data(), _data.size(), _stride, &w, &h, &st, &fid) != PM_OK)
+                throw Exception(pm_io_last_error());
+        } else {
+            throw Exception("no loader for " + path);
+        }
+    }
+
   private:
+    static bool ends_with(const std::string& s, const char* e)
+    {
+        const size_t n = strlen(e);
+        return s.size() >= n && s.compare(s.size() - n, n, e) == 0;
+    }
+    static int format_id(const IFormat& f)
+    {
+        if (f == IFormat::GRAY_FLOAT) return PM_IFORMAT_GRAY_FLOAT;
+        if (f == IFormat::RGBA_UINT8) return PM_IFORMAT_RGBA_UINT8;
+        return PM_IFORMAT_RGBA_FLOAT;
+    }
     size_t _w, _h;
     IFormat _fmt;
     size_t _stride;

@@ -254,6 +254,24 @@ float pm_exit_threshold_host(float m, float b);
 int pm_scene_generate(uint64_t seed, int width, int height, int nplanes, float dlo, float dhi, float nmax,
                       float sigma, uint8_t* left, uint8_t* right, int stride, float* gt_disp, float* gt_normal);
 
+/* ---- images on disk (host buffers), in the formats cvt saves them in ---------------
+ * PFM (plugins/isaver/PFM/PFMSaver.cpp, plugins/iloader/PFM/PFMLoader.cpp): "Pf" grey or
+ * "PF" RGB, "<width> <height>", scale (negative: little endian), float rows bottom to top.
+ * Saving a 4-channel image drops its alpha (as PFMSaver does); loading "PF" gives 4
+ * channels with alpha 1 (as PFMLoader does).  stride in bytes.  pm_pfm_load with out NULL
+ * only reads the size; capacity counts floats.
+ * CVTRaw (plugins/isaver/CVTRaw/, plugins/iloader/CVTRaw/): uint32 width, height, stride
+ * (bytes), IFormat id (PM_IFORMAT_*), then height rows of stride bytes.  pm_cvtraw_load with
+ * out NULL only reads the header; out_stride 0 keeps the saved stride; capacity in bytes.
+ * Errors: a status code, the message in pm_io_last_error(). */
+enum { PM_IFORMAT_GRAY_FLOAT = 4, PM_IFORMAT_RGBA_UINT8 = 9, PM_IFORMAT_RGBA_FLOAT = 12 };
+int pm_pfm_save(const char* path, const float* data, int width, int height, int channels, size_t stride);
+int pm_pfm_load(const char* path, float* out, size_t capacity, int* width, int* height, int* channels);
+int pm_cvtraw_save(const char* path, const void* data, int width, int height, size_t stride, int format_id);
+int pm_cvtraw_load(const char* path, void* out, size_t capacity, size_t out_stride, int* width, int* height,
+                   size_t* stride, int* format_id);
+const char* pm_io_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

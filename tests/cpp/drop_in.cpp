@@ -1,6 +1,7 @@
 // A user of cvt::PMHuberStereo switching to this library: the reference's calls,
 // unchanged, on a procedural pair.  Writes the disparity map of disparityMap (float32, W*H)
-// to argv[1] and, given argv[2], the map of depthMap (default dscale 1 / depthmax) there.
+// to argv[1] and, given argv[2], the map of depthMap (default dscale 1 / depthmax) there;
+// given argv[3], round-trips the disparity map through a .pfm file of that name.
 #include <cstdio>
 #include <cstring>
 
@@ -24,6 +25,15 @@ int main(int argc, char** argv)
         FILE* f = fopen(argv[1], "wb");
         for (int y = 0; y < H; y++) fwrite(pd + y * sd, 4, W, f);
         fclose(f);
+        if (argc > 3) {   // the disparity map through Image::save / Image::load (.pfm)
+            dmap.save(argv[3]);
+            cvt::Image back;
+            back.load(argv[3]);
+            size_t sb;
+            const uint8_t* pb = back.map(&sb);
+            for (int y = 0; y < H; y++)
+                if (memcmp(pb + y * sb, pd + y * sd, 4 * W) != 0) return 5;
+        }
         if (argc > 2) {
             pmh.depthMap(dmap, left, right, 4, 24.0f, 5);
             pd = dmap.map(&sd);

@@ -354,7 +354,7 @@ def test_cpp_drop_in_matches_python(native, torch_cuda, tmp_path):
 
     exe = build_drop_in(tmp_path)
     out, outd = tmp_path / "d.raw", tmp_path / "depth.raw"
-    subprocess.run([exe, str(out), str(outd)], check=True)
+    subprocess.run([exe, str(out), str(outd), str(tmp_path / "d.pfm")], check=True)
     d = np.fromfile(str(out), np.float32).reshape(64, 96)
     L, R = scene.generate(7, 96, 64, 6, 2.0, 20.0)
     pm = PMHuberStereo()
