@@ -226,8 +226,10 @@ __device__ __forceinline__ bool eval_sample(const float4* __restrict__ q1, const
         const float a = t - fl;
         const float4* __restrict__ b = row2 + (int)fl;
         tx = lerp_texel<F>(a, 1.0f - a, texel_at(b, plane), texel_at(b + 1, plane));
-    } else {
-        tx = lerp_texel_at<F>(row2, plane, W, p2x + 0.5f);
+    } else {   // a non-finite coordinate reads the positive quiet NaN (lerp_texel_at)
+        const float n = qnan();
+        tx.c = f4(n, n, n, n);
+        tx.g = tx.c;
     }
     float cost = PM_K033_8 * ad_sum<CHK>(tx.c, q);
     // cost + 0.875f * (0.25f * n): the product 0.21875 n is exact, so one fma rounds the same
