@@ -131,7 +131,7 @@ def window_positions(W, H, r):
     return int(axis(W)) * int(axis(H))
 
 
-def cpu_sample(kind_pref, crop, wl, scene_lr):
+def cpu_sample(kind_pref, crop, wl, scene_lr, mode="disparity"):
     """time the CPU implementation on a crop; returns (Mpx*it/s, seconds, kind, cores)"""
     from oracle import build as obuild
     from oracle.pyoracle import Oracle, available
@@ -148,12 +148,13 @@ def cpu_sample(kind_pref, crop, wl, scene_lr):
         obuild.build_oracle()
     o = Oracle("ref" if kind == "reference" else "orc")
     t0 = time.perf_counter()
-    if kind == "reference":
-        o.disparity_map(L, R, r, dmax, iters, pp=pp, views=views)
+    extra = {} if kind == "reference" else {"fused": 0}
+    if mode == "depth":
+        o.depth_map(L, R, r, dmax, iters, pp=pp, views=views, **extra)
     else:
-        o.disparity_map(L, R, r, dmax, iters, pp=pp, views=views, fused=0)
+        o.disparity_map(L, R, r, dmax, iters, pp=pp, views=views, levels=3 if mode == "pyramid" else 1, **extra)
     dt = time.perf_counter() - t0
-    rate = cw * ch * executed(iters) / dt / 1e6
+    rate = cw * ch * (iters if mode == "depth" else executed(iters)) / dt / 1e6
     return rate, dt, kind, os.cpu_count()
 
 
@@ -264,6 +265,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="hd", choices=sorted(WORKLOADS) + ["batch"])
+    ap.add_argument("--mode", default="disparity", choices=["disparity", "depth", "pyramid"],
+                    help="disparityMap (default), depthMap (Huber variant, iterations not made odd) or "
+                         "disparityMap over 3 pyramid levels (value counts the full-size pixels)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run warmup + steps of the device pipeline (for ncu captures) and print the step times")
@@ -293,25 +297,34 @@ def main():
     W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
     L, R = scene.generate(pair_seed(rank), W, H, npl, dlo, dhi)
     dL, dR = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
-    pm = PMHuberStereo(views=views, fused=True, device=local)
+    levels = 3 if args.mode == "pyramid" else 1
+    pm = PMHuberStereo(views=views, fused=True, device=local, levels=levels)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    depth = args.mode == "depth"
+    run_iters = iters if depth else executed(iters)   # depthMap does not make the count odd
+
+    def call(a, b):
+        if depth:
+            return pm.depth_map(a, b, r, dmax, iters, pp=pp)
+        return pm.disparity_map(a, b, r, dmax, iters, pp=pp)
+
     if args.profile_run:
         for _ in range(args.warmup):
-            pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+            call(dL, dR)
         pm.set_profiling(True)
         for k in range(args.steps):
-            pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+            call(dL, dR)
             print(json.dumps({"step": k, "phase_ms": pm.phase_times()}))
         return
 
     # counting pass (untimed): window samples of the propagate launches
     pm.set_counting(True)
-    pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+    call(dL, dR)
     torch.cuda.synchronize()
     ctr = pm.counters()
     pm.set_counting(False)
     for _ in range(args.warmup):
-        pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+        call(dL, dR)
     torch.cuda.synchronize()
 
     # timed region: the product path (each call one CUDA graph launch, enqueued back to back)
@@ -323,7 +336,7 @@ def main():
     for k in range(args.steps):
         flush.fill_(k & 0xff)
         ev[k][0].record()
-        pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+        call(dL, dR)
         ev[k][1].record()
     torch.cuda.synchronize()
     if world > 1:
@@ -331,14 +344,14 @@ def main():
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = max_over_ranks(sum(step_ms), world)
-    px_it = W * H * executed(iters)
+    px_it = W * H * run_iters
     value = world * px_it * args.steps / (total_ms * 1e-3) / 1e6
 
     # one more step with per-phase events (eager launches), outside the timed region: the
     # propagate kernels' device time for the roofline and the launch count per step
     flush.fill_(0x5a)
     pm.set_profiling(True)
-    pm.disparity_map(dL, dR, r, dmax, iters, pp=pp)
+    call(dL, dR)
     ph = pm.phase_times()
     pm.set_profiling(False)
     prop_ms = ph["propagate"][0]
@@ -347,13 +360,13 @@ def main():
     # end to end through the host API: pinned host images in, disparity map out
     pl = torch.from_numpy(L).pin_memory().numpy()
     pr = torch.from_numpy(R).pin_memory().numpy()
-    pm.disparity_map(pl, pr, r, dmax, iters, pp=pp)
+    call(pl, pr)
     e2e = []
     for k in range(args.steps):
         flush.fill_(k & 0xff)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        pm.disparity_map(pl, pr, r, dmax, iters, pp=pp)
+        call(pl, pr)
         b.record()
         torch.cuda.synchronize()
         e2e.append(a.elapsed_time(b))
@@ -363,8 +376,12 @@ def main():
     # = 10 per hoisted support weight + 41 per cost-window sample + 129 per
     #   Gauss-Newton window sample, over the launch's measured average duration
     # one propagate pass = the three kernels of one view and iteration (pm_propagate.cu)
-    nlaunch = views * executed(iters)
-    flops_launch = (10.0 * window_positions(W, H, r) * nlaunch + 41.0 * ctr[0] + 129.0 * ctr[1]) / nlaunch
+    sizes = [(W, H)]
+    for _ in range(1, levels):
+        sizes.append((int(np.float32(sizes[-1][0]) * np.float32(0.35)), int(np.float32(sizes[-1][1]) * np.float32(0.35))))
+    nlaunch = views * run_iters * levels
+    wpos = sum(window_positions(w, h, r) for w, h in sizes) * views * run_iters
+    flops_launch = (10.0 * wpos + 41.0 * ctr[0] + 129.0 * ctr[1]) / nlaunch
     avg_launch_s = prop_ms / nlaunch * 1e-3
     peak = None
     import ctypes as C
@@ -374,7 +391,7 @@ def main():
     achieved = flops_launch / avg_launch_s / 1e12
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "propagate_%s_dram.json" % args.config)
-    if os.path.exists(tfile):
+    if args.mode == "disparity" and os.path.exists(tfile):
         traffic = json.load(open(tfile)).get("bytes_per_launch")
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": (achieved / peak) if peak else None, "traffic": traffic,
@@ -384,8 +401,9 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "Mpixel·iterations/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.config, "width": W, "height": H, "planes": npl, "dispmax": dmax,
-                       "window": 2 * r + 1, "iterations": iters, "iterations_executed": executed(iters),
+            "config": {"workload": args.config, "mode": args.mode, "levels": levels, "width": W, "height": H,
+                       "planes": npl, "dispmax": dmax, "window": 2 * r + 1, "iterations": iters,
+                       "iterations_executed": run_iters,
                        "views": views, "pp": "lrcheck" if pp == 1 else "none", "parallelism": "pairs%d" % world,
                        "l2": "flushed between steps (256 MiB write)"},
             "e2e": {"value": e2e_value, "unit": "Mpixel·iterations/s", "h2d_bytes_per_step": 2 * W * H * 4,
@@ -394,7 +412,7 @@ def main():
             "counters": {"cost_samples": ctr[0], "gn_samples": ctr[1], "cost_evals": ctr[2], "early_exits": ctr[3]},
             "phase_ms": {k: v[0] for k, v in ph.items()}}
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, dt, kind, cores = cpu_sample("port", CPU_CROP[args.config], wl, (L, R))
+        rate, dt, kind, cores = cpu_sample("port", CPU_CROP[args.config], wl, (L, R), mode=args.mode)
         cw, ch = CPU_CROP[args.config]
         line["cpu_baseline"] = {"value": rate, "unit": "Mpixel·iterations/s", "cores": cores, "kind": kind,
                                 "sample": "%dx%d crop of the same pair, same window/range/iterations, %.1f s" % (
