@@ -203,6 +203,7 @@ inline float clamp(float x, float lo, float hi) { return fmin(fmax(x, lo), hi); 
 inline int min(int a, int b) { return a < b ? a : b; }
 inline int max(int a, int b) { return a > b ? a : b; }
 inline int mad24(int a, int b, int c) { return a * b + c; }
+inline int mul24(int a, int b) { return a * b; }   /* exact for the 24-bit operands the kernels pass */
 inline uint mad_hi(uint a, uint b, uint c) { return (uint)(((ulong)a * (ulong)b) >> 32) + c; }
 inline int isfinite(float x) { return std::isfinite(x) ? 1 : 0; }
 inline int convert_int(float f)

@@ -1067,6 +1067,209 @@ int orc_pyrup_mul(float* out, int Wo, int Ho, const float* in, int Wi, int Hi, i
     return 0;
 }
 
+/* ---- VPMStereoCL (cvt/vision/VPMStereoCL.cpp, cvt/cl/kernel/VPMStereo.cl) ------------- */
+/* A simpler slanted-plane PatchMatch on one view: states (a, b, c) with x' = a x + b y + c,
+ * van der Corput candidates, eight fixed neighbour offsets, three Gauss-Newton steps. */
+
+/* grad_gray_xydiag (cvt/cl/kernel/gradxy.cl): central grey differences with a zero border
+ * (CLK_ADDRESS_CLAMP); the diagonal channels repeat them */
+int orc_vpm_grad(float* out, const uint8_t* img, int W, int H, int stride)
+{
+    const std::vector<float> f = rgba8_to_float(img, W, H, stride);
+    const Img4 src = {f.data(), W, H};
+    auto gray = [&](int x, int y) { return dot3(xyz(src.zero(x, y)), f3(GW_R, GW_G, GW_B)); };
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const float dx = gray(x + 1, y) - gray(x - 1, y), dy = gray(x, y + 1) - gray(x, y - 1);
+            put4(out, (size_t)y * W + x, f4(dx, dy, dx, dy));
+        }
+    return 0;
+}
+
+static inline float vdc2(uint32_t v)   /* vpmsstate_vanDerCorput2 (VPMStereo.cl:47-55): bit reversal * 2^-32 */
+{
+    v = (v << 16) | (v >> 16);
+    v = ((v & 0x55555555u) << 1) | ((v & 0xAAAAAAAAu) >> 1);
+    v = ((v & 0x33333333u) << 2) | ((v & 0xCCCCCCCCu) >> 2);
+    v = ((v & 0x0F0F0F0Fu) << 4) | ((v & 0xF0F0F0F0u) >> 4);
+    v = ((v & 0x00FF00FFu) << 8) | ((v & 0xFF00FF00u) >> 8);
+    return 2.3283064365386963e-10f * (float)v;
+}
+
+/* vpmsstate_from_disparity_normal with normal (0, 0, 1) (:57-61, :63-66) */
+static inline F3 vpm_fronto(float cx, float cy, float d)
+{
+    const F3 n = f3(0.0f, 0.0f, 1.0f);
+    return f3(1.0f - (-n.x / n.z), 0.0f - (-n.y / n.z), 0.0f - ((n.x * cx + n.y * cy) / n.z + d));
+}
+
+struct VpmViews {
+    Img4 c1, g1, c2, g2;   /* colours as floats, gradients */
+    int W, H, r;
+};
+
+/* patch_eval_census of VPMStereo.cl (:203-256): no early exit */
+static float vpm_eval(const VpmViews& V, int px, int py, F3 s)
+{
+    const float cx = (float)px, cy = (float)py;
+    const float alpha = 0.05f;
+    const float c2x = s.x * cx + s.y * cy + s.z;
+    if (c2x < 0 || c2x >= (float)V.W) return 1.0f;
+    const F3 valc1 = xyz(V.c1.at(px, py));
+    float wsum = 0.0f, census = 0.0f;
+    for (int dy = -V.r; dy <= V.r; dy++)
+        for (int dx = -V.r; dx <= V.r; dx++) {
+            const float qx = cx + (float)dx * 1.0f, qy = cy + (float)dy * 1.0f;
+            const float p2x = s.x * qx + s.y * qy + s.z;
+            if (p2x < 0 || p2x >= (float)V.W || qx < 0 || qx >= (float)V.W || qy < 0 || qy >= (float)V.H) continue;
+            const int ix = px + dx, iy = py + dy;
+            const F3 valin = xyz(V.c1.at(ix, iy));
+            const F3 val1 = f3(valin.x - valc1.x, valin.y - valc1.y, valin.z - valc1.z);
+            const float w = orc_expf(-fabsf(dot3(val1, f3(GW_R, GW_G, GW_B))) * 8.0f);
+            const F4 v2 = lerp_row(0, V.c2, p2x + 0.5f, iy);
+            const float ccx = fminf(fabsf(v2.x - valin.x), 0.05f) / 0.05f;
+            const float ccy = fminf(fabsf(v2.y - valin.y), 0.05f) / 0.05f;
+            const float ccz = fminf(fabsf(v2.z - valin.z), 0.05f) / 0.05f;
+            census += w * alpha * 0.33f * (ccx + ccy + ccz);
+            const F4 gval1 = V.g1.at(ix, iy);
+            const F4 gval2 = lerp_row(0, V.g2, p2x + 0.5f, iy);
+            census += w * (1.0f - alpha) * 0.25f * (float)popc4(signbits4(gval1) ^ signbits4(gval2));
+            wsum += w;
+        }
+    return census / wsum;
+}
+
+/* patch_census_klt of VPMStereo.cl (:113-201): every sample updates J and H (no curvature test) */
+static F3 vpm_klt(const VpmViews& V, int px, int py, F3 s)
+{
+    const float cx = (float)px, cy = (float)py;
+    const float alpha = 0.05f;
+    float J[3] = {0, 0, 0};
+    float Hm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    const F3 valc1 = xyz(V.c1.at(px, py));
+    for (float dy = (float)-V.r; dy <= (float)V.r; dy += 1.0f)
+        for (float dx = (float)-V.r; dx <= (float)V.r; dx += 1.0f) {
+            const float qx = cx + dx * 1.0f, qy = cy + dy * 1.0f;
+            if (qx < 0 || qx >= (float)V.W || qy < 0 || qy >= (float)V.H) continue;
+            const int ix = (int)qx, iy = (int)qy;
+            const F3 valin = xyz(V.c1.at(ix, iy));
+            const F3 val1 = f3(valin.x - valc1.x, valin.y - valc1.y, valin.z - valc1.z);
+            const F4 gval1 = V.g1.at(ix, iy);
+            const float w1 = orc_expf(-fabsf(dot3(val1, f3(GW_R, GW_G, GW_B))) * 8.0f);
+            const float p2x = s.x * qx + s.y * qy + s.z;
+            if (qx < 1 || qx >= (float)(V.W - 1)) continue;
+            const uint32_t sg1 = signbits4(gval1);
+            float C3[3];
+            const float us[3] = {p2x + 0.5f, (p2x + 1.0f) + 0.5f, (p2x + -1.0f) + 0.5f};
+            for (int k = 0; k < 3; k++) {
+                const F4 v2 = lerp_row(0, V.c2, us[k], iy);
+                const float ccx = fminf(fabsf(v2.x - valin.x), 0.05f) / 0.05f;
+                const float ccy = fminf(fabsf(v2.y - valin.y), 0.05f) / 0.05f;
+                const float ccz = fminf(fabsf(v2.z - valin.z), 0.05f) / 0.05f;
+                float C = w1 * alpha * 0.33f * (ccx + ccy + ccz);
+                const F4 g2 = lerp_row(0, V.g2, us[k], iy);
+                /* 0.25 is a double literal: the sum is formed in double and rounded once */
+                C = (float)((double)C + (double)(w1 * (1.0f - alpha)) * 0.25 * (double)(float)popc4(sg1 ^ signbits4(g2)));
+                C3[k] = C;
+            }
+            const float C = C3[0], Cxp = C3[1], Cxm = C3[2];
+            const float p[3] = {qx, qy, 1.0f};
+            const float t = w1 * (Cxm - Cxp) * 0.5f;
+            const float sc = w1 * (Cxp + Cxm - 2.0f * C);
+            for (int i = 0; i < 3; i++) J[i] = J[i] + t * p[i];
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) Hm[i][j] = Hm[i][j] + sc * (p[i] * p[j]);
+        }
+    const F3 d = lusolve(Hm, f3(J[0], J[1], J[2]));
+    return f3(s.x - d.x, s.y - d.y, s.z - d.z);
+}
+
+/* vpmstereo_init / vpmstereo_init_disparity (VPMStereo.cl:258-309): initdisp NULL for the
+ * first; the van der Corput index is x * W + y as the source forms it */
+int orc_vpm_init(float* out, const uint8_t* c1, const float* g1, const uint8_t* c2, const float* g2, int W, int H,
+                 int stride, int r, float dmax, const float* initdisp)
+{
+    const std::vector<float> f1 = rgba8_to_float(c1, W, H, stride), f2 = rgba8_to_float(c2, W, H, stride);
+    const VpmViews V = {{f1.data(), W, H}, {g1, W, H}, {f2.data(), W, H}, {g2, W, H}, W, H, r};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const float cx = (float)x, cy = (float)y;
+            F3 st;
+            const float d = initdisp ? initdisp[(size_t)y * W + x] : -1.0f;
+            if (initdisp && d >= 0 && d < dmax) st = vpm_fronto(cx, cy, d);
+            else st = vpm_fronto(cx, cy, vdc2((uint32_t)x * (uint32_t)W + (uint32_t)y) * dmax);
+            put4(out, (size_t)y * W + x, f4(st.x, st.y, st.z, vpm_eval(V, x, y, st)));
+        }
+    return 0;
+}
+
+/* vpmstereo_iter_simple (VPMStereo.cl:311-356) */
+int orc_vpm_iter(float* out, const float* in, const uint8_t* c1, const float* g1, const uint8_t* c2,
+                 const float* g2, int W, int H, int stride, int r, float dmax, int iter)
+{
+    const std::vector<float> f1 = rgba8_to_float(c1, W, H, stride), f2 = rgba8_to_float(c2, W, H, stride);
+    const VpmViews V = {{f1.data(), W, H}, {g1, W, H}, {f2.data(), W, H}, {g2, W, H}, W, H, r};
+    const Img4 I = {in, W, H};
+    static const int off[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {16, 0}, {-16, 0}, {0, 16}, {0, -16}};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const float cx = (float)x, cy = (float)y;
+            F4 cur = I.at(x, y);
+            F3 st = vpm_fronto(cx, cy, vdc2((uint32_t)((x & 7) * (y & 7)) + (uint32_t)iter) * dmax);
+            float cost = vpm_eval(V, x, y, st);
+            if (cost < cur.w) cur = f4(st.x, st.y, st.z, cost);
+            for (int i = 0; i < 8; i++) {
+                const int* o = off[(iter + i) & 7];
+                st = xyz(I.edge(x + o[0], y + o[1]));
+                cost = vpm_eval(V, x, y, st);
+                if (cost < cur.w) cur = f4(st.x, st.y, st.z, cost);
+            }
+            st = vpm_klt(V, x, y, xyz(cur));
+            for (int k = 0; k < 2; k++) st = vpm_klt(V, x, y, st);
+            cost = vpm_eval(V, x, y, st);
+            if (cost < cur.w) cur = f4(st.x, st.y, st.z, cost);
+            put4(out, (size_t)y * W + x, cur);
+        }
+    return 0;
+}
+
+/* vpmstereo_disparity (VPMStereo.cl:358-373): |x' - x| * scale */
+int orc_vpm_disparity(float* out, const float* states, int W, int H, float scale)
+{
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const size_t i = (size_t)y * W + x;
+            const float cx = (float)x, cy = (float)y;
+            out[i] = fabsf(states[4 * i] * cx + states[4 * i + 1] * cy + states[4 * i + 2] - cx) * scale;
+        }
+    return 0;
+}
+
+/* VPMStereoCL::disparitySimple (cvt/vision/VPMStereoCL.cpp:54-85) without its debugging block
+ * (:74-81: a PNG of every iterate and a wait for a key press; no result depends on it).  The
+ * states ping-pong: init writes out1, iteration i reads out[1 - swap] and writes out[swap]. */
+int orc_vpm_disparity_simple(float* disparity, float* states, const uint8_t* c1, const uint8_t* c2, int W, int H,
+                             int stride, int r, int iterations, float dmax, const float* initdisp)
+{
+    const size_t N = (size_t)W * H;
+    std::vector<float> g1(4 * N), g2(4 * N), s0(4 * N), s1(4 * N);
+    orc_vpm_grad(g1.data(), c1, W, H, stride);
+    orc_vpm_grad(g2.data(), c2, W, H, stride);
+    float* out[2] = {s0.data(), s1.data()};
+    orc_vpm_init(out[1], c1, g1.data(), c2, g2.data(), W, H, stride, r, dmax, initdisp);
+    int swap = 0;
+    for (int i = 0; i < iterations; i++) {
+        orc_vpm_iter(out[swap], out[1 - swap], c1, g1.data(), c2, g2.data(), W, H, stride, r, dmax, i);
+        swap = 1 - swap;
+    }
+    orc_vpm_disparity(disparity, out[1 - swap], W, H, 1.0f);
+    if (states) memcpy(states, out[1 - swap], 4 * N * sizeof(float));
+    return 0;
+}
+
 static const PmKernels ORC_KERNELS = {orc_prep, orc_init, orc_propagate, orc_normal_depth, orc_rof,
                                       orc_consistency, orc_to_disparity, orc_fill_depthmap, orc_fill_normalmap,
                                       orc_disparity_to_normal, orc_pyrdown, orc_pyrup_mul, orc_prep_raw,

@@ -136,6 +136,18 @@ int orc_depth_map_dump(const uint8_t* left, const uint8_t* right, int W, int H, 
                        const float* initdisp, const float* initnormal, float* planesL, float* planesR, int fused,
                        int64_t* counters, void (*dump)(const char*, int, int, int, const float*, void*), void* user);
 
+/* VPMStereoCL (cvt/vision/VPMStereoCL.cpp, cvt/cl/kernel/VPMStereo.cl, gradxy.cl): colour
+ * images RGBA8 with `stride` bytes per row, plane states W*H*4 floats (a, b, c, cost) */
+int orc_vpm_grad(float* out, const uint8_t* img, int W, int H, int stride);
+int orc_vpm_init(float* out, const uint8_t* c1, const float* g1, const uint8_t* c2, const float* g2, int W, int H,
+                 int stride, int r, float dmax, const float* initdisp);
+int orc_vpm_iter(float* out, const float* in, const uint8_t* c1, const float* g1, const uint8_t* c2,
+                 const float* g2, int W, int H, int stride, int r, float dmax, int iter);
+int orc_vpm_disparity(float* out, const float* states, int W, int H, float scale);
+/* VPMStereoCL::disparitySimple; states (NULL: not returned) gets the final plane states */
+int orc_vpm_disparity_simple(float* disparity, float* states, const uint8_t* c1, const uint8_t* c2, int W, int H,
+                             int stride, int r, int iterations, float dmax, const float* initdisp);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,22 @@ class Oracle:
             fn.restype = i32
             fn.argtypes = args
             setattr(self, "_" + name, fn)
+        # VPMStereoCL: the restatement takes a row stride for its colour images, the
+        # reference glue packed rows
+        st = [i32] if kind == "orc" else []
+        vsig = {
+            "vpm_grad": [vp, vp, i32, i32] + st,
+            "vpm_init": [vp, vp, vp, vp, vp, i32, i32] + st + [i32, f32, vp],
+            "vpm_iter": [vp, vp, vp, vp, vp, vp, i32, i32] + st + [i32, f32, i32],
+            "vpm_disparity": [vp, vp, i32, i32, f32],
+            "vpm_disparity_simple": [vp, vp, vp, vp, i32, i32] + st + [i32, i32, f32, vp],
+        }
+        for name, args in vsig.items():
+            fn = getattr(self.L, p + name)
+            fn.restype = i32
+            fn.argtypes = args
+            setattr(self, "_" + name, fn)
+        self._st = (lambda W: [W * 4]) if kind == "orc" else (lambda W: [])
         if kind == "orc":
             self.L.orc_disparity_map_dump.restype = i32
             self.L.orc_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, i32, vp, vp, vp,
@@ -258,6 +274,57 @@ class Oracle:
         assert self._huber(out.ctypes.data, _p(np.ascontiguousarray(inp, np.float32)),
                            _p(np.ascontiguousarray(dt, np.float32)), lm, eps, iters, W, H) == 0
         return out
+
+    # ---- VPMStereoCL (cvt/vision/VPMStereoCL.cpp) -----------------------------------
+    def vpm_grad(self, img):
+        """grad_gray_xydiag (gradxy.cl:60-97) of an RGBA8 image: (dx, dy, dx, dy)."""
+        H, W = img.shape[:2]
+        img = np.ascontiguousarray(img, np.uint8)
+        out = _f4((H, W))
+        assert self._vpm_grad(out.ctypes.data, img.ctypes.data, W, H, *self._st(W)) == 0
+        return out
+
+    def vpm_init(self, c1, g1, c2, g2, r, dmax, initdisp=None):
+        """vpmstereo_init, or vpmstereo_init_disparity with initdisp (VPMStereo.cl:260-309)."""
+        H, W = c1.shape[:2]
+        c1, c2 = np.ascontiguousarray(c1, np.uint8), np.ascontiguousarray(c2, np.uint8)
+        g1, g2 = np.ascontiguousarray(g1, np.float32), np.ascontiguousarray(g2, np.float32)
+        if initdisp is not None:
+            initdisp = np.ascontiguousarray(initdisp, np.float32)
+        out = _f4((H, W))
+        assert self._vpm_init(out.ctypes.data, c1.ctypes.data, g1.ctypes.data, c2.ctypes.data, g2.ctypes.data, W, H,
+                              *self._st(W), r, dmax, _p(initdisp)) == 0
+        return out
+
+    def vpm_iter(self, states, c1, g1, c2, g2, r, dmax, it):
+        """vpmstereo_iter_simple (VPMStereo.cl:311-361)."""
+        H, W = c1.shape[:2]
+        c1, c2 = np.ascontiguousarray(c1, np.uint8), np.ascontiguousarray(c2, np.uint8)
+        g1, g2 = np.ascontiguousarray(g1, np.float32), np.ascontiguousarray(g2, np.float32)
+        states = np.ascontiguousarray(states, np.float32)
+        out = _f4((H, W))
+        assert self._vpm_iter(out.ctypes.data, states.ctypes.data, c1.ctypes.data, g1.ctypes.data, c2.ctypes.data,
+                              g2.ctypes.data, W, H, *self._st(W), r, dmax, it) == 0
+        return out
+
+    def vpm_disparity(self, states, scale=1.0):
+        """vpmstereo_disparity (VPMStereo.cl:363-377)."""
+        H, W = states.shape[:2]
+        states = np.ascontiguousarray(states, np.float32)
+        out = np.zeros((H, W), np.float32)
+        assert self._vpm_disparity(out.ctypes.data, states.ctypes.data, W, H, scale) == 0
+        return out
+
+    def vpm_disparity_simple(self, c1, c2, r, iterations, dmax, initdisp=None):
+        """VPMStereoCL::disparitySimple (VPMStereoCL.cpp:54-85). Returns (disparity, states)."""
+        H, W = c1.shape[:2]
+        c1, c2 = np.ascontiguousarray(c1, np.uint8), np.ascontiguousarray(c2, np.uint8)
+        if initdisp is not None:
+            initdisp = np.ascontiguousarray(initdisp, np.float32)
+        disp, states = np.zeros((H, W), np.float32), _f4((H, W))
+        assert self._vpm_disparity_simple(disp.ctypes.data, states.ctypes.data, c1.ctypes.data, c2.ctypes.data, W, H,
+                                          *self._st(W), r, iterations, dmax, _p(initdisp)) == 0
+        return disp, states
 
     # ---- helpers (restatement only) ------------------------------------------------
     def rng_floats(self, linpos, nd, n):
