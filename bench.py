@@ -16,6 +16,10 @@ Metric: Mpixel*iterations/s = width * height * executed iterations / step time.
 One process per GPU: each rank processes its own pair (weak scaling, no
 collective on the data path); the step time is the maximum over ranks.
 
+`--mode vpm` measures the sibling path cvt::VPMStereoCL::disparitySimple
+(VPMStereoCL.cpp:54-85) on the same pair: 21x21 window, disparity range 0-128,
+8 iterations, the same metric (one iteration = one vpmstereo_iter_simple pass).
+
 `--impl reference` times the reference's CPU implementation instead: the
 reference kernel sources compiled through the OpenCL-C shim (oracle/_ref) when
 built, otherwise the CPU restatement (oracle/), on a bounded crop of the same
@@ -149,12 +153,14 @@ def cpu_sample(kind_pref, crop, wl, scene_lr, mode="disparity"):
     o = Oracle("ref" if kind == "reference" else "orc")
     t0 = time.perf_counter()
     extra = {} if kind == "reference" else {"fused": 0}
-    if mode == "depth":
+    if mode == "vpm":
+        o.vpm_disparity_simple(L, R, r, iters, dmax)
+    elif mode == "depth":
         o.depth_map(L, R, r, dmax, iters, pp=pp, views=views, **extra)
     else:
         o.disparity_map(L, R, r, dmax, iters, pp=pp, views=views, levels=3 if mode == "pyramid" else 1, **extra)
     dt = time.perf_counter() - t0
-    rate = cw * ch * (iters if mode == "depth" else executed(iters)) / dt / 1e6
+    rate = cw * ch * (iters if mode in ("depth", "vpm") else executed(iters)) / dt / 1e6
     return rate, dt, kind, os.cpu_count()
 
 
@@ -167,22 +173,28 @@ def run_reference(args, wl, rank, world):
     W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
     crop = REF_CROP[args.config]
     L, R = scene.generate(0, crop[0], crop[1], max(2, npl * crop[0] * crop[1] // (W * H) + 2), dlo, dhi)
+    mode = args.mode if args.mode in ("disparity", "vpm") else "disparity"
+    n_it = iters if mode == "vpm" else executed(iters)
     for _ in range(args.warmup):
-        cpu_sample("reference", crop, wl, (L, R))
+        cpu_sample("reference", crop, wl, (L, R), mode=mode)
     rates, secs = [], []
     kind, cores = None, None
     for _ in range(args.steps):
-        rate, dt, kind, cores = cpu_sample("reference", crop, wl, (L, R))
+        rate, dt, kind, cores = cpu_sample("reference", crop, wl, (L, R), mode=mode)
         rates.append(rate)
         secs.append(dt)
-    value = crop[0] * crop[1] * executed(iters) * len(secs) / sum(secs) / 1e6
-    sample = "%dx%d crop, window %dx%d, dispmax %g, %d iterations executed, %s" % (
-        crop[0], crop[1], 2 * r + 1, 2 * r + 1, dmax, executed(iters), "both views, LR check" if views == 2 else
-        "left view")
+    value = crop[0] * crop[1] * n_it * len(secs) / sum(secs) / 1e6
+    if mode == "vpm":
+        sample = "%dx%d crop, VPMStereoCL::disparitySimple, window %dx%d, dispmax %g, %d iterations" % (
+            crop[0], crop[1], 2 * r + 1, 2 * r + 1, dmax, n_it)
+    else:
+        sample = "%dx%d crop, window %dx%d, dispmax %g, %d iterations executed, %s" % (
+            crop[0], crop[1], 2 * r + 1, 2 * r + 1, dmax, n_it, "both views, LR check" if views == 2 else
+            "left view")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpixel·iterations/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.config, "sample": sample},
+            "config": {"workload": args.config, "mode": mode, "sample": sample},
             "cpu_baseline": {"value": value, "unit": "Mpixel·iterations/s", "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": "Mpixel·iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -258,6 +270,116 @@ def run_batch(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_vpm(args, wl, rank, world, local):
+    """--mode vpm: VPMStereoCL::disparitySimple on the workload's pair (same size, window,
+    disparity range and iteration count), one pair per rank (weak scaling)."""
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    from cvt_b200 import _lib, scene
+    from cvt_b200.vpm import VPMStereoCL
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
+    L, R = scene.generate(pair_seed(rank), W, H, npl, dlo, dhi)
+    dL, dR = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    vpm = VPMStereoCL(r, iters, dmax, device=local)
+    vpm0 = VPMStereoCL(r, 0, dmax, device=local)   # gradients, init and |x' - x| only
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # counting pass (untimed): window taps of the iteration kernel
+    vpm.set_counting(True)
+    vpm.disparity_simple(dL, dR)
+    torch.cuda.synchronize()
+    taps = vpm.counters()
+    vpm.set_counting(False)
+    for _ in range(args.warmup):
+        vpm.disparity_simple(dL, dR)
+        vpm0.disparity_simple(dL, dR)
+    torch.cuda.synchronize()
+
+    def timed(v):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            ev[k][0].record()
+            v.disparity_simple(dL, dR)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in ev]
+
+    clocks = Clocks(local).start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = timed(vpm)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = max_over_ranks(sum(step_ms), world)
+    base_ms = timed(vpm0)   # outside the timed region: the per-call work other than the iterations
+    px_it = W * H * iters
+    value = world * px_it * args.steps / (total_ms * 1e-3) / 1e6
+
+    # end to end through the host API: pinned host images in, disparity map out
+    pl = torch.from_numpy(L).pin_memory().numpy()
+    pr = torch.from_numpy(R).pin_memory().numpy()
+    vpm.disparity_simple(pl, pr)
+    e2e = []
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        vpm.disparity_simple(pl, pr)
+        b.record()
+        torch.cuda.synchronize()
+        e2e.append(a.elapsed_time(b))
+    e2e_value = world * px_it * args.steps / (max_over_ranks(sum(e2e), world) * 1e-3) / 1e6
+
+    # roofline of the iteration kernel (FP32-bound): 61 flop per cost-window tap + 178 flop per
+    # Gauss-Newton tap (taps counted by the kernel), over its average duration = (step time
+    # - step time of a 0-iteration call) / iterations
+    flops_launch = (61.0 * taps[0] + 178.0 * taps[1]) / iters
+    iter_ms = (statistics.median(step_ms) - statistics.median(base_ms)) / iters
+    pk = C.c_float(0.0)
+    peak = float(pk.value) if _lib.lib().pm_measure_fp32_peak(local, 200.0, C.byref(pk)) == 0 else None
+    achieved = flops_launch / (iter_ms * 1e-3) / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "vpm_iter_%s_dram.json" % args.config)
+    if os.path.exists(tfile):
+        traffic = json.load(open(tfile)).get("bytes_per_launch")
+    roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if peak else None, "traffic": traffic, "kernel": "k_iter (vpmstereo_iter_simple)",
+            "avg_launch_ms": iter_ms, "flops_per_launch": flops_launch,
+            "peak_source": "FP32 fma probe measured in this run (pm_measure_fp32_peak)"}
+    line = {"metric": METRIC, "value": value, "unit": "Mpixel·iterations/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config, "mode": "vpm", "width": W, "height": H, "planes": npl,
+                       "dispmax": dmax, "window": 2 * r + 1, "iterations": iters, "parallelism": "pairs%d" % world,
+                       "l2": "flushed between steps (256 MiB write)"},
+            "e2e": {"value": e2e_value, "unit": "Mpixel·iterations/s", "h2d_bytes_per_step": 2 * W * H * 4,
+                    "d2h_bytes_per_step": W * H * 4},
+            "roofline": roof, "clocks": clk, "gpu_launches": (4 + iters) * args.steps,
+            "counters": {"cost_taps": taps[0], "gn_taps": taps[1]},
+            "phase_ms": {"iterations": iter_ms * iters, "rest": statistics.median(base_ms)}}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, dt, kind, cores = cpu_sample("port", CPU_CROP[args.config], wl, (L, R), mode="vpm")
+        cw, ch = CPU_CROP[args.config]
+        line["cpu_baseline"] = {"value": rate, "unit": "Mpixel·iterations/s", "cores": cores, "kind": kind,
+                                "sample": "%dx%d crop of the same pair, same window/range/iterations, %.1f s" % (
+                                    cw, ch, dt)}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -265,9 +387,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="hd", choices=sorted(WORKLOADS) + ["batch"])
-    ap.add_argument("--mode", default="disparity", choices=["disparity", "depth", "pyramid"],
-                    help="disparityMap (default), depthMap (Huber variant, iterations not made odd) or "
-                         "disparityMap over 3 pyramid levels (value counts the full-size pixels)")
+    ap.add_argument("--mode", default="disparity", choices=["disparity", "depth", "pyramid", "vpm"],
+                    help="disparityMap (default), depthMap (Huber variant, iterations not made odd), "
+                         "disparityMap over 3 pyramid levels (value counts the full-size pixels) or "
+                         "VPMStereoCL::disparitySimple")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run warmup + steps of the device pipeline (for ncu captures) and print the step times")
@@ -282,6 +405,9 @@ def main():
     wl = WORKLOADS[args.config]
     if args.impl == "reference":
         run_reference(args, wl, rank, world)
+        return
+    if args.mode == "vpm":
+        run_vpm(args, wl, rank, world, local)
         return
 
     import torch

@@ -272,6 +272,49 @@ int pm_cvtraw_load(const char* path, void* out, size_t capacity, size_t out_stri
                    size_t* stride, int* format_id);
 const char* pm_io_last_error(void);
 
+/* ---- VPMStereoCL (cvt/vision/VPMStereoCL.h:33-65, VPMStereoCL.cpp, cvt/cl/kernel/VPMStereo.cl)
+ * The one-view slanted-plane PatchMatch: states (a, b, c) with x' = a x + b y + c, van der
+ * Corput candidates, eight neighbour states, three Gauss-Newton steps per iteration.
+ * Images RGBA8 with `stride` bytes per row; disparities and initial disparities W*H floats;
+ * states (optional) W*H float4 (a, b, c, cost).  Errors: a status code, the message in
+ * pm_vpm_last_error(handle) (NULL handle: the calling thread's last handle-free error). */
+typedef struct pm_vpm pm_vpm;
+
+/* VPMStereoCL::VPMStereoCL(patchsize, iterations, disparitymax) (VPMStereoCL.cpp:36-48) on a
+ * CUDA device; PM_ENODEV without one */
+int pm_vpm_create(pm_vpm** out, int patchsize, int iterations, float disparitymax, int device);
+/* VPMStereoCL::~VPMStereoCL (:50-52) */
+int pm_vpm_destroy(pm_vpm* h);
+const char* pm_vpm_last_error(const pm_vpm* h);
+/* VPMStereoCL::disparitySimple(output, image0, image1, initdisparity) (:54-85), host buffers,
+ * synchronous.  The reference's debugging block (:74-81: a PNG of every iterate and a wait
+ * for a key press) is not reproduced; it changes no result.  initdisparity and states may be
+ * NULL. */
+int pm_vpm_disparity_simple(pm_vpm* h, const uint8_t* image0, const uint8_t* image1, int W, int H, size_t stride,
+                            float* disparity, const float* initdisparity, float* states);
+/* the same on device buffers, enqueued on `stream` (a cudaStream_t; NULL: legacy default) */
+int pm_vpm_disparity_simple_device(pm_vpm* h, const uint8_t* image0, const uint8_t* image1, int W, int H,
+                                   size_t stride, float* disparity, const float* initdisparity, float* states,
+                                   void* stream);
+/* window-tap counters of the calls made while counting is on: c[0] cost-window taps,
+ * c[1] Gauss-Newton taps (for the FLOP count of the iteration kernel) */
+int pm_vpm_set_counting(pm_vpm* h, int on);
+int pm_vpm_get_counters(pm_vpm* h, uint64_t c[2]);
+
+/* One reference kernel per call, device buffers, enqueued on `stream`.  c1 / c2 RGBA8 images
+ * with `stride` bytes per row, g1 / g2 their gradient images (W*H float4), states W*H float4.
+ *   pm_k_vpm_grad       grad_gray_xydiag (cvt/cl/kernel/gradxy.cl:60-97)
+ *   pm_k_vpm_init       vpmstereo_init, or vpmstereo_init_disparity when initdisp is given
+ *                       (VPMStereo.cl:260-309)
+ *   pm_k_vpm_iter       vpmstereo_iter_simple (:311-361)
+ *   pm_k_vpm_disparity  vpmstereo_disparity (:363-377) */
+int pm_k_vpm_grad(float* out, const uint8_t* img, int W, int H, size_t stride, void* stream);
+int pm_k_vpm_init(float* out, const uint8_t* c1, const float* g1, const uint8_t* c2, const float* g2, int W, int H,
+                  size_t stride, int r, float dmax, const float* initdisp, void* stream);
+int pm_k_vpm_iter(float* out, const float* in, const uint8_t* c1, const float* g1, const uint8_t* c2, const float* g2,
+                  int W, int H, size_t stride, int r, float dmax, int iter, void* stream);
+int pm_k_vpm_disparity(float* out, const float* states, int W, int H, float scale, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

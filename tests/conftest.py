@@ -46,7 +46,7 @@ def ref():
 
 def golden_cases():
     """disparityMap, single level (the reference's setting)"""
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith(("pyr", "depth")))
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith(("pyr", "depth", "vpm")))
 
 
 def pyramid_cases():
@@ -57,6 +57,11 @@ def pyramid_cases():
 def depth_cases():
     """depthMap (the Huber-smoothed variant)"""
     return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("depth"))
+
+
+def vpm_cases():
+    """VPMStereoCL::disparitySimple"""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("vpm"))
 
 
 def load_golden(name):

@@ -1,9 +1,10 @@
 """Generate the golden fixtures of tests/golden/ from the reference kernels.
 
-The outputs come from cvt/cl/kernel/pmhstereo.cl, PDDiffTensor.cl and
-PDDROFDiffTensor.cl compiled from their own source through the OpenCL-C shim
-(oracle/build.py -> oracle/_ref/libpmref.so), driven by the restated host loop
-of PMHuberStereo::disparityMap.  Inputs are seeded procedural scenes from
+The outputs come from cvt/cl/kernel/pmhstereo.cl, PDDiffTensor.cl,
+PDDROFDiffTensor.cl, PDDHuberDiffTensor.cl, pyr/pyrdown.cl, pyr/pyrupmul.cl,
+VPMStereo.cl and gradxy.cl compiled from their own source through the OpenCL-C shim
+(oracle/build.py -> oracle/_ref/libpmref.so), driven by the restated host loops
+of PMHuberStereo::disparityMap / depthMap and VPMStereoCL::disparitySimple.  Inputs are seeded procedural scenes from
 cvt_b200.scene.  Run from the repository root where the reference tree is
 available:
 
@@ -36,6 +37,12 @@ CASES = {
 PYR_CASES = {
     "pyr_96x64": (11, 96, 64, 6, 2.0, 20.0, 2, 24.0, 1, 1, 2, 2, False),
     "pyr3_100x70": (12, 100, 70, 6, 2.0, 30.0, 1, 32.0, 1, 2, 2, 3, True),
+}
+
+# VPMStereoCL::disparitySimple; name: (seed, W, H, nplanes, dlo, dhi, r, dmax, iterations, init_from_gt)
+VPM_CASES = {
+    "vpm_48x32": (21, 48, 32, 5, 2.0, 12.0, 3, 16.0, 3, False),
+    "vpm_init_41x27": (22, 41, 27, 4, 1.0, 9.0, 2, 12.0, 2, True),
 }
 
 
@@ -145,6 +152,30 @@ def make_depth_case(ref, name, spec):
     np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
 
 
+def make_vpm_case(ref, name, spec):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, init = spec
+    left, right, gtd, gtn = scene.generate(seed, W, H, npl, dlo, dhi, with_gt=True)
+    initd = None
+    if init:
+        initd = gtd.copy()
+        initd[::4, ::3] = -1.0          # below the range: the van der Corput init
+        initd[2::5, 1::4] = dmax + 1.0  # above the range: the van der Corput init
+    disp, states = ref.vpm_disparity_simple(left, right, r, iters, dmax, initd)
+    arrays = {"left": left, "right": right, "disparity": disp, "states": states,
+              "spec": np.array([seed, W, H, npl, dlo, dhi, r, dmax, iters, int(init)], np.float64)}
+    if init:
+        arrays["initdisp"] = initd
+    # per-kernel fixtures: both gradients, init, two iterations (the neighbour offsets rotate
+    # with the iteration index), the scaled disparity
+    g0, g1 = ref.vpm_grad(left), ref.vpm_grad(right)
+    s0 = ref.vpm_init(left, g0, right, g1, r, dmax, initd)
+    s1 = ref.vpm_iter(s0, left, g0, right, g1, r, dmax, 0)
+    s5 = ref.vpm_iter(s1, left, g0, right, g1, r, dmax, 5)
+    arrays.update(k_grad0=g0, k_grad1=g1, k_init=s0, k_iter0=s1, k_iter5=s5,
+                  k_disp_scaled=ref.vpm_disparity(s5, 1.0 / dmax))
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+
+
 def main():
     so = obuild.build_ref()
     if so is None:
@@ -159,6 +190,9 @@ def main():
         print("wrote", name)
     for name, spec in DEPTH_CASES.items():
         make_depth_case(ref, name, spec)
+        print("wrote", name)
+    for name, spec in VPM_CASES.items():
+        make_vpm_case(ref, name, spec)
         print("wrote", name)
 
 

@@ -161,3 +161,37 @@ def test_pyramid_sizes_follow_float_scaling(native):
         for levels in range(1, 5):
             assert native.pm_pyramid_size(n, levels) == m, (n, levels)
             m = int(np.float32(m) * np.float32(0.35))
+
+
+def test_vpm_rejects_bad_arguments_without_touching_the_device(native):
+    from cvt_b200 import _lib
+
+    h = C.c_void_p()
+    assert native.pm_vpm_create(C.byref(h), 99, 3, 16.0, 0) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_vpm_create(C.byref(h), 3, -1, 16.0, 0) == _lib.PM_EINVAL_ARG
+    assert native.pm_vpm_create(C.byref(h), 3, 3, 0.0, 0) == _lib.PM_EINVAL_ARG
+    assert native.pm_vpm_create(C.byref(h), 3, 3, float("nan"), 0) == _lib.PM_EINVAL_ARG
+    assert native.pm_vpm_create(None, 3, 3, 16.0, 0) == _lib.PM_EINVAL_ARG
+    assert b"null" in native.pm_vpm_last_error(None)
+    assert native.pm_vpm_disparity_simple(None, None, None, 8, 8, 32, None, None, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_k_vpm_grad(None, None, 0, 8, 32, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_k_vpm_grad(None, None, 8, 8, 16, None) == _lib.PM_EINVAL_SHAPE   # stride < 4 W
+    assert native.pm_k_vpm_grad(None, None, 8, 8, 32, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_k_vpm_init(None, None, None, None, None, 8, 8, 32, 40, 4.0, None, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_k_vpm_iter(None, None, None, None, None, None, 8, 8, 32, 2, 4.0, -1, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_k_vpm_disparity(None, None, 8, 0, 1.0, None) == _lib.PM_EINVAL_SHAPE
+
+
+def test_vpm_create_fails_loudly_without_device(native):
+    import torch
+
+    from cvt_b200 import _lib
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    h = C.c_void_p()
+    assert native.pm_vpm_create(C.byref(h), 3, 3, 16.0, 0) == _lib.PM_ENODEV
+    from cvt_b200.vpm import StereoError, VPMStereoCL
+
+    with pytest.raises(StereoError):
+        VPMStereoCL(3, 3, 16.0)

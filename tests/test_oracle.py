@@ -4,7 +4,7 @@ tests for the arithmetic it fixes."""
 import numpy as np
 import pytest
 
-from conftest import depth_cases, golden_cases, load_golden, pyramid_cases
+from conftest import depth_cases, golden_cases, load_golden, pyramid_cases, vpm_cases
 from oracle.pyoracle import bits_equal
 
 
@@ -221,3 +221,38 @@ def test_depth_restatement_matches_reference_live(orc, ref):
         for k in a["stages"]:
             assert bits_equal(a["stages"][k], b["stages"][k]).all(), (iters, k)
         assert bits_equal(a["dmap"], b["dmap"]).all()
+
+
+def vpm_spec(g):
+    seed, W, H, npl, dlo, dhi, r, dmax, iters, init = g["spec"]
+    return dict(W=int(W), H=int(H), r=int(r), dmax=float(dmax), iters=int(iters), init=bool(init))
+
+
+@pytest.mark.parametrize("case", vpm_cases())
+def test_vpm_restatement_matches_reference_golden(orc, case):
+    """VPMStereoCL::disparitySimple and each of its kernels, bit for bit"""
+    g = load_golden(case)
+    s = vpm_spec(g)
+    r, dmax = s["r"], s["dmax"]
+    initd = g.get("initdisp")
+    disp, states = orc.vpm_disparity_simple(g["left"], g["right"], r, s["iters"], dmax, initd)
+    assert bits_equal(disp, g["disparity"]).all() and bits_equal(states, g["states"]).all()
+    g0, g1 = orc.vpm_grad(g["left"]), orc.vpm_grad(g["right"])
+    assert bits_equal(g0, g["k_grad0"]).all() and bits_equal(g1, g["k_grad1"]).all()
+    s0 = orc.vpm_init(g["left"], g0, g["right"], g1, r, dmax, initd)
+    assert bits_equal(s0, g["k_init"]).all()
+    assert bits_equal(orc.vpm_iter(g["k_init"], g["left"], g0, g["right"], g1, r, dmax, 0), g["k_iter0"]).all()
+    assert bits_equal(orc.vpm_iter(g["k_iter0"], g["left"], g0, g["right"], g1, r, dmax, 5), g["k_iter5"]).all()
+    assert bits_equal(orc.vpm_disparity(g["k_iter5"], 1.0 / dmax), g["k_disp_scaled"]).all()
+
+
+@pytest.mark.parametrize("W,H,r,iters", [(1, 1, 2, 2), (2, 3, 0, 1), (3, 2, 1, 2), (37, 5, 4, 1), (33, 34, 2, 0)])
+def test_vpm_restatement_matches_reference_live(orc, ref, W, H, r, iters):
+    """edge sizes: a single pixel, images narrower than the Gauss-Newton taps' column range
+    (singular steps), r = 0, zero iterations, sizes off the 32x32 work-group grid"""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(40 + W, W, H, 3, 0.5, 4.0)
+    a = orc.vpm_disparity_simple(L, R, r, iters, 6.0)
+    b = ref.vpm_disparity_simple(L, R, r, iters, 6.0)
+    assert bits_equal(a[0], b[0]).all() and bits_equal(a[1], b[1]).all()
