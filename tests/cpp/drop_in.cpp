@@ -1,11 +1,14 @@
 // A user of cvt::PMHuberStereo switching to this library: the reference's calls,
 // unchanged, on a procedural pair.  Writes the disparity map of disparityMap (float32, W*H)
 // to argv[1] and, given argv[2], the map of depthMap (default dscale 1 / depthmax) there;
-// given argv[3], round-trips the disparity map through a .pfm file of that name.
+// given argv[3], round-trips the disparity map through a .pfm file of that name; given
+// argv[4], writes the map of cvt::VPMStereoCL::disparitySimple (patch 3, 4 iterations,
+// range 24) there.
 #include <cstdio>
 #include <cstring>
 
 #include "cvt/vision/PMHuberStereo.h"
+#include "cvt/vision/VPMStereoCL.h"
 
 int main(int argc, char** argv)
 {
@@ -38,6 +41,15 @@ int main(int argc, char** argv)
             pmh.depthMap(dmap, left, right, 4, 24.0f, 5);
             pd = dmap.map(&sd);
             f = fopen(argv[2], "wb");
+            for (int y = 0; y < H; y++) fwrite(pd + y * sd, 4, W, f);
+            fclose(f);
+        }
+        if (argc > 4) {
+            cvt::VPMStereoCL vpm(3, 4, 24.0f);
+            cvt::Image vd;
+            vpm.disparitySimple(vd, left, right);
+            pd = vd.map(&sd);
+            f = fopen(argv[4], "wb");
             for (int y = 0; y < H; y++) fwrite(pd + y * sd, 4, W, f);
             fclose(f);
         }

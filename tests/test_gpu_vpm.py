@@ -175,3 +175,19 @@ def test_vpm_hd_properties(torch_cuda, native):
     assert np.nanmin(c) >= 0.0 and np.nanmax(c) <= 1.0 + 1e-6
     good = np.abs(d1 - gd) < 1.0
     assert np.mean(good[:, 160:]) > 0.5, np.mean(good[:, 160:])
+
+
+def test_vpm_cpp_drop_in_matches_oracle(native, torch_cuda, orc, tmp_path):
+    """cvt::VPMStereoCL::disparitySimple through the C++ header (tests/cpp/drop_in.cpp)"""
+    import subprocess
+
+    from cvt_b200 import scene
+    from test_abi import build_drop_in
+
+    exe = build_drop_in(tmp_path)
+    outv = tmp_path / "vpm.raw"
+    subprocess.run([exe, str(tmp_path / "d.raw"), str(tmp_path / "depth.raw"), str(tmp_path / "d.pfm"), str(outv)],
+                   check=True)
+    d = np.fromfile(str(outv), np.float32).reshape(64, 96)
+    L, R = scene.generate(7, 96, 64, 6, 2.0, 20.0)
+    assert bits_equal(d, orc.vpm_disparity_simple(L, R, 3, 4, 24.0)[0]).all()
