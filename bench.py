@@ -20,6 +20,10 @@ collective on the data path); the step time is the maximum over ranks.
 (VPMStereoCL.cpp:54-85) on the same pair: 21x21 window, disparity range 0-128,
 8 iterations, the same metric (one iteration = one vpmstereo_iter_simple pass).
 
+`--mode svpm` measures the optical-flow sibling cvt::SVPMFlowCL::flow
+(SVPMFlowCL.cpp:58-89) on the same pair taken as two frames: 7x7 window, flow
+range 128, the reference's 200 passes; metric Mpixel*passes/s.
+
 `--impl reference` times the reference's CPU implementation instead: the
 reference kernel sources compiled through the OpenCL-C shim (oracle/_ref) when
 built, otherwise the CPU restatement (oracle/), on a bounded crop of the same
@@ -45,6 +49,9 @@ WORKLOADS = {
     "hd": (1280, 720, 40, 2.0, 120.0, 10, 128.0, 8, 2, 1),
     "small": (320, 240, 12, 2.0, 30.0, 7, 32.0, 4, 1, 0),
 }
+# SVPMFlowCL::flow: window half-width, flow range, passes (the reference's MAXITER), and the
+# passes of the bounded CPU samples
+SVPM = {"r": 3, "flowmax": 128.0, "passes": 200, "cpu_passes": 40, "ref_passes": 20}
 # bounded CPU samples (crop of the same scene, same window / range / iterations)
 CPU_CROP = {"hd": (256, 144), "small": (320, 240)}
 REF_CROP = {"hd": (96, 54), "small": (96, 72)}
@@ -153,6 +160,11 @@ def cpu_sample(kind_pref, crop, wl, scene_lr, mode="disparity"):
     o = Oracle("ref" if kind == "reference" else "orc")
     t0 = time.perf_counter()
     extra = {} if kind == "reference" else {"fused": 0}
+    if mode == "svpm":
+        passes = SVPM["ref_passes"] if kind == "reference" else SVPM["cpu_passes"]
+        o.svpm_flow(L, R, SVPM["r"], SVPM["flowmax"], passes)
+        dt = time.perf_counter() - t0
+        return cw * ch * passes / dt / 1e6, dt, kind, os.cpu_count()
     if mode == "vpm":
         o.vpm_disparity_simple(L, R, r, iters, dmax)
     elif mode == "depth":
@@ -173,8 +185,8 @@ def run_reference(args, wl, rank, world):
     W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
     crop = REF_CROP[args.config]
     L, R = scene.generate(0, crop[0], crop[1], max(2, npl * crop[0] * crop[1] // (W * H) + 2), dlo, dhi)
-    mode = args.mode if args.mode in ("disparity", "vpm") else "disparity"
-    n_it = iters if mode == "vpm" else executed(iters)
+    mode = args.mode if args.mode in ("disparity", "vpm", "svpm") else "disparity"
+    n_it = {"vpm": iters, "svpm": SVPM["ref_passes"]}.get(mode, executed(iters))
     for _ in range(args.warmup):
         cpu_sample("reference", crop, wl, (L, R), mode=mode)
     rates, secs = [], []
@@ -184,20 +196,26 @@ def run_reference(args, wl, rank, world):
         rates.append(rate)
         secs.append(dt)
     value = crop[0] * crop[1] * n_it * len(secs) / sum(secs) / 1e6
-    if mode == "vpm":
+    if mode == "svpm":
+        sample = "%dx%d crop, SVPMFlowCL::flow, window %dx%d, flowmax %g, %d passes" % (
+            crop[0], crop[1], 2 * SVPM["r"] + 1, 2 * SVPM["r"] + 1, SVPM["flowmax"], n_it)
+    elif mode == "vpm":
         sample = "%dx%d crop, VPMStereoCL::disparitySimple, window %dx%d, dispmax %g, %d iterations" % (
             crop[0], crop[1], 2 * r + 1, 2 * r + 1, dmax, n_it)
     else:
         sample = "%dx%d crop, window %dx%d, dispmax %g, %d iterations executed, %s" % (
             crop[0], crop[1], 2 * r + 1, 2 * r + 1, dmax, n_it, "both views, LR check" if views == 2 else
             "left view")
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpixel·iterations/s", "n_gpus": args.gpus,
+    metric = "Mpixel·passes/s" if mode == "svpm" else METRIC
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": "Mpixel·iterations/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.config, "mode": mode, "sample": sample},
             "cpu_baseline": {"value": value, "unit": "Mpixel·iterations/s", "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": "Mpixel·iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if mode == "svpm":
+        line["unit"] = line["cpu_baseline"]["unit"] = line["e2e"]["unit"] = metric
     print(json.dumps(line))
 
 
@@ -380,6 +398,109 @@ def run_vpm(args, wl, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_svpm(args, wl, rank, world, local):
+    """--mode svpm: SVPMFlowCL::flow on the workload's pair as two frames (7x7 window, flow
+    range 128, 200 passes), one pair per rank (weak scaling)."""
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    from cvt_b200 import _lib, scene
+    from cvt_b200.svpm import SVPMFlowCL
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    W, H, npl, dlo, dhi = wl[:5]
+    r, fmax, passes = SVPM["r"], SVPM["flowmax"], SVPM["passes"]
+    L, R = scene.generate(pair_seed(rank), W, H, npl, dlo, dhi)
+    dL, dR = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    f = SVPMFlowCL(device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    metric = "Mpixel·passes/s"
+
+    f.set_counting(True)   # counting pass (untimed): cost-window taps of the propagation passes
+    f.flow(dL, dR, r, fmax, passes)
+    torch.cuda.synchronize()
+    taps = f.counters()
+    f.set_counting(False)
+    for _ in range(args.warmup):
+        f.flow(dL, dR, r, fmax, passes)
+    torch.cuda.synchronize()
+
+    def timed(n):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            ev[k][0].record()
+            f.flow(dL, dR, r, fmax, n)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in ev]
+
+    clocks = Clocks(local).start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = timed(passes)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = max_over_ranks(sum(step_ms), world)
+    base_ms = timed(0)   # outside the timed region: colour planes, init, flow extraction
+    px_it = W * H * passes
+    value = world * px_it * args.steps / (total_ms * 1e-3) / 1e6
+
+    pl = torch.from_numpy(L).pin_memory().numpy()
+    pr = torch.from_numpy(R).pin_memory().numpy()
+    f.flow(pl, pr, r, fmax, passes)
+    e2e = []
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        f.flow(pl, pr, r, fmax, passes)
+        b.record()
+        torch.cuda.synchronize()
+        e2e.append(a.elapsed_time(b))
+    e2e_value = world * px_it * args.steps / (max_over_ranks(sum(e2e), world) * 1e-3) / 1e6
+
+    # roofline of the propagation pass (FP32-bound): 52 flop per cost-window tap (taps counted by
+    # the kernel), over its average duration = (step time - time of a 0-pass call) / passes
+    flops_launch = 52.0 * taps / passes
+    pass_ms = (statistics.median(step_ms) - statistics.median(base_ms)) / passes
+    pk = C.c_float(0.0)
+    peak = float(pk.value) if _lib.lib().pm_measure_fp32_peak(local, 200.0, C.byref(pk)) == 0 else None
+    achieved = flops_launch / (pass_ms * 1e-3) / 1e12
+    roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if peak else None, "traffic": None,
+            "kernel": "k_prop (svpmflow_prop_local_tv_admm)", "avg_launch_ms": pass_ms, "flops_per_launch": flops_launch,
+            "peak_source": "FP32 fma probe measured in this run (pm_measure_fp32_peak)"}
+    line = {"metric": metric, "value": value, "unit": metric, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config, "mode": "svpm", "width": W, "height": H, "planes": npl,
+                       "flowmax": fmax, "window": 2 * r + 1, "passes": passes, "parallelism": "pairs%d" % world,
+                       "l2": "flushed between steps (256 MiB write)"},
+            "e2e": {"value": e2e_value, "unit": metric, "h2d_bytes_per_step": 2 * W * H * 4,
+                    "d2h_bytes_per_step": W * H * 8},
+            "roofline": roof, "clocks": clk, "gpu_launches": (4 + passes) * args.steps,
+            "counters": {"cost_taps": taps},
+            "phase_ms": {"passes": pass_ms * passes, "rest": statistics.median(base_ms)}}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, dt, kind, cores = cpu_sample("port", CPU_CROP[args.config], wl, (L, R), mode="svpm")
+        cw, ch = CPU_CROP[args.config]
+        line["cpu_baseline"] = {"value": rate, "unit": metric, "cores": cores, "kind": kind,
+                                "sample": "%dx%d crop of the same frames, same window/range, %d passes, %.1f s" % (
+                                    cw, ch, SVPM["cpu_passes"], dt)}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,10 +508,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="hd", choices=sorted(WORKLOADS) + ["batch"])
-    ap.add_argument("--mode", default="disparity", choices=["disparity", "depth", "pyramid", "vpm"],
+    ap.add_argument("--mode", default="disparity", choices=["disparity", "depth", "pyramid", "vpm", "svpm"],
                     help="disparityMap (default), depthMap (Huber variant, iterations not made odd), "
                          "disparityMap over 3 pyramid levels (value counts the full-size pixels) or "
-                         "VPMStereoCL::disparitySimple")
+                         "VPMStereoCL::disparitySimple or SVPMFlowCL::flow (200 passes)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run warmup + steps of the device pipeline (for ncu captures) and print the step times")
@@ -408,6 +529,9 @@ def main():
         return
     if args.mode == "vpm":
         run_vpm(args, wl, rank, world, local)
+        return
+    if args.mode == "svpm":
+        run_svpm(args, wl, rank, world, local)
         return
 
     import torch

@@ -25,10 +25,12 @@ SYMBOLS = [
     "pm_k_fill_state", "pm_k_huber", "pm_k_prep_raw",
     "pm_pfm_save", "pm_pfm_load", "pm_cvtraw_save", "pm_cvtraw_load", "pm_io_last_error",
     "pm_rng_floats", "pm_expf_host", "pm_sinf_host", "pm_cosf_host", "pm_acospif_host",
-    "pm_exit_threshold_host", "pm_scene_generate",
+    "pm_exit_threshold_host", "pm_scene_generate", "pm_logf_host",
     "pm_vpm_create", "pm_vpm_destroy", "pm_vpm_last_error", "pm_vpm_disparity_simple",
     "pm_vpm_disparity_simple_device", "pm_vpm_set_counting", "pm_vpm_get_counters",
     "pm_k_vpm_grad", "pm_k_vpm_init", "pm_k_vpm_iter", "pm_k_vpm_disparity",
+    "pm_svpm_create", "pm_svpm_destroy", "pm_svpm_last_error", "pm_svpm_flow", "pm_svpm_flow_device",
+    "pm_svpm_set_counting", "pm_svpm_get_counters", "pm_k_svpm_init", "pm_k_svpm_prop", "pm_k_svpm_to_flow",
 ]
 
 
@@ -111,6 +113,7 @@ def lib():
         "pm_sinf_host": (f32, [f32]),
         "pm_cosf_host": (f32, [f32]),
         "pm_acospif_host": (f32, [f32]),
+        "pm_logf_host": (f32, [f32]),
         "pm_exit_threshold_host": (f32, [f32, f32]),
         "pm_scene_generate": (i32, [C.c_uint64, i32, i32, i32, f32, f32, f32, f32, vp, vp, i32, vp, vp]),
         "pm_vpm_create": (i32, [C.POINTER(vp), i32, i32, f32, i32]),
@@ -124,6 +127,16 @@ def lib():
         "pm_k_vpm_init": (i32, [vp, vp, vp, vp, vp, i32, i32, sz, i32, f32, vp, vp]),
         "pm_k_vpm_iter": (i32, [vp, vp, vp, vp, vp, vp, i32, i32, sz, i32, f32, i32, vp]),
         "pm_k_vpm_disparity": (i32, [vp, vp, i32, i32, f32, vp]),
+        "pm_svpm_create": (i32, [C.POINTER(vp), i32]),
+        "pm_svpm_destroy": (i32, [vp]),
+        "pm_svpm_last_error": (C.c_char_p, [vp]),
+        "pm_svpm_flow": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, vp, vp, vp]),
+        "pm_svpm_flow_device": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, vp, vp, vp, vp]),
+        "pm_svpm_set_counting": (i32, [vp, i32]),
+        "pm_svpm_get_counters": (i32, [vp, C.POINTER(C.c_uint64)]),
+        "pm_k_svpm_init": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, vp]),
+        "pm_k_svpm_prop": (i32, [vp, vp, vp, vp, vp, vp, i32, i32, sz, i32, f32, i32, vp]),
+        "pm_k_svpm_to_flow": (i32, [vp, vp, i32, i32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

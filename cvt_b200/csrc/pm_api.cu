@@ -1413,6 +1413,7 @@ float pm_expf_host(float x) { return expf_(x); }
 float pm_sinf_host(float x) { float s, c; sincosf_(x, &s, &c); return s; }
 float pm_cosf_host(float x) { float s, c; sincosf_(x, &s, &c); return c; }
 float pm_acospif_host(float x) { return acospif_(x); }
+float pm_logf_host(float x) { return logf_(x); }
 float pm_exit_threshold_host(float m, float b) { return exit_threshold(m, b); }
 
 }  // extern "C"

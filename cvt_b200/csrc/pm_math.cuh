@@ -12,7 +12,9 @@
 //   sincos  Cody-Waite reduction by pi/2 (three-part constant), Taylor
 //           polynomials of degree 9 / 10 on |r| <= pi/4 (1.42 ulp);
 //   acospi  arcsine Maclaurin series on |x| <= 1/2, half-angle identity beyond
-//           (2.4 ulp).
+//           (2.4 ulp);
+//   log     (SVPMFlow.cl:42) x = 2^k m, m in [sqrt(1/2), sqrt(2)], s = (m-1)/(m+1),
+//           log(m) = 2 atanh(s) by its series to s^11, plus k ln2 (two-part).
 // Build with -fmad=false (device) and -ffp-contract=off (host) so that only the
 // explicit fmaf calls fuse.
 #pragma once
@@ -47,6 +49,41 @@ PM_HD uint32_t f2u(float f)
 }
 
 PM_HD float pow2i(int n) { return u2f((uint32_t)(n + 127) << 23); }
+
+PM_HD float logf_(float x)
+{
+    if (x != x) return x;
+    if (x < 0.0f) return (x - x) / (x - x);
+    if (x == 0.0f) return u2f(0xff800000u);
+    if (x == u2f(0x7f800000u)) return x;
+    int k = 0;
+    uint32_t u = f2u(x);
+    if (u < 0x00800000u) {
+        x *= 8388608.0f;
+        k = -23;
+        u = f2u(x);
+    }
+    k += (int)(u >> 23) - 127;
+    u = (u & 0x007fffffu) | 0x3f800000u;
+    if (u > 0x3fb504f3u) {
+        u -= 0x00800000u;
+        k += 1;
+    }
+    const float f = u2f(u) - 1.0f;
+    const float s = f / (2.0f + f);
+    const float z = s * s;
+    // log(m) = f - (f^2/2 - s (f^2/2 + R)), R = 2 (z/3 + ... + z^5/11) (fdlibm's e_log.c form)
+    float R = 1.8181819e-1f;               /* 2/11 */
+    R = fmaf(R, z, 2.2222222e-1f);
+    R = fmaf(R, z, 2.8571430e-1f);
+    R = fmaf(R, z, 4.0000001e-1f);
+    R = fmaf(R, z, 6.6666669e-1f);
+    R = R * z;
+    const float hfsq = (0.5f * f) * f;
+    const float kf = (float)k;
+    const float lo = fmaf(s, hfsq + R, kf * 1.428606765330187045e-06f);
+    return fmaf(kf, 0.693145751953125f, f - (hfsq - lo));
+}
 
 PM_HD float expf_(float x)
 {

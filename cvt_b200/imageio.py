@@ -3,7 +3,8 @@ libcvtpm's host I/O (pm_pfm_* / pm_cvtraw_*).
 
     save_pfm(path, a)      a: (H, W) or (H, W, 4) float32; RGBA is saved without alpha
     load_pfm(path)         -> (H, W) or (H, W, 4) float32 (alpha 1)
-    save_cvtraw(path, a)   a: (H, W) float32, (H, W, 4) float32 or (H, W, 4) uint8
+    save_cvtraw(path, a)   a: (H, W) float32, (H, W, 2) float32 (flow), (H, W, 4) float32 or
+                           (H, W, 4) uint8
     load_cvtraw(path)      -> array of the saved format
 """
 import ctypes as C
@@ -13,8 +14,9 @@ import numpy as np
 from . import _lib
 
 # IFormat ids of cvt/gfx/IFormat.h:36-65 (PM_IFORMAT_* of cvtpm.h)
-_FORMATS = {(1, np.dtype(np.float32)): 4, (4, np.dtype(np.uint8)): 9, (4, np.dtype(np.float32)): 12}
-_DTYPES = {4: (np.float32, 1), 9: (np.uint8, 4), 12: (np.float32, 4)}
+_FORMATS = {(1, np.dtype(np.float32)): 4, (2, np.dtype(np.float32)): 8, (4, np.dtype(np.uint8)): 9,
+            (4, np.dtype(np.float32)): 12}
+_DTYPES = {4: (np.float32, 1), 8: (np.float32, 2), 9: (np.uint8, 4), 12: (np.float32, 4)}
 
 
 def _check(st):
@@ -46,7 +48,7 @@ def save_cvtraw(path, a):
     ch = 1 if a.ndim == 2 else a.shape[2]
     fid = _FORMATS.get((ch, a.dtype))
     if fid is None:
-        raise ValueError("CVTRaw: GRAY_FLOAT, RGBA_FLOAT or RGBA_UINT8 images")
+        raise ValueError("CVTRaw: GRAY_FLOAT, GRAYALPHA_FLOAT, RGBA_FLOAT or RGBA_UINT8 images")
     H, W = a.shape[:2]
     _check(_lib.lib().pm_cvtraw_save(str(path).encode(), a.ctypes.data, W, H, a.strides[0], fid))
 

@@ -10,8 +10,8 @@
  *                     DisparityPostProcessing pp = DISPARITY_PP_LRCHECK, Image* normalmap = NULL,
  *                     const Image* initdisparity = NULL, const Image* initnormalmap = NULL);
  * and its error behaviour (a cvt::Exception on inconsistent inputs or a device error).
- * cvt::Image here is a minimal host image with the three formats the path uses:
- * RGBA_UINT8 (inputs), GRAY_FLOAT (disparity), RGBA_FLOAT (normals).  As in the
+ * cvt::Image here is a minimal host image with the formats the path uses:
+ * RGBA_UINT8 (inputs), GRAY_FLOAT (disparity), RGBA_FLOAT (normals), GRAYALPHA_FLOAT (flow).  As in the
  * reference, dmap and *normalmap are reallocated by the callee.
  *
  * Differences from the reference, by design: no OpenCL context (CL::init) is needed;
@@ -39,18 +39,20 @@ class Exception : public std::runtime_error {
 };
 
 struct IFormat {
-    enum Id { GRAY_FLOAT_ID, RGBA_UINT8_ID, RGBA_FLOAT_ID };
+    enum Id { GRAY_FLOAT_ID, RGBA_UINT8_ID, RGBA_FLOAT_ID, GRAYALPHA_FLOAT_ID };
     Id id;
     size_t channels, bpc;
     static const IFormat GRAY_FLOAT;
     static const IFormat RGBA_UINT8;
     static const IFormat RGBA_FLOAT;
+    static const IFormat GRAYALPHA_FLOAT;
     bool operator==(const IFormat& o) const { return id == o.id; }
     bool operator!=(const IFormat& o) const { return id != o.id; }
 };
 inline const IFormat IFormat::GRAY_FLOAT = {IFormat::GRAY_FLOAT_ID, 1, 4};
 inline const IFormat IFormat::RGBA_UINT8 = {IFormat::RGBA_UINT8_ID, 4, 1};
 inline const IFormat IFormat::RGBA_FLOAT = {IFormat::RGBA_FLOAT_ID, 4, 4};
+inline const IFormat IFormat::GRAYALPHA_FLOAT = {IFormat::GRAYALPHA_FLOAT_ID, 2, 4};
 
 /* host image, rows of `stride` bytes */
 class Image {
@@ -82,7 +84,8 @@ class Image {
         const int w = (int)_w, h = (int)_h;
         int rc;
         if (ends_with(path, ".pfm") || ends_with(path, ".PFM")) {
-            if (_fmt == IFormat::RGBA_UINT8) throw Exception("PFM holds float images");
+            if (_fmt == IFormat::RGBA_UINT8 || _fmt == IFormat::GRAYALPHA_FLOAT)
+                throw Exception("PFM holds grey or RGB float images");
             rc = pm_pfm_save(path.c_str(), reinterpret_cast<const float*>(_data.data()), w, h, (int)_fmt.channels,
                              _stride);
         } else if (ends_with(path, ".cvtraw")) {
@@ -106,6 +109,7 @@ class Image {
             if (fid == PM_IFORMAT_GRAY_FLOAT) reallocate(w, h, IFormat::GRAY_FLOAT);
             else if (fid == PM_IFORMAT_RGBA_UINT8) reallocate(w, h, IFormat::RGBA_UINT8);
             else if (fid == PM_IFORMAT_RGBA_FLOAT) reallocate(w, h, IFormat::RGBA_FLOAT);
+            else if (fid == PM_IFORMAT_GRAYALPHA_FLOAT) reallocate(w, h, IFormat::GRAYALPHA_FLOAT);
             else throw Exception("CVTRaw: format not supported here");
             if (pm_cvtraw_load(path.c_str(), _data.data(), _data.size(), _stride, &w, &h, &st, &fid) != PM_OK)
                 throw Exception(pm_io_last_error());
@@ -124,6 +128,7 @@ class Image {
     {
         if (f == IFormat::GRAY_FLOAT) return PM_IFORMAT_GRAY_FLOAT;
         if (f == IFormat::RGBA_UINT8) return PM_IFORMAT_RGBA_UINT8;
+        if (f == IFormat::GRAYALPHA_FLOAT) return PM_IFORMAT_GRAYALPHA_FLOAT;
         return PM_IFORMAT_RGBA_FLOAT;
     }
     size_t _w, _h;

@@ -244,6 +244,7 @@ float pm_expf_host(float x);
 float pm_sinf_host(float x);
 float pm_cosf_host(float x);
 float pm_acospif_host(float x);
+float pm_logf_host(float x);
 /* smallest c >= 0 with RN(c / b) >= m (the early-exit threshold of the cost loop) */
 float pm_exit_threshold_host(float m, float b);
 
@@ -264,7 +265,7 @@ int pm_scene_generate(uint64_t seed, int width, int height, int nplanes, float d
  * (bytes), IFormat id (PM_IFORMAT_*), then height rows of stride bytes.  pm_cvtraw_load with
  * out NULL only reads the header; out_stride 0 keeps the saved stride; capacity in bytes.
  * Errors: a status code, the message in pm_io_last_error(). */
-enum { PM_IFORMAT_GRAY_FLOAT = 4, PM_IFORMAT_RGBA_UINT8 = 9, PM_IFORMAT_RGBA_FLOAT = 12 };
+enum { PM_IFORMAT_GRAY_FLOAT = 4, PM_IFORMAT_GRAYALPHA_FLOAT = 8, PM_IFORMAT_RGBA_UINT8 = 9, PM_IFORMAT_RGBA_FLOAT = 12 };
 int pm_pfm_save(const char* path, const float* data, int width, int height, int channels, size_t stride);
 int pm_pfm_load(const char* path, float* out, size_t capacity, int* width, int* height, int* channels);
 int pm_cvtraw_save(const char* path, const void* data, int width, int height, size_t stride, int format_id);
@@ -314,6 +315,46 @@ int pm_k_vpm_init(float* out, const uint8_t* c1, const float* g1, const uint8_t*
 int pm_k_vpm_iter(float* out, const float* in, const uint8_t* c1, const float* g1, const uint8_t* c2, const float* g2,
                   int W, int H, size_t stride, int r, float dmax, int iter, void* stream);
 int pm_k_vpm_disparity(float* out, const float* states, int W, int H, float scale, void* stream);
+
+/* ---- SVPMFlowCL (cvt/vision/SVPMFlowCL.h, SVPMFlowCL.cpp, cvt/cl/kernel/SVPMFlow.cl) ----
+ * PatchMatch optical flow with a TV pull: states (u, v, cost, 0) (pixel (x, y) of the first
+ * frame moves to (x + u, y + v)), duals W*H float4 (the dual field p of the flow's TV), flow
+ * W*H float2 (u, v).  Frames RGBA8 with `stride` bytes per row.  Errors: a status code, the
+ * message in pm_svpm_last_error(handle) (NULL handle: the calling thread's last handle-free
+ * error).
+ * The reference's propagation kernel reads and writes the group buffer in one barrier
+ * interval in its jump steps (SVPMFlow.cl:673-690), which OpenCL leaves undefined; here every
+ * jump step reads the states of the previous step.  Its svpmflow_state_refine reads an
+ * unwritten vector (:60-61), taken as zero. */
+typedef struct pm_svpm pm_svpm;
+enum { PM_SVPM_MAXITER = 200 };   /* MAXITER, the passes SVPMFlowCL::flow runs (SVPMFlowCL.cpp:40) */
+
+/* SVPMFlowCL::SVPMFlowCL / ~SVPMFlowCL (SVPMFlowCL.cpp:41-56) on a CUDA device; PM_ENODEV without one */
+int pm_svpm_create(pm_svpm** out, int device);
+int pm_svpm_destroy(pm_svpm* h);
+const char* pm_svpm_last_error(const pm_svpm* h);
+/* SVPMFlowCL::flow(flow, first, second, patchsize, flowmax) (:58-89), host buffers, synchronous,
+ * with `iterations` passes (PM_SVPM_MAXITER in the reference).  Its debugging block (:74-84: an
+ * AEE print, a colour-coded PNG and a wait for a key press after every pass) is not reproduced;
+ * it changes no result.  states and duals may be NULL. */
+int pm_svpm_flow(pm_svpm* h, const uint8_t* first, const uint8_t* second, int W, int H, size_t stride, int patchsize,
+                 float flowmax, int iterations, float* flow, float* states, float* duals);
+/* the same on device buffers, enqueued on `stream` */
+int pm_svpm_flow_device(pm_svpm* h, const uint8_t* first, const uint8_t* second, int W, int H, size_t stride,
+                        int patchsize, float flowmax, int iterations, float* flow, float* states, float* duals,
+                        void* stream);
+/* cost-window taps of the propagation passes of the calls made while counting is on */
+int pm_svpm_set_counting(pm_svpm* h, int on);
+int pm_svpm_get_counters(pm_svpm* h, uint64_t c[1]);
+/* One reference kernel per call, device buffers, enqueued on `stream`:
+ *   pm_k_svpm_init     svpmflow_init (SVPMFlow.cl:213-233)
+ *   pm_k_svpm_prop     svpmflow_prop_local_tv_admm (:574-731), pass index `iter` (1-based in flow)
+ *   pm_k_svpm_to_flow  svpmflow_flow (:733-744) */
+int pm_k_svpm_init(float* out, const uint8_t* first, const uint8_t* second, int W, int H, size_t stride, int r,
+                   float flowmax, void* stream);
+int pm_k_svpm_prop(float* out, float* pout, const float* in, const float* pin, const uint8_t* first,
+                   const uint8_t* second, int W, int H, size_t stride, int r, float flowmax, int iter, void* stream);
+int pm_k_svpm_to_flow(float* flow, const float* states, int W, int H, void* stream);
 
 #ifdef __cplusplus
 }

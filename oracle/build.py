@@ -8,7 +8,7 @@ cpu_baseline leg:
                            (cvt/cl/kernel/pmhstereo.cl, PDDiffTensor.cl,
                            PDDROFDiffTensor.cl, PDDHuberDiffTensor.cl,
                            pyr/pyrdown.cl, pyr/pyrupmul.cl, VPMStereo.cl,
-                           gradxy.cl)
+                           gradxy.cl, SVPMFlow.cl)
                            rewritten by translate.py and
                            compiled against clshim.h, when the reference tree is
                            present (it is not on GPU machines; the built .so
@@ -52,11 +52,11 @@ def build_ref(force=False, kernel_dir=REF_KERNELS):
         return out if os.path.exists(out) else None
     os.makedirs(refdir, exist_ok=True)
     cls = ["pmhstereo.cl", "PDDiffTensor.cl", "PDDROFDiffTensor.cl", "PDDHuberDiffTensor.cl", "VPMStereo.cl",
-           "gradxy.cl"]
+           "gradxy.cl", "SVPMFlow.cl"]
     deps = [os.path.join(kernel_dir, f) for f in cls + ["RNG.cl", "MWC64X.cl", "Matrix3.cl"]]
     pyr = ["pyrdown.cl", "pyrupmul.cl"]
     deps += [os.path.join(kernel_dir, "pyr", f) for f in pyr]
-    glue = [os.path.join(HERE, f) for f in ("ref_pmh.cpp", "ref_pd.cpp", "ref_pyr.cpp", "ref_vpm.cpp", "ref_driver.cpp")]
+    glue = [os.path.join(HERE, f) for f in ("ref_pmh.cpp", "ref_pd.cpp", "ref_pyr.cpp", "ref_vpm.cpp", "ref_svpm.cpp", "ref_driver.cpp")]
     hdrs = [os.path.join(HERE, f) for f in ("clshim.h", "ref_exec.h", "pm_hostloop.h", "pm_libm.h", "translate.py")]
     if not (force or _stale(out, deps + glue + hdrs)):
         return out

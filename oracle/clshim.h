@@ -11,8 +11,9 @@
  *  - vector types with the swizzles the sources use (.x .y .z .w, .xy .yz .xyz,
  *    .lo .hi; the multi-letter ones become member calls in the rewrite);
  *  - vector relational results are -1 per true lane, scalar ones 1;
- *  - exp/native_exp, sin, cos, acospi come from oracle/pm_libm.h; sqrt, the
+ *  - exp/native_exp, log, sin, cos, acospi come from oracle/pm_libm.h; sqrt, the
  *    division and native_rsqrt (1/sqrt) are correctly rounded; pow(x, 1) = x;
+ *    length(v) = sqrt(dot(v, v));
  *  - normalize follows OpenCL 1.2 s6.12.5 (a zero vector is returned as is);
  *  - convert_int*: NaN -> 0, out-of-range values saturate;
  *  - image reads implement OpenCL 1.2 s8.2 in full FP32 (UNORM_INT8 as v/255),
@@ -110,6 +111,9 @@ template <class V, class P> struct Half {
         N2 xy() const { return N2(x, y); }                                             \
         N2 yz() const { return N2(y, z); }                                             \
         N3 xyz() const { return N3(x, y, z); }                                         \
+        N2 zw() const { return N2(z, w); }                                             \
+        N2 lo() const { return N2(x, y); }                                             \
+        N2 hi() const { return N2(z, w); }                                             \
     };
 
 CL_VEC2(float, float2)
@@ -190,7 +194,7 @@ inline float native_sqrt(float x) { return std::sqrt(x); }
 inline float native_rsqrt(float x) { return 1.0f / std::sqrt(x); }
 inline float exp(float x) { return orc_expf(x); }
 inline float native_exp(float x) { return orc_expf(x); }
-inline float log(float x) { return std::log(x); }
+inline float log(float x) { return orc_logf(x); }
 inline double log(double x) { return std::log(x); }
 inline float native_log(float x) { return std::log(x); }
 inline float cos(float x) { return orc_cosf(x); }
@@ -224,6 +228,10 @@ inline float3 fabs(float3 v) { return float3(fabs(v.x), fabs(v.y), fabs(v.z)); }
 inline float4 fabs(float4 v) { return float4(fabs(v.x), fabs(v.y), fabs(v.z), fabs(v.w)); }
 inline float3 fmin(float3 a, float3 b) { return float3(fmin(a.x, b.x), fmin(a.y, b.y), fmin(a.z, b.z)); }
 inline float3 fmin(float3 a, float b) { return fmin(a, float3(b)); }
+inline float3 fmax(float3 a, float3 b) { return float3(fmax(a.x, b.x), fmax(a.y, b.y), fmax(a.z, b.z)); }
+inline float3 clamp(float3 x, float3 lo, float3 hi) { return fmin(fmax(x, lo), hi); }
+inline float2 fmin(float2 a, float2 b) { return float2(fmin(a.x, b.x), fmin(a.y, b.y)); }
+inline float2 fmax(float2 a, float2 b) { return float2(fmax(a.x, b.x), fmax(a.y, b.y)); }
 inline float4 fmin(float4 a, float4 b) { return float4(fmin(a.x, b.x), fmin(a.y, b.y), fmin(a.z, b.z), fmin(a.w, b.w)); }
 inline float4 fmin(float4 a, float b) { return fmin(a, float4(b)); }
 inline float4 fmax(float4 a, float4 b) { return float4(fmax(a.x, b.x), fmax(a.y, b.y), fmax(a.z, b.z), fmax(a.w, b.w)); }
@@ -232,6 +240,8 @@ inline float4 fmax(float4 a, float b) { return fmax(a, float4(b)); }
 inline float3 sqrt(float3 v) { return float3(sqrt(v.x), sqrt(v.y), sqrt(v.z)); }
 inline float4 sqrt(float4 v) { return float4(sqrt(v.x), sqrt(v.y), sqrt(v.z), sqrt(v.w)); }
 inline float dot(float2 a, float2 b) { return a.x * b.x + a.y * b.y; }
+inline float length(float2 v) { return sqrt(dot(v, v)); }
+inline float4 xxyy_(float2 v) { return float4(v.x, v.x, v.y, v.y); }
 inline float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline float dot(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
 inline float length(float3 v) { return sqrt(dot(v, v)); }

@@ -26,6 +26,11 @@
  *  - acospi: arcsine Maclaurin series (coefficients (2k)!/(4^k (k!)^2 (2k+1)))
  *            on |x| <= 1/2 and the half-angle identity
  *            acos(x) = 2 asin(sqrt((1-x)/2)) beyond.
+ *  - log:    (cvt/cl/kernel/SVPMFlow.cl:42, Box-Muller) x = 2^k m with m in
+ *            [sqrt(1/2), sqrt(2)], f = m - 1 (exact), s = f / (2 + f) and
+ *            log(m) = 2 atanh(s) = f - (f^2/2 - s (f^2/2 + R)) with R = 2 (s^2/3 + ... + s^10/11)
+ *            (the arrangement of fdlibm's e_log.c), |s| <= 0.1716;
+ *            log(x) = k ln2 + log(m) with the two-part ln2 of exp.
  * Every operation is an IEEE single-precision add, multiply, fma, sqrt or
  * divide, so the results are the same on any conforming machine.
  */
@@ -131,6 +136,42 @@ static inline float orc_acospif(float x)
         a = 1.57079637050628662f - orc_asin_small(x);
     }
     return a * INV_PI;
+}
+
+static inline float orc_logf(float x)
+{
+    if (x != x) return x;
+    if (x < 0.0f) return (x - x) / (x - x);
+    if (x == 0.0f) return -INFINITY;
+    if (x == INFINITY) return x;
+    int k = 0;
+    uint32_t u = orc_f2bits(x);
+    if (u < 0x00800000u) {   /* subnormal: scale by 2^23 */
+        x *= 8388608.0f;
+        k = -23;
+        u = orc_f2bits(x);
+    }
+    k += (int)(u >> 23) - 127;
+    u = (u & 0x007fffffu) | 0x3f800000u;   /* m in [1, 2) */
+    if (u > 0x3fb504f3u) {                 /* above sqrt(2): m / 2 */
+        u -= 0x00800000u;
+        k += 1;
+    }
+    const float f = orc_bits2f(u) - 1.0f;
+    const float s = f / (2.0f + f);
+    const float z = s * s;
+    /* R = 2 (z/3 + z^2/5 + ... + z^5/11); log(m) = f - (f^2/2 - s (f^2/2 + R)), the form of
+     * fdlibm's e_log.c, which keeps the rounding of s out of the leading term */
+    float R = 1.8181819e-1f;               /* 2/11 */
+    R = fmaf(R, z, 2.2222222e-1f);         /* 2/9 */
+    R = fmaf(R, z, 2.8571430e-1f);         /* 2/7 */
+    R = fmaf(R, z, 4.0000001e-1f);         /* 2/5 */
+    R = fmaf(R, z, 6.6666669e-1f);         /* 2/3 */
+    R = R * z;
+    const float hfsq = (0.5f * f) * f;
+    const float kf = (float)k;
+    const float lo = fmaf(s, hfsq + R, kf * 1.428606765330187045e-06f);
+    return fmaf(kf, 0.693145751953125f, f - (hfsq - lo));
 }
 
 #endif

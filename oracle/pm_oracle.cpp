@@ -529,6 +529,7 @@ extern "C" {
 int orc_version(void) { return 1; }
 
 float orc_exp(float x) { return orc_expf(x); }
+float orc_log(float x) { return orc_logf(x); }
 float orc_sin(float x) { return orc_sinf(x); }
 float orc_cos(float x) { return orc_cosf(x); }
 float orc_acospi(float x) { return orc_acospif(x); }
@@ -1267,6 +1268,248 @@ int orc_vpm_disparity_simple(float* disparity, float* states, const uint8_t* c1,
     }
     orc_vpm_disparity(disparity, out[1 - swap], W, H, 1.0f);
     if (states) memcpy(states, out[1 - swap], 4 * N * sizeof(float));
+    return 0;
+}
+
+/* ---- SVPMFlowCL (cvt/vision/SVPMFlowCL.cpp, cvt/cl/kernel/SVPMFlow.cl) --------------------
+ * PatchMatch optical flow: a state is (u, v, cost, 0); candidates are tested against a
+ * quadratic pull towards a TV-smoothed flow (a primal-dual step on a dual field p, ADMM
+ * style).  The kernel works on 16x16 work-groups with the states of the group and a 4-pixel
+ * apron in local memory; the neighbour tests of a group see each other's updates. */
+
+/* read_imagef with SAMPLER_BILINEAR (CLK_ADDRESS_CLAMP_TO_EDGE) at (u, v), OpenCL 1.2 s8.2:
+ * the four weights (1-a)(1-b), a(1-b), (1-a)b, ab and the sum in that order */
+static F4 bilinear2d(const Img4& im, float u, float v)
+{
+    if (!isfin(u) || !isfin(v)) { const float n = orc_bits2f(0x7fffffffu); return f4(n, n, n, n); }
+    const float tu = u - 0.5f, tv = v - 0.5f;
+    const float fu = floorf(tu), fv = floorf(tv);
+    const float a = tu - fu, b = tv - fv;
+    const int i0 = (int)fminf(fmaxf(fu, -2.0f), (float)im.W + 1.0f), j0 = (int)fminf(fmaxf(fv, -2.0f), (float)im.H + 1.0f);
+    const F4 T00 = im.edge(i0, j0), T10 = im.edge(i0 + 1, j0), T01 = im.edge(i0, j0 + 1), T11 = im.edge(i0 + 1, j0 + 1);
+    const float w00 = (1.0f - a) * (1.0f - b), w10 = a * (1.0f - b), w01 = (1.0f - a) * b, w11 = a * b;
+    return f4(((w00 * T00.x + w10 * T10.x) + w01 * T01.x) + w11 * T11.x,
+              ((w00 * T00.y + w10 * T10.y) + w01 * T01.y) + w11 * T11.y,
+              ((w00 * T00.z + w10 * T10.z) + w01 * T01.z) + w11 * T11.z,
+              ((w00 * T00.w + w10 * T10.w) + w01 * T01.w) + w11 * T11.w);
+}
+
+/* svpmflow_eval_bilateral_trunc_sad (SVPMFlow.cl:170-209), the cost svpmflow_eval names (:211) */
+static float svpm_eval(const Img4& c1, const Img4& c2, float cx, float cy, float fx, float fy, int r)
+{
+    if (!(isfin(fx) && isfin(fy))) return 1e10f;
+    const int W = c2.W, H = c2.H;
+    const F4 vc = bilinear2d(c1, cx + 0.5f, cy + 0.5f);
+    float ret = 0.0f, wsum = 0.0f;
+    for (float dy = (float)-r; dy <= (float)r; dy += 1.0f)
+        for (float dx = (float)-r; dx <= (float)r; dx += 1.0f) {
+            const float px = cx + dx, py = cy + dy;
+            const float qx = px + fx, qy = py + fy;
+            if (px < 0 || px >= W || py < 0 || py >= H || qx < 0 || qx >= W || qy < 0 || qy >= H) continue;
+            const F4 v1 = bilinear2d(c1, px + 0.5f, py + 0.5f);
+            const F4 v2 = bilinear2d(c2, qx + 0.5f, qy + 0.5f);
+            const float w = orc_expf(-((fabsf(vc.x - v1.x) * 1.0f + fabsf(vc.y - v1.y) * 1.0f) + fabsf(vc.z - v1.z) * 1.0f) * 2.6f);
+            wsum += w;
+            ret += w * ((fminf(fabsf(v1.x - v2.x), 0.02f) * 1.0f + fminf(fabsf(v1.y - v2.y), 0.02f) * 1.0f) +
+                        fminf(fabsf(v1.z - v2.z), 0.02f) * 1.0f);
+        }
+    if (wsum < 1.1f) return 1e5f;
+    return ret / wsum;
+}
+
+/* box_mueller (:38-46): theta = 2.0f * M_PI * y is formed in double (M_PI is a double) */
+static void svpm_box_mueller(Rng& g, float* bx, float* by)
+{
+    const float x = g.next(), y = g.next();
+    const float rr = sqrtf(-2.0f * orc_logf(x));
+    const float theta = (float)(2.0 * M_PI * (double)y);
+    *bx = rr * orc_sinf(theta);
+    *by = rr * orc_cosf(theta);
+}
+
+/* svpmflow_state_init (:48-56) */
+static F4 svpm_state_init(Rng& g, float flowmax)
+{
+    float bx, by;
+    svpm_box_mueller(g, &bx, &by);
+    return f4(bx * flowmax * 0.5f, by * flowmax * 0.5f, 1e10f, 0.0f);
+}
+
+/* svpmflow_state_refine (:58-64).  Its `ret` is read before it is written (`ret.xy += ...`);
+ * it is taken as zero, the value-initialised vector of the reference kernels' host build, so
+ * the candidate is a small flow around zero */
+static F4 svpm_state_refine(Rng& g, float refinemax)
+{
+    float bx, by;
+    svpm_box_mueller(g, &bx, &by);
+    return f4(0.0f + bx * refinemax * 0.5f, 0.0f + by * refinemax * 0.5f, 1e10f, 0.0f);
+}
+
+/* RNG_init(&rng, linpos, 2 * (NUMRNDTRIES) * iter): the macro does not parenthesise its
+ * third argument, so the distance is the int product linpos * 2 * 2 * iter (RNG.cl:54-57) */
+static int32_t svpm_skip(int linpos, int factor) { return (int32_t)((uint32_t)linpos * (uint32_t)factor); }
+
+/* the flow images of both frames, RGBA8 read as k / 255 */
+struct SvpmFrames {
+    std::vector<float> f1, f2;
+    Img4 c1, c2;
+    SvpmFrames(const uint8_t* a, const uint8_t* b, int W, int H, int stride)
+        : f1(rgba8_to_float(a, W, H, stride)), f2(rgba8_to_float(b, W, H, stride))
+    {
+        c1 = {f1.data(), W, H};
+        c2 = {f2.data(), W, H};
+    }
+};
+
+/* svpmflow_init (:213-233) */
+int orc_svpm_init(float* out, const uint8_t* img1, const uint8_t* img2, int W, int H, int stride, int r, float flowmax)
+{
+    const SvpmFrames F(img1, img2, W, H, stride);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            Rng g;
+            g.init_skip(svpm_skip(y * W + x, 2));
+            F4 st = svpm_state_init(g, flowmax);
+            st.z = svpm_eval(F.c1, F.c2, (float)x, (float)y, st.x, st.y, r);
+            put4(out, (size_t)y * W + x, st);
+        }
+    return 0;
+}
+
+/* svpmflow_prop_local_tv_admm (:574-731), one 16x16 work-group at a time.  The neighbour
+ * tests (:673-690) read a neighbour's cell of the group buffer while that neighbour may be
+ * writing it in the same barrier interval; here every test reads the cells as they were at
+ * the interval's start (all reads of a step happen before its writes). */
+int orc_svpm_prop(float* out, float* pout, const float* in, const float* pin, const uint8_t* img1,
+                  const uint8_t* img2, int W, int H, int stride, int r, float flowmax, int iter)
+{
+    const SvpmFrames F(img1, img2, W, H, stride);
+    const Img4 I = {in, W, H}, P = {pin, W, H};
+    const int GX = (W + 15) / 16, GY = (H + 15) / 16;
+    const float tau = 0.1f, lambda0 = 0.01f;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int gid = 0; gid < GX * GY; gid++) {
+        const int gx = gid % GX, gy = gid / GX;
+        const int bx = gx * 16 - 4, by = gy * 16 - 4, bpx = gx * 16 - 1, bpy = gy * 16 - 1;
+        static thread_local F4 buf[24][24], bufp[18][18];
+        for (int y = 0; y < 24; y++)
+            for (int x = 0; x < 24; x++) buf[y][x] = I.edge(bx + x, by + y);
+        for (int y = 0; y < 18; y++)
+            for (int x = 0; x < 18; x++) {
+                const F4 p = P.zero(bpx + x, bpy + y);
+                const F4 A = buf[y + 3][x + 3], Bx = buf[y + 3][x + 4], By = buf[y + 4][x + 3];
+                const float dxx = Bx.x - A.x, dxy = Bx.y - A.y, dyx = By.x - A.x, dyy = By.y - A.y;
+                const F4 z = f4(p.x + dxx, p.y + dxy, p.z + dyx, p.w + dyy);
+                const float zx = fmaxf(0.0f, 1.0f - tau / fmaxf(sqrtf(z.x * z.x + z.y * z.y), 1e-10f));
+                const float zy = fmaxf(0.0f, 1.0f - tau / fmaxf(sqrtf(z.z * z.z + z.w * z.w), 1e-10f));
+                const F4 pn = f4((p.x + dxx) - z.x * zx, (p.y + dxy) - z.y * zx, (p.z + dyx) - z.z * zy,
+                                 (p.w + dyy) - z.w * zy);
+                bufp[y][x] = f4(pn.x + 0.5f * (pn.x - p.x), pn.y + 0.5f * (pn.y - p.y), pn.z + 0.5f * (pn.z - p.z),
+                                pn.w + 0.5f * (pn.w - p.w));
+            }
+        F4 ret[16][16], pw[16][16];
+        float curx[16][16], cury[16][16];
+        Rng g[16][16];
+        const float lam = iter < 5 ? 0.0f : 1.0f / (2.0f * lambda0 * 5.0f);
+        auto test = [&](int lx, int ly, float nx, float ny, float cost) {
+            F4& R = ret[ly][lx];
+            const float cx = curx[ly][lx], cy = cury[ly][lx];
+            const float an = nx - cx, bn = ny - cy, ar = R.x - cx, br = R.y - cy;
+            if (cost + lam * (an * an + bn * bn) < R.z + lam * (ar * ar + br * br)) {
+                R.x = nx;
+                R.y = ny;
+                R.z = cost;
+            }
+        };
+        for (int ly = 0; ly < 16; ly++)
+            for (int lx = 0; lx < 16; lx++) {
+                const int x = gx * 16 + lx, y = gy * 16 + ly;
+                const float fx = (float)x, fy = (float)y;
+                g[ly][lx].init_skip(svpm_skip(y * W + x, 2 * 2 * iter));
+                const F4 p = iter < 5 ? f4(0.0f, 0.0f, 0.0f, 0.0f) : bufp[ly + 1][lx + 1];
+                const F4 L = bufp[ly + 1][lx], U = bufp[ly][lx + 1];
+                const float divx = ((p.x - L.x) + p.z) - U.z, divy = ((p.y - L.y) + p.w) - U.w;
+                pw[ly][lx] = p;
+                ret[ly][lx] = buf[ly + 4][lx + 4];
+                curx[ly][lx] = ret[ly][lx].x + (lambda0 / tau) * divx;
+                cury[ly][lx] = ret[ly][lx].y + (lambda0 / tau) * divy;
+                test(lx, ly, curx[ly][lx], cury[ly][lx], svpm_eval(F.c1, F.c2, fx, fy, curx[ly][lx], cury[ly][lx], r));
+                for (int k = 0; k < 2; k++) {   /* random tries (:637-645) */
+                    const F4 n = svpm_state_init(g[ly][lx], flowmax);
+                    test(lx, ly, n.x, n.y, svpm_eval(F.c1, F.c2, fx, fy, n.x, n.y, r));
+                }
+                for (int k = 0; k < 2; k++) {   /* random neighbours within 5 px (:648-656) */
+                    const float rx = g[ly][lx].next();
+                    const int ox = (int)((rx - 0.5f) * 2.0f * 5.0f + 0.5f);
+                    const float ry = g[ly][lx].next();
+                    const int oy = (int)((ry - 0.5f) * 2.0f * 5.0f + 0.5f);
+                    const F4 n = I.edge(x + ox, y + oy);
+                    test(lx, ly, n.x, n.y, svpm_eval(F.c1, F.c2, fx, fy, n.x, n.y, r));
+                }
+            }
+        for (int ly = 0; ly < 16; ly++)
+            for (int lx = 0; lx < 16; lx++) buf[ly + 4][lx + 4] = ret[ly][lx];
+        /* jump steps 4, 2, 1 in the directions +x, +y, -x, -y (:668-694) */
+        for (int step = 4; step >= 1; step >>= 1) {
+            const int dirs[4][2] = {{step, 0}, {0, step}, {-step, 0}, {0, -step}};
+            for (int d = 0; d < 4; d++) {
+                for (int ly = 0; ly < 16; ly++)
+                    for (int lx = 0; lx < 16; lx++) {
+                        const F4 n = buf[(ly + 4 + dirs[d][1]) % 24][(lx + 4 + dirs[d][0]) % 24];
+                        const float fx = (float)(gx * 16 + lx), fy = (float)(gy * 16 + ly);
+                        test(lx, ly, n.x, n.y, svpm_eval(F.c1, F.c2, fx, fy, n.x, n.y, r));
+                    }
+                for (int ly = 0; ly < 16; ly++)
+                    for (int lx = 0; lx < 16; lx++) buf[ly + 4][lx + 4] = ret[ly][lx];
+            }
+        }
+        for (int ly = 0; ly < 16; ly++)
+            for (int lx = 0; lx < 16; lx++) {
+                const int x = gx * 16 + lx, y = gy * 16 + ly;
+                for (int k = 0; k < 2; k++) {   /* random refinement (:700-708) */
+                    const F4 n = svpm_state_refine(g[ly][lx], 1.0f);
+                    test(lx, ly, n.x, n.y, svpm_eval(F.c1, F.c2, (float)x, (float)y, n.x, n.y, r));
+                }
+                if (x < W && y < H) {
+                    put4(pout, (size_t)y * W + x, pw[ly][lx]);
+                    put4(out, (size_t)y * W + x, ret[ly][lx]);
+                }
+            }
+    }
+    return 0;
+}
+
+/* svpmflow_flow (:733-744): (u, v) per pixel */
+int orc_svpm_to_flow(float* flow, const float* states, int W, int H)
+{
+    for (size_t i = 0; i < (size_t)W * H; i++) {
+        flow[2 * i] = states[4 * i];
+        flow[2 * i + 1] = states[4 * i + 1];
+    }
+    return 0;
+}
+
+/* SVPMFlowCL::flow (SVPMFlowCL.cpp:58-89) with `iterations` passes (the reference runs MAXITER
+ * = 200, :40) and without its debugging block (:74-84: AEE print, a colour-coded PNG and a wait
+ * for a key press after every pass; no result depends on it).  states / duals (NULL: not
+ * returned) get the final state and dual fields. */
+int orc_svpm_flow(float* flow, float* states, float* duals, const uint8_t* img1, const uint8_t* img2, int W, int H,
+                  int stride, int r, float flowmax, int iterations)
+{
+    const size_t N = (size_t)W * H;
+    std::vector<float> s0(4 * N), s1(4 * N), p0(4 * N, 0.0f), p1(4 * N, 0.0f);
+    float* buf[2] = {s0.data(), s1.data()};
+    float* bufp[2] = {p0.data(), p1.data()};
+    orc_svpm_init(buf[1], img1, img2, W, H, stride, r, flowmax);
+    for (int i = 0; i < iterations; i++) {
+        const int swap = i & 1;
+        orc_svpm_prop(buf[swap], bufp[swap], buf[1 - swap], bufp[1 - swap], img1, img2, W, H, stride, r, flowmax, i + 1);
+    }
+    const int last = 1 - (iterations & 1);
+    orc_svpm_to_flow(flow, buf[last], W, H);
+    if (states) memcpy(states, buf[last], 4 * N * sizeof(float));
+    if (duals) memcpy(duals, bufp[last], 4 * N * sizeof(float));
     return 0;
 }
 

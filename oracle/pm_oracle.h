@@ -95,6 +95,7 @@ int orc_disparity_to_normal(float* out, const float* disp, int W, int H);
 int orc_rng_floats(int64_t linpos, int nd, int ndraws, float* out);
 /* elementary functions, for tests */
 float orc_exp(float x);
+float orc_log(float x);
 float orc_sin(float x);
 float orc_cos(float x);
 float orc_acospi(float x);
@@ -147,6 +148,15 @@ int orc_vpm_disparity(float* out, const float* states, int W, int H, float scale
 /* VPMStereoCL::disparitySimple; states (NULL: not returned) gets the final plane states */
 int orc_vpm_disparity_simple(float* disparity, float* states, const uint8_t* c1, const uint8_t* c2, int W, int H,
                              int stride, int r, int iterations, float dmax, const float* initdisp);
+
+/* SVPMFlowCL (cvt/vision/SVPMFlowCL.cpp, cvt/cl/kernel/SVPMFlow.cl): RGBA8 frames with
+ * `stride` bytes per row, states and duals W*H float4, flow W*H float2 */
+int orc_svpm_init(float* out, const uint8_t* img1, const uint8_t* img2, int W, int H, int stride, int r, float flowmax);
+int orc_svpm_prop(float* out, float* pout, const float* in, const float* pin, const uint8_t* img1,
+                  const uint8_t* img2, int W, int H, int stride, int r, float flowmax, int iter);
+int orc_svpm_to_flow(float* flow, const float* states, int W, int H);
+int orc_svpm_flow(float* flow, float* states, float* duals, const uint8_t* img1, const uint8_t* img2, int W, int H,
+                  int stride, int r, float flowmax, int iterations);
 
 #ifdef __cplusplus
 }

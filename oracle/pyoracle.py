@@ -83,6 +83,18 @@ class Oracle:
             fn.argtypes = args
             setattr(self, "_" + name, fn)
         self._st = (lambda W: [W * 4]) if kind == "orc" else (lambda W: [])
+        # SVPMFlowCL, same convention
+        fsig = {
+            "svpm_init": [vp, vp, vp, i32, i32] + st + [i32, f32],
+            "svpm_prop": [vp, vp, vp, vp, vp, vp, i32, i32] + st + [i32, f32, i32],
+            "svpm_to_flow": [vp, vp, i32, i32],
+            "svpm_flow": [vp, vp, vp, vp, vp, i32, i32] + st + [i32, f32, i32],
+        }
+        for name, args in fsig.items():
+            fn = getattr(self.L, p + name)
+            fn.restype = i32
+            fn.argtypes = args
+            setattr(self, "_" + name, fn)
         if kind == "orc":
             self.L.orc_disparity_map_dump.restype = i32
             self.L.orc_disparity_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, i32, i32, i32, vp, vp, vp,
@@ -90,7 +102,7 @@ class Oracle:
             self.L.orc_depth_map_dump.restype = i32
             self.L.orc_depth_map_dump.argtypes = [vp, vp, i32, i32, i32, i32, f32, i32, f32, i32, i32, vp, vp, vp,
                                                   vp, vp, vp, i32, vp, DUMP_FN, vp]
-            for fn in ("orc_exp", "orc_sin", "orc_cos", "orc_acospi"):
+            for fn in ("orc_exp", "orc_sin", "orc_cos", "orc_acospi", "orc_log"):
                 getattr(self.L, fn).restype = f32
                 getattr(self.L, fn).argtypes = [f32]
             self.L.orc_rng_floats.restype = i32
@@ -325,6 +337,42 @@ class Oracle:
         assert self._vpm_disparity_simple(disp.ctypes.data, states.ctypes.data, c1.ctypes.data, c2.ctypes.data, W, H,
                                           *self._st(W), r, iterations, dmax, _p(initdisp)) == 0
         return disp, states
+
+    # ---- SVPMFlowCL (cvt/vision/SVPMFlowCL.cpp) --------------------------------------
+    def svpm_init(self, img1, img2, r, flowmax):
+        """svpmflow_init (SVPMFlow.cl:213-233): states (u, v, cost, 0)."""
+        H, W = img1.shape[:2]
+        a, b = np.ascontiguousarray(img1, np.uint8), np.ascontiguousarray(img2, np.uint8)
+        out = _f4((H, W))
+        assert self._svpm_init(out.ctypes.data, a.ctypes.data, b.ctypes.data, W, H, *self._st(W), r, flowmax) == 0
+        return out
+
+    def svpm_prop(self, states, duals, img1, img2, r, flowmax, it):
+        """svpmflow_prop_local_tv_admm (SVPMFlow.cl:574-731). Returns (states, duals)."""
+        H, W = img1.shape[:2]
+        a, b = np.ascontiguousarray(img1, np.uint8), np.ascontiguousarray(img2, np.uint8)
+        s_in, p_in = np.ascontiguousarray(states, np.float32), np.ascontiguousarray(duals, np.float32)
+        out, pout = _f4((H, W)), _f4((H, W))
+        assert self._svpm_prop(out.ctypes.data, pout.ctypes.data, s_in.ctypes.data, p_in.ctypes.data, a.ctypes.data,
+                               b.ctypes.data, W, H, *self._st(W), r, flowmax, it) == 0
+        return out, pout
+
+    def svpm_to_flow(self, states):
+        H, W = states.shape[:2]
+        s_in = np.ascontiguousarray(states, np.float32)
+        out = np.zeros((H, W, 2), np.float32)
+        assert self._svpm_to_flow(out.ctypes.data, s_in.ctypes.data, W, H) == 0
+        return out
+
+    def svpm_flow(self, img1, img2, r, flowmax, iterations):
+        """SVPMFlowCL::flow (SVPMFlowCL.cpp:58-89) with `iterations` passes (reference: 200).
+        Returns (flow, states, duals)."""
+        H, W = img1.shape[:2]
+        a, b = np.ascontiguousarray(img1, np.uint8), np.ascontiguousarray(img2, np.uint8)
+        flow, states, duals = np.zeros((H, W, 2), np.float32), _f4((H, W)), _f4((H, W))
+        assert self._svpm_flow(flow.ctypes.data, states.ctypes.data, duals.ctypes.data, a.ctypes.data, b.ctypes.data,
+                               W, H, *self._st(W), r, flowmax, iterations) == 0
+        return flow, states, duals
 
     # ---- helpers (restatement only) ------------------------------------------------
     def rng_floats(self, linpos, nd, n):

@@ -46,7 +46,7 @@ def ref():
 
 def golden_cases():
     """disparityMap, single level (the reference's setting)"""
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith(("pyr", "depth", "vpm")))
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith(("pyr", "depth", "vpm", "svpm")))
 
 
 def pyramid_cases():
@@ -62,6 +62,11 @@ def depth_cases():
 def vpm_cases():
     """VPMStereoCL::disparitySimple"""
     return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("vpm"))
+
+
+def svpm_cases():
+    """SVPMFlowCL::flow"""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("svpm"))
 
 
 def load_golden(name):

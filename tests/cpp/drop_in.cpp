@@ -3,11 +3,13 @@
 // to argv[1] and, given argv[2], the map of depthMap (default dscale 1 / depthmax) there;
 // given argv[3], round-trips the disparity map through a .pfm file of that name; given
 // argv[4], writes the map of cvt::VPMStereoCL::disparitySimple (patch 3, 4 iterations,
-// range 24) there.
+// range 24) there; given argv[5], writes the flow of cvt::SVPMFlowCL::flow (patch 2, range 16,
+// 8 passes) there and checks that flowInit throws, as it does in the reference.
 #include <cstdio>
 #include <cstring>
 
 #include "cvt/vision/PMHuberStereo.h"
+#include "cvt/vision/SVPMFlowCL.h"
 #include "cvt/vision/VPMStereoCL.h"
 
 int main(int argc, char** argv)
@@ -52,6 +54,20 @@ int main(int argc, char** argv)
             f = fopen(argv[4], "wb");
             for (int y = 0; y < H; y++) fwrite(pd + y * sd, 4, W, f);
             fclose(f);
+        }
+        if (argc > 5) {
+            cvt::SVPMFlowCL svpm;
+            cvt::Image fl;
+            svpm.flow(fl, left, right, 2, 16.0f, NULL, 8);
+            pd = fl.map(&sd);
+            f = fopen(argv[5], "wb");
+            for (int y = 0; y < H; y++) fwrite(pd + y * sd, 8, W, f);
+            fclose(f);
+            try {
+                svpm.flowInit(fl, left, right, fl, 2, 16.0f);
+                return 6;
+            } catch (const cvt::Exception&) {
+            }
         }
         // inconsistent inputs throw, as in the reference (PMHuberStereo.cpp:412-414)
         cvt::Image small(W / 2, H, cvt::IFormat::RGBA_UINT8);

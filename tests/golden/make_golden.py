@@ -2,9 +2,9 @@
 
 The outputs come from cvt/cl/kernel/pmhstereo.cl, PDDiffTensor.cl,
 PDDROFDiffTensor.cl, PDDHuberDiffTensor.cl, pyr/pyrdown.cl, pyr/pyrupmul.cl,
-VPMStereo.cl and gradxy.cl compiled from their own source through the OpenCL-C shim
+VPMStereo.cl, gradxy.cl and SVPMFlow.cl compiled from their own source through the OpenCL-C shim
 (oracle/build.py -> oracle/_ref/libpmref.so), driven by the restated host loops
-of PMHuberStereo::disparityMap / depthMap and VPMStereoCL::disparitySimple.  Inputs are seeded procedural scenes from
+of PMHuberStereo::disparityMap / depthMap, VPMStereoCL::disparitySimple and SVPMFlowCL::flow.  Inputs are seeded procedural scenes from
 cvt_b200.scene.  Run from the repository root where the reference tree is
 available:
 
@@ -43,6 +43,13 @@ PYR_CASES = {
 VPM_CASES = {
     "vpm_48x32": (21, 48, 32, 5, 2.0, 12.0, 3, 16.0, 3, False),
     "vpm_init_41x27": (22, 41, 27, 4, 1.0, 9.0, 2, 12.0, 2, True),
+}
+
+# SVPMFlowCL::flow; name: (seed, W, H, nplanes, dlo, dhi, r, flowmax, passes).  The reference
+# runs 200 passes; the fixtures keep 7 and 12 (the TV pull starts at pass 5).
+SVPM_CASES = {
+    "svpm_40x30": (31, 40, 30, 4, 1.0, 8.0, 2, 8.0, 7),
+    "svpm_53x37": (32, 53, 37, 5, 1.0, 10.0, 3, 24.0, 12),
 }
 
 
@@ -176,6 +183,20 @@ def make_vpm_case(ref, name, spec):
     np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
 
 
+def make_svpm_case(ref, name, spec):
+    seed, W, H, npl, dlo, dhi, r, flowmax, passes = spec
+    first, second = scene.generate(seed, W, H, npl, dlo, dhi)
+    flow, states, duals = ref.svpm_flow(first, second, r, flowmax, passes)
+    arrays = {"first": first, "second": second, "flow": flow, "states": states, "duals": duals,
+              "spec": np.array([seed, W, H, npl, dlo, dhi, r, flowmax, passes], np.float64)}
+    # per-kernel fixtures: init, the first pass (no pull) and pass 6 (pull on) from fixed inputs
+    s0 = ref.svpm_init(first, second, r, flowmax)
+    s1, p1 = ref.svpm_prop(s0, np.zeros_like(s0), first, second, r, flowmax, 1)
+    s6, p6 = ref.svpm_prop(s1, p1 + 0.25, first, second, r, flowmax, 6)
+    arrays.update(k_init=s0, k_prop1=s1, k_dual1=p1, k_prop6=s6, k_dual6=p6, k_flow=ref.svpm_to_flow(s6))
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+
+
 def main():
     so = obuild.build_ref()
     if so is None:
@@ -193,6 +214,9 @@ def main():
         print("wrote", name)
     for name, spec in VPM_CASES.items():
         make_vpm_case(ref, name, spec)
+        print("wrote", name)
+    for name, spec in SVPM_CASES.items():
+        make_svpm_case(ref, name, spec)
         print("wrote", name)
 
 

@@ -74,6 +74,11 @@ def test_elementary_functions_match_oracle(native, orc):
     for x in np.linspace(-1, 1, 4001).astype(np.float32):
         assert np.float32(native.pm_acospif_host(float(x))).view(np.uint32) == \
             np.float32(orc.L.orc_acospi(float(x))).view(np.uint32)
+    lx = np.concatenate([rng.integers(0, 0x7f800001, 6000, dtype=np.uint32).view(np.float32),
+                         np.float32([0.0, 1.0, 2.3283064e-10, 1e-45, 0.5, 0.70710677, 1.4142135])])
+    for x in lx:
+        a, b = np.float32(native.pm_logf_host(float(x))), np.float32(orc.L.orc_log(float(x)))
+        assert a.view(np.uint32) == b.view(np.uint32) or (np.isnan(a) and np.isnan(b)), x
 
 
 def test_exit_threshold_is_exact(native):
@@ -195,3 +200,32 @@ def test_vpm_create_fails_loudly_without_device(native):
 
     with pytest.raises(StereoError):
         VPMStereoCL(3, 3, 16.0)
+
+
+def test_svpm_rejects_bad_arguments_without_touching_the_device(native):
+    from cvt_b200 import _lib
+
+    assert native.pm_svpm_create(None, 0) == _lib.PM_EINVAL_ARG
+    assert native.pm_svpm_flow(None, None, None, 8, 8, 32, 2, 4.0, 5, None, None, None) == _lib.PM_EINVAL_ARG
+    assert b"null" in native.pm_svpm_last_error(None)
+    assert native.pm_k_svpm_init(None, None, None, 0, 8, 32, 2, 4.0, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_k_svpm_init(None, None, None, 8, 8, 32, 40, 4.0, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_k_svpm_init(None, None, None, 8, 8, 32, 2, -1.0, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_k_svpm_init(None, None, None, 8, 8, 32, 2, 4.0, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_k_svpm_prop(None, None, None, None, None, None, 8, 8, 32, 2, 4.0, -1, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_k_svpm_to_flow(None, None, 8, 8, None) == _lib.PM_EINVAL_ARG
+
+
+def test_svpm_create_fails_loudly_without_device(native):
+    import torch
+
+    from cvt_b200 import _lib
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    h = C.c_void_p()
+    assert native.pm_svpm_create(C.byref(h), 0) == _lib.PM_ENODEV
+    from cvt_b200.svpm import StereoError, SVPMFlowCL
+
+    with pytest.raises(StereoError):
+        SVPMFlowCL()

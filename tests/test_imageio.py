@@ -58,12 +58,13 @@ def test_pfm_errors(io, tmp_path):
         io.load_pfm(tmp_path / "missing.pfm")
 
 
-@pytest.mark.parametrize("kind", ["gray", "rgba8", "rgbaf"])
+@pytest.mark.parametrize("kind", ["gray", "rgba8", "rgbaf", "flow"])
 def test_cvtraw_layout_and_round_trip(io, tmp_path, kind):
     rng = np.random.default_rng(1)
     a = {"gray": rng.random((5, 7), np.float32), "rgba8": rng.integers(0, 256, (5, 7, 4), dtype=np.uint8),
-         "rgbaf": rng.standard_normal((5, 7, 4)).astype(np.float32)}[kind]
-    fid = {"gray": 4, "rgba8": 9, "rgbaf": 12}[kind]
+         "rgbaf": rng.standard_normal((5, 7, 4)).astype(np.float32),
+         "flow": rng.standard_normal((5, 7, 2)).astype(np.float32)}[kind]
+    fid = {"gray": 4, "rgba8": 9, "rgbaf": 12, "flow": 8}[kind]
     p = tmp_path / "x.cvtraw"
     io.save_cvtraw(p, a)
     raw = p.read_bytes()

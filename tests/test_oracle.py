@@ -4,7 +4,7 @@ tests for the arithmetic it fixes."""
 import numpy as np
 import pytest
 
-from conftest import depth_cases, golden_cases, load_golden, pyramid_cases, vpm_cases
+from conftest import depth_cases, golden_cases, load_golden, pyramid_cases, svpm_cases, vpm_cases
 from oracle.pyoracle import bits_equal
 
 
@@ -256,3 +256,49 @@ def test_vpm_restatement_matches_reference_live(orc, ref, W, H, r, iters):
     a = orc.vpm_disparity_simple(L, R, r, iters, 6.0)
     b = ref.vpm_disparity_simple(L, R, r, iters, 6.0)
     assert bits_equal(a[0], b[0]).all() and bits_equal(a[1], b[1]).all()
+
+
+@pytest.mark.parametrize("case", svpm_cases())
+def test_svpm_restatement_matches_reference_golden(orc, case):
+    """SVPMFlowCL::flow and each of its kernels, bit for bit"""
+    g = load_golden(case)
+    seed, W, H, npl, dlo, dhi, r, flowmax, passes = g["spec"]
+    r, flowmax, passes = int(r), float(flowmax), int(passes)
+    flow, states, duals = orc.svpm_flow(g["first"], g["second"], r, flowmax, passes)
+    for a, k in ((flow, "flow"), (states, "states"), (duals, "duals")):
+        assert bits_equal(a, g[k]).all(), k
+    assert bits_equal(orc.svpm_init(g["first"], g["second"], r, flowmax), g["k_init"]).all()
+    s1, p1 = orc.svpm_prop(g["k_init"], np.zeros_like(g["k_init"]), g["first"], g["second"], r, flowmax, 1)
+    assert bits_equal(s1, g["k_prop1"]).all() and bits_equal(p1, g["k_dual1"]).all()
+    s6, p6 = orc.svpm_prop(g["k_prop1"], g["k_dual1"] + np.float32(0.25), g["first"], g["second"], r, flowmax, 6)
+    assert bits_equal(s6, g["k_prop6"]).all() and bits_equal(p6, g["k_dual6"]).all()
+    assert bits_equal(orc.svpm_to_flow(g["k_prop6"]), g["k_flow"]).all()
+
+
+@pytest.mark.parametrize("W,H,r,passes", [(1, 1, 1, 6), (5, 3, 0, 6), (17, 33, 2, 7), (16, 16, 3, 5)])
+def test_svpm_restatement_matches_reference_live(orc, ref, W, H, r, passes):
+    """edge sizes: a single pixel, r = 0, sizes one past the 16x16 work-group, exactly one group"""
+    from cvt_b200 import scene
+
+    a, b = scene.generate(60 + W, W, H, 3, 0.5, 4.0)
+    x = orc.svpm_flow(a, b, r, 6.0, passes)
+    y = ref.svpm_flow(a, b, r, 6.0, passes)
+    for u, v in zip(x, y):
+        assert bits_equal(u, v).all()
+
+
+def test_log_within_a_ulp(orc):
+    """the oracle's log (Box-Muller of SVPMFlow.cl:42) against double precision: <= 1 ulp,
+    and its special values"""
+    rng = np.random.default_rng(3)
+    bits = np.concatenate([rng.integers(1, 0x7f800000, 200000, dtype=np.uint32),
+                           np.arange(0x3f000000, 0x3f000000 + 20000, dtype=np.uint32),
+                           np.arange(0x3f800000 - 10000, 0x3f800000 + 10000, dtype=np.uint32)])
+    xs = bits.view(np.float32)
+    got = np.array([orc.L.orc_log(float(x)) for x in xs], np.float32)
+    want = np.log(xs.astype(np.float64))
+    ulp = np.spacing(np.abs(want).astype(np.float32)).astype(np.float64)
+    err = np.abs(got.astype(np.float64) - want) / ulp
+    assert err.max() <= 1.0, (err.max(), xs[err.argmax()])
+    assert orc.L.orc_log(1.0) == 0.0 and np.isneginf(orc.L.orc_log(0.0)) and np.isnan(orc.L.orc_log(-1.0))
+    assert np.isposinf(orc.L.orc_log(float("inf")))
