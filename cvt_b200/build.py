@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcvtpm.so")
 BUILD = os.path.join(HERE, "_build")
 
-CU_SOURCES = ["pm_kernels.cu", "pm_propagate.cu", "pm_api.cu", "pm_vpm.cu", "pm_svpm.cu"]
+CU_SOURCES = ["pm_kernels.cu", "pm_propagate.cu", "pm_api.cu", "pm_vpm.cu", "pm_svpm.cu", "pm_learn.cu"]
 CXX_SOURCES = ["pm_scene.cpp", "pm_io.cpp"]
 HEADERS = ["pm_math.cuh", "pm_device.cuh", "pm_window.cuh", "pm_kernels.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-fmad=false", "-std=c++17",
