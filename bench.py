@@ -24,6 +24,14 @@ collective on the data path); the step time is the maximum over ranks.
 (SVPMFlowCL.cpp:58-89) on the same pair taken as two frames: 7x7 window, flow
 range 128, the reference's 200 passes; metric Mpixel*passes/s.
 
+`--mode learned` measures the second half of the metric, "ms to plain-8-iter cost": a
+BF16 plane-proposal CNN (cvt_b200/learn.py; tcgen05 convolutions) is trained on the
+GPU (outside the timed region) on 64 procedural 512x384 pairs against plain 8-iteration
+PatchMatch, then on the hd pair the GPU time of proposal + k PatchMatch iterations is
+timed for growing k until its mean matching cost is within 1% of plain 8-iteration
+PatchMatch and its disparity within 1 px of it on >= 98% of the pixels plain
+PatchMatch keeps (LR check); value = that time in ms (null if no k up to 9 reaches it).
+
 `--impl reference` times the reference's CPU implementation instead: the
 reference kernel sources compiled through the OpenCL-C shim (oracle/_ref) when
 built, otherwise the CPU restatement (oracle/), on a bounded crop of the same
@@ -501,6 +509,95 @@ def run_svpm(args, wl, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_learned(args, wl, rank, world, local):
+    """--mode learned: time to plain 8-iteration PatchMatch's cost with the learned proposal"""
+    import torch
+    import torch.distributed as dist
+
+    from cvt_b200 import PMHuberStereo, scene
+    from cvt_b200.learn import PlaneProposal, make_training_set
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900))
+    W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
+    t0 = time.perf_counter()
+    feats, target = make_training_set(64, 512, 384, seed=100 + 1000 * rank, device=local)
+    t1 = time.perf_counter()
+    prop = PlaneProposal(seed=rank, device=local)
+    losses = prop.train(feats, target, steps=800, batch=8, lr=2e-3, seed=rank)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    L, R = scene.generate(pair_seed(rank), W, H, npl, dlo, dhi)
+    dL, dR = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    pm = PMHuberStereo(views=views, fused=True, device=local)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            out = fn()
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return out, statistics.median(ms)
+
+    def stats(res):
+        c = res["planes_left"][..., 3]
+        c = c[c < 2.0]
+        return float(c.mean().item()), res["dmap"]
+
+    clocks = Clocks(local).start()
+    plain, t_plain = timed(lambda: pm.disparity_map(dL, dR, r, dmax, iters, pp=pp, planes=True))
+    c_plain, d_plain = stats(plain)
+    keep = d_plain > 0
+    rows, found, found_cost = [], None, None
+    for k in (1, 3, 5, 7, 9):
+        res, t_k = timed(lambda: pm.disparity_map(dL, dR, r, dmax, k, pp=pp, planes=True,
+                                                  initdisparity=prop.propose(dL, dR)))
+        c_k, d_k = stats(res)
+        agree = float(((d_k - d_plain).abs() < 1.0)[keep].float().mean().item())
+        rnd, t_r = timed(lambda: pm.disparity_map(dL, dR, r, dmax, k, pp=pp, planes=True))
+        c_r, d_r = stats(rnd)
+        agree_r = float(((d_r - d_plain).abs() < 1.0)[keep].float().mean().item())
+        rows.append({"iterations": k, "learned_ms": t_k, "learned_cost": c_k, "learned_agree_1px": agree,
+                     "random_ms": t_r, "random_cost": c_r, "random_agree_1px": agree_r})
+        if found is None and c_k <= 1.01 * c_plain and agree >= 0.98:
+            found = rows[-1]
+        if found_cost is None and c_k <= 1.01 * c_plain:
+            found_cost = rows[-1]
+    clk = clocks.stop()
+    _, t_prop = timed(lambda: prop.propose(dL, dR))
+    prop.check_error()
+    value = found["learned_ms"] if found else None
+    line = {"metric": "ms to plain-8-iter cost (learned vs random init)", "value": value, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (CNN) / f32 (PatchMatch)", "data": "synthetic",
+            "config": {"workload": args.config, "mode": "learned", "width": W, "height": H, "dispmax": dmax,
+                       "window": 2 * r + 1, "plain_iterations": iters, "parallelism": "pairs%d" % world,
+                       "criterion": "mean cost <= 1.01 x plain and >= 98% of plain's kept pixels within 1 px",
+                       "training": {"pairs": 64, "size": "512x384", "steps": 800, "batch": 8,
+                                    "data_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
+                                    "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:]))}},
+            "plain": {"ms": t_plain, "cost": c_plain, "fraction_of_plain_time": None},
+            "proposal_ms": t_prop, "sweep": rows, "clocks": clk,
+            "cost_criterion_only": None if found_cost is None else {
+                "iterations": found_cost["iterations"], "ms": found_cost["learned_ms"],
+                "fraction_of_plain_time": found_cost["learned_ms"] / t_plain},
+            "target": "<= 1/3 of plain's time", "met": bool(found and found["learned_ms"] <= t_plain / 3.0)}
+    if found:
+        line["plain"]["fraction_of_plain_time"] = found["learned_ms"] / t_plain
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -508,10 +605,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="hd", choices=sorted(WORKLOADS) + ["batch"])
-    ap.add_argument("--mode", default="disparity", choices=["disparity", "depth", "pyramid", "vpm", "svpm"],
+    ap.add_argument("--mode", default="disparity", choices=["disparity", "depth", "pyramid", "vpm", "svpm", "learned"],
                     help="disparityMap (default), depthMap (Huber variant, iterations not made odd), "
                          "disparityMap over 3 pyramid levels (value counts the full-size pixels) or "
-                         "VPMStereoCL::disparitySimple or SVPMFlowCL::flow (200 passes)")
+                         "VPMStereoCL::disparitySimple, SVPMFlowCL::flow (200 passes) or the learned plane "
+                         "proposal (ms to plain 8-iteration cost)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--profile-run", action="store_true",
                     help="only run warmup + steps of the device pipeline (for ncu captures) and print the step times")
@@ -532,6 +630,9 @@ def main():
         return
     if args.mode == "svpm":
         run_svpm(args, wl, rank, world, local)
+        return
+    if args.mode == "learned":
+        run_learned(args, wl, rank, world, local)
         return
 
     import torch

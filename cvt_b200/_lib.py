@@ -146,13 +146,13 @@ def lib():
         "pm_lpp_conv": (i32, [i32, i32, vp, vp, vp, vp, vp, i32, i32, i32, vp, vp]),
         "pm_lpp_wgrad_scratch_floats": (sz, [i32, i32, i32, i32]),
         "pm_lpp_wgrad": (i32, [vp, vp, vp, vp, i32, i32, i32, i32, vp]),
-        "pm_lpp_softargmin": (i32, [vp, vp, vp, vp, vp, i32, f32, vp]),
+        "pm_lpp_softargmin": (i32, [vp, vp, f32, vp, vp, vp, vp, i32, f32, vp]),
         "pm_lpp_target4": (i32, [vp, i32, i32, vp, vp]),
         "pm_lpp_upsample": (i32, [vp, i32, i32, i32, i32, vp, vp]),
         "pm_lpp_adam": (i32, [vp, vp, vp, vp, i32, f32, i32, vp]),
         "pm_lpp_weights_bf16": (i32, [vp, vp, vp, vp]),
         "pm_lpp_propose_workspace_bytes": (sz, [i32, i32]),
-        "pm_lpp_propose_device": (i32, [vp, vp, i32, vp, vp, i32, i32, sz, vp, vp, sz, vp, vp]),
+        "pm_lpp_propose_device": (i32, [vp, vp, i32, f32, vp, vp, i32, i32, sz, vp, vp, sz, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -8,8 +8,9 @@
 //             (0 .. 31 quarter pixels): 3x3 mean of |gL(x, y) - gR(x - d, y)|, times 8
 //   6 convs   3x3, 32 -> 32 channels, BF16 weights and activations, FP32 accumulation; ReLU
 //             after the first five; the sixth gives 32 logits per pixel (FP32)
-//   output    soft-argmin: disparity4 = sum_d d softmax(-logit)_d; upsampled bilinearly and
-//             scaled by 4 to a full-resolution initial disparity
+//   output    soft-argmin: disparity4 = sum_d d softmax(-(logit_d + skip * cost_d))_d (the
+//             network corrects the matching cost); upsampled bilinearly and scaled by 4 to a
+//             full-resolution initial disparity
 // Training (cvt_b200/learn.py drives it): smooth-L1 loss against the quarter-resolution mean
 // of plain PatchMatch's disparity, hand-written backward kernels (data gradients through the
 // same tensor-core kernel with the transposed, mirrored weights; weight gradients on the CUDA
@@ -327,17 +328,21 @@ __global__ void k_costvol(const float* __restrict__ gl, const float* __restrict_
     }
 }
 
-// soft-argmin over the 32 logits and the smooth-L1 loss against target (quarter pixels; a
+// soft-argmin over the 32 logits plus `skip` times the input cost volume (the network learns a
+// correction to the matching cost), and the smooth-L1 loss against target (quarter pixels; a
 // target < 0 is masked): disparity out, dLogits (BF16, scaled by 1 / count) and per-block loss
 // sums
-__global__ void k_softargmin(const float* __restrict__ logits, const float* __restrict__ target, float* __restrict__ disp,
+__global__ void k_softargmin(const float* __restrict__ logits, const __nv_bfloat16* __restrict__ feats, float skip,
+                             const float* __restrict__ target, float* __restrict__ disp,
                              __nv_bfloat16* __restrict__ dlogits, float* __restrict__ loss_part, int M, float inv_count)
 {
     __shared__ float red[256];
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     float l = 0.0f;
     if (m < M) {
-        const float* lg = logits + (size_t)m * CH;
+        float lg[CH];
+        for (int d = 0; d < CH; d++)
+            lg[d] = logits[(size_t)m * CH + d] + (feats ? skip * __bfloat162float(feats[(size_t)m * CH + d]) : 0.0f);
         float mn = lg[0];
         for (int d = 1; d < CH; d++) mn = fminf(mn, lg[d]);
         float p[CH], z = 0.0f;
@@ -522,12 +527,12 @@ int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, siz
     return check_launch("pm_lpp_features");
 }
 
-int pm_lpp_softargmin(const float* logits, const float* target, float* disp, void* dlogits, float* loss_part, int M,
-                      float inv_count, void* stream)
+int pm_lpp_softargmin(const float* logits, const void* feats, float skip, const float* target, float* disp, void* dlogits,
+                      float* loss_part, int M, float inv_count, void* stream)
 {
     if (M <= 0 || !logits || !disp) return lfail(PM_EINVAL_ARG, "bad argument");
-    k_softargmin<<<(M + 255) / 256, 256, 0, S(stream)>>>(logits, target, disp, static_cast<__nv_bfloat16*>(dlogits),
-                                                          loss_part, M, inv_count);
+    k_softargmin<<<(M + 255) / 256, 256, 0, S(stream)>>>(logits, static_cast<const __nv_bfloat16*>(feats), skip, target, disp,
+                                                          static_cast<__nv_bfloat16*>(dlogits), loss_part, M, inv_count);
     return check_launch("pm_lpp_softargmin");
 }
 
@@ -567,13 +572,14 @@ size_t pm_lpp_propose_workspace_bytes(int W, int H)
 {
     if (W < 4 || H < 4) return 0;
     const size_t M = (size_t)(W / 4) * (H / 4);
-    // two grey planes, two BF16 activation buffers, FP32 logits, the quarter disparity
-    return 2 * M * 4 + 2 * M * CH * 2 + M * CH * 4 + M * 4 + 5 * 256;
+    // two grey planes, the features and two BF16 activation buffers, FP32 logits, the quarter
+    // disparity
+    return 2 * M * 4 + 3 * M * CH * 2 + M * CH * 4 + M * 4 + 6 * 256;
 }
 
-int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, const uint8_t* left, const uint8_t* right,
-                          int W, int H, size_t stride, float* initdisp, void* workspace, size_t ws_bytes, int* err,
-                          void* stream)
+int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, const uint8_t* left,
+                          const uint8_t* right, int W, int H, size_t stride, float* initdisp, void* workspace, size_t ws_bytes,
+                          int* err, void* stream)
 {
     if (W < 4 || H < 4 || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
     if (!wmats || !biases || nlayers < 1 || !left || !right || !initdisp || !workspace || !err)
@@ -585,6 +591,8 @@ int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, c
     char* ws = static_cast<char*>(workspace);
     float* grey = reinterpret_cast<float*>(ws);
     size_t off = (2 * M * 4 + 255) & ~(size_t)255;
+    __nv_bfloat16* feats = reinterpret_cast<__nv_bfloat16*>(ws + off);
+    off += (M * CH * 2 + 255) & ~(size_t)255;
     __nv_bfloat16* act[2] = {reinterpret_cast<__nv_bfloat16*>(ws + off), nullptr};
     off += (M * CH * 2 + 255) & ~(size_t)255;
     act[1] = reinterpret_cast<__nv_bfloat16*>(ws + off);
@@ -592,17 +600,19 @@ int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, c
     float* logits = reinterpret_cast<float*>(ws + off);
     off += (M * CH * 4 + 255) & ~(size_t)255;
     float* d4 = reinterpret_cast<float*>(ws + off);
-    int rc = pm_lpp_features(left, right, W, H, stride, grey, act[0], stream);
+    int rc = pm_lpp_features(left, right, W, H, stride, grey, feats, stream);
     if (rc) return rc;
     const auto* w = static_cast<const __nv_bfloat16*>(wmats);
+    const __nv_bfloat16* x = feats;
     for (int l = 0; l < nlayers; l++) {
         const bool last = l == nlayers - 1;
-        rc = pm_lpp_conv(last ? EPI_BIAS_F32 : EPI_RELU_BF16, 1, act[l & 1], w + (size_t)l * CH * KTOT, biases + l * CH,
-                         nullptr, last ? static_cast<void*>(logits) : static_cast<void*>(act[(l + 1) & 1]), 1, H4, W4, err,
-                         stream);
+        void* y = last ? static_cast<void*>(logits) : static_cast<void*>(act[l & 1]);
+        rc = pm_lpp_conv(last ? EPI_BIAS_F32 : EPI_RELU_BF16, 1, x, w + (size_t)l * CH * KTOT, biases + l * CH, nullptr, y, 1,
+                         H4, W4, err, stream);
         if (rc) return rc;
+        x = act[l & 1];
     }
-    rc = pm_lpp_softargmin(logits, nullptr, d4, nullptr, nullptr, (int)M, 0.0f, stream);
+    rc = pm_lpp_softargmin(logits, feats, skip, nullptr, d4, nullptr, nullptr, (int)M, 0.0f, stream);
     if (rc) return rc;
     return pm_lpp_upsample(d4, W4, H4, W, H, initdisp, stream);
 }

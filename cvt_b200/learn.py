@@ -23,6 +23,7 @@ from . import _lib
 CH = 32
 KTOT = 9 * CH
 NLAYERS = 6
+SKIP = 4.0   # the cost volume's weight in the soft-argmin: the network learns a correction to it
 EPI_RELU, EPI_LOGITS, EPI_DGRAD = 0, 1, 2
 
 
@@ -133,7 +134,8 @@ class PlaneProposal:
         _, logits = self.forward(feats)
         B, H4, W4 = feats.shape[:3]
         d = torch.empty((B, H4, W4), dtype=torch.float32, device=self.dev)
-        _check(_lib.lib().pm_lpp_softargmin(_p(logits), None, _p(d), None, None, B * H4 * W4, 0.0, self._stream()))
+        _check(_lib.lib().pm_lpp_softargmin(_p(logits), _p(feats), SKIP, None, _p(d), None, None, B * H4 * W4, 0.0,
+                                            self._stream()))
         return d
 
     def gradients(self, feats, target4):
@@ -146,8 +148,8 @@ class PlaneProposal:
         dy = torch.empty((B, H4, W4, CH), dtype=torch.bfloat16, device=self.dev)
         parts = torch.empty((M + 255) // 256, dtype=torch.float32, device=self.dev)
         count = max(int((target4 >= 0).sum().item()), 1)
-        _check(L.pm_lpp_softargmin(_p(logits), _p(target4.contiguous()), _p(disp), _p(dy), _p(parts), M, 1.0 / count,
-                                   self._stream()))
+        _check(L.pm_lpp_softargmin(_p(logits), _p(feats), SKIP, _p(target4.contiguous()), _p(disp), _p(dy), _p(parts), M,
+                                   1.0 / count, self._stream()))
         per_block = 256
         scratch = torch.empty(L.pm_lpp_wgrad_scratch_floats(B, H4, W4, per_block), dtype=torch.float32, device=self.dev)
         grads = [None] * NLAYERS
@@ -196,7 +198,7 @@ class PlaneProposal:
         ws = torch.empty(L.pm_lpp_propose_workspace_bytes(W, H) + 256, dtype=torch.uint8, device=self.dev)
         off = (-ws.data_ptr()) % 256
         out = torch.empty((H, W), dtype=torch.float32, device=self.dev)
-        _check(L.pm_lpp_propose_device(_p(self.wmat[0]), _p(self.ball), NLAYERS, _p(left.contiguous()),
+        _check(L.pm_lpp_propose_device(_p(self.wmat[0]), _p(self.ball), NLAYERS, SKIP, _p(left.contiguous()),
                                        _p(right.contiguous()), W, H, W * 4, _p(out), ws.data_ptr() + off,
                                        ws.numel() - off, _p(self.err), self._stream()))
         return out

@@ -360,8 +360,8 @@ int pm_k_svpm_to_flow(float* flow, const float* states, int W, int H, void* stre
  * A small BF16 CNN at a quarter of the image resolution whose output replaces the random
  * initialisation of disparityMap through its initdisp argument (pmhstereo_init_disparity_normal,
  * pmhstereo.cl:802-828): a 32-hypothesis cost volume of 4x4-block grey values, six 3x3
- * convolutions of 32 channels (ReLU after the first five), soft-argmin over the 32 logits,
- * bilinear upsampling times 4.  Activations are NHWC BF16 (batch, rows, columns, 32); a layer's
+ * convolutions of 32 channels (ReLU after the first five), soft-argmin over the 32 logits plus
+ * a fixed multiple of the cost volume, bilinear upsampling times 4.  Activations are NHWC BF16 (batch, rows, columns, 32); a layer's
  * weights wmat[n][t][c] (output channel, tap t = (dy + 1) * 3 + (dx + 1), input channel), 32 * 288
  * BF16, and 32 FP32 biases.  The convolution runs on the tensor cores (tcgen05, FP32
  * accumulation) or, for checking, on the CUDA cores (tensor_cores = 0).  `err` (device int) is
@@ -383,11 +383,11 @@ int pm_lpp_conv(int epi, int tensor_cores, const void* in, const void* wmat, con
  * in order (deterministic) */
 size_t pm_lpp_wgrad_scratch_floats(int B, int H4, int W4, int per_block);
 int pm_lpp_wgrad(const void* x, const void* dy, float* scratch, float* grad, int B, int H4, int W4, int per_block, void* stream);
-/* soft-argmin of M x 32 logits into disparities (quarter pixels); with dlogits, also the
- * smooth-L1 loss against target (< 0: ignored), its gradient times inv_count (BF16) and per-256-
- * pixel loss sums in loss_part */
-int pm_lpp_softargmin(const float* logits, const float* target, float* disp, void* dlogits, float* loss_part, int M,
-                      float inv_count, void* stream);
+/* soft-argmin of M x 32 logits plus skip times the features (the cost volume; NULL: none) into
+ * disparities (quarter pixels); with dlogits, also the smooth-L1 loss against target (< 0:
+ * ignored), its gradient times inv_count (BF16) and per-256-pixel loss sums in loss_part */
+int pm_lpp_softargmin(const float* logits, const void* feats, float skip, const float* target, float* disp, void* dlogits,
+                      float* loss_part, int M, float inv_count, void* stream);
 /* training target: the mean of the positive disparities of each 4x4 block, in quarter pixels
  * (-1 where fewer than 8 of 16 are positive) */
 int pm_lpp_target4(const float* disp, int W, int H, float* out, void* stream);
@@ -400,9 +400,9 @@ int pm_lpp_weights_bf16(const float* p, void* wmat, void* wt, void* stream);
 /* the whole proposal for one pair: nlayers convolutions with weights wmats (nlayers * 32 * 288
  * BF16, 256-byte aligned) and biases (nlayers * 32), initdisp W * H floats (pixels) */
 size_t pm_lpp_propose_workspace_bytes(int W, int H);
-int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, const uint8_t* left, const uint8_t* right,
-                          int W, int H, size_t stride, float* initdisp, void* workspace, size_t ws_bytes, int* err,
-                          void* stream);
+int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, const uint8_t* left,
+                          const uint8_t* right, int W, int H, size_t stride, float* initdisp, void* workspace, size_t ws_bytes,
+                          int* err, void* stream);
 
 #ifdef __cplusplus
 }

@@ -56,17 +56,23 @@ def forward(feat, layers):
     return acts, logits
 
 
-def softargmin(logits):
+SKIP = 4.0
+
+
+def softargmin(logits, feat=None):
+    """soft-argmin over the logits plus SKIP times the cost volume (the features)"""
     l = logits.astype(np.float64)
+    if feat is not None:
+        l = l + SKIP * feat.astype(np.float64)
     p = np.exp(-(l - l.min(-1, keepdims=True)))
     p /= p.sum(-1, keepdims=True)
     d = (p * np.arange(CH)).sum(-1)
     return p, d
 
 
-def loss_grad(logits, target):
+def loss_grad(logits, target, feat=None):
     """smooth-L1 mean over targets >= 0; returns (loss, dlogits as BF16)"""
-    p, d = softargmin(logits)
+    p, d = softargmin(logits, feat)
     valid = target >= 0
     n = max(int(valid.sum()), 1)
     r = d - target

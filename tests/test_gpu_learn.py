@@ -102,7 +102,7 @@ def test_backward_matches_oracle(torch_cuda, native, tc):
     loss, grads = pp.gradients(bf(torch, feats), torch.from_numpy(target).cuda())
     layers = [(a[:CH * KTOT].reshape(CH, KTOT), a[CH * KTOT:]) for a in pp.params()]
     acts, logits = O.forward(feats, layers)
-    oloss, dl = O.loss_grad(logits, target)
+    oloss, dl = O.loss_grad(logits, target, feats)
     og = O.backward(acts, layers, dl)
     assert abs(loss - oloss) < 1e-3 * max(1.0, abs(oloss)), (loss, oloss)
     for l in range(6):
