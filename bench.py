@@ -26,8 +26,9 @@ range 128, the reference's 200 passes; metric Mpixel*passes/s.
 
 `--mode learned` measures the second half of the metric, "ms to plain-8-iter cost": a
 BF16 plane-proposal CNN (cvt_b200/learn.py; tcgen05 convolutions) is trained on the
-GPU (outside the timed region) on 64 procedural 512x384 pairs against plain 8-iteration
-PatchMatch, then on the hd pair the GPU time of proposal + k PatchMatch iterations is
+GPU (outside the timed region) on 128 procedural 512x384 pairs (both views) against plain
+8-iteration PatchMatch, then on the hd pair the GPU time of proposals for both views + k
+PatchMatch iterations is
 timed for growing k until its mean matching cost is within 1% of plain 8-iteration
 PatchMatch and its disparity within 1 px of it on >= 98% of the pixels plain
 PatchMatch keeps (LR check); value = that time in ms (null if no k up to 9 reaches it).
@@ -523,10 +524,10 @@ def run_learned(args, wl, rank, world, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=900))
     W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
     t0 = time.perf_counter()
-    feats, target = make_training_set(64, 512, 384, seed=100 + 1000 * rank, device=local)
+    feats, target = make_training_set(128, 512, 384, seed=100 + 1000 * rank, device=local)   # 256 maps, both views
     t1 = time.perf_counter()
     prop = PlaneProposal(seed=rank, device=local)
-    losses = prop.train(feats, target, steps=800, batch=8, lr=2e-3, seed=rank)
+    losses = prop.train(feats, target, steps=3000, batch=16, lr=1e-3, seed=rank)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     L, R = scene.generate(pair_seed(rank), W, H, npl, dlo, dhi)
@@ -559,7 +560,8 @@ def run_learned(args, wl, rank, world, local):
     rows, found, found_cost = [], None, None
     for k in (1, 3, 5, 7, 9):
         res, t_k = timed(lambda: pm.disparity_map(dL, dR, r, dmax, k, pp=pp, planes=True,
-                                                  initdisparity=prop.propose(dL, dR)))
+                                                  initdisparity=prop.propose(dL, dR, 0),
+                                                  initdisparity_right=prop.propose(dL, dR, 1)))
         c_k, d_k = stats(res)
         agree = float(((d_k - d_plain).abs() < 1.0)[keep].float().mean().item())
         rnd, t_r = timed(lambda: pm.disparity_map(dL, dR, r, dmax, k, pp=pp, planes=True))
@@ -572,7 +574,7 @@ def run_learned(args, wl, rank, world, local):
         if found_cost is None and c_k <= 1.01 * c_plain:
             found_cost = rows[-1]
     clk = clocks.stop()
-    _, t_prop = timed(lambda: prop.propose(dL, dR))
+    _, t_prop = timed(lambda: (prop.propose(dL, dR, 0), prop.propose(dL, dR, 1)))
     prop.check_error()
     value = found["learned_ms"] if found else None
     line = {"metric": "ms to plain-8-iter cost (learned vs random init)", "value": value, "unit": "ms", "n_gpus": world,
@@ -581,7 +583,7 @@ def run_learned(args, wl, rank, world, local):
             "config": {"workload": args.config, "mode": "learned", "width": W, "height": H, "dispmax": dmax,
                        "window": 2 * r + 1, "plain_iterations": iters, "parallelism": "pairs%d" % world,
                        "criterion": "mean cost <= 1.01 x plain and >= 98% of plain's kept pixels within 1 px",
-                       "training": {"pairs": 64, "size": "512x384", "steps": 800, "batch": 8,
+                       "training": {"pairs": 128, "maps": 256, "size": "512x384", "steps": 3000, "batch": 16,
                                     "data_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
                                     "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:]))}},
             "plain": {"ms": t_plain, "cost": c_plain, "fraction_of_plain_time": None},

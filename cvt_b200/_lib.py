@@ -18,7 +18,7 @@ SYMBOLS = [
     "pm_options_default", "pm_create", "pm_destroy", "pm_last_error", "pm_status_string",
     "pm_disparity_map", "pm_disparity_map_device", "pm_depth_map", "pm_depth_map_device", "pm_set_counting", "pm_get_counters",
     "pm_set_profiling", "pm_get_phase_times", "pm_measure_fp32_peak",
-    "pm_disparity_map_batch_device",
+    "pm_disparity_map_batch_device", "pm_disparity_map_init2_device",
     "pm_k_prep", "pm_k_init", "pm_k_cost", "pm_k_klt", "pm_k_propagate", "pm_k_normal_depth",
     "pm_rof_scratch_bytes", "pm_k_rof", "pm_k_rof_static", "pm_k_consistency", "pm_k_to_disparity", "pm_k_fill_depthmap",
     "pm_k_fill_normalmap", "pm_k_disparity_to_normal", "pm_k_pyrdown", "pm_k_pyrup_mul", "pm_pyramid_size",
@@ -142,7 +142,7 @@ def lib():
         "pm_k_svpm_to_flow": (i32, [vp, vp, i32, i32, vp]),
         "pm_lpp_channels": (i32, []),
         "pm_lpp_last_error": (C.c_char_p, []),
-        "pm_lpp_features": (i32, [vp, vp, i32, i32, sz, vp, vp, vp]),
+        "pm_lpp_features": (i32, [vp, vp, i32, i32, sz, i32, vp, vp, vp]),
         "pm_lpp_conv": (i32, [i32, i32, vp, vp, vp, vp, vp, i32, i32, i32, vp, vp]),
         "pm_lpp_wgrad_scratch_floats": (sz, [i32, i32, i32, i32]),
         "pm_lpp_wgrad": (i32, [vp, vp, vp, vp, i32, i32, i32, i32, vp]),
@@ -152,7 +152,9 @@ def lib():
         "pm_lpp_adam": (i32, [vp, vp, vp, vp, i32, f32, i32, vp]),
         "pm_lpp_weights_bf16": (i32, [vp, vp, vp, vp]),
         "pm_lpp_propose_workspace_bytes": (sz, [i32, i32]),
-        "pm_lpp_propose_device": (i32, [vp, vp, i32, f32, vp, vp, i32, i32, sz, vp, vp, sz, vp, vp]),
+        "pm_lpp_propose_device": (i32, [vp, vp, i32, f32, vp, vp, i32, i32, sz, i32, vp, vp, sz, vp, vp]),
+        "pm_disparity_map_init2_device": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, i32, vp, vp, vp, vp, vp, vp,
+                                                vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

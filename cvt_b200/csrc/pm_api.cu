@@ -47,6 +47,8 @@ struct pm_handle {
     // pyramid levels 1.. of single-pair calls: one workspace each
     std::vector<void*> lws;
     std::vector<size_t> lws_bytes;
+    // the right view's initial disparity of the call in progress (pm_disparity_map_init2_device)
+    const float* init_right = nullptr;
 };
 
 namespace {
@@ -531,8 +533,8 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
     prof_mark(h, st, PM_PHASE_PREP, 0);
     int rc;
     if (levels == 1) {
-        rc = run_level(h, ws, L, left, right, W, H, stride, r, dmax, iterations, o.thetamin, initdisp, nullptr,
-                       initnormal, nullptr, ctr, errf, st);   // :92-93
+        rc = run_level(h, ws, L, left, right, W, H, stride, r, dmax, iterations, o.thetamin, initdisp, h->init_right,
+                       initnormal, nullptr, ctr, errf, st);   // :92-93 (the right view's init: disparityMapAll's)
         if (rc) return rc;
     } else {
         std::vector<int> Wl, Hl;
@@ -771,7 +773,7 @@ int pipeline_on(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* righ
         (uint64_t)(uintptr_t)normal, (uint64_t)(uintptr_t)initdisp, (uint64_t)(uintptr_t)initnormal,
         (uint64_t)(uintptr_t)planesL, (uint64_t)(uintptr_t)planesR, (uint64_t)o.views, (uint64_t)o.fused,
         fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff), (uint64_t)o.rof_iters, (uint64_t)h->counting,
-        (uint64_t)o.levels, (uint64_t)depth, fbits(dscale)};
+        (uint64_t)o.levels, (uint64_t)depth, fbits(dscale), (uint64_t)(uintptr_t)h->init_right};
     for (void* p : h->lws) key.push_back((uint64_t)(uintptr_t)p);
     return run_graph(h, h->key1, h->exec1, key, st, run);
 }
@@ -1018,6 +1020,22 @@ int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* ri
 {
     return entry_device(h, 0, 0.0f, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap, normalmap,
                         initdisp, initnormal, planes_left, planes_right, S(stream));
+}
+
+int pm_disparity_map_init2_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
+                                  int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
+                                  const float* initdisp_left, const float* initdisp_right, float* planes_left,
+                                  float* planes_right, void* stream)
+{
+    if (!h) return fail(nullptr, PM_EINVAL_ARG, "null handle");
+    if (initdisp_right && (h->opt.levels != 1 || h->opt.views != 2))
+        return fail(h, PM_EINVAL_ARG, "a right-view initial disparity needs one pyramid level and both views");
+    if (!aligned(initdisp_right, 4)) return fail(h, PM_EINVAL_ARG, "float fields must be 4-byte aligned");
+    h->init_right = initdisp_right;
+    const int rc = entry_device(h, 0, 0.0f, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap, normalmap,
+                                initdisp_left, nullptr, planes_left, planes_right, S(stream));
+    h->init_right = nullptr;
+    return rc;
 }
 
 int pm_disparity_map(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,

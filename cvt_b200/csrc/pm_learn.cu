@@ -301,9 +301,10 @@ __global__ void k_grey4(const uint8_t* __restrict__ img, size_t stride, int W4, 
     out[(size_t)y * W4 + x] = s * (1.0f / (16.0f * 255.0f));
 }
 
-// cost volume: channel d = 8 x the 3x3 mean of |gL(x, y) - gR(x - d, y)| (columns left of the
-// image count as a difference of 1), BF16 NHWC
-__global__ void k_costvol(const float* __restrict__ gl, const float* __restrict__ gr, int W4, int H4,
+// cost volume: channel d = 8 x the 3x3 mean of |g1(x, y) - g2(x + sd, y)|, s = -1 for the left
+// view (g1 left, g2 right), +1 for the right view (g1 right, g2 left); columns outside the image
+// count as a difference of 1; BF16 NHWC
+__global__ void k_costvol(const float* __restrict__ gl, const float* __restrict__ gr, int W4, int H4, int sgn,
                           __nv_bfloat16* __restrict__ out)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
@@ -319,7 +320,8 @@ __global__ void k_costvol(const float* __restrict__ gl, const float* __restrict_
                 const int xx = x + i;
                 if (xx < 0 || xx >= W4) continue;
                 const float a = gl[(size_t)yy * W4 + xx];
-                const float c = xx - d >= 0 ? gr[(size_t)yy * W4 + xx - d] : a + 1.0f;
+                const int xm = xx + sgn * d;
+                const float c = xm >= 0 && xm < W4 ? gr[(size_t)yy * W4 + xm] : a + 1.0f;
                 s += fabsf(a - c);
                 n++;
             }
@@ -514,8 +516,8 @@ int pm_lpp_wgrad(const void* x, const void* dy, float* scratch, float* grad, int
     return check_launch("pm_lpp_wgrad");
 }
 
-int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, float* grey_scratch, void* out,
-                    void* stream)
+int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view,
+                    float* grey_scratch, void* out, void* stream)
 {
     if (W < 4 || H < 4 || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
     if (!left || !right || !grey_scratch || !out || stride < (size_t)W * 4 || stride % 4) return lfail(PM_EINVAL_ARG, "bad argument");
@@ -523,7 +525,10 @@ int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, siz
     const dim3 g((W4 + 127) / 128, H4);
     k_grey4<<<g, 128, 0, S(stream)>>>(left, stride, W4, H4, grey_scratch);
     k_grey4<<<g, 128, 0, S(stream)>>>(right, stride, W4, H4, grey_scratch + (size_t)W4 * H4);
-    k_costvol<<<g, 128, 0, S(stream)>>>(grey_scratch, grey_scratch + (size_t)W4 * H4, W4, H4, static_cast<__nv_bfloat16*>(out));
+    float* g0 = grey_scratch;
+    float* g1 = grey_scratch + (size_t)W4 * H4;
+    if (right_view) k_costvol<<<g, 128, 0, S(stream)>>>(g1, g0, W4, H4, 1, static_cast<__nv_bfloat16*>(out));
+    else k_costvol<<<g, 128, 0, S(stream)>>>(g0, g1, W4, H4, -1, static_cast<__nv_bfloat16*>(out));
     return check_launch("pm_lpp_features");
 }
 
@@ -578,8 +583,8 @@ size_t pm_lpp_propose_workspace_bytes(int W, int H)
 }
 
 int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, const uint8_t* left,
-                          const uint8_t* right, int W, int H, size_t stride, float* initdisp, void* workspace, size_t ws_bytes,
-                          int* err, void* stream)
+                          const uint8_t* right, int W, int H, size_t stride, int right_view, float* initdisp, void* workspace,
+                          size_t ws_bytes, int* err, void* stream)
 {
     if (W < 4 || H < 4 || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
     if (!wmats || !biases || nlayers < 1 || !left || !right || !initdisp || !workspace || !err)
@@ -600,7 +605,7 @@ int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, f
     float* logits = reinterpret_cast<float*>(ws + off);
     off += (M * CH * 4 + 255) & ~(size_t)255;
     float* d4 = reinterpret_cast<float*>(ws + off);
-    int rc = pm_lpp_features(left, right, W, H, stride, grey, feats, stream);
+    int rc = pm_lpp_features(left, right, W, H, stride, right_view, grey, feats, stream);
     if (rc) return rc;
     const auto* w = static_cast<const __nv_bfloat16*>(wmats);
     const __nv_bfloat16* x = feats;

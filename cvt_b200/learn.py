@@ -101,15 +101,16 @@ class PlaneProposal:
             raise _lib.StereoError(_lib.PM_ETIMEOUT, "a tensor-core convolution's bounded wait ran out")
 
     # ---- network ---------------------------------------------------------------
-    def features(self, left, right):
-        """(H, W, 4) uint8 CUDA tensors -> (1, H/4, W/4, 32) BF16 cost volume"""
+    def features(self, left, right, view=0):
+        """(H, W, 4) uint8 CUDA tensors -> (1, H/4, W/4, 32) BF16 cost volume of the left (view 0)
+        or the right view (1)"""
         torch = self.torch
         H, W = left.shape[:2]
         H4, W4 = H // 4, W // 4
         grey = torch.empty(2 * H4 * W4, dtype=torch.float32, device=self.dev)
         out = torch.empty((1, H4, W4, CH), dtype=torch.bfloat16, device=self.dev)
-        _check(_lib.lib().pm_lpp_features(_p(left.contiguous()), _p(right.contiguous()), W, H, W * 4, _p(grey), _p(out),
-                                          self._stream()))
+        _check(_lib.lib().pm_lpp_features(_p(left.contiguous()), _p(right.contiguous()), W, H, W * 4, int(view), _p(grey),
+                                          _p(out), self._stream()))
         return out
 
     def forward(self, feats):
@@ -190,23 +191,24 @@ class PlaneProposal:
         self.check_error()
         return losses
 
-    def propose(self, left, right):
-        """full-resolution initial disparity (pixels) for a pair of (H, W, 4) uint8 CUDA tensors,
-        through the single native call pm_lpp_propose_device"""
+    def propose(self, left, right, view=0):
+        """full-resolution initial disparity (pixels) of the left (view 0) or right view (1) for a
+        pair of (H, W, 4) uint8 CUDA tensors, through the single native call pm_lpp_propose_device"""
         torch, L = self.torch, _lib.lib()
         H, W = left.shape[:2]
         ws = torch.empty(L.pm_lpp_propose_workspace_bytes(W, H) + 256, dtype=torch.uint8, device=self.dev)
         off = (-ws.data_ptr()) % 256
         out = torch.empty((H, W), dtype=torch.float32, device=self.dev)
         _check(L.pm_lpp_propose_device(_p(self.wmat[0]), _p(self.ball), NLAYERS, SKIP, _p(left.contiguous()),
-                                       _p(right.contiguous()), W, H, W * 4, _p(out), ws.data_ptr() + off,
+                                       _p(right.contiguous()), W, H, W * 4, int(view), _p(out), ws.data_ptr() + off,
                                        ws.numel() - off, _p(self.err), self._stream()))
         return out
 
 
 def make_training_set(pairs, width, height, seed, iterations=8, patch=7, dmax=None, device=0):
-    """Training maps from procedural scenes: features and the quarter-resolution mean of plain
-    (random-init) PatchMatch's left disparity after `iterations` iterations, LR-checked."""
+    """Training maps from procedural scenes, two per pair: the left view's features with the
+    quarter-resolution mean of plain (random-init) PatchMatch's LR-checked left disparity after
+    `iterations` iterations, and the right view's features with its right disparity."""
     import torch
 
     from . import scene
@@ -216,14 +218,19 @@ def make_training_set(pairs, width, height, seed, iterations=8, patch=7, dmax=No
     pm = PMHuberStereo(device=device)
     pp = PlaneProposal(device=device)
     H4, W4 = height // 4, width // 4
-    feats = torch.empty((pairs, H4, W4, CH), dtype=torch.bfloat16, device=dev)
-    target = torch.empty((pairs, H4, W4), dtype=torch.float32, device=dev)
+    feats = torch.empty((2 * pairs, H4, W4, CH), dtype=torch.bfloat16, device=dev)
+    target = torch.empty((2 * pairs, H4, W4), dtype=torch.float32, device=dev)
+    dright = torch.empty((height, width), dtype=torch.float32, device=dev)
     L = _lib.lib()
     dmax = float(dmax if dmax is not None else 4 * CH)
     for i in range(pairs):
         l, r = scene.generate(seed + i, width, height, 8 + (seed + i) % 24, 2.0, min(0.9 * dmax, 30.0 + (i % 4) * 30.0))
         dl, dr = torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev)
-        feats[i] = pp.features(dl, dr)[0]
-        d = pm.disparity_map(dl, dr, patch, dmax, iterations, pp=1)
-        _check(L.pm_lpp_target4(_p(d), width, height, _p(target[i]), torch.cuda.current_stream(dev).cuda_stream))
+        st = torch.cuda.current_stream(dev).cuda_stream
+        feats[2 * i] = pp.features(dl, dr, 0)[0]
+        feats[2 * i + 1] = pp.features(dl, dr, 1)[0]
+        res = pm.disparity_map(dl, dr, patch, dmax, iterations, pp=1, planes=True)
+        _check(L.pm_lpp_target4(_p(res["dmap"]), width, height, _p(target[2 * i]), st))
+        _lib.check(L.pm_k_to_disparity(_p(dright), _p(res["planes_right"]), width, height, 1.0, 0, st))
+        _check(L.pm_lpp_target4(_p(dright), width, height, _p(target[2 * i + 1]), st))
     return feats, target

@@ -75,9 +75,14 @@ class PMHuberStereo:
         return {p: (float(ms[i]), int(n[i])) for i, p in enumerate(self.PHASES)}
 
     def disparity_map(self, left, right, patchsize, disparitymax, iterations, pp=PP_LRCHECK, normalmap=False,
-                      initdisparity=None, initnormalmap=None, planes=False, stream=None):
+                      initdisparity=None, initnormalmap=None, planes=False, stream=None, initdisparity_right=None):
         """Returns dmap, or a dict {dmap, normal?, planes_left?, planes_right?} when
-        normalmap or planes is requested.  left/right: (H, W, 4) uint8."""
+        normalmap or planes is requested.  left/right: (H, W, 4) uint8.  initdisparity_right
+        (CUDA tensors only, without initnormalmap) also starts the right view from a disparity,
+        as disparityMapAll allows (pm_disparity_map_init2_device)."""
+        if initdisparity_right is not None:
+            return self._device(left, right, patchsize, disparitymax, iterations, pp, normalmap, initdisparity,
+                                initnormalmap, planes, stream, None, initdisparity_right)
         return self._run(None, left, right, patchsize, disparitymax, iterations, pp, normalmap, initdisparity,
                          initnormalmap, planes, stream)
 
@@ -164,7 +169,7 @@ class PMHuberStereo:
         return [{"dmap": d, "planes_left": a, "planes_right": b} for d, a, b in zip(dm, pl, pr)]
 
     def _device(self, left, right, patchsize, dmax, iterations, pp, normalmap, initd, initn, planes, stream,
-                dscale=None):
+                dscale=None, initd_right=None):
         import torch
 
         L = _lib.lib()
@@ -185,7 +190,14 @@ class PMHuberStereo:
         def p(t):
             return None if t is None else t.data_ptr()
 
-        if dscale is None:
+        if initd_right is not None:
+            if not _is_torch(left) or initn is not None:
+                raise StereoError(_lib.PM_EINVAL_ARG, "initdisparity_right: CUDA tensors, no initnormalmap")
+            ir = initd_right.contiguous().float()
+            _lib.check(L.pm_disparity_map_init2_device(self._h, p(left), p(right), W, H, W * 4, int(patchsize), float(dmax),
+                                                       int(iterations), int(pp), p(dmap), p(nmap), p(initd), p(ir), p(pl),
+                                                       p(pr), st), self._h)
+        elif dscale is None:
             _lib.check(L.pm_disparity_map_device(self._h, p(left), p(right), W, H, W * 4, int(patchsize), float(dmax),
                                                  int(iterations), int(pp), p(dmap), p(nmap), p(initd), p(initn), p(pl),
                                                  p(pr), st), self._h)

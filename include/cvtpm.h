@@ -97,6 +97,16 @@ int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* ri
                             float* normalmap, const float* initdisp, const float* initnormal, float* planes_left,
                             float* planes_right, void* stream);
 
+/* As pm_disparity_map_device with an initial disparity for each view, as disparityMapAll takes
+ * them (PMHuberStereo.cpp:406-581, :469-483; disparityMap passes the right one as NULL): the
+ * right view's disparity is positive, its match in the left image at x + d.  Either may be NULL;
+ * the normals come from the disparities (pmhstereo_disparity_to_normal).  One pyramid level and
+ * both views. */
+int pm_disparity_map_init2_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int width, int height,
+                                  size_t stride, int patchsize, float dispmax, int iterations, int pp, float* dmap,
+                                  float* normalmap, const float* initdisp_left, const float* initdisp_right,
+                                  float* planes_left, float* planes_right, void* stream);
+
 /* PMHuberStereo::depthMap (PMHuberStereo.cpp:145-347), the Huber-smoothed variant: its kernels
  * read the images themselves as colour, the diffusion tensors use alpha 12, each iteration
  * smooths the gap-filled planes (pmhstereo_fill_state) with the tensor-weighted Huber model
@@ -369,10 +379,11 @@ int pm_k_svpm_to_flow(float* flow, const float* states, int W, int H, void* stre
  * message in pm_lpp_last_error().  All entry points enqueue on `stream`. */
 int pm_lpp_channels(void);
 const char* pm_lpp_last_error(void);
-/* cost-volume features of a pair (W, H >= 4; W4 = W / 4, H4 = H / 4): grey_scratch 2 * W4 * H4
- * floats, out W4 * H4 * 32 BF16 */
-int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, float* grey_scratch, void* out,
-                    void* stream);
+/* cost-volume features of a pair (W, H >= 4; W4 = W / 4, H4 = H / 4) for the left view
+ * (right_view 0: channel d compares left x with right x - d) or the right view (1: right x with
+ * left x + d): grey_scratch 2 * W4 * H4 floats, out W4 * H4 * 32 BF16 */
+int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view,
+                    float* grey_scratch, void* out, void* stream);
 /* one convolution over a batch of B activation maps; epi 0: + bias, ReLU, BF16 out; 1: + bias,
  * FP32 out (logits); 2: data gradient: times (mask > 0), BF16 out (wmat then holds the transposed,
  * mirrored weights wt[c][8 - t][n] = w[n][t][c]) */
@@ -401,8 +412,8 @@ int pm_lpp_weights_bf16(const float* p, void* wmat, void* wt, void* stream);
  * BF16, 256-byte aligned) and biases (nlayers * 32), initdisp W * H floats (pixels) */
 size_t pm_lpp_propose_workspace_bytes(int W, int H);
 int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, const uint8_t* left,
-                          const uint8_t* right, int W, int H, size_t stride, float* initdisp, void* workspace, size_t ws_bytes,
-                          int* err, void* stream);
+                          const uint8_t* right, int W, int H, size_t stride, int right_view, float* initdisp, void* workspace,
+                          size_t ws_bytes, int* err, void* stream);
 
 #ifdef __cplusplus
 }

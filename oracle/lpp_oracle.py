@@ -104,19 +104,26 @@ def backward(acts, layers, dlogits):
     return grads
 
 
-def features(left, right):
-    """grey of 4x4 blocks and the 32-hypothesis cost volume (BF16 values), as k_grey4 / k_costvol"""
+def features(left, right, view=0):
+    """grey of 4x4 blocks and the 32-hypothesis cost volume (BF16 values) of the left (view 0) or
+    right view (1), as k_grey4 / k_costvol"""
     def grey4(img):
         H4, W4 = img.shape[0] // 4, img.shape[1] // 4
         f = img[:4 * H4, :4 * W4, :3].astype(np.float32)
         g = (f[..., 0] * np.float32(0.2126) + f[..., 1] * np.float32(0.7152) + f[..., 2] * np.float32(0.0722))
         return g.reshape(H4, 4, W4, 4).sum((1, 3)) / np.float32(16 * 255)
     gl, gr = grey4(left).astype(np.float64), grey4(right).astype(np.float64)
+    if view:
+        gl, gr = gr, gl
+    sgn = 1 if view else -1
     H4, W4 = gl.shape
     cv = np.zeros((H4, W4, CH))
     xs = np.arange(W4)
     for d in range(CH):
-        diff = np.where(xs[None, :] - d >= 0, np.abs(gl - np.roll(gr, d, axis=1)), 1.0)
+        xm = xs + sgn * d
+        inside = (xm >= 0) & (xm < W4)
+        other = gr[:, np.clip(xm, 0, W4 - 1)]
+        diff = np.where(inside[None, :], np.abs(gl - other), 1.0)
         s = np.zeros_like(diff)
         n = np.zeros_like(diff)
         for j in (-1, 0, 1):

@@ -119,10 +119,11 @@ def test_features_match_oracle(torch_cuda, native):
     from cvt_b200.learn import PlaneProposal
 
     L, R = scene.generate(3, 203, 121, 6, 2.0, 60.0)
-    f = to_np(PlaneProposal().features(torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()))
-    want = O.features(L, R)
-    assert f.shape == want.shape
-    assert (np.abs(f - want) <= 2 ** -7 * np.abs(want) + 1e-6).all()
+    for view in (0, 1):
+        f = to_np(PlaneProposal().features(torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda(), view))
+        want = O.features(L, R, view)
+        assert f.shape == want.shape
+        assert (np.abs(f - want) <= 2 ** -7 * np.abs(want) + 1e-6).all(), view
 
 
 def test_training_gains_over_random_init(torch_cuda, native):
@@ -145,7 +146,8 @@ def test_training_gains_over_random_init(torch_cuda, native):
         dl, dr = torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()
         ref = pm.disparity_map(dl, dr, 7, 128.0, 8, pp=0, planes=True)
         rnd = pm.disparity_map(dl, dr, 7, 128.0, 1, pp=0, planes=True)
-        lrn = pm.disparity_map(dl, dr, 7, 128.0, 1, pp=0, planes=True, initdisparity=pp.propose(dl, dr))
+        lrn = pm.disparity_map(dl, dr, 7, 128.0, 1, pp=0, planes=True, initdisparity=pp.propose(dl, dr, 0),
+                               initdisparity_right=pp.propose(dl, dr, 1))
         d8 = to_np(ref["dmap"])
         res = []
         for run in (rnd, lrn):
