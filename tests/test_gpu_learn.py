@@ -157,3 +157,36 @@ def test_training_gains_over_random_init(torch_cuda, native):
         print("scene %d: random+1 cost %.4f agree %.3f | learned+1 cost %.4f agree %.3f" % (i, *res[0], *res[1]))
         gains.append((res[0][0] - res[1][0], res[1][1] - res[0][1]))
     assert all(c > 0 for c, _ in gains) and all(a > 0 for _, a in gains), gains
+
+
+def test_init2_without_right_equals_disparity_map(torch_cuda, native):
+    """pm_disparity_map_init2_device with no right initial disparity is disparityMap itself, bit
+    for bit; with one it is deterministic and its right view starts from it (cost after one
+    iteration below the random start's)"""
+    torch = torch_cuda
+    from cvt_b200 import scene
+    from cvt_b200.stereo import PMHuberStereo
+    from oracle.pyoracle import bits_equal
+
+    l, r, gd, gn = scene.generate(41, 160, 96, 6, 2.0, 24.0, with_gt=True)
+    dl, dr = torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()
+    pm = PMHuberStereo()
+    initl = torch.from_numpy(gd).cuda()
+    a = pm.disparity_map(dl, dr, 4, 32.0, 1, pp=1, planes=True, initdisparity=initl)
+    b = pm.disparity_map(dl, dr, 4, 32.0, 1, pp=1, planes=True, initdisparity=initl,
+                         initdisparity_right=torch.full((96, 160), -1.0, device="cuda"))
+    for k in ("dmap", "planes_left", "planes_right"):
+        assert bits_equal(to_np(a[k]), to_np(b[k])).all(), k
+    # right view from the left ground truth warped to the right image (x_R = x_L - d)
+    dgr = np.zeros_like(gd)
+    ys, xs = np.nonzero(gd > 0)
+    xr = np.round(xs - gd[ys, xs]).astype(int)
+    ok = (xr >= 0) & (xr < 160)
+    dgr[ys[ok], xr[ok]] = gd[ys[ok], xs[ok]]
+    initr = torch.from_numpy(dgr).cuda()
+    c1 = pm.disparity_map(dl, dr, 4, 32.0, 1, pp=0, planes=True, initdisparity=initl, initdisparity_right=initr)
+    c2 = pm.disparity_map(dl, dr, 4, 32.0, 1, pp=0, planes=True, initdisparity=initl, initdisparity_right=initr)
+    assert bits_equal(to_np(c1["planes_right"]), to_np(c2["planes_right"])).all()
+    rc = to_np(c1["planes_right"])[..., 3]
+    rr = to_np(a["planes_right"])[..., 3]
+    assert np.mean(rc[rc < 2]) < np.mean(rr[rr < 2])
