@@ -173,8 +173,11 @@ def test_init2_without_right_equals_disparity_map(torch_cuda, native):
     pm = PMHuberStereo()
     initl = torch.from_numpy(gd).cuda()
     a = pm.disparity_map(dl, dr, 4, 32.0, 1, pp=1, planes=True, initdisparity=initl)
-    b = pm.disparity_map(dl, dr, 4, 32.0, 1, pp=1, planes=True, initdisparity=initl,
-                         initdisparity_right=torch.full((96, 160), -1.0, device="cuda"))
+    b = {k: torch.empty_like(v) for k, v in a.items()}
+    assert native.pm_disparity_map_init2_device(pm._h, dl.data_ptr(), dr.data_ptr(), 160, 96, 640, 4, 32.0, 1, 1,
+                                                b["dmap"].data_ptr(), None, initl.data_ptr(), None,
+                                                b["planes_left"].data_ptr(), b["planes_right"].data_ptr(),
+                                                torch.cuda.current_stream().cuda_stream) == 0
     for k in ("dmap", "planes_left", "planes_right"):
         assert bits_equal(to_np(a[k]), to_np(b[k])).all(), k
     # right view from the left ground truth warped to the right image (x_R = x_L - d)
