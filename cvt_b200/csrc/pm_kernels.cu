@@ -198,19 +198,33 @@ __device__ __forceinline__ Dual rof_dual(const float4* __restrict__ u, const flo
     return d;
 }
 
+constexpr int ROF_BX = 32, ROF_BY = 8;   // k_rof_step block; its duals need a one-pixel apron left and above
+
 // one primal-dual step (PDDROFDiffTensor.cl:102-126; with HUBER PDDHuberDiffTensor.cl:92-106);
-// first: p = q = 0
+// first: p = q = 0.  The divergence at (x, y) needs the duals at (x, y), (x - 1, y) and
+// (x, y - 1): the block computes the duals of its tile and of the column left of it and the
+// row above it once each, in shared memory, instead of three times per pixel.
 template <bool HUBER>
-__global__ void k_rof_step(float4* __restrict__ unew, float4* __restrict__ pnew, float4* __restrict__ qnew,
-                           const float4* __restrict__ u, const float4* __restrict__ p, const float4* __restrict__ q,
-                           const float4* __restrict__ img, const float4* __restrict__ dt, float4 lam, int W, int H,
-                           int first, float eps)
+__global__ void __launch_bounds__(ROF_BX* ROF_BY) k_rof_step(float4* __restrict__ unew, float4* __restrict__ pnew,
+                                                           float4* __restrict__ qnew, const float4* __restrict__ u,
+                                                           const float4* __restrict__ p, const float4* __restrict__ q,
+                                                           const float4* __restrict__ img,
+                                                           const float4* __restrict__ dt, float4 lam, int W, int H,
+                                                           int first, float eps)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    __shared__ Dual sd[ROF_BY + 1][ROF_BX + 1];
+    const int x0 = blockIdx.x * ROF_BX, y0 = blockIdx.y * ROF_BY;
+    const int tid = threadIdx.y * ROF_BX + threadIdx.x;
+    for (int i = tid; i < (ROF_BX + 1) * (ROF_BY + 1); i += ROF_BX * ROF_BY) {
+        const int ex = i % (ROF_BX + 1), ey = i / (ROF_BX + 1);
+        sd[ey][ex] = rof_dual<HUBER>(u, p, dt, W, H, x0 - 1 + ex, y0 - 1 + ey, first, eps);
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     if (x >= W || y >= H) return;
-    const Dual c = rof_dual<HUBER>(u, p, dt, W, H, x, y, first, eps);
-    const Dual l = rof_dual<HUBER>(u, p, dt, W, H, x - 1, y, first, eps);
-    const Dual t = rof_dual<HUBER>(u, p, dt, W, H, x, y - 1, first, eps);
+    const Dual c = sd[threadIdx.y + 1][threadIdx.x + 1];
+    const Dual l = sd[threadIdx.y + 1][threadIdx.x];
+    const Dual t = sd[threadIdx.y][threadIdx.x + 1];
     const size_t i = (size_t)y * W + x;
     const float4 im = img[i], uu = u[i];
     const float4 qq = first ? f4(0, 0, 0, 0) : q[i];
@@ -593,7 +607,7 @@ void launch_pd(float4* out, const float4* input, const float4* dt, float4 lam, f
     // PDOptCL.cpp:1137-1166: `iters` steps, plus one when the last left the result in the scratch image
     const int steps = (iters > 0 && iters % 2 == 0) ? iters : iters + 1;
     // step k writes `out` when (steps - 1 - k) is even, so that the last step lands in `out`
-    const dim3 b(32, 8), g = grid2d(W, H, b);
+    const dim3 b(ROF_BX, ROF_BY), g = grid2d(W, H, b);
     const float4* ucur = input;
     for (int k = 0; k < steps; k++) {
         float4* unew = ((steps - 1 - k) % 2 == 0) ? out : ut;
