@@ -273,6 +273,9 @@ def run_batch(args, rank, world, local):
         for a, b, r, d in zip(dl, dr, rs, dm):
             seq.disparity_map(a, b, r, d, iters, pp=1)
 
+    # the branch count of the batch graph, picked by timing this batch at 1 iteration (untimed)
+    from cvt_b200.autotune import tune_batch
+    tuned = tune_batch(pm, dl, dr, rs, dm, iterations=1, candidates=(4, 8, 16))
     for _ in range(args.warmup):
         batched()
     clocks = Clocks(local).start()
@@ -286,7 +289,10 @@ def run_batch(args, rank, world, local):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "batch", "pairs": len(specs), "megapixels": px_it / executed(iters) / 1e6,
                        "window": 21, "iterations": iters, "iterations_executed": executed(iters), "views": 2,
-                       "pp": "lrcheck", "parallelism": "pairs%d" % world, "schedule": "one graph launch",
+                       "pp": "lrcheck", "parallelism": "pairs%d" % world,
+                       "schedule": "one graph launch, %d concurrent branches (autotuned: %s ms per "
+                                   "1-iteration batch)" % (tuned["branches"],
+                                                           {k: round(v, 1) for k, v in tuned["ms"].items()}),
                        "l2": "inputs and workspaces (~25 GB) far larger than L2"},
             "sequential": {"value": world * px_it * args.steps / (ts * 1e-3) / 1e6, "ms_per_step": ts / args.steps,
                            "schedule": "64 eager single-pair calls"},

@@ -1,0 +1,33 @@
+"""Autotuner of the batched schedule (pm_disparity_map_batch_device).
+
+A batch of uneven pairs runs as one CUDA graph whose branches execute concurrently;
+how many branches share the GPU trades overlap (small pairs and short smoothing
+kernels beside long propagate kernels) against contention.  tune_batch times the
+caller's own batch, with a short iteration count, at each candidate branch count and
+keeps the fastest on the handle (pm_set_batch_branches); results equal those of any
+other setting (every pair's arithmetic is the same), only the time differs.
+"""
+import statistics
+
+
+def tune_batch(pm, lefts, rights, patchsizes, disparitymaxs, iterations=1, candidates=(2, 4, 8, 16), reps=2, pp=1):
+    """Returns {"branches": best, "ms": {candidate: median ms}} and leaves `best` set on pm."""
+    import torch
+
+    timings = {}
+    for nb in candidates:
+        pm.set_batch_branches(nb)
+        pm.disparity_map_batch(lefts, rights, patchsizes, disparitymaxs, iterations, pp=pp)   # capture, warm
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            pm.disparity_map_batch(lefts, rights, patchsizes, disparitymaxs, iterations, pp=pp)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        timings[nb] = statistics.median(ms)
+    best = min(timings, key=timings.get)
+    pm.set_batch_branches(best)
+    return {"branches": best, "ms": timings}

@@ -49,6 +49,8 @@ struct pm_handle {
     std::vector<size_t> lws_bytes;
     // the right view's initial disparity of the call in progress (pm_disparity_map_init2_device)
     const float* init_right = nullptr;
+    // concurrent branches of batched calls (pm_set_batch_branches; 0: PM_BATCH_BRANCHES)
+    int batch_branches = 0;
 };
 
 namespace {
@@ -901,6 +903,14 @@ int pm_measure_fp32_peak(int device, float ms, float* tflops)
 
 const char* pm_last_error(const pm_handle* h) { return h ? h->err.c_str() : t_err.c_str(); }
 
+int pm_set_batch_branches(pm_handle* h, int n)
+{
+    if (!h) return fail(nullptr, PM_EINVAL_ARG, "null handle");
+    if (n < 0 || n > PM_BATCH_BRANCHES) return fail(h, PM_EINVAL_ARG, "branch count out of range");
+    h->batch_branches = n;
+    return PM_OK;
+}
+
 int pm_set_counting(pm_handle* h, int on)
 {
     if (!h) return PM_EINVAL_ARG;
@@ -1088,7 +1098,8 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
     }
     // pairs in decreasing window work, each to the least loaded branch (longest processing
     // time first); the branches run concurrently inside one graph
-    const int nb = n < PM_BATCH_BRANCHES ? n : PM_BATCH_BRANCHES;
+    const int cap = h->batch_branches > 0 ? h->batch_branches : PM_BATCH_BRANCHES;
+    const int nb = n < cap ? n : cap;
     while ((int)h->branch.size() < nb) {
         cudaStream_t b;
         PM_CUDA(h, cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
@@ -1143,7 +1154,8 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
         return rc;
     }
     const pm_options& o = h->opt;
-    std::vector<uint64_t> key = {(uint64_t)n, (uint64_t)iterations, (uint64_t)pp, (uint64_t)o.views, (uint64_t)o.fused,
+    std::vector<uint64_t> key = {(uint64_t)n, (uint64_t)nb, (uint64_t)iterations, (uint64_t)pp, (uint64_t)o.views,
+                                 (uint64_t)o.fused,
                                  fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff), (uint64_t)o.rof_iters,
                                  (uint64_t)h->counting};
     for (int i = 0; i < n; i++) {

@@ -54,6 +54,10 @@ class PMHuberStereo:
         except Exception:
             pass
 
+    def set_batch_branches(self, n):
+        """concurrent branches of later batched calls (0: the library's default, 16)"""
+        _lib.check(_lib.lib().pm_set_batch_branches(self._h, int(n)), self._h)
+
     def set_counting(self, on):
         _lib.check(_lib.lib().pm_set_counting(self._h, int(bool(on))), self._h)
 

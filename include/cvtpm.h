@@ -157,6 +157,9 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
                                   const int* patchsize, const float* dispmax, int iterations, int pp,
                                   float* const* dmap, float* const* planes_left, float* const* planes_right,
                                   void* stream);
+/* the number of concurrent branches of later batched calls on this handle, 1..PM_BATCH_BRANCHES
+ * (0: PM_BATCH_BRANCHES); cvt_b200.autotune picks it by timing the caller's batch */
+int pm_set_batch_branches(pm_handle* h, int n);
 
 /* ---- per-kernel entry points (device pointers, enqueued on `stream`) ----------------
  * These expose each reference kernel on injected state for parity testing. */

@@ -79,3 +79,29 @@ def test_batch_rejects_bad_pair(torch_cuda):
     with pytest.raises(StereoError):
         pm.disparity_map_batch([pairs[0][0], pairs[1][0]], [pairs[0][1], pairs[1][1]], [3, 99], [16.0, 12.0], 3)
     assert pm.disparity_map_batch([], [], [], [], 3) == []
+
+
+def test_branch_counts_and_autotuner_keep_results(torch_cuda, native):
+    """every concurrent-branch count gives the same results bit for bit; the autotuner picks one
+    of its candidates and leaves it set"""
+    from cvt_b200 import PMHuberStereo
+    from cvt_b200.autotune import tune_batch
+
+    torch = torch_cuda
+    pairs = _pairs(torch)
+    ls, rs = [p[0] for p in pairs], [p[1] for p in pairs]
+    r, d = [p[2] for p in pairs], [p[3] for p in pairs]
+    pm = PMHuberStereo()
+    ref = [_host(t) for t in pm.disparity_map_batch(ls, rs, r, d, 3)]
+    for nb in (1, 2, 3):
+        pm.set_batch_branches(nb)
+        got = [_host(t) for t in pm.disparity_map_batch(ls, rs, r, d, 3)]
+        assert all(bits_equal(a, b).all() for a, b in zip(got, ref)), nb
+    tuned = tune_batch(pm, ls, rs, r, d, iterations=1, candidates=(1, 2, 4), reps=1)
+    assert tuned["branches"] in (1, 2, 4) and set(tuned["ms"]) == {1, 2, 4}
+    got = [_host(t) for t in pm.disparity_map_batch(ls, rs, r, d, 3)]
+    assert all(bits_equal(a, b).all() for a, b in zip(got, ref))
+    from cvt_b200 import _lib
+
+    with pytest.raises(_lib.StereoError):
+        pm.set_batch_branches(99)
