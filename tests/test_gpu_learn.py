@@ -193,3 +193,28 @@ def test_init2_without_right_equals_disparity_map(torch_cuda, native):
     rc = to_np(c1["planes_right"])[..., 3]
     rr = to_np(a["planes_right"])[..., 3]
     assert np.mean(rc[rc < 2]) < np.mean(rr[rr < 2])
+
+
+def test_one_call_proposal_equals_the_step_by_step_path(torch_cuda, native):
+    """pm_lpp_propose_device (one native call) equals features -> six convolutions ->
+    soft-argmin -> upsampling run call by call, bit for bit, for both views"""
+    torch = torch_cuda
+    from cvt_b200 import scene
+    from cvt_b200.learn import SKIP, PlaneProposal
+    from oracle.pyoracle import bits_equal
+
+    pp = PlaneProposal(seed=4)
+    L, R = scene.generate(8, 150, 93, 6, 2.0, 60.0)
+    dl, dr = torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda()
+    s = torch.cuda.current_stream().cuda_stream
+    for view in (0, 1):
+        one = to_np(pp.propose(dl, dr, view))
+        f = pp.features(dl, dr, view)
+        _, logits = pp.forward(f)
+        H4, W4 = f.shape[1:3]
+        d4 = torch.empty((H4, W4), dtype=torch.float32, device="cuda")
+        assert native.pm_lpp_softargmin(logits.data_ptr(), f.data_ptr(), SKIP, None, d4.data_ptr(), None, None,
+                                        H4 * W4, 0.0, s) == 0
+        up = torch.empty((93, 150), dtype=torch.float32, device="cuda")
+        assert native.pm_lpp_upsample(d4.data_ptr(), W4, H4, 150, 93, up.data_ptr(), s) == 0
+        assert bits_equal(one, to_np(up)).all(), view
