@@ -531,10 +531,13 @@ def run_learned(args, wl, rank, world, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=900))
     W, H, npl, dlo, dhi, r, dmax, iters, views, pp = wl
+    # the proposal's 32 hypotheses cover 124 px at step 1 and 248 px at step 2
+    step = 1 if dmax <= 128 else 2
+    tw, th, tpairs = (512, 384, 128) if step == 1 else (1024, 576, 64)
     t0 = time.perf_counter()
-    feats, target = make_training_set(128, 512, 384, seed=100 + 1000 * rank, device=local)   # 256 maps, both views
+    feats, target = make_training_set(tpairs, tw, th, seed=100 + 1000 * rank, device=local, step=step, dmax=dmax)
     t1 = time.perf_counter()
-    prop = PlaneProposal(seed=rank, device=local)
+    prop = PlaneProposal(seed=rank, device=local, step=step)
     losses = prop.train(feats, target, steps=3000, batch=16, lr=1e-3, seed=rank)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
@@ -565,11 +568,14 @@ def run_learned(args, wl, rank, world, local):
     plain, t_plain = timed(lambda: pm.disparity_map(dL, dR, r, dmax, iters, pp=pp, planes=True))
     c_plain, d_plain = stats(plain)
     keep = d_plain > 0
+    # fixed proposal buffers: the disparityMap graph is captured once and replayed
+    iL = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    iR = torch.empty((H, W), dtype=torch.float32, device="cuda")
     rows, found, found_cost = [], None, None
-    for k in (1, 3, 5, 7, 9):
+    for k in ((1, 3, 5, 7, 9) if step == 1 else (3, 5, 9)):
         res, t_k = timed(lambda: pm.disparity_map(dL, dR, r, dmax, k, pp=pp, planes=True,
-                                                  initdisparity=prop.propose(dL, dR, 0),
-                                                  initdisparity_right=prop.propose(dL, dR, 1)))
+                                                  initdisparity=prop.propose(dL, dR, 0, out=iL),
+                                                  initdisparity_right=prop.propose(dL, dR, 1, out=iR)))
         c_k, d_k = stats(res)
         agree = float(((d_k - d_plain).abs() < 1.0)[keep].float().mean().item())
         rnd, t_r = timed(lambda: pm.disparity_map(dL, dR, r, dmax, k, pp=pp, planes=True))
@@ -582,7 +588,7 @@ def run_learned(args, wl, rank, world, local):
         if found_cost is None and c_k <= 1.01 * c_plain:
             found_cost = rows[-1]
     clk = clocks.stop()
-    _, t_prop = timed(lambda: (prop.propose(dL, dR, 0), prop.propose(dL, dR, 1)))
+    _, t_prop = timed(lambda: (prop.propose(dL, dR, 0, out=iL), prop.propose(dL, dR, 1, out=iR)))
     prop.check_error()
     value = found["learned_ms"] if found else None
     line = {"metric": "ms to plain-8-iter cost (learned vs random init)", "value": value, "unit": "ms", "n_gpus": world,
@@ -591,7 +597,8 @@ def run_learned(args, wl, rank, world, local):
             "config": {"workload": args.config, "mode": "learned", "width": W, "height": H, "dispmax": dmax,
                        "window": 2 * r + 1, "plain_iterations": iters, "parallelism": "pairs%d" % world,
                        "criterion": "mean cost <= 1.01 x plain and >= 98% of plain's kept pixels within 1 px",
-                       "training": {"pairs": 128, "maps": 256, "size": "512x384", "steps": 3000, "batch": 16,
+                       "training": {"pairs": tpairs, "maps": 2 * tpairs, "size": "%dx%d" % (tw, th),
+                                    "hypothesis_step": step, "steps": 3000, "batch": 16,
                                     "data_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
                                     "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:]))}},
             "plain": {"ms": t_plain, "cost": c_plain, "fraction_of_plain_time": None},

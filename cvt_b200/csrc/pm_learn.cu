@@ -5,7 +5,8 @@
 //
 // Network, at a quarter of the image resolution (W4 = W / 4, H4 = H / 4, floor):
 //   features  grey of 4x4 blocks of both images; a cost volume of D = 32 disparity hypotheses
-//             (0 .. 31 quarter pixels): 3x3 mean of |gL(x, y) - gR(x - d, y)|, times 8
+//             (0, k, .. 31 k quarter pixels, k = 1 up to 124 px, 2 up to 248 px): 3x3 mean of
+//             |gL(x, y) - gR(x - k d, y)|, times 8
 //   6 convs   3x3, 32 -> 32 channels, BF16 weights and activations, FP32 accumulation; ReLU
 //             after the first five; the sixth gives 32 logits per pixel (FP32)
 //   output    soft-argmin: disparity4 = sum_d d softmax(-(logit_d + skip * cost_d))_d (the
@@ -301,9 +302,9 @@ __global__ void k_grey4(const uint8_t* __restrict__ img, size_t stride, int W4, 
     out[(size_t)y * W4 + x] = s * (1.0f / (16.0f * 255.0f));
 }
 
-// cost volume: channel d = 8 x the 3x3 mean of |g1(x, y) - g2(x + sd, y)|, s = -1 for the left
-// view (g1 left, g2 right), +1 for the right view (g1 right, g2 left); columns outside the image
-// count as a difference of 1; BF16 NHWC
+// cost volume: channel d = 8 x the 3x3 mean of |g1(x, y) - g2(x + s k d, y)| (hypothesis d at k d
+// quarter pixels, k = step), s = -1 for the left view (g1 left, g2 right), +1 for the right view
+// (g1 right, g2 left); columns outside the image count as a difference of 1; BF16 NHWC
 __global__ void k_costvol(const float* __restrict__ gl, const float* __restrict__ gr, int W4, int H4, int sgn,
                           __nv_bfloat16* __restrict__ out)
 {
@@ -335,7 +336,7 @@ __global__ void k_costvol(const float* __restrict__ gl, const float* __restrict_
 // target < 0 is masked): disparity out, dLogits (BF16, scaled by 1 / count) and per-block loss
 // sums
 __global__ void k_softargmin(const float* __restrict__ logits, const __nv_bfloat16* __restrict__ feats, float skip,
-                             const float* __restrict__ target, float* __restrict__ disp,
+                             float step, const float* __restrict__ target, float* __restrict__ disp,
                              __nv_bfloat16* __restrict__ dlogits, float* __restrict__ loss_part, int M, float inv_count)
 {
     __shared__ float red[256];
@@ -357,6 +358,7 @@ __global__ void k_softargmin(const float* __restrict__ logits, const __nv_bfloat
             p[d] /= z;
             e += (float)d * p[d];
         }
+        e *= step;   // hypotheses are `step` quarter pixels apart
         disp[m] = e;
         if (dlogits) {
             float g = 0.0f;
@@ -366,7 +368,8 @@ __global__ void k_softargmin(const float* __restrict__ logits, const __nv_bfloat
                 l = fabsf(r) < 1.0f ? 0.5f * r * r : fabsf(r) - 0.5f;
                 g = (fabsf(r) < 1.0f ? r : copysignf(1.0f, r)) * inv_count;
             }
-            for (int d = 0; d < CH; d++) dlogits[(size_t)m * CH + d] = __float2bfloat16_rn(-p[d] * ((float)d - e) * g);
+            for (int d = 0; d < CH; d++)
+                dlogits[(size_t)m * CH + d] = __float2bfloat16_rn(-p[d] * (step * (float)d - e) * g);
         }
     }
     red[threadIdx.x] = l;
@@ -516,7 +519,7 @@ int pm_lpp_wgrad(const void* x, const void* dy, float* scratch, float* grad, int
     return check_launch("pm_lpp_wgrad");
 }
 
-int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view,
+int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view, int step,
                     float* grey_scratch, void* out, void* stream)
 {
     if (W < 4 || H < 4 || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
@@ -527,16 +530,18 @@ int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, siz
     k_grey4<<<g, 128, 0, S(stream)>>>(right, stride, W4, H4, grey_scratch + (size_t)W4 * H4);
     float* g0 = grey_scratch;
     float* g1 = grey_scratch + (size_t)W4 * H4;
-    if (right_view) k_costvol<<<g, 128, 0, S(stream)>>>(g1, g0, W4, H4, 1, static_cast<__nv_bfloat16*>(out));
-    else k_costvol<<<g, 128, 0, S(stream)>>>(g0, g1, W4, H4, -1, static_cast<__nv_bfloat16*>(out));
+    if (step < 1 || step > 8) return lfail(PM_EINVAL_ARG, "hypothesis step out of range");
+    if (right_view) k_costvol<<<g, 128, 0, S(stream)>>>(g1, g0, W4, H4, step, static_cast<__nv_bfloat16*>(out));
+    else k_costvol<<<g, 128, 0, S(stream)>>>(g0, g1, W4, H4, -step, static_cast<__nv_bfloat16*>(out));
     return check_launch("pm_lpp_features");
 }
 
-int pm_lpp_softargmin(const float* logits, const void* feats, float skip, const float* target, float* disp, void* dlogits,
-                      float* loss_part, int M, float inv_count, void* stream)
+int pm_lpp_softargmin(const float* logits, const void* feats, float skip, float step, const float* target, float* disp,
+                      void* dlogits, float* loss_part, int M, float inv_count, void* stream)
 {
-    if (M <= 0 || !logits || !disp) return lfail(PM_EINVAL_ARG, "bad argument");
-    k_softargmin<<<(M + 255) / 256, 256, 0, S(stream)>>>(logits, static_cast<const __nv_bfloat16*>(feats), skip, target, disp,
+    if (M <= 0 || !logits || !disp || !(step > 0.0f)) return lfail(PM_EINVAL_ARG, "bad argument");
+    k_softargmin<<<(M + 255) / 256, 256, 0, S(stream)>>>(logits, static_cast<const __nv_bfloat16*>(feats), skip, step, target,
+                                                          disp,
                                                           static_cast<__nv_bfloat16*>(dlogits), loss_part, M, inv_count);
     return check_launch("pm_lpp_softargmin");
 }
@@ -582,7 +587,7 @@ size_t pm_lpp_propose_workspace_bytes(int W, int H)
     return 2 * M * 4 + 3 * M * CH * 2 + M * CH * 4 + M * 4 + 6 * 256;
 }
 
-int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, const uint8_t* left,
+int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, int step, const uint8_t* left,
                           const uint8_t* right, int W, int H, size_t stride, int right_view, float* initdisp, void* workspace,
                           size_t ws_bytes, int* err, void* stream)
 {
@@ -605,7 +610,7 @@ int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, f
     float* logits = reinterpret_cast<float*>(ws + off);
     off += (M * CH * 4 + 255) & ~(size_t)255;
     float* d4 = reinterpret_cast<float*>(ws + off);
-    int rc = pm_lpp_features(left, right, W, H, stride, right_view, grey, feats, stream);
+    int rc = pm_lpp_features(left, right, W, H, stride, right_view, step, grey, feats, stream);
     if (rc) return rc;
     const auto* w = static_cast<const __nv_bfloat16*>(wmats);
     const __nv_bfloat16* x = feats;
@@ -617,7 +622,7 @@ int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, f
         if (rc) return rc;
         x = act[l & 1];
     }
-    rc = pm_lpp_softargmin(logits, feats, skip, nullptr, d4, nullptr, nullptr, (int)M, 0.0f, stream);
+    rc = pm_lpp_softargmin(logits, feats, skip, (float)step, nullptr, d4, nullptr, nullptr, (int)M, 0.0f, stream);
     if (rc) return rc;
     return pm_lpp_upsample(d4, W4, H4, W, H, initdisp, stream);
 }

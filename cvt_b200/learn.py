@@ -40,10 +40,12 @@ def _p(t):
 class PlaneProposal:
     """The network's FP32 master weights, their BF16 copies and Adam state, on one device."""
 
-    def __init__(self, seed=0, device=0, tensor_cores=True):
+    def __init__(self, seed=0, device=0, tensor_cores=True, step=1):
+        """step: quarter pixels between the 32 disparity hypotheses (1: 0-124 px, 2: 0-248 px)"""
         import torch
 
         self.torch = torch
+        self.hstep = int(step)
         self.dev = torch.device("cuda", device)
         self.tc = int(bool(tensor_cores))
         rng = np.random.default_rng(seed)
@@ -83,12 +85,12 @@ class PlaneProposal:
         return [a.cpu().numpy() for a in self.p]
 
     def save(self, path):
-        np.savez_compressed(path, *self.params(), step=self.step)
+        np.savez_compressed(path, *self.params(), step=self.step, hstep=self.hstep)
 
     @classmethod
     def load(cls, path, device=0, tensor_cores=True):
         z = np.load(path)
-        pp = cls(device=device, tensor_cores=tensor_cores)
+        pp = cls(device=device, tensor_cores=tensor_cores, step=int(z["hstep"]) if "hstep" in z else 1)
         pp.set_params([z["arr_%d" % l] for l in range(NLAYERS)])
         pp.step = int(z["step"])
         return pp
@@ -109,8 +111,8 @@ class PlaneProposal:
         H4, W4 = H // 4, W // 4
         grey = torch.empty(2 * H4 * W4, dtype=torch.float32, device=self.dev)
         out = torch.empty((1, H4, W4, CH), dtype=torch.bfloat16, device=self.dev)
-        _check(_lib.lib().pm_lpp_features(_p(left.contiguous()), _p(right.contiguous()), W, H, W * 4, int(view), _p(grey),
-                                          _p(out), self._stream()))
+        _check(_lib.lib().pm_lpp_features(_p(left.contiguous()), _p(right.contiguous()), W, H, W * 4, int(view),
+                                          self.hstep, _p(grey), _p(out), self._stream()))
         return out
 
     def forward(self, feats):
@@ -135,8 +137,8 @@ class PlaneProposal:
         _, logits = self.forward(feats)
         B, H4, W4 = feats.shape[:3]
         d = torch.empty((B, H4, W4), dtype=torch.float32, device=self.dev)
-        _check(_lib.lib().pm_lpp_softargmin(_p(logits), _p(feats), SKIP, None, _p(d), None, None, B * H4 * W4, 0.0,
-                                            self._stream()))
+        _check(_lib.lib().pm_lpp_softargmin(_p(logits), _p(feats), SKIP, float(self.hstep), None, _p(d), None, None,
+                                            B * H4 * W4, 0.0, self._stream()))
         return d
 
     def gradients(self, feats, target4):
@@ -149,8 +151,8 @@ class PlaneProposal:
         dy = torch.empty((B, H4, W4, CH), dtype=torch.bfloat16, device=self.dev)
         parts = torch.empty((M + 255) // 256, dtype=torch.float32, device=self.dev)
         count = max(int((target4 >= 0).sum().item()), 1)
-        _check(L.pm_lpp_softargmin(_p(logits), _p(feats), SKIP, _p(target4.contiguous()), _p(disp), _p(dy), _p(parts), M,
-                                   1.0 / count, self._stream()))
+        _check(L.pm_lpp_softargmin(_p(logits), _p(feats), SKIP, float(self.hstep), _p(target4.contiguous()), _p(disp),
+                                   _p(dy), _p(parts), M, 1.0 / count, self._stream()))
         per_block = 256
         scratch = torch.empty(L.pm_lpp_wgrad_scratch_floats(B, H4, W4, per_block), dtype=torch.float32, device=self.dev)
         grads = [None] * NLAYERS
@@ -191,21 +193,27 @@ class PlaneProposal:
         self.check_error()
         return losses
 
-    def propose(self, left, right, view=0):
+    def propose(self, left, right, view=0, out=None):
         """full-resolution initial disparity (pixels) of the left (view 0) or right view (1) for a
-        pair of (H, W, 4) uint8 CUDA tensors, through the single native call pm_lpp_propose_device"""
+        pair of (H, W, 4) uint8 CUDA tensors, through the single native call pm_lpp_propose_device;
+        `out` (an (H, W) float32 CUDA tensor) is filled in place when given, so that a following
+        disparity_map call sees the same buffer and replays its graph"""
         torch, L = self.torch, _lib.lib()
         H, W = left.shape[:2]
-        ws = torch.empty(L.pm_lpp_propose_workspace_bytes(W, H) + 256, dtype=torch.uint8, device=self.dev)
+        nbytes = L.pm_lpp_propose_workspace_bytes(W, H) + 256
+        if getattr(self, "_ws", None) is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.dev)
+        ws = self._ws
         off = (-ws.data_ptr()) % 256
-        out = torch.empty((H, W), dtype=torch.float32, device=self.dev)
-        _check(L.pm_lpp_propose_device(_p(self.wmat[0]), _p(self.ball), NLAYERS, SKIP, _p(left.contiguous()),
+        if out is None:
+            out = torch.empty((H, W), dtype=torch.float32, device=self.dev)
+        _check(L.pm_lpp_propose_device(_p(self.wmat[0]), _p(self.ball), NLAYERS, SKIP, self.hstep, _p(left.contiguous()),
                                        _p(right.contiguous()), W, H, W * 4, int(view), _p(out), ws.data_ptr() + off,
                                        ws.numel() - off, _p(self.err), self._stream()))
         return out
 
 
-def make_training_set(pairs, width, height, seed, iterations=8, patch=7, dmax=None, device=0):
+def make_training_set(pairs, width, height, seed, iterations=8, patch=7, dmax=None, device=0, step=1):
     """Training maps from procedural scenes, two per pair: the left view's features with the
     quarter-resolution mean of plain (random-init) PatchMatch's LR-checked left disparity after
     `iterations` iterations, and the right view's features with its right disparity."""
@@ -216,15 +224,16 @@ def make_training_set(pairs, width, height, seed, iterations=8, patch=7, dmax=No
 
     dev = torch.device("cuda", device)
     pm = PMHuberStereo(device=device)
-    pp = PlaneProposal(device=device)
+    pp = PlaneProposal(device=device, step=step)
     H4, W4 = height // 4, width // 4
     feats = torch.empty((2 * pairs, H4, W4, CH), dtype=torch.bfloat16, device=dev)
     target = torch.empty((2 * pairs, H4, W4), dtype=torch.float32, device=dev)
     dright = torch.empty((height, width), dtype=torch.float32, device=dev)
     L = _lib.lib()
-    dmax = float(dmax if dmax is not None else 4 * CH)
+    dmax = float(dmax if dmax is not None else 4 * CH * step)
     for i in range(pairs):
-        l, r = scene.generate(seed + i, width, height, 8 + (seed + i) % 24, 2.0, min(0.9 * dmax, 30.0 + (i % 4) * 30.0))
+        l, r = scene.generate(seed + i, width, height, 8 + (seed + i) % 24, 2.0,
+                              min(0.9 * dmax, (30.0 + (i % 4) * 30.0) * step))
         dl, dr = torch.from_numpy(l).to(dev), torch.from_numpy(r).to(dev)
         st = torch.cuda.current_stream(dev).cuda_stream
         feats[2 * i] = pp.features(dl, dr, 0)[0]

@@ -383,9 +383,10 @@ int pm_k_svpm_to_flow(float* flow, const float* states, int W, int H, void* stre
 int pm_lpp_channels(void);
 const char* pm_lpp_last_error(void);
 /* cost-volume features of a pair (W, H >= 4; W4 = W / 4, H4 = H / 4) for the left view
- * (right_view 0: channel d compares left x with right x - d) or the right view (1: right x with
- * left x + d): grey_scratch 2 * W4 * H4 floats, out W4 * H4 * 32 BF16 */
-int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view,
+ * (right_view 0: channel d compares left x with right x - step d) or the right view (1: right x
+ * with left x + step d), hypotheses `step` (1..8) quarter pixels apart: grey_scratch 2 * W4 * H4
+ * floats, out W4 * H4 * 32 BF16 */
+int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view, int step,
                     float* grey_scratch, void* out, void* stream);
 /* one convolution over a batch of B activation maps; epi 0: + bias, ReLU, BF16 out; 1: + bias,
  * FP32 out (logits); 2: data gradient: times (mask > 0), BF16 out (wmat then holds the transposed,
@@ -398,10 +399,10 @@ int pm_lpp_conv(int epi, int tensor_cores, const void* in, const void* wmat, con
 size_t pm_lpp_wgrad_scratch_floats(int B, int H4, int W4, int per_block);
 int pm_lpp_wgrad(const void* x, const void* dy, float* scratch, float* grad, int B, int H4, int W4, int per_block, void* stream);
 /* soft-argmin of M x 32 logits plus skip times the features (the cost volume; NULL: none) into
- * disparities (quarter pixels); with dlogits, also the smooth-L1 loss against target (< 0:
+ * disparities (quarter pixels; hypotheses `step` quarter pixels apart); with dlogits, also the smooth-L1 loss against target (< 0:
  * ignored), its gradient times inv_count (BF16) and per-256-pixel loss sums in loss_part */
-int pm_lpp_softargmin(const float* logits, const void* feats, float skip, const float* target, float* disp, void* dlogits,
-                      float* loss_part, int M, float inv_count, void* stream);
+int pm_lpp_softargmin(const float* logits, const void* feats, float skip, float step, const float* target, float* disp,
+                      void* dlogits, float* loss_part, int M, float inv_count, void* stream);
 /* training target: the mean of the positive disparities of each 4x4 block, in quarter pixels
  * (-1 where fewer than 8 of 16 are positive) */
 int pm_lpp_target4(const float* disp, int W, int H, float* out, void* stream);
@@ -414,7 +415,7 @@ int pm_lpp_weights_bf16(const float* p, void* wmat, void* wt, void* stream);
 /* the whole proposal for one pair: nlayers convolutions with weights wmats (nlayers * 32 * 288
  * BF16, 256-byte aligned) and biases (nlayers * 32), initdisp W * H floats (pixels) */
 size_t pm_lpp_propose_workspace_bytes(int W, int H);
-int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, const uint8_t* left,
+int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, int step, const uint8_t* left,
                           const uint8_t* right, int W, int H, size_t stride, int right_view, float* initdisp, void* workspace,
                           size_t ws_bytes, int* err, void* stream);
 

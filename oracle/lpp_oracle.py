@@ -59,27 +59,28 @@ def forward(feat, layers):
 SKIP = 4.0
 
 
-def softargmin(logits, feat=None):
-    """soft-argmin over the logits plus SKIP times the cost volume (the features)"""
+def softargmin(logits, feat=None, step=1.0):
+    """soft-argmin over the logits plus SKIP times the cost volume (the features); hypotheses
+    `step` quarter pixels apart"""
     l = logits.astype(np.float64)
     if feat is not None:
         l = l + SKIP * feat.astype(np.float64)
     p = np.exp(-(l - l.min(-1, keepdims=True)))
     p /= p.sum(-1, keepdims=True)
-    d = (p * np.arange(CH)).sum(-1)
+    d = step * (p * np.arange(CH)).sum(-1)
     return p, d
 
 
-def loss_grad(logits, target, feat=None):
+def loss_grad(logits, target, feat=None, step=1.0):
     """smooth-L1 mean over targets >= 0; returns (loss, dlogits as BF16)"""
-    p, d = softargmin(logits, feat)
+    p, d = softargmin(logits, feat, step)
     valid = target >= 0
     n = max(int(valid.sum()), 1)
     r = d - target
     l = np.where(np.abs(r) < 1, 0.5 * r * r, np.abs(r) - 0.5)
     g = np.where(np.abs(r) < 1, r, np.sign(r)) / n
     g = np.where(valid, g, 0.0)
-    dl = -p * (np.arange(CH) - d[..., None]) * g[..., None]
+    dl = -p * (step * np.arange(CH) - d[..., None]) * g[..., None]
     return float(np.where(valid, l, 0).sum() / n), bf16(dl.astype(np.float32))
 
 
@@ -104,7 +105,7 @@ def backward(acts, layers, dlogits):
     return grads
 
 
-def features(left, right, view=0):
+def features(left, right, view=0, step=1):
     """grey of 4x4 blocks and the 32-hypothesis cost volume (BF16 values) of the left (view 0) or
     right view (1), as k_grey4 / k_costvol"""
     def grey4(img):
@@ -120,7 +121,7 @@ def features(left, right, view=0):
     cv = np.zeros((H4, W4, CH))
     xs = np.arange(W4)
     for d in range(CH):
-        xm = xs + sgn * d
+        xm = xs + sgn * step * d
         inside = (xm >= 0) & (xm < W4)
         other = gr[:, np.clip(xm, 0, W4 - 1)]
         diff = np.where(inside[None, :], np.abs(gl - other), 1.0)

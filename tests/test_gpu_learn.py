@@ -86,14 +86,14 @@ def test_weight_gradient_matches_oracle(torch_cuda, native):
     assert np.abs(g[CH * KTOT:] - dyn.astype(np.float64).sum((0, 1, 2))).max() < 1e-5
 
 
-@pytest.mark.parametrize("tc", [1, 0])
-def test_backward_matches_oracle(torch_cuda, native, tc):
+@pytest.mark.parametrize("tc,step", [(1, 1), (0, 1), (1, 2)])
+def test_backward_matches_oracle(torch_cuda, native, tc, step):
     """loss and the gradients of all six layers against the oracle's backward pass on the same
     BF16 weights and inputs: relative error of each layer's gradient < 1e-2, cosine > 0.999"""
     torch = torch_cuda
     from cvt_b200.learn import PlaneProposal
 
-    pp = PlaneProposal(seed=3, tensor_cores=bool(tc))
+    pp = PlaneProposal(seed=3, tensor_cores=bool(tc), step=step)
     rng = np.random.default_rng(7)
     B, H, W = 2, 12, 20
     feats = O.bf16((rng.random((B, H, W, CH)) * 2).astype(np.float32))
@@ -102,7 +102,7 @@ def test_backward_matches_oracle(torch_cuda, native, tc):
     loss, grads = pp.gradients(bf(torch, feats), torch.from_numpy(target).cuda())
     layers = [(a[:CH * KTOT].reshape(CH, KTOT), a[CH * KTOT:]) for a in pp.params()]
     acts, logits = O.forward(feats, layers)
-    oloss, dl = O.loss_grad(logits, target, feats)
+    oloss, dl = O.loss_grad(logits, target, feats, step)
     og = O.backward(acts, layers, dl)
     assert abs(loss - oloss) < 1e-3 * max(1.0, abs(oloss)), (loss, oloss)
     for l in range(6):
@@ -120,10 +120,11 @@ def test_features_match_oracle(torch_cuda, native):
 
     L, R = scene.generate(3, 203, 121, 6, 2.0, 60.0)
     for view in (0, 1):
-        f = to_np(PlaneProposal().features(torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda(), view))
-        want = O.features(L, R, view)
-        assert f.shape == want.shape
-        assert (np.abs(f - want) <= 2 ** -7 * np.abs(want) + 1e-6).all(), view
+        for step in (1, 2):
+            f = to_np(PlaneProposal(step=step).features(torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda(), view))
+            want = O.features(L, R, view, step)
+            assert f.shape == want.shape
+            assert (np.abs(f - want) <= 2 ** -7 * np.abs(want) + 1e-6).all(), (view, step)
 
 
 def test_training_gains_over_random_init(torch_cuda, native):
@@ -213,8 +214,8 @@ def test_one_call_proposal_equals_the_step_by_step_path(torch_cuda, native):
         _, logits = pp.forward(f)
         H4, W4 = f.shape[1:3]
         d4 = torch.empty((H4, W4), dtype=torch.float32, device="cuda")
-        assert native.pm_lpp_softargmin(logits.data_ptr(), f.data_ptr(), SKIP, None, d4.data_ptr(), None, None,
-                                        H4 * W4, 0.0, s) == 0
+        assert native.pm_lpp_softargmin(logits.data_ptr(), f.data_ptr(), SKIP, float(pp.hstep), None, d4.data_ptr(),
+                                        None, None, H4 * W4, 0.0, s) == 0
         up = torch.empty((93, 150), dtype=torch.float32, device="cuda")
         assert native.pm_lpp_upsample(d4.data_ptr(), W4, H4, 150, 93, up.data_ptr(), s) == 0
         assert bits_equal(one, to_np(up)).all(), view
