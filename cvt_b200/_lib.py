@@ -32,7 +32,7 @@ SYMBOLS = [
     "pm_svpm_create", "pm_svpm_destroy", "pm_svpm_last_error", "pm_svpm_flow", "pm_svpm_flow_device",
     "pm_svpm_set_counting", "pm_svpm_get_counters", "pm_k_svpm_init", "pm_k_svpm_prop", "pm_k_svpm_to_flow",
     "pm_lpp_channels", "pm_lpp_last_error", "pm_lpp_features", "pm_lpp_conv", "pm_lpp_wgrad_scratch_floats",
-    "pm_lpp_wgrad", "pm_lpp_softargmin", "pm_lpp_target4", "pm_lpp_upsample", "pm_lpp_adam", "pm_lpp_weights_bf16",
+    "pm_lpp_wgrad", "pm_lpp_softargmin", "pm_lpp_target", "pm_lpp_upsample", "pm_lpp_adam", "pm_lpp_weights_bf16",
     "pm_lpp_propose_workspace_bytes", "pm_lpp_propose_device",
 ]
 
@@ -143,17 +143,17 @@ def lib():
         "pm_k_svpm_to_flow": (i32, [vp, vp, i32, i32, vp]),
         "pm_lpp_channels": (i32, []),
         "pm_lpp_last_error": (C.c_char_p, []),
-        "pm_lpp_features": (i32, [vp, vp, i32, i32, sz, i32, i32, vp, vp, vp]),
+        "pm_lpp_features": (i32, [vp, vp, i32, i32, sz, i32, i32, i32, vp, vp, vp]),
         "pm_lpp_conv": (i32, [i32, i32, vp, vp, vp, vp, vp, i32, i32, i32, vp, vp]),
         "pm_lpp_wgrad_scratch_floats": (sz, [i32, i32, i32, i32]),
         "pm_lpp_wgrad": (i32, [vp, vp, vp, vp, i32, i32, i32, i32, vp]),
         "pm_lpp_softargmin": (i32, [vp, vp, f32, f32, vp, vp, vp, vp, i32, f32, vp]),
-        "pm_lpp_target4": (i32, [vp, i32, i32, vp, vp]),
-        "pm_lpp_upsample": (i32, [vp, i32, i32, i32, i32, vp, vp]),
+        "pm_lpp_target": (i32, [vp, i32, i32, i32, vp, vp]),
+        "pm_lpp_upsample": (i32, [vp, i32, i32, i32, i32, i32, vp, vp]),
         "pm_lpp_adam": (i32, [vp, vp, vp, vp, i32, f32, i32, vp]),
         "pm_lpp_weights_bf16": (i32, [vp, vp, vp, vp]),
-        "pm_lpp_propose_workspace_bytes": (sz, [i32, i32]),
-        "pm_lpp_propose_device": (i32, [vp, vp, i32, f32, i32, vp, vp, i32, i32, sz, i32, vp, vp, sz, vp, vp]),
+        "pm_lpp_propose_workspace_bytes": (sz, [i32, i32, i32]),
+        "pm_lpp_propose_device": (i32, [vp, vp, i32, f32, i32, i32, vp, vp, i32, i32, sz, i32, vp, vp, sz, vp, vp]),
         "pm_disparity_map_init2_device": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, i32, vp, vp, vp, vp, vp, vp,
                                                 vp]),
     }

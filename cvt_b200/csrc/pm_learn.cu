@@ -3,15 +3,16 @@
 // pmhstereo_init_disparity_normal, pmhstereo.cl:802-828; normals then come from
 // pmhstereo_disparity_to_normal).
 //
-// Network, at a quarter of the image resolution (W4 = W / 4, H4 = H / 4, floor):
-//   features  grey of 4x4 blocks of both images; a cost volume of D = 32 disparity hypotheses
-//             (0, k, .. 31 k quarter pixels, k = 1 up to 124 px, 2 up to 248 px): 3x3 mean of
-//             |gL(x, y) - gR(x - k d, y)|, times 8
+// Network, at a quarter (scale 4) or half (scale 2) of the image resolution (W4 = W / scale,
+// H4 = H / scale, floor; "feature pixels"):
+//   features  grey of scale x scale blocks of both images; a cost volume of D = 32 disparity
+//             hypotheses (0, k, .. 31 k feature pixels; at scale 4, k = 1 reaches 124 px and 2
+//             reaches 248 px): 3x3 mean of |gL(x, y) - gR(x - k d, y)|, times 8
 //   6 convs   3x3, 32 -> 32 channels, BF16 weights and activations, FP32 accumulation; ReLU
 //             after the first five; the sixth gives 32 logits per pixel (FP32)
-//   output    soft-argmin: disparity4 = sum_d d softmax(-(logit_d + skip * cost_d))_d (the
-//             network corrects the matching cost); upsampled bilinearly and scaled by 4 to a
-//             full-resolution initial disparity
+//   output    soft-argmin: disparity = k sum_d d softmax(-(logit_d + skip * cost_d))_d (the
+//             network corrects the matching cost); upsampled bilinearly and scaled by `scale`
+//             to a full-resolution initial disparity
 // Training (cvt_b200/learn.py drives it): smooth-L1 loss against the quarter-resolution mean
 // of plain PatchMatch's disparity, hand-written backward kernels (data gradients through the
 // same tensor-core kernel with the transposed, mirrored weights; weight gradients on the CUDA
@@ -286,20 +287,20 @@ __global__ void k_wgrad_sum(const float* __restrict__ part, float* __restrict__ 
     grad[i] = s;
 }
 
-// grey of the 4x4 blocks of an RGBA8 image (0.2126, 0.7152, 0.0722 weights on k / 255)
-__global__ void k_grey4(const uint8_t* __restrict__ img, size_t stride, int W4, int H4, float* __restrict__ out)
+// grey of the sc x sc blocks of an RGBA8 image (0.2126, 0.7152, 0.0722 weights on k / 255)
+__global__ void k_grey(const uint8_t* __restrict__ img, size_t stride, int sc, int W4, int H4, float* __restrict__ out)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W4) return;
     float s = 0.0f;
-    for (int j = 0; j < 4; j++) {
-        const uchar4* row = reinterpret_cast<const uchar4*>(img + (size_t)(4 * y + j) * stride) + 4 * x;
-        for (int i = 0; i < 4; i++) {
+    for (int j = 0; j < sc; j++) {
+        const uchar4* row = reinterpret_cast<const uchar4*>(img + (size_t)(sc * y + j) * stride) + sc * x;
+        for (int i = 0; i < sc; i++) {
             const uchar4 p = __ldg(row + i);
             s += 0.2126f * (float)p.x + 0.7152f * (float)p.y + 0.0722f * (float)p.z;
         }
     }
-    out[(size_t)y * W4 + x] = s * (1.0f / (16.0f * 255.0f));
+    out[(size_t)y * W4 + x] = s * (1.0f / ((float)(sc * sc) * 255.0f));
 }
 
 // cost volume: channel d = 8 x the 3x3 mean of |g1(x, y) - g2(x + s k d, y)| (hypothesis d at k d
@@ -381,37 +382,38 @@ __global__ void k_softargmin(const float* __restrict__ logits, const __nv_bfloat
     if (threadIdx.x == 0 && loss_part) loss_part[blockIdx.x] = red[0];
 }
 
-// quarter-resolution training target: mean of the valid (> 0) disparities of each 4x4 block / 4,
-// -1 when fewer than half are valid
-__global__ void k_target4(const float* __restrict__ disp, int W, int W4, int H4, float* __restrict__ out)
+// training target at 1 / sc resolution: mean of the valid (> 0) disparities of each sc x sc block
+// / sc, -1 when fewer than half are valid
+__global__ void k_target(const float* __restrict__ disp, int W, int sc, int W4, int H4, float* __restrict__ out)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W4) return;
     float s = 0.0f;
     int n = 0;
-    for (int j = 0; j < 4; j++)
-        for (int i = 0; i < 4; i++) {
-            const float v = disp[(size_t)(4 * y + j) * W + 4 * x + i];
+    for (int j = 0; j < sc; j++)
+        for (int i = 0; i < sc; i++) {
+            const float v = disp[(size_t)(sc * y + j) * W + sc * x + i];
             if (v > 0.0f) {
                 s += v;
                 n++;
             }
         }
-    out[(size_t)y * W4 + x] = n >= 8 ? s / (4.0f * (float)n) : -1.0f;
+    out[(size_t)y * W4 + x] = 2 * n >= sc * sc ? s / ((float)sc * (float)n) : -1.0f;
 }
 
-// full-resolution initial disparity: bilinear upsampling of the quarter-resolution result, times 4
-__global__ void k_upsample(const float* __restrict__ d4, int W4, int H4, int W, int H, float* __restrict__ out)
+// full-resolution initial disparity: bilinear upsampling of the 1 / sc resolution result, times sc
+__global__ void k_upsample(const float* __restrict__ d4, int W4, int H4, int W, int H, int sc, float* __restrict__ out)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= W) return;
-    const float u = fminf(fmaxf(((float)x + 0.5f) * 0.25f - 0.5f, 0.0f), (float)(W4 - 1));
-    const float v = fminf(fmaxf(((float)y + 0.5f) * 0.25f - 0.5f, 0.0f), (float)(H4 - 1));
+    const float inv = 1.0f / (float)sc;
+    const float u = fminf(fmaxf(((float)x + 0.5f) * inv - 0.5f, 0.0f), (float)(W4 - 1));
+    const float v = fminf(fmaxf(((float)y + 0.5f) * inv - 0.5f, 0.0f), (float)(H4 - 1));
     const int x0 = (int)u, y0 = (int)v, x1 = min(x0 + 1, W4 - 1), y1 = min(y0 + 1, H4 - 1);
     const float a = u - (float)x0, b = v - (float)y0;
     const float r0 = (1.0f - a) * d4[(size_t)y0 * W4 + x0] + a * d4[(size_t)y0 * W4 + x1];
     const float r1 = (1.0f - a) * d4[(size_t)y1 * W4 + x0] + a * d4[(size_t)y1 * W4 + x1];
-    out[(size_t)y * W + x] = 4.0f * ((1.0f - b) * r0 + b * r1);
+    out[(size_t)y * W + x] = (float)sc * ((1.0f - b) * r0 + b * r1);
 }
 
 // Adam on the FP32 master weights of one layer (CH * KTOT weights then CH biases), then the BF16
@@ -520,14 +522,15 @@ int pm_lpp_wgrad(const void* x, const void* dy, float* scratch, float* grad, int
 }
 
 int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view, int step,
-                    float* grey_scratch, void* out, void* stream)
+                    int scale, float* grey_scratch, void* out, void* stream)
 {
-    if (W < 4 || H < 4 || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
+    if (scale != 2 && scale != 4) return lfail(PM_EINVAL_ARG, "scale must be 2 or 4");
+    if (W < scale || H < scale || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
     if (!left || !right || !grey_scratch || !out || stride < (size_t)W * 4 || stride % 4) return lfail(PM_EINVAL_ARG, "bad argument");
-    const int W4 = W / 4, H4 = H / 4;
+    const int W4 = W / scale, H4 = H / scale;
     const dim3 g((W4 + 127) / 128, H4);
-    k_grey4<<<g, 128, 0, S(stream)>>>(left, stride, W4, H4, grey_scratch);
-    k_grey4<<<g, 128, 0, S(stream)>>>(right, stride, W4, H4, grey_scratch + (size_t)W4 * H4);
+    k_grey<<<g, 128, 0, S(stream)>>>(left, stride, scale, W4, H4, grey_scratch);
+    k_grey<<<g, 128, 0, S(stream)>>>(right, stride, scale, W4, H4, grey_scratch + (size_t)W4 * H4);
     float* g0 = grey_scratch;
     float* g1 = grey_scratch + (size_t)W4 * H4;
     if (step < 1 || step > 8) return lfail(PM_EINVAL_ARG, "hypothesis step out of range");
@@ -546,18 +549,18 @@ int pm_lpp_softargmin(const float* logits, const void* feats, float skip, float 
     return check_launch("pm_lpp_softargmin");
 }
 
-int pm_lpp_target4(const float* disp, int W, int H, float* out, void* stream)
+int pm_lpp_target(const float* disp, int W, int H, int scale, float* out, void* stream)
 {
-    if (W < 4 || H < 4 || !disp || !out) return lfail(PM_EINVAL_ARG, "bad argument");
-    const int W4 = W / 4, H4 = H / 4;
-    k_target4<<<dim3((W4 + 127) / 128, H4), 128, 0, S(stream)>>>(disp, W, W4, H4, out);
-    return check_launch("pm_lpp_target4");
+    if ((scale != 2 && scale != 4) || W < scale || H < scale || !disp || !out) return lfail(PM_EINVAL_ARG, "bad argument");
+    const int W4 = W / scale, H4 = H / scale;
+    k_target<<<dim3((W4 + 127) / 128, H4), 128, 0, S(stream)>>>(disp, W, scale, W4, H4, out);
+    return check_launch("pm_lpp_target");
 }
 
-int pm_lpp_upsample(const float* d4, int W4, int H4, int W, int H, float* out, void* stream)
+int pm_lpp_upsample(const float* d4, int W4, int H4, int W, int H, int scale, float* out, void* stream)
 {
-    if (W4 <= 0 || H4 <= 0 || W <= 0 || H <= 0 || !d4 || !out) return lfail(PM_EINVAL_ARG, "bad argument");
-    k_upsample<<<dim3((W + 127) / 128, H), 128, 0, S(stream)>>>(d4, W4, H4, W, H, out);
+    if (W4 <= 0 || H4 <= 0 || W <= 0 || H <= 0 || scale < 1 || !d4 || !out) return lfail(PM_EINVAL_ARG, "bad argument");
+    k_upsample<<<dim3((W + 127) / 128, H), 128, 0, S(stream)>>>(d4, W4, H4, W, H, scale, out);
     return check_launch("pm_lpp_upsample");
 }
 
@@ -578,25 +581,26 @@ int pm_lpp_weights_bf16(const float* p, void* wmat, void* wt, void* stream)
     return check_launch("pm_lpp_weights_bf16");
 }
 
-size_t pm_lpp_propose_workspace_bytes(int W, int H)
+size_t pm_lpp_propose_workspace_bytes(int W, int H, int scale)
 {
-    if (W < 4 || H < 4) return 0;
-    const size_t M = (size_t)(W / 4) * (H / 4);
+    if ((scale != 2 && scale != 4) || W < scale || H < scale) return 0;
+    const size_t M = (size_t)(W / scale) * (H / scale);
     // two grey planes, the features and two BF16 activation buffers, FP32 logits, the quarter
     // disparity
     return 2 * M * 4 + 3 * M * CH * 2 + M * CH * 4 + M * 4 + 6 * 256;
 }
 
-int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, int step, const uint8_t* left,
-                          const uint8_t* right, int W, int H, size_t stride, int right_view, float* initdisp, void* workspace,
-                          size_t ws_bytes, int* err, void* stream)
+int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, int step, int scale,
+                          const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view,
+                          float* initdisp, void* workspace, size_t ws_bytes, int* err, void* stream)
 {
-    if (W < 4 || H < 4 || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
+    if (scale != 2 && scale != 4) return lfail(PM_EINVAL_ARG, "scale must be 2 or 4");
+    if (W < scale || H < scale || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
     if (!wmats || !biases || nlayers < 1 || !left || !right || !initdisp || !workspace || !err)
         return lfail(PM_EINVAL_ARG, "null argument");
-    if (ws_bytes < pm_lpp_propose_workspace_bytes(W, H)) return lfail(PM_EINVAL_ARG, "workspace too small");
+    if (ws_bytes < pm_lpp_propose_workspace_bytes(W, H, scale)) return lfail(PM_EINVAL_ARG, "workspace too small");
     if (((uintptr_t)workspace | (uintptr_t)wmats) & 255) return lfail(PM_EINVAL_ARG, "workspace and weights must be 256-byte aligned");
-    const int W4 = W / 4, H4 = H / 4;
+    const int W4 = W / scale, H4 = H / scale;
     const size_t M = (size_t)W4 * H4;
     char* ws = static_cast<char*>(workspace);
     float* grey = reinterpret_cast<float*>(ws);
@@ -610,7 +614,7 @@ int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, f
     float* logits = reinterpret_cast<float*>(ws + off);
     off += (M * CH * 4 + 255) & ~(size_t)255;
     float* d4 = reinterpret_cast<float*>(ws + off);
-    int rc = pm_lpp_features(left, right, W, H, stride, right_view, step, grey, feats, stream);
+    int rc = pm_lpp_features(left, right, W, H, stride, right_view, step, scale, grey, feats, stream);
     if (rc) return rc;
     const auto* w = static_cast<const __nv_bfloat16*>(wmats);
     const __nv_bfloat16* x = feats;
@@ -624,7 +628,7 @@ int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, f
     }
     rc = pm_lpp_softargmin(logits, feats, skip, (float)step, nullptr, d4, nullptr, nullptr, (int)M, 0.0f, stream);
     if (rc) return rc;
-    return pm_lpp_upsample(d4, W4, H4, W, H, initdisp, stream);
+    return pm_lpp_upsample(d4, W4, H4, W, H, scale, initdisp, stream);
 }
 
 }  // extern "C"

@@ -40,12 +40,15 @@ def _p(t):
 class PlaneProposal:
     """The network's FP32 master weights, their BF16 copies and Adam state, on one device."""
 
-    def __init__(self, seed=0, device=0, tensor_cores=True, step=1):
-        """step: quarter pixels between the 32 disparity hypotheses (1: 0-124 px, 2: 0-248 px)"""
+    def __init__(self, seed=0, device=0, tensor_cores=True, step=1, scale=4):
+        """scale: the network's resolution is 1 / scale of the image's (4 or 2); step: feature
+        pixels between the 32 disparity hypotheses (scale 4: step 1 reaches 124 px, 2 reaches
+        248 px; scale 2: step 2 reaches 124 px)"""
         import torch
 
         self.torch = torch
         self.hstep = int(step)
+        self.scale = int(scale)
         self.dev = torch.device("cuda", device)
         self.tc = int(bool(tensor_cores))
         rng = np.random.default_rng(seed)
@@ -85,12 +88,13 @@ class PlaneProposal:
         return [a.cpu().numpy() for a in self.p]
 
     def save(self, path):
-        np.savez_compressed(path, *self.params(), step=self.step, hstep=self.hstep)
+        np.savez_compressed(path, *self.params(), step=self.step, hstep=self.hstep, scale=self.scale)
 
     @classmethod
     def load(cls, path, device=0, tensor_cores=True):
         z = np.load(path)
-        pp = cls(device=device, tensor_cores=tensor_cores, step=int(z["hstep"]) if "hstep" in z else 1)
+        pp = cls(device=device, tensor_cores=tensor_cores, step=int(z["hstep"]) if "hstep" in z else 1,
+                 scale=int(z["scale"]) if "scale" in z else 4)
         pp.set_params([z["arr_%d" % l] for l in range(NLAYERS)])
         pp.step = int(z["step"])
         return pp
@@ -108,11 +112,11 @@ class PlaneProposal:
         or the right view (1)"""
         torch = self.torch
         H, W = left.shape[:2]
-        H4, W4 = H // 4, W // 4
+        H4, W4 = H // self.scale, W // self.scale
         grey = torch.empty(2 * H4 * W4, dtype=torch.float32, device=self.dev)
         out = torch.empty((1, H4, W4, CH), dtype=torch.bfloat16, device=self.dev)
         _check(_lib.lib().pm_lpp_features(_p(left.contiguous()), _p(right.contiguous()), W, H, W * 4, int(view),
-                                          self.hstep, _p(grey), _p(out), self._stream()))
+                                          self.hstep, self.scale, _p(grey), _p(out), self._stream()))
         return out
 
     def forward(self, feats):
@@ -200,20 +204,21 @@ class PlaneProposal:
         disparity_map call sees the same buffer and replays its graph"""
         torch, L = self.torch, _lib.lib()
         H, W = left.shape[:2]
-        nbytes = L.pm_lpp_propose_workspace_bytes(W, H) + 256
+        nbytes = L.pm_lpp_propose_workspace_bytes(W, H, self.scale) + 256
         if getattr(self, "_ws", None) is None or self._ws.numel() < nbytes:
             self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.dev)
         ws = self._ws
         off = (-ws.data_ptr()) % 256
         if out is None:
             out = torch.empty((H, W), dtype=torch.float32, device=self.dev)
-        _check(L.pm_lpp_propose_device(_p(self.wmat[0]), _p(self.ball), NLAYERS, SKIP, self.hstep, _p(left.contiguous()),
+        _check(L.pm_lpp_propose_device(_p(self.wmat[0]), _p(self.ball), NLAYERS, SKIP, self.hstep, self.scale,
+                                       _p(left.contiguous()),
                                        _p(right.contiguous()), W, H, W * 4, int(view), _p(out), ws.data_ptr() + off,
                                        ws.numel() - off, _p(self.err), self._stream()))
         return out
 
 
-def make_training_set(pairs, width, height, seed, iterations=8, patch=7, dmax=None, device=0, step=1):
+def make_training_set(pairs, width, height, seed, iterations=8, patch=7, dmax=None, device=0, step=1, scale=4):
     """Training maps from procedural scenes, two per pair: the left view's features with the
     quarter-resolution mean of plain (random-init) PatchMatch's LR-checked left disparity after
     `iterations` iterations, and the right view's features with its right disparity."""
@@ -224,13 +229,13 @@ def make_training_set(pairs, width, height, seed, iterations=8, patch=7, dmax=No
 
     dev = torch.device("cuda", device)
     pm = PMHuberStereo(device=device)
-    pp = PlaneProposal(device=device, step=step)
-    H4, W4 = height // 4, width // 4
+    pp = PlaneProposal(device=device, step=step, scale=scale)
+    H4, W4 = height // scale, width // scale
     feats = torch.empty((2 * pairs, H4, W4, CH), dtype=torch.bfloat16, device=dev)
     target = torch.empty((2 * pairs, H4, W4), dtype=torch.float32, device=dev)
     dright = torch.empty((height, width), dtype=torch.float32, device=dev)
     L = _lib.lib()
-    dmax = float(dmax if dmax is not None else 4 * CH * step)
+    dmax = float(dmax if dmax is not None else scale * CH * step)
     for i in range(pairs):
         l, r = scene.generate(seed + i, width, height, 8 + (seed + i) % 24, 2.0,
                               min(0.9 * dmax, (30.0 + (i % 4) * 30.0) * step))
@@ -239,7 +244,7 @@ def make_training_set(pairs, width, height, seed, iterations=8, patch=7, dmax=No
         feats[2 * i] = pp.features(dl, dr, 0)[0]
         feats[2 * i + 1] = pp.features(dl, dr, 1)[0]
         res = pm.disparity_map(dl, dr, patch, dmax, iterations, pp=1, planes=True)
-        _check(L.pm_lpp_target4(_p(res["dmap"]), width, height, _p(target[2 * i]), st))
+        _check(L.pm_lpp_target(_p(res["dmap"]), width, height, scale, _p(target[2 * i]), st))
         _lib.check(L.pm_k_to_disparity(_p(dright), _p(res["planes_right"]), width, height, 1.0, 0, st))
-        _check(L.pm_lpp_target4(_p(dright), width, height, _p(target[2 * i + 1]), st))
+        _check(L.pm_lpp_target(_p(dright), width, height, scale, _p(target[2 * i + 1]), st))
     return feats, target

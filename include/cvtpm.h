@@ -370,11 +370,12 @@ int pm_k_svpm_prop(float* out, float* pout, const float* in, const float* pin, c
 int pm_k_svpm_to_flow(float* flow, const float* states, int W, int H, void* stream);
 
 /* ---- learned plane proposal (cvt_b200/csrc/pm_learn.cu) -----------------------------
- * A small BF16 CNN at a quarter of the image resolution whose output replaces the random
- * initialisation of disparityMap through its initdisp argument (pmhstereo_init_disparity_normal,
- * pmhstereo.cl:802-828): a 32-hypothesis cost volume of 4x4-block grey values, six 3x3
- * convolutions of 32 channels (ReLU after the first five), soft-argmin over the 32 logits plus
- * a fixed multiple of the cost volume, bilinear upsampling times 4.  Activations are NHWC BF16 (batch, rows, columns, 32); a layer's
+ * A small BF16 CNN at a quarter or half of the image resolution whose output replaces the
+ * random initialisation of disparityMap through its initdisp argument
+ * (pmhstereo_init_disparity_normal, pmhstereo.cl:802-828): a 32-hypothesis cost volume of
+ * block grey values, six 3x3 convolutions of 32 channels (ReLU after the first five),
+ * soft-argmin over the 32 logits plus a fixed multiple of the cost volume, bilinear upsampling
+ * to full resolution.  Activations are NHWC BF16 (batch, rows, columns, 32); a layer's
  * weights wmat[n][t][c] (output channel, tap t = (dy + 1) * 3 + (dx + 1), input channel), 32 * 288
  * BF16, and 32 FP32 biases.  The convolution runs on the tensor cores (tcgen05, FP32
  * accumulation) or, for checking, on the CUDA cores (tensor_cores = 0).  `err` (device int) is
@@ -382,12 +383,12 @@ int pm_k_svpm_to_flow(float* flow, const float* states, int W, int H, void* stre
  * message in pm_lpp_last_error().  All entry points enqueue on `stream`. */
 int pm_lpp_channels(void);
 const char* pm_lpp_last_error(void);
-/* cost-volume features of a pair (W, H >= 4; W4 = W / 4, H4 = H / 4) for the left view
- * (right_view 0: channel d compares left x with right x - step d) or the right view (1: right x
- * with left x + step d), hypotheses `step` (1..8) quarter pixels apart: grey_scratch 2 * W4 * H4
- * floats, out W4 * H4 * 32 BF16 */
+/* cost-volume features of a pair at 1 / scale of its resolution (scale 2 or 4; W4 = W / scale,
+ * H4 = H / scale, "feature pixels") for the left view (right_view 0: channel d compares left x
+ * with right x - step d) or the right view (1: right x with left x + step d), hypotheses `step`
+ * (1..8) feature pixels apart: grey_scratch 2 * W4 * H4 floats, out W4 * H4 * 32 BF16 */
 int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view, int step,
-                    float* grey_scratch, void* out, void* stream);
+                    int scale, float* grey_scratch, void* out, void* stream);
 /* one convolution over a batch of B activation maps; epi 0: + bias, ReLU, BF16 out; 1: + bias,
  * FP32 out (logits); 2: data gradient: times (mask > 0), BF16 out (wmat then holds the transposed,
  * mirrored weights wt[c][8 - t][n] = w[n][t][c]) */
@@ -399,25 +400,25 @@ int pm_lpp_conv(int epi, int tensor_cores, const void* in, const void* wmat, con
 size_t pm_lpp_wgrad_scratch_floats(int B, int H4, int W4, int per_block);
 int pm_lpp_wgrad(const void* x, const void* dy, float* scratch, float* grad, int B, int H4, int W4, int per_block, void* stream);
 /* soft-argmin of M x 32 logits plus skip times the features (the cost volume; NULL: none) into
- * disparities (quarter pixels; hypotheses `step` quarter pixels apart); with dlogits, also the smooth-L1 loss against target (< 0:
+ * disparities (feature pixels; hypotheses `step` feature pixels apart); with dlogits, also the smooth-L1 loss against target (< 0:
  * ignored), its gradient times inv_count (BF16) and per-256-pixel loss sums in loss_part */
 int pm_lpp_softargmin(const float* logits, const void* feats, float skip, float step, const float* target, float* disp,
                       void* dlogits, float* loss_part, int M, float inv_count, void* stream);
-/* training target: the mean of the positive disparities of each 4x4 block, in quarter pixels
- * (-1 where fewer than 8 of 16 are positive) */
-int pm_lpp_target4(const float* disp, int W, int H, float* out, void* stream);
-/* bilinear upsampling of a quarter-resolution disparity, times 4 */
-int pm_lpp_upsample(const float* d4, int W4, int H4, int W, int H, float* out, void* stream);
+/* training target: the mean of the positive disparities of each scale x scale block, in feature
+ * pixels (-1 where fewer than half are positive) */
+int pm_lpp_target(const float* disp, int W, int H, int scale, float* out, void* stream);
+/* bilinear upsampling of a 1 / scale resolution disparity, times scale */
+int pm_lpp_upsample(const float* d4, int W4, int H4, int W, int H, int scale, float* out, void* stream);
 /* one Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected for `step` >= 1) on n FP32 values */
 int pm_lpp_adam(float* p, const float* g, float* m1, float* m2, int n, float lr, int step, void* stream);
 /* BF16 copies of a layer's FP32 weights: wmat and the data-gradient matrix wt */
 int pm_lpp_weights_bf16(const float* p, void* wmat, void* wt, void* stream);
 /* the whole proposal for one pair: nlayers convolutions with weights wmats (nlayers * 32 * 288
  * BF16, 256-byte aligned) and biases (nlayers * 32), initdisp W * H floats (pixels) */
-size_t pm_lpp_propose_workspace_bytes(int W, int H);
-int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, int step, const uint8_t* left,
-                          const uint8_t* right, int W, int H, size_t stride, int right_view, float* initdisp, void* workspace,
-                          size_t ws_bytes, int* err, void* stream);
+size_t pm_lpp_propose_workspace_bytes(int W, int H, int scale);
+int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, int step, int scale,
+                          const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view,
+                          float* initdisp, void* workspace, size_t ws_bytes, int* err, void* stream);
 
 #ifdef __cplusplus
 }

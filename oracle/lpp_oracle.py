@@ -105,14 +105,14 @@ def backward(acts, layers, dlogits):
     return grads
 
 
-def features(left, right, view=0, step=1):
-    """grey of 4x4 blocks and the 32-hypothesis cost volume (BF16 values) of the left (view 0) or
-    right view (1), as k_grey4 / k_costvol"""
+def features(left, right, view=0, step=1, scale=4):
+    """grey of scale x scale blocks and the 32-hypothesis cost volume (BF16 values) of the left
+    (view 0) or right view (1), hypotheses `step` feature pixels apart, as k_grey / k_costvol"""
     def grey4(img):
-        H4, W4 = img.shape[0] // 4, img.shape[1] // 4
-        f = img[:4 * H4, :4 * W4, :3].astype(np.float32)
+        H4, W4 = img.shape[0] // scale, img.shape[1] // scale
+        f = img[:scale * H4, :scale * W4, :3].astype(np.float32)
         g = (f[..., 0] * np.float32(0.2126) + f[..., 1] * np.float32(0.7152) + f[..., 2] * np.float32(0.0722))
-        return g.reshape(H4, 4, W4, 4).sum((1, 3)) / np.float32(16 * 255)
+        return g.reshape(H4, scale, W4, scale).sum((1, 3)) / np.float32(scale * scale * 255)
     gl, gr = grey4(left).astype(np.float64), grey4(right).astype(np.float64)
     if view:
         gl, gr = gr, gl

@@ -239,12 +239,14 @@ def test_lpp_rejects_bad_arguments_without_touching_the_device(native):
     assert native.pm_lpp_conv(3, 1, None, None, None, None, None, 1, 4, 4, None, None) == _lib.PM_EINVAL_ARG
     assert native.pm_lpp_conv(0, 1, None, None, None, None, None, 1, 4, 4, None, None) == _lib.PM_EINVAL_ARG
     assert b"null" in native.pm_lpp_last_error()
-    assert native.pm_lpp_features(None, None, 3, 8, 16, 0, 1, None, None, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_lpp_features(None, None, 3, 8, 16, 0, 1, 4, None, None, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_lpp_features(None, None, 8, 8, 32, 0, 1, 3, None, None, None) == _lib.PM_EINVAL_ARG
     assert native.pm_lpp_softargmin(None, None, 4.0, 1.0, None, None, None, None, 0, 1.0, None) == _lib.PM_EINVAL_ARG
     assert native.pm_lpp_adam(None, None, None, None, 10, 1e-3, 0, None) == _lib.PM_EINVAL_ARG
-    assert native.pm_lpp_propose_workspace_bytes(2, 2) == 0
-    assert native.pm_lpp_propose_workspace_bytes(64, 48) > 16 * 12 * 32 * 2 * 3
-    assert native.pm_lpp_propose_device(None, None, 6, 4.0, 1, None, None, 64, 48, 256, 0, None, None, 0, None,
+    assert native.pm_lpp_propose_workspace_bytes(2, 2, 4) == 0
+    assert native.pm_lpp_propose_workspace_bytes(64, 48, 4) > 16 * 12 * 32 * 2 * 3
+    assert native.pm_lpp_propose_workspace_bytes(64, 48, 2) > 32 * 24 * 32 * 2 * 3
+    assert native.pm_lpp_propose_device(None, None, 6, 4.0, 1, 4, None, None, 64, 48, 256, 0, None, None, 0, None,
                                         None) == _lib.PM_EINVAL_ARG
     assert native.pm_lpp_wgrad_scratch_floats(1, 4, 4, 0) == 0
     assert native.pm_lpp_wgrad_scratch_floats(1, 4, 4, 8) == 2 * (32 * 288 + 32)

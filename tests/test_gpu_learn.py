@@ -120,11 +120,12 @@ def test_features_match_oracle(torch_cuda, native):
 
     L, R = scene.generate(3, 203, 121, 6, 2.0, 60.0)
     for view in (0, 1):
-        for step in (1, 2):
-            f = to_np(PlaneProposal(step=step).features(torch.from_numpy(L).cuda(), torch.from_numpy(R).cuda(), view))
-            want = O.features(L, R, view, step)
+        for step, scale in ((1, 4), (2, 4), (2, 2)):
+            f = to_np(PlaneProposal(step=step, scale=scale).features(torch.from_numpy(L).cuda(),
+                                                                     torch.from_numpy(R).cuda(), view))
+            want = O.features(L, R, view, step, scale)
             assert f.shape == want.shape
-            assert (np.abs(f - want) <= 2 ** -7 * np.abs(want) + 1e-6).all(), (view, step)
+            assert (np.abs(f - want) <= 2 ** -7 * np.abs(want) + 1e-6).all(), (view, step, scale)
 
 
 def test_training_gains_over_random_init(torch_cuda, native):
@@ -217,5 +218,5 @@ def test_one_call_proposal_equals_the_step_by_step_path(torch_cuda, native):
         assert native.pm_lpp_softargmin(logits.data_ptr(), f.data_ptr(), SKIP, float(pp.hstep), None, d4.data_ptr(),
                                         None, None, H4 * W4, 0.0, s) == 0
         up = torch.empty((93, 150), dtype=torch.float32, device="cuda")
-        assert native.pm_lpp_upsample(d4.data_ptr(), W4, H4, 150, 93, up.data_ptr(), s) == 0
+        assert native.pm_lpp_upsample(d4.data_ptr(), W4, H4, 150, 93, pp.scale, up.data_ptr(), s) == 0
         assert bits_equal(one, to_np(up)).all(), view
