@@ -278,7 +278,7 @@ int run_level(pm_handle* h, void* ws, const Layout& L, const uint8_t* left, cons
         nl += window_kernel_launches(F, false);
     }
     float theta = thetamin;
-    const int rof_launches = (o.rof_iters > 0 && o.rof_iters % 2 == 0) ? o.rof_iters : o.rof_iters + 1;
+    const int rof_launches = pd_launch_count(o.rof_iters);
     const float4 lam0 = make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);
     if (initdL) {   // :473-477
         launch_normal_depth(tmp, mL[0], W, H, 1.0f / dmax, 1, st);
@@ -405,7 +405,7 @@ int run_depth(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* right,
         nl += window_kernel_launches(F, false);
     }
     prof_mark(h, st, PM_PHASE_INIT, nl);
-    const int pd_launches = (o.rof_iters > 0 && o.rof_iters % 2 == 0) ? o.rof_iters : o.rof_iters + 1;
+    const int pd_launches = pd_launch_count(o.rof_iters);
     float theta = 1e-3f;   // :163
     int swap = 0;
     for (int iter = 0; iter < iterations; iter++) {

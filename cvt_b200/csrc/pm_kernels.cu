@@ -143,21 +143,12 @@ __global__ void k_normal_depth(float4* __restrict__ out, const float4* __restric
     out[i] = v;
 }
 
-// tensor-weighted, projected dual of PDDROFDiffTensor (PDDROFDiffTensor.cl:72-100) at
-// pixel (x, y); outside the image the tensor and the previous dual read as 0
+// tensor-weighted, projected dual of PDDROFDiffTensor (PDDROFDiffTensor.cl:72-100) from the
+// primal at the pixel (uc), right of it (ux) and below it (uy), the tensor D and the previous dual
 struct Dual { float4 lo, hi; };
 template <bool HUBER>
-__device__ __forceinline__ Dual rof_dual(const float4* __restrict__ u, const float4* __restrict__ p,
-                                         const float4* __restrict__ dt, int W, int H, int x, int y, bool first,
-                                         float eps)
+__device__ __forceinline__ Dual dual_step(float4 uc, float4 ux, float4 uy, float4 D, float4 plo, float4 phi, float eps)
 {
-    const int xc = min(max(x, 0), W - 1), yc = min(max(y, 0), H - 1);
-    const int xp = min(max(x + 1, 0), W - 1), yp = min(max(y + 1, 0), H - 1);
-    const float4 uc = u[(size_t)yc * W + xc], ux = u[(size_t)yc * W + xp], uy = u[(size_t)yp * W + xc];
-    const bool inside = x >= 0 && x < W && y >= 0 && y < H;
-    const float4 D = inside ? dt[(size_t)y * W + x] : f4(0, 0, 0, 0);
-    float4 plo = f4(0, 0, 0, 0), phi = f4(0, 0, 0, 0);
-    if (inside && !first) { plo = p[(size_t)y * 2 * W + 2 * x]; phi = p[(size_t)y * 2 * W + 2 * x + 1]; }
     const float dxv[4] = {uc.x - ux.x, uc.y - ux.y, uc.z - ux.z, uc.w - ux.w};
     const float dyv[4] = {uc.x - uy.x, uc.y - uy.y, uc.z - uy.z, uc.w - uy.w};
     const float pl[4] = {plo.x, plo.y, plo.z, plo.w}, ph[4] = {phi.x, phi.y, phi.z, phi.w};
@@ -187,8 +178,10 @@ __device__ __forceinline__ Dual rof_dual(const float4* __restrict__ u, const flo
     float l[4], h[4];
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-        a[c] = a[c] / pr[c];
-        b[c] = b[c] / pr[c];
+        if (pr[c] != 1.0f) {   // x / 1 is x: inside the unit ball the projection divides by 1
+            a[c] = a[c] / pr[c];
+            b[c] = b[c] / pr[c];
+        }
         l[c] = D.x * a[c] + D.z * b[c];
         h[c] = D.y * a[c] + D.w * b[c];
     }
@@ -196,6 +189,46 @@ __device__ __forceinline__ Dual rof_dual(const float4* __restrict__ u, const flo
     d.lo = f4(l[0], l[1], l[2], l[3]);
     d.hi = f4(h[0], h[1], h[2], h[3]);
     return d;
+}
+
+// the dual at pixel (x, y) from global fields; the primal is read clamped to the image,
+// outside it the tensor and the previous dual read as 0
+template <bool HUBER>
+__device__ __forceinline__ Dual rof_dual(const float4* __restrict__ u, const float4* __restrict__ p,
+                                         const float4* __restrict__ dt, int W, int H, int x, int y, bool first,
+                                         float eps)
+{
+    const int xc = min(max(x, 0), W - 1), yc = min(max(y, 0), H - 1);
+    const int xp = min(max(x + 1, 0), W - 1), yp = min(max(y + 1, 0), H - 1);
+    const float4 uc = u[(size_t)yc * W + xc], ux = u[(size_t)yc * W + xp], uy = u[(size_t)yp * W + xc];
+    const bool inside = x >= 0 && x < W && y >= 0 && y < H;
+    const float4 D = inside ? dt[(size_t)y * W + x] : f4(0, 0, 0, 0);
+    float4 plo = f4(0, 0, 0, 0), phi = f4(0, 0, 0, 0);
+    if (inside && !first) { plo = p[(size_t)y * 2 * W + 2 * x]; phi = p[(size_t)y * 2 * W + 2 * x + 1]; }
+    return dual_step<HUBER>(uc, ux, uy, D, plo, phi, eps);
+}
+
+// the primal and q updates of one step (PDDROFDiffTensor.cl:102-126) from the divergence of
+// the duals at the pixel (c), left of it (l) and above it (t)
+__device__ __forceinline__ void primal_step(float4 uu, float4 qq, float4 im, const Dual& c, const Dual& l,
+                                            const Dual& t, float4 lam, float4& uout, float4& qout)
+{
+    const float div[4] = {c.lo.x - l.lo.x + c.hi.x - t.hi.x, c.lo.y - l.lo.y + c.hi.y - t.hi.y,
+                          c.lo.z - l.lo.z + c.hi.z - t.hi.z, c.lo.w - l.lo.w + c.hi.w - t.hi.w};
+    const float imv[4] = {im.x, im.y, im.z, im.w}, qv[4] = {qq.x, qq.y, qq.z, qq.w}, uv[4] = {uu.x, uu.y, uu.z, uu.w};
+    const float lm[4] = {lam.x, lam.y, lam.z, lam.w};
+    float on[4], qn[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float o = (uv[k] + 0.05f * (lm[k] * imv[k] - div[k] - qv[k])) / (1.0f + 0.05f * lm[k]);   // TAU
+        o = o + 0.5f * (o - uv[k]);                                                               // THETA
+        float qn_ = (qv[k] + 8.0f * (o - imv[k])) / (1.0f + 4.0f * 8.0f / lm[k]);                 // ETA
+        qn_ = qn_ + 0.5f * (qn_ - qv[k]);
+        on[k] = o;
+        qn[k] = qn_;
+    }
+    uout = f4(on[0], on[1], on[2], on[3]);
+    qout = f4(qn[0], qn[1], qn[2], qn[3]);
 }
 
 constexpr int ROF_BX = 32, ROF_BY = 8;   // k_rof_step block; its duals need a one-pixel apron left and above
@@ -226,26 +259,88 @@ __global__ void __launch_bounds__(ROF_BX* ROF_BY) k_rof_step(float4* __restrict_
     const Dual l = sd[threadIdx.y + 1][threadIdx.x];
     const Dual t = sd[threadIdx.y][threadIdx.x + 1];
     const size_t i = (size_t)y * W + x;
-    const float4 im = img[i], uu = u[i];
-    const float4 qq = first ? f4(0, 0, 0, 0) : q[i];
-    const float div[4] = {c.lo.x - l.lo.x + c.hi.x - t.hi.x, c.lo.y - l.lo.y + c.hi.y - t.hi.y,
-                          c.lo.z - l.lo.z + c.hi.z - t.hi.z, c.lo.w - l.lo.w + c.hi.w - t.hi.w};
-    const float imv[4] = {im.x, im.y, im.z, im.w}, qv[4] = {qq.x, qq.y, qq.z, qq.w}, uv[4] = {uu.x, uu.y, uu.z, uu.w};
-    const float lm[4] = {lam.x, lam.y, lam.z, lam.w};
-    float on[4], qn[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        float o = (uv[k] + 0.05f * (lm[k] * imv[k] - div[k] - qv[k])) / (1.0f + 0.05f * lm[k]);   // TAU
-        o = o + 0.5f * (o - uv[k]);                                                               // THETA
-        float qn_ = (qv[k] + 8.0f * (o - imv[k])) / (1.0f + 4.0f * 8.0f / lm[k]);                 // ETA
-        qn_ = qn_ + 0.5f * (qn_ - qv[k]);
-        on[k] = o;
-        qn[k] = qn_;
-    }
-    unew[i] = f4(on[0], on[1], on[2], on[3]);
-    qnew[i] = f4(qn[0], qn[1], qn[2], qn[3]);
+    float4 un, qn;
+    primal_step(u[i], first ? f4(0, 0, 0, 0) : q[i], img[i], c, l, t, lam, un, qn);
+    unew[i] = un;
+    qnew[i] = qn;
     pnew[(size_t)y * 2 * W + 2 * x] = c.lo;
     pnew[(size_t)y * 2 * W + 2 * x + 1] = c.hi;
+}
+
+constexpr int RF_BX = 32, RF_BY = 16, RF_NT = 256;   // k_rof_step2: output tile and threads
+
+// two primal-dual steps in one launch (temporal blocking): the block computes the first
+// step's duals over its tile grown by two columns/rows left and above and one right and
+// below, the first step's primal over the tile grown by one on every side, and from those
+// the second step on its tile.  The fields cross DRAM once per two steps instead of twice;
+// every value is formed by the same operations as in k_rof_step, so the result is the same
+// bit for bit.  first: p = q = 0 before the first of the two steps.
+template <bool HUBER>
+__global__ void __launch_bounds__(RF_NT) k_rof_step2(float4* __restrict__ unew, float4* __restrict__ pnew,
+                                                   float4* __restrict__ qnew, const float4* __restrict__ u,
+                                                   const float4* __restrict__ p, const float4* __restrict__ q,
+                                                   const float4* __restrict__ img, const float4* __restrict__ dt,
+                                                   float4 lam, int W, int H, int first, float eps)
+{
+    // duals: first step over x0-2 .. x0+BX, y0-2 .. y0+BY; the second step overwrites the
+    // points x0-1 .. x0+BX-1, y0-1 .. y0+BY-1 in place (each point reads only its own first-step dual)
+    __shared__ float4 sdl[RF_BY + 3][RF_BX + 3], sdh[RF_BY + 3][RF_BX + 3];
+    __shared__ float4 su[RF_BY + 2][RF_BX + 2];   // first-step primal over x0-1 .. x0+BX, y0-1 .. y0+BY (in-image points)
+    __shared__ float4 sq[RF_BY][RF_BX];           // first-step q over the tile
+    const int x0 = blockIdx.x * RF_BX, y0 = blockIdx.y * RF_BY;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < (RF_BX + 3) * (RF_BY + 3); i += RF_NT) {
+        const int ex = i % (RF_BX + 3), ey = i / (RF_BX + 3);
+        const Dual d = rof_dual<HUBER>(u, p, dt, W, H, x0 - 2 + ex, y0 - 2 + ey, first, eps);
+        sdl[ey][ex] = d.lo;
+        sdh[ey][ex] = d.hi;
+    }
+    __syncthreads();
+    for (int i = tid; i < (RF_BX + 2) * (RF_BY + 2); i += RF_NT) {
+        const int ex = i % (RF_BX + 2), ey = i / (RF_BX + 2);
+        const int x = x0 - 1 + ex, y = y0 - 1 + ey;
+        if (x < 0 || x >= W || y < 0 || y >= H) continue;
+        const Dual c = {sdl[ey + 1][ex + 1], sdh[ey + 1][ex + 1]};
+        const Dual l = {sdl[ey + 1][ex], sdh[ey + 1][ex]};
+        const Dual t = {sdl[ey][ex + 1], sdh[ey][ex + 1]};
+        const size_t gi = (size_t)y * W + x;
+        float4 un, qn;
+        primal_step(u[gi], first ? f4(0, 0, 0, 0) : q[gi], img[gi], c, l, t, lam, un, qn);
+        su[ey][ex] = un;
+        if (ex >= 1 && ex <= RF_BX && ey >= 1 && ey <= RF_BY) sq[ey - 1][ex - 1] = qn;
+    }
+    __syncthreads();
+    // second-step duals; the clamped neighbours of a point of this range lie inside the image
+    // and inside su's range
+    for (int i = tid; i < (RF_BX + 1) * (RF_BY + 1); i += RF_NT) {
+        const int ex = i % (RF_BX + 1), ey = i / (RF_BX + 1);
+        const int x = x0 - 1 + ex, y = y0 - 1 + ey;
+        const int xc = min(max(x, 0), W - 1) - (x0 - 1), yc = min(max(y, 0), H - 1) - (y0 - 1);
+        const int xp = min(max(x + 1, 0), W - 1) - (x0 - 1), yp = min(max(y + 1, 0), H - 1) - (y0 - 1);
+        const bool inside = x >= 0 && x < W && y >= 0 && y < H;
+        const float4 D = inside ? dt[(size_t)y * W + x] : f4(0, 0, 0, 0);
+        const float4 plo = inside ? sdl[ey + 1][ex + 1] : f4(0, 0, 0, 0);
+        const float4 phi = inside ? sdh[ey + 1][ex + 1] : f4(0, 0, 0, 0);
+        const Dual d = dual_step<HUBER>(su[yc][xc], su[yc][xp], su[yp][xc], D, plo, phi, eps);
+        sdl[ey + 1][ex + 1] = d.lo;
+        sdh[ey + 1][ex + 1] = d.hi;
+    }
+    __syncthreads();
+    for (int i = tid; i < RF_BX * RF_BY; i += RF_NT) {
+        const int ex = i % RF_BX, ey = i / RF_BX;
+        const int x = x0 + ex, y = y0 + ey;
+        if (x >= W || y >= H) continue;
+        const Dual c = {sdl[ey + 2][ex + 2], sdh[ey + 2][ex + 2]};
+        const Dual l = {sdl[ey + 2][ex + 1], sdh[ey + 2][ex + 1]};
+        const Dual t = {sdl[ey + 1][ex + 2], sdh[ey + 1][ex + 2]};
+        const size_t gi = (size_t)y * W + x;
+        float4 un, qn;
+        primal_step(su[ey + 1][ex + 1], sq[ey][ex], img[gi], c, l, t, lam, un, qn);
+        unew[gi] = un;
+        qnew[gi] = qn;
+        pnew[(size_t)y * 2 * W + 2 * x] = c.lo;
+        pnew[(size_t)y * 2 * W + 2 * x + 1] = c.hi;
+    }
 }
 
 __global__ void k_consistency(float4* __restrict__ out, const float4* __restrict__ L, const float4* __restrict__ R,
@@ -604,20 +699,33 @@ void launch_pd(float4* out, const float4* input, const float4* dt, float4 lam, f
     float4* ut = static_cast<float4*>(scratch);
     float4* p[2] = {ut + N, ut + 3 * N};
     float4* q[2] = {ut + 5 * N, ut + 6 * N};
-    // PDOptCL.cpp:1137-1166: `iters` steps, plus one when the last left the result in the scratch image
+    // PDOptCL.cpp:1137-1166: `iters` steps, plus one when the last left the result in the scratch image;
+    // an odd count (iters = 0) starts with one single step, the rest run two per launch
     const int steps = (iters > 0 && iters % 2 == 0) ? iters : iters + 1;
-    // step k writes `out` when (steps - 1 - k) is even, so that the last step lands in `out`
-    const dim3 b(ROF_BX, ROF_BY), g = grid2d(W, H, b);
+    const int launches = pd_launch_count(iters);
+    const dim3 b1(ROF_BX, ROF_BY), g1 = grid2d(W, H, b1);
+    const dim3 b2(RF_NT), g2((W + RF_BX - 1) / RF_BX, (H + RF_BY - 1) / RF_BY);
+    // launch j writes `out` when (launches - 1 - j) is even, so that the last lands in `out`
     const float4* ucur = input;
-    for (int k = 0; k < steps; k++) {
-        float4* unew = ((steps - 1 - k) % 2 == 0) ? out : ut;
-        const int pi = k & 1;
-        k_rof_step<HUBER><<<g, b, 0, st>>>(unew, p[pi], q[pi], ucur, p[1 - pi], q[1 - pi], input, dt, lam, W, H,
-                                           k == 0, eps);
+    for (int j = 0; j < launches; j++) {
+        float4* unew = ((launches - 1 - j) % 2 == 0) ? out : ut;
+        const int pi = j & 1;
+        if (j == 0 && steps % 2)
+            k_rof_step<HUBER><<<g1, b1, 0, st>>>(unew, p[pi], q[pi], ucur, p[1 - pi], q[1 - pi], input, dt, lam, W, H,
+                                                 1, eps);
+        else
+            k_rof_step2<HUBER><<<g2, b2, 0, st>>>(unew, p[pi], q[pi], ucur, p[1 - pi], q[1 - pi], input, dt, lam, W,
+                                                  H, j == 0, eps);
         ucur = unew;
     }
 }
 }  // namespace
+
+int pd_launch_count(int iters)
+{
+    const int steps = (iters > 0 && iters % 2 == 0) ? iters : iters + 1;
+    return steps % 2 + steps / 2;
+}
 
 void launch_rof(float4* out, const float4* input, const float4* dt, float4 lam, int iters, int W, int H, void* scratch,
                 cudaStream_t st)

@@ -53,6 +53,8 @@ void launch_propagate(const PropParams& P, int fused, cudaStream_t st);
 inline int window_kernel_launches(int fused, bool counting) { return fused && !counting ? 2 : 1; }
 void launch_normal_depth(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st);
 size_t rof_scratch_bytes(int W, int H);
+// kernel launches of launch_rof / launch_huber for `iters` steps (two steps per launch)
+int pd_launch_count(int iters);
 void launch_huber(float4* out, const float4* input, const float4* dt, float4 lam, float eps, int iters, int W, int H,
                   void* scratch, cudaStream_t st);
 void launch_fill_state(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st);

@@ -460,6 +460,32 @@ def test_depth_kernels_match_reference_golden(D, case):
         assert bits_equal(host(o), g[k]).all(), k
 
 
+@pytest.mark.parametrize("W,H", [(1, 1), (3, 2), (31, 15), (33, 17), (65, 33), (97, 50)])
+def test_primal_dual_steps_ragged_sizes(D, orc, W, H):
+    """ROF and Huber smoothing (two steps per launch, one single step for an odd count) against
+    the oracle on image sizes that do not fill the launch tiles, for even and odd step counts,
+    on fields holding NaN and infinities"""
+    rng = np.random.default_rng(W * 131 + H)
+    inp = rng.standard_normal((H, W, 4)).astype(np.float32)
+    dt = rng.uniform(-1.0, 1.0, (H, W, 4)).astype(np.float32)
+    flat = inp.reshape(-1)
+    flat[rng.integers(0, flat.size, max(1, flat.size // 97))] = np.nan
+    flat[rng.integers(0, flat.size, max(1, flat.size // 89))] = np.inf
+    di, dd = dev(D.t, inp), dev(D.t, dt)
+    scratch = D.t.zeros(D.L.pm_rof_scratch_bytes(W, H), dtype=D.t.uint8, device="cuda")
+    lam = [1.7, 0.9, 2.3, 1.1]
+    lam_c = (C.c_float * 4)(*lam)
+    for iters in (0, 1, 2, 3, 8):
+        o = D.f4(H, W)
+        assert D.L.pm_k_rof(o.data_ptr(), di.data_ptr(), dd.data_ptr(), lam_c, iters, W, H, scratch.data_ptr(),
+                            stream(D.t)) == 0
+        assert bits_equal(host(o), orc.rof(inp, dt, lam, iters)).all(), ("rof", iters)
+        o = D.f4(H, W)
+        assert D.L.pm_k_huber(o.data_ptr(), di.data_ptr(), dd.data_ptr(), lam_c, 1e-4, iters, W, H,
+                              scratch.data_ptr(), stream(D.t)) == 0
+        assert bits_equal(host(o), orc.huber(inp, dt, lam, 1e-4, iters)).all(), ("huber", iters)
+
+
 @pytest.mark.parametrize("case", depth_cases())
 def test_depth_pipeline_strict_matches_reference_golden(native, torch_cuda, case):
     from cvt_b200 import PMHuberStereo
