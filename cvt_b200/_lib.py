@@ -11,6 +11,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcvtpm.so")
 
 PM_OK, PM_EINVAL_SHAPE, PM_EINVAL_ARG, PM_ENOMEM, PM_ECUDA, PM_ETIMEOUT, PM_ENOTIMPL, PM_ENODEV = range(8)
+PM_MAX_WIDTH, PM_MAX_HEIGHT, PM_MAX_RADIUS = 4096, 4096, 32   # the image and window limits of cvtpm.h
 PP_NONE, PP_LRCHECK, PP_LRCHECK_FILL = 0, 1, 2
 
 # every exported symbol of include/cvtpm.h

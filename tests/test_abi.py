@@ -39,6 +39,22 @@ def test_rejects_bad_shapes_without_touching_the_device(native):
     assert b"null" in native.pm_last_error(None)
 
 
+def test_size_limits_follow_the_header(native):
+    import os
+    import re
+
+    from cvt_b200 import _lib
+
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "cvtpm.h")).read()
+    for name in ("PM_MAX_WIDTH", "PM_MAX_HEIGHT", "PM_MAX_RADIUS"):
+        assert int(re.search(name + r"\s*=\s*(\d+)", hdr).group(1)) == getattr(_lib, name), name
+    W, r = _lib.PM_MAX_WIDTH, _lib.PM_MAX_RADIUS
+    # one past each limit is refused before any device work
+    assert native.pm_k_prep(None, W + 1, 4, 4 * (W + 1), 2, 1, None, None, None, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_k_prep(None, 4, _lib.PM_MAX_HEIGHT + 1, 16, 2, 1, None, None, None, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_k_prep(None, 4, 4, 16, r + 1, 1, None, None, None, None) == _lib.PM_EINVAL_SHAPE
+
+
 def test_create_fails_loudly_without_device(native):
     import torch
 

@@ -286,6 +286,41 @@ def test_pipeline_fused_matches_oracle(native, torch_cuda, orc, W, H, r, dmax, i
     assert pm.counters() == [int(v) for v in ctr], "window-sample counts equal the oracle's"
 
 
+@pytest.mark.parametrize("W,H,r,dmax,iters,seed", [(4096, 6, 10, 64.0, 2, 3), (72, 40, 32, 24.0, 2, 4),
+                                                    (5, 4096, 3, 4.0, 1, 5)])
+def test_maximum_width_height_and_radius_match_oracle(native, torch_cuda, orc, W, H, r, dmax, iters, seed):
+    """the largest accepted width (PM_MAX_WIDTH), height (PM_MAX_HEIGHT) and window radius
+    (PM_MAX_RADIUS), each on an image narrow in the other direction"""
+    from cvt_b200 import PMHuberStereo, _lib, scene
+
+    assert W == _lib.PM_MAX_WIDTH or H == _lib.PM_MAX_HEIGHT or r == _lib.PM_MAX_RADIUS
+    L, R = scene.generate(seed, W, H, 6, 1.0, dmax - 2.0)
+    o = orc.disparity_map(L, R, r, dmax, iters, pp=1, fused=1)
+    res = PMHuberStereo(fused=True).disparity_map(L, R, r, dmax, iters, pp=1, planes=True)
+    assert bits_equal(res["planes_left"], o["planesL"]).all()
+    assert bits_equal(res["planes_right"], o["planesR"]).all()
+    assert bits_equal(res["dmap"], o["dmap"]).all()
+
+
+def test_maximum_image_size_is_deterministic_and_accurate(native, torch_cuda):
+    """4096x4096 (the largest accepted image), 21x21, disparity 0-128, both views, LR check:
+    size-independent checks (two runs equal bit for bit; after 3 iterations more than half of
+    the kept pixels within 1 px of the scene's ground truth, 57% measured)"""
+    from cvt_b200 import PMHuberStereo, _lib, scene
+
+    torch = torch_cuda
+    W, H = _lib.PM_MAX_WIDTH, _lib.PM_MAX_HEIGHT
+    L, R, gt, _ = scene.generate(11, W, H, 60, 2.0, 120.0, with_gt=True)
+    pm = PMHuberStereo()
+    dL, dR = dev(torch, L), dev(torch, R)
+    a = host(pm.disparity_map(dL, dR, 10, 128.0, 3, pp=1))
+    b = host(pm.disparity_map(dL, dR, 10, 128.0, 3, pp=1))
+    assert bits_equal(a, b).all()
+    valid = a > 0
+    assert valid.mean() > 0.3, valid.mean()
+    assert (np.abs(a - gt)[valid] < 1.0).mean() > 0.5
+
+
 def test_device_entry_matches_host_entry(native, torch_cuda):
     from cvt_b200 import PMHuberStereo, scene
 
