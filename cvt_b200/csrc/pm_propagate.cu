@@ -66,6 +66,17 @@ __device__ __forceinline__ bool view_insert(unsigned long long* slot, unsigned i
     return false;
 }
 
+// A candidate whose plane (a, b, c) equals the current one bit for bit has the current
+// plane's smoothing distance d (smoothDistance reads no cost).  Evaluated without an early
+// exit it returns the current cost and is taken, which changes nothing; with an exit it
+// returns 1 and is taken only if 1 + theta d <= cost + theta d.  When that comparison fails,
+// the candidate leaves the state as it is whatever its window gives, and is not evaluated.
+__device__ __forceinline__ bool known_outcome(float4 nb, float4 self, float theta, float sd_self)
+{
+    return __float_as_uint(nb.x) == __float_as_uint(self.x) && __float_as_uint(nb.y) == __float_as_uint(self.y) &&
+           __float_as_uint(nb.z) == __float_as_uint(self.z) && !(1.0f + theta * sd_self <= self.w + theta * sd_self);
+}
+
 // pmhstereo_propagate_view (:927-1028): candidates k = 0 (the current plane, re-evaluated,
 // :939-940), 1 smooth (:968-976), 2-5 random neighbours with offsets drawn x first, in
 // [-4, 5] (:982-991), 6 a random plane (:996-1002), 7-8 cross-view planes (:1007-1016),
@@ -128,6 +139,7 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_CHAIN_BLOCKS) k_prop_chain(Pr
                 self.w = patch_eval<F, COUNT, CHK>(V, px, py, nb, 1e10f, cnt);
                 sd_self = smooth_dist1(self, smooth, cx, cy, dmax, lr);
             } else {
+                if (known_outcome(nb, self, theta, sd_self)) continue;
                 const float sd = smooth_dist1(nb, smooth, cx, cy, dmax, lr);
                 // minimalCost (:873-877)
                 const float mincost = self.w + theta * sd_self - theta * sd;
@@ -179,9 +191,11 @@ __global__ void __launch_bounds__(PROP_THREADS) k_prop_final(PropParams P)
         float4 self = P.tmp_self[idx];
         float4 nb = P.tmp_nb[idx];
         const float2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
-        const float mincost = self.w + theta * sd.y - theta * sd.x;
-        nb.w = patch_eval<F, COUNT, CHK>(V, px, py, nb, mincost, cnt);
-        if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
+        if (!known_outcome(nb, self, theta, sd.y)) {
+            const float mincost = self.w + theta * sd.y - theta * sd.x;
+            nb.w = patch_eval<F, COUNT, CHK>(V, px, py, nb, mincost, cnt);
+            if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
+        }
 
         if (P.vout_count) {
             const float sidesign = lr ? -1.0f : 1.0f;

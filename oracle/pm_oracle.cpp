@@ -428,15 +428,39 @@ inline float minimal_cost(F4 nb, F4 self, F4 smooth, float cx, float cy, float t
     return self.w + theta * sd.y - theta * sd.x;
 }
 
-/* the select at :976 / :990 / :1002 / :1015 / :1027 / :1052 */
+inline bool same_plane(F4 a, F4 b) { return memcmp(&a, &b, 3 * sizeof(float)) == 0; }
+
+/* candidates whose outcome was known without evaluating them, and those of them that
+ * changed the state all the same (must stay 0; see try_candidate) */
+int64_t g_known = 0, g_known_changed = 0;
+
+/* the select at :976 / :990 / :1002 / :1015 / :1027 / :1052.
+ * A candidate whose plane equals the current one bit for bit has the current plane's
+ * smoothing distance (smoothDistance reads no cost).  Evaluated without an early exit it
+ * returns the current cost and is taken, which changes nothing; with an exit it returns 1
+ * and is taken only if 1 + theta d <= cost + theta d.  When that comparison fails the
+ * outcome is known: the CUDA kernels skip the evaluation.  Here it is still evaluated, but
+ * its window samples are not counted (the counters are the work the kernels do), and a
+ * state change by such a candidate is recorded in g_known_changed. */
 inline void try_candidate(const Views& V, int fused, int px, int py, F4& self, F4 nb, F4 smooth,
                           float theta, float dmax, int lr, int64_t* cnt)
 {
     const float cx = (float)px, cy = (float)py;
     const float mincost = minimal_cost(nb, self, smooth, cx, cy, theta, dmax, lr);
-    nb.w = patch_eval(V, fused, px, py, nb, mincost, cnt);
+    const F2 sd0 = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
+    const bool known = same_plane(nb, self) && !(1.0f + theta * sd0.y <= self.w + theta * sd0.y);
+    const F4 before = self;
+    nb.w = patch_eval(V, fused, px, py, nb, mincost, known ? nullptr : cnt);
     const F2 sd = smooth_distance(nb, self, smooth, cx, cy, dmax, lr);
     if (nb.w + theta * sd.x <= self.w + theta * sd.y) self = nb;
+    if (known) {
+#pragma omp atomic
+        g_known++;
+        if (memcmp(&self, &before, sizeof(F4)) != 0) {
+#pragma omp atomic
+            g_known_changed++;
+        }
+    }
 }
 
 struct ScatterReq { int target; int src; F4 value; };
@@ -527,6 +551,7 @@ void add_counters(int64_t* dst, const int64_t* src) { if (dst) for (int i = 0; i
 extern "C" {
 
 int orc_version(void) { return 1; }
+void orc_known_counts(int64_t out[2]) { out[0] = g_known; out[1] = g_known_changed; }
 
 float orc_exp(float x) { return orc_expf(x); }
 float orc_log(float x) { return orc_logf(x); }

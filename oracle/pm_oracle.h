@@ -40,7 +40,9 @@ extern "C" {
 /* counters[0] = ASW cost window samples evaluated (passed the skip test)
  * counters[1] = Gauss-Newton window samples with the 3-point cost evaluated
  * counters[2] = patch_eval calls that entered the window loop
- * counters[3] = early exits taken                                        */
+ * counters[3] = early exits taken
+ * Evaluations of candidates whose plane equals the current plane and whose outcome is
+ * known are not counted: the CUDA kernels skip them (try_candidate in pm_oracle.cpp). */
 enum { ORC_NCOUNTERS = 4 };
 
 int orc_version(void);
@@ -93,6 +95,10 @@ int orc_disparity_to_normal(float* out, const float* disp, int W, int H);
 
 /* MWC64X seeded and skipped by linpos * nd, followed by `ndraws` RNG_float draws (RNG.cl:54-57, MWC64X.cl) */
 int orc_rng_floats(int64_t linpos, int nd, int ndraws, float* out);
+/* out[0]: candidates the CUDA kernels skip as known (plane equal to the current one, see
+ * try_candidate in pm_oracle.cpp) since the library was loaded; out[1]: those of them that
+ * changed the state when evaluated (must stay 0) */
+void orc_known_counts(int64_t out[2]);
 /* elementary functions, for tests */
 float orc_exp(float x);
 float orc_log(float x);

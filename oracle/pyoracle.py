@@ -375,6 +375,13 @@ class Oracle:
         return flow, states, duals
 
     # ---- helpers (restatement only) ------------------------------------------------
+    def known_counts(self):
+        """(candidates with a known outcome, skipped by the CUDA kernels; those of them that
+        changed the state when evaluated), since the library was loaded"""
+        out = np.zeros(2, np.int64)
+        self.L.orc_known_counts(out.ctypes.data_as(C.c_void_p))
+        return int(out[0]), int(out[1])
+
     def rng_floats(self, linpos, nd, n):
         out = np.zeros(n, np.float32)
         assert self.L.orc_rng_floats(linpos, nd, n, out.ctypes.data) == 0

@@ -302,3 +302,22 @@ def test_log_within_a_ulp(orc):
     assert err.max() <= 1.0, (err.max(), xs[err.argmax()])
     assert orc.L.orc_log(1.0) == 0.0 and np.isneginf(orc.L.orc_log(0.0)) and np.isnan(orc.L.orc_log(-1.0))
     assert np.isposinf(orc.L.orc_log(float("inf")))
+
+
+def test_known_candidates_leave_the_state_unchanged(orc):
+    """Candidates whose plane equals the current plane, with the current cost below the
+    early-exit value, are skipped by the CUDA kernels.  The restatement still evaluates them and
+    records any that changed the state: none may, on scenes that make many (converged planes
+    copied between neighbours), in both arithmetic modes and with the depth variant."""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(21, 160, 96, 5, 2.0, 30.0)
+    known0, changed0 = orc.known_counts()
+    for fused in (0, 1):
+        o = orc.disparity_map(L, R, 5, 32.0, 5, pp=1, fused=fused)
+        assert np.isfinite(o["dmap"]).all()
+    orc.depth_map(L, R, 5, 32.0, 4, fused=1)
+    known, changed = orc.known_counts()
+    assert known - known0 > 1000, known - known0
+    assert changed == changed0 == 0
+
