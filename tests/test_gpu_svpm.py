@@ -77,9 +77,11 @@ def test_svpm_flow_matches_reference_golden(torch_cuda, native, case):
 
 
 @pytest.mark.parametrize("W,H,r,passes,flowmax", [(1, 1, 1, 6, 6.0), (5, 3, 0, 6, 6.0), (17, 33, 2, 7, 6.0),
-                                                  (16, 16, 3, 5, 6.0), (130, 75, 3, 9, 24.0)])
+                                                  (16, 16, 3, 5, 6.0), (130, 75, 3, 9, 24.0), (4096, 2, 2, 3, 16.0),
+                                                  (3, 4096, 1, 3, 6.0), (20, 18, 32, 3, 6.0)])
 def test_svpm_matches_oracle_edge_sizes(torch_cuda, native, orc, W, H, r, passes, flowmax):
-    """a single pixel, r = 0, one past a 16x16 group, exactly one group, several groups"""
+    """a single pixel, r = 0, one past a 16x16 group, exactly one group, several groups, the
+    largest accepted width, height and window radius"""
     from cvt_b200 import scene
     from cvt_b200.svpm import SVPMFlowCL
 

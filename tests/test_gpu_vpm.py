@@ -110,10 +110,11 @@ def test_vpm_disparity_simple_matches_reference_golden(torch_cuda, native, case)
 
 
 @pytest.mark.parametrize("W,H,r,iters", [(1, 1, 2, 2), (2, 3, 0, 1), (3, 2, 1, 2), (37, 5, 4, 1), (33, 34, 2, 0),
-                                         (160, 96, 5, 3)])
+                                         (160, 96, 5, 3), (4096, 3, 3, 1), (4, 4096, 2, 1), (40, 24, 32, 1)])
 def test_vpm_matches_oracle_edge_sizes(torch_cuda, native, orc, W, H, r, iters):
     """a single pixel, images narrower than the Gauss-Newton taps' column range (singular
-    steps: NaN states whose costs are finite), r = 0, zero iterations, sizes off every tile"""
+    steps: NaN states whose costs are finite), r = 0, zero iterations, sizes off every tile,
+    the largest accepted width, height and window radius"""
     from cvt_b200 import scene
     from cvt_b200.vpm import VPMStereoCL
 
