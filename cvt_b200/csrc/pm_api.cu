@@ -329,13 +329,17 @@ int run_level(pm_handle* h, void* ws, const Layout& L, const uint8_t* left, cons
             launch_propagate(P, F, st);   // :542-543
         }
         prof_mark(h, st, PM_PHASE_PROPAGATE, 3 * window_kernel_launches(F, h->counting) * views);
-        launch_normal_depth(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :552-553
-        launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
-        if (views == 2) {
-            launch_normal_depth(tmp, mR[1 - swap], W, H, 1.0f / dmax, 0, st);   // :566-567
-            launch_rof(Rs, tmp, RDT, lam, o.rof_iters, W, H, rofs, st);
+        // the smoothing feeds the next iteration's propagation only: after the last one it is
+        // left out (every output is formed from the planes, :105-142)
+        if (iter + 1 < iterations) {
+            launch_normal_depth(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :552-553
+            launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
+            if (views == 2) {
+                launch_normal_depth(tmp, mR[1 - swap], W, H, 1.0f / dmax, 0, st);   // :566-567
+                launch_rof(Rs, tmp, RDT, lam, o.rof_iters, W, H, rofs, st);
+            }
+            prof_mark(h, st, PM_PHASE_SMOOTH, views * (1 + rof_launches));
         }
-        prof_mark(h, st, PM_PHASE_SMOOTH, views * (1 + rof_launches));
         theta = (float)iter / (float)iterations;   // :575-576
         theta = powf(theta, 4.0f) + thetamin;
         swap = 1 - swap;
@@ -445,13 +449,16 @@ int run_depth(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* right,
             launch_propagate(P, F, st);   // :268-269
         }
         prof_mark(h, st, PM_PHASE_PROPAGATE, 3 * window_kernel_launches(F, h->counting) * views);
-        launch_fill_state(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :273-274
-        launch_huber(Ls, tmp, LDT, lam, HUBEREPS, o.rof_iters, W, H, pds, st);
-        if (views == 2) {
-            launch_fill_state(tmp, mR[1 - swap], W, H, 1.0f / dmax, 0, st);   // :295-296
-            launch_huber(Rs, tmp, RDT, lam, HUBEREPS, o.rof_iters, W, H, pds, st);
+        // as in run_level, the smoothing after the last iteration feeds nothing (:326-345)
+        if (iter + 1 < iterations) {
+            launch_fill_state(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :273-274
+            launch_huber(Ls, tmp, LDT, lam, HUBEREPS, o.rof_iters, W, H, pds, st);
+            if (views == 2) {
+                launch_fill_state(tmp, mR[1 - swap], W, H, 1.0f / dmax, 0, st);   // :295-296
+                launch_huber(Rs, tmp, RDT, lam, HUBEREPS, o.rof_iters, W, H, pds, st);
+            }
+            prof_mark(h, st, PM_PHASE_SMOOTH, views * (1 + pd_launches));
         }
-        prof_mark(h, st, PM_PHASE_SMOOTH, views * (1 + pd_launches));
         if (iter >= 3) {   // :320-323
             theta = ((float)iter - 3.0f) / ((float)iterations - 4.0f);
             theta = theta * theta * theta + 1e-3f;
