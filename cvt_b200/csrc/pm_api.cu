@@ -1080,6 +1080,38 @@ int pm_depth_map(pm_handle* h, const uint8_t* left, const uint8_t* right, int W,
                       initdisp, initnormal, planes_left, planes_right);
 }
 
+// longest processing time first: pairs in decreasing window work W*H*(2r+1)^2 (stable), each
+// to the least loaded of nb branches (the lowest index among equals)
+static void batch_schedule(int n, int nb, const int* width, const int* height, const int* patchsize, int* order,
+                           int* owner)
+{
+    std::vector<double> work(n), load(nb, 0.0);
+    for (int i = 0; i < n; i++) {
+        order[i] = i;
+        work[i] = (double)width[i] * height[i] * (2.0 * patchsize[i] + 1.0) * (2.0 * patchsize[i] + 1.0);
+    }
+    std::stable_sort(order, order + n, [&](int a, int b) { return work[a] > work[b]; });
+    for (int k = 0; k < n; k++) {
+        const int i = order[k];
+        int best = 0;
+        for (int b = 1; b < nb; b++)
+            if (load[b] < load[best]) best = b;
+        owner[i] = best;
+        load[best] += work[i];
+    }
+}
+
+int pm_batch_schedule(int n, int branches, const int* width, const int* height, const int* patchsize, int* order,
+                      int* owner)
+{
+    if (n < 0 || n > PM_MAX_BATCH) return fail(nullptr, PM_EINVAL_ARG, "batch size out of range");
+    if (branches < 1 || branches > PM_BATCH_BRANCHES) return fail(nullptr, PM_EINVAL_ARG, "branch count out of range");
+    if (n == 0) return PM_OK;
+    if (!width || !height || !patchsize || !order || !owner) return fail(nullptr, PM_EINVAL_ARG, "null array");
+    batch_schedule(n, n < branches ? n : branches, width, height, patchsize, order, owner);
+    return PM_OK;
+}
+
 int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* left, const uint8_t* const* right,
                                   const int* width, const int* height, const size_t* stride, const int* patchsize,
                                   const float* dispmax, int iterations, int pp, float* const* dmap,
@@ -1118,19 +1150,7 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
         h->bev.push_back(e);
     }
     std::vector<int> order(n), owner(n);
-    std::vector<double> work(n), load(nb, 0.0);
-    for (int i = 0; i < n; i++) {
-        order[i] = i;
-        work[i] = (double)width[i] * height[i] * (2.0 * patchsize[i] + 1.0) * (2.0 * patchsize[i] + 1.0);
-    }
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
-    for (int i : order) {
-        int best = 0;
-        for (int b = 1; b < nb; b++)
-            if (load[b] < load[best]) best = b;
-        owner[i] = best;
-        load[best] += work[i];
-    }
+    batch_schedule(n, nb, width, height, patchsize, order.data(), owner.data());
     auto body = [&](cudaStream_t cs) -> int {
         PM_CUDA(h, cudaEventRecord(h->bev[nb], cs));
         for (int b = 0; b < nb; b++) PM_CUDA(h, cudaStreamWaitEvent(h->branch[b], h->bev[nb], 0));

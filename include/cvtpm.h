@@ -160,6 +160,11 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
 /* the number of concurrent branches of later batched calls on this handle, 1..PM_BATCH_BRANCHES
  * (0: PM_BATCH_BRANCHES); cvt_b200.autotune picks it by timing the caller's batch */
 int pm_set_batch_branches(pm_handle* h, int n);
+/* the schedule a batched call uses, host only: order[] = the pairs in decreasing window work
+ * W*H*(2r+1)^2 (stable), owner[i] = the branch of pair i (least loaded when the pair is
+ * placed, lowest index among equals) over min(n, branches) branches */
+int pm_batch_schedule(int n, int branches, const int* width, const int* height, const int* patchsize, int* order,
+                      int* owner);
 
 /* ---- per-kernel entry points (device pointers, enqueued on `stream`) ----------------
  * These expose each reference kernel on injected state for parity testing. */

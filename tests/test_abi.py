@@ -40,13 +40,10 @@ def test_rejects_bad_shapes_without_touching_the_device(native):
 
 
 def test_size_limits_follow_the_header(native):
-    import os
-    import re
-
     from cvt_b200 import _lib
 
-    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "cvtpm.h")).read()
-    for name in ("PM_MAX_WIDTH", "PM_MAX_HEIGHT", "PM_MAX_RADIUS"):
+    hdr = open(os.path.join(ROOT, "include", "cvtpm.h")).read()
+    for name in ("PM_MAX_WIDTH", "PM_MAX_HEIGHT", "PM_MAX_RADIUS", "PM_MAX_BATCH", "PM_BATCH_BRANCHES"):
         assert int(re.search(name + r"\s*=\s*(\d+)", hdr).group(1)) == getattr(_lib, name), name
     W, r = _lib.PM_MAX_WIDTH, _lib.PM_MAX_RADIUS
     # one past each limit is refused before any device work
@@ -152,6 +149,49 @@ def test_cpp_drop_in_header_compiles_and_fails_loudly(native, tmp_path):
     if not torch.cuda.is_available():
         p = subprocess.run([exe, str(tmp_path / "d.raw")], capture_output=True, text=True)
         assert p.returncode == 1 and "no CUDA device" in p.stderr
+
+
+def _lpt_schedule(sizes, branches):
+    """longest processing time first, as the batched entry documents it"""
+    work = [w * h * (2 * r + 1) ** 2 for w, h, r in sizes]
+    order = sorted(range(len(sizes)), key=lambda i: -work[i])   # sorted() is stable
+    nb = min(len(sizes), branches)
+    load, owner = [0] * nb, [0] * len(sizes)
+    for i in order:
+        b = min(range(nb), key=lambda k: (load[k], k))
+        owner[i] = b
+        load[b] += work[i]
+    return order, owner, load
+
+
+def test_batch_schedule_is_longest_first_onto_least_loaded(native):
+    """the schedule of pm_disparity_map_batch_device, computed on the host: the 64-pair
+    workload, ties in work (equal sizes keep their order), fewer pairs than branches"""
+    from cvt_b200 import _lib, scene
+
+    specs = scene.batch_specs()
+    cases = [([(s["width"], s["height"], 10) for s in specs], b) for b in (1, 4, 16)]
+    cases.append(([(64, 48, 2), (320, 240, 7), (64, 48, 2), (320, 240, 7), (96, 16, 32)], 3))
+    cases.append(([(5, 5, 1), (7, 3, 0)], 16))
+    for sizes, branches in cases:
+        n = len(sizes)
+        W = np.array([s[0] for s in sizes], np.int32)
+        H = np.array([s[1] for s in sizes], np.int32)
+        R = np.array([s[2] for s in sizes], np.int32)
+        order, owner = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        assert native.pm_batch_schedule(n, branches, W.ctypes.data, H.ctypes.data, R.ctypes.data, order.ctypes.data,
+                                        owner.ctypes.data) == _lib.PM_OK
+        want_order, want_owner, load = _lpt_schedule(sizes, branches)
+        assert order.tolist() == want_order and owner.tolist() == want_owner
+        assert len(load) == min(n, branches) and sorted(set(owner.tolist())) == list(range(len(load)))
+    x = np.zeros(4, np.int32)
+    assert native.pm_batch_schedule(2, 0, x.ctypes.data, x.ctypes.data, x.ctypes.data, x.ctypes.data,
+                                    x.ctypes.data) == _lib.PM_EINVAL_ARG
+    assert native.pm_batch_schedule(2, _lib.PM_BATCH_BRANCHES + 1, x.ctypes.data, x.ctypes.data, x.ctypes.data,
+                                    x.ctypes.data, x.ctypes.data) == _lib.PM_EINVAL_ARG
+    assert native.pm_batch_schedule(2, 4, None, x.ctypes.data, x.ctypes.data, x.ctypes.data,
+                                    x.ctypes.data) == _lib.PM_EINVAL_ARG
+    assert native.pm_batch_schedule(0, 4, None, None, None, None, None) == _lib.PM_OK
 
 
 def test_batch_specs_seeded_and_in_range():
