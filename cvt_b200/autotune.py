@@ -10,24 +10,30 @@ other setting (every pair's arithmetic is the same), only the time differs.
 import statistics
 
 
-def tune_batch(pm, lefts, rights, patchsizes, disparitymaxs, iterations=1, candidates=(2, 4, 8, 16), reps=2, pp=1):
-    """Returns {"branches": best, "ms": {candidate: median ms}} and leaves `best` set on pm."""
+def cuda_event_ms(fn):
+    """milliseconds of one call of fn between CUDA events on the current stream"""
     import torch
+
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def tune_batch(pm, lefts, rights, patchsizes, disparitymaxs, iterations=1, candidates=(2, 4, 8, 16), reps=2, pp=1,
+               timer=cuda_event_ms):
+    """Returns {"branches": best, "ms": {candidate: median ms}} and leaves `best` set on pm.
+    Each candidate's first call (graph capture) is not timed; ties go to the earlier candidate."""
+    def run():
+        pm.disparity_map_batch(lefts, rights, patchsizes, disparitymaxs, iterations, pp=pp)
 
     timings = {}
     for nb in candidates:
         pm.set_batch_branches(nb)
-        pm.disparity_map_batch(lefts, rights, patchsizes, disparitymaxs, iterations, pp=pp)   # capture, warm
-        torch.cuda.synchronize()
-        ms = []
-        for _ in range(reps):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            pm.disparity_map_batch(lefts, rights, patchsizes, disparitymaxs, iterations, pp=pp)
-            b.record()
-            torch.cuda.synchronize()
-            ms.append(a.elapsed_time(b))
-        timings[nb] = statistics.median(ms)
+        timer(run)   # capture, warm
+        timings[nb] = statistics.median(timer(run) for _ in range(reps))
     best = min(timings, key=timings.get)
     pm.set_batch_branches(best)
     return {"branches": best, "ms": timings}

@@ -306,3 +306,34 @@ def test_lpp_rejects_bad_arguments_without_touching_the_device(native):
                                         None) == _lib.PM_EINVAL_ARG
     assert native.pm_lpp_wgrad_scratch_floats(1, 4, 4, 0) == 0
     assert native.pm_lpp_wgrad_scratch_floats(1, 4, 4, 8) == 2 * (32 * 288 + 32)
+
+
+def test_autotuner_keeps_the_fastest_branch_count():
+    """tune_batch with a stand-in handle and timer: every candidate is set, warmed once and
+    timed `reps` times; the fastest stays set; ties go to the earlier candidate"""
+    from cvt_b200.autotune import tune_batch
+
+    class FakeHandle:
+        def __init__(self):
+            self.branches, self.calls, self.set_log = 0, [], []
+
+        def set_batch_branches(self, n):
+            self.branches = n
+            self.set_log.append(n)
+
+        def disparity_map_batch(self, lefts, rights, patchsizes, dmaxs, iterations, pp=1):
+            self.calls.append((self.branches, iterations, pp))
+
+    for cost, want in (({2: 50.0, 4: 30.0, 8: 20.0, 16: 25.0}, 8), ({2: 9.0, 4: 9.0, 8: 12.0, 16: 9.0}, 2)):
+        pm = FakeHandle()
+
+        def timer(fn):
+            fn()
+            return cost[pm.branches]
+
+        res = tune_batch(pm, [], [], [], [], iterations=1, reps=3, timer=timer)
+        assert res["branches"] == want and pm.branches == want
+        assert res["ms"] == cost
+        assert pm.set_log == [2, 4, 8, 16, want]
+        assert [c[0] for c in pm.calls] == [b for b in (2, 4, 8, 16) for _ in range(4)]
+
