@@ -80,6 +80,35 @@ def test_tiny_images_match_reference(orc, ref, W, H, r):
     assert bits_equal(a["normal"], b["normal"]).all()
 
 
+def _sweep_cases(n=8, seed=2024):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        W, H, r, it = int(rng.integers(9, 33)), int(rng.integers(5, 21)), int(rng.integers(0, 5)), int(rng.integers(1, 4))
+        views = int(rng.choice([1, 2]))
+        pp = 0 if views == 1 else int(rng.choice([0, 1, 2]))
+        out.append((W, H, r, it, views, pp, float(rng.uniform(3, 12)), bool(rng.integers(0, 2))))
+    return out
+
+
+@pytest.mark.parametrize("W,H,r,it,views,pp,dmax,init", _sweep_cases())
+def test_restatement_matches_reference_parameter_sweep(orc, ref, W, H, r, it, views, pp, dmax, init):
+    """Seeded draws of size, window radius (0 included), iterations, views, post-processing and
+    disparity range; half start from a given disparity whose negative entries take the random
+    start per pixel (pmhstereo_init_disparity_normal).  Every stage equal bit for bit."""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(W * 31 + H, W, H, 3, 0.5, dmax - 1.0)
+    idisp = np.random.default_rng(W + H).uniform(-1.0, dmax, (H, W)).astype(np.float32) if init else None
+    a = orc.disparity_map(L, R, r, dmax, it, pp=pp, views=views, initdisp=idisp, dump=True)
+    b = ref.disparity_map(L, R, r, dmax, it, pp=pp, views=views, initdisp=idisp, dump=True)
+    assert a["stages"].keys() == b["stages"].keys()
+    for k in a["stages"]:
+        assert bits_equal(a["stages"][k], b["stages"][k]).all(), k
+    for k in ("dmap", "normal", "planesL"):
+        assert bits_equal(a[k], b[k]).all(), k
+
+
 def _mwc_step(x, c):
     A = 4294883355
     xn = (A * x + c) & 0xffffffff
