@@ -109,6 +109,76 @@ def test_restatement_matches_reference_parameter_sweep(orc, ref, W, H, r, it, vi
         assert bits_equal(a[k], b[k]).all(), k
 
 
+def _sibling_cases(seed=77):
+    rng = np.random.default_rng(seed)
+    vpm = [(int(rng.integers(9, 41)), int(rng.integers(5, 25)), int(rng.integers(0, 6)), int(rng.integers(0, 4)),
+            float(rng.uniform(3, 16)), bool(rng.integers(0, 2))) for _ in range(6)]
+    svpm = [(int(rng.integers(5, 40)), int(rng.integers(5, 40)), int(rng.integers(0, 5)), int(rng.integers(1, 9)),
+             float(rng.uniform(2, 12))) for _ in range(6)]
+    depth = []
+    for i in range(4):
+        views = 1 + i % 2
+        depth.append((int(rng.integers(9, 33)), int(rng.integers(5, 21)), int(rng.integers(0, 4)), int(rng.integers(1, 4)),
+                      float(rng.uniform(3, 12)), views, 0 if views == 1 else int(rng.choice([0, 1, 2])),
+                      float(rng.choice([-1.0, 0.5]))))
+    return vpm, svpm, depth
+
+
+_VPM_SWEEP, _SVPM_SWEEP, _DEPTH_SWEEP = _sibling_cases()
+
+
+@pytest.mark.parametrize("W,H,r,it,dmax,init", _VPM_SWEEP)
+def test_vpm_restatement_matches_reference_parameter_sweep(orc, ref, W, H, r, it, dmax, init):
+    """VPMStereoCL::disparitySimple over seeded sizes, radius 0-5, 0-3 iterations and disparity
+    ranges; half start from a given disparity with entries outside [0, dmax)"""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(W * 13 + H, W, H, 3, 0.5, min(dmax - 1.0, 8.0))
+    idisp = np.random.default_rng(W * H).uniform(-1.0, dmax + 1.0, (H, W)).astype(np.float32) if init else None
+    a = orc.vpm_disparity_simple(L, R, r, it, dmax, idisp)
+    b = ref.vpm_disparity_simple(L, R, r, it, dmax, idisp)
+    assert bits_equal(a[0], b[0]).all() and bits_equal(a[1], b[1]).all()
+
+
+@pytest.mark.parametrize("W,H,r,passes,flowmax", _SVPM_SWEEP)
+def test_svpm_restatement_matches_reference_parameter_sweep(orc, ref, W, H, r, passes, flowmax):
+    """SVPMFlowCL::flow over seeded sizes (below, at and past one 16x16 group), radius 0-4,
+    1-8 passes and flow ranges"""
+    from cvt_b200 import scene
+
+    a1, a2 = scene.generate(W * 17 + H, W, H, 3, 0.5, 4.0)
+    for x, y in zip(orc.svpm_flow(a1, a2, r, flowmax, passes), ref.svpm_flow(a1, a2, r, flowmax, passes)):
+        assert bits_equal(x, y).all()
+
+
+@pytest.mark.parametrize("W,H,r,it,dmax,views,pp,dscale", _DEPTH_SWEEP)
+def test_depth_restatement_matches_reference_parameter_sweep(orc, ref, W, H, r, it, dmax, views, pp, dscale):
+    """PMHuberStereo::depthMap over seeded sizes, radius 0-3, iterations, views, post-processing
+    and the output scale (1 / dmax by default, or given); every stage equal bit for bit"""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(W * 7 + H, W, H, 3, 0.5, dmax - 1.0)
+    a = orc.depth_map(L, R, r, dmax, it, dscale=dscale, pp=pp, views=views, dump=True)
+    b = ref.depth_map(L, R, r, dmax, it, dscale=dscale, pp=pp, views=views, dump=True)
+    assert a["stages"].keys() == b["stages"].keys()
+    for k in a["stages"]:
+        assert bits_equal(a["stages"][k], b["stages"][k]).all(), k
+    assert bits_equal(a["dmap"], b["dmap"]).all()
+
+
+@pytest.mark.parametrize("W,H,r,it,levels", [(24, 20, 1, 1, 3), (30, 18, 2, 1, 2)])
+def test_pyramid_restatement_matches_reference_parameter_sweep(orc, ref, W, H, r, it, levels):
+    """the coarse-to-fine loop at sizes whose levels round down unevenly"""
+    from cvt_b200 import scene
+
+    L, R = scene.generate(W * 5 + H, W, H, 3, 0.5, 8.0)
+    a = orc.disparity_map(L, R, r, 10.0, it, pp=1, levels=levels, dump=True)
+    b = ref.disparity_map(L, R, r, 10.0, it, pp=1, levels=levels, dump=True)
+    for k in a["stages"]:
+        assert bits_equal(a["stages"][k], b["stages"][k]).all(), k
+    assert bits_equal(a["dmap"], b["dmap"]).all()
+
+
 def _mwc_step(x, c):
     A = 4294883355
     xn = (A * x + c) & 0xffffffff
