@@ -81,3 +81,41 @@ def test_cvtraw_padded_stride_loads(io, tmp_path):
     p = tmp_path / "pad.cvtraw"
     p.write_bytes(struct.pack("<4I", 6, 4, 32, 4) + padded.tobytes())
     assert (io.load_cvtraw(p) == a).all()
+
+
+def test_round_trips_of_random_shapes_and_values(io, tmp_path):
+    """Hypothesis draws shapes (1x1 upwards, odd sizes) and values (NaN, infinities, signed
+    zeros and subnormals included): CVTRaw keeps every bit of every format; PFM keeps every bit
+    of its float channels (alpha reads back as 1)."""
+    from hypothesis import HealthCheck, given, settings
+    from hypothesis import strategies as st
+
+    floats = st.floats(width=32, allow_nan=True, allow_infinity=True, allow_subnormal=True)
+
+    @settings(max_examples=60, deadline=None, suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(h=st.integers(1, 9), w=st.integers(1, 11), kind=st.sampled_from(["gray", "rgba8", "rgbaf", "flow"]),
+           data=st.data())
+    def check(h, w, kind, data):
+        ch = {"gray": 1, "rgba8": 4, "rgbaf": 4, "flow": 2}[kind]
+        n = h * w * ch
+        if kind == "rgba8":
+            vals = data.draw(st.lists(st.integers(0, 255), min_size=n, max_size=n))
+            a = np.array(vals, np.uint8)
+        else:
+            a = np.array(data.draw(st.lists(floats, min_size=n, max_size=n)), np.float32)
+        a = a.reshape((h, w) if ch == 1 else (h, w, ch))
+        p = tmp_path / "r.cvtraw"
+        io.save_cvtraw(p, a)
+        b = io.load_cvtraw(p)
+        assert b.shape == a.shape and (b.view(np.uint8) == a.view(np.uint8)).all()
+        if kind in ("gray", "rgbaf"):
+            q = tmp_path / "r.pfm"
+            io.save_pfm(q, a)
+            c = io.load_pfm(q)
+            got = c if kind == "gray" else c[..., :3]
+            want = a if kind == "gray" else a[..., :3]
+            assert (got.view(np.uint32) == want.view(np.uint32)).all()
+            if kind == "rgbaf":
+                assert (c[..., 3] == 1.0).all()
+
+    check()
