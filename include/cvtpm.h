@@ -50,7 +50,7 @@ enum {
 enum { PM_PP_NONE = 0, PM_PP_LRCHECK = 1, PM_PP_LRCHECK_FILL = 2 };
 
 /* limits: images up to 4096 columns (window coordinates stay exact in FP32
- * products), window half-width 1..32 */
+ * products), window half-width 0..32 */
 enum { PM_MAX_WIDTH = 4096, PM_MAX_HEIGHT = 4096, PM_MAX_RADIUS = 32 };
 
 typedef struct pm_options {

@@ -52,6 +52,28 @@ def test_size_limits_follow_the_header(native):
     assert native.pm_k_prep(None, 4, 4, 16, r + 1, 1, None, None, None, None) == _lib.PM_EINVAL_SHAPE
 
 
+def test_option_defaults_are_the_reference_constants(native):
+    """pm_options_default: both views (disparityMapAll), thetamin 1e-4 (PMHuberStereo.cpp:92),
+    LR check at 1 px and 5 degrees (:79-80), 40 ROF steps (PDOPTITER), one pyramid level (:78);
+    the structure's layout matches the header's; every status has a name"""
+    from cvt_b200 import _lib
+
+    o = _lib.Options()
+    assert native.pm_options_default(C.byref(o)) == _lib.PM_OK
+    assert (o.views, o.fused, o.rof_iters, o.device, o.use_graph, o.levels) == (2, 1, 40, 0, 1, 1)
+    assert np.float32(o.thetamin) == np.float32(1e-4)
+    assert (o.maxdispdiff, o.maxanglediff) == (1.0, 5.0)
+    assert native.pm_options_default(None) == _lib.PM_EINVAL_ARG
+    hdr = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "cvtpm.h")).read(), flags=re.S)
+    body = re.search(r"typedef struct\s*(?:pm_options)?\s*\{([^}]*)\}\s*pm_options;", hdr).group(1)
+    fields = re.findall(r"(int|float)\s+(\w+);", body)
+    assert [(n, {"int": C.c_int, "float": C.c_float}[t]) for t, n in fields] == list(_lib.Options._fields_)
+    native.pm_status_string.restype = C.c_char_p
+    names = [native.pm_status_string(s) for s in range(8)]
+    assert len(set(names)) == 8 and all(n and n != b"unknown status" for n in names)
+    assert native.pm_status_string(99) == b"unknown status"
+
+
 def test_create_fails_loudly_without_device(native):
     import torch
 
