@@ -6,18 +6,22 @@ import os
 import subprocess
 import sys
 
+import pytest
+
 from conftest import ROOT
 
 
-def _run(env_extra):
+def _run(env_extra, mode="disparity"):
     env = dict(os.environ, **env_extra)
     return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--config", "small",
-                           "--steps", "1", "--warmup", "0"], capture_output=True, text=True, env=env, cwd=ROOT,
-                          timeout=600)
+                           "--mode", mode, "--steps", "1", "--warmup", "0"], capture_output=True, text=True, env=env,
+                          cwd=ROOT, timeout=600)
 
 
-def test_reference_arm_prints_one_contract_line(orc):
-    p = _run({})
+@pytest.mark.parametrize("mode,metric", [("disparity", "Mpixel·iterations/s"), ("depth", "Mpixel·iterations/s"),
+                                         ("vpm", "Mpixel·iterations/s"), ("svpm", "Mpixel·passes/s")])
+def test_reference_arm_prints_one_contract_line(orc, mode, metric):
+    p = _run({}, mode)
     assert p.returncode == 0, p.stderr[-2000:]
     lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
@@ -26,7 +30,7 @@ def test_reference_arm_prints_one_contract_line(orc):
         assert d["impl"] == "reference"
         return
     assert d["impl"] == "reference"
-    assert d["metric"] == "Mpixel·iterations/s" and d["unit"] == d["metric"] and d["higher_is_better"] is True
+    assert d["metric"] == metric and d["unit"] == d["metric"] and d["higher_is_better"] is True
     assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 0 and d["n_gpus"] == 1
     assert d["config"]["workload"] == "small"
     cb = d["cpu_baseline"]
