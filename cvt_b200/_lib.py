@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(_HERE, "libcvtpm.so")
 
 PM_OK, PM_EINVAL_SHAPE, PM_EINVAL_ARG, PM_ENOMEM, PM_ECUDA, PM_ETIMEOUT, PM_ENOTIMPL, PM_ENODEV = range(8)
 PM_MAX_WIDTH, PM_MAX_HEIGHT, PM_MAX_RADIUS = 4096, 4096, 32   # the image and window limits of cvtpm.h
-PM_MAX_BATCH, PM_BATCH_BRANCHES = 4096, 16   # the batch limits of cvtpm.h
+PM_MAX_BATCH, PM_BATCH_BRANCHES, PM_MAX_RANKS = 4096, 16, 1024   # the batch limits of cvtpm.h
 PP_NONE, PP_LRCHECK, PP_LRCHECK_FILL = 0, 1, 2
 
 # every exported symbol of include/cvtpm.h
@@ -21,6 +21,7 @@ SYMBOLS = [
     "pm_disparity_map", "pm_disparity_map_device", "pm_depth_map", "pm_depth_map_device", "pm_set_counting", "pm_get_counters",
     "pm_set_profiling", "pm_get_phase_times", "pm_measure_fp32_peak",
     "pm_disparity_map_batch_device", "pm_disparity_map_init2_device", "pm_set_batch_branches", "pm_batch_schedule",
+    "pm_batch_partition",
     "pm_k_prep", "pm_k_init", "pm_k_cost", "pm_k_klt", "pm_k_propagate", "pm_k_normal_depth",
     "pm_rof_scratch_bytes", "pm_k_rof", "pm_k_rof_static", "pm_k_consistency", "pm_k_to_disparity", "pm_k_fill_depthmap",
     "pm_k_fill_normalmap", "pm_k_disparity_to_normal", "pm_k_pyrdown", "pm_k_pyrup_mul", "pm_pyramid_size",
@@ -33,9 +34,9 @@ SYMBOLS = [
     "pm_k_vpm_grad", "pm_k_vpm_init", "pm_k_vpm_iter", "pm_k_vpm_disparity",
     "pm_svpm_create", "pm_svpm_destroy", "pm_svpm_last_error", "pm_svpm_flow", "pm_svpm_flow_device",
     "pm_svpm_set_counting", "pm_svpm_get_counters", "pm_k_svpm_init", "pm_k_svpm_prop", "pm_k_svpm_to_flow",
-    "pm_lpp_channels", "pm_lpp_last_error", "pm_lpp_features", "pm_lpp_conv", "pm_lpp_wgrad_scratch_floats",
-    "pm_lpp_wgrad", "pm_lpp_softargmin", "pm_lpp_target", "pm_lpp_upsample", "pm_lpp_adam", "pm_lpp_weights_bf16",
-    "pm_lpp_propose_workspace_bytes", "pm_lpp_propose_device",
+    "pm_lpp_last_error", "pm_lpp_layers", "pm_lpp_layer_shape", "pm_lpp_param_count", "pm_lpp_input", "pm_lpp_conv",
+    "pm_lpp_wgrad_scratch_floats", "pm_lpp_wgrad", "pm_lpp_target", "pm_lpp_loss", "pm_lpp_upsample", "pm_lpp_adam",
+    "pm_lpp_weights_bf16", "pm_lpp_propose_workspace_bytes", "pm_lpp_propose_device",
 ]
 
 
@@ -83,6 +84,7 @@ def lib():
         "pm_set_counting": (i32, [vp, i32]),
         "pm_set_batch_branches": (i32, [vp, i32]),
         "pm_batch_schedule": (i32, [i32, i32, vp, vp, vp, vp, vp]),
+        "pm_batch_partition": (i32, [i32, i32, vp, vp, vp, vp, vp, vp]),
         "pm_get_counters": (i32, [vp, C.POINTER(C.c_uint64)]),
         "pm_set_profiling": (i32, [vp, i32]),
         "pm_get_phase_times": (i32, [vp, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
@@ -144,21 +146,23 @@ def lib():
         "pm_k_svpm_init": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, vp]),
         "pm_k_svpm_prop": (i32, [vp, vp, vp, vp, vp, vp, i32, i32, sz, i32, f32, i32, vp]),
         "pm_k_svpm_to_flow": (i32, [vp, vp, i32, i32, vp]),
-        "pm_lpp_channels": (i32, []),
         "pm_lpp_last_error": (C.c_char_p, []),
-        "pm_lpp_features": (i32, [vp, vp, i32, i32, sz, i32, i32, i32, vp, vp, vp]),
-        "pm_lpp_conv": (i32, [i32, i32, vp, vp, vp, vp, vp, i32, i32, i32, vp, vp]),
+        "pm_lpp_layers": (i32, []),
+        "pm_lpp_layer_shape": (i32, [i32, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "pm_lpp_param_count": (sz, []),
+        "pm_lpp_input": (i32, [vp, vp, i32, i32, sz, i32, i32, vp, vp]),
+        "pm_lpp_conv": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, i32, i32, i32, vp, vp]),
         "pm_lpp_wgrad_scratch_floats": (sz, [i32, i32, i32, i32]),
-        "pm_lpp_wgrad": (i32, [vp, vp, vp, vp, i32, i32, i32, i32, vp]),
-        "pm_lpp_softargmin": (i32, [vp, vp, f32, f32, vp, vp, vp, vp, i32, f32, vp]),
-        "pm_lpp_target": (i32, [vp, i32, i32, i32, vp, vp]),
-        "pm_lpp_upsample": (i32, [vp, i32, i32, i32, i32, i32, vp, vp]),
+        "pm_lpp_wgrad": (i32, [i32, i32, vp, vp, vp, vp, i32, i32, i32, vp, vp]),
+        "pm_lpp_target": (i32, [vp, vp, i32, i32, i32, i32, f32, vp, vp]),
+        "pm_lpp_loss": (i32, [vp, vp, f32, f32, i32, vp, vp, vp]),
+        "pm_lpp_upsample": (i32, [vp, i32, i32, i32, i32, i32, i32, f32, vp, vp, vp]),
         "pm_lpp_adam": (i32, [vp, vp, vp, vp, i32, f32, i32, vp]),
-        "pm_lpp_weights_bf16": (i32, [vp, vp, vp, vp]),
+        "pm_lpp_weights_bf16": (i32, [i32, vp, vp, vp, vp]),
         "pm_lpp_propose_workspace_bytes": (sz, [i32, i32, i32]),
-        "pm_lpp_propose_device": (i32, [vp, vp, i32, f32, i32, i32, vp, vp, i32, i32, sz, i32, vp, vp, sz, vp, vp]),
+        "pm_lpp_propose_device": (i32, [vp, vp, i32, vp, vp, i32, i32, sz, i32, f32, vp, vp, vp, sz, vp, vp]),
         "pm_disparity_map_init2_device": (i32, [vp, vp, vp, i32, i32, sz, i32, f32, i32, i32, vp, vp, vp, vp, vp, vp,
-                                                vp]),
+                                                vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1,6 +1,7 @@
 // C ABI of the library (include/cvtpm.h): handles, device workspaces and the
 // host orchestration of PMHuberStereo::disparityMap / disparityMapAll
 // (cvt/vision/PMHuberStereo.cpp:75-143, :406-581) on one CUDA stream.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -49,6 +50,7 @@ struct pm_handle {
     std::vector<size_t> lws_bytes;
     // the right view's initial disparity of the call in progress (pm_disparity_map_init2_device)
     const float* init_right = nullptr;
+    const float* init_normal_right = nullptr;   // with init_right: the right view's initial normals
     // concurrent branches of batched calls (pm_set_batch_branches; 0: PM_BATCH_BRANCHES)
     int batch_branches = 0;
 };
@@ -79,25 +81,73 @@ int cuda_fail(pm_handle* h, cudaError_t e, const char* what)
 // allocates nothing.  It holds the ROF intermediates of launch_rof (7 float4 per
 // pixel: u, two dual images p of 2 float4, two q) for up to
 // PM_ROF_STATIC_MAX_PIXELS pixels = 28 MiB of every context that loads this
-// library.  Its device address is looked up once per device, under a lock.
+// library.  Its device address belongs to the CUDA context it was looked up in, so
+// it is cached per context, keyed on the driver's unique context id
+// (cuCtxGetId: never reused within a process, unlike a context handle or a
+// device ordinal after cudaDeviceReset).  The driver functions are taken through
+// cudaGetDriverEntryPointByVersion, so the library does not link the driver.
 constexpr size_t kRofStaticBytes = (size_t)PM_ROF_STATIC_MAX_PIXELS * 7 * sizeof(float4);
 __device__ __align__(256) unsigned char g_rof_static[kRofStaticBytes];
-constexpr int kMaxDevices = 64;
+constexpr int kRofCacheSlots = 64;
 std::mutex g_rof_static_mu;
-void* g_rof_static_ptr[kMaxDevices] = {};
+struct RofStaticSlot {
+    unsigned long long ctx_id;
+    void* ptr;
+};
+RofStaticSlot g_rof_static_cache[kRofCacheSlots] = {};
+int g_rof_static_used = 0;
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
 
-int rof_static_scratch(void** out)
+// id of the calling thread's current context (0 when none is current yet)
+int current_ctx_id(unsigned long long* id)
 {
-    int dev = 0;
-    PM_CUDA(nullptr, cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(nullptr, PM_EINVAL_ARG, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_rof_static_mu);
-    if (!g_rof_static_ptr[dev]) {
-        void* p = nullptr;
-        PM_CUDA(nullptr, cudaGetSymbolAddress(&p, g_rof_static));
-        g_rof_static_ptr[dev] = p;
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa = cudaDriverEntryPointSymbolNotFound, qb = qa;
+        PM_CUDA(nullptr, cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &a, 12000, cudaEnableDefault, &qa));
+        PM_CUDA(nullptr, cudaGetDriverEntryPointByVersion("cuCtxGetId", &b, 12000, cudaEnableDefault, &qb));
+        if (qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b)
+            return fail(nullptr, PM_ECUDA, "pm_k_rof_static: the driver lacks cuCtxGetCurrent or cuCtxGetId");
+        get_current = reinterpret_cast<CtxGetCurrentFn>(a);
+        get_id = reinterpret_cast<CtxGetIdFn>(b);
     }
-    *out = g_rof_static_ptr[dev];
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) return fail(nullptr, PM_ECUDA, "pm_k_rof_static: cuCtxGetCurrent failed");
+    *id = 0;
+    if (ctx && get_id(ctx, id) != CUDA_SUCCESS) return fail(nullptr, PM_ECUDA, "pm_k_rof_static: cuCtxGetId failed");
+    return PM_OK;
+}
+
+// device address of g_rof_static in the current context; the first call in a context looks
+// it up, which must not happen while `st` is being captured into a graph
+int rof_static_scratch(cudaStream_t st, void** out)
+{
+    std::lock_guard<std::mutex> lock(g_rof_static_mu);
+    unsigned long long id = 0;
+    int rc = current_ctx_id(&id);
+    if (rc) return rc;
+    for (int i = 0; id && i < g_rof_static_used; i++)
+        if (g_rof_static_cache[i].ctx_id == id) {
+            *out = g_rof_static_cache[i].ptr;
+            return PM_OK;
+        }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PM_CUDA(nullptr, cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(nullptr, PM_EINVAL_ARG,
+                    "pm_k_rof_static: the first call in a CUDA context looks up the static scratch and must come "
+                    "before stream capture; call it once outside the capture first");
+    void* p = nullptr;
+    PM_CUDA(nullptr, cudaGetSymbolAddress(&p, g_rof_static));   // makes the primary context current if none was
+    if (!id) {
+        rc = current_ctx_id(&id);
+        if (rc) return rc;
+    }
+    if (id && g_rof_static_used < kRofCacheSlots) g_rof_static_cache[g_rof_static_used++] = RofStaticSlot{id, p};
+    *out = p;
     return PM_OK;
 }
 
@@ -543,7 +593,7 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
     int rc;
     if (levels == 1) {
         rc = run_level(h, ws, L, left, right, W, H, stride, r, dmax, iterations, o.thetamin, initdisp, h->init_right,
-                       initnormal, nullptr, ctr, errf, st);   // :92-93 (the right view's init: disparityMapAll's)
+                       initnormal, reinterpret_cast<const float4*>(h->init_normal_right), ctr, errf, st);   // :92-93 (the right view's init: disparityMapAll's)
         if (rc) return rc;
     } else {
         std::vector<int> Wl, Hl;
@@ -782,7 +832,8 @@ int pipeline_on(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* righ
         (uint64_t)(uintptr_t)normal, (uint64_t)(uintptr_t)initdisp, (uint64_t)(uintptr_t)initnormal,
         (uint64_t)(uintptr_t)planesL, (uint64_t)(uintptr_t)planesR, (uint64_t)o.views, (uint64_t)o.fused,
         fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff), (uint64_t)o.rof_iters, (uint64_t)h->counting,
-        (uint64_t)o.levels, (uint64_t)depth, fbits(dscale), (uint64_t)(uintptr_t)h->init_right};
+        (uint64_t)o.levels, (uint64_t)depth, fbits(dscale), (uint64_t)(uintptr_t)h->init_right,
+        (uint64_t)(uintptr_t)h->init_normal_right};
     for (void* p : h->lws) key.push_back((uint64_t)(uintptr_t)p);
     return run_graph(h, h->key1, h->exec1, key, st, run);
 }
@@ -810,7 +861,7 @@ int pm_options_default(pm_options* o)
 {
     if (!o) return PM_EINVAL_ARG;
     o->views = 2;
-    o->fused = 1;
+    o->fused = 0;
     o->thetamin = 1e-4f;
     o->maxdispdiff = 1.0f;
     o->maxanglediff = 5.0f;
@@ -1041,17 +1092,22 @@ int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* ri
 
 int pm_disparity_map_init2_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
                                   int patchsize, float dispmax, int iterations, int pp, float* dmap, float* normalmap,
-                                  const float* initdisp_left, const float* initdisp_right, float* planes_left,
-                                  float* planes_right, void* stream)
+                                  const float* initdisp_left, const float* initdisp_right, const float* initnormal_left,
+                                  const float* initnormal_right, float* planes_left, float* planes_right, void* stream)
 {
     if (!h) return fail(nullptr, PM_EINVAL_ARG, "null handle");
     if (initdisp_right && (h->opt.levels != 1 || h->opt.views != 2))
         return fail(h, PM_EINVAL_ARG, "a right-view initial disparity needs one pyramid level and both views");
-    if (!aligned(initdisp_right, 4)) return fail(h, PM_EINVAL_ARG, "float fields must be 4-byte aligned");
+    if (initnormal_right && !initdisp_right)
+        return fail(h, PM_EINVAL_ARG, "a right-view initial normal map needs a right-view initial disparity");
+    if (!aligned(initdisp_right, 4) || !aligned(initnormal_right, 16))
+        return fail(h, PM_EINVAL_ARG, "float fields must be 4-byte aligned, normal maps 16-byte aligned");
     h->init_right = initdisp_right;
+    h->init_normal_right = initnormal_right;
     const int rc = entry_device(h, 0, 0.0f, left, right, W, H, stride, patchsize, dispmax, iterations, pp, dmap, normalmap,
-                                initdisp_left, nullptr, planes_left, planes_right, S(stream));
+                                initdisp_left, initnormal_left, planes_left, planes_right, S(stream));
     h->init_right = nullptr;
+    h->init_normal_right = nullptr;
     return rc;
 }
 
@@ -1109,6 +1165,40 @@ int pm_batch_schedule(int n, int branches, const int* width, const int* height, 
     if (n == 0) return PM_OK;
     if (!width || !height || !patchsize || !order || !owner) return fail(nullptr, PM_EINVAL_ARG, "null array");
     batch_schedule(n, n < branches ? n : branches, width, height, patchsize, order, owner);
+    return PM_OK;
+}
+
+// Split of a batch over `ranks` processes (one GPU each), balanced by each pair's work
+// W*H*(2r+1)^2*dispmax: the pairs in decreasing work (stable), each to the least loaded rank
+// (the lowest index among equals).  Host only; no collective is involved, every rank computes
+// the same split from the same arrays.
+int pm_batch_partition(int n, int ranks, const int* width, const int* height, const int* patchsize,
+                       const float* dispmax, int* rank_of, double* load)
+{
+    if (n < 0 || n > PM_MAX_BATCH) return fail(nullptr, PM_EINVAL_ARG, "batch size out of range");
+    if (ranks < 1 || ranks > PM_MAX_RANKS) return fail(nullptr, PM_EINVAL_ARG, "rank count out of range");
+    if (n > 0 && (!width || !height || !patchsize || !dispmax || !rank_of))
+        return fail(nullptr, PM_EINVAL_ARG, "null array");
+    std::vector<double> work(n), ld(ranks, 0.0);
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) {
+        if (width[i] < 1 || height[i] < 1 || patchsize[i] < 0 || !(dispmax[i] > 0.0f))
+            return fail(nullptr, PM_EINVAL_ARG, "pair " + std::to_string(i) + " has no work");
+        order[i] = i;
+        const double win = (2.0 * patchsize[i] + 1.0) * (2.0 * patchsize[i] + 1.0);
+        work[i] = (double)width[i] * height[i] * win * dispmax[i];
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+    for (int k = 0; k < n; k++) {
+        const int i = order[k];
+        int best = 0;
+        for (int r = 1; r < ranks; r++)
+            if (ld[r] < ld[best]) best = r;
+        rank_of[i] = best;
+        ld[best] += work[i];
+    }
+    if (load)
+        for (int r = 0; r < ranks; r++) load[r] = ld[r];
     return PM_OK;
 }
 
@@ -1310,6 +1400,7 @@ int pm_k_rof(float* out, const float* input, const float* dt, const float lambda
     int rc = check_shape(nullptr, W, H, 0);
     if (rc) return rc;
     if (!out || !input || !dt || !lambda || !scratch || out == input) return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    if (iters < 0) return fail(nullptr, PM_EINVAL_ARG, "pm_k_rof: negative step count");
     launch_rof((float4*)out, (const float4*)input, (const float4*)dt,
                make_float4(lambda[0], lambda[1], lambda[2], lambda[3]), iters, W, H, scratch, S(stream));
     PM_CUDA(nullptr, cudaGetLastError());
@@ -1332,8 +1423,9 @@ int pm_k_rof_static(float* out, const float* input, const float* dt, const float
                         " pixels exceed the static scratch of PM_ROF_STATIC_MAX_PIXELS = " +
                         std::to_string(PM_ROF_STATIC_MAX_PIXELS) + "; use pm_k_rof with a caller buffer");
     if (!out || !input || !dt || !lambda || out == input) return fail(nullptr, PM_EINVAL_ARG, "bad argument");
+    if (iters < 0) return fail(nullptr, PM_EINVAL_ARG, "pm_k_rof_static: negative step count");
     void* scratch = nullptr;
-    rc = rof_static_scratch(&scratch);
+    rc = rof_static_scratch(S(stream), &scratch);
     if (rc) return rc;
     launch_rof((float4*)out, (const float4*)input, (const float4*)dt,
                make_float4(lambda[0], lambda[1], lambda[2], lambda[3]), iters, W, H, scratch, S(stream));

@@ -1,32 +1,40 @@
-// Learned plane proposal: a small BF16 CNN whose output replaces the random initialisation
-// of PMHuberStereo::disparityMap through its initdisparity argument (PMHuberStereo.cpp:92-93,
-// pmhstereo_init_disparity_normal, pmhstereo.cl:802-828; normals then come from
-// pmhstereo_disparity_to_normal).
+// Learned plane proposal: a BF16 CNN whose per-pixel (disparity, nx, ny) replaces the random
+// initialisation of PMHuberStereo::disparityMap through its initdisparity and initnormalmap
+// arguments (PMHuberStereo.cpp:92-93, :469-470 -> pmhstereo_init_disparity_normal,
+// pmhstereo.cl:802-828, which builds each pixel's plane with nd_state_from_disparity_normal,
+// :99-106).
 //
-// Network, at a quarter (scale 4) or half (scale 2) of the image resolution (W4 = W / scale,
-// H4 = H / scale, floor; "feature pixels"):
-//   features  grey of scale x scale blocks of both images; a cost volume of D = 32 disparity
-//             hypotheses (0, k, .. 31 k feature pixels; at scale 4, k = 1 reaches 124 px and 2
-//             reaches 248 px): 3x3 mean of |gL(x, y) - gR(x - k d, y)|, times 8
-//   6 convs   3x3, 32 -> 32 channels, BF16 weights and activations, FP32 accumulation; ReLU
-//             after the first five; the sixth gives 32 logits per pixel (FP32)
-//   output    soft-argmin: disparity = k sum_d d softmax(-(logit_d + skip * cost_d))_d (the
-//             network corrects the matching cost); upsampled bilinearly and scaled by `scale`
-//             to a full-resolution initial disparity
-// Training (cvt_b200/learn.py drives it): smooth-L1 loss against the quarter-resolution mean
-// of plain PatchMatch's disparity, hand-written backward kernels (data gradients through the
-// same tensor-core kernel with the transposed, mirrored weights; weight gradients on the CUDA
-// cores, reduced in a fixed order), and Adam.
+// Network, at 1 / scale of the image resolution (W4 = W / scale, H4 = H / scale, floor;
+// "feature pixels"):
+//   input   6 channels: the left and right images' RGB, means of scale x scale blocks of
+//           k / 255, minus 0.5, padded with zeros to 16 channels (BF16, NHWC)
+//   8 convs 3x3, channels 16(6) -> 32 -> 32 -> 64 -> 64 -> 64 -> 64 -> 32 -> 16(3), dilations
+//           1, 1, 2, 4, 8, 16, 1, 1 (a receptive field of 69 feature pixels), BF16 weights and
+//           activations, FP32 accumulation, bias and ReLU after the first seven; the eighth
+//           gives (d, nx, ny) in FP32: disparity in feature pixels and the normal's x and y
+//   output  bilinear upsampling to full resolution: disparity d * scale, normal (nx, ny,
+//           sqrt(max(1 - nx^2 - ny^2, 0.01)))
+// The right view's proposal is the network applied to the mirrored, swapped pair (the right
+// image flipped left-right as the first view): its disparities are the right view's, and
+// its normal (nx', ny') becomes (nx', -ny') in the convention pmhstereo_init_disparity_normal
+// uses for the right view (there nx / nz is the x-slope of the right disparity, for the left
+// view minus the x-slope of the left one).
 //
-// Tensor cores.  k_conv_tc is an implicit GEMM on tcgen05: one CTA of 128 threads computes
-// 128 pixels x 32 output channels, K = 9 taps x 32 input channels = 288 as 18 MMAs of
-// M128 N32 K16 (kind::f16, BF16 A and B, FP32 accumulator in 32 TMEM columns).  A (the 128
-// pixels' 3x3 neighbourhoods) and B (the weights) are staged in shared memory in the
-// canonical K-major layout without swizzle: 8-row x 16-byte core matrices, the row groups
-// 128 bytes apart (SBO), the 8-element K chunks a whole tile apart (LBO).  One thread issues
-// the MMAs and commits them to an mbarrier; every warp then reads its 32 TMEM lanes
-// (tcgen05.ld 32x32b) for the epilogue.  The wait on the mbarrier is bounded: past the limit
-// the kernel raises an error flag that the host reads.
+// Tensor cores (tcgen05, kind::f16, BF16 x BF16 -> FP32 in TMEM):
+//   k_conv_tc   forward and data gradient: an implicit GEMM, per CTA 128 pixels (M) x COUT (N),
+//               K = 9 taps x CIN, all taps of A and all of B staged in shared memory in the
+//               canonical K-major layout without swizzle; one thread issues the MMAs and
+//               commits them to an mbarrier; the epilogue reads TMEM (tcgen05.ld 32x32b).  The
+//               data gradient is the same kernel with the layer's transposed, tap-mirrored
+//               weights and the ReLU mask of the layer's input in the epilogue.
+//   k_wgrad_tc  weight gradient: D[(tap, ci)][co] = sum over pixels of x[p + tap][ci] dy[p][co]
+//               as MMAs of M128 (tap, ci rows) x N COUT x K16 (pixels), both operands MN-major
+//               (16-byte NHWC channel groups are the core-matrix rows, so cp.async copies them
+//               unchanged), a row of ones in A gives the bias gradient; two shared-memory
+//               stages so that the copies of 64 pixels overlap the MMAs of the previous 64;
+//               per-CTA partial sums reduced in CTA order (deterministic).
+// Every wait on an mbarrier is bounded by clock (about two seconds); past the limit the kernel
+// raises the error flag that the host reads.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -39,19 +47,19 @@
 namespace pm {
 namespace lpp {
 
-constexpr int CH = 32;            // channels of every layer, and disparity hypotheses
-constexpr int TAPS = 9;
-constexpr int KTOT = CH * TAPS;   // 288
-constexpr int TM = 128;           // pixels per CTA
-constexpr int A_BYTES = TM * KTOT * 2;
-constexpr int B_BYTES = CH * KTOT * 2;
-constexpr int CONV_SMEM = A_BYTES + B_BYTES;
-constexpr uint32_t A_LBO = (TM / 8) * 128;   // bytes between K chunks of A
-constexpr uint32_t B_LBO = (CH / 8) * 128;   // bytes between K chunks of B
-// kind::f16 instruction descriptor: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1),
-// both K-major, N >> 3 at bit 17, M >> 4 at bit 24
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(CH >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+constexpr int NL = 8;
+constexpr int LCIN[NL] = {16, 32, 32, 64, 64, 64, 64, 32};
+constexpr int LCOUT[NL] = {32, 32, 64, 64, 64, 64, 32, 16};
+constexpr int LDIL[NL] = {1, 1, 2, 4, 8, 16, 1, 1};
+constexpr int IN_CH = 16, OUT_CH = 16, MAX_CH = 64;
+constexpr int TM = 128;                           // pixels per CTA (conv)
 constexpr long long WAIT_CYCLES = 4000000000ll;   // about two seconds at the B200's clock
+constexpr int WG_PIX = 1024;                      // pixels per CTA of the weight gradient
+constexpr int WG_G = 4;                           // K steps of 16 pixels per stage
+
+enum { EPI_RELU_BF16 = 0, EPI_BIAS_F32 = 1, EPI_MASK_BF16 = 2 };
+
+__host__ __device__ constexpr int tmem_cols(int n) { return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : n <= 256 ? 256 : 512; }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -63,9 +71,34 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// kind::f16 instruction descriptor: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1),
+// A and B MN-major when the flags are set (bits 15, 16), N >> 3 at bit 17, M >> 4 at bit 24
+__host__ __device__ constexpr uint32_t idesc(int M, int N, bool a_mn, bool b_mn)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
 // byte offset of the 16-byte chunk `c` (8 K elements) of row `r` in a canonical K-major tile of
-// `rows` rows
+// `rows` rows: 8-row x 16-byte core matrices, row groups 128 bytes apart (SBO), K chunks a
+// whole column of core matrices apart (LBO = rows / 8 * 128)
 __device__ __forceinline__ uint32_t canon(int c, int r, int rows) { return (uint32_t)(c * (rows / 8) * 128 + (r >> 3) * 128 + (r & 7) * 16); }
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t id, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        :
+        : "r"(tmem), "l"(ad), "l"(bd), "r"(id), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
 
 // non-blocking test of an mbarrier phase
 __device__ __forceinline__ bool mbar_test(uint32_t addr, uint32_t phase)
@@ -90,49 +123,90 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t phase,
     return true;
 }
 
-enum { EPI_RELU_BF16 = 0, EPI_BIAS_F32 = 1, EPI_MASK_BF16 = 2 };
+// 16 consecutive TMEM columns of this warp's 32 lanes
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+        "[%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(addr));
+}
+
+// 16-byte asynchronous copy global -> shared; zeros when !ok (the source is then not read)
+__device__ __forceinline__ void cp16(void* dst, const void* src, bool ok)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(ok ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, int cols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+__device__ __forceinline__ void tmem_free(uint32_t tmem, int cols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols));
+}
+
+// pixel m of a B x H x W batch shifted by tap t (3x3, dilation dil): its linear index, or -1
+// outside the image (zero padding)
+__device__ __forceinline__ int tap_pixel(int m, int M, int H, int W, int t, int dil)
+{
+    if (m >= M) return -1;
+    const int HW = H * W;
+    const int b = m / HW, rem = m - b * HW, y = rem / W, x = rem - y * W;
+    const int yy = y + (t / 3 - 1) * dil, xx = x + (t % 3 - 1) * dil;
+    if (yy < 0 || yy >= H || xx < 0 || xx >= W) return -1;
+    return b * HW + yy * W + xx;
+}
 
 // out[m][n] = sum over taps t and channels c of in[pixel m shifted by tap t][c] * wmat[n][t][c],
-// 3x3 taps (dy, dx) = (t / 3 - 1, t % 3 - 1) with zero padding, then per EPI:
+// then per EPI:
 //   EPI_RELU_BF16  + bias, ReLU, BF16 out          (forward, hidden layers)
-//   EPI_BIAS_F32   + bias, FP32 out                (forward, logits)
-//   EPI_MASK_BF16  times (mask[m][n] > 0), BF16 out (backward: data gradient through ReLU)
-template <int EPI>
-__global__ void __launch_bounds__(TM) k_conv_tc(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ wmat,
-                                                const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask,
-                                                void* __restrict__ out, int B, int H, int W, int* err)
+//   EPI_BIAS_F32   + bias, FP32 out                (forward, last layer)
+//   EPI_MASK_BF16  times (mask[m][n] > 0), BF16 out (data gradient through the ReLU)
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(TM) k_conv_tc(const __nv_bfloat16* __restrict__ in,
+                                                const __nv_bfloat16* __restrict__ wmat, const float* __restrict__ bias,
+                                                const __nv_bfloat16* __restrict__ mask, void* __restrict__ out, int B,
+                                                int H, int W, int dil, int* err)
 {
+    constexpr int KTOT = 9 * CIN, KC = KTOT / 8;   // K and its 16-byte chunks
+    constexpr int A_BYTES = TM * KTOT * 2;
+    constexpr uint32_t A_LBO = (TM / 8) * 128, B_LBO = (COUT / 8) * 128;
+    constexpr int TCOLS = tmem_cols(COUT);
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
     uint8_t* sA = smem;
     uint8_t* sB = smem + A_BYTES;
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int HW = H * W, M = B * HW;
+    const int M = B * H * W;
     const int m = blockIdx.x * TM + tid;
-    const int b = m / HW, rem = m - b * HW, y = rem / W, x = rem - y * W;
-    for (int t = 0; t < TAPS; t++) {
-        const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
-        const bool ok = m < M && yy >= 0 && yy < H && xx >= 0 && xx < W;
-        const uint4* src = ok ? reinterpret_cast<const uint4*>(in + ((size_t)b * HW + (size_t)yy * W + xx) * CH) : nullptr;
+    // A: this thread's pixel, every tap, CIN / 8 chunks each; B: the weights
+#pragma unroll 1
+    for (int t = 0; t < 9; t++) {
+        const int src = tap_pixel(m, M, H, W, t, dil);
+        const uint4* s = reinterpret_cast<const uint4*>(in + (size_t)(src < 0 ? 0 : src) * CIN);
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const uint4 v = ok ? __ldg(src + q) : make_uint4(0, 0, 0, 0);
-            *reinterpret_cast<uint4*>(sA + canon(t * 4 + q, tid, TM)) = v;
-        }
+        for (int q = 0; q < CIN / 8; q++) cp16(sA + canon(t * (CIN / 8) + q, tid, TM), s + q, src >= 0);
     }
-    for (int i = tid; i < CH * (KTOT / 8); i += TM) {
-        const int n = i / (KTOT / 8), c = i - n * (KTOT / 8);
-        *reinterpret_cast<uint4*>(sB + canon(c, n, CH)) = __ldg(reinterpret_cast<const uint4*>(wmat + (size_t)n * KTOT) + c);
+    for (int i = tid; i < COUT * KC; i += TM) {
+        const int n = i / KC, c = i - n * KC;
+        cp16(sB + canon(c, n, COUT), reinterpret_cast<const uint4*>(wmat + (size_t)n * KTOT) + c, true);
     }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)), "r"(CH));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
+    cp_commit();
+    if (warp == 0) tmem_alloc(&tmem_base, TCOLS);
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
+    cp_wait_all();
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // staged tiles -> tensor core reads
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -141,283 +215,397 @@ __global__ void __launch_bounds__(TM) k_conv_tc(const __nv_bfloat16* __restrict_
     if (tid == 0) {
         const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
 #pragma unroll 1
-        for (int j = 0; j < KTOT / 16; j++) {
-            const uint64_t ad = smem_desc(a0 + 2 * j * A_LBO, A_LBO, 128);
-            const uint64_t bd = smem_desc(b0 + 2 * j * B_LBO, B_LBO, 128);
-            const uint32_t acc = j > 0 ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "setp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                :
-                : "r"(tmem), "l"(ad), "l"(bd), "r"(IDESC), "r"(acc)
-                : "memory");
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&mbar))
-                     : "memory");
+        for (int j = 0; j < KTOT / 16; j++)
+            mma_f16(tmem, smem_desc(a0 + 2 * j * A_LBO, A_LBO, 128), smem_desc(b0 + 2 * j * B_LBO, B_LBO, 128),
+                    idesc(TM, COUT, false, false), j > 0 ? 1u : 0u);
+        mma_commit(smem_u32(&mbar));
     }
     bool done = mbar_wait_bounded(smem_u32(&mbar), 0, WAIT_CYCLES);
     if (!done) {
         atomicExch(err, 1);
-        // the MMAs of this CTA may still run: wait for them once more before freeing TMEM (a
-        // CTA whose MMAs never complete reads nothing and leaves its 32 columns allocated)
+        // the MMAs of this CTA may still run: wait for them once more before freeing TMEM
         done = mbar_wait_bounded(smem_u32(&mbar), 0, WAIT_CYCLES);
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (done) {
-        uint32_t r[32];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-            "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-              "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-              "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-              "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-            : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (m < M) {
-            if (EPI == EPI_BIAS_F32) {
-                float4* o = reinterpret_cast<float4*>(static_cast<float*>(out) + (size_t)m * CH);
 #pragma unroll
-                for (int j = 0; j < CH; j += 4)
-                    o[j / 4] = make_float4(__uint_as_float(r[j]) + bias[j], __uint_as_float(r[j + 1]) + bias[j + 1],
-                                           __uint_as_float(r[j + 2]) + bias[j + 2], __uint_as_float(r[j + 3]) + bias[j + 3]);
-            } else {
-                __nv_bfloat162 v[CH / 2];
-                const __nv_bfloat16* mk = mask + (size_t)m * CH;
+        for (int j0 = 0; j0 < COUT; j0 += 16) {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + j0, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < M) {
+                if (EPI == EPI_BIAS_F32) {
+                    float4* o = reinterpret_cast<float4*>(static_cast<float*>(out) + (size_t)m * COUT + j0);
 #pragma unroll
-                for (int j = 0; j < CH; j += 2) {
-                    float a = __uint_as_float(r[j]), c = __uint_as_float(r[j + 1]);
-                    if (EPI == EPI_RELU_BF16) {
-                        a = fmaxf(a + bias[j], 0.0f);
-                        c = fmaxf(c + bias[j + 1], 0.0f);
-                    } else {
-                        a = __bfloat162float(mk[j]) > 0.0f ? a : 0.0f;
-                        c = __bfloat162float(mk[j + 1]) > 0.0f ? c : 0.0f;
+                    for (int j = 0; j < 16; j += 4)
+                        o[j / 4] = make_float4(__uint_as_float(r[j]) + bias[j0 + j], __uint_as_float(r[j + 1]) + bias[j0 + j + 1],
+                                               __uint_as_float(r[j + 2]) + bias[j0 + j + 2],
+                                               __uint_as_float(r[j + 3]) + bias[j0 + j + 3]);
+                } else {
+                    __align__(16) __nv_bfloat162 v[8];
+                    const __nv_bfloat16* mk = mask + (size_t)m * COUT + j0;
+#pragma unroll
+                    for (int j = 0; j < 16; j += 2) {
+                        float a = __uint_as_float(r[j]), c = __uint_as_float(r[j + 1]);
+                        if (EPI == EPI_RELU_BF16) {
+                            a = fmaxf(a + bias[j0 + j], 0.0f);
+                            c = fmaxf(c + bias[j0 + j + 1], 0.0f);
+                        } else {
+                            a = __bfloat162float(mk[j]) > 0.0f ? a : 0.0f;
+                            c = __bfloat162float(mk[j + 1]) > 0.0f ? c : 0.0f;
+                        }
+                        v[j / 2] = __floats2bfloat162_rn(a, c);
                     }
-                    v[j / 2] = __floats2bfloat162_rn(a, c);
+                    uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + (size_t)m * COUT + j0);
+                    o[0] = reinterpret_cast<const uint4*>(v)[0];
+                    o[1] = reinterpret_cast<const uint4*>(v)[1];
                 }
-                uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + (size_t)m * CH);
-#pragma unroll
-                for (int q = 0; q < 4; q++) o[q] = reinterpret_cast<const uint4*>(v)[q];
             }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0 && done) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(CH));
+    if (warp == 0 && done) tmem_free(tmem, TCOLS);
 }
 
+template <int CIN, int COUT>
+constexpr int conv_smem() { return TM * 9 * CIN * 2 + COUT * 9 * CIN * 2; }
+
 // The same convolution on the CUDA cores (FP32 accumulation in tap-channel order): the
-// reference the tensor-core kernel is checked against on the device.
+// reference the tensor-core kernel is checked against on the device.  One thread per output.
 template <int EPI>
 __global__ void k_conv_ref(const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ wmat,
                            const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask, void* __restrict__ out,
-                           int B, int H, int W)
+                           int B, int H, int W, int dil, int CIN, int COUT)
 {
-    const int HW = H * W, M = B * HW;
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= M) return;
-    const int b = m / HW, rem = m - b * HW, y = rem / W, x = rem - y * W;
-    float acc[CH];
-#pragma unroll
-    for (int n = 0; n < CH; n++) acc[n] = 0.0f;
-    for (int t = 0; t < TAPS; t++) {
-        const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
-        if (yy < 0 || yy >= H || xx < 0 || xx >= W) continue;
-        const __nv_bfloat16* src = in + ((size_t)b * HW + (size_t)yy * W + xx) * CH;
-        for (int c = 0; c < CH; c++) {
-            const float a = __bfloat162float(src[c]);
-#pragma unroll
-            for (int n = 0; n < CH; n++) acc[n] = fmaf(a, __bfloat162float(wmat[(size_t)n * KTOT + t * CH + c]), acc[n]);
-        }
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int M = B * H * W;
+    if (i >= (long long)M * COUT) return;
+    const int m = (int)(i / COUT), n = (int)(i - (long long)m * COUT);
+    float acc = 0.0f;
+    for (int t = 0; t < 9; t++) {
+        const int src = tap_pixel(m, M, H, W, t, dil);
+        if (src < 0) continue;
+        for (int c = 0; c < CIN; c++)
+            acc += __bfloat162float(in[(size_t)src * CIN + c]) * __bfloat162float(wmat[(size_t)n * 9 * CIN + t * CIN + c]);
     }
-    if (EPI == EPI_BIAS_F32) {
-        float* o = static_cast<float*>(out) + (size_t)m * CH;
-        for (int n = 0; n < CH; n++) o[n] = acc[n] + bias[n];
-    } else {
-        __nv_bfloat16* o = static_cast<__nv_bfloat16*>(out) + (size_t)m * CH;
-        for (int n = 0; n < CH; n++) {
-            float v = acc[n];
-            if (EPI == EPI_RELU_BF16) v = fmaxf(v + bias[n], 0.0f);
-            else v = __bfloat162float(mask[(size_t)m * CH + n]) > 0.0f ? v : 0.0f;
-            o[n] = __float2bfloat16_rn(v);
-        }
-    }
+    if (EPI == EPI_BIAS_F32) static_cast<float*>(out)[i] = acc + bias[n];
+    else if (EPI == EPI_RELU_BF16) static_cast<__nv_bfloat16*>(out)[i] = __float2bfloat16_rn(fmaxf(acc + bias[n], 0.0f));
+    else static_cast<__nv_bfloat16*>(out)[i] = __float2bfloat16_rn(__bfloat162float(mask[i]) > 0.0f ? acc : 0.0f);
 }
 
-// weight gradient, stage 1: block `blk` sums over its pixels dW[n][t][c] += dy[m][n] x[m + t][c]
-// and db[n] += dy[m][n]; partial sums to part[blk][CH * KTOT + CH]
-__global__ void __launch_bounds__(KTOT) k_wgrad_part(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ dy,
-                                                     float* __restrict__ part, int B, int H, int W, int per_block)
+// Weight gradient on the tensor cores, stage 1: CTA `blockIdx.x` sums over its WG_PIX pixels
+// D[r][co] = sum_p A[r][p] dy[p][co] with A[t * CIN + ci][p] = x[p shifted by tap t][ci] and
+// A[9 * CIN][p] = 1 (the bias gradient), and writes part[cta][r][co] for r <= 9 * CIN.
+// Shared memory per K step (16 pixels), MN-major without swizzle: core matrices of 8 pixel rows
+// x 16 bytes (8 channels); the two K halves of a channel group side by side (LBO = 128 bytes),
+// the channel groups 256 bytes apart (SBO).  Both strides stay inside the tile whichever way
+// the descriptor fields are read, so no access can leave the stage's buffer.
+template <int CIN, int COUT>
+struct WgradShape {
+    static constexpr int ROWS = 9 * CIN + 1;          // (tap, ci) rows and the row of ones
+    static constexpr int MB = (ROWS + 127) / 128;     // M blocks of 128 rows
+    static constexpr int A_KSTEP = MB * 16 * 256;     // bytes of A per K step
+    static constexpr int B_KSTEP = (COUT / 8) * 256;  // bytes of B per K step
+    static constexpr int STAGE = WG_G * (A_KSTEP + B_KSTEP);
+    static constexpr int SMEM = 2 * STAGE;
+    static constexpr int TCOLS = tmem_cols(MB * COUT);
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) k_wgrad_tc(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ dy,
+                                                  float* __restrict__ part, int B, int H, int W, int dil, int* err)
 {
-    __shared__ float sdy[CH];
-    const int k = threadIdx.x, t = k / CH, c = k - t * CH;
-    const int HW = H * W, M = B * HW;
-    const int m0 = blockIdx.x * per_block, m1 = min(m0 + per_block, M);
-    float acc[CH];
-#pragma unroll
-    for (int n = 0; n < CH; n++) acc[n] = 0.0f;
-    float dbias = 0.0f;
-    for (int m = m0; m < m1; m++) {
-        __syncthreads();
-        if (k < CH) sdy[k] = __bfloat162float(dy[(size_t)m * CH + k]);
-        __syncthreads();
-        if (k < CH) dbias += sdy[k];
-        const int b = m / HW, rem = m - b * HW, y = rem / W, xq = rem - y * W;
-        const int yy = y + t / 3 - 1, xx = xq + t % 3 - 1;
-        if (yy < 0 || yy >= H || xx < 0 || xx >= W) continue;
-        const float a = __bfloat162float(x[((size_t)b * HW + (size_t)yy * W + xx) * CH + c]);
-#pragma unroll
-        for (int n = 0; n < CH; n++) acc[n] = fmaf(sdy[n], a, acc[n]);
+    using S = WgradShape<CIN, COUT>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int M = B * H * W;
+    const int p0 = blockIdx.x * WG_PIX;
+    constexpr int NGROUPS = WG_PIX / (16 * WG_G);
+    constexpr uint32_t ID = idesc(128, COUT, true, true);
+
+    // rows 9 * CIN .. of every K step of both stages: the row of ones, then zeros
+    for (int i = tid; i < 2 * WG_G * 16 * (S::MB * 16 - 9 * CIN / 8); i += 128) {
+        const int per = 16 * (S::MB * 16 - 9 * CIN / 8);
+        const int ks = i / per, rem = i - ks * per;
+        const int mi = 9 * CIN / 8 + rem / 16, k = rem % 16;
+        uint8_t* a = smem + (ks / WG_G) * S::STAGE + (ks % WG_G) * S::A_KSTEP;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (mi == 9 * CIN / 8) v.x = 0x3F80u;   // BF16 1.0 in the first element of the row
+        *reinterpret_cast<uint4*>(a + mi * 256 + (k >> 3) * 128 + (k & 7) * 16) = v;
     }
-    float* p = part + (size_t)blockIdx.x * (CH * KTOT + CH);
-#pragma unroll
-    for (int n = 0; n < CH; n++) p[(size_t)n * KTOT + k] = acc[n];
-    if (k < CH) p[CH * KTOT + k] = dbias;
-}
-
-// weight gradient, stage 2: sum of the partials in block order (deterministic)
-__global__ void k_wgrad_sum(const float* __restrict__ part, float* __restrict__ grad, int nblocks)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= CH * KTOT + CH) return;
-    float s = 0.0f;
-    for (int b = 0; b < nblocks; b++) s += part[(size_t)b * (CH * KTOT + CH) + i];
-    grad[i] = s;
-}
-
-// grey of the sc x sc blocks of an RGBA8 image (0.2126, 0.7152, 0.0722 weights on k / 255)
-__global__ void k_grey(const uint8_t* __restrict__ img, size_t stride, int sc, int W4, int H4, float* __restrict__ out)
-{
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= W4) return;
-    float s = 0.0f;
-    for (int j = 0; j < sc; j++) {
-        const uchar4* row = reinterpret_cast<const uchar4*>(img + (size_t)(sc * y + j) * stride) + sc * x;
-        for (int i = 0; i < sc; i++) {
-            const uchar4 p = __ldg(row + i);
-            s += 0.2126f * (float)p.x + 0.7152f * (float)p.y + 0.0722f * (float)p.z;
-        }
-    }
-    out[(size_t)y * W4 + x] = s * (1.0f / ((float)(sc * sc) * 255.0f));
-}
-
-// cost volume: channel d = 8 x the 3x3 mean of |g1(x, y) - g2(x + s k d, y)| (hypothesis d at k d
-// quarter pixels, k = step), s = -1 for the left view (g1 left, g2 right), +1 for the right view
-// (g1 right, g2 left); columns outside the image count as a difference of 1; BF16 NHWC
-__global__ void k_costvol(const float* __restrict__ gl, const float* __restrict__ gr, int W4, int H4, int sgn,
-                          __nv_bfloat16* __restrict__ out)
-{
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= W4) return;
-    __nv_bfloat16* o = out + ((size_t)y * W4 + x) * CH;
-    for (int d = 0; d < CH; d++) {
-        float s = 0.0f;
-        int n = 0;
-        for (int j = -1; j <= 1; j++) {
-            const int yy = y + j;
-            if (yy < 0 || yy >= H4) continue;
-            for (int i = -1; i <= 1; i++) {
-                const int xx = x + i;
-                if (xx < 0 || xx >= W4) continue;
-                const float a = gl[(size_t)yy * W4 + xx];
-                const int xm = xx + sgn * d;
-                const float c = xm >= 0 && xm < W4 ? gr[(size_t)yy * W4 + xm] : a + 1.0f;
-                s += fabsf(a - c);
-                n++;
+    // stage g's copies: 16 * WG_G pixels, each the 9 taps x CIN / 8 chunks of A and COUT / 8 of B
+    auto stage = [&](int g) {
+        uint8_t* base = smem + (g & 1) * S::STAGE;
+        constexpr int QA = 9 * CIN / 8, QB = COUT / 8;
+        for (int i = tid; i < 16 * WG_G * (QA + QB); i += 128) {
+            const int kk = i / (QA + QB), q = i - kk * (QA + QB);
+            const int ks = kk >> 4, k = kk & 15;
+            const int p = p0 + g * 16 * WG_G + kk;
+            if (q < QA) {
+                const int t = q / (CIN / 8), c = q - t * (CIN / 8);
+                const int src = tap_pixel(p, M, H, W, t, dil);
+                uint8_t* a = base + ks * S::A_KSTEP;
+                cp16(a + q * 256 + (k >> 3) * 128 + (k & 7) * 16,
+                     reinterpret_cast<const uint4*>(x + (size_t)(src < 0 ? 0 : src) * CIN) + c, src >= 0);
+            } else {
+                const int c = q - QA;
+                uint8_t* b = base + WG_G * S::A_KSTEP + ks * S::B_KSTEP;
+                cp16(b + c * 256 + (k >> 3) * 128 + (k & 7) * 16,
+                     reinterpret_cast<const uint4*>(dy + (size_t)(p < M ? p : 0) * COUT) + c, p < M);
             }
         }
-        o[d] = __float2bfloat16_rn(8.0f * s / (float)n);
+        cp_commit();
+    };
+    if (warp == 0) tmem_alloc(&tmem_base, S::TCOLS);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;");
     }
+    stage(0);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    bool ok = true;
+    for (int g = 0; g < NGROUPS; g++) {
+        cp_wait_all();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+            const uint32_t base = smem_u32(smem + (g & 1) * S::STAGE);
+#pragma unroll 1
+            for (int ks = 0; ks < WG_G; ks++) {
+                const uint32_t a = base + ks * S::A_KSTEP, b = base + WG_G * S::A_KSTEP + ks * S::B_KSTEP;
+#pragma unroll
+                for (int j = 0; j < S::MB; j++)
+                    mma_f16(tmem + j * COUT, smem_desc(a + j * 16 * 256, 128, 256), smem_desc(b, 128, 256), ID,
+                            (g > 0 || ks > 0) ? 1u : 0u);
+            }
+            mma_commit(smem_u32(&mbar[g & 1]));
+        }
+        if (g + 1 < NGROUPS) {
+            // the buffer of stage g + 1 was read by the MMAs of stage g - 1
+            if (g >= 1 && !mbar_wait_bounded(smem_u32(&mbar[(g + 1) & 1]), ((g - 1) >> 1) & 1, WAIT_CYCLES)) {
+                ok = false;
+                atomicExch(err, 1);
+                break;
+            }
+            stage(g + 1);
+        }
+    }
+    cp_wait_all();
+    // the last commit covers every earlier MMA of the CTA
+    bool done = ok && mbar_wait_bounded(smem_u32(&mbar[(NGROUPS - 1) & 1]), ((NGROUPS - 1) >> 1) & 1, WAIT_CYCLES);
+    if (!done) {
+        atomicExch(err, 1);
+        done = mbar_wait_bounded(smem_u32(&mbar[(NGROUPS - 1) & 1]), ((NGROUPS - 1) >> 1) & 1, WAIT_CYCLES);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (done) {
+        float* dst = part + (size_t)blockIdx.x * (9 * CIN + 1) * COUT;
+#pragma unroll 1
+        for (int j = 0; j < S::MB; j++) {
+            const int row = j * 128 + warp * 32 + (tid & 31);
+#pragma unroll
+            for (int c0 = 0; c0 < COUT; c0 += 16) {
+                uint32_t r[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + j * COUT + c0, r);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (row <= 9 * CIN) {
+                    float4* o = reinterpret_cast<float4*>(dst + (size_t)row * COUT + c0);
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        o[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                           __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0 && done) tmem_free(tmem, S::TCOLS);
 }
 
-// soft-argmin over the 32 logits plus `skip` times the input cost volume (the network learns a
-// correction to the matching cost), and the smooth-L1 loss against target (quarter pixels; a
-// target < 0 is masked): disparity out, dLogits (BF16, scaled by 1 / count) and per-block loss
-// sums
-__global__ void k_softargmin(const float* __restrict__ logits, const __nv_bfloat16* __restrict__ feats, float skip,
-                             float step, const float* __restrict__ target, float* __restrict__ disp,
-                             __nv_bfloat16* __restrict__ dlogits, float* __restrict__ loss_part, int M, float inv_count)
+// weight gradient, stage 2: grad[co][r] (r < 9 CIN) and grad[COUT * 9 CIN + co] (bias) = sums of
+// the CTAs' partials in CTA order
+__global__ void k_wgrad_sum(const float* __restrict__ part, float* __restrict__ grad, int nblocks, int CIN, int COUT)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int rows = 9 * CIN + 1;
+    if (i >= rows * COUT) return;
+    const int r = i / COUT, co = i - r * COUT;
+    float s = 0.0f;
+    for (int b = 0; b < nblocks; b++) s += part[(size_t)b * rows * COUT + i];
+    if (r < 9 * CIN) grad[(size_t)co * 9 * CIN + r] = s;
+    else grad[(size_t)COUT * 9 * CIN + co] = s;
+}
+
+// the same weight gradient on the CUDA cores, one thread per (co, r) (reference for tests)
+__global__ void k_wgrad_ref(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ dy,
+                            float* __restrict__ grad, int B, int H, int W, int dil, int CIN, int COUT)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int rows = 9 * CIN + 1, M = B * H * W;
+    if (i >= rows * COUT) return;
+    const int co = i / rows, r = i - co * rows;
+    float s = 0.0f;
+    for (int p = 0; p < M; p++) {
+        const float g = __bfloat162float(dy[(size_t)p * COUT + co]);
+        if (r == 9 * CIN) {
+            s += g;
+        } else {
+            const int t = r / CIN, ci = r - t * CIN;
+            const int src = tap_pixel(p, M, H, W, t, dil);
+            if (src >= 0) s += __bfloat162float(x[(size_t)src * CIN + ci]) * g;
+        }
+    }
+    if (r < 9 * CIN) grad[(size_t)co * 9 * CIN + r] = s;
+    else grad[(size_t)COUT * 9 * CIN + co] = s;
+}
+
+// input of the network: 16 BF16 channels per feature pixel, the first view's then the second
+// view's RGB as scale x scale block means of k / 255 minus 0.5, then zeros.  right_view: the
+// first view is the right image mirrored left-right, the second the left image mirrored.
+__global__ void k_input(const uint8_t* __restrict__ left, const uint8_t* __restrict__ right, size_t stride, int W, int sc,
+                        int W4, int H4, int right_view, __nv_bfloat16* __restrict__ out)
+{
+    const int x4 = blockIdx.x * blockDim.x + threadIdx.x, y4 = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x4 >= W4 || y4 >= H4) return;
+    float acc[6] = {0, 0, 0, 0, 0, 0};
+    const uint8_t* first = right_view ? right : left;
+    const uint8_t* second = right_view ? left : right;
+    for (int dy = 0; dy < sc; dy++)
+        for (int dx = 0; dx < sc; dx++) {
+            const int xf = x4 * sc + dx;
+            const int x = right_view ? W - 1 - xf : xf;
+            const size_t o = (size_t)(y4 * sc + dy) * stride + (size_t)x * 4;
+            for (int c = 0; c < 3; c++) {
+                acc[c] += (float)first[o + c] / 255.0f;
+                acc[3 + c] += (float)second[o + c] / 255.0f;
+            }
+        }
+    const float inv = 1.0f / (float)(sc * sc);
+    __align__(16) __nv_bfloat16 v[IN_CH];
+    for (int c = 0; c < IN_CH; c++) v[c] = __float2bfloat16_rn(c < 6 ? acc[c] * inv - 0.5f : 0.0f);
+    uint4* o = reinterpret_cast<uint4*>(out + ((size_t)y4 * W4 + x4) * IN_CH);
+    o[0] = reinterpret_cast<const uint4*>(v)[0];
+    o[1] = reinterpret_cast<const uint4*>(v)[1];
+}
+
+// training target at 1 / sc resolution from plain PatchMatch's final planes of one view
+// (planes, float4 a b c cost: the pixel matches a x + b y + c in the other view) and of the
+// other view (for the consistency test).  Per pixel: disparity d = x - (a x + b y + c) for the
+// left view, (a x + b y + c) - x for the right; normal (a - 1, b, 1) normalised, which is the
+// normal pmhstereo_init_disparity_normal turns back into the same a and b for the left view
+// (nd_state_from_disparity_normal, pmhstereo.cl:99-106); for the right view the network sees the
+// mirrored pair, in which the right view is a left view with normal (a - 1, -b, 1).  A pixel is
+// valid when its plane is finite, 0 < d <= dmax, and the other view's disparity at the matched
+// column (rounded) is within 1 px of d.  Per feature block (mirrored for the right view): the
+// means of d / sc, nx, ny over its valid pixels, and 1 when at least half of it is valid.
+__global__ void k_target(const float4* __restrict__ planes, const float4* __restrict__ other, int W, int sc, int W4,
+                         int H4, int right_view, float dmax, float4* __restrict__ out)
+{
+    const int x4 = blockIdx.x * blockDim.x + threadIdx.x, y4 = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x4 >= W4 || y4 >= H4) return;
+    float d = 0.0f, nx = 0.0f, ny = 0.0f;
+    int n = 0;
+    for (int dy = 0; dy < sc; dy++)
+        for (int dx = 0; dx < sc; dx++) {
+            const int y = y4 * sc + dy, xf = x4 * sc + dx;
+            const int x = right_view ? W - 1 - xf : xf;
+            const float4 s = planes[(size_t)y * W + x];
+            if (!(isfinite(s.x) && isfinite(s.y) && isfinite(s.z))) continue;
+            const float tx = s.x * (float)x + s.y * (float)y + s.z;
+            const float dv = right_view ? tx - (float)x : (float)x - tx;
+            if (!(dv > 0.0f && dv <= dmax)) continue;
+            const int xo = __float2int_rn(tx);
+            if (xo < 0 || xo >= W) continue;
+            const float4 o = other[(size_t)y * W + xo];
+            const float txo = o.x * (float)xo + o.y * (float)y + o.z;
+            const float dov = right_view ? (float)xo - txo : txo - (float)xo;
+            if (!(fabsf(dov - dv) <= 1.0f)) continue;
+            const float vx = s.x - 1.0f, vy = right_view ? -s.y : s.y;
+            const float inv = rsqrtf(vx * vx + vy * vy + 1.0f);
+            d += dv;
+            nx += vx * inv;
+            ny += vy * inv;
+            n++;
+        }
+    const bool ok = 2 * n >= sc * sc && n > 0;
+    out[(size_t)y4 * W4 + x4] = ok ? make_float4(d / (float)n / (float)sc, nx / (float)n, ny / (float)n, 1.0f)
+                                   : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// L1 loss of the network output (channels d, nx, ny of OUT_CH) against target (d, nx, ny, valid):
+// |d - d*| + wn (|nx - nx*| + |ny - ny*|) over valid pixels, times `scale`; dout = its gradient
+// (BF16, zero in the unused channels); parts[block] = the block's loss sum (unscaled)
+__global__ void k_loss(const float* __restrict__ outp, const float4* __restrict__ target, float wn, float scale, int M,
+                       __nv_bfloat16* __restrict__ dout, float* __restrict__ parts)
 {
     __shared__ float red[256];
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     float l = 0.0f;
     if (m < M) {
-        float lg[CH];
-        for (int d = 0; d < CH; d++)
-            lg[d] = logits[(size_t)m * CH + d] + (feats ? skip * __bfloat162float(feats[(size_t)m * CH + d]) : 0.0f);
-        float mn = lg[0];
-        for (int d = 1; d < CH; d++) mn = fminf(mn, lg[d]);
-        float p[CH], z = 0.0f;
-        for (int d = 0; d < CH; d++) {
-            p[d] = __expf(-(lg[d] - mn));
-            z += p[d];
+        const float* o = outp + (size_t)m * OUT_CH;
+        const float4 t = target[m];
+        float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
+        if (t.w > 0.0f) {
+            const float e0 = o[0] - t.x, e1 = o[1] - t.y, e2 = o[2] - t.z;
+            l = fabsf(e0) + wn * (fabsf(e1) + fabsf(e2));
+            g0 = scale * (float)((e0 > 0.0f) - (e0 < 0.0f));
+            g1 = scale * wn * (float)((e1 > 0.0f) - (e1 < 0.0f));
+            g2 = scale * wn * (float)((e2 > 0.0f) - (e2 < 0.0f));
         }
-        float e = 0.0f;
-        for (int d = 0; d < CH; d++) {
-            p[d] /= z;
-            e += (float)d * p[d];
-        }
-        e *= step;   // hypotheses are `step` quarter pixels apart
-        disp[m] = e;
-        if (dlogits) {
-            float g = 0.0f;
-            const float t = target ? target[m] : -1.0f;
-            if (t >= 0.0f) {
-                const float r = e - t;
-                l = fabsf(r) < 1.0f ? 0.5f * r * r : fabsf(r) - 0.5f;
-                g = (fabsf(r) < 1.0f ? r : copysignf(1.0f, r)) * inv_count;
-            }
-            for (int d = 0; d < CH; d++)
-                dlogits[(size_t)m * CH + d] = __float2bfloat16_rn(-p[d] * (step * (float)d - e) * g);
-        }
+        __align__(16) __nv_bfloat16 v[OUT_CH];
+        for (int c = 0; c < OUT_CH; c++) v[c] = __float2bfloat16_rn(c == 0 ? g0 : c == 1 ? g1 : c == 2 ? g2 : 0.0f);
+        uint4* d = reinterpret_cast<uint4*>(dout + (size_t)m * OUT_CH);
+        d[0] = reinterpret_cast<const uint4*>(v)[0];
+        d[1] = reinterpret_cast<const uint4*>(v)[1];
     }
     red[threadIdx.x] = l;
     __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    for (int s = 128; s > 0; s >>= 1) {
         if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0 && loss_part) loss_part[blockIdx.x] = red[0];
+    if (threadIdx.x == 0 && parts) parts[blockIdx.x] = red[0];
 }
 
-// training target at 1 / sc resolution: mean of the valid (> 0) disparities of each sc x sc block
-// / sc, -1 when fewer than half are valid
-__global__ void k_target(const float* __restrict__ disp, int W, int sc, int W4, int H4, float* __restrict__ out)
+// full-resolution initial disparity and normal map from the network output (W4 x H4 x OUT_CH):
+// bilinear in (d, nx, ny) at ((x + 0.5) / sc - 0.5, (y + 0.5) / sc - 0.5), clamped to the map;
+// disparity d * sc clamped to [0, dmax], normal (nx, ny, sqrt(max(1 - nx^2 - ny^2, 0.01)), 0).
+// right_view: the map is of the mirrored pair, read at the mirrored column, ny negated.
+__global__ void k_upsample(const float* __restrict__ o4, int W4, int H4, int W, int H, int sc, int right_view,
+                           float dmax, float* __restrict__ disp, float4* __restrict__ normal)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= W4) return;
-    float s = 0.0f;
-    int n = 0;
-    for (int j = 0; j < sc; j++)
-        for (int i = 0; i < sc; i++) {
-            const float v = disp[(size_t)(sc * y + j) * W + sc * x + i];
-            if (v > 0.0f) {
-                s += v;
-                n++;
-            }
-        }
-    out[(size_t)y * W4 + x] = 2 * n >= sc * sc ? s / ((float)sc * (float)n) : -1.0f;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const int xs = right_view ? W - 1 - x : x;
+    const float u = fminf(fmaxf(((float)xs + 0.5f) / (float)sc - 0.5f, 0.0f), (float)(W4 - 1));
+    const float v = fminf(fmaxf(((float)y + 0.5f) / (float)sc - 0.5f, 0.0f), (float)(H4 - 1));
+    const int u0 = (int)u, v0 = (int)v;
+    const int u1 = min(u0 + 1, W4 - 1), v1 = min(v0 + 1, H4 - 1);
+    const float a = u - (float)u0, b = v - (float)v0;
+    float r[3];
+    for (int c = 0; c < 3; c++) {
+        const float p00 = o4[((size_t)v0 * W4 + u0) * OUT_CH + c], p01 = o4[((size_t)v0 * W4 + u1) * OUT_CH + c];
+        const float p10 = o4[((size_t)v1 * W4 + u0) * OUT_CH + c], p11 = o4[((size_t)v1 * W4 + u1) * OUT_CH + c];
+        r[c] = (1.0f - b) * ((1.0f - a) * p00 + a * p01) + b * ((1.0f - a) * p10 + a * p11);
+    }
+    const size_t i = (size_t)y * W + x;
+    disp[i] = fminf(fmaxf(r[0] * (float)sc, 0.0f), dmax);
+    if (normal) {
+        const float nx = r[1], ny = right_view ? -r[2] : r[2];
+        normal[i] = make_float4(nx, ny, sqrtf(fmaxf(1.0f - nx * nx - ny * ny, 0.01f)), 0.0f);
+    }
 }
 
-// full-resolution initial disparity: bilinear upsampling of the 1 / sc resolution result, times sc
-__global__ void k_upsample(const float* __restrict__ d4, int W4, int H4, int W, int H, int sc, float* __restrict__ out)
-{
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= W) return;
-    const float inv = 1.0f / (float)sc;
-    const float u = fminf(fmaxf(((float)x + 0.5f) * inv - 0.5f, 0.0f), (float)(W4 - 1));
-    const float v = fminf(fmaxf(((float)y + 0.5f) * inv - 0.5f, 0.0f), (float)(H4 - 1));
-    const int x0 = (int)u, y0 = (int)v, x1 = min(x0 + 1, W4 - 1), y1 = min(y0 + 1, H4 - 1);
-    const float a = u - (float)x0, b = v - (float)y0;
-    const float r0 = (1.0f - a) * d4[(size_t)y0 * W4 + x0] + a * d4[(size_t)y0 * W4 + x1];
-    const float r1 = (1.0f - a) * d4[(size_t)y1 * W4 + x0] + a * d4[(size_t)y1 * W4 + x1];
-    out[(size_t)y * W + x] = (float)sc * ((1.0f - b) * r0 + b * r1);
-}
-
-// Adam on the FP32 master weights of one layer (CH * KTOT weights then CH biases), then the BF16
-// copies: wmat[n][t][c] and the data-gradient matrix wt[c][8 - t][n]
+// Adam on FP32 master parameters (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected)
 __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1, float* __restrict__ m2,
                        int n, float lr, float b1, float b2, float eps, float c1, float c2)
 {
@@ -430,14 +618,18 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
     p[i] -= lr * (a / c1) / (sqrtf(v / c2) + eps);
 }
 
-__global__ void k_weights_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ wmat, __nv_bfloat16* __restrict__ wt)
+// BF16 copies of one layer's weights: wmat[co][t][ci] (forward) and wt[ci][8 - t][co] (data
+// gradient: the transposed, tap-mirrored convolution)
+__global__ void k_weights_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ wmat, __nv_bfloat16* __restrict__ wt,
+                               int CIN, int COUT)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= CH * KTOT) return;
-    const int n = i / KTOT, k = i - n * KTOT, t = k / CH, c = k - t * CH;
+    const int K = 9 * CIN;
+    if (i >= COUT * K) return;
+    const int co = i / K, k = i - co * K, t = k / CIN, ci = k - t * CIN;
     const __nv_bfloat16 v = __float2bfloat16_rn(p[i]);
     wmat[i] = v;
-    wt[(size_t)c * KTOT + (8 - t) * CH + n] = v;
+    if (wt) wt[(size_t)ci * 9 * COUT + (8 - t) * COUT + co] = v;
 }
 
 }  // namespace lpp
@@ -464,171 +656,251 @@ int check_dims(int B, int H4, int W4)
     if (B <= 0 || H4 <= 0 || W4 <= 0 || (long long)B * H4 * W4 > (1ll << 28)) return lfail(PM_EINVAL_SHAPE, "tensor size out of range");
     return PM_OK;
 }
+inline bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+// launch k_conv_tc for a (CIN, COUT) pair that the network has
+template <int CIN, int COUT>
+int conv_tc(int epi, const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, const __nv_bfloat16* mk, void* out,
+            int B, int H, int W, int dil, int* err, cudaStream_t st)
+{
+    constexpr int SM = conv_smem<CIN, COUT>();
+    const int grid = (B * H * W + TM - 1) / TM;
+    if (epi == EPI_RELU_BF16) {
+        cudaFuncSetAttribute(k_conv_tc<CIN, COUT, EPI_RELU_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        k_conv_tc<CIN, COUT, EPI_RELU_BF16><<<grid, TM, SM, st>>>(x, w, bias, mk, out, B, H, W, dil, err);
+    } else if (epi == EPI_BIAS_F32) {
+        cudaFuncSetAttribute(k_conv_tc<CIN, COUT, EPI_BIAS_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        k_conv_tc<CIN, COUT, EPI_BIAS_F32><<<grid, TM, SM, st>>>(x, w, bias, mk, out, B, H, W, dil, err);
+    } else {
+        cudaFuncSetAttribute(k_conv_tc<CIN, COUT, EPI_MASK_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        k_conv_tc<CIN, COUT, EPI_MASK_BF16><<<grid, TM, SM, st>>>(x, w, bias, mk, out, B, H, W, dil, err);
+    }
+    return check_launch("k_conv_tc");
+}
+
+int conv_dispatch(int CIN, int COUT, int epi, const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias,
+                  const __nv_bfloat16* mk, void* out, int B, int H, int W, int dil, int* err, cudaStream_t st)
+{
+#define PM_CONV_CASE(A, Bc) \
+    if (CIN == A && COUT == Bc) return conv_tc<A, Bc>(epi, x, w, bias, mk, out, B, H, W, dil, err, st);
+    PM_CONV_CASE(16, 32) PM_CONV_CASE(32, 32) PM_CONV_CASE(32, 64) PM_CONV_CASE(64, 64) PM_CONV_CASE(64, 32)
+    PM_CONV_CASE(32, 16)
+#undef PM_CONV_CASE
+    return lfail(PM_EINVAL_ARG, "no tensor-core convolution for these channel counts");
+}
+
+template <int CIN, int COUT>
+int wgrad_tc(const __nv_bfloat16* x, const __nv_bfloat16* dy, float* part, float* grad, int B, int H, int W, int dil,
+             int* err, cudaStream_t st)
+{
+    using Sh = WgradShape<CIN, COUT>;
+    const int M = B * H * W, nb = (M + WG_PIX - 1) / WG_PIX;
+    cudaFuncSetAttribute(k_wgrad_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::SMEM);
+    k_wgrad_tc<CIN, COUT><<<nb, 128, Sh::SMEM, st>>>(x, dy, part, B, H, W, dil, err);
+    int rc = check_launch("k_wgrad_tc");
+    if (rc) return rc;
+    const int n = (9 * CIN + 1) * COUT;
+    k_wgrad_sum<<<(n + 255) / 256, 256, 0, st>>>(part, grad, nb, CIN, COUT);
+    return check_launch("k_wgrad_sum");
+}
+
+int check_layer(int l)
+{
+    if (l < 0 || l >= NL) return lfail(PM_EINVAL_ARG, "layer out of range");
+    return PM_OK;
+}
+
+size_t layer_params(int l) { return (size_t)LCOUT[l] * 9 * LCIN[l] + LCOUT[l]; }
+size_t layer_weights(int l) { return (size_t)LCOUT[l] * 9 * LCIN[l]; }
 }  // namespace
 
 extern "C" {
 
 const char* pm_lpp_last_error(void) { return t_lpp_err.c_str(); }
 
-int pm_lpp_channels(void) { return CH; }
+int pm_lpp_layers(void) { return NL; }
 
-int pm_lpp_conv(int epi, int tensor_cores, const void* in, const void* wmat, const float* bias, const void* mask, void* out,
-                int B, int H4, int W4, int* err, void* stream)
+int pm_lpp_layer_shape(int layer, int* cin, int* cout, int* dilation)
 {
-    int rc = check_dims(B, H4, W4);
+    int rc = check_layer(layer);
     if (rc) return rc;
-    if (epi < 0 || epi > 2) return lfail(PM_EINVAL_ARG, "unknown epilogue");
-    if (!in || !wmat || !out || (epi != EPI_MASK_BF16 && !bias) || (epi == EPI_MASK_BF16 && !mask) || (tensor_cores && !err))
+    if (cin) *cin = LCIN[layer];
+    if (cout) *cout = LCOUT[layer];
+    if (dilation) *dilation = LDIL[layer];
+    return PM_OK;
+}
+
+int pm_lpp_conv(int layer, int mode, int tensor_cores, const void* in, const void* w, const float* bias, const void* mask,
+                void* out, int B, int H4, int W4, int* err, void* stream)
+{
+    int rc = check_layer(layer);
+    if (rc) return rc;
+    rc = check_dims(B, H4, W4);
+    if (rc) return rc;
+    if (mode != 0 && mode != 1) return lfail(PM_EINVAL_ARG, "mode must be 0 (forward) or 1 (data gradient)");
+    if (mode == 1 && layer == 0) return lfail(PM_EINVAL_ARG, "the first layer's input has no gradient");
+    const bool last = layer == NL - 1;
+    const int epi = mode == 1 ? EPI_MASK_BF16 : last ? EPI_BIAS_F32 : EPI_RELU_BF16;
+    if (!in || !w || !out || (epi != EPI_MASK_BF16 && !bias) || (epi == EPI_MASK_BF16 && !mask) || (tensor_cores && !err))
         return lfail(PM_EINVAL_ARG, "null buffer");
-    if (((uintptr_t)in | (uintptr_t)wmat | (uintptr_t)out) & 15) return lfail(PM_EINVAL_ARG, "buffers must be 16-byte aligned");
-    const int M = B * H4 * W4;
+    if (!aligned16(in) || !aligned16(w) || !aligned16(out) || (mask && !aligned16(mask)))
+        return lfail(PM_EINVAL_ARG, "buffers must be 16-byte aligned");
+    // forward: CIN -> COUT; data gradient: COUT -> CIN with the transposed weights
+    const int cin = mode ? LCOUT[layer] : LCIN[layer], cout = mode ? LCIN[layer] : LCOUT[layer];
     const auto* x = static_cast<const __nv_bfloat16*>(in);
-    const auto* w = static_cast<const __nv_bfloat16*>(wmat);
+    const auto* wm = static_cast<const __nv_bfloat16*>(w);
     const auto* mk = static_cast<const __nv_bfloat16*>(mask);
-    if (tensor_cores) {
-        cudaFuncSetAttribute(k_conv_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, CONV_SMEM);
-        cudaFuncSetAttribute(k_conv_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, CONV_SMEM);
-        cudaFuncSetAttribute(k_conv_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, CONV_SMEM);
-        const int grid = (M + TM - 1) / TM;
-        if (epi == 0) k_conv_tc<0><<<grid, TM, CONV_SMEM, S(stream)>>>(x, w, bias, mk, out, B, H4, W4, err);
-        else if (epi == 1) k_conv_tc<1><<<grid, TM, CONV_SMEM, S(stream)>>>(x, w, bias, mk, out, B, H4, W4, err);
-        else k_conv_tc<2><<<grid, TM, CONV_SMEM, S(stream)>>>(x, w, bias, mk, out, B, H4, W4, err);
-    } else {
-        const int grid = (M + 127) / 128;
-        if (epi == 0) k_conv_ref<0><<<grid, 128, 0, S(stream)>>>(x, w, bias, mk, out, B, H4, W4);
-        else if (epi == 1) k_conv_ref<1><<<grid, 128, 0, S(stream)>>>(x, w, bias, mk, out, B, H4, W4);
-        else k_conv_ref<2><<<grid, 128, 0, S(stream)>>>(x, w, bias, mk, out, B, H4, W4);
-    }
-    return check_launch("pm_lpp_conv");
+    if (tensor_cores) return conv_dispatch(cin, cout, epi, x, wm, bias, mk, out, B, H4, W4, LDIL[layer], err, S(stream));
+    const long long n = (long long)B * H4 * W4 * cout;
+    const int grid = (int)((n + 255) / 256);
+    if (epi == EPI_RELU_BF16) k_conv_ref<EPI_RELU_BF16><<<grid, 256, 0, S(stream)>>>(x, wm, bias, mk, out, B, H4, W4, LDIL[layer], cin, cout);
+    else if (epi == EPI_BIAS_F32) k_conv_ref<EPI_BIAS_F32><<<grid, 256, 0, S(stream)>>>(x, wm, bias, mk, out, B, H4, W4, LDIL[layer], cin, cout);
+    else k_conv_ref<EPI_MASK_BF16><<<grid, 256, 0, S(stream)>>>(x, wm, bias, mk, out, B, H4, W4, LDIL[layer], cin, cout);
+    return check_launch("k_conv_ref");
 }
 
-size_t pm_lpp_wgrad_scratch_floats(int B, int H4, int W4, int per_block)
+size_t pm_lpp_wgrad_scratch_floats(int layer, int B, int H4, int W4)
 {
-    if (per_block <= 0) return 0;
+    if (layer < 0 || layer >= NL || B <= 0 || H4 <= 0 || W4 <= 0) return 0;
     const long long M = (long long)B * H4 * W4;
-    return (size_t)((M + per_block - 1) / per_block) * (CH * KTOT + CH);
+    return (size_t)((M + WG_PIX - 1) / WG_PIX) * (9 * LCIN[layer] + 1) * LCOUT[layer];
 }
 
-int pm_lpp_wgrad(const void* x, const void* dy, float* scratch, float* grad, int B, int H4, int W4, int per_block, void* stream)
+int pm_lpp_wgrad(int layer, int tensor_cores, const void* x, const void* dy, float* scratch, float* grad, int B, int H4,
+                 int W4, int* err, void* stream)
 {
-    int rc = check_dims(B, H4, W4);
+    int rc = check_layer(layer);
     if (rc) return rc;
-    if (!x || !dy || !scratch || !grad || per_block <= 0) return lfail(PM_EINVAL_ARG, "bad argument");
-    const int M = B * H4 * W4, nb = (M + per_block - 1) / per_block;
-    k_wgrad_part<<<nb, KTOT, 0, S(stream)>>>(static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy),
-                                              scratch, B, H4, W4, per_block);
-    k_wgrad_sum<<<(CH * KTOT + CH + 255) / 256, 256, 0, S(stream)>>>(scratch, grad, nb);
-    return check_launch("pm_lpp_wgrad");
+    rc = check_dims(B, H4, W4);
+    if (rc) return rc;
+    if (!x || !dy || !grad || (tensor_cores && (!scratch || !err))) return lfail(PM_EINVAL_ARG, "null buffer");
+    if (!aligned16(x) || !aligned16(dy) || (scratch && !aligned16(scratch)))
+        return lfail(PM_EINVAL_ARG, "buffers must be 16-byte aligned");
+    const auto* xb = static_cast<const __nv_bfloat16*>(x);
+    const auto* db = static_cast<const __nv_bfloat16*>(dy);
+    const int dil = LDIL[layer], cin = LCIN[layer], cout = LCOUT[layer];
+    if (!tensor_cores) {
+        const int n = (9 * cin + 1) * cout;
+        k_wgrad_ref<<<(n + 127) / 128, 128, 0, S(stream)>>>(xb, db, grad, B, H4, W4, dil, cin, cout);
+        return check_launch("k_wgrad_ref");
+    }
+#define PM_WG_CASE(A, Bc) \
+    if (cin == A && cout == Bc) return wgrad_tc<A, Bc>(xb, db, scratch, grad, B, H4, W4, dil, err, S(stream));
+    PM_WG_CASE(16, 32) PM_WG_CASE(32, 32) PM_WG_CASE(32, 64) PM_WG_CASE(64, 64) PM_WG_CASE(64, 32) PM_WG_CASE(32, 16)
+#undef PM_WG_CASE
+    return lfail(PM_EINVAL_ARG, "no tensor-core weight gradient for these channel counts");
 }
 
-int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view, int step,
-                    int scale, float* grey_scratch, void* out, void* stream)
+int pm_lpp_input(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int scale, int right_view,
+                 void* out, void* stream)
 {
-    if (scale != 2 && scale != 4) return lfail(PM_EINVAL_ARG, "scale must be 2 or 4");
-    if (W < scale || H < scale || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
-    if (!left || !right || !grey_scratch || !out || stride < (size_t)W * 4 || stride % 4) return lfail(PM_EINVAL_ARG, "bad argument");
+    if (!left || !right || !out) return lfail(PM_EINVAL_ARG, "null buffer");
+    if (scale < 1 || W < scale || H < scale || stride < (size_t)W * 4) return lfail(PM_EINVAL_SHAPE, "bad image size or scale");
+    if (!aligned16(out)) return lfail(PM_EINVAL_ARG, "output must be 16-byte aligned");
     const int W4 = W / scale, H4 = H / scale;
-    const dim3 g((W4 + 127) / 128, H4);
-    k_grey<<<g, 128, 0, S(stream)>>>(left, stride, scale, W4, H4, grey_scratch);
-    k_grey<<<g, 128, 0, S(stream)>>>(right, stride, scale, W4, H4, grey_scratch + (size_t)W4 * H4);
-    float* g0 = grey_scratch;
-    float* g1 = grey_scratch + (size_t)W4 * H4;
-    if (step < 1 || step > 8) return lfail(PM_EINVAL_ARG, "hypothesis step out of range");
-    if (right_view) k_costvol<<<g, 128, 0, S(stream)>>>(g1, g0, W4, H4, step, static_cast<__nv_bfloat16*>(out));
-    else k_costvol<<<g, 128, 0, S(stream)>>>(g0, g1, W4, H4, -step, static_cast<__nv_bfloat16*>(out));
-    return check_launch("pm_lpp_features");
+    const dim3 b(16, 16), g((W4 + 15) / 16, (H4 + 15) / 16);
+    k_input<<<g, b, 0, S(stream)>>>(left, right, stride, W, scale, W4, H4, right_view, static_cast<__nv_bfloat16*>(out));
+    return check_launch("k_input");
 }
 
-int pm_lpp_softargmin(const float* logits, const void* feats, float skip, float step, const float* target, float* disp,
-                      void* dlogits, float* loss_part, int M, float inv_count, void* stream)
+int pm_lpp_target(const float* planes, const float* other, int W, int H, int scale, int right_view, float dmax,
+                  float* out, void* stream)
 {
-    if (M <= 0 || !logits || !disp || !(step > 0.0f)) return lfail(PM_EINVAL_ARG, "bad argument");
-    k_softargmin<<<(M + 255) / 256, 256, 0, S(stream)>>>(logits, static_cast<const __nv_bfloat16*>(feats), skip, step, target,
-                                                          disp,
-                                                          static_cast<__nv_bfloat16*>(dlogits), loss_part, M, inv_count);
-    return check_launch("pm_lpp_softargmin");
-}
-
-int pm_lpp_target(const float* disp, int W, int H, int scale, float* out, void* stream)
-{
-    if ((scale != 2 && scale != 4) || W < scale || H < scale || !disp || !out) return lfail(PM_EINVAL_ARG, "bad argument");
+    if (!planes || !other || !out) return lfail(PM_EINVAL_ARG, "null buffer");
+    if (scale < 1 || W < scale || H < scale) return lfail(PM_EINVAL_SHAPE, "bad image size or scale");
     const int W4 = W / scale, H4 = H / scale;
-    k_target<<<dim3((W4 + 127) / 128, H4), 128, 0, S(stream)>>>(disp, W, scale, W4, H4, out);
-    return check_launch("pm_lpp_target");
+    const dim3 b(16, 16), g((W4 + 15) / 16, (H4 + 15) / 16);
+    k_target<<<g, b, 0, S(stream)>>>(reinterpret_cast<const float4*>(planes), reinterpret_cast<const float4*>(other), W,
+                                     scale, W4, H4, right_view, dmax, reinterpret_cast<float4*>(out));
+    return check_launch("k_target");
 }
 
-int pm_lpp_upsample(const float* d4, int W4, int H4, int W, int H, int scale, float* out, void* stream)
+int pm_lpp_loss(const float* out, const float* target, float wn, float scale, int M, void* dout, float* parts, void* stream)
 {
-    if (W4 <= 0 || H4 <= 0 || W <= 0 || H <= 0 || scale < 1 || !d4 || !out) return lfail(PM_EINVAL_ARG, "bad argument");
-    k_upsample<<<dim3((W + 127) / 128, H), 128, 0, S(stream)>>>(d4, W4, H4, W, H, scale, out);
-    return check_launch("pm_lpp_upsample");
+    if (!out || !target || !dout) return lfail(PM_EINVAL_ARG, "null buffer");
+    if (M <= 0) return lfail(PM_EINVAL_SHAPE, "no pixels");
+    if (!aligned16(dout) || !aligned16(target)) return lfail(PM_EINVAL_ARG, "buffers must be 16-byte aligned");
+    k_loss<<<(M + 255) / 256, 256, 0, S(stream)>>>(out, reinterpret_cast<const float4*>(target), wn, scale, M,
+                                                  static_cast<__nv_bfloat16*>(dout), parts);
+    return check_launch("k_loss");
+}
+
+int pm_lpp_upsample(const float* o4, int W4, int H4, int W, int H, int scale, int right_view, float dmax, float* disp,
+                    float* normal, void* stream)
+{
+    if (!o4 || !disp) return lfail(PM_EINVAL_ARG, "null buffer");
+    if (W4 < 1 || H4 < 1 || W < 1 || H < 1 || scale < 1) return lfail(PM_EINVAL_SHAPE, "bad size");
+    const dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
+    k_upsample<<<g, b, 0, S(stream)>>>(o4, W4, H4, W, H, scale, right_view, dmax, disp, reinterpret_cast<float4*>(normal));
+    return check_launch("k_upsample");
 }
 
 int pm_lpp_adam(float* p, const float* g, float* m1, float* m2, int n, float lr, int step, void* stream)
 {
-    if (n <= 0 || step <= 0 || !p || !g || !m1 || !m2) return lfail(PM_EINVAL_ARG, "bad argument");
+    if (!p || !g || !m1 || !m2 || n <= 0 || step < 1) return lfail(PM_EINVAL_ARG, "bad argument");
     const float b1 = 0.9f, b2 = 0.999f;
-    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
-    k_adam<<<(n + 255) / 256, 256, 0, S(stream)>>>(p, g, m1, m2, n, lr, b1, b2, 1e-8f, c1, c2);
-    return check_launch("pm_lpp_adam");
+    k_adam<<<(n + 255) / 256, 256, 0, S(stream)>>>(p, g, m1, m2, n, lr, b1, b2, 1e-8f, 1.0f - powf(b1, (float)step),
+                                                  1.0f - powf(b2, (float)step));
+    return check_launch("k_adam");
 }
 
-int pm_lpp_weights_bf16(const float* p, void* wmat, void* wt, void* stream)
+int pm_lpp_weights_bf16(int layer, const float* p, void* wmat, void* wt, void* stream)
 {
-    if (!p || !wmat || !wt) return lfail(PM_EINVAL_ARG, "bad argument");
-    k_weights_bf16<<<(CH * KTOT + 255) / 256, 256, 0, S(stream)>>>(p, static_cast<__nv_bfloat16*>(wmat),
-                                                                    static_cast<__nv_bfloat16*>(wt));
-    return check_launch("pm_lpp_weights_bf16");
+    int rc = check_layer(layer);
+    if (rc) return rc;
+    if (!p || !wmat) return lfail(PM_EINVAL_ARG, "null buffer");
+    const int n = (int)layer_weights(layer);
+    k_weights_bf16<<<(n + 255) / 256, 256, 0, S(stream)>>>(p, static_cast<__nv_bfloat16*>(wmat),
+                                                          static_cast<__nv_bfloat16*>(wt), LCIN[layer], LCOUT[layer]);
+    return check_launch("k_weights_bf16");
+}
+
+size_t pm_lpp_param_count(void)
+{
+    size_t n = 0;
+    for (int l = 0; l < NL; l++) n += layer_params(l);
+    return n;
 }
 
 size_t pm_lpp_propose_workspace_bytes(int W, int H, int scale)
 {
-    if ((scale != 2 && scale != 4) || W < scale || H < scale) return 0;
-    const size_t M = (size_t)(W / scale) * (H / scale);
-    // two grey planes, the features and two BF16 activation buffers, FP32 logits, the quarter
-    // disparity
-    return 2 * M * 4 + 3 * M * CH * 2 + M * CH * 4 + M * 4 + 6 * 256;
+    if (scale < 1 || W < scale || H < scale) return 0;
+    const size_t px = (size_t)(W / scale) * (H / scale);
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    return up(px * IN_CH * 2) + 2 * up(px * MAX_CH * 2) + up(px * OUT_CH * 4);
 }
 
-int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, int step, int scale,
-                          const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view,
-                          float* initdisp, void* workspace, size_t ws_bytes, int* err, void* stream)
+// wall: the BF16 weight matrices of all layers back to back (wmat layout, each starting at a
+// 16-byte boundary: layer sizes are multiples of 8 elements); ball: all biases back to back
+int pm_lpp_propose_device(const void* wall, const float* ball, int scale, const uint8_t* left, const uint8_t* right, int W,
+                          int H, size_t stride, int right_view, float dmax, float* disp, float* normal, void* ws,
+                          size_t ws_bytes, int* err, void* stream)
 {
-    if (scale != 2 && scale != 4) return lfail(PM_EINVAL_ARG, "scale must be 2 or 4");
-    if (W < scale || H < scale || W > PM_MAX_WIDTH || H > PM_MAX_HEIGHT) return lfail(PM_EINVAL_SHAPE, "image size out of range");
-    if (!wmats || !biases || nlayers < 1 || !left || !right || !initdisp || !workspace || !err)
-        return lfail(PM_EINVAL_ARG, "null argument");
-    if (ws_bytes < pm_lpp_propose_workspace_bytes(W, H, scale)) return lfail(PM_EINVAL_ARG, "workspace too small");
-    if (((uintptr_t)workspace | (uintptr_t)wmats) & 255) return lfail(PM_EINVAL_ARG, "workspace and weights must be 256-byte aligned");
+    if (!wall || !ball || !left || !right || !disp || !ws || !err) return lfail(PM_EINVAL_ARG, "null buffer");
+    if (!aligned16(wall) || ((uintptr_t)ws & 255)) return lfail(PM_EINVAL_ARG, "weights 16-byte, workspace 256-byte aligned");
+    const size_t need = pm_lpp_propose_workspace_bytes(W, H, scale);
+    if (!need || ws_bytes < need) return lfail(PM_EINVAL_ARG, "workspace too small (pm_lpp_propose_workspace_bytes)");
     const int W4 = W / scale, H4 = H / scale;
-    const size_t M = (size_t)W4 * H4;
-    char* ws = static_cast<char*>(workspace);
-    float* grey = reinterpret_cast<float*>(ws);
-    size_t off = (2 * M * 4 + 255) & ~(size_t)255;
-    __nv_bfloat16* feats = reinterpret_cast<__nv_bfloat16*>(ws + off);
-    off += (M * CH * 2 + 255) & ~(size_t)255;
-    __nv_bfloat16* act[2] = {reinterpret_cast<__nv_bfloat16*>(ws + off), nullptr};
-    off += (M * CH * 2 + 255) & ~(size_t)255;
-    act[1] = reinterpret_cast<__nv_bfloat16*>(ws + off);
-    off += (M * CH * 2 + 255) & ~(size_t)255;
-    float* logits = reinterpret_cast<float*>(ws + off);
-    off += (M * CH * 4 + 255) & ~(size_t)255;
-    float* d4 = reinterpret_cast<float*>(ws + off);
-    int rc = pm_lpp_features(left, right, W, H, stride, right_view, step, scale, grey, feats, stream);
+    const size_t px = (size_t)W4 * H4;
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    uint8_t* p = static_cast<uint8_t*>(ws);
+    void* x0 = p;
+    void* act[2] = {p + up(px * IN_CH * 2), p + up(px * IN_CH * 2) + up(px * MAX_CH * 2)};
+    float* o4 = reinterpret_cast<float*>(p + up(px * IN_CH * 2) + 2 * up(px * MAX_CH * 2));
+    int rc = pm_lpp_input(left, right, W, H, stride, scale, right_view, x0, stream);
     if (rc) return rc;
-    const auto* w = static_cast<const __nv_bfloat16*>(wmats);
-    const __nv_bfloat16* x = feats;
-    for (int l = 0; l < nlayers; l++) {
-        const bool last = l == nlayers - 1;
-        void* y = last ? static_cast<void*>(logits) : static_cast<void*>(act[l & 1]);
-        rc = pm_lpp_conv(last ? EPI_BIAS_F32 : EPI_RELU_BF16, 1, x, w + (size_t)l * CH * KTOT, biases + l * CH, nullptr, y, 1,
-                         H4, W4, err, stream);
+    const auto* w = static_cast<const __nv_bfloat16*>(wall);
+    const float* b = ball;
+    const void* cur = x0;
+    for (int l = 0; l < NL; l++) {
+        void* dst = l == NL - 1 ? static_cast<void*>(o4) : act[l & 1];
+        rc = pm_lpp_conv(l, 0, 1, cur, w, b, nullptr, dst, 1, H4, W4, err, stream);
         if (rc) return rc;
-        x = act[l & 1];
+        w += layer_weights(l);
+        b += LCOUT[l];
+        cur = dst;
     }
-    rc = pm_lpp_softargmin(logits, feats, skip, (float)step, nullptr, d4, nullptr, nullptr, (int)M, 0.0f, stream);
-    if (rc) return rc;
-    return pm_lpp_upsample(d4, W4, H4, W, H, scale, initdisp, stream);
+    return pm_lpp_upsample(o4, W4, H4, W, H, scale, right_view, dmax, disp, normal, stream);
 }
 
 }  // extern "C"

@@ -58,8 +58,13 @@ template <bool F>
 __device__ __forceinline__ float2 lerp2(float2 a2, float2 b2, float2 t0, float2 t1)
 {
     if (F) return __ffma2_rn(a2, t1, __fmul2_rn(b2, t0));
+#if PM_STRICT_FMUL2
+    const float2 p0 = __fmul2_rn(b2, t0), p1 = __fmul2_rn(a2, t1);
+    return make_float2(__fadd_rn(p0.x, p1.x), __fadd_rn(p0.y, p1.y));
+#else
     return make_float2(__fadd_rn(__fmul_rn(b2.x, t0.x), __fmul_rn(a2.x, t1.x)),
                        __fadd_rn(__fmul_rn(b2.y, t0.y), __fmul_rn(a2.y, t1.y)));
+#endif
 }
 
 // one texel: colour (r, g, b, w) and gradient (4 components)
@@ -157,17 +162,33 @@ __device__ __forceinline__ float ad_sum(float4 v2, float4 ref)
 // 0.33f is exact, and scaling by a power of two commutes with rounding
 #define PM_K033_8 0.04125000163912773f
 
+// Per-sample weights of a Gauss-Newton window sample for klt_cost: k1 = w1 * 0.125 * 0.33
+// (one multiply, see PM_K033_8) and the census weight x = w1 * 0.875f.
+struct KltWeights {
+    float k1, x;
+};
+
+template <bool F>
+__device__ __forceinline__ KltWeights klt_weights(float w1)
+{
+    KltWeights k;
+    k.k1 = w1 * PM_K033_8;
+    k.x = F ? w1 * 0.21875f : w1 * 0.875f;
+    return k;
+}
+
 // the cost of one Gauss-Newton tap from its interpolated texel (:361-370).
 // `w1 * (1.0f - alpha) * 0.25 * (float)cnt` (:370) carries a double literal, so the sum is a
 // double-precision one rounded once: formed exactly in double (strict) or with one fma
-// (fused); w1 * 0.875f * 0.25f is one multiply by 0.21875 for the same reason as above.
+// (fused; w1 * 0.875f * 0.25f is one multiply by 0.21875 for the same reason as above).  FP64
+// runs at half the FP32 rate on B200, so the strict form costs about as much as a guarded fma.
 template <bool F, bool CHK>
-__device__ __forceinline__ float klt_cost(float k1, float w1, float4 val1, uint32_t sb1, const Texel& t)
+__device__ __forceinline__ float klt_cost(const KltWeights& kw, float4 val1, uint32_t sb1, const Texel& t)
 {
-    float C = k1 * ad_sum<CHK>(t.c, val1);
+    float C = kw.k1 * ad_sum<CHK>(t.c, val1);
     const int n = sign_mismatch(sb1, sign_bytes(t.g));
-    if (F) C = fmaf(w1 * 0.21875f, (float)n, C);
-    else C = (float)((double)C + (double)(w1 * 0.875f) * 0.25 * (double)(float)n);
+    if (F) C = fmaf(kw.x, (float)n, C);
+    else C = (float)((double)C + (double)kw.x * 0.25 * (double)(float)n);
     return C;
 }
 
@@ -313,7 +334,7 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
             const float4 val1 = make_float4(q.x - c1.x, q.y - c1.y, q.z - c1.z, 0.0f);
             const float w1 = support_weight<F>(val1.x, val1.y, val1.z);
             const uint32_t sb1 = __float_as_uint(q.w);
-            const float k1 = w1 * PM_K033_8;
+            const KltWeights kw = klt_weights<F>(w1);
             const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
             // Common case: 1 <= p2x < W - 1 and p2x + 1.5 in the binade of p2x.  Then p2x is a
             // multiple of its ulp (<= 0.5), every +-1 and +-0.5 below is exact, the three taps'
@@ -342,13 +363,13 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
                 const Texel tA = texel_at(b, plane), tB = texel_at(b + 1, plane);
                 const Texel tC = texel_at(b + 2, plane), tD = texel_at(b + 3, plane);
                 const float b0 = 1.0f - a0;
-                Cxm = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tA, tB));
-                C = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tB, tC));
-                Cxp = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel<F>(a0, b0, tC, tD));
+                Cxm = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel<F>(a0, b0, tA, tB));
+                C = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel<F>(a0, b0, tB, tC));
+                Cxp = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel<F>(a0, b0, tC, tD));
             } else {
-                Cxm = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + -1.0f) + 0.5f));
-                C = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, p2x + 0.5f));
-                Cxp = klt_cost<F, CHK>(k1, w1, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + 1.0f) + 0.5f));
+                Cxm = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + -1.0f) + 0.5f));
+                C = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel_at<F>(row2, plane, W, p2x + 0.5f));
+                Cxp = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + 1.0f) + 0.5f));
             }
             if (COUNT) cnt.klt++;
             // the update of :394-402 without a branch: a rejected sample adds exact zeros, and

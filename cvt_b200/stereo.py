@@ -28,7 +28,7 @@ def _is_torch(x):
 class PMHuberStereo:
     """Slanted-plane PatchMatch stereo with ROF-coupled smoothing on one B200."""
 
-    def __init__(self, views=2, fused=True, device=0, thetamin=1e-4, maxdispdiff=1.0, maxanglediff=5.0,
+    def __init__(self, views=2, fused=False, device=0, thetamin=1e-4, maxdispdiff=1.0, maxanglediff=5.0,
                  rof_iters=40, use_graph=True, levels=1):
         L = _lib.lib()
         opt = _lib.Options()
@@ -79,14 +79,16 @@ class PMHuberStereo:
         return {p: (float(ms[i]), int(n[i])) for i, p in enumerate(self.PHASES)}
 
     def disparity_map(self, left, right, patchsize, disparitymax, iterations, pp=PP_LRCHECK, normalmap=False,
-                      initdisparity=None, initnormalmap=None, planes=False, stream=None, initdisparity_right=None):
+                      initdisparity=None, initnormalmap=None, planes=False, stream=None, initdisparity_right=None,
+                      initnormalmap_right=None):
         """Returns dmap, or a dict {dmap, normal?, planes_left?, planes_right?} when
         normalmap or planes is requested.  left/right: (H, W, 4) uint8.  initdisparity_right
-        (CUDA tensors only, without initnormalmap) also starts the right view from a disparity,
-        as disparityMapAll allows (pm_disparity_map_init2_device)."""
+        (CUDA tensors only) also starts the right view from a disparity and, with
+        initnormalmap_right, a normal map, as disparityMapAll allows
+        (pm_disparity_map_init2_device)."""
         if initdisparity_right is not None:
             return self._device(left, right, patchsize, disparitymax, iterations, pp, normalmap, initdisparity,
-                                initnormalmap, planes, stream, None, initdisparity_right)
+                                initnormalmap, planes, stream, None, initdisparity_right, initnormalmap_right)
         return self._run(None, left, right, patchsize, disparitymax, iterations, pp, normalmap, initdisparity,
                          initnormalmap, planes, stream)
 
@@ -173,7 +175,7 @@ class PMHuberStereo:
         return [{"dmap": d, "planes_left": a, "planes_right": b} for d, a, b in zip(dm, pl, pr)]
 
     def _device(self, left, right, patchsize, dmax, iterations, pp, normalmap, initd, initn, planes, stream,
-                dscale=None, initd_right=None):
+                dscale=None, initd_right=None, initn_right=None):
         import torch
 
         L = _lib.lib()
@@ -195,12 +197,13 @@ class PMHuberStereo:
             return None if t is None else t.data_ptr()
 
         if initd_right is not None:
-            if not _is_torch(left) or initn is not None:
-                raise StereoError(_lib.PM_EINVAL_ARG, "initdisparity_right: CUDA tensors, no initnormalmap")
+            if not _is_torch(left):
+                raise StereoError(_lib.PM_EINVAL_ARG, "initdisparity_right: CUDA tensors only")
             ir = initd_right.contiguous().float()
+            inr = None if initn_right is None else initn_right.contiguous().float()
             _lib.check(L.pm_disparity_map_init2_device(self._h, p(left), p(right), W, H, W * 4, int(patchsize), float(dmax),
-                                                       int(iterations), int(pp), p(dmap), p(nmap), p(initd), p(ir), p(pl),
-                                                       p(pr), st), self._h)
+                                                       int(iterations), int(pp), p(dmap), p(nmap), p(initd), p(ir),
+                                                       p(initn), p(inr), p(pl), p(pr), st), self._h)
         elif dscale is None:
             _lib.check(L.pm_disparity_map_device(self._h, p(left), p(right), W, H, W * 4, int(patchsize), float(dmax),
                                                  int(iterations), int(pp), p(dmap), p(nmap), p(initd), p(initn), p(pl),

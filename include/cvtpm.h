@@ -55,7 +55,9 @@ enum { PM_MAX_WIDTH = 4096, PM_MAX_HEIGHT = 4096, PM_MAX_RADIUS = 32 };
 
 typedef struct pm_options {
     int views;           /* 2: both views, as the reference (default); 1: left view only (pp must be NONE) */
-    int fused;           /* 1 (default): window loops contract a*b+c into fma; 0: every op rounds separately */
+    int fused;           /* 0 (default): every operation rounds separately, in the reference kernels' order
+                            (bit-exact with them); 1: the window loops contract a*b+c into fma (faster,
+                            results differ from the reference in the last bits and then diverge) */
     float thetamin;      /* 1e-4 (PMHuberStereo.cpp:92) */
     float maxdispdiff;   /* 1.0 px (PMHuberStereo.cpp:79) */
     float maxanglediff;  /* 5.0 degrees (PMHuberStereo.cpp:80) */
@@ -99,13 +101,17 @@ int pm_disparity_map_device(pm_handle* h, const uint8_t* left, const uint8_t* ri
 
 /* As pm_disparity_map_device with an initial disparity for each view, as disparityMapAll takes
  * them (PMHuberStereo.cpp:406-581, :469-483; disparityMap passes the right one as NULL): the
- * right view's disparity is positive, its match in the left image at x + d.  Either may be NULL;
- * the normals come from the disparities (pmhstereo_disparity_to_normal).  One pyramid level and
- * both views. */
+ * right view's disparity is positive, its match in the left image at x + d.  Either may be NULL.
+ * initnormal_left / initnormal_right (float4 per pixel, nullable): the views' initial normals,
+ * as disparityMapAll's initnormalleft / initnormalright; where NULL they come from the
+ * disparities (pmhstereo_disparity_to_normal).  For the right view, nx / nz and ny / nz are the
+ * x- and y-slopes of its disparity (pmhstereo_init_disparity_normal, pmhstereo.cl:816-819).  One
+ * pyramid level and both views. */
 int pm_disparity_map_init2_device(pm_handle* h, const uint8_t* left, const uint8_t* right, int width, int height,
                                   size_t stride, int patchsize, float dispmax, int iterations, int pp, float* dmap,
                                   float* normalmap, const float* initdisp_left, const float* initdisp_right,
-                                  float* planes_left, float* planes_right, void* stream);
+                                  const float* initnormal_left, const float* initnormal_right, float* planes_left,
+                                  float* planes_right, void* stream);
 
 /* PMHuberStereo::depthMap (PMHuberStereo.cpp:145-347), the Huber-smoothed variant: its kernels
  * read the images themselves as colour, the diffusion tensors use alpha 12, each iteration
@@ -165,6 +171,15 @@ int pm_set_batch_branches(pm_handle* h, int n);
  * placed, lowest index among equals) over min(n, branches) branches */
 int pm_batch_schedule(int n, int branches, const int* width, const int* height, const int* patchsize, int* order,
                       int* owner);
+/* the split of a batch over `ranks` processes, one GPU each (pairs are independent: no
+ * collective on the data path), host only: rank_of[i] = the rank of pair i, chosen longest
+ * processing time first by the work W*H*(2r+1)^2*dispmax (pairs in decreasing work, stable,
+ * each to the least loaded rank, the lowest index among equals); load[r] (nullable) = the
+ * work given to rank r.  The reference runs one pair per call on one device and has no
+ * counterpart (cvt/cl/OpenCL.cpp:30-45, a single global queue). */
+enum { PM_MAX_RANKS = 1024 };
+int pm_batch_partition(int n, int ranks, const int* width, const int* height, const int* patchsize,
+                       const float* dispmax, int* rank_of, double* load);
 
 /* ---- per-kernel entry points (device pointers, enqueued on `stream`) ----------------
  * These expose each reference kernel on injected state for parity testing. */
@@ -197,7 +212,8 @@ int pm_k_normal_depth(float* out, const float* planes, int width, int height, fl
                       void* stream);
 /* PDOptCL::denoiseDiffusionTensorROF_PDD (PDOptCL.cpp:1114-1168): `iters` steps of
  * PDDROFDiffTensor (PDDROFDiffTensor.cl:43-127) from u = input, p = q = 0.
- * scratch: device buffer of pm_rof_scratch_bytes(width, height) bytes. */
+ * scratch: device buffer of pm_rof_scratch_bytes(width, height) bytes; iters < 0 returns
+ * PM_EINVAL_ARG. */
 size_t pm_rof_scratch_bytes(int width, int height);
 int pm_k_rof(float* out, const float* input, const float* dt, const float lambda[4], int iters, int width,
              int height, void* scratch, void* stream);
@@ -209,9 +225,13 @@ int pm_k_rof(float* out, const float* input, const float* dt, const float lambda
  * that only passes image pointers and has no device allocator to make a scratch
  * buffer, or a loop under a fixed device-memory budget that must not stall other
  * streams behind cudaMalloc/cudaFree.  Results equal pm_k_rof's.
- * - The first call on each device (the device current at the call) looks up the
- *   array's address; make that first call before any stream capture begins.
- * - width*height > PM_ROF_STATIC_MAX_PIXELS returns PM_EINVAL_SHAPE with a message.
+ * - The first call in each CUDA context (the context current at the call) looks up
+ *   the array's address in that context; make that first call before any stream
+ *   capture begins.  A first call while `stream` is being captured returns
+ *   PM_EINVAL_ARG with a message.  After cudaDeviceReset the next call looks it up
+ *   again in the new context.
+ * - width*height > PM_ROF_STATIC_MAX_PIXELS returns PM_EINVAL_SHAPE with a message;
+ *   iters < 0 returns PM_EINVAL_ARG.
  * - All calls share one array: calls in flight at the same time (two streams, two
  *   host threads) race; serialise them. */
 #define PM_ROF_STATIC_MAX_PIXELS 262144
@@ -375,55 +395,73 @@ int pm_k_svpm_prop(float* out, float* pout, const float* in, const float* pin, c
 int pm_k_svpm_to_flow(float* flow, const float* states, int W, int H, void* stream);
 
 /* ---- learned plane proposal (cvt_b200/csrc/pm_learn.cu) -----------------------------
- * A small BF16 CNN at a quarter or half of the image resolution whose output replaces the
- * random initialisation of disparityMap through its initdisp argument
- * (pmhstereo_init_disparity_normal, pmhstereo.cl:802-828): a 32-hypothesis cost volume of
- * block grey values, six 3x3 convolutions of 32 channels (ReLU after the first five),
- * soft-argmin over the 32 logits plus a fixed multiple of the cost volume, bilinear upsampling
- * to full resolution.  Activations are NHWC BF16 (batch, rows, columns, 32); a layer's
- * weights wmat[n][t][c] (output channel, tap t = (dy + 1) * 3 + (dx + 1), input channel), 32 * 288
- * BF16, and 32 FP32 biases.  The convolution runs on the tensor cores (tcgen05, FP32
- * accumulation) or, for checking, on the CUDA cores (tensor_cores = 0).  `err` (device int) is
- * set when a bounded wait inside a tensor-core kernel runs out.  Errors: a status code, the
- * message in pm_lpp_last_error().  All entry points enqueue on `stream`. */
-int pm_lpp_channels(void);
+ * A BF16 CNN at 1 / scale of the image resolution (W4 = W / scale, H4 = H / scale, "feature
+ * pixels") whose per-pixel (disparity, nx, ny) replaces the random initialisation of
+ * disparityMap through its initdisparity and initnormalmap arguments
+ * (pmhstereo_init_disparity_normal, pmhstereo.cl:802-828).  Input: the left and right RGB as
+ * 16 BF16 channels (6 used); 8 layers of 3x3 convolutions, channels 16 -> 32 -> 32 -> 64 ->
+ * 64 -> 64 -> 64 -> 32 -> 16 (3 used), dilations 1, 1, 2, 4, 8, 16, 1, 1, ReLU after the first
+ * seven (pm_lpp_layer_shape).  Activations are NHWC BF16 (batch, rows, columns, channels);
+ * layer l's parameters are COUT * 9 * CIN weights w[co][t][ci] (tap t = (dy + 1) * 3 + (dx + 1)
+ * in units of the dilation) then COUT biases, FP32 masters with BF16 copies.  Convolutions
+ * and weight gradients run on the tensor cores (tcgen05, FP32 accumulation) or, for checking,
+ * on the CUDA cores (tensor_cores = 0).  `err` (device int) is set when a bounded wait inside
+ * a tensor-core kernel runs out.  Errors: a status code, the message in pm_lpp_last_error().
+ * All entry points enqueue on `stream`.  The reference has no learned component; this is the
+ * initdisparity / initnormalmap producer north of its init kernel. */
 const char* pm_lpp_last_error(void);
-/* cost-volume features of a pair at 1 / scale of its resolution (scale 2 or 4; W4 = W / scale,
- * H4 = H / scale, "feature pixels") for the left view (right_view 0: channel d compares left x
- * with right x - step d) or the right view (1: right x with left x + step d), hypotheses `step`
- * (1..8) feature pixels apart: grey_scratch 2 * W4 * H4 floats, out W4 * H4 * 32 BF16 */
-int pm_lpp_features(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view, int step,
-                    int scale, float* grey_scratch, void* out, void* stream);
-/* one convolution over a batch of B activation maps; epi 0: + bias, ReLU, BF16 out; 1: + bias,
- * FP32 out (logits); 2: data gradient: times (mask > 0), BF16 out (wmat then holds the transposed,
- * mirrored weights wt[c][8 - t][n] = w[n][t][c]) */
-int pm_lpp_conv(int epi, int tensor_cores, const void* in, const void* wmat, const float* bias, const void* mask, void* out,
-                int B, int H4, int W4, int* err, void* stream);
-/* weight and bias gradients of a convolution (32 * 288 then 32 floats), from its input x and the
- * gradient dy of its output, summed over blocks of `per_block` pixels and then over the blocks
- * in order (deterministic) */
-size_t pm_lpp_wgrad_scratch_floats(int B, int H4, int W4, int per_block);
-int pm_lpp_wgrad(const void* x, const void* dy, float* scratch, float* grad, int B, int H4, int W4, int per_block, void* stream);
-/* soft-argmin of M x 32 logits plus skip times the features (the cost volume; NULL: none) into
- * disparities (feature pixels; hypotheses `step` feature pixels apart); with dlogits, also the smooth-L1 loss against target (< 0:
- * ignored), its gradient times inv_count (BF16) and per-256-pixel loss sums in loss_part */
-int pm_lpp_softargmin(const float* logits, const void* feats, float skip, float step, const float* target, float* disp,
-                      void* dlogits, float* loss_part, int M, float inv_count, void* stream);
-/* training target: the mean of the positive disparities of each scale x scale block, in feature
- * pixels (-1 where fewer than half are positive) */
-int pm_lpp_target(const float* disp, int W, int H, int scale, float* out, void* stream);
-/* bilinear upsampling of a 1 / scale resolution disparity, times scale */
-int pm_lpp_upsample(const float* d4, int W4, int H4, int W, int H, int scale, float* out, void* stream);
+int pm_lpp_layers(void);
+int pm_lpp_layer_shape(int layer, int* cin, int* cout, int* dilation);
+/* total FP32 parameters of all layers (weights then biases per layer, layer after layer) */
+size_t pm_lpp_param_count(void);
+/* the network's input for a pair (RGBA8 rows of `stride` bytes): W4 * H4 * 16 BF16, channels
+ * 0-5 = the first and second view's RGB block means of k / 255 minus 0.5.  right_view 0: left
+ * then right; 1: the mirrored pair (right image flipped left-right first), whose output is the
+ * right view's proposal */
+int pm_lpp_input(const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int scale, int right_view,
+                 void* out, void* stream);
+/* one convolution of layer `layer` over a batch of B maps.  mode 0 (forward): + bias, ReLU, BF16
+ * out (the last layer: + bias, FP32 out); mode 1 (data gradient, layer >= 1): in = the gradient
+ * of the layer's output, w = the transposed, tap-mirrored weights wt[ci][8 - t][co], mask = the
+ * layer's input (the previous ReLU's output), out = the gradient of the layer's input, zero
+ * where mask <= 0 */
+int pm_lpp_conv(int layer, int mode, int tensor_cores, const void* in, const void* w, const float* bias,
+                const void* mask, void* out, int B, int H4, int W4, int* err, void* stream);
+/* weight and bias gradients of layer `layer` (COUT * 9 * CIN then COUT floats) from its input x
+ * and the gradient dy of its output; the tensor-core path sums 1024-pixel blocks into
+ * `scratch` (pm_lpp_wgrad_scratch_floats floats) and then the blocks in order (deterministic) */
+size_t pm_lpp_wgrad_scratch_floats(int layer, int B, int H4, int W4);
+int pm_lpp_wgrad(int layer, int tensor_cores, const void* x, const void* dy, float* scratch, float* grad, int B, int H4,
+                 int W4, int* err, void* stream);
+/* training target at 1 / scale resolution from plain PatchMatch's final planes of one view
+ * (W * H float4 a b c cost) and of the other view: out = W4 * H4 float4 (d / scale, nx, ny,
+ * valid), the means over each block's valid pixels (finite plane, 0 < d <= dmax, the other
+ * view's disparity at the matched column within 1 px) of the disparity and of the normal
+ * (a - 1, b, 1) / |..|, valid = 1 when at least half of the block is.  right_view: the right
+ * view's planes, as seen in the mirrored pair (blocks mirrored, normal (a - 1, -b, 1) / |..|) */
+int pm_lpp_target(const float* planes, const float* other, int W, int H, int scale, int right_view, float dmax,
+                  float* out, void* stream);
+/* L1 loss of M outputs (16 FP32 channels, d nx ny used) against M targets (float4 d nx ny valid):
+ * |d - d*| + wn (|nx - nx*| + |ny - ny*|) over valid pixels; dout (M * 16 BF16) = its gradient
+ * times `scale`; parts (nullable) = per-256-pixel loss sums */
+int pm_lpp_loss(const float* out, const float* target, float wn, float scale, int M, void* dout, float* parts,
+                void* stream);
+/* full-resolution initial disparity (pixels, clamped to [0, dmax]) and, when normal is not NULL,
+ * normal map (float4 nx ny nz 0) from the last layer's W4 x H4 output, bilinear; right_view: the
+ * output of the mirrored pair (read mirrored, ny negated) */
+int pm_lpp_upsample(const float* out4, int W4, int H4, int W, int H, int scale, int right_view, float dmax,
+                    float* disp, float* normal, void* stream);
 /* one Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected for `step` >= 1) on n FP32 values */
 int pm_lpp_adam(float* p, const float* g, float* m1, float* m2, int n, float lr, int step, void* stream);
-/* BF16 copies of a layer's FP32 weights: wmat and the data-gradient matrix wt */
-int pm_lpp_weights_bf16(const float* p, void* wmat, void* wt, void* stream);
-/* the whole proposal for one pair: nlayers convolutions with weights wmats (nlayers * 32 * 288
- * BF16, 256-byte aligned) and biases (nlayers * 32), initdisp W * H floats (pixels) */
+/* BF16 copies of layer `layer`'s FP32 weights p: wmat (forward) and wt (data gradient, nullable) */
+int pm_lpp_weights_bf16(int layer, const float* p, void* wmat, void* wt, void* stream);
+/* the whole proposal for one view of a pair: weights = every layer's BF16 wmat back to back,
+ * biases = every layer's biases back to back; disp W * H floats, normal W * H float4 (nullable);
+ * workspace 256-byte aligned, pm_lpp_propose_workspace_bytes(W, H, scale) bytes */
 size_t pm_lpp_propose_workspace_bytes(int W, int H, int scale);
-int pm_lpp_propose_device(const void* wmats, const float* biases, int nlayers, float skip, int step, int scale,
-                          const uint8_t* left, const uint8_t* right, int W, int H, size_t stride, int right_view,
-                          float* initdisp, void* workspace, size_t ws_bytes, int* err, void* stream);
+int pm_lpp_propose_device(const void* weights, const float* biases, int scale, const uint8_t* left, const uint8_t* right,
+                          int W, int H, size_t stride, int right_view, float dmax, float* disp, float* normal,
+                          void* workspace, size_t ws_bytes, int* err, void* stream);
 
 #ifdef __cplusplus
 }

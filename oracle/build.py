@@ -14,6 +14,10 @@ cpu_baseline leg:
                            present (it is not on GPU machines; the built .so
                            travels with the checkout instead).
 
+The reference checkout is found at $CVT_REFERENCE_ROOT, or given as
+`python oracle/build.py --reference DIR`; by default it is a directory named
+`reference` beside this repository.
+
 Both are built with -O2 -ffp-contract=off -fno-fast-math: every C operator
 rounds once, so results do not depend on the compiler's contraction choices.
 """
@@ -22,7 +26,17 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_KERNELS = "/root/reference/cvt/cl/kernel"
+
+
+def reference_kernels(root=None):
+    """cvt/cl/kernel of the reference checkout: `root`, else $CVT_REFERENCE_ROOT, else the
+    directory `reference` beside this repository"""
+    root = root or os.environ.get("CVT_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(HERE)),
+                                                                        "reference")
+    return os.path.join(root, "cvt", "cl", "kernel")
+
+
+
 CXXFLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-std=c++17"]
 
 
@@ -45,7 +59,8 @@ def build_oracle(force=False):
     return out
 
 
-def build_ref(force=False, kernel_dir=REF_KERNELS):
+def build_ref(force=False, kernel_dir=None):
+    kernel_dir = kernel_dir or reference_kernels()
     refdir = os.path.join(HERE, "_ref")
     out = os.path.join(refdir, "libpmref.so")
     if not os.path.isdir(kernel_dir):
@@ -70,5 +85,11 @@ def build_ref(force=False, kernel_dir=REF_KERNELS):
 
 
 if __name__ == "__main__":
-    print(build_oracle(force="-f" in sys.argv))
-    print(build_ref(force="-f" in sys.argv))
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("-f", action="store_true", help="rebuild even when up to date")
+    ap.add_argument("--reference", help="root of the reference checkout")
+    a = ap.parse_args()
+    print(build_oracle(force=a.f))
+    print(build_ref(force=a.f, kernel_dir=reference_kernels(a.reference) if a.reference else None))

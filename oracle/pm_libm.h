@@ -12,7 +12,7 @@
  * (exp 3 ulp, sin/cos 4 ulp, acospi 5 ulp).  The oracle pins one concrete
  * choice inside those bounds so that it and the CUDA kernels can agree bit for
  * bit; the CUDA side carries an independent copy of the same algorithms
- * (cvt_b200/csrc/pm_libm.cuh), and the GPU tests compare the two over every
+ * (cvt_b200/csrc/pm_math.cuh), and the GPU tests compare the two over every
  * input they meet.
  *
  * Methods (all from textbook numerical analysis, no vendor code):

@@ -54,13 +54,14 @@ def test_size_limits_follow_the_header(native):
 
 def test_option_defaults_are_the_reference_constants(native):
     """pm_options_default: both views (disparityMapAll), thetamin 1e-4 (PMHuberStereo.cpp:92),
-    LR check at 1 px and 5 degrees (:79-80), 40 ROF steps (PDOPTITER), one pyramid level (:78);
-    the structure's layout matches the header's; every status has a name"""
+    LR check at 1 px and 5 degrees (:79-80), 40 ROF steps (PDOPTITER), one pyramid level (:78),
+    strict arithmetic (bit-exact with the reference kernels); the structure's layout matches the
+    header's; every status has a name"""
     from cvt_b200 import _lib
 
     o = _lib.Options()
     assert native.pm_options_default(C.byref(o)) == _lib.PM_OK
-    assert (o.views, o.fused, o.rof_iters, o.device, o.use_graph, o.levels) == (2, 1, 40, 0, 1, 1)
+    assert (o.views, o.fused, o.rof_iters, o.device, o.use_graph, o.levels) == (2, 0, 40, 0, 1, 1)
     assert np.float32(o.thetamin) == np.float32(1e-4)
     assert (o.maxdispdiff, o.maxanglediff) == (1.0, 5.0)
     assert native.pm_options_default(None) == _lib.PM_EINVAL_ARG
@@ -310,24 +311,36 @@ def test_svpm_create_fails_loudly_without_device(native):
 
 
 def test_lpp_rejects_bad_arguments_without_touching_the_device(native):
+    import ctypes as C
+
     from cvt_b200 import _lib
 
-    assert native.pm_lpp_channels() == 32
-    assert native.pm_lpp_conv(0, 1, None, None, None, None, None, 0, 4, 4, None, None) == _lib.PM_EINVAL_SHAPE
-    assert native.pm_lpp_conv(3, 1, None, None, None, None, None, 1, 4, 4, None, None) == _lib.PM_EINVAL_ARG
-    assert native.pm_lpp_conv(0, 1, None, None, None, None, None, 1, 4, 4, None, None) == _lib.PM_EINVAL_ARG
+    # the network of cfg4: 8 layers of 3x3 convolutions, 32-64 channels, dilations growing to 16
+    assert native.pm_lpp_layers() == 8
+    shapes = []
+    for l in range(8):
+        ci, co, di = C.c_int(), C.c_int(), C.c_int()
+        assert native.pm_lpp_layer_shape(l, C.byref(ci), C.byref(co), C.byref(di)) == 0
+        shapes.append((ci.value, co.value, di.value))
+    assert shapes == [(16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 4), (64, 64, 8), (64, 64, 16), (64, 32, 1),
+                      (32, 16, 1)]
+    assert native.pm_lpp_layer_shape(8, None, None, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_lpp_param_count() == sum(co * 9 * ci + co for ci, co, _ in shapes)
+    assert native.pm_lpp_conv(0, 0, 1, None, None, None, None, None, 0, 4, 4, None, None) == _lib.PM_EINVAL_SHAPE
+    assert native.pm_lpp_conv(9, 0, 1, None, None, None, None, None, 1, 4, 4, None, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_lpp_conv(0, 1, 1, None, None, None, None, None, 1, 4, 4, None, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_lpp_conv(2, 0, 1, None, None, None, None, None, 1, 4, 4, None, None) == _lib.PM_EINVAL_ARG
     assert b"null" in native.pm_lpp_last_error()
-    assert native.pm_lpp_features(None, None, 3, 8, 16, 0, 1, 4, None, None, None) == _lib.PM_EINVAL_SHAPE
-    assert native.pm_lpp_features(None, None, 8, 8, 32, 0, 1, 3, None, None, None) == _lib.PM_EINVAL_ARG
-    assert native.pm_lpp_softargmin(None, None, 4.0, 1.0, None, None, None, None, 0, 1.0, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_lpp_input(None, None, 3, 8, 16, 4, 0, None, None) == _lib.PM_EINVAL_ARG
+    assert native.pm_lpp_loss(None, None, 1.0, 1.0, 0, None, None, None) == _lib.PM_EINVAL_ARG
     assert native.pm_lpp_adam(None, None, None, None, 10, 1e-3, 0, None) == _lib.PM_EINVAL_ARG
     assert native.pm_lpp_propose_workspace_bytes(2, 2, 4) == 0
-    assert native.pm_lpp_propose_workspace_bytes(64, 48, 4) > 16 * 12 * 32 * 2 * 3
-    assert native.pm_lpp_propose_workspace_bytes(64, 48, 2) > 32 * 24 * 32 * 2 * 3
-    assert native.pm_lpp_propose_device(None, None, 6, 4.0, 1, 4, None, None, 64, 48, 256, 0, None, None, 0, None,
+    assert native.pm_lpp_propose_workspace_bytes(64, 48, 4) >= 16 * 12 * (16 * 2 + 2 * 64 * 2 + 16 * 4)
+    assert native.pm_lpp_propose_device(None, None, 4, None, None, 64, 48, 256, 0, 64.0, None, None, None, 0, None,
                                         None) == _lib.PM_EINVAL_ARG
-    assert native.pm_lpp_wgrad_scratch_floats(1, 4, 4, 0) == 0
-    assert native.pm_lpp_wgrad_scratch_floats(1, 4, 4, 8) == 2 * (32 * 288 + 32)
+    assert native.pm_lpp_wgrad_scratch_floats(8, 1, 4, 4) == 0
+    # one 1024-pixel block of partial sums per CTA: 9 * CIN + 1 rows (the last one the bias) x COUT
+    assert native.pm_lpp_wgrad_scratch_floats(3, 1, 32, 40) == 2 * (9 * 64 + 1) * 64
 
 
 def test_autotuner_keeps_the_fastest_branch_count():
