@@ -650,11 +650,13 @@ void launch_init(float4* out, const ViewData& V, float dmax, int lr, const float
 {
     const dim3 b(32, 4);
     const dim3 g = grid2d(V.W, V.H, b);
-    if (fused) {   // both variants; the one that does not apply returns at once (pm_window.cuh)
+    // both variants; the one that does not apply returns at once (pm_window.cuh)
+    if (fused) {
         k_init<true, false><<<g, b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal, 1);
         k_init<true, true><<<g, b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal, 1);
     } else {
-        k_init<false, true><<<g, b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal, 0);
+        k_init<false, false><<<g, b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal, 1);
+        k_init<false, true><<<g, b, 0, st>>>(out, V, dmax, lr, initdisp, initnormal, 1);
     }
 }
 
@@ -662,11 +664,13 @@ void launch_cost(float* cost, const float4* planes, const ViewData& V, float min
 {
     const dim3 b(32, 4);
     const dim3 g = grid2d(V.W, V.H, b);
+    // both variants; the one that does not apply returns at once (pm_window.cuh)
     if (fused) {
         k_cost<true, false><<<g, b, 0, st>>>(cost, planes, V, mincost, 1);
         k_cost<true, true><<<g, b, 0, st>>>(cost, planes, V, mincost, 1);
     } else {
-        k_cost<false, true><<<g, b, 0, st>>>(cost, planes, V, mincost, 0);
+        k_cost<false, false><<<g, b, 0, st>>>(cost, planes, V, mincost, 1);
+        k_cost<false, true><<<g, b, 0, st>>>(cost, planes, V, mincost, 1);
     }
 }
 
@@ -674,11 +678,13 @@ void launch_klt(float4* out, const float4* planes, const ViewData& V, int fused,
 {
     const dim3 b(32, 4);
     const dim3 g = grid2d(V.W, V.H, b);
+    // both variants; the one that does not apply returns at once (pm_window.cuh)
     if (fused) {
         k_klt<true, false><<<g, b, 0, st>>>(out, planes, V, 1);
         k_klt<true, true><<<g, b, 0, st>>>(out, planes, V, 1);
     } else {
-        k_klt<false, true><<<g, b, 0, st>>>(out, planes, V, 0);
+        k_klt<false, false><<<g, b, 0, st>>>(out, planes, V, 1);
+        k_klt<false, true><<<g, b, 0, st>>>(out, planes, V, 1);
     }
 }
 

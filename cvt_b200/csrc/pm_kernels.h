@@ -49,8 +49,12 @@ void launch_cost(float* cost, const float4* planes, const ViewData& V, float min
 void launch_klt(float4* out, const float4* planes, const ViewData& V, int fused, cudaStream_t st);
 void launch_propagate(const PropParams& P, int fused, cudaStream_t st);
 // launches per window-loop kernel (init, cost, klt, each of the three propagate kernels):
-// fused and uncounted runs launch both variants (pm_window.cuh)
-inline int window_kernel_launches(int fused, bool counting) { return fused && !counting ? 2 : 1; }
+// uncounted runs launch both variants (pm_window.cuh)
+inline int window_kernel_launches(int fused, bool counting)
+{
+    (void)fused;
+    return counting ? 1 : 2;
+}
 void launch_normal_depth(float4* out, const float4* planes, int W, int H, float dispscale, int lr, cudaStream_t st);
 size_t rof_scratch_bytes(int W, int H);
 // kernel launches of launch_rof / launch_huber for `iters` steps (two steps per launch)

@@ -227,21 +227,29 @@ void launch_propagate(const PropParams& P, int fused, cudaStream_t st)
         k_prop_final<FF, CC, KK><<<g, b, 0, st>>>(PP);  \
     } while (0)
     PropParams Q = P;
-    if (fused && !count) {
+    if (!count) {
         // both variants; the one that does not apply returns at once (pm_window.cuh).  Each
         // kernel of the pass finishes before the next starts, for either variant.
         Q.dual = 1;
-        k_prop_chain<true, false, false><<<g, b, 0, st>>>(Q);
-        k_prop_chain<true, false, true><<<g, b, 0, st>>>(Q);
-        k_prop_klt<true, false, false><<<g, b, 0, st>>>(Q);
-        k_prop_klt<true, false, true><<<g, b, 0, st>>>(Q);
-        k_prop_final<true, false, false><<<g, b, 0, st>>>(Q);
-        k_prop_final<true, false, true><<<g, b, 0, st>>>(Q);
+        if (fused) {
+            k_prop_chain<true, false, false><<<g, b, 0, st>>>(Q);
+            k_prop_chain<true, false, true><<<g, b, 0, st>>>(Q);
+            k_prop_klt<true, false, false><<<g, b, 0, st>>>(Q);
+            k_prop_klt<true, false, true><<<g, b, 0, st>>>(Q);
+            k_prop_final<true, false, false><<<g, b, 0, st>>>(Q);
+            k_prop_final<true, false, true><<<g, b, 0, st>>>(Q);
+        } else {
+            k_prop_chain<false, false, false><<<g, b, 0, st>>>(Q);
+            k_prop_chain<false, false, true><<<g, b, 0, st>>>(Q);
+            k_prop_klt<false, false, false><<<g, b, 0, st>>>(Q);
+            k_prop_klt<false, false, true><<<g, b, 0, st>>>(Q);
+            k_prop_final<false, false, false><<<g, b, 0, st>>>(Q);
+            k_prop_final<false, false, true><<<g, b, 0, st>>>(Q);
+        }
     } else {
         Q.dual = 0;
         if (fused) PM_PROP_LAUNCH(true, true, true, Q);
-        else if (count) PM_PROP_LAUNCH(false, true, true, Q);
-        else PM_PROP_LAUNCH(false, false, true, Q);
+        else PM_PROP_LAUNCH(false, true, true, Q);
     }
 #undef PM_PROP_LAUNCH
 }

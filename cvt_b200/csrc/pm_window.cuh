@@ -51,9 +51,14 @@ struct Counters {
 
 __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
 
-// bilinear pair: (1-a)*T0 + a*T1 per element; fused contracts a*T1.  The strict form
-// stays scalar: nvcc contracts a packed multiply feeding a packed add into FFMA2 even
-// under -fmad=false, which would change the rounding.
+// bilinear pair: (1-a)*T0 + a*T1 per element; fused contracts a*T1.  The strict form rounds
+// the two products (one packed multiply each) and adds them with scalar, explicitly rounded
+// adds: packed adds fed by packed multiplies were measured to come out fused, which would
+// change the rounding; a packed multiply feeding __fadd_rn does not (the 1280x720 results are
+// bit-identical to the all-scalar form, which PM_STRICT_FMUL2=0 selects).
+#ifndef PM_STRICT_FMUL2
+#define PM_STRICT_FMUL2 1
+#endif
 template <bool F>
 __device__ __forceinline__ float2 lerp2(float2 a2, float2 b2, float2 t0, float2 t1)
 {
@@ -385,7 +390,7 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
                 h00_01 = __ffma2_rn(s2, f2(qx * qx, qx * qy), h00_01);
                 h02_11 = __ffma2_rn(s2, f2(qx, yy), h02_11);
                 h12_22 = __ffma2_rn(s2, f2(qy, 1.0f), h12_22);
-            } else {   // scalar: see lerp2
+            } else {   // scalar, explicitly rounded (see lerp2)
                 J01 = f2(__fadd_rn(J01.x, __fmul_rn(t, qx)), __fadd_rn(J01.y, __fmul_rn(t, qy)));
                 J2 = J2 + t * 1.0f;
                 h00_01 = f2(__fadd_rn(h00_01.x, __fmul_rn(sc, qx * qx)), __fadd_rn(h00_01.y, __fmul_rn(sc, qx * qy)));

@@ -191,11 +191,13 @@ def test_tiny_colours_take_exact_division(D, orc):
     bwR[5:20, :, :3] *= tiny
     gL, gR, P = g["gL"], g["gR"], g["k_planes"]
     dL, dR, dgL, dgR, dP = (dev(D.t, a) for a in (bwL, bwR, gL, gR, P))
-    for m in (1e10, 0.2):
-        assert bits_equal(host(D.cost(dP, dL, dR, dgL, dgR, r, m, 1)), orc.cost(P, bwL, bwR, gL, gR, r, m, fused=1)).all()
-    assert bits_equal(host(D.klt(dP, dL, dR, dgL, dgR, r, 1)), orc.klt(P, bwL, bwR, gL, gR, r, fused=1)).all()
-    init = host(D.init(dL, dR, dgL, dgR, r, dmax, 1, 1))
-    assert bits_equal(init, orc.init(bwL, bwR, gL, gR, r, dmax, 1, fused=1)).all()
+    for f in (0, 1):   # both arithmetics launch the unchecked and the checked variant
+        for m in (1e10, 0.2):
+            assert bits_equal(host(D.cost(dP, dL, dR, dgL, dgR, r, m, f)),
+                              orc.cost(P, bwL, bwR, gL, gR, r, m, fused=f)).all()
+        assert bits_equal(host(D.klt(dP, dL, dR, dgL, dgR, r, f)), orc.klt(P, bwL, bwR, gL, gR, r, fused=f)).all()
+        init = host(D.init(dL, dR, dgL, dgR, r, dmax, 1, f))
+        assert bits_equal(init, orc.init(bwL, bwR, gL, gR, r, dmax, 1, fused=f)).all()
 
 
 def test_propagate_view_exchange_matches_oracle(D, orc):
