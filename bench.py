@@ -59,13 +59,15 @@ WORKLOADS = {
     "small": (320, 240, 12, 2.0, 30.0, 7, 32.0, 4, 1, 0),
     # one pair of the 4K configuration (3840x2160, 120 planes, disparity 0-256, 35x35 window)
     "4k": (3840, 2160, 120, 2.0, 240.0, 17, 256.0, 8, 2, 1),
+    # a quarter-size pair with the hd window (the small case of ncu captures of the hd kernels)
+    "quarter": (640, 360, 20, 2.0, 60.0, 10, 64.0, 2, 2, 1),
 }
 # SVPMFlowCL::flow: window half-width, flow range, passes (the reference's MAXITER), and the
 # passes of the bounded CPU samples
 SVPM = {"r": 3, "flowmax": 128.0, "passes": 200, "cpu_passes": 40, "ref_passes": 20}
 # bounded CPU samples (crop of the same scene, same window / range / iterations)
-CPU_CROP = {"hd": (256, 144), "small": (320, 240), "4k": (192, 108)}
-REF_CROP = {"hd": (96, 54), "small": (96, 72), "4k": (64, 36)}
+CPU_CROP = {"hd": (256, 144), "small": (320, 240), "4k": (192, 108), "quarter": (160, 90)}
+REF_CROP = {"hd": (96, 54), "small": (96, 72), "4k": (64, 36), "quarter": (64, 36)}
 
 
 def executed(iters):
