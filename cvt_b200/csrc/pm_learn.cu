@@ -21,12 +21,14 @@
 // view minus the x-slope of the left one).
 //
 // Tensor cores (tcgen05, kind::f16, BF16 x BF16 -> FP32 in TMEM):
-//   k_conv_tc   forward and data gradient: an implicit GEMM, per CTA 128 pixels (M) x COUT (N),
-//               K = 9 taps x CIN, all taps of A and all of B staged in shared memory in the
-//               canonical K-major layout without swizzle; one thread issues the MMAs and
-//               commits them to an mbarrier; the epilogue reads TMEM (tcgen05.ld 32x32b).  The
-//               data gradient is the same kernel with the layer's transposed, tap-mirrored
-//               weights and the ReLU mask of the layer's input in the epilogue.
+//   k_conv_tc   forward and data gradient: an implicit GEMM, 128-pixel tiles (M) x COUT (N),
+//               K = 9 taps x CIN; persistent (one CTA per SM), warp-specialised: TMA loads of
+//               each tap's shifted 16 x 8-pixel box (zero padding by the TMA) through a ring of
+//               shared-memory buffers, one thread issuing the MMAs into two TMEM accumulators,
+//               four warps reading TMEM (tcgen05.ld 32x32b) for the epilogue and storing
+//               through shared memory, coalesced.  The data gradient is the same kernel with
+//               the layer's transposed, tap-mirrored weights and the ReLU mask of the layer's
+//               input in the epilogue.
 //   k_wgrad_tc  weight gradient: D[(tap, ci)][co] = sum over pixels of x[p + tap][ci] dy[p][co]
 //               as MMAs of M128 (tap, ci rows) x N COUT x K16 (pixels), both operands MN-major
 //               (16-byte NHWC channel groups are the core-matrix rows, so cp.async copies them
@@ -35,11 +37,13 @@
 //               per-CTA partial sums reduced in CTA order (deterministic).
 // Every wait on an mbarrier is bounded by clock (about two seconds); past the limit the kernel
 // raises the error flag that the host reads.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 
 #include "../../include/cvtpm.h"
@@ -165,111 +169,426 @@ __device__ __forceinline__ int tap_pixel(int m, int M, int H, int W, int t, int 
     return b * HW + yy * W + xx;
 }
 
+// the convolution's pixel tiles: TX x TY pixels of one image, x fastest (the MMA's M rows)
+constexpr int TX = 16, TY = 8;
+constexpr int CONV_THREADS = 224;   // warps 0-3 epilogue, 4 loads (TMA), 5 MMAs, 6 waits for 5
+constexpr int CONV_LOADERS = 8;     // lanes of warp 4 that issue the loads, one step each in turn
+
+template <int CIN, int COUT, int EPI>
+struct ConvShape {
+    static constexpr int A_STAGE = TM * CIN * 2;          // one tap's 128 pixels x CIN, BF16
+    static constexpr int B_BYTES = COUT * 9 * CIN * 2;    // all the weights
+    static constexpr int RB = COUT * (EPI == EPI_BIAS_F32 ? 4 : 2);   // output bytes per pixel
+    static constexpr int STG = 4 * 32 * RB;               // the epilogue warps' staging rows
+    static constexpr int FIT = (225 * 1024 - B_BYTES - STG - 1024) / A_STAGE / CONV_LOADERS * CONV_LOADERS;
+    static constexpr int STAGES = FIT > 16 ? 16 : FIT;   // a multiple of CONV_LOADERS
+    static constexpr int SMEM = STAGES * A_STAGE + B_BYTES + STG + 1024;   // + alignment of the ring to 1024
+    static_assert(STAGES >= CONV_LOADERS && STAGES % CONV_LOADERS == 0, "shared memory");
+    static_assert(RB == 32 || RB == 64 || RB == 128, "staging row");
+};
+
+// epilogue of one warp's 32 pixels of a tile (lane = TMEM lane = pixel p of the warp: tile row
+// 2 warp + p / TX, column p % TX; rows y0.., columns x0.. of image b), per EPI (see k_conv_tc).
+// The accumulator row is read from TMEM (tcgen05.ld 32x32b), finished in registers and written
+// to the warp's staging rows in shared memory (16-byte chunk q of pixel p at chunk
+// q ^ ((p / (128 / RB)) % (RB / 16)), so that 32 lanes writing one chunk each hit distinct
+// banks); then the warp stores the rows with consecutive lanes on consecutive 16-byte chunks
+// (two image rows of TX pixels, each contiguous in NHWC).  The ReLU mask of the data gradient
+// comes in the same way, coalesced, before the accumulator is read.
+template <int COUT, int EPI>
+struct EpiGeom {
+    static constexpr int ES = EPI == EPI_BIAS_F32 ? 4 : 2, RB = COUT * ES, NQ = RB / 16, PPR = 128 / RB;
+    // pixel p of warp `warp` in the tile at (b, y0, x0): its linear index, or -1 outside the image
+    __device__ __forceinline__ static long long pixel(int p, int warp, int b, int y0, int x0, int H, int W)
+    {
+        const int y = y0 + 2 * warp + p / TX, x = x0 + p % TX;
+        return (y < H && x < W) ? ((long long)b * H + y) * W + x : -1;
+    }
+    __device__ __forceinline__ static uint8_t* chunk(uint8_t* stg, int p, int q) { return stg + p * RB + ((q ^ ((p / PPR) % NQ)) << 4); }
+};
+
+// this lane's share of the warp's 32 pixels' mask rows (chunk c = lane + 32 i), loaded coalesced;
+// issued before the accumulator wait so that the loads are in flight meanwhile
+template <int COUT>
+__device__ __forceinline__ void conv_mask_load(uint4 (&mk)[COUT * 2 / 16], int warp, int lane, int b, int y0, int x0, int H,
+                                               int W, const __nv_bfloat16* __restrict__ mask)
+{
+    using G = EpiGeom<COUT, EPI_MASK_BF16>;
+#pragma unroll
+    for (int i = 0; i < G::NQ; i++) {
+        const int c = lane + 32 * i, p = c / G::NQ, q = c % G::NQ;
+        const long long m = G::pixel(p, warp, b, y0, x0, H, W);
+        mk[i] = m >= 0 ? *reinterpret_cast<const uint4*>(reinterpret_cast<const uint8_t*>(mask) + m * G::RB + q * 16)
+                       : make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
+template <int COUT, int EPI>
+__device__ __forceinline__ void conv_epilogue(uint32_t tacc, int warp, int lane, uint8_t* stg, int b, int y0, int x0,
+                                              int H, int W, const float* __restrict__ sbias, const uint4* mkreg,
+                                              void* __restrict__ out)
+{
+    using G = EpiGeom<COUT, EPI>;
+    constexpr int RB = G::RB, NQ = G::NQ;
+    auto pixel = [&](int p) { return G::pixel(p, warp, b, y0, x0, H, W); };
+    auto chunk = [&](int p, int q) { return G::chunk(stg, p, q); };
+    if (EPI == EPI_MASK_BF16) {
+#pragma unroll
+        for (int i = 0; i < NQ; i++) {
+            const int c = lane + 32 * i;
+            *reinterpret_cast<uint4*>(chunk(c / NQ, c % NQ)) = mkreg[i];
+        }
+        __syncwarp();
+    }
+    uint32_t r[COUT];
+#pragma unroll
+    for (int j0 = 0; j0 < COUT; j0 += 16) tmem_ld16(tacc + ((uint32_t)(warp * 32) << 16) + j0, *reinterpret_cast<uint32_t(*)[16]>(r + j0));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    const int p = lane;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        uint4* dst = reinterpret_cast<uint4*>(chunk(p, q));
+        if (EPI == EPI_BIAS_F32) {
+            const int j = 4 * q;
+            *reinterpret_cast<float4*>(dst) =
+                make_float4(__uint_as_float(r[j]) + sbias[j], __uint_as_float(r[j + 1]) + sbias[j + 1],
+                            __uint_as_float(r[j + 2]) + sbias[j + 2], __uint_as_float(r[j + 3]) + sbias[j + 3]);
+        } else {
+            const int j = 8 * q;
+            __align__(16) __nv_bfloat162 v[4];
+            __align__(16) __nv_bfloat162 mk[4];
+            if (EPI == EPI_MASK_BF16) *reinterpret_cast<uint4*>(mk) = *dst;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                float x0v = __uint_as_float(r[j + 2 * i]), x1v = __uint_as_float(r[j + 2 * i + 1]);
+                if (EPI == EPI_RELU_BF16) {
+                    x0v = fmaxf(x0v + sbias[j + 2 * i], 0.0f);
+                    x1v = fmaxf(x1v + sbias[j + 2 * i + 1], 0.0f);
+                } else {
+                    x0v = __low2float(mk[i]) > 0.0f ? x0v : 0.0f;
+                    x1v = __high2float(mk[i]) > 0.0f ? x1v : 0.0f;
+                }
+                v[i] = __floats2bfloat162_rn(x0v, x1v);
+            }
+            *dst = *reinterpret_cast<const uint4*>(v);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = lane; c < 32 * NQ; c += 32) {
+        const int pp = c / NQ, q = c % NQ;
+        const long long m = pixel(pp);
+        if (m >= 0) *reinterpret_cast<uint4*>(static_cast<uint8_t*>(out) + m * RB + q * 16) = *reinterpret_cast<const uint4*>(chunk(pp, q));
+    }
+    __syncwarp();
+}
+
+// shared-memory descriptor of a K-major operand whose rows (row = 32, 64 or 128 bytes) are
+// swizzled at their own width, as the TMA writes them: 8-row atoms SBO = 8 row apart, layout
+// type 6 (32B), 4 (64B) or 2 (128B) in bits 61-63; the leading offset is unused (1)
+__device__ __forceinline__ uint64_t smem_desc_sw(uint32_t addr, int row)
+{
+    const uint64_t lt = row == 128 ? 2u : row == 64 ? 4u : 6u;
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(((8 * row) >> 4) & 0x3FFF) << 32) |
+           (1ull << 46) | (lt << 61);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+}
+
+// tiled TMA load of one box of a 4-D tensor map into this CTA's shared memory; completion is
+// counted in bytes on the mbarrier
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, uint32_t mbar, int c0, int c1, int c2,
+                                            int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+        "[%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(mbar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+
+// mbarrier.try_wait: the thread may sleep in it until the phase completes or a short,
+// hardware-chosen time passes; true once the phase has completed
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t phase)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.cta.shared::cta.b32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v)
+{
+    asm volatile("st.release.cta.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
+
+// wait for an mbarrier phase for at most WAIT_CYCLES, giving up early once another role of the
+// CTA has given up (*abort); a timeout sets *abort.  The common case (the phase completes within
+// the first try_wait) reads neither the clock nor the flag.
+__device__ __forceinline__ bool mbar_wait_role(uint32_t addr, uint32_t phase, volatile int* abort)
+{
+    if (mbar_try(addr, phase)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try(addr, phase)) {
+        if (*abort) return false;
+        if (clock64() - t0 > WAIT_CYCLES) {
+            *abort = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
 // out[m][n] = sum over taps t and channels c of in[pixel m shifted by tap t][c] * wmat[n][t][c],
-// then per EPI:
+// 3x3 taps (dy, dx) = ((t / 3 - 1) dil, (t % 3 - 1) dil) with zero padding, then per EPI:
 //   EPI_RELU_BF16  + bias, ReLU, BF16 out          (forward, hidden layers)
 //   EPI_BIAS_F32   + bias, FP32 out                (forward, last layer)
 //   EPI_MASK_BF16  times (mask[m][n] > 0), BF16 out (data gradient through the ReLU)
+// Persistent and warp-specialised; CTA c takes tiles c, c + grid, ... of TX x TY pixels.  The
+// weights (B, canonical K-major without swizzle, K = 9 CIN) are copied into shared memory once.
+// A step is one (tile, tap): its A operand is one TMA box (CIN, TX, TY, 1) of the NHWC input
+// at the tile's corner shifted by the tap, which the TMA fills with zeros outside the image
+// (the padding), written with the swizzle of a CIN * 2-byte row so that it is the MMA's K-major
+// swizzled layout as it lands.  Roles:
+//   warp 4, lanes 0..CONV_LOADERS-1: the loads, into a ring of STAGES buffers, lane l taking
+//     steps l, l + CONV_LOADERS, ... (one thread can have only a few boxes in issue at a time);
+//     a full barrier per buffer counts the bytes, an empty barrier per buffer is the MMAs'
+//   warp 6: tests the next 8 steps' full barriers (and, at a tile's first step, whether the
+//     epilogue has released the tile's accumulator) and publishes the count of ready steps
+//   warp 5, lane 0: issues each ready step's CIN / 16 MMAs (M128, N COUT, K16) into one of two
+//     TMEM accumulators, alternating per tile, commits them to the buffer's empty barrier and,
+//     after the ninth tap, to the accumulator's full barrier; it reads the published count
+//     instead of waiting on mbarriers, whose round trip would stall it
+//   warps 0-3: the epilogue (conv_epilogue), then release of the accumulator
+// So loads, MMAs and the previous tile's epilogue overlap.  Every wait is bounded; a role that
+// times out raises the CTA's abort flag and the error flag, the others stop at their next wait,
+// and the CTA waits (bounded) for the loads and MMAs it has in flight before it frees TMEM.
 template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(TM) k_conv_tc(const __nv_bfloat16* __restrict__ in,
-                                                const __nv_bfloat16* __restrict__ wmat, const float* __restrict__ bias,
-                                                const __nv_bfloat16* __restrict__ mask, void* __restrict__ out, int B,
-                                                int H, int W, int dil, int* err)
+__global__ void __launch_bounds__(CONV_THREADS, 1)
+    k_conv_tc(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16* __restrict__ wmat,
+              const float* __restrict__ bias, const __nv_bfloat16* __restrict__ mask, void* __restrict__ out, int B,
+              int H, int W, int dil, int* err)
 {
-    constexpr int KTOT = 9 * CIN, KC = KTOT / 8;   // K and its 16-byte chunks
-    constexpr int A_BYTES = TM * KTOT * 2;
-    constexpr uint32_t A_LBO = (TM / 8) * 128, B_LBO = (COUT / 8) * 128;
-    constexpr int TCOLS = tmem_cols(COUT);
-    extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(8) uint64_t mbar;
+    using Sh = ConvShape<CIN, COUT, EPI>;
+    constexpr int S = Sh::STAGES, A_STAGE = Sh::A_STAGE, ROW = CIN * 2;
+    constexpr int KTOT = 9 * CIN, KC = KTOT / 8;
+    constexpr uint32_t B_LBO = (COUT / 8) * 128;
+    constexpr int TCOLS = tmem_cols(2 * COUT);
+    constexpr uint32_t ID = idesc(TM, COUT, false, false);
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full[S], empty[S], accf[2], acce[2];
     __shared__ uint32_t tmem_base;
-    uint8_t* sA = smem;
-    uint8_t* sB = smem + A_BYTES;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int M = B * H * W;
-    const int m = blockIdx.x * TM + tid;
-    // A: this thread's pixel, every tap, CIN / 8 chunks each; B: the weights
-#pragma unroll 1
-    for (int t = 0; t < 9; t++) {
-        const int src = tap_pixel(m, M, H, W, t, dil);
-        const uint4* s = reinterpret_cast<const uint4*>(in + (size_t)(src < 0 ? 0 : src) * CIN);
-#pragma unroll
-        for (int q = 0; q < CIN / 8; q++) cp16(sA + canon(t * (CIN / 8) + q, tid, TM), s + q, src >= 0);
-    }
-    for (int i = tid; i < COUT * KC; i += TM) {
+    __shared__ int abort_flag, n_loaded[CONV_LOADERS], n_consumed, n_committed, n_ready;
+    __shared__ float sbias[COUT];
+    volatile int* abort = &abort_flag;
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t sA = (raw + 1023u) & ~1023u;   // swizzle atoms need 1024-byte alignment
+    uint8_t* sBp = smem_raw + (sA - raw) + S * A_STAGE;
+    const uint32_t sB = smem_u32(sBp);
+    uint8_t* stg = sBp + Sh::B_BYTES;   // 4 x 32 x RB bytes
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int txn = (W + TX - 1) / TX, tyn = (H + TY - 1) / TY, per_img = txn * tyn;
+    const int ntiles = B * per_img;
+    const int mine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int nsteps = 9 * mine;
+
+    for (int i = tid; i < COUT * KC; i += CONV_THREADS) {
         const int n = i / KC, c = i - n * KC;
-        cp16(sB + canon(c, n, COUT), reinterpret_cast<const uint4*>(wmat + (size_t)n * KTOT) + c, true);
+        cp16(sBp + canon(c, n, COUT), reinterpret_cast<const uint4*>(wmat + (size_t)n * KTOT) + c, true);
     }
     cp_commit();
-    if (warp == 0) tmem_alloc(&tmem_base, TCOLS);
+    if (tid < COUT) sbias[tid] = (EPI == EPI_MASK_BF16) ? 0.0f : bias[tid];
+    if (warp == 4) tmem_alloc(&tmem_base, TCOLS);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
-        asm volatile("fence.mbarrier_init.release.cluster;");
+        for (int i = 0; i < S; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&accf[i], 1);
+            mbar_init(&acce[i], 4);
+        }
+        abort_flag = 0;
+        for (int i = 0; i < CONV_LOADERS; i++) n_loaded[i] = 0;
+        n_consumed = 0;
+        n_committed = 0;
+        n_ready = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     cp_wait_all();
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // staged tiles -> tensor core reads
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the weights, for the tensor cores
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
-    if (tid == 0) {
-        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-#pragma unroll 1
-        for (int j = 0; j < KTOT / 16; j++)
-            mma_f16(tmem, smem_desc(a0 + 2 * j * A_LBO, A_LBO, 128), smem_desc(b0 + 2 * j * B_LBO, B_LBO, 128),
-                    idesc(TM, COUT, false, false), j > 0 ? 1u : 0u);
-        mma_commit(smem_u32(&mbar));
-    }
-    bool done = mbar_wait_bounded(smem_u32(&mbar), 0, WAIT_CYCLES);
-    if (!done) {
-        atomicExch(err, 1);
-        // the MMAs of this CTA may still run: wait for them once more before freeing TMEM
-        done = mbar_wait_bounded(smem_u32(&mbar), 0, WAIT_CYCLES);
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (done) {
+
+    if (warp == 4) {
+        // loads: lane l issues steps l, l + CONV_LOADERS, ... (a TMA issue holds its thread for
+        // a while, so several lanes keep more boxes in flight); step k's buffer k % S belongs to
+        // one lane, as S is a multiple of CONV_LOADERS
+        if (lane < CONV_LOADERS) {
+            int k = lane;
+            for (; k < nsteps; k += CONV_LOADERS) {
+                const int s = k % S, use = k / S;
+                if (use > 0 && !mbar_wait_role(smem_u32(&empty[s]), (use - 1) & 1, abort)) break;
+                const int t = (int)blockIdx.x + (k / 9) * (int)gridDim.x, tap = k % 9;
+                const int b = t / per_img, r = t - b * per_img, ty = r / txn, tx = r - ty * txn;
+                mbar_expect_tx(smem_u32(&full[s]), A_STAGE);
+                tma_load_4d(sA + s * A_STAGE, &xmap, smem_u32(&full[s]), 0, tx * TX + (tap % 3 - 1) * dil,
+                            ty * TY + (tap / 3 - 1) * dil, b);
+            }
+            n_loaded[lane] = k;   // the first step this lane did not issue
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {   // MMAs
+            // The MMA thread never waits on an mbarrier: such a wait, issued behind MMAs, holds
+            // the thread for a few hundred cycles, longer than a step's MMAs run at N <= 64.
+            // Warp 6 does the waiting and publishes how many steps are ready (their loads
+            // landed, their accumulator free); the MMA thread reads that count (acquire) only
+            // when it has used up the steps it knew of.
+            const uint64_t adesc0 = smem_desc_sw(sA, ROW), bdesc0 = smem_desc(sB, B_LBO, 128);
+            const uint32_t empty0 = smem_u32(&empty[0]);
+            int avail = 0, k = 0, s = 0;   // s = k % S
+            bool ok = true;
+            for (int i = 0; i < mine && ok; i++) {
+                const uint32_t acc = tmem + (uint32_t)((i & 1) * COUT);
 #pragma unroll
-        for (int j0 = 0; j0 < COUT; j0 += 16) {
-            uint32_t r[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + j0, r);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (m < M) {
-                if (EPI == EPI_BIAS_F32) {
-                    float4* o = reinterpret_cast<float4*>(static_cast<float*>(out) + (size_t)m * COUT + j0);
-#pragma unroll
-                    for (int j = 0; j < 16; j += 4)
-                        o[j / 4] = make_float4(__uint_as_float(r[j]) + bias[j0 + j], __uint_as_float(r[j + 1]) + bias[j0 + j + 1],
-                                               __uint_as_float(r[j + 2]) + bias[j0 + j + 2],
-                                               __uint_as_float(r[j + 3]) + bias[j0 + j + 3]);
-                } else {
-                    __align__(16) __nv_bfloat162 v[8];
-                    const __nv_bfloat16* mk = mask + (size_t)m * COUT + j0;
-#pragma unroll
-                    for (int j = 0; j < 16; j += 2) {
-                        float a = __uint_as_float(r[j]), c = __uint_as_float(r[j + 1]);
-                        if (EPI == EPI_RELU_BF16) {
-                            a = fmaxf(a + bias[j0 + j], 0.0f);
-                            c = fmaxf(c + bias[j0 + j + 1], 0.0f);
-                        } else {
-                            a = __bfloat162float(mk[j]) > 0.0f ? a : 0.0f;
-                            c = __bfloat162float(mk[j + 1]) > 0.0f ? c : 0.0f;
+                for (int tap = 0; tap < 9; tap++) {
+                    if (k >= avail) {
+                        avail = ld_acquire(&n_ready);
+                        if (k >= avail) {
+                            const long long t0 = clock64();
+                            while (k >= avail && !*abort) {
+                                if (clock64() - t0 > WAIT_CYCLES) *abort = 1;
+                                avail = ld_acquire(&n_ready);
+                            }
+                            if (k >= avail) {
+                                ok = false;
+                                break;
+                            }
                         }
-                        v[j / 2] = __floats2bfloat162_rn(a, c);
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     }
-                    uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(out) + (size_t)m * COUT + j0);
-                    o[0] = reinterpret_cast<const uint4*>(v)[0];
-                    o[1] = reinterpret_cast<const uint4*>(v)[1];
+                    // descriptors advance by address >> 4 in their low bits
+                    const uint64_t ad = adesc0 + (uint64_t)(s * (A_STAGE >> 4));
+                    const uint64_t bd = bdesc0 + (uint64_t)((tap * (CIN / 8) * B_LBO) >> 4);
+#pragma unroll
+                    for (int j = 0; j < CIN / 16; j++)
+                        mma_f16(acc, ad + (uint64_t)(2 * j), bd + (uint64_t)((2 * j * B_LBO) >> 4), ID,
+                                (tap > 0 || j > 0) ? 1u : 0u);
+                    mma_commit(empty0 + 8 * s);
+                    k++;
+                    s = s + 1 == S ? 0 : s + 1;
                 }
+                if (ok) mma_commit(smem_u32(&accf[i & 1]));
+            }
+            n_committed = k;
+        }
+    } else if (warp == 6) {
+        // waits for the MMA thread: a step is ready once its load has landed and, for a tile's
+        // first step, the tile's accumulator has been released.  Lanes 0..7 test the next 8
+        // steps at once (mbarrier.test_wait, each a round trip of a few hundred cycles); the
+        // run of ready steps from the first is published.  Testing at most S steps ahead
+        // keeps each barrier within one phase of the one tested, so the parity is exact.
+        constexpr int WL = 8;
+        static_assert(S >= WL, "test window");
+        int k = 0;   // steps published
+        long long t0 = 0;
+        bool waiting = false;
+        while (k < nsteps) {
+            const int kk = k + lane;
+            bool ready = false;
+            if (lane < WL && kk < nsteps) {
+                ready = mbar_test(smem_u32(&full[kk % S]), (kk / S) & 1);
+                const int i = kk / 9;
+                if (ready && kk % 9 == 0 && i >= 2) ready = mbar_test(smem_u32(&acce[i & 1]), ((i >> 1) - 1) & 1);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, ready);
+            const int run = __ffs(~m) - 1;   // ready steps from lane 0 on (at most WL: lanes >= WL vote no)
+            if (run > 0) {
+                k += run;
+                if (lane == 0) st_release(&n_ready, k);
+                waiting = false;
+            } else {
+                if (!waiting) {
+                    t0 = clock64();
+                    waiting = true;
+                }
+                int stop = 0;
+                if (lane == 0) {
+                    if (*abort) stop = 1;
+                    else if (clock64() - t0 > WAIT_CYCLES) {
+                        *abort = 1;
+                        stop = 1;
+                    }
+                }
+                if (__shfl_sync(0xffffffffu, stop, 0)) break;
             }
         }
+        if (lane == 0) n_consumed = k;
+    } else {   // epilogue, warps 0-3
+        for (int i = 0; i < mine; i++) {
+            const int a = i & 1;
+            const int t = (int)blockIdx.x + i * (int)gridDim.x;
+            const int b = t / per_img, r = t - b * per_img, ty = r / txn, tx = r - ty * txn;
+            uint4 mk[EPI == EPI_MASK_BF16 ? COUT * 2 / 16 : 1];
+            if constexpr (EPI == EPI_MASK_BF16) conv_mask_load<COUT>(mk, warp, lane, b, ty * TY, tx * TX, H, W, mask);
+            int ok = 0;
+            if (lane == 0) ok = mbar_wait_role(smem_u32(&accf[a]), (i >> 1) & 1, abort);
+            if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            conv_epilogue<COUT, EPI>(tmem + (uint32_t)(a * COUT), warp, lane, stg + warp * 32 * Sh::RB, b, ty * TY,
+                                     tx * TX, H, W, sbias, mk, out);
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[a]);
+        }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0 && done) tmem_free(tmem, TCOLS);
+    bool done = true;
+    if (abort_flag) {
+        // loads still landing (issued, never waited for by the MMA warp), then the MMAs issued
+        // (their last commit covers all of them)
+        if (tid == 0) {
+            atomicExch(err, 1);
+            for (int k = n_consumed; k < n_consumed + S && done; k++)
+                if (k < n_loaded[k % CONV_LOADERS])
+                    done = mbar_wait_bounded(smem_u32(&full[k % S]), (k / S) & 1, WAIT_CYCLES);
+            if (n_committed > 0 && done)
+                done = mbar_wait_bounded(smem_u32(&empty[(n_committed - 1) % S]), ((n_committed - 1) / S) & 1, WAIT_CYCLES);
+            abort_flag = done ? 1 : 2;
+        }
+        __syncthreads();
+        done = abort_flag == 1;
+    }
+    if (warp == 4 && done) {
+        __syncwarp();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        tmem_free(tmem, TCOLS);
+    }
 }
-
-template <int CIN, int COUT>
-constexpr int conv_smem() { return TM * 9 * CIN * 2 + COUT * 9 * CIN * 2; }
 
 // The same convolution on the CUDA cores (FP32 accumulation in tap-channel order): the
 // reference the tensor-core kernel is checked against on the device.  One thread per output.
@@ -658,22 +977,78 @@ int check_dims(int B, int H4, int W4)
 }
 inline bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
-// launch k_conv_tc for a (CIN, COUT) pair that the network has
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library does not link
+// the driver)
+EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// the tensor map of a B x H x W x C BF16 NHWC activation for the convolution's loads: box
+// (C, TX, TY, 1), rows of C * 2 bytes swizzled at that width, zeros outside
+int conv_input_map(CUtensorMap* map, const void* x, int C, int B, int H, int W)
+{
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return lfail(PM_ECUDA, "the driver lacks cuTensorMapEncodeTiled");
+    const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    const cuuint32_t box[4] = {(cuuint32_t)C, TX, TY, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUtensorMapSwizzle sw = C == 64   ? CU_TENSOR_MAP_SWIZZLE_128B
+                                  : C == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                            : CU_TENSOR_MAP_SWIZZLE_32B;
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return lfail(PM_ECUDA, "cuTensorMapEncodeTiled failed for the convolution input");
+    return PM_OK;
+}
+
+// launch k_conv_tc for a (CIN, COUT) pair that the network has: one CTA per SM (persistent)
 template <int CIN, int COUT>
 int conv_tc(int epi, const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, const __nv_bfloat16* mk, void* out,
             int B, int H, int W, int dil, int* err, cudaStream_t st)
 {
-    constexpr int SM = conv_smem<CIN, COUT>();
-    const int grid = (B * H * W + TM - 1) / TM;
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            nsm = 148;
+    }
+    CUtensorMap map;
+    int rc = conv_input_map(&map, x, CIN, B, H, W);
+    if (rc) return rc;
+    const long long ntiles = (long long)B * ((H + TY - 1) / TY) * ((W + TX - 1) / TX);
+    const int grid = (int)(ntiles < nsm ? ntiles : nsm);
     if (epi == EPI_RELU_BF16) {
+        constexpr int SM = ConvShape<CIN, COUT, EPI_RELU_BF16>::SMEM;
         cudaFuncSetAttribute(k_conv_tc<CIN, COUT, EPI_RELU_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
-        k_conv_tc<CIN, COUT, EPI_RELU_BF16><<<grid, TM, SM, st>>>(x, w, bias, mk, out, B, H, W, dil, err);
+        k_conv_tc<CIN, COUT, EPI_RELU_BF16><<<grid, CONV_THREADS, SM, st>>>(map, w, bias, mk, out, B, H, W, dil, err);
     } else if (epi == EPI_BIAS_F32) {
-        cudaFuncSetAttribute(k_conv_tc<CIN, COUT, EPI_BIAS_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
-        k_conv_tc<CIN, COUT, EPI_BIAS_F32><<<grid, TM, SM, st>>>(x, w, bias, mk, out, B, H, W, dil, err);
+        if constexpr (COUT == OUT_CH) {   // the last layer only
+            constexpr int SM = ConvShape<CIN, COUT, EPI_BIAS_F32>::SMEM;
+            cudaFuncSetAttribute(k_conv_tc<CIN, COUT, EPI_BIAS_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+            k_conv_tc<CIN, COUT, EPI_BIAS_F32><<<grid, CONV_THREADS, SM, st>>>(map, w, bias, mk, out, B, H, W, dil, err);
+        } else {
+            return lfail(PM_EINVAL_ARG, "an FP32 output is the last layer's only");
+        }
     } else {
+        constexpr int SM = ConvShape<CIN, COUT, EPI_MASK_BF16>::SMEM;
         cudaFuncSetAttribute(k_conv_tc<CIN, COUT, EPI_MASK_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
-        k_conv_tc<CIN, COUT, EPI_MASK_BF16><<<grid, TM, SM, st>>>(x, w, bias, mk, out, B, H, W, dil, err);
+        k_conv_tc<CIN, COUT, EPI_MASK_BF16><<<grid, CONV_THREADS, SM, st>>>(map, w, bias, mk, out, B, H, W, dil, err);
     }
     return check_launch("k_conv_tc");
 }

@@ -57,14 +57,17 @@ def run_conv(torch, native, layer, mode, tc, x, w, b, mask, B, H, W):
     return to_np(out)
 
 
+@pytest.mark.parametrize("dims", [(2, 11, 37), (1, 5, 9), (3, 24, 40)])
 @pytest.mark.parametrize("layer", range(8))
-def test_conv_layers_tensor_cores_match_cuda_cores_and_oracle(torch_cuda, native, layer):
-    """forward and data gradient of each layer (its channel counts and dilation) on 2 maps of
-    11 x 37 feature pixels (a partial last tile of 128 pixels; dilation 16 reaches past the map)"""
+def test_conv_layers_tensor_cores_match_cuda_cores_and_oracle(torch_cuda, native, layer, dims):
+    """forward and data gradient of each layer (its channel counts and dilation) on B maps of
+    H x W feature pixels: 11 x 37 (partial 16 x 8 tiles at the right and bottom; dilation 16
+    reaches past the map), 5 x 9 (a map smaller than one tile), 3 maps of 24 x 40 (several
+    tiles per map and per CTA)"""
     torch = torch_cuda
     ci, co, dil = O.SHAPES[layer]
-    B, H, W = 2, 11, 37
-    rng = np.random.default_rng(layer)
+    B, H, W = dims
+    rng = np.random.default_rng(layer + 100 * H)
     xn = O.bf16(rng.standard_normal((B, H, W, ci)).astype(np.float32))
     wn = O.bf16((rng.standard_normal((co, 9 * ci)) * 0.1).astype(np.float32))
     bn = (rng.standard_normal(co) * 0.1).astype(np.float32)
