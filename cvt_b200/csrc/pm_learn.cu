@@ -58,8 +58,6 @@ constexpr int LDIL[NL] = {1, 1, 2, 4, 8, 16, 1, 1};
 constexpr int IN_CH = 16, OUT_CH = 16, MAX_CH = 64;
 constexpr int TM = 128;                           // pixels per CTA (conv)
 constexpr long long WAIT_CYCLES = 4000000000ll;   // about two seconds at the B200's clock
-constexpr int WG_PIX = 1024;                      // pixels per CTA of the weight gradient
-constexpr int WG_G = 4;                           // K steps of 16 pixels per stage
 
 enum { EPI_RELU_BF16 = 0, EPI_BIAS_F32 = 1, EPI_MASK_BF16 = 2 };
 
@@ -613,123 +611,154 @@ __global__ void k_conv_ref(const __nv_bfloat16* __restrict__ in, const __nv_bflo
     else static_cast<__nv_bfloat16*>(out)[i] = __float2bfloat16_rn(__bfloat162float(mask[i]) > 0.0f ? acc : 0.0f);
 }
 
-// Weight gradient on the tensor cores, stage 1: CTA `blockIdx.x` sums over its WG_PIX pixels
-// D[r][co] = sum_p A[r][p] dy[p][co] with A[t * CIN + ci][p] = x[p shifted by tap t][ci] and
-// A[9 * CIN][p] = 1 (the bias gradient), and writes part[cta][r][co] for r <= 9 * CIN.
-// Shared memory per K step (16 pixels), MN-major without swizzle: core matrices of 8 pixel rows
-// x 16 bytes (8 channels); the two K halves of a channel group side by side (LBO = 128 bytes),
-// the channel groups 256 bytes apart (SBO).  Both strides stay inside the tile whichever way
-// the descriptor fields are read, so no access can leave the stage's buffer.
+// Weight gradient on the tensor cores, stage 1: D[r][co] = sum over pixels p of A[r][p] dy[p][co]
+// with A[t * CIN + ci][p] = x[p shifted by tap t][ci] and A[9 * CIN][p] = 1 (the bias
+// gradient).  Persistent: CTA c sums over units c, c + grid, ... of TX x WG_TY pixels (one
+// image's rows) and writes part[c][r][co] for r <= 9 * CIN.  A unit's operands are TMA boxes:
+// x at the unit shifted by each tap (box (CIN, TX, WG_TY, 1), zeros outside the image) and dy
+// at the unit (zeros outside, so pixels past the image add nothing), each landing as an
+// MN-major operand swizzled at its row width (pixel = K row, channels = M or N): an M block of
+// 128 rows is 128 / CIN consecutive tap boxes, one swizzle atom per box along M (LBO = a box),
+// the last block padded with a box whose first channel is 1 (the row of ones) and zero boxes,
+// written once per buffer.  Warp 1, lanes 0..9, issue a unit's 10 boxes into a ring of STAGES
+// buffers; warp 0's lane 0 issues its MB x WG_TY MMAs (M128, N COUT, K16) into MB TMEM
+// accumulators that persist over all the CTA's units, and commits each unit to its buffer's
+// empty barrier; at the end all four warps read TMEM (tcgen05.ld 32x32b) and store the partial
+// sums.  Every wait is bounded, as in k_conv_tc.
+constexpr int WG_TY = 4;                  // pixel rows of a unit: 16 x 4 = 64 pixels = 4 K steps
+constexpr int WG_PX = TX * WG_TY;
+constexpr int WG_MAX_CTAS = 160;          // the partial sums' scratch is sized for this many CTAs
+
 template <int CIN, int COUT>
 struct WgradShape {
     static constexpr int ROWS = 9 * CIN + 1;          // (tap, ci) rows and the row of ones
     static constexpr int MB = (ROWS + 127) / 128;     // M blocks of 128 rows
-    static constexpr int A_KSTEP = MB * 16 * 256;     // bytes of A per K step
-    static constexpr int B_KSTEP = (COUT / 8) * 256;  // bytes of B per K step
-    static constexpr int STAGE = WG_G * (A_KSTEP + B_KSTEP);
-    static constexpr int SMEM = 2 * STAGE;
+    static constexpr int TPB = 128 / CIN;             // boxes per M block
+    static constexpr int NBOX = MB * TPB;             // 9 tap boxes, the ones box, zero boxes
+    static constexpr int XROW = CIN * 2, DROW = COUT * 2;
+    static constexpr int XBOX = WG_PX * XROW, DBOX = WG_PX * DROW;
+    static constexpr int STAGE = NBOX * XBOX + DBOX;
+    static constexpr int LOADED = 9 * XBOX + DBOX;    // bytes the TMA brings per unit
+    static constexpr int FIT = (220 * 1024 - 1024) / STAGE;
+    static constexpr int STAGES = FIT > 4 ? 4 : FIT;
+    static constexpr int SMEM = STAGES * STAGE + 1024;
     static constexpr int TCOLS = tmem_cols(MB * COUT);
+    static_assert(STAGES >= 2 && NBOX >= 10 && MB * COUT <= 512, "weight-gradient shape");
+    static_assert(STAGE % 1024 == 0 && XBOX % 1024 == 0, "swizzle atoms stay aligned");
 };
 
+// descriptor of an MN-major operand swizzled at its row width (row = 32, 64 or 128 bytes: one
+// swizzle atom is 8 K rows of one row width along MN): LBO = the stride between atoms along MN
+// (an operand one atom wide passes 8 rows, so that every field stays inside its buffer),
+// SBO = the stride between 8-row groups along K
+__device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr, int row, uint32_t lbo)
+{
+    const uint64_t lt = row == 128 ? 2u : row == 64 ? 4u : 6u;
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)(((8 * row) >> 4) & 0x3FFF) << 32) | (1ull << 46) | (lt << 61);
+}
+
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(128) k_wgrad_tc(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ dy,
-                                                  float* __restrict__ part, int B, int H, int W, int dil, int* err)
+__global__ void __launch_bounds__(128, 1)
+    k_wgrad_tc(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dmap,
+               float* __restrict__ part, int B, int H, int W, int dil, int* err)
 {
     using S = WgradShape<CIN, COUT>;
-    extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(8) uint64_t mbar[2];
-    __shared__ uint32_t tmem_base;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int M = B * H * W;
-    const int p0 = blockIdx.x * WG_PIX;
-    constexpr int NGROUPS = WG_PIX / (16 * WG_G);
+    constexpr int NS = S::STAGES;
     constexpr uint32_t ID = idesc(128, COUT, true, true);
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full[NS], empty[NS], done_bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int abort_flag, n_loaded, n_seen, n_committed;
+    volatile int* abort = &abort_flag;
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t sbase = (raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (sbase - raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int txn = (W + TX - 1) / TX, tyn = (H + WG_TY - 1) / WG_TY, per_img = txn * tyn;
+    const int nunits = B * per_img;
+    const int mine = (int)blockIdx.x < nunits ? (nunits - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
-    // rows 9 * CIN .. of every K step of both stages: the row of ones, then zeros
-    for (int i = tid; i < 2 * WG_G * 16 * (S::MB * 16 - 9 * CIN / 8); i += 128) {
-        const int per = 16 * (S::MB * 16 - 9 * CIN / 8);
-        const int ks = i / per, rem = i - ks * per;
-        const int mi = 9 * CIN / 8 + rem / 16, k = rem % 16;
-        uint8_t* a = smem + (ks / WG_G) * S::STAGE + (ks % WG_G) * S::A_KSTEP;
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (mi == 9 * CIN / 8) v.x = 0x3F80u;   // BF16 1.0 in the first element of the row
-        *reinterpret_cast<uint4*>(a + mi * 256 + (k >> 3) * 128 + (k & 7) * 16) = v;
-    }
-    // stage g's copies: 16 * WG_G pixels, each the 9 taps x CIN / 8 chunks of A and COUT / 8 of B
-    auto stage = [&](int g) {
-        uint8_t* base = smem + (g & 1) * S::STAGE;
-        constexpr int QA = 9 * CIN / 8, QB = COUT / 8;
-        for (int i = tid; i < 16 * WG_G * (QA + QB); i += 128) {
-            const int kk = i / (QA + QB), q = i - kk * (QA + QB);
-            const int ks = kk >> 4, k = kk & 15;
-            const int p = p0 + g * 16 * WG_G + kk;
-            if (q < QA) {
-                const int t = q / (CIN / 8), c = q - t * (CIN / 8);
-                const int src = tap_pixel(p, M, H, W, t, dil);
-                uint8_t* a = base + ks * S::A_KSTEP;
-                cp16(a + q * 256 + (k >> 3) * 128 + (k & 7) * 16,
-                     reinterpret_cast<const uint4*>(x + (size_t)(src < 0 ? 0 : src) * CIN) + c, src >= 0);
-            } else {
-                const int c = q - QA;
-                uint8_t* b = base + WG_G * S::A_KSTEP + ks * S::B_KSTEP;
-                cp16(b + c * 256 + (k >> 3) * 128 + (k & 7) * 16,
-                     reinterpret_cast<const uint4*>(dy + (size_t)(p < M ? p : 0) * COUT) + c, p < M);
-            }
+    // the constant boxes 9 .. NBOX - 1 of every buffer: box 9 has 1 in channel 0 of every pixel
+    // row (the row of ones; chunk 0 of row r sits at chunk 0 ^ swizzle(r)), the rest zeros
+    {
+        constexpr int NQ = S::XROW / 16, PPR = 128 / S::XROW, CH = S::XBOX / 16;
+        for (int i = tid; i < NS * (S::NBOX - 9) * CH; i += 128) {
+            const int st = i / ((S::NBOX - 9) * CH), rem = i - st * ((S::NBOX - 9) * CH);
+            const int bx = 9 + rem / CH, c = rem % CH, r = c / NQ, pc = c % NQ;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (bx == 9 && (pc ^ ((r / PPR) % NQ)) == 0) v.x = 0x3F80u;   // BF16 1.0
+            *reinterpret_cast<uint4*>(gbase + st * S::STAGE + bx * S::XBOX + c * 16) = v;
         }
-        cp_commit();
-    };
+    }
     if (warp == 0) tmem_alloc(&tmem_base, S::TCOLS);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
-        asm volatile("fence.mbarrier_init.release.cluster;");
+        for (int i = 0; i < NS; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(&done_bar, 1);
+        abort_flag = 0;
+        n_loaded = 0;
+        n_seen = 0;
+        n_committed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    stage(0);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the constant boxes, for the tensor cores
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
-    bool ok = true;
-    for (int g = 0; g < NGROUPS; g++) {
-        cp_wait_all();
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (tid == 0) {
-            const uint32_t base = smem_u32(smem + (g & 1) * S::STAGE);
-#pragma unroll 1
-            for (int ks = 0; ks < WG_G; ks++) {
-                const uint32_t a = base + ks * S::A_KSTEP, b = base + WG_G * S::A_KSTEP + ks * S::B_KSTEP;
+
+    if (warp == 1) {   // loads: lane b < 9 the box of tap b, lane 9 the dy box
+        int k = 0;
+        for (; k < mine; k++) {
+            const int st = k % NS, use = k / NS;
+            int ok = 1;
+            if (lane == 0 && use > 0) ok = mbar_wait_role(smem_u32(&empty[st]), (use - 1) & 1, abort);
+            if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+            const int u = (int)blockIdx.x + k * (int)gridDim.x;
+            const int b = u / per_img, r = u - b * per_img, uy = r / txn, ux = r - uy * txn;
+            const int x0 = ux * TX, y0 = uy * WG_TY;
+            const uint32_t fb = smem_u32(&full[st]), dst = sbase + st * S::STAGE;
+            if (lane == 0) mbar_expect_tx(fb, S::LOADED);
+            __syncwarp();
+            if (lane < 9)
+                tma_load_4d(dst + lane * S::XBOX, &xmap, fb, 0, x0 + (lane % 3 - 1) * dil, y0 + (lane / 3 - 1) * dil, b);
+            else if (lane == 9)
+                tma_load_4d(dst + S::NBOX * S::XBOX, &dmap, fb, 0, x0, y0, b);
+        }
+        if (lane == 0) n_loaded = k;
+    } else if (warp == 0 && lane == 0) {   // MMAs
+        int k = 0, committed = 0;
+        for (; k < mine; k++) {
+            const int st = k % NS;
+            if (!mbar_wait_role(smem_u32(&full[st]), (k / NS) & 1, abort)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = sbase + st * S::STAGE, b0 = a0 + S::NBOX * S::XBOX;
+#pragma unroll
+            for (int ks = 0; ks < WG_TY; ks++)
 #pragma unroll
                 for (int j = 0; j < S::MB; j++)
-                    mma_f16(tmem + j * COUT, smem_desc(a + j * 16 * 256, 128, 256), smem_desc(b, 128, 256), ID,
-                            (g > 0 || ks > 0) ? 1u : 0u);
-            }
-            mma_commit(smem_u32(&mbar[g & 1]));
+                    mma_f16(tmem + j * COUT, smem_desc_mn(a0 + j * S::TPB * S::XBOX + ks * 16 * S::XROW, S::XROW, S::XBOX),
+                            smem_desc_mn(b0 + ks * 16 * S::DROW, S::DROW, 8 * S::DROW), ID, (k > 0 || ks > 0) ? 1u : 0u);
+            mma_commit(smem_u32(&empty[st]));
+            committed = k + 1;
         }
-        if (g + 1 < NGROUPS) {
-            // the buffer of stage g + 1 was read by the MMAs of stage g - 1
-            if (g >= 1 && !mbar_wait_bounded(smem_u32(&mbar[(g + 1) & 1]), ((g - 1) >> 1) & 1, WAIT_CYCLES)) {
-                ok = false;
-                atomicExch(err, 1);
-                break;
-            }
-            stage(g + 1);
-        }
+        n_seen = k;
+        n_committed = committed;
+        if (k == mine) mma_commit(smem_u32(&done_bar));   // covers every MMA of the CTA
     }
-    cp_wait_all();
-    // the last commit covers every earlier MMA of the CTA
-    bool done = ok && mbar_wait_bounded(smem_u32(&mbar[(NGROUPS - 1) & 1]), ((NGROUPS - 1) >> 1) & 1, WAIT_CYCLES);
-    if (!done) {
-        atomicExch(err, 1);
-        done = mbar_wait_bounded(smem_u32(&mbar[(NGROUPS - 1) & 1]), ((NGROUPS - 1) >> 1) & 1, WAIT_CYCLES);
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (done) {
+    // all four warps: the partial sums
+    int ok = 1;
+    if (lane == 0) ok = mbar_wait_role(smem_u32(&done_bar), 0, abort);
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (ok) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         float* dst = part + (size_t)blockIdx.x * (9 * CIN + 1) * COUT;
 #pragma unroll 1
         for (int j = 0; j < S::MB; j++) {
-            const int row = j * 128 + warp * 32 + (tid & 31);
+            const int row = j * 128 + warp * 32 + lane;
 #pragma unroll
             for (int c0 = 0; c0 < COUT; c0 += 16) {
                 uint32_t r[16];
@@ -745,9 +774,27 @@ __global__ void __launch_bounds__(128) k_wgrad_tc(const __nv_bfloat16* __restric
             }
         }
     }
+    __syncthreads();
+    bool done = true;
+    if (abort_flag) {
+        // loads still landing (issued, never seen by the MMA thread), then the MMAs issued
+        if (tid == 0) {
+            atomicExch(err, 1);
+            for (int k = n_seen; k < n_loaded && done; k++)
+                done = mbar_wait_bounded(smem_u32(&full[k % NS]), (k / NS) & 1, WAIT_CYCLES);
+            if (n_committed > 0 && done)
+                done = mbar_wait_bounded(smem_u32(&empty[(n_committed - 1) % NS]), ((n_committed - 1) / NS) & 1, WAIT_CYCLES);
+            abort_flag = done ? 1 : 2;
+        }
+        __syncthreads();
+        done = abort_flag == 1;
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0 && done) tmem_free(tmem, S::TCOLS);
+    if (warp == 0 && done) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        tmem_free(tmem, S::TCOLS);
+    }
 }
 
 // weight gradient, stage 2: grad[co][r] (r < 9 CIN) and grad[COUT * 9 CIN + co] (bias) = sums of
@@ -997,15 +1044,15 @@ EncodeTiledFn encode_tiled()
     return fn;
 }
 
-// the tensor map of a B x H x W x C BF16 NHWC activation for the convolution's loads: box
-// (C, TX, TY, 1), rows of C * 2 bytes swizzled at that width, zeros outside
-int conv_input_map(CUtensorMap* map, const void* x, int C, int B, int H, int W)
+// the tensor map of a B x H x W x C BF16 NHWC activation for the tensor-core kernels' loads:
+// box (C, TX, rows, 1), rows of C * 2 bytes swizzled at that width, zeros outside
+int act_map(CUtensorMap* map, const void* x, int C, int B, int H, int W, int rows)
 {
     EncodeTiledFn enc = encode_tiled();
     if (!enc) return lfail(PM_ECUDA, "the driver lacks cuTensorMapEncodeTiled");
     const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
     const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
-    const cuuint32_t box[4] = {(cuuint32_t)C, TX, TY, 1};
+    const cuuint32_t box[4] = {(cuuint32_t)C, (cuuint32_t)TX, (cuuint32_t)rows, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUtensorMapSwizzle sw = C == 64   ? CU_TENSOR_MAP_SWIZZLE_128B
                                   : C == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
@@ -1013,7 +1060,7 @@ int conv_input_map(CUtensorMap* map, const void* x, int C, int B, int H, int W)
     const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return lfail(PM_ECUDA, "cuTensorMapEncodeTiled failed for the convolution input");
+    if (r != CUDA_SUCCESS) return lfail(PM_ECUDA, "cuTensorMapEncodeTiled failed for an activation");
     return PM_OK;
 }
 
@@ -1029,7 +1076,7 @@ int conv_tc(int epi, const __nv_bfloat16* x, const __nv_bfloat16* w, const float
             nsm = 148;
     }
     CUtensorMap map;
-    int rc = conv_input_map(&map, x, CIN, B, H, W);
+    int rc = act_map(&map, x, CIN, B, H, W, TY);
     if (rc) return rc;
     const long long ntiles = (long long)B * ((H + TY - 1) / TY) * ((W + TX - 1) / TX);
     const int grid = (int)(ntiles < nsm ? ntiles : nsm);
@@ -1069,13 +1116,26 @@ int wgrad_tc(const __nv_bfloat16* x, const __nv_bfloat16* dy, float* part, float
              int* err, cudaStream_t st)
 {
     using Sh = WgradShape<CIN, COUT>;
-    const int M = B * H * W, nb = (M + WG_PIX - 1) / WG_PIX;
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            nsm = 148;
+    }
+    CUtensorMap xm, dm;
+    int rc = act_map(&xm, x, CIN, B, H, W, WG_TY);
+    if (rc) return rc;
+    rc = act_map(&dm, dy, COUT, B, H, W, WG_TY);
+    if (rc) return rc;
+    const long long units = (long long)B * ((H + WG_TY - 1) / WG_TY) * ((W + TX - 1) / TX);
+    long long grid = units < nsm ? units : nsm;
+    if (grid > WG_MAX_CTAS) grid = WG_MAX_CTAS;
     cudaFuncSetAttribute(k_wgrad_tc<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::SMEM);
-    k_wgrad_tc<CIN, COUT><<<nb, 128, Sh::SMEM, st>>>(x, dy, part, B, H, W, dil, err);
-    int rc = check_launch("k_wgrad_tc");
+    k_wgrad_tc<CIN, COUT><<<(int)grid, 128, Sh::SMEM, st>>>(xm, dm, part, B, H, W, dil, err);
+    rc = check_launch("k_wgrad_tc");
     if (rc) return rc;
     const int n = (9 * CIN + 1) * COUT;
-    k_wgrad_sum<<<(n + 255) / 256, 256, 0, st>>>(part, grad, nb, CIN, COUT);
+    k_wgrad_sum<<<(n + 255) / 256, 256, 0, st>>>(part, grad, (int)grid, CIN, COUT);
     return check_launch("k_wgrad_sum");
 }
 
@@ -1137,8 +1197,8 @@ int pm_lpp_conv(int layer, int mode, int tensor_cores, const void* in, const voi
 size_t pm_lpp_wgrad_scratch_floats(int layer, int B, int H4, int W4)
 {
     if (layer < 0 || layer >= NL || B <= 0 || H4 <= 0 || W4 <= 0) return 0;
-    const long long M = (long long)B * H4 * W4;
-    return (size_t)((M + WG_PIX - 1) / WG_PIX) * (9 * LCIN[layer] + 1) * LCOUT[layer];
+    const long long units = (long long)B * ((H4 + WG_TY - 1) / WG_TY) * ((W4 + TX - 1) / TX);
+    return (size_t)(units < WG_MAX_CTAS ? units : WG_MAX_CTAS) * (9 * LCIN[layer] + 1) * LCOUT[layer];
 }
 
 int pm_lpp_wgrad(int layer, int tensor_cores, const void* x, const void* dy, float* scratch, float* grad, int B, int H4,
