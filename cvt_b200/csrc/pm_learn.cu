@@ -797,16 +797,31 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
-// weight gradient, stage 2: grad[co][r] (r < 9 CIN) and grad[COUT * 9 CIN + co] (bias) = sums of
-// the CTAs' partials in CTA order
+// weight gradient, stage 2: grad[co][r] (r < 9 CIN) and grad[COUT * 9 CIN + co] (bias) = the sum
+// of the CTAs' partials, in a fixed order (deterministic): first WG_SUM_GROUPS groups of
+// consecutive CTAs, each summed in CTA order into the group's first partial (in place), then
+// the group sums in group order.
+constexpr int WG_SUM_GROUPS = 8;
+__global__ void k_wgrad_sum_groups(float* __restrict__ part, int nblocks, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, g = blockIdx.y;
+    const int per = (nblocks + WG_SUM_GROUPS - 1) / WG_SUM_GROUPS;
+    const int b0 = g * per, b1 = b0 + per < nblocks ? b0 + per : nblocks;
+    if (i >= n || b0 >= b1) return;
+    float s = 0.0f;
+#pragma unroll 4
+    for (int b = b0; b < b1; b++) s += __ldg(part + (size_t)b * n + i);
+    part[(size_t)b0 * n + i] = s;
+}
 __global__ void k_wgrad_sum(const float* __restrict__ part, float* __restrict__ grad, int nblocks, int CIN, int COUT)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int rows = 9 * CIN + 1;
-    if (i >= rows * COUT) return;
+    const int rows = 9 * CIN + 1, n = rows * COUT;
+    if (i >= n) return;
     const int r = i / COUT, co = i - r * COUT;
+    const int per = (nblocks + WG_SUM_GROUPS - 1) / WG_SUM_GROUPS;
     float s = 0.0f;
-    for (int b = 0; b < nblocks; b++) s += part[(size_t)b * rows * COUT + i];
+    for (int b = 0; b < nblocks; b += per) s += part[(size_t)b * n + i];
     if (r < 9 * CIN) grad[(size_t)co * 9 * CIN + r] = s;
     else grad[(size_t)COUT * 9 * CIN + co] = s;
 }
@@ -1135,6 +1150,9 @@ int wgrad_tc(const __nv_bfloat16* x, const __nv_bfloat16* dy, float* part, float
     rc = check_launch("k_wgrad_tc");
     if (rc) return rc;
     const int n = (9 * CIN + 1) * COUT;
+    k_wgrad_sum_groups<<<dim3((n + 255) / 256, WG_SUM_GROUPS), 256, 0, st>>>(part, (int)grid, n);
+    rc = check_launch("k_wgrad_sum_groups");
+    if (rc) return rc;
     k_wgrad_sum<<<(n + 255) / 256, 256, 0, st>>>(part, grad, (int)grid, CIN, COUT);
     return check_launch("k_wgrad_sum");
 }

@@ -428,8 +428,9 @@ int pm_lpp_input(const uint8_t* left, const uint8_t* right, int W, int H, size_t
 int pm_lpp_conv(int layer, int mode, int tensor_cores, const void* in, const void* w, const float* bias,
                 const void* mask, void* out, int B, int H4, int W4, int* err, void* stream);
 /* weight and bias gradients of layer `layer` (COUT * 9 * CIN then COUT floats) from its input x
- * and the gradient dy of its output; the tensor-core path sums 1024-pixel blocks into
- * `scratch` (pm_lpp_wgrad_scratch_floats floats) and then the blocks in order (deterministic) */
+ * and the gradient dy of its output; the tensor-core path writes one partial sum per CTA (each
+ * CTA sums a fixed set of 16 x 4-pixel units) into `scratch` (pm_lpp_wgrad_scratch_floats
+ * floats) and then reduces them in a fixed order (deterministic) */
 size_t pm_lpp_wgrad_scratch_floats(int layer, int B, int H4, int W4);
 int pm_lpp_wgrad(int layer, int tensor_cores, const void* x, const void* dy, float* scratch, float* grad, int B, int H4,
                  int W4, int* err, void* stream);

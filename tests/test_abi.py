@@ -339,8 +339,10 @@ def test_lpp_rejects_bad_arguments_without_touching_the_device(native):
     assert native.pm_lpp_propose_device(None, None, 4, None, None, 64, 48, 256, 0, 64.0, None, None, None, 0, None,
                                         None) == _lib.PM_EINVAL_ARG
     assert native.pm_lpp_wgrad_scratch_floats(8, 1, 4, 4) == 0
-    # one 1024-pixel block of partial sums per CTA: 9 * CIN + 1 rows (the last one the bias) x COUT
-    assert native.pm_lpp_wgrad_scratch_floats(3, 1, 32, 40) == 2 * (9 * 64 + 1) * 64
+    # partial sums per CTA, at most one CTA per 16 x 4-pixel unit and at most 160 CTAs:
+    # 9 * CIN + 1 rows (the last one the bias) x COUT
+    assert native.pm_lpp_wgrad_scratch_floats(3, 1, 32, 40) == 8 * 3 * (9 * 64 + 1) * 64
+    assert native.pm_lpp_wgrad_scratch_floats(3, 32, 96, 128) == 160 * (9 * 64 + 1) * 64
 
 
 def test_autotuner_keeps_the_fastest_branch_count():

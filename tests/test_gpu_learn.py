@@ -101,14 +101,16 @@ def test_conv_layers_tensor_cores_match_cuda_cores_and_oracle(torch_cuda, native
     assert one_rounding(got_tc, want).all()
 
 
+@pytest.mark.parametrize("dims", [(3, 19, 41), (4, 40, 64)])
 @pytest.mark.parametrize("layer", range(8))
-def test_weight_gradients_tensor_cores_match_cuda_cores_and_oracle(torch_cuda, native, layer):
-    """weight and bias gradients of each layer over 3 maps of 19 x 41 (2337 pixels: three
-    1024-pixel blocks, the last one partial)"""
+def test_weight_gradients_tensor_cores_match_cuda_cores_and_oracle(torch_cuda, native, layer, dims):
+    """weight and bias gradients of each layer over 3 maps of 19 x 41 (45 units of 16 x 4
+    pixels, partial at the right and bottom) and 4 maps of 40 x 64 (160 units: CTAs that sum
+    two units, partial sums reduced in groups)"""
     torch = torch_cuda
     ci, co, dil = O.SHAPES[layer]
-    B, H, W = 3, 19, 41
-    rng = np.random.default_rng(10 + layer)
+    B, H, W = dims
+    rng = np.random.default_rng(10 + layer + H)
     xn = O.bf16(rng.standard_normal((B, H, W, ci)).astype(np.float32))
     dyn = O.bf16(rng.standard_normal((B, H, W, co)).astype(np.float32))
     x, dy = bf(torch, xn), bf(torch, dyn)
