@@ -696,6 +696,16 @@ def learned_sweep(pm, prop, dL, dR, wl, timed, plain_ms, plain_res, ks=(1, 2, 4,
         rows.append(row)
         if found is None and c_k <= 1.01 * c_plain and agree >= 0.98:
             found = row
+    # plain random-init PatchMatch run on past the configured 8 iterations, against its own
+    # 8-iteration result: how far plain itself still moves (the agreement criterion compares with
+    # a field that is not converged)
+    longer = []
+    for k in (12, 16):
+        rnd, t_r = timed(lambda: pm.disparity_map(dL, dR, r, dmax, k, pp=pp, planes=True))
+        c_r, d_r = stats(rnd)
+        longer.append({"iterations": k, "iterations_executed": executed(k), "random_ms": t_r,
+                       "random_cost_ratio": c_r / c_plain,
+                       "random_agree_1px": float(((d_r - d_plain).abs() < 1.0)[keep].float().mean().item())})
     _, t_prop = timed(lambda: (prop.propose(dL, dR, dmax, 0, dl, nl), prop.propose(dL, dR, dmax, 1, drr, nr)))
     prop.check_error()
     cfg4 = next((x for x in rows if x["iterations"] == 2), None)
@@ -706,7 +716,7 @@ def learned_sweep(pm, prop, dL, dR, wl, timed, plain_ms, plain_res, ks=(1, 2, 4,
             "plain_ms": plain_ms, "plain_mean_cost": c_plain, "proposal_ms_both_views": t_prop,
             "criterion": "mean cost <= 1.01 x plain and >= 98% of plain's kept pixels within 1 px, both views, "
                          "LR check",
-            "learned_plus_2": cfg4, "sweep": rows}
+            "learned_plus_2": cfg4, "sweep": rows, "plain_longer": longer}
 
 
 def run_learned(args, wl, rank, world, local):
