@@ -19,11 +19,15 @@ namespace pm {
 
 namespace {
 
-// block shape: a warp is 32 consecutive pixels of a row, PM_PROP_BY rows per block
+// block shape: PM_PROP_BX consecutive pixels of a row (a warp is 32 of them, or two rows of 16
+// when PM_PROP_BX = 16), PM_PROP_BY rows per block
+#ifndef PM_PROP_BX
+#define PM_PROP_BX 32
+#endif
 #ifndef PM_PROP_BY
 #define PM_PROP_BY 4
 #endif
-constexpr int PROP_BX = 32, PROP_BY = PM_PROP_BY, PROP_THREADS = PROP_BX * PROP_BY;
+constexpr int PROP_BX = PM_PROP_BX, PROP_BY = PM_PROP_BY, PROP_THREADS = PROP_BX * PROP_BY;
 // resident threads per SM asked of the register allocator for each kernel (768 threads =
 // 80 registers, 640 = 96; measured best at 768 for both)
 #ifndef PM_CHAIN_THREADS
