@@ -20,8 +20,9 @@
 // Blackwell specifics: the 7-channel bilinear reads of the second view and the
 // truncated absolute differences run as packed FP32 pairs (FFMA2 / FMUL2,
 // sm_100), the sign census packs the four gradient sign bits with byte
-// permutes, and the three Gauss-Newton taps at x'-1, x', x'+1 share four texels
-// when their fractional parts agree (checked exactly; otherwise each tap is
+// permutes, and the three Gauss-Newton taps at x'-1, x', x'+1 read four shared
+// texels whenever their floors chain (checked exactly; each with its own weight
+// where the fractional parts differ, near powers of two; otherwise each tap is
 // read on its own).  Every packed operation rounds per element exactly like its
 // scalar form, so results equal the scalar restatement bit for bit.
 #pragma once
@@ -59,6 +60,7 @@ __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y
 #ifndef PM_STRICT_FMUL2
 #define PM_STRICT_FMUL2 1
 #endif
+
 template <bool F>
 __device__ __forceinline__ float2 lerp2(float2 a2, float2 b2, float2 t0, float2 t1)
 {
@@ -341,16 +343,22 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
             const uint32_t sb1 = __float_as_uint(q.w);
             const KltWeights kw = klt_weights<F>(w1);
             const float p2x = F ? fmaf(s.x, qx, byq) + s.z : s.x * qx + byq + s.z;
-            // Common case: 1 <= p2x < W - 1 and p2x + 1.5 in the binade of p2x.  Then p2x is a
-            // multiple of its ulp (<= 0.5), every +-1 and +-0.5 below is exact, the three taps'
-            // coordinates are p2x - 1, p2x, p2x + 1 and they share the weight p2x - floor(p2x).
-            // Otherwise the coordinates are formed as the source forms them and compared.
-            float f0, a0;
-            bool shared = p2x >= 1.0f && p2x < fWm1 &&
-                          ((__float_as_uint(p2x + 1.5f) ^ __float_as_uint(p2x)) < 0x00800000u);
-            if (shared) {
+            // The three taps read at t - 1, t, t + 1 (t the tap coordinate minus 0.5, each formed
+            // as the source forms it).  Common case: 1 <= p2x < W - 1 and p2x + 1.5 in the binade
+            // of p2x; then p2x is a multiple of its ulp (<= 0.5), every +-1 and +-0.5 below is
+            // exact, the coordinates are p2x - 1, p2x, p2x + 1 and share the weight
+            // p2x - floor(p2x).  Otherwise the coordinates and their floors are formed exactly;
+            // when the floors still chain (f0 - 1, f0, f0 + 1) the taps read the same four texels
+            // with their own weights, and only then, or off the padded row, each tap is read on
+            // its own.  Every path gives the bilinear values lerp_texel_at gives.
+            float f0, am, a0, ap;
+            bool chain = p2x >= 1.0f && p2x < fWm1 &&
+                         ((__float_as_uint(p2x + 1.5f) ^ __float_as_uint(p2x)) < 0x00800000u);
+            if (chain) {
                 f0 = floorf(p2x);
                 a0 = p2x - f0;
+                am = a0;
+                ap = a0;
             } else {
                 const float t0 = (p2x + 0.5f) - 0.5f;
                 const float tp = ((p2x + 1.0f) + 0.5f) - 0.5f;
@@ -358,24 +366,27 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
                 f0 = floorf(t0);
                 const float fp = floorf(tp), fm = floorf(tm);
                 a0 = t0 - f0;
-                shared = fp == f0 + 1.0f && fm == f0 - 1.0f && tp - fp == a0 && tm - fm == a0 && f0 >= -1.0f &&
-                         f0 <= fWm2;
+                ap = tp - fp;
+                am = tm - fm;
+                chain = fp == f0 + 1.0f && fm == f0 - 1.0f && f0 >= -1.0f && f0 <= fWm2;
             }
-            float C, Cxp, Cxm;
-            if (shared) {
-                // the three taps read texels f0-1 .. f0+2 (inside the padded row) with one weight
+            Texel xm, x0, xp;
+            if (chain) {
+                // texels f0-1 .. f0+2, inside the padded row
                 const float4* __restrict__ b = row2 + ((int)f0 - 1);
                 const Texel tA = texel_at(b, plane), tB = texel_at(b + 1, plane);
                 const Texel tC = texel_at(b + 2, plane), tD = texel_at(b + 3, plane);
-                const float b0 = 1.0f - a0;
-                Cxm = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel<F>(a0, b0, tA, tB));
-                C = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel<F>(a0, b0, tB, tC));
-                Cxp = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel<F>(a0, b0, tC, tD));
+                xm = lerp_texel<F>(am, 1.0f - am, tA, tB);
+                x0 = lerp_texel<F>(a0, 1.0f - a0, tB, tC);
+                xp = lerp_texel<F>(ap, 1.0f - ap, tC, tD);
             } else {
-                Cxm = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + -1.0f) + 0.5f));
-                C = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel_at<F>(row2, plane, W, p2x + 0.5f));
-                Cxp = klt_cost<F, CHK>(kw, val1, sb1, lerp_texel_at<F>(row2, plane, W, (p2x + 1.0f) + 0.5f));
+                xm = lerp_texel_at<F>(row2, plane, W, (p2x + -1.0f) + 0.5f);
+                x0 = lerp_texel_at<F>(row2, plane, W, p2x + 0.5f);
+                xp = lerp_texel_at<F>(row2, plane, W, (p2x + 1.0f) + 0.5f);
             }
+            const float Cxm = klt_cost<F, CHK>(kw, val1, sb1, xm);
+            const float C = klt_cost<F, CHK>(kw, val1, sb1, x0);
+            const float Cxp = klt_cost<F, CHK>(kw, val1, sb1, xp);
             if (COUNT) cnt.klt++;
             // the update of :394-402 without a branch: a rejected sample adds exact zeros, and
             // no accumulator can be -0, so adding +0 or -0 leaves it unchanged
