@@ -297,9 +297,10 @@ def run_batch(args, rank, world, local):
         for a, b, r, d in zip(dl, dr, rs, dm):
             seq.disparity_map(a, b, r, d, iters, pp=1)
 
-    # the branch count of the batch graph, picked by timing this batch at 1 iteration (untimed)
-    from cvt_b200.autotune import tune_batch
-    tuned = tune_batch(pm, dl, dr, rs, dm, iterations=1, candidates=(4, 8, 16))
+    # the schedule of the batch (lockstep persistent launches or branches, CTAs per SM, tile
+    # order, branch count), picked by timing this batch at 1 iteration (untimed)
+    from cvt_b200.autotune import label, tune_batch
+    tuned = tune_batch(pm, dl, dr, rs, dm, iterations=1, reps=1)
     for _ in range(args.warmup):
         batched()
     clocks = Clocks(local).start()
@@ -324,9 +325,9 @@ def run_batch(args, rank, world, local):
                        "iterations_executed": executed(iters), "views": 2, "pp": "lrcheck",
                        "parallelism": "pairs split over %d ranks (pm_batch_partition)" % world,
                        "rank_load_share": [float(x) for x in (load / load.sum())],
-                       "schedule": "one graph launch per rank, %d concurrent branches (autotuned: %s ms per "
-                                   "1-iteration batch)" % (tuned["branches"],
-                                                           {k: round(v, 1) for k, v in tuned["ms"].items()}),
+                       "schedule": "one graph launch per rank: %s (autotuned; ms per 1-iteration batch: %s)" % (
+                           label(tuned["best"]), {k: round(v, 1) for k, v in tuned["ms"].items()}),
+                       "autotuned": tuned["best"],
                        "l2": "inputs and workspaces (~25 GB) far larger than L2"},
             "sequential": {"value": px_it_all * args.steps / (ts * 1e-3) / 1e6, "ms_per_step": ts / args.steps,
                            "schedule": "eager single-pair calls"},

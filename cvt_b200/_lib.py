@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(_HERE, "libcvtpm.so")
 PM_OK, PM_EINVAL_SHAPE, PM_EINVAL_ARG, PM_ENOMEM, PM_ECUDA, PM_ETIMEOUT, PM_ENOTIMPL, PM_ENODEV = range(8)
 PM_MAX_WIDTH, PM_MAX_HEIGHT, PM_MAX_RADIUS = 4096, 4096, 32   # the image and window limits of cvtpm.h
 PM_MAX_BATCH, PM_BATCH_BRANCHES, PM_MAX_RANKS = 4096, 16, 1024   # the batch limits of cvtpm.h
+PM_BATCH_LOCKSTEP, PM_BATCH_BRANCHED = 0, 1   # batch schedules (pm_set_batch_schedule)
 PP_NONE, PP_LRCHECK, PP_LRCHECK_FILL = 0, 1, 2
 
 # every exported symbol of include/cvtpm.h
@@ -21,7 +22,7 @@ SYMBOLS = [
     "pm_disparity_map", "pm_disparity_map_device", "pm_depth_map", "pm_depth_map_device", "pm_set_counting", "pm_get_counters",
     "pm_set_profiling", "pm_get_phase_times", "pm_measure_fp32_peak",
     "pm_disparity_map_batch_device", "pm_disparity_map_init2_device", "pm_set_batch_branches", "pm_batch_schedule",
-    "pm_batch_partition",
+    "pm_batch_partition", "pm_set_batch_schedule", "pm_batch_jobs",
     "pm_k_prep", "pm_k_init", "pm_k_cost", "pm_k_klt", "pm_k_propagate", "pm_k_normal_depth",
     "pm_rof_scratch_bytes", "pm_k_rof", "pm_k_rof_static", "pm_k_consistency", "pm_k_to_disparity", "pm_k_fill_depthmap",
     "pm_k_fill_normalmap", "pm_k_disparity_to_normal", "pm_k_pyrdown", "pm_k_pyrup_mul", "pm_pyramid_size",
@@ -85,6 +86,8 @@ def lib():
         "pm_set_batch_branches": (i32, [vp, i32]),
         "pm_batch_schedule": (i32, [i32, i32, vp, vp, vp, vp, vp]),
         "pm_batch_partition": (i32, [i32, i32, vp, vp, vp, vp, vp, vp]),
+        "pm_set_batch_schedule": (i32, [vp, i32, i32, i32]),
+        "pm_batch_jobs": (i32, [i32, vp, vp, vp, i32, i32, i32, vp, i32, C.POINTER(C.c_int)]),
         "pm_get_counters": (i32, [vp, C.POINTER(C.c_uint64)]),
         "pm_set_profiling": (i32, [vp, i32]),
         "pm_get_phase_times": (i32, [vp, C.POINTER(C.c_float), C.POINTER(C.c_int)]),

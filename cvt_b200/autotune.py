@@ -1,13 +1,24 @@
 """Autotuner of the batched schedule (pm_disparity_map_batch_device).
 
-A batch of uneven pairs runs as one CUDA graph whose branches execute concurrently;
-how many branches share the GPU trades overlap (small pairs and short smoothing
-kernels beside long propagate kernels) against contention.  tune_batch times the
-caller's own batch, with a short iteration count, at each candidate branch count and
-keeps the fastest on the handle (pm_set_batch_branches); results equal those of any
-other setting (every pair's arithmetic is the same), only the time differs.
+A batch of uneven pairs runs either in lockstep (every iteration's propagate passes and
+smoothing stages of all pairs as persistent launches over one tile list, the pairs' prep and
+post-processing as concurrent graph branches) or branched (each pair's whole pipeline a
+branch of one graph).  The knobs trade overlap, tails and cache locality against each other:
+the schedule, the propagate CTAs per SM (the persistent grid; 0 = as many as fit), the tile
+order (pair after pair, or the pairs' tile rows interleaved) and the number of concurrent
+branches.  tune_batch times the caller's own batch, with a short iteration count, under each
+candidate and keeps the fastest on the handle; results are the same bit for bit under every
+candidate, only the time differs.
 """
 import statistics
+
+# candidates tried by default: {schedule, ctas_per_sm, tile_order, branches}
+DEFAULT_CANDIDATES = (
+    {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 0, "branches": 16},
+    {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 1, "branches": 16},
+    {"schedule": "lockstep", "ctas_per_sm": 4, "tile_order": 0, "branches": 16},
+    {"schedule": "branched", "ctas_per_sm": 0, "tile_order": 0, "branches": 16},
+)
 
 
 def cuda_event_ms(fn):
@@ -22,18 +33,41 @@ def cuda_event_ms(fn):
     return a.elapsed_time(b)
 
 
-def tune_batch(pm, lefts, rights, patchsizes, disparitymaxs, iterations=1, candidates=(2, 4, 8, 16), reps=2, pp=1,
-               timer=cuda_event_ms):
-    """Returns {"branches": best, "ms": {candidate: median ms}} and leaves `best` set on pm.
-    Each candidate's first call (graph capture) is not timed; ties go to the earlier candidate."""
+def _full(c):
+    d = {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 0, "branches": 16}
+    d.update(c)
+    return d
+
+
+def label(c):
+    c = _full(c)
+    if c["schedule"] == "branched":
+        return "branched/%d" % c["branches"]
+    return "lockstep/ctas%d/order%d/%d" % (c["ctas_per_sm"], c["tile_order"], c["branches"])
+
+
+def apply(pm, c):
+    """set candidate c on the handle of pm"""
+    c = _full(c)
+    pm.set_batch_schedule(c["schedule"], c["ctas_per_sm"], c["tile_order"])
+    pm.set_batch_branches(c["branches"])
+
+
+def tune_batch(pm, lefts, rights, patchsizes, disparitymaxs, iterations=1, candidates=DEFAULT_CANDIDATES, reps=2,
+               pp=1, timer=cuda_event_ms):
+    """Returns {"best": candidate, "ms": {label: median ms}} and leaves the best candidate set on
+    pm.  Each candidate's first call (graph capture, table upload) is not timed; ties go to the
+    earlier candidate."""
     def run():
         pm.disparity_map_batch(lefts, rights, patchsizes, disparitymaxs, iterations, pp=pp)
 
-    timings = {}
-    for nb in candidates:
-        pm.set_batch_branches(nb)
+    timings, best, best_ms = {}, None, None
+    for c in candidates:
+        apply(pm, c)
         timer(run)   # capture, warm
-        timings[nb] = statistics.median(timer(run) for _ in range(reps))
-    best = min(timings, key=timings.get)
-    pm.set_batch_branches(best)
-    return {"branches": best, "ms": timings}
+        ms = statistics.median(timer(run) for _ in range(reps))
+        timings[label(c)] = ms
+        if best_ms is None or ms < best_ms:
+            best, best_ms = c, ms
+    apply(pm, best)
+    return {"best": best, "ms": timings}

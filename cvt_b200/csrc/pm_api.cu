@@ -53,6 +53,13 @@ struct pm_handle {
     const float* init_normal_right = nullptr;   // with init_right: the right view's initial normals
     // concurrent branches of batched calls (pm_set_batch_branches; 0: PM_BATCH_BRANCHES)
     int batch_branches = 0;
+    // schedule of batched calls (pm_set_batch_schedule)
+    int batch_schedule = PM_BATCH_LOCKSTEP, batch_ctas = 0, batch_order = 0;
+    // lockstep batched calls: per-pair argument tables, job lists and work counters in one
+    // device allocation, and the host bytes last uploaded into it
+    void* btab = nullptr;
+    size_t btab_bytes = 0;
+    std::vector<unsigned char> btab_host;
 };
 
 namespace {
@@ -268,6 +275,161 @@ int ensure_ws(pm_handle* h, int W, int H, size_t stride)
     return grow(h, h->ws, h->ws_bytes, layout(W, H, stride).total);
 }
 
+// the fields of one pair's workspace that disparityMapAll works on
+struct LevelBufs {
+    float4 *Lbw, *Rbw, *Lg, *Rg, *LDT, *RDT, *Ls, *Rs, *tmp;
+    float4* mL[2];
+    float4* mR[2];
+    int *vb1c, *vb2c;
+    unsigned long long *vb1s, *vb2s;
+    void* rofs;
+    float4 *texL, *texR, *pself, *pnb;
+    ViewData VL, VR;
+    int W, H;
+};
+
+LevelBufs level_bufs(void* ws, const Layout& L, int W, int H, int r)
+{
+    LevelBufs B;
+    B.Lbw = at<float4>(ws, L, Layout::Lbw);
+    B.Rbw = at<float4>(ws, L, Layout::Rbw);
+    B.Lg = at<float4>(ws, L, Layout::Lg);
+    B.Rg = at<float4>(ws, L, Layout::Rg);
+    B.LDT = at<float4>(ws, L, Layout::LDT);
+    B.RDT = at<float4>(ws, L, Layout::RDT);
+    B.Ls = at<float4>(ws, L, Layout::Ls);
+    B.Rs = at<float4>(ws, L, Layout::Rs);
+    B.tmp = at<float4>(ws, L, Layout::tmp);
+    B.mL[0] = at<float4>(ws, L, Layout::mL0);
+    B.mL[1] = at<float4>(ws, L, Layout::mL1);
+    B.mR[0] = at<float4>(ws, L, Layout::mR0);
+    B.mR[1] = at<float4>(ws, L, Layout::mR1);
+    B.vb1c = at<int>(ws, L, Layout::vb1c);
+    B.vb2c = at<int>(ws, L, Layout::vb2c);
+    B.vb1s = at<unsigned long long>(ws, L, Layout::vb1s);
+    B.vb2s = at<unsigned long long>(ws, L, Layout::vb2s);
+    B.rofs = at<void>(ws, L, Layout::rof);
+    B.texL = at<float4>(ws, L, Layout::texL);
+    B.texR = at<float4>(ws, L, Layout::texR);
+    B.pself = at<float4>(ws, L, Layout::pself);
+    B.pnb = at<float4>(ws, L, Layout::pnb);
+    B.VL = make_view(B.texL, B.texR, W, H, r);
+    B.VR = make_view(B.texR, B.texL, W, H, r);
+    B.W = W;
+    B.H = H;
+    return B;
+}
+
+// theta of iteration k of `iterations` (already made odd): thetamin, then
+// (k - 1) / iterations to the fourth plus thetamin (PMHuberStereo.cpp:575-576)
+float theta_at(int k, int iterations, float thetamin)
+{
+    if (k == 0) return thetamin;
+    float theta = (float)(k - 1) / (float)iterations;
+    return powf(theta, 4.0f) + thetamin;
+}
+
+// the arguments of the propagate pass of view `view` (0 left, 1 right) in iteration `iter`
+// (:536-537, :542-543), `swap` the parity of the plane fields
+PropParams prop_params(const pm_handle* h, const LevelBufs& B, int view, int iter, int swap, float theta, float dmax,
+                       unsigned long long* ctr, int* errf)
+{
+    const int views = h->opt.views;
+    PropParams P;
+    P.V = view ? B.VR : B.VL;
+    P.out = view ? B.mR[1 - swap] : B.mL[1 - swap];
+    P.old = view ? B.mR[swap] : B.mL[swap];
+    P.smooth = view ? B.Rs : B.Ls;
+    P.theta = theta * 50.0f;
+    P.dmax = dmax;
+    P.lr = view ? 0 : 1;
+    P.iter = iter;
+    if (view == 0) {
+        P.vin_count = views == 2 ? B.vb2c : nullptr;
+        P.vin_src = B.vb2s;
+        P.vin_planes = B.mR[swap];
+        P.vout_count = views == 2 ? B.vb1c : nullptr;
+        P.vout_src = B.vb1s;
+    } else {
+        P.vin_count = B.vb1c;
+        P.vin_src = B.vb1s;
+        P.vin_planes = B.mL[1 - swap];
+        P.vout_count = B.vb2c;
+        P.vout_src = B.vb2s;
+    }
+    P.counters = h->counting ? ctr : nullptr;
+    P.error = errf;
+    P.tmp_self = B.pself;
+    P.tmp_nb = B.pnb;
+    P.dual = 0;
+    return P;
+}
+
+// the part of disparityMapAll before its iterations (:445-483): prep, clears, texel planes,
+// init (random or from given fields) and, with given fields, the first smoothing
+int level_begin(pm_handle* h, const LevelBufs& B, const uint8_t* left, const uint8_t* right, size_t stride, int r,
+                float dmax, float thetamin, const float* initdL, const float* initdR, const float4* initnL,
+                const float4* initnR, float4* nrmL, float4* nrmR, cudaStream_t st)
+{
+    const pm_options& o = h->opt;
+    const int views = o.views;
+    const int F = o.fused;
+    const int W = B.W, H = B.H;
+    const size_t N = (size_t)W * H;
+
+    // prep (PMHuberStereo.cpp:445-454)
+    launch_prep(left, stride, W, H, r, F, B.Lbw, B.Lg, B.LDT, st);
+    if (views == 2) launch_prep(right, stride, W, H, r, F, B.Rbw, B.Rg, B.RDT, st);
+    else launch_prep(right, stride, W, H, r, F, B.Rbw, B.Rg, nullptr, st);
+    // clear the smoothing images (:457-458) and both view buffers (:487)
+    PM_CUDA(h, cudaMemsetAsync(B.Ls, 0, N * 16, st));
+    PM_CUDA(h, cudaMemsetAsync(B.Rs, 0, N * 16, st));
+    launch_view_clear(B.vb1c, B.vb1s, N, st);
+    launch_view_clear(B.vb2c, B.vb2s, N, st);
+    launch_pack_tex(B.texL, B.Lbw, B.Lg, W, H, st);
+    launch_pack_tex(B.texR, B.Rbw, B.Rg, W, H, st);
+    prof_mark(h, st, PM_PHASE_PREP, 6);
+    // init (:469-470, :349-379): a given disparity without normals gets normals from it
+    int nl = 0;
+    if (initdL && !initnL) {
+        launch_disparity_to_normal(nrmL, initdL, W, H, st);   // :363-365
+        initnL = nrmL;
+        nl++;
+    }
+    if (initdR && !initnR && views == 2) {
+        launch_disparity_to_normal(nrmR, initdR, W, H, st);
+        initnR = nrmR;
+        nl++;
+    }
+    launch_init(B.mL[0], B.VL, dmax, 1, initdL, initnL, F, st);
+    nl += window_kernel_launches(F, false);
+    if (views == 2) {
+        launch_init(B.mR[0], B.VR, dmax, 0, initdR, initnR, F, st);
+        nl += window_kernel_launches(F, false);
+    }
+    const int rof_launches = pd_launch_count(o.rof_iters);
+    const float theta = thetamin;
+    const float4 lam0 = make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);
+    if (initdL) {   // :473-477
+        launch_normal_depth(B.tmp, B.mL[0], W, H, 1.0f / dmax, 1, st);
+        launch_rof(B.Ls, B.tmp, B.LDT, lam0, o.rof_iters, W, H, B.rofs, st);
+        nl += 1 + rof_launches;
+    }
+    if (initdR && views == 2) {   // :479-483
+        launch_normal_depth(B.tmp, B.mR[0], W, H, 1.0f / dmax, 0, st);
+        launch_rof(B.Rs, B.tmp, B.RDT, lam0, o.rof_iters, W, H, B.rofs, st);
+        nl += 1 + rof_launches;
+    }
+    prof_mark(h, st, PM_PHASE_INIT, nl);
+    return PM_OK;
+}
+
+// the smoothing weight of an iteration at theta (:532)
+float4 smooth_lambda(float theta)
+{
+    return make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);
+}
+
 // PMHuberStereo::disparityMapAll (PMHuberStereo.cpp:406-581) on one pyramid level, in the
 // workspace `ws` (layout L): the final plane fields end in mL1 and mR1.  initdL/initnL and
 // initdR/initnR are W x H init fields of the views (NULL: random init); counters and the
@@ -280,118 +442,30 @@ int run_level(pm_handle* h, void* ws, const Layout& L, const uint8_t* left, cons
     const pm_options& o = h->opt;
     const int views = o.views;
     const int F = o.fused;
-    const size_t N = L.N;
-    float4 *Lbw = at<float4>(ws, L, Layout::Lbw), *Rbw = at<float4>(ws, L, Layout::Rbw);
-    float4 *Lg = at<float4>(ws, L, Layout::Lg), *Rg = at<float4>(ws, L, Layout::Rg);
-    float4 *LDT = at<float4>(ws, L, Layout::LDT), *RDT = at<float4>(ws, L, Layout::RDT);
-    float4 *Ls = at<float4>(ws, L, Layout::Ls), *Rs = at<float4>(ws, L, Layout::Rs), *tmp = at<float4>(ws, L, Layout::tmp);
-    float4* mL[2] = {at<float4>(ws, L, Layout::mL0), at<float4>(ws, L, Layout::mL1)};
-    float4* mR[2] = {at<float4>(ws, L, Layout::mR0), at<float4>(ws, L, Layout::mR1)};
-    int *vb1c = at<int>(ws, L, Layout::vb1c), *vb2c = at<int>(ws, L, Layout::vb2c);
-    unsigned long long *vb1s = at<unsigned long long>(ws, L, Layout::vb1s), *vb2s = at<unsigned long long>(ws, L, Layout::vb2s);
-    void* rofs = at<void>(ws, L, Layout::rof);
-
-    // prep (PMHuberStereo.cpp:445-454)
-    launch_prep(left, stride, W, H, r, F, Lbw, Lg, LDT, st);
-    if (views == 2) launch_prep(right, stride, W, H, r, F, Rbw, Rg, RDT, st);
-    else launch_prep(right, stride, W, H, r, F, Rbw, Rg, nullptr, st);
-    // clear the smoothing images (:457-458) and both view buffers (:487)
-    PM_CUDA(h, cudaMemsetAsync(Ls, 0, N * 16, st));
-    PM_CUDA(h, cudaMemsetAsync(Rs, 0, N * 16, st));
-    launch_view_clear(vb1c, vb1s, N, st);
-    launch_view_clear(vb2c, vb2s, N, st);
-    float4* texL = at<float4>(ws, L, Layout::texL);
-    float4* texR = at<float4>(ws, L, Layout::texR);
-    launch_pack_tex(texL, Lbw, Lg, W, H, st);
-    launch_pack_tex(texR, Rbw, Rg, W, H, st);
-    prof_mark(h, st, PM_PHASE_PREP, 6);
-    // init (:469-470, :349-379): a given disparity without normals gets normals from it
-    int nl = 0;
-    if (initdL && !initnL) {
-        float4* nrm = at<float4>(ws, L, Layout::nrm);
-        launch_disparity_to_normal(nrm, initdL, W, H, st);   // :363-365
-        initnL = nrm;
-        nl++;
-    }
-    if (initdR && !initnR && views == 2) {
-        float4* nrm = at<float4>(ws, L, Layout::initnR);
-        launch_disparity_to_normal(nrm, initdR, W, H, st);
-        initnR = nrm;
-        nl++;
-    }
-    const ViewData VL = make_view(texL, texR, W, H, r);
-    const ViewData VR = make_view(texR, texL, W, H, r);
-    launch_init(mL[0], VL, dmax, 1, initdL, initnL, F, st);
-    nl += window_kernel_launches(F, false);
-    if (views == 2) {
-        launch_init(mR[0], VR, dmax, 0, initdR, initnR, F, st);
-        nl += window_kernel_launches(F, false);
-    }
-    float theta = thetamin;
+    const LevelBufs B = level_bufs(ws, L, W, H, r);
+    int rc = level_begin(h, B, left, right, stride, r, dmax, thetamin, initdL, initdR, initnL, initnR,
+                         at<float4>(ws, L, Layout::nrm), at<float4>(ws, L, Layout::initnR), st);
+    if (rc) return rc;
     const int rof_launches = pd_launch_count(o.rof_iters);
-    const float4 lam0 = make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);
-    if (initdL) {   // :473-477
-        launch_normal_depth(tmp, mL[0], W, H, 1.0f / dmax, 1, st);
-        launch_rof(Ls, tmp, LDT, lam0, o.rof_iters, W, H, rofs, st);
-        nl += 1 + rof_launches;
-    }
-    if (initdR && views == 2) {   // :479-483
-        launch_normal_depth(tmp, mR[0], W, H, 1.0f / dmax, 0, st);
-        launch_rof(Rs, tmp, RDT, lam0, o.rof_iters, W, H, rofs, st);
-        nl += 1 + rof_launches;
-    }
-    prof_mark(h, st, PM_PHASE_INIT, nl);
     int swap = 0;
     iterations |= 1;   // :490
     for (int iter = 0; iter < iterations; iter++) {
-        const float4 lam = make_float4(theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, theta * 10.0f + 1.0f, 1.0f);   // :532
-        PropParams P;
-        P.V = VL;
-        P.out = mL[1 - swap];
-        P.old = mL[swap];
-        P.smooth = Ls;
-        P.theta = theta * 50.0f;
-        P.dmax = dmax;
-        P.lr = 1;
-        P.iter = iter;
-        P.vin_count = views == 2 ? vb2c : nullptr;
-        P.vin_src = vb2s;
-        P.vin_planes = mR[swap];
-        P.vout_count = views == 2 ? vb1c : nullptr;
-        P.vout_src = vb1s;
-        P.counters = h->counting ? ctr : nullptr;
-        P.error = errf;
-        P.tmp_self = at<float4>(ws, L, Layout::pself);
-        P.tmp_nb = at<float4>(ws, L, Layout::pnb);
-        P.dual = 0;
-        launch_propagate(P, F, st);   // :536-537
-        if (views == 2) {
-            P.V = VR;
-            P.out = mR[1 - swap];
-            P.old = mR[swap];
-            P.smooth = Rs;
-            P.lr = 0;
-            P.vin_count = vb1c;
-            P.vin_src = vb1s;
-            P.vin_planes = mL[1 - swap];
-            P.vout_count = vb2c;
-            P.vout_src = vb2s;
-            launch_propagate(P, F, st);   // :542-543
-        }
+        const float theta = theta_at(iter, iterations, thetamin);
+        const float4 lam = smooth_lambda(theta);
+        launch_propagate(prop_params(h, B, 0, iter, swap, theta, dmax, ctr, errf), F, st);   // :536-537
+        if (views == 2) launch_propagate(prop_params(h, B, 1, iter, swap, theta, dmax, ctr, errf), F, st);   // :542-543
         prof_mark(h, st, PM_PHASE_PROPAGATE, 3 * window_kernel_launches(F, h->counting) * views);
         // the smoothing feeds the next iteration's propagation only: after the last one it is
         // left out (every output is formed from the planes, :105-142)
         if (iter + 1 < iterations) {
-            launch_normal_depth(tmp, mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :552-553
-            launch_rof(Ls, tmp, LDT, lam, o.rof_iters, W, H, rofs, st);
+            launch_normal_depth(B.tmp, B.mL[1 - swap], W, H, 1.0f / dmax, 1, st);   // :552-553
+            launch_rof(B.Ls, B.tmp, B.LDT, lam, o.rof_iters, W, H, B.rofs, st);
             if (views == 2) {
-                launch_normal_depth(tmp, mR[1 - swap], W, H, 1.0f / dmax, 0, st);   // :566-567
-                launch_rof(Rs, tmp, RDT, lam, o.rof_iters, W, H, rofs, st);
+                launch_normal_depth(B.tmp, B.mR[1 - swap], W, H, 1.0f / dmax, 0, st);   // :566-567
+                launch_rof(B.Rs, B.tmp, B.RDT, lam, o.rof_iters, W, H, B.rofs, st);
             }
             prof_mark(h, st, PM_PHASE_SMOOTH, views * (1 + rof_launches));
         }
-        theta = (float)iter / (float)iterations;   // :575-576
-        theta = powf(theta, 4.0f) + thetamin;
         swap = 1 - swap;
     }
     return PM_OK;
@@ -573,6 +647,36 @@ int ensure_level_ws(pm_handle* h, int W, int H)
 // levels the coarse-to-fine loop of :83-120 (CLPyramid with scale 0.35, each finer level
 // initialised from the upsampled coarser result).  Level 0 runs in `ws`, levels 1.. in the
 // handle's level workspaces (ensure_level_ws first).
+// the end of disparityMap (PMHuberStereo.cpp:123-141) on the final plane fields mL1 / mR1 of
+// `ws`: plane outputs, LR check, disparity and normal maps
+int pair_post(pm_handle* h, void* ws, const Layout& L, int W, int H, int pp, float* dmap, float4* normal,
+              float4* planesL, float4* planesR, cudaStream_t st)
+{
+    const pm_options& o = h->opt;
+    const size_t N = L.N;
+    float4* chk = at<float4>(ws, L, Layout::chk);
+    float4* ml = at<float4>(ws, L, Layout::mL1);
+    float4* mr = at<float4>(ws, L, Layout::mR1);
+    if (planesL) PM_CUDA(h, cudaMemcpyAsync(planesL, ml, N * 16, cudaMemcpyDeviceToDevice, st));
+    if (planesR && o.views == 2) PM_CUDA(h, cudaMemcpyAsync(planesR, mr, N * 16, cudaMemcpyDeviceToDevice, st));
+    int nl = 0;
+    if (pp == PM_PP_NONE) {   // :123-129
+        if (dmap) { launch_to_disparity(dmap, ml, W, H, 1.0f, 1, st); nl++; }
+        if (normal) { launch_fill_normalmap(normal, ml, W, H, st); nl++; }
+    } else {   // :130-141
+        launch_consistency(chk, ml, mr, W, H, o.maxdispdiff, o.maxanglediff, st);
+        nl++;
+        if (dmap) {
+            if (pp == PM_PP_LRCHECK) launch_to_disparity(dmap, chk, W, H, 1.0f, 1, st);
+            else launch_fill_depthmap(dmap, chk, W, H, 1.0f, st);
+            nl++;
+        }
+        if (normal) { launch_fill_normalmap(normal, chk, W, H, st); nl++; }
+    }
+    prof_mark(h, st, PM_PHASE_POST, nl);
+    return PM_OK;
+}
+
 int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* right, int W, int H, size_t stride,
                  int r, float dmax, int iterations, int pp, float* dmap, float4* normal, const float* initdisp,
                  const float4* initnormal, float4* planesL, float4* planesR, cudaStream_t st)
@@ -581,8 +685,6 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
     const int views = o.views;
     const int levels = o.levels;
     const Layout L = layout(W, H, stride);
-    const size_t N = L.N;
-    float4* chk = at<float4>(ws, L, Layout::chk);
     unsigned long long* ctr = at<unsigned long long>(ws, L, Layout::ctr);
     int* errf = at<int>(ws, L, Layout::errf);
 
@@ -684,25 +786,8 @@ int run_pipeline(pm_handle* h, void* ws, const uint8_t* left, const uint8_t* rig
             if (rc) return rc;
         }
     }
-    float4* ml = at<float4>(ws, L, Layout::mL1);
-    float4* mr = at<float4>(ws, L, Layout::mR1);
-    if (planesL) PM_CUDA(h, cudaMemcpyAsync(planesL, ml, N * 16, cudaMemcpyDeviceToDevice, st));
-    if (planesR && views == 2) PM_CUDA(h, cudaMemcpyAsync(planesR, mr, N * 16, cudaMemcpyDeviceToDevice, st));
-    int nl = 0;
-    if (pp == PM_PP_NONE) {   // :123-129
-        if (dmap) { launch_to_disparity(dmap, ml, W, H, 1.0f, 1, st); nl++; }
-        if (normal) { launch_fill_normalmap(normal, ml, W, H, st); nl++; }
-    } else {   // :130-141
-        launch_consistency(chk, ml, mr, W, H, o.maxdispdiff, o.maxanglediff, st);
-        nl++;
-        if (dmap) {
-            if (pp == PM_PP_LRCHECK) launch_to_disparity(dmap, chk, W, H, 1.0f, 1, st);
-            else launch_fill_depthmap(dmap, chk, W, H, 1.0f, st);
-            nl++;
-        }
-        if (normal) { launch_fill_normalmap(normal, chk, W, H, st); nl++; }
-    }
-    prof_mark(h, st, PM_PHASE_POST, nl);
+    rc = pair_post(h, ws, L, W, H, pp, dmap, normal, planesL, planesR, st);
+    if (rc) return rc;
     PM_CUDA(h, cudaGetLastError());
     return prof_collect(h, st);
 }
@@ -902,6 +987,7 @@ int pm_destroy(pm_handle* h)
         if (p) cudaFree(p);
     for (void* p : h->lws)
         if (p) cudaFree(p);
+    if (h->btab) cudaFree(h->btab);
     for (cudaStream_t b : h->branch) cudaStreamDestroy(b);
     for (cudaEvent_t e : h->bev) cudaEventDestroy(e);
     if (h->own) cudaStreamDestroy(h->own);
@@ -1202,6 +1288,228 @@ int pm_batch_partition(int n, int ranks, const int* width, const int* height, co
     return PM_OK;
 }
 
+// the tile jobs of a lockstep batch (pm_batch_jobs): `order` lists the pairs in decreasing work
+static void batch_jobs(int n, const int* width, const int* height, const int* order, int tw, int th, int tile_order,
+                       std::vector<uint32_t>& jobs)
+{
+    jobs.clear();
+    int rows_max = 0;
+    for (int k = 0; k < n; k++) rows_max = std::max(rows_max, (height[order[k]] + th - 1) / th);
+    auto row = [&](int i, int by) {
+        const int gx = (width[i] + tw - 1) / tw;
+        for (int bx = 0; bx < gx; bx++) {
+            jobs.push_back((uint32_t)i);
+            jobs.push_back(((uint32_t)by << 16) | (uint32_t)bx);
+        }
+    };
+    if (tile_order == 0) {
+        for (int k = 0; k < n; k++)
+            for (int by = 0; by < (height[order[k]] + th - 1) / th; by++) row(order[k], by);
+    } else {
+        for (int by = 0; by < rows_max; by++)
+            for (int k = 0; k < n; k++)
+                if (by < (height[order[k]] + th - 1) / th) row(order[k], by);
+    }
+}
+
+int pm_set_batch_schedule(pm_handle* h, int schedule, int ctas_per_sm, int tile_order)
+{
+    if (!h) return fail(nullptr, PM_EINVAL_ARG, "null handle");
+    if (schedule != PM_BATCH_LOCKSTEP && schedule != PM_BATCH_BRANCHED) return fail(h, PM_EINVAL_ARG, "unknown batch schedule");
+    if (ctas_per_sm < 0 || ctas_per_sm > 64) return fail(h, PM_EINVAL_ARG, "CTAs per SM out of range");
+    if (tile_order != 0 && tile_order != 1) return fail(h, PM_EINVAL_ARG, "unknown tile order");
+    h->batch_schedule = schedule;
+    h->batch_ctas = ctas_per_sm;
+    h->batch_order = tile_order;
+    return PM_OK;
+}
+
+int pm_batch_jobs(int n, const int* width, const int* height, const int* patchsize, int tile_w, int tile_h,
+                  int tile_order, uint32_t* jobs, int njobs_cap, int* njobs)
+{
+    if (n < 0 || n > PM_MAX_BATCH) return fail(nullptr, PM_EINVAL_ARG, "batch size out of range");
+    if (!njobs) return fail(nullptr, PM_EINVAL_ARG, "null job count");
+    if (tile_w < 1 || tile_h < 1) return fail(nullptr, PM_EINVAL_ARG, "tile size out of range");
+    if (tile_order != 0 && tile_order != 1) return fail(nullptr, PM_EINVAL_ARG, "unknown tile order");
+    *njobs = 0;
+    if (n == 0) return PM_OK;
+    if (!width || !height || !patchsize) return fail(nullptr, PM_EINVAL_ARG, "null array");
+    for (int i = 0; i < n; i++)
+        if (width[i] < 1 || height[i] < 1 || width[i] > PM_MAX_WIDTH || height[i] > PM_MAX_HEIGHT)
+            return fail(nullptr, PM_EINVAL_SHAPE, "pair " + std::to_string(i) + " has an unsupported size");
+    std::vector<int> order(n), owner(n);
+    batch_schedule(n, 1, width, height, patchsize, order.data(), owner.data());
+    std::vector<uint32_t> v;
+    batch_jobs(n, width, height, order.data(), tile_w, tile_h, tile_order, v);
+    const int cnt = (int)(v.size() / 2);
+    *njobs = cnt;
+    if (jobs) {
+        if (njobs_cap < cnt) return fail(nullptr, PM_EINVAL_ARG, "job array too small");
+        memcpy(jobs, v.data(), v.size() * sizeof(uint32_t));
+    }
+    return PM_OK;
+}
+
+// Lockstep batched call (PM_BATCH_LOCKSTEP): the pairs' prep / init and post-processing as
+// branches of `cs`, every iteration's propagate passes and smoothing stages as persistent
+// launches over the tiles of all pairs.  Each pair sees the same operations in the same order
+// as in run_pipeline (levels 1), so the results are the same.
+static int batch_lockstep(pm_handle* h, int n, const uint8_t* const* left, const uint8_t* const* right,
+                          const int* width, const int* height, const size_t* stride, const int* patchsize,
+                          const float* dispmax, int iterations, int pp, float* const* dmap,
+                          float* const* planes_left, float* const* planes_right, int nb, const int* order,
+                          const int* owner, cudaStream_t st, bool graph)
+{
+    const pm_options& o = h->opt;
+    const int views = o.views, F = o.fused;
+    const int itx = iterations | 1;   // PMHuberStereo.cpp:490
+    std::vector<Layout> L(n);
+    std::vector<LevelBufs> B(n);
+    for (int i = 0; i < n; i++) {
+        L[i] = layout(width[i], height[i], stride[i]);
+        B[i] = level_bufs(h->bws[i], L[i], width[i], height[i], patchsize[i]);
+    }
+    // host tables: propagate arguments per (iteration, view, pair), smoothing arguments per
+    // (view, pair), the three job lists, then the work counters (zeroed in the stream)
+    std::vector<PropParams> ptab((size_t)itx * views * n);
+    for (int it = 0; it < itx; it++) {
+        const float theta = theta_at(it, itx, o.thetamin);
+        for (int v = 0; v < views; v++)
+            for (int i = 0; i < n; i++) {
+                PropParams P = prop_params(h, B[i], v, it, it & 1, theta, dispmax[i],
+                                           at<unsigned long long>(h->bws[i], L[i], Layout::ctr),
+                                           at<int>(h->bws[i], L[i], Layout::errf));
+                P.dual = h->counting ? 0 : 1;
+                ptab[((size_t)it * views + v) * n + i] = P;
+            }
+    }
+    std::vector<SmoothArgs> stab((size_t)views * n);
+    for (int v = 0; v < views; v++)
+        for (int i = 0; i < n; i++) {
+            SmoothArgs A;
+            A.out = v ? B[i].Rs : B[i].Ls;
+            A.tmp = B[i].tmp;
+            A.dt = v ? B[i].RDT : B[i].LDT;
+            A.scratch = static_cast<float4*>(B[i].rofs);
+            A.planes[0] = v ? B[i].mR[0] : B[i].mL[0];
+            A.planes[1] = v ? B[i].mR[1] : B[i].mL[1];
+            A.dispscale = 1.0f / dispmax[i];
+            A.lr = v ? 0 : 1;
+            A.W = width[i];
+            A.H = height[i];
+            stab[(size_t)v * n + i] = A;
+        }
+    int ptw, pth;
+    prop_tile_shape(&ptw, &pth);
+    std::vector<uint32_t> jp, j8, j16;
+    batch_jobs(n, width, height, order, ptw, pth, h->batch_order, jp);
+    batch_jobs(n, width, height, order, SMOOTH_TW, SMOOTH_TH8, h->batch_order, j8);
+    batch_jobs(n, width, height, order, SMOOTH_TW, SMOOTH_TH16, h->batch_order, j16);
+    const int per_iter = views * (propagate_batch_launches(h->counting) + smooth_batch_launches(o.rof_iters));
+    const size_t nslots = (size_t)itx * per_iter;
+    auto pad = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t o_p = 0, o_s = o_p + pad(ptab.size() * sizeof(PropParams));
+    const size_t o_jp = o_s + pad(stab.size() * sizeof(SmoothArgs));
+    const size_t o_j8 = o_jp + pad(jp.size() * 4), o_j16 = o_j8 + pad(j8.size() * 4);
+    const size_t o_ctr = o_j16 + pad(j16.size() * 4), total = o_ctr + pad(nslots * 4);
+    std::vector<unsigned char> hb(o_ctr, 0);
+    memcpy(hb.data() + o_p, ptab.data(), ptab.size() * sizeof(PropParams));
+    memcpy(hb.data() + o_s, stab.data(), stab.size() * sizeof(SmoothArgs));
+    memcpy(hb.data() + o_jp, jp.data(), jp.size() * 4);
+    memcpy(hb.data() + o_j8, j8.data(), j8.size() * 4);
+    memcpy(hb.data() + o_j16, j16.data(), j16.size() * 4);
+    if (!(h->btab && h->btab_bytes >= total && h->btab_host == hb)) {
+        // earlier calls on this stream may still read the tables: let them finish first
+        PM_CUDA(h, cudaStreamSynchronize(st));
+        if (h->btab_bytes < total) {
+            if (h->btab) cudaFree(h->btab);
+            h->btab = nullptr;
+            h->btab_bytes = 0;
+            h->btab_host.clear();
+            int rc = grow(h, h->btab, h->btab_bytes, total);
+            if (rc) return rc;
+        }
+        PM_CUDA(h, cudaMemcpy(h->btab, hb.data(), hb.size(), cudaMemcpyHostToDevice));
+        h->btab_host.swap(hb);
+    }
+    char* base = static_cast<char*>(h->btab);
+    const PropParams* dP = reinterpret_cast<const PropParams*>(base + o_p);
+    const SmoothArgs* dS = reinterpret_cast<const SmoothArgs*>(base + o_s);
+    const JobList Jp{reinterpret_cast<const uint2*>(base + o_jp), (int)(jp.size() / 2)};
+    const JobList J8{reinterpret_cast<const uint2*>(base + o_j8), (int)(j8.size() / 2)};
+    const JobList J16{reinterpret_cast<const uint2*>(base + o_j16), (int)(j16.size() / 2)};
+    int* slots = reinterpret_cast<int*>(base + o_ctr);
+
+    auto fork = [&](cudaStream_t cs) -> int {
+        PM_CUDA(h, cudaEventRecord(h->bev[nb], cs));
+        for (int b = 0; b < nb; b++) PM_CUDA(h, cudaStreamWaitEvent(h->branch[b], h->bev[nb], 0));
+        return PM_OK;
+    };
+    auto join = [&](cudaStream_t cs) -> int {
+        for (int b = 0; b < nb; b++) {
+            PM_CUDA(h, cudaEventRecord(h->bev[b], h->branch[b]));
+            PM_CUDA(h, cudaStreamWaitEvent(cs, h->bev[b], 0));
+        }
+        return PM_OK;
+    };
+    auto body = [&](cudaStream_t cs) -> int {
+        PM_CUDA(h, cudaMemsetAsync(slots, 0, nslots * 4, cs));
+        int rc = fork(cs);
+        if (rc) return rc;
+        for (int k = 0; k < n; k++) {
+            const int i = order[k];
+            const cudaStream_t bs = h->branch[owner[i]];
+            PM_CUDA(h, cudaMemsetAsync(at<void>(h->bws[i], L[i], Layout::ctr), 0, 64, bs));
+            PM_CUDA(h, cudaMemsetAsync(at<void>(h->bws[i], L[i], Layout::errf), 0, 64, bs));
+            rc = level_begin(h, B[i], left[i], right[i], stride[i], patchsize[i], dispmax[i], o.thetamin, nullptr,
+                             nullptr, nullptr, nullptr, at<float4>(h->bws[i], L[i], Layout::nrm),
+                             at<float4>(h->bws[i], L[i], Layout::initnR), bs);
+            if (rc) return rc;
+        }
+        if ((rc = join(cs))) return rc;
+        int* next = slots;
+        for (int it = 0; it < itx; it++) {
+            for (int v = 0; v < views; v++) {
+                launch_propagate_batch(dP + ((size_t)it * views + v) * n, Jp, h->batch_ctas, F, h->counting, next, cs);
+                next += propagate_batch_launches(h->counting);
+            }
+            if (it + 1 < itx) {   // as in run_level: no smoothing after the last iteration
+                const float4 lam = smooth_lambda(theta_at(it, itx, o.thetamin));
+                for (int v = 0; v < views; v++) {
+                    launch_smooth_batch(dS + (size_t)v * n, J8, J16, 1 - (it & 1), lam, o.rof_iters, next, cs);
+                    next += smooth_batch_launches(o.rof_iters);
+                }
+            }
+        }
+        if ((rc = fork(cs))) return rc;
+        for (int k = 0; k < n; k++) {
+            const int i = order[k];
+            rc = pair_post(h, h->bws[i], L[i], width[i], height[i], pp, dmap ? dmap[i] : nullptr, nullptr,
+                           planes_left ? reinterpret_cast<float4*>(planes_left[i]) : nullptr,
+                           planes_right ? reinterpret_cast<float4*>(planes_right[i]) : nullptr,
+                           h->branch[owner[i]]);
+            if (rc) return rc;
+        }
+        if ((rc = join(cs))) return rc;
+        PM_CUDA(h, cudaGetLastError());
+        return PM_OK;
+    };
+    if (!graph) return body(st);
+    std::vector<uint64_t> key = {(uint64_t)n, (uint64_t)nb, (uint64_t)iterations, (uint64_t)pp, (uint64_t)o.views,
+                                 (uint64_t)o.fused, fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff),
+                                 (uint64_t)o.rof_iters, (uint64_t)h->counting, (uint64_t)PM_BATCH_LOCKSTEP,
+                                 (uint64_t)h->batch_ctas, (uint64_t)h->batch_order, (uint64_t)(uintptr_t)h->btab};
+    for (int i = 0; i < n; i++) {
+        const uint64_t v[] = {(uint64_t)(uintptr_t)h->bws[i], (uint64_t)(uintptr_t)left[i], (uint64_t)(uintptr_t)right[i],
+                              (uint64_t)width[i], (uint64_t)height[i], (uint64_t)stride[i], (uint64_t)patchsize[i],
+                              fbits(dispmax[i]), (uint64_t)(uintptr_t)(dmap ? dmap[i] : nullptr),
+                              (uint64_t)(uintptr_t)(planes_left ? planes_left[i] : nullptr),
+                              (uint64_t)(uintptr_t)(planes_right ? planes_right[i] : nullptr)};
+        key.insert(key.end(), v, v + 11);
+    }
+    return run_graph(h, h->keyb, h->execb, key, st, body);
+}
+
 int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* left, const uint8_t* const* right,
                                   const int* width, const int* height, const size_t* stride, const int* patchsize,
                                   const float* dispmax, int iterations, int pp, float* const* dmap,
@@ -1241,6 +1549,23 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
     }
     std::vector<int> order(n), owner(n);
     batch_schedule(n, nb, width, height, patchsize, order.data(), owner.data());
+    const cudaStream_t st = S(stream);
+    if (h->batch_schedule == PM_BATCH_LOCKSTEP) {
+        // lockstep needs its tables uploaded before the launch: not inside a caller's capture
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (st) PM_CUDA(h, cudaStreamIsCapturing(st, &cap));
+        if (cap == cudaStreamCaptureStatusNone) {
+            bool graph = false;
+            int rc = use_graph(h, st, &graph);
+            if (rc) return rc;
+            const int saved = h->profiling;
+            h->profiling = 0;   // per-phase timing covers single-pair calls only
+            rc = batch_lockstep(h, n, left, right, width, height, stride, patchsize, dispmax, iterations, pp, dmap,
+                                planes_left, planes_right, nb, order.data(), owner.data(), st, graph);
+            h->profiling = saved;
+            return rc;
+        }
+    }
     auto body = [&](cudaStream_t cs) -> int {
         PM_CUDA(h, cudaEventRecord(h->bev[nb], cs));
         for (int b = 0; b < nb; b++) PM_CUDA(h, cudaStreamWaitEvent(h->branch[b], h->bev[nb], 0));
@@ -1258,7 +1583,6 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
         }
         return PM_OK;
     };
-    const cudaStream_t st = S(stream);
     bool graph = false;
     int rc = use_graph(h, st, &graph);
     if (rc) return rc;
@@ -1274,7 +1598,7 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
     std::vector<uint64_t> key = {(uint64_t)n, (uint64_t)nb, (uint64_t)iterations, (uint64_t)pp, (uint64_t)o.views,
                                  (uint64_t)o.fused,
                                  fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff), (uint64_t)o.rof_iters,
-                                 (uint64_t)h->counting};
+                                 (uint64_t)h->counting, (uint64_t)PM_BATCH_BRANCHED};
     for (int i = 0; i < n; i++) {
         const uint64_t v[] = {(uint64_t)(uintptr_t)h->bws[i], (uint64_t)(uintptr_t)left[i], (uint64_t)(uintptr_t)right[i],
                               (uint64_t)width[i], (uint64_t)height[i], (uint64_t)stride[i], (uint64_t)patchsize[i],

@@ -132,15 +132,21 @@ __global__ void k_klt(float4* __restrict__ out, const float4* __restrict__ plane
     out[i] = klt2<F, false, CHK>(V, x, y, planes[i], cnt);
 }
 
-__global__ void k_normal_depth(float4* __restrict__ out, const float4* __restrict__ planes, int W, int H,
-                               float dispscale, int lr)
+__device__ __forceinline__ void normal_depth_px(float4* __restrict__ out, const float4* __restrict__ planes, int W,
+                                                int H, float dispscale, int lr, int x, int y)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
     const size_t i = (size_t)y * W + x;
     float4 v = to_ref_normal_depth(planes[i], (float)x, (float)y, lr);   // pmhstereo.cl:1397-1399
     v.w = v.w * dispscale;
     out[i] = v;
+}
+
+__global__ void k_normal_depth(float4* __restrict__ out, const float4* __restrict__ planes, int W, int H,
+                               float dispscale, int lr)
+{
+    normal_depth_px(out, planes, W, H, dispscale, lr, blockIdx.x * blockDim.x + threadIdx.x,
+                    blockIdx.y * blockDim.y + threadIdx.y);
 }
 
 // tensor-weighted, projected dual of PDDROFDiffTensor (PDDROFDiffTensor.cl:72-100) from the
@@ -238,15 +244,13 @@ constexpr int ROF_BX = 32, ROF_BY = 8;   // k_rof_step block; its duals need a o
 // (x, y - 1): the block computes the duals of its tile and of the column left of it and the
 // row above it once each, in shared memory, instead of three times per pixel.
 template <bool HUBER>
-__global__ void __launch_bounds__(ROF_BX* ROF_BY) k_rof_step(float4* __restrict__ unew, float4* __restrict__ pnew,
-                                                           float4* __restrict__ qnew, const float4* __restrict__ u,
-                                                           const float4* __restrict__ p, const float4* __restrict__ q,
-                                                           const float4* __restrict__ img,
-                                                           const float4* __restrict__ dt, float4 lam, int W, int H,
-                                                           int first, float eps)
+__device__ __forceinline__ void rof_step_tile(float4* __restrict__ unew, float4* __restrict__ pnew,
+                                              float4* __restrict__ qnew, const float4* __restrict__ u,
+                                              const float4* __restrict__ p, const float4* __restrict__ q,
+                                              const float4* __restrict__ img, const float4* __restrict__ dt,
+                                              float4 lam, int W, int H, int first, float eps, int x0, int y0)
 {
     __shared__ Dual sd[ROF_BY + 1][ROF_BX + 1];
-    const int x0 = blockIdx.x * ROF_BX, y0 = blockIdx.y * ROF_BY;
     const int tid = threadIdx.y * ROF_BX + threadIdx.x;
     for (int i = tid; i < (ROF_BX + 1) * (ROF_BY + 1); i += ROF_BX * ROF_BY) {
         const int ex = i % (ROF_BX + 1), ey = i / (ROF_BX + 1);
@@ -267,6 +271,18 @@ __global__ void __launch_bounds__(ROF_BX* ROF_BY) k_rof_step(float4* __restrict_
     pnew[(size_t)y * 2 * W + 2 * x + 1] = c.hi;
 }
 
+template <bool HUBER>
+__global__ void __launch_bounds__(ROF_BX* ROF_BY) k_rof_step(float4* __restrict__ unew, float4* __restrict__ pnew,
+                                                           float4* __restrict__ qnew, const float4* __restrict__ u,
+                                                           const float4* __restrict__ p, const float4* __restrict__ q,
+                                                           const float4* __restrict__ img,
+                                                           const float4* __restrict__ dt, float4 lam, int W, int H,
+                                                           int first, float eps)
+{
+    rof_step_tile<HUBER>(unew, pnew, qnew, u, p, q, img, dt, lam, W, H, first, eps, blockIdx.x * ROF_BX,
+                         blockIdx.y * ROF_BY);
+}
+
 constexpr int RF_BX = 32, RF_BY = 16, RF_NT = 256;   // k_rof_step2: output tile and threads
 
 // two primal-dual steps in one launch (temporal blocking): the block computes the first
@@ -276,18 +292,17 @@ constexpr int RF_BX = 32, RF_BY = 16, RF_NT = 256;   // k_rof_step2: output tile
 // every value is formed by the same operations as in k_rof_step, so the result is the same
 // bit for bit.  first: p = q = 0 before the first of the two steps.
 template <bool HUBER>
-__global__ void __launch_bounds__(RF_NT) k_rof_step2(float4* __restrict__ unew, float4* __restrict__ pnew,
-                                                   float4* __restrict__ qnew, const float4* __restrict__ u,
-                                                   const float4* __restrict__ p, const float4* __restrict__ q,
-                                                   const float4* __restrict__ img, const float4* __restrict__ dt,
-                                                   float4 lam, int W, int H, int first, float eps)
+__device__ __forceinline__ void rof_step2_tile(float4* __restrict__ unew, float4* __restrict__ pnew,
+                                               float4* __restrict__ qnew, const float4* __restrict__ u,
+                                               const float4* __restrict__ p, const float4* __restrict__ q,
+                                               const float4* __restrict__ img, const float4* __restrict__ dt,
+                                               float4 lam, int W, int H, int first, float eps, int x0, int y0)
 {
     // duals: first step over x0-2 .. x0+BX, y0-2 .. y0+BY; the second step overwrites the
     // points x0-1 .. x0+BX-1, y0-1 .. y0+BY-1 in place (each point reads only its own first-step dual)
     __shared__ float4 sdl[RF_BY + 3][RF_BX + 3], sdh[RF_BY + 3][RF_BX + 3];
     __shared__ float4 su[RF_BY + 2][RF_BX + 2];   // first-step primal over x0-1 .. x0+BX, y0-1 .. y0+BY (in-image points)
     __shared__ float4 sq[RF_BY][RF_BX];           // first-step q over the tile
-    const int x0 = blockIdx.x * RF_BX, y0 = blockIdx.y * RF_BY;
     const int tid = threadIdx.x;
     for (int i = tid; i < (RF_BX + 3) * (RF_BY + 3); i += RF_NT) {
         const int ex = i % (RF_BX + 3), ey = i / (RF_BX + 3);
@@ -340,6 +355,88 @@ __global__ void __launch_bounds__(RF_NT) k_rof_step2(float4* __restrict__ unew, 
         qnew[gi] = qn;
         pnew[(size_t)y * 2 * W + 2 * x] = c.lo;
         pnew[(size_t)y * 2 * W + 2 * x + 1] = c.hi;
+    }
+}
+
+template <bool HUBER>
+__global__ void __launch_bounds__(RF_NT) k_rof_step2(float4* __restrict__ unew, float4* __restrict__ pnew,
+                                                   float4* __restrict__ qnew, const float4* __restrict__ u,
+                                                   const float4* __restrict__ p, const float4* __restrict__ q,
+                                                   const float4* __restrict__ img, const float4* __restrict__ dt,
+                                                   float4 lam, int W, int H, int first, float eps)
+{
+    rof_step2_tile<HUBER>(unew, pnew, qnew, u, p, q, img, dt, lam, W, H, first, eps, blockIdx.x * RF_BX,
+                          blockIdx.y * RF_BY);
+}
+
+static_assert(RF_BX == SMOOTH_TW && RF_BY == SMOOTH_TH16 && ROF_BX == SMOOTH_TW && ROF_BY == SMOOTH_TH8,
+              "smoothing job tiles");
+
+// the buffers of launch j of `launches` of a primal-dual run (launch_pd's schedule)
+struct PdStep {
+    float4 *unew, *pnew, *qnew;
+    const float4 *u, *p, *q;
+};
+__device__ __forceinline__ PdStep pd_step(const SmoothArgs& A, int j, int launches)
+{
+    const size_t N = (size_t)A.W * A.H;
+    float4* ut = A.scratch;
+    float4* pp[2] = {ut + N, ut + 3 * N};
+    float4* qq[2] = {ut + 5 * N, ut + 6 * N};
+    const int pi = j & 1;
+    PdStep s;
+    s.unew = ((launches - 1 - j) % 2 == 0) ? A.out : ut;
+    // the previous launch wrote `out` exactly when this one writes the scratch
+    s.u = j == 0 ? A.tmp : (((launches - j) % 2 == 0) ? A.out : ut);
+    s.pnew = pp[pi];
+    s.qnew = qq[pi];
+    s.p = pp[1 - pi];
+    s.q = qq[1 - pi];
+    return s;
+}
+
+// batched smoothing stage (launch_smooth_batch): persistent CTAs over the tiles of all pairs
+__global__ void __launch_bounds__(ROF_BX* ROF_BY) k_normal_depth_b(const SmoothArgs* __restrict__ tab, int sel,
+                                                                 const uint2* __restrict__ jobs, int njobs,
+                                                                 int* next)
+{
+    for (;;) {
+        const int j = grab_job(next);
+        if (j >= njobs) return;
+        const uint2 job = jobs[j];
+        const SmoothArgs& A = tab[job.x];
+        normal_depth_px(A.tmp, A.planes[sel], A.W, A.H, A.dispscale, A.lr,
+                        (int)(job.y & 0xffffu) * ROF_BX + threadIdx.x, (int)(job.y >> 16) * ROF_BY + threadIdx.y);
+    }
+}
+
+__global__ void __launch_bounds__(ROF_BX* ROF_BY) k_rof_step_b(const SmoothArgs* __restrict__ tab, float4 lam,
+                                                             int launch, int launches,
+                                                             const uint2* __restrict__ jobs, int njobs, int* next)
+{
+    for (;;) {
+        const int j = grab_job(next);
+        if (j >= njobs) return;
+        const uint2 job = jobs[j];
+        const SmoothArgs& A = tab[job.x];
+        const PdStep s = pd_step(A, launch, launches);
+        rof_step_tile<false>(s.unew, s.pnew, s.qnew, s.u, s.p, s.q, A.tmp, A.dt, lam, A.W, A.H, launch == 0, 0.0f,
+                             (int)(job.y & 0xffffu) * ROF_BX, (int)(job.y >> 16) * ROF_BY);
+    }
+}
+
+__global__ void __launch_bounds__(RF_NT) k_rof_step2_b(const SmoothArgs* __restrict__ tab, float4 lam, int launch,
+                                                     int launches, const uint2* __restrict__ jobs, int njobs,
+                                                     int* next)
+{
+    for (;;) {
+        const int j = grab_job(next);
+        if (j >= njobs) return;
+        const uint2 job = jobs[j];
+        const SmoothArgs& A = tab[job.x];
+        const PdStep s = pd_step(A, launch, launches);
+        rof_step2_tile<false>(s.unew, s.pnew, s.qnew, s.u, s.p, s.q, A.tmp, A.dt, lam, A.W, A.H, launch == 0, 0.0f,
+                              (int)(job.y & 0xffffu) * RF_BX, (int)(job.y >> 16) * RF_BY);
     }
 }
 
@@ -731,6 +828,50 @@ int pd_launch_count(int iters)
 {
     const int steps = (iters > 0 && iters % 2 == 0) ? iters : iters + 1;
     return steps % 2 + steps / 2;
+}
+
+namespace {
+template <class K>
+unsigned persistent_grid(K kernel, int threads, int njobs)
+{
+    int dev = 0, sms = 1, per = 0;
+    cudaGetDevice(&dev);
+    // a failed query only shrinks the grid; its error is cleared, a pending launch error is not
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 1;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess) {
+        cudaGetLastError();
+        per = 1;
+    }
+    sms = sms < 1 ? 1 : sms;
+    per = per < 1 ? 1 : per;
+    const long long g = (long long)per * sms;
+    return (unsigned)(g < njobs ? g : njobs);
+}
+}  // namespace
+
+int smooth_batch_launches(int iters) { return 1 + pd_launch_count(iters); }
+
+void launch_smooth_batch(const SmoothArgs* tab, const JobList& j8, const JobList& j16, int sel, float4 lam, int iters,
+                         int* next, cudaStream_t st)
+{
+    if (j8.njobs <= 0) return;
+    const dim3 b8(ROF_BX, ROF_BY);
+    k_normal_depth_b<<<persistent_grid(k_normal_depth_b, ROF_BX * ROF_BY, j8.njobs), b8, 0, st>>>(
+        tab, sel, j8.jobs, j8.njobs, next);
+    // launch_pd's schedule: an odd step count starts with one single step, the rest run two per launch
+    const int steps = (iters > 0 && iters % 2 == 0) ? iters : iters + 1;
+    const int launches = pd_launch_count(iters);
+    for (int j = 0; j < launches; j++) {
+        if (j == 0 && steps % 2)
+            k_rof_step_b<<<persistent_grid(k_rof_step_b, ROF_BX * ROF_BY, j8.njobs), b8, 0, st>>>(
+                tab, lam, j, launches, j8.jobs, j8.njobs, next + 1 + j);
+        else
+            k_rof_step2_b<<<persistent_grid(k_rof_step2_b, RF_NT, j16.njobs), RF_NT, 0, st>>>(
+                tab, lam, j, launches, j16.jobs, j16.njobs, next + 1 + j);
+    }
 }
 
 void launch_rof(float4* out, const float4* input, const float4* dt, float4 lam, int iters, int W, int H, void* scratch,

@@ -39,6 +39,55 @@ struct PropParams {
     int dual;                       // the window-loop kernels run as two variants (pm_window.cuh)
 };
 
+// Batched launches over many pairs (pm_disparity_map_batch_device run in lockstep): a job is
+// one tile of one pair, jobs[k] = (pair, (tile row << 16) | tile column), in schedule order.
+// The kernels are persistent: a grid of a few CTAs per SM takes jobs in list order from a work
+// counter (zero before the launch) until the list is exhausted.
+struct JobList {
+    const uint2* jobs;
+    int njobs;
+};
+
+// next job of the calling CTA: one atomic per CTA, broadcast through shared memory.  The
+// first barrier also orders the previous job's shared-memory reads before the next job's writes.
+__device__ __forceinline__ int grab_job(int* next)
+{
+    __shared__ int s_job;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) s_job = atomicAdd(next, 1);
+    __syncthreads();
+    return s_job;
+}
+
+// propagate tile (threads per CTA = width x height pixels)
+void prop_tile_shape(int* w, int* h);
+// the propagate pass of every pair of a batch: tab[pair] (device memory) holds each pair's
+// arguments, J its tiles (prop_tile_shape); at most ctas_per_sm CTAs per SM (0: as many as
+// fit); next: propagate_batch_launches(counting) work counters, zero
+void launch_propagate_batch(const PropParams* tab, const JobList& J, int ctas_per_sm, int fused, int counting,
+                            int* next, cudaStream_t st);
+int propagate_batch_launches(int counting);
+
+// Per pair and view, the smoothing stage of one iteration of a batch: the normal/depth image
+// of the plane field planes[sel] (k_normal_depth) and the tensor-weighted ROF steps on it
+// (launch_rof), which leave the smoothing image in `out`.
+struct SmoothArgs {
+    float4* out;
+    float4* tmp;               // normal/depth image: the ROF input
+    const float4* dt;
+    float4* scratch;           // rof_scratch_bytes(W, H)
+    const float4* planes[2];
+    float dispscale;
+    int lr, W, H;
+};
+// tile shapes of the smoothing jobs: j8 lists 32x8 tiles (normal/depth, single ROF steps),
+// j16 32x16 tiles (double ROF steps)
+constexpr int SMOOTH_TW = 32, SMOOTH_TH8 = 8, SMOOTH_TH16 = 16;
+// every pair's smoothing stage of one iteration; next: smooth_batch_launches(iters) counters, zero
+void launch_smooth_batch(const SmoothArgs* tab, const JobList& j8, const JobList& j16, int sel, float4 lam, int iters,
+                         int* next, cudaStream_t st);
+int smooth_batch_launches(int iters);
+
 // prep of disparityMapAll (bw = colour + window weight sum, tensor edge weight alpha = 24) or,
 // with raw, of depthMap (bw = the image as floats, alpha = 12)
 void launch_prep(const uint8_t* img, size_t stride, int W, int H, int r, int fused, float4* bw, float4* grad,

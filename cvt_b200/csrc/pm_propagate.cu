@@ -37,6 +37,13 @@ constexpr int PROP_BX = PM_PROP_BX, PROP_BY = PM_PROP_BY, PROP_THREADS = PROP_BX
 #define PM_KLT_THREADS 768
 #endif
 constexpr int PM_CHAIN_BLOCKS = PM_CHAIN_THREADS / PROP_THREADS, PM_KLT_BLOCKS = PM_KLT_THREADS / PROP_THREADS;
+// the batched (persistent) forms read each pair's arguments from global memory instead of the
+// parameter bank, which takes registers: at 768 threads per SM they spill in the window loops,
+// so they are compiled for 640 (96 registers)
+#ifndef PM_BATCH_THREADS
+#define PM_BATCH_THREADS 640
+#endif
+constexpr int PM_BATCH_BLOCKS = PM_BATCH_THREADS / PROP_THREADS;
 
 inline dim3 grid2d(int W, int H, dim3 b) { return dim3((W + b.x - 1) / b.x, (H + b.y - 1) / b.y); }
 
@@ -87,12 +94,10 @@ __device__ __forceinline__ bool known_outcome(float4 nb, float4 self, float thet
 // 9 the randomized refinement (:1021-1028).  One loop, so that the window evaluation has a
 // single call site.
 template <bool F, bool COUNT, bool CHK>
-__global__ void __launch_bounds__(PROP_THREADS, PM_CHAIN_BLOCKS) k_prop_chain(PropParams P)
+__device__ __forceinline__ void chain_tile(const PropParams& P, int bx, int by, Counters& cnt)
 {
-    if (variant_skips<CHK>(P.V, P.dual)) return;
     const ViewData& V = P.V;
-    const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
-    Counters cnt = {0, 0, 0, 0};
+    const int px = bx * PROP_BX + threadIdx.x, py = by * PROP_BY + threadIdx.y;
     if (px < V.W && py < V.H) {
         const int W = V.W;
         const size_t idx = (size_t)py * W + px;
@@ -156,34 +161,46 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_CHAIN_BLOCKS) k_prop_chain(Pr
         }
         P.tmp_self[idx] = self;
     }
+}
+
+template <bool F, bool COUNT, bool CHK>
+__global__ void __launch_bounds__(PROP_THREADS, PM_CHAIN_BLOCKS) k_prop_chain(PropParams P)
+{
+    if (variant_skips<CHK>(P.V, P.dual)) return;
+    Counters cnt = {0, 0, 0, 0};
+    chain_tile<F, COUNT, CHK>(P, blockIdx.x, blockIdx.y, cnt);
     flush_counters<COUNT>(cnt, P.counters);
 }
 
 // Gauss-Newton plane steps (:1034-1038)
 template <bool F, bool COUNT, bool CHK>
-__global__ void __launch_bounds__(PROP_THREADS, PM_KLT_BLOCKS) k_prop_klt(PropParams P)
+__device__ __forceinline__ void klt_tile(const PropParams& P, int bx, int by, Counters& cnt)
 {
-    if (variant_skips<CHK>(P.V, P.dual)) return;
     const ViewData& V = P.V;
-    const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
-    Counters cnt = {0, 0, 0, 0};
+    const int px = bx * PROP_BX + threadIdx.x, py = by * PROP_BY + threadIdx.y;
     if (px < V.W && py < V.H) {
         const size_t idx = (size_t)py * V.W + px;
         float4 nb = P.tmp_self[idx];
         for (int k = 0; k < 6; k++) nb = klt2<F, COUNT, CHK>(V, px, py, nb, cnt);
         P.tmp_nb[idx] = nb;
     }
+}
+
+template <bool F, bool COUNT, bool CHK>
+__global__ void __launch_bounds__(PROP_THREADS, PM_KLT_BLOCKS) k_prop_klt(PropParams P)
+{
+    if (variant_skips<CHK>(P.V, P.dual)) return;
+    Counters cnt = {0, 0, 0, 0};
+    klt_tile<F, COUNT, CHK>(P, blockIdx.x, blockIdx.y, cnt);
     flush_counters<COUNT>(cnt, P.counters);
 }
 
 // evaluation of the Gauss-Newton result (:1039-1052), view scatter (:1060-1067), output (:1070)
 template <bool F, bool COUNT, bool CHK>
-__global__ void __launch_bounds__(PROP_THREADS) k_prop_final(PropParams P)
+__device__ __forceinline__ void final_tile(const PropParams& P, int bx, int by, Counters& cnt)
 {
-    if (variant_skips<CHK>(P.V, P.dual)) return;
     const ViewData& V = P.V;
-    const int px = blockIdx.x * PROP_BX + threadIdx.x, py = blockIdx.y * PROP_BY + threadIdx.y;
-    Counters cnt = {0, 0, 0, 0};
+    const int px = bx * PROP_BX + threadIdx.x, py = by * PROP_BY + threadIdx.y;
     if (px < V.W && py < V.H) {
         const int W = V.W;
         const size_t idx = (size_t)py * W + px;
@@ -214,10 +231,132 @@ __global__ void __launch_bounds__(PROP_THREADS) k_prop_final(PropParams P)
         }
         P.out[idx] = self;
     }
+}
+
+template <bool F, bool COUNT, bool CHK>
+__global__ void __launch_bounds__(PROP_THREADS) k_prop_final(PropParams P)
+{
+    if (variant_skips<CHK>(P.V, P.dual)) return;
+    Counters cnt = {0, 0, 0, 0};
+    final_tile<F, COUNT, CHK>(P, blockIdx.x, blockIdx.y, cnt);
     flush_counters<COUNT>(cnt, P.counters);
 }
 
+// Batched propagate passes (a batch of pairs in lockstep): persistent CTAs take tiles of
+// any pair from the job list (grab_job) and run the single-pair kernels' tile functions on
+// them with that pair's arguments (tab[pair]).  Every pixel runs the same operations on the
+// same fields as in a single-pair launch, so the results are the same bit for bit.
+template <bool F, bool COUNT, bool CHK>
+__global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
+    k_prop_chain_b(const PropParams* __restrict__ tab, const uint2* __restrict__ jobs, int njobs, int* next)
+{
+    for (;;) {
+        const int j = grab_job(next);
+        if (j >= njobs) return;
+        const uint2 job = jobs[j];
+        const PropParams& P = tab[job.x];
+        if (variant_skips<CHK>(P.V, P.dual)) continue;
+        Counters cnt = {0, 0, 0, 0};
+        chain_tile<F, COUNT, CHK>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
+        flush_counters<COUNT>(cnt, P.counters);
+    }
+}
+
+template <bool F, bool COUNT, bool CHK>
+__global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
+    k_prop_klt_b(const PropParams* __restrict__ tab, const uint2* __restrict__ jobs, int njobs, int* next)
+{
+    for (;;) {
+        const int j = grab_job(next);
+        if (j >= njobs) return;
+        const uint2 job = jobs[j];
+        const PropParams& P = tab[job.x];
+        if (variant_skips<CHK>(P.V, P.dual)) continue;
+        Counters cnt = {0, 0, 0, 0};
+        klt_tile<F, COUNT, CHK>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
+        flush_counters<COUNT>(cnt, P.counters);
+    }
+}
+
+template <bool F, bool COUNT, bool CHK>
+__global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
+    k_prop_final_b(const PropParams* __restrict__ tab, const uint2* __restrict__ jobs, int njobs, int* next)
+{
+    for (;;) {
+        const int j = grab_job(next);
+        if (j >= njobs) return;
+        const uint2 job = jobs[j];
+        const PropParams& P = tab[job.x];
+        if (variant_skips<CHK>(P.V, P.dual)) continue;
+        Counters cnt = {0, 0, 0, 0};
+        final_tile<F, COUNT, CHK>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
+        flush_counters<COUNT>(cnt, P.counters);
+    }
+}
+
+// resident CTAs per SM of a kernel with PROP_THREADS threads (at least 1)
+template <class K>
+int resident_ctas(K kernel)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, PROP_THREADS, 0) != cudaSuccess) {
+        cudaGetLastError();
+        n = 1;
+    }
+    return n < 1 ? 1 : n;
+}
+
+template <bool F, bool COUNT, bool CHK>
+void launch_batch_variant(const PropParams* tab, const JobList& J, int ctas_per_sm, int sms, int* next,
+                          cudaStream_t st)
+{
+    const dim3 b(PROP_BX, PROP_BY);
+    auto grid = [&](int resident) {
+        const int per_sm = ctas_per_sm > 0 && ctas_per_sm < resident ? ctas_per_sm : resident;
+        const long long g = (long long)per_sm * sms;
+        return (unsigned)(g < J.njobs ? g : J.njobs);
+    };
+    k_prop_chain_b<F, COUNT, CHK><<<grid(resident_ctas(k_prop_chain_b<F, COUNT, CHK>)), b, 0, st>>>(tab, J.jobs,
+                                                                                                   J.njobs, next);
+    k_prop_klt_b<F, COUNT, CHK><<<grid(resident_ctas(k_prop_klt_b<F, COUNT, CHK>)), b, 0, st>>>(tab, J.jobs, J.njobs,
+                                                                                               next + 1);
+    k_prop_final_b<F, COUNT, CHK><<<grid(resident_ctas(k_prop_final_b<F, COUNT, CHK>)), b, 0, st>>>(tab, J.jobs,
+                                                                                                   J.njobs, next + 2);
+}
+
 }  // namespace
+
+void prop_tile_shape(int* w, int* h)
+{
+    *w = PROP_BX;
+    *h = PROP_BY;
+}
+
+int propagate_batch_launches(int counting) { return counting ? 3 : 6; }
+
+void launch_propagate_batch(const PropParams* tab, const JobList& J, int ctas_per_sm, int fused, int counting,
+                            int* next, cudaStream_t st)
+{
+    if (J.njobs <= 0) return;
+    int dev = 0, sms = 1;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
+        cudaGetLastError();
+        sms = 1;
+    }
+    // as launch_propagate: uncounted passes run both variants (each table entry has dual = 1),
+    // counted ones the checked variant alone (dual = 0)
+    if (counting) {
+        if (fused) launch_batch_variant<true, true, true>(tab, J, ctas_per_sm, sms, next, st);
+        else launch_batch_variant<false, true, true>(tab, J, ctas_per_sm, sms, next, st);
+    } else if (fused) {
+        launch_batch_variant<true, false, false>(tab, J, ctas_per_sm, sms, next, st);
+        launch_batch_variant<true, false, true>(tab, J, ctas_per_sm, sms, next + 3, st);
+    } else {
+        launch_batch_variant<false, false, false>(tab, J, ctas_per_sm, sms, next, st);
+        launch_batch_variant<false, false, true>(tab, J, ctas_per_sm, sms, next + 3, st);
+    }
+}
 
 void launch_propagate(const PropParams& P, int fused, cudaStream_t st)
 {

@@ -166,6 +166,27 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
 /* the number of concurrent branches of later batched calls on this handle, 1..PM_BATCH_BRANCHES
  * (0: PM_BATCH_BRANCHES); cvt_b200.autotune picks it by timing the caller's batch */
 int pm_set_batch_branches(pm_handle* h, int n);
+/* How later batched calls on this handle run.  PM_BATCH_LOCKSTEP (the default): the pairs'
+ * prep, init and post-processing are graph branches as above, and every iteration's
+ * propagate passes and smoothing stages run for ALL pairs at once as persistent launches:
+ * a few CTAs per SM take tiles of any pair from one job list until it is exhausted
+ * (pm_batch_jobs; tile_order 0: pairs in decreasing window work, each pair's tiles row-major;
+ * 1: the pairs' tile rows interleaved, row 0 of every pair first), so one launch spans the
+ * whole batch and no pair waits on a launch tail.  ctas_per_sm caps the propagate launches'
+ * CTAs per SM (0: as many as fit).  PM_BATCH_BRANCHED: every pair's whole pipeline is one
+ * branch.  Results are the same bit for bit under every schedule.  A lockstep call uploads
+ * per-pair argument tables before its launch, waiting for the handle's earlier work on
+ * `stream` when they change; when the caller is capturing `stream` itself, the call runs
+ * branched.  The reference runs one pair per call (PMHuberStereo.cpp:75) and has no
+ * counterpart. */
+enum { PM_BATCH_LOCKSTEP = 0, PM_BATCH_BRANCHED = 1 };
+int pm_set_batch_schedule(pm_handle* h, int schedule, int ctas_per_sm, int tile_order);
+/* host only: the tile job list of a lockstep batch for tiles of tile_w x tile_h pixels, as the
+ * batched call builds it: jobs[2k] = the pair, jobs[2k + 1] = (tile row << 16) | tile column.
+ * *njobs receives the job count; jobs may be NULL to query it, else it has room for njobs_cap
+ * jobs (2 * njobs_cap entries).  Pairs in decreasing W*H*(2r+1)^2 (stable). */
+int pm_batch_jobs(int n, const int* width, const int* height, const int* patchsize, int tile_w, int tile_h,
+                  int tile_order, uint32_t* jobs, int njobs_cap, int* njobs);
 /* the schedule a batched call uses, host only: order[] = the pairs in decreasing window work
  * W*H*(2r+1)^2 (stable), owner[i] = the branch of pair i (least loaded when the pair is
  * placed, lowest index among equals) over min(n, branches) branches */

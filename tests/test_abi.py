@@ -217,6 +217,66 @@ def test_batch_schedule_is_longest_first_onto_least_loaded(native):
     assert native.pm_batch_schedule(0, 4, None, None, None, None, None) == _lib.PM_OK
 
 
+def _jobs_restatement(sizes, tw, th, tile_order):
+    """the job list of a lockstep batch: pairs in decreasing W*H*(2r+1)^2 (stable), tiles
+    row-major per pair (order 0) or the pairs' tile rows interleaved (order 1)"""
+    order = sorted(range(len(sizes)), key=lambda i: -sizes[i][0] * sizes[i][1] * (2 * sizes[i][2] + 1) ** 2)
+    rows = {i: -(-sizes[i][1] // th) for i in order}
+    cols = {i: -(-sizes[i][0] // tw) for i in order}
+    out = []
+    if tile_order == 0:
+        for i in order:
+            out += [(i, by, bx) for by in range(rows[i]) for bx in range(cols[i])]
+    else:
+        for by in range(max(rows.values())):
+            for i in order:
+                if by < rows[i]:
+                    out += [(i, by, bx) for bx in range(cols[i])]
+    return out
+
+
+def test_batch_jobs_cover_every_tile_once(native):
+    """pm_batch_jobs, the tile list the lockstep batch walks: every tile of every pair exactly
+    once, in the documented order, for the 64-pair workload and ragged small cases"""
+    from cvt_b200 import _lib, scene
+
+    specs = scene.batch_specs()
+    cases = [[(s["width"], s["height"], 10) for s in specs],
+             [(64, 48, 2), (320, 240, 7), (64, 48, 2), (33, 17, 1), (1, 1, 0)], [(4096, 4096, 32)]]
+    for sizes in cases:
+        n = len(sizes)
+        W = np.array([s[0] for s in sizes], np.int32)
+        H = np.array([s[1] for s in sizes], np.int32)
+        R = np.array([s[2] for s in sizes], np.int32)
+        for tw, th in ((32, 4), (32, 8), (32, 16)):
+            for order in (0, 1):
+                cnt = C.c_int()
+                assert native.pm_batch_jobs(n, W.ctypes.data, H.ctypes.data, R.ctypes.data, tw, th, order, None, 0,
+                                            C.byref(cnt)) == _lib.PM_OK
+                jobs = np.zeros(2 * cnt.value, np.uint32)
+                assert native.pm_batch_jobs(n, W.ctypes.data, H.ctypes.data, R.ctypes.data, tw, th, order,
+                                            jobs.ctypes.data, cnt.value, C.byref(cnt)) == _lib.PM_OK
+                got = [(int(p), int(t) >> 16, int(t) & 0xFFFF) for p, t in zip(jobs[0::2], jobs[1::2])]
+                want = _jobs_restatement(sizes, tw, th, order)
+                assert got == want
+                assert len(set(got)) == len(got) == sum(-(-w // tw) * -(-h // th) for w, h, _ in sizes)
+        small = C.c_int()
+        assert native.pm_batch_jobs(n, W.ctypes.data, H.ctypes.data, R.ctypes.data, 32, 4, 0, jobs.ctypes.data, 0,
+                                    C.byref(small)) == _lib.PM_EINVAL_ARG
+    x = np.zeros(4, np.int32)
+    cnt = C.c_int()
+    assert native.pm_batch_jobs(2, x.ctypes.data, x.ctypes.data, x.ctypes.data, 32, 4, 0, None, 0,
+                                C.byref(cnt)) == _lib.PM_EINVAL_SHAPE
+    w = np.array([8, 8], np.int32)
+    assert native.pm_batch_jobs(2, w.ctypes.data, w.ctypes.data, x.ctypes.data, 32, 4, 2, None, 0,
+                                C.byref(cnt)) == _lib.PM_EINVAL_ARG
+    assert native.pm_batch_jobs(2, w.ctypes.data, w.ctypes.data, x.ctypes.data, 0, 4, 0, None, 0,
+                                C.byref(cnt)) == _lib.PM_EINVAL_ARG
+    assert native.pm_batch_jobs(0, None, None, None, 32, 4, 0, None, 0, C.byref(cnt)) == _lib.PM_OK
+    assert cnt.value == 0
+    assert native.pm_set_batch_schedule(None, 0, 0, 0) == _lib.PM_EINVAL_ARG
+
+
 def test_batch_specs_seeded_and_in_range():
     from cvt_b200 import scene
 
@@ -345,32 +405,44 @@ def test_lpp_rejects_bad_arguments_without_touching_the_device(native):
     assert native.pm_lpp_wgrad_scratch_floats(3, 32, 96, 128) == 160 * (9 * 64 + 1) * 64
 
 
-def test_autotuner_keeps_the_fastest_branch_count():
-    """tune_batch with a stand-in handle and timer: every candidate is set, warmed once and
-    timed `reps` times; the fastest stays set; ties go to the earlier candidate"""
-    from cvt_b200.autotune import tune_batch
+def test_autotuner_keeps_the_fastest_candidate():
+    """tune_batch with a stand-in handle and timer: every candidate (schedule, CTAs per SM, tile
+    order, branches) is set, warmed once and timed `reps` times; the fastest stays set; ties go to
+    the earlier candidate"""
+    from cvt_b200.autotune import DEFAULT_CANDIDATES, label, tune_batch
 
     class FakeHandle:
         def __init__(self):
-            self.branches, self.calls, self.set_log = 0, [], []
+            self.state, self.calls, self.set_log = None, [], []
+            self.sched = self.branches = None
+
+        def set_batch_schedule(self, schedule, ctas, order):
+            self.sched = (schedule, ctas, order)
 
         def set_batch_branches(self, n):
             self.branches = n
-            self.set_log.append(n)
+            self.state = self.sched + (n,)
+            self.set_log.append(self.state)
 
         def disparity_map_batch(self, lefts, rights, patchsizes, dmaxs, iterations, pp=1):
-            self.calls.append((self.branches, iterations, pp))
+            self.calls.append((self.state, iterations, pp))
 
-    for cost, want in (({2: 50.0, 4: 30.0, 8: 20.0, 16: 25.0}, 8), ({2: 9.0, 4: 9.0, 8: 12.0, 16: 9.0}, 2)):
+    cands = [{"schedule": "branched", "branches": 4}, {"schedule": "lockstep", "ctas_per_sm": 3},
+             {"schedule": "lockstep", "tile_order": 1, "branches": 8}]
+    keys = [("branched", 0, 0, 4), ("lockstep", 3, 0, 16), ("lockstep", 0, 1, 8)]
+    for cost, want in (([50.0, 20.0, 30.0], 1), ([9.0, 12.0, 9.0], 0)):
         pm = FakeHandle()
+        table = dict(zip(keys, cost))
 
         def timer(fn):
             fn()
-            return cost[pm.branches]
+            return table[pm.state]
 
-        res = tune_batch(pm, [], [], [], [], iterations=1, reps=3, timer=timer)
-        assert res["branches"] == want and pm.branches == want
-        assert res["ms"] == cost
-        assert pm.set_log == [2, 4, 8, 16, want]
-        assert [c[0] for c in pm.calls] == [b for b in (2, 4, 8, 16) for _ in range(4)]
+        res = tune_batch(pm, [], [], [], [], iterations=1, candidates=cands, reps=3, timer=timer)
+        assert res["best"] == cands[want] and pm.state == keys[want]
+        assert res["ms"] == {label(c): t for c, t in zip(cands, cost)}
+        assert pm.set_log == keys + [keys[want]]
+        assert [c[0] for c in pm.calls] == [k for k in keys for _ in range(4)]
+        assert all(c[1:] == (1, 1) for c in pm.calls)
+    assert len({label(c) for c in DEFAULT_CANDIDATES}) == len(DEFAULT_CANDIDATES)
 
