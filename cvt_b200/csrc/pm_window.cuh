@@ -60,33 +60,14 @@ __device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y
 #ifndef PM_STRICT_FMUL2
 #define PM_STRICT_FMUL2 1
 #endif
-// Packed adds in strict arithmetic: `add.rn.f32x2` written as PTX.  An add with an explicit
-// rounding modifier is never contracted with the multiply that feeds it, and each element
-// rounds as `add.rn.f32` does, so a pair of scalar rounded adds becomes one instruction with
-// the same results.
-#ifndef PM_STRICT_ADD2
-#define PM_STRICT_ADD2 1
-#endif
-
-__device__ __forceinline__ float2 add2_rn(float2 a, float2 b)
-{
-#if PM_STRICT_ADD2
-    const unsigned long long ua = ((unsigned long long)__float_as_uint(a.y) << 32) | __float_as_uint(a.x);
-    const unsigned long long ub = ((unsigned long long)__float_as_uint(b.y) << 32) | __float_as_uint(b.x);
-    unsigned long long ud;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(ud) : "l"(ua), "l"(ub));
-    return make_float2(__uint_as_float((unsigned int)ud), __uint_as_float((unsigned int)(ud >> 32)));
-#else
-    return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
-#endif
-}
 
 template <bool F>
 __device__ __forceinline__ float2 lerp2(float2 a2, float2 b2, float2 t0, float2 t1)
 {
     if (F) return __ffma2_rn(a2, t1, __fmul2_rn(b2, t0));
 #if PM_STRICT_FMUL2
-    return add2_rn(__fmul2_rn(b2, t0), __fmul2_rn(a2, t1));
+    const float2 p0 = __fmul2_rn(b2, t0), p1 = __fmul2_rn(a2, t1);
+    return make_float2(__fadd_rn(p0.x, p1.x), __fadd_rn(p0.y, p1.y));
 #else
     return make_float2(__fadd_rn(__fmul_rn(b2.x, t0.x), __fmul_rn(a2.x, t1.x)),
                        __fadd_rn(__fmul_rn(b2.y, t0.y), __fmul_rn(a2.y, t1.y)));
@@ -281,19 +262,8 @@ __device__ __forceinline__ bool eval_sample(const float4* __restrict__ q1, const
     float cost = PM_K033_8 * ad_sum<CHK>(tx.c, q);
     // cost + 0.875f * (0.25f * n): the product 0.21875 n is exact, so one fma rounds the same
     cost = fmaf(0.21875f, (float)sign_mismatch(__float_as_uint(q.w), sign_bytes(tx.g)), cost);
-#if PM_STRICT_ADD2
-    if (F) {
-        census = fmaf(w, cost, census);
-        wsum += w;
-    } else {   // (census, wsum) + (w * cost, w), each sum rounded on its own
-        const float2 cw = add2_rn(f2(census, wsum), f2(__fmul_rn(w, cost), w));
-        census = cw.x;
-        wsum = cw.y;
-    }
-#else
     census = F ? fmaf(w, cost, census) : census + w * cost;
     wsum += w;
-#endif
     return true;
 }
 
@@ -431,21 +401,12 @@ __device__ __forceinline__ float4 klt2(const ViewData& V, int px, int py, float4
                 h00_01 = __ffma2_rn(s2, f2(qx * qx, qx * qy), h00_01);
                 h02_11 = __ffma2_rn(s2, f2(qx, yy), h02_11);
                 h12_22 = __ffma2_rn(s2, f2(qy, 1.0f), h12_22);
-            } else {   // each product and sum rounded on its own (see lerp2)
-#if PM_STRICT_ADD2
-                const float2 t2 = f2(t, t), s2 = f2(sc, sc);
-                J01 = add2_rn(J01, __fmul2_rn(t2, f2(qx, qy)));
-                J2 = J2 + t * 1.0f;
-                h00_01 = add2_rn(h00_01, __fmul2_rn(s2, __fmul2_rn(f2(qx, qx), f2(qx, qy))));
-                h02_11 = add2_rn(h02_11, __fmul2_rn(s2, f2(qx, yy)));
-                h12_22 = add2_rn(h12_22, f2(__fmul_rn(sc, qy), sc));   // sc * 1.0f is sc
-#else
+            } else {   // scalar, explicitly rounded (see lerp2)
                 J01 = f2(__fadd_rn(J01.x, __fmul_rn(t, qx)), __fadd_rn(J01.y, __fmul_rn(t, qy)));
                 J2 = J2 + t * 1.0f;
                 h00_01 = f2(__fadd_rn(h00_01.x, __fmul_rn(sc, qx * qx)), __fadd_rn(h00_01.y, __fmul_rn(sc, qx * qy)));
                 h02_11 = f2(__fadd_rn(h02_11.x, __fmul_rn(sc, qx)), __fadd_rn(h02_11.y, __fmul_rn(sc, yy)));
                 h12_22 = f2(__fadd_rn(h12_22.x, __fmul_rn(sc, qy)), __fadd_rn(h12_22.y, __fmul_rn(sc, 1.0f)));
-#endif
             }
         }
     }

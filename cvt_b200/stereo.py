@@ -58,11 +58,12 @@ class PMHuberStereo:
         """concurrent branches of later batched calls (0: the library's default, 16)"""
         _lib.check(_lib.lib().pm_set_batch_branches(self._h, int(n)), self._h)
 
-    def set_batch_schedule(self, schedule="lockstep", ctas_per_sm=0, tile_order=0):
-        """how later batched calls run: "lockstep" (every iteration's propagate passes and
-        smoothing stages of all pairs as persistent launches over one tile list; ctas_per_sm caps
-        the propagate CTAs per SM, 0 = as many as fit; tile_order 0 = pair after pair, 1 = the
-        pairs' tile rows interleaved) or "branched" (each pair's pipeline a graph branch)"""
+    def set_batch_schedule(self, schedule="branched", ctas_per_sm=0, tile_order=0):
+        """how later batched calls run: "branched" (the default: each pair's pipeline a graph
+        branch) or "lockstep" (every iteration's propagate passes and smoothing stages of all
+        pairs as persistent launches over one tile list; ctas_per_sm caps the propagate CTAs per
+        SM, 0 = as many as fit; tile_order 0 = pair after pair, 1 = the pairs' tile rows
+        interleaved)"""
         mode = {"lockstep": _lib.PM_BATCH_LOCKSTEP, "branched": _lib.PM_BATCH_BRANCHED}[schedule]
         _lib.check(_lib.lib().pm_set_batch_schedule(self._h, mode, int(ctas_per_sm), int(tile_order)), self._h)
 

@@ -166,15 +166,16 @@ int pm_disparity_map_batch_device(pm_handle* h, int n, const uint8_t* const* lef
 /* the number of concurrent branches of later batched calls on this handle, 1..PM_BATCH_BRANCHES
  * (0: PM_BATCH_BRANCHES); cvt_b200.autotune picks it by timing the caller's batch */
 int pm_set_batch_branches(pm_handle* h, int n);
-/* How later batched calls on this handle run.  PM_BATCH_LOCKSTEP (the default): the pairs'
- * prep, init and post-processing are graph branches as above, and every iteration's
- * propagate passes and smoothing stages run for ALL pairs at once as persistent launches:
+/* How later batched calls on this handle run.  PM_BATCH_BRANCHED (the default): every pair's
+ * whole pipeline is one branch, as above.  PM_BATCH_LOCKSTEP: the pairs' prep, init and
+ * post-processing are graph branches, and every iteration's propagate passes and smoothing
+ * stages run for ALL pairs at once as persistent launches:
  * a few CTAs per SM take tiles of any pair from one job list until it is exhausted
  * (pm_batch_jobs; tile_order 0: pairs in decreasing window work, each pair's tiles row-major;
  * 1: the pairs' tile rows interleaved, row 0 of every pair first), so one launch spans the
  * whole batch and no pair waits on a launch tail.  ctas_per_sm caps the propagate launches'
- * CTAs per SM (0: as many as fit).  PM_BATCH_BRANCHED: every pair's whole pipeline is one
- * branch.  Results are the same bit for bit under every schedule.  A lockstep call uploads
+ * CTAs per SM (0: as many as fit).  Results are the same bit for bit under every schedule;
+ * cvt_b200.autotune picks one by timing the caller's batch.  A lockstep call uploads
  * per-pair argument tables before its launch, waiting for the handle's earlier work on
  * `stream` when they change; when the caller is capturing `stream` itself, the call runs
  * branched.  The reference runs one pair per call (PMHuberStereo.cpp:75) and has no
