@@ -1369,8 +1369,9 @@ static int batch_lockstep(pm_handle* h, int n, const uint8_t* const* left, const
         L[i] = layout(width[i], height[i], stride[i]);
         B[i] = level_bufs(h->bws[i], L[i], width[i], height[i], patchsize[i]);
     }
-    // host tables: propagate arguments per (iteration, view, pair), smoothing arguments per
-    // (view, pair), the three job lists, then the work counters (zeroed in the stream)
+    // host tables: propagate arguments per (iteration, view, pair) (launch parameters),
+    // smoothing arguments per (view, pair), the job lists and the work counters (device
+    // memory, the counters zeroed in the stream)
     std::vector<PropParams> ptab((size_t)itx * views * n);
     for (int it = 0; it < itx; it++) {
         const float theta = theta_at(it, itx, o.thetamin);
@@ -1399,21 +1400,41 @@ static int batch_lockstep(pm_handle* h, int n, const uint8_t* const* left, const
             A.H = height[i];
             stab[(size_t)v * n + i] = A;
         }
+    // the propagate passes run per group of up to PROP_GROUP pairs (consecutive in `order`),
+    // whose arguments are the launch's parameters: group g's table lists its pairs' arguments
+    // in order and its job list indexes that table
     int ptw, pth;
     prop_tile_shape(&ptw, &pth);
+    const int ngroups = (n + PROP_GROUP - 1) / PROP_GROUP;
+    std::vector<std::vector<PropParams>> gtab((size_t)ngroups * itx * views);
+    std::vector<std::vector<uint32_t>> jpg(ngroups);
+    for (int g = 0; g < ngroups; g++) {
+        const int k0 = g * PROP_GROUP, m = std::min(n - k0, PROP_GROUP);
+        std::vector<int> gw(m), gh(m), gorder(m);
+        for (int k = 0; k < m; k++) {
+            gw[k] = width[order[k0 + k]];
+            gh[k] = height[order[k0 + k]];
+            gorder[k] = k;
+        }
+        batch_jobs(m, gw.data(), gh.data(), gorder.data(), ptw, pth, h->batch_order, jpg[g]);
+        for (int it = 0; it < itx; it++)
+            for (int v = 0; v < views; v++) {
+                std::vector<PropParams>& t = gtab[((size_t)g * itx + it) * views + v];
+                for (int k = 0; k < m; k++) t.push_back(ptab[((size_t)it * views + v) * n + order[k0 + k]]);
+            }
+    }
     std::vector<uint32_t> jp, j8, j16;
-    batch_jobs(n, width, height, order, ptw, pth, h->batch_order, jp);
+    for (int g = 0; g < ngroups; g++) jp.insert(jp.end(), jpg[g].begin(), jpg[g].end());
     batch_jobs(n, width, height, order, SMOOTH_TW, SMOOTH_TH8, h->batch_order, j8);
     batch_jobs(n, width, height, order, SMOOTH_TW, SMOOTH_TH16, h->batch_order, j16);
-    const int per_iter = views * (propagate_batch_launches(h->counting) + smooth_batch_launches(o.rof_iters));
+    const int per_iter = views * (ngroups * propagate_batch_launches(h->counting) + smooth_batch_launches(o.rof_iters));
     const size_t nslots = (size_t)itx * per_iter;
     auto pad = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t o_p = 0, o_s = o_p + pad(ptab.size() * sizeof(PropParams));
+    const size_t o_s = 0;
     const size_t o_jp = o_s + pad(stab.size() * sizeof(SmoothArgs));
     const size_t o_j8 = o_jp + pad(jp.size() * 4), o_j16 = o_j8 + pad(j8.size() * 4);
     const size_t o_ctr = o_j16 + pad(j16.size() * 4), total = o_ctr + pad(nslots * 4);
     std::vector<unsigned char> hb(o_ctr, 0);
-    memcpy(hb.data() + o_p, ptab.data(), ptab.size() * sizeof(PropParams));
     memcpy(hb.data() + o_s, stab.data(), stab.size() * sizeof(SmoothArgs));
     memcpy(hb.data() + o_jp, jp.data(), jp.size() * 4);
     memcpy(hb.data() + o_j8, j8.data(), j8.size() * 4);
@@ -1433,9 +1454,10 @@ static int batch_lockstep(pm_handle* h, int n, const uint8_t* const* left, const
         h->btab_host.swap(hb);
     }
     char* base = static_cast<char*>(h->btab);
-    const PropParams* dP = reinterpret_cast<const PropParams*>(base + o_p);
     const SmoothArgs* dS = reinterpret_cast<const SmoothArgs*>(base + o_s);
-    const JobList Jp{reinterpret_cast<const uint2*>(base + o_jp), (int)(jp.size() / 2)};
+    std::vector<JobList> Jp(ngroups);
+    for (int g = 0, off = 0; g < ngroups; off += (int)(jpg[g].size() / 2), g++)
+        Jp[g] = JobList{reinterpret_cast<const uint2*>(base + o_jp) + off, (int)(jpg[g].size() / 2)};
     const JobList J8{reinterpret_cast<const uint2*>(base + o_j8), (int)(j8.size() / 2)};
     const JobList J16{reinterpret_cast<const uint2*>(base + o_j16), (int)(j16.size() / 2)};
     int* slots = reinterpret_cast<int*>(base + o_ctr);
@@ -1469,10 +1491,12 @@ static int batch_lockstep(pm_handle* h, int n, const uint8_t* const* left, const
         if ((rc = join(cs))) return rc;
         int* next = slots;
         for (int it = 0; it < itx; it++) {
-            for (int v = 0; v < views; v++) {
-                launch_propagate_batch(dP + ((size_t)it * views + v) * n, Jp, h->batch_ctas, F, h->counting, next, cs);
-                next += propagate_batch_launches(h->counting);
-            }
+            for (int v = 0; v < views; v++)
+                for (int g = 0; g < ngroups; g++) {
+                    const std::vector<PropParams>& t = gtab[((size_t)g * itx + it) * views + v];
+                    launch_propagate_batch(t.data(), (int)t.size(), Jp[g], h->batch_ctas, F, h->counting, next, cs);
+                    next += propagate_batch_launches(h->counting);
+                }
             if (it + 1 < itx) {   // as in run_level: no smoothing after the last iteration
                 const float4 lam = smooth_lambda(theta_at(it, itx, o.thetamin));
                 for (int v = 0; v < views; v++) {

@@ -61,11 +61,19 @@ __device__ __forceinline__ int grab_job(int* next)
 
 // propagate tile (threads per CTA = width x height pixels)
 void prop_tile_shape(int* w, int* h);
-// the propagate pass of every pair of a batch: tab[pair] (device memory) holds each pair's
-// arguments, J its tiles (prop_tile_shape); at most ctas_per_sm CTAs per SM (0: as many as
-// fit); next: propagate_batch_launches(counting) work counters, zero
-void launch_propagate_batch(const PropParams* tab, const JobList& J, int ctas_per_sm, int fused, int counting,
-                            int* next, cudaStream_t st);
+// pairs per batched propagate launch: their arguments are one kernel parameter block
+// (128 x 184 bytes, within the 32,764 bytes a launch may pass)
+constexpr int PROP_GROUP = 128;
+struct PropGroup {
+    PropParams p[PROP_GROUP];
+};
+static_assert(sizeof(PropGroup) + 64 <= 32764, "a batched propagate launch's parameters exceed the launch limit");
+// the propagate pass of a group of n <= PROP_GROUP pairs of a batch: group[k] (host memory)
+// holds pair k's arguments, J the group's tiles (prop_tile_shape) with job.x = k; at most
+// ctas_per_sm CTAs per SM (0: as many as fit); next: propagate_batch_launches(counting) work
+// counters, zero
+void launch_propagate_batch(const PropParams* group, int n, const JobList& J, int ctas_per_sm, int fused,
+                            int counting, int* next, cudaStream_t st);
 int propagate_batch_launches(int counting);
 
 // Per pair and view, the smoothing stage of one iteration of a batch: the normal/depth image

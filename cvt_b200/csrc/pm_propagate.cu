@@ -243,18 +243,20 @@ __global__ void __launch_bounds__(PROP_THREADS) k_prop_final(PropParams P)
 }
 
 // Batched propagate passes (a batch of pairs in lockstep): persistent CTAs take tiles of
-// any pair from the job list (grab_job) and run the single-pair kernels' tile functions on
-// them with that pair's arguments (tab[pair]).  Every pixel runs the same operations on the
-// same fields as in a single-pair launch, so the results are the same bit for bit.
+// any pair of a group from the job list (grab_job) and run the single-pair kernels' tile
+// functions on them with that pair's arguments.  The group's arguments travel as one kernel
+// parameter block (read through the constant cache, as a single-pair launch reads its own),
+// job.x indexing it.  Every pixel runs the same operations on the same fields as in a
+// single-pair launch, so the results are the same bit for bit.
 template <bool F, bool COUNT, bool CHK>
 __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
-    k_prop_chain_b(const PropParams* __restrict__ tab, const uint2* __restrict__ jobs, int njobs, int* next)
+    k_prop_chain_b(const __grid_constant__ PropGroup G, const uint2* __restrict__ jobs, int njobs, int* next)
 {
     for (;;) {
         const int j = grab_job(next);
         if (j >= njobs) return;
         const uint2 job = jobs[j];
-        const PropParams& P = tab[job.x];
+        const PropParams& P = G.p[job.x];
         if (variant_skips<CHK>(P.V, P.dual)) continue;
         Counters cnt = {0, 0, 0, 0};
         chain_tile<F, COUNT, CHK>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
@@ -264,13 +266,13 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
 
 template <bool F, bool COUNT, bool CHK>
 __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
-    k_prop_klt_b(const PropParams* __restrict__ tab, const uint2* __restrict__ jobs, int njobs, int* next)
+    k_prop_klt_b(const __grid_constant__ PropGroup G, const uint2* __restrict__ jobs, int njobs, int* next)
 {
     for (;;) {
         const int j = grab_job(next);
         if (j >= njobs) return;
         const uint2 job = jobs[j];
-        const PropParams& P = tab[job.x];
+        const PropParams& P = G.p[job.x];
         if (variant_skips<CHK>(P.V, P.dual)) continue;
         Counters cnt = {0, 0, 0, 0};
         klt_tile<F, COUNT, CHK>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
@@ -280,13 +282,13 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
 
 template <bool F, bool COUNT, bool CHK>
 __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
-    k_prop_final_b(const PropParams* __restrict__ tab, const uint2* __restrict__ jobs, int njobs, int* next)
+    k_prop_final_b(const __grid_constant__ PropGroup G, const uint2* __restrict__ jobs, int njobs, int* next)
 {
     for (;;) {
         const int j = grab_job(next);
         if (j >= njobs) return;
         const uint2 job = jobs[j];
-        const PropParams& P = tab[job.x];
+        const PropParams& P = G.p[job.x];
         if (variant_skips<CHK>(P.V, P.dual)) continue;
         Counters cnt = {0, 0, 0, 0};
         final_tile<F, COUNT, CHK>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
@@ -307,7 +309,7 @@ int resident_ctas(K kernel)
 }
 
 template <bool F, bool COUNT, bool CHK>
-void launch_batch_variant(const PropParams* tab, const JobList& J, int ctas_per_sm, int sms, int* next,
+void launch_batch_variant(const PropGroup& tab, const JobList& J, int ctas_per_sm, int sms, int* next,
                           cudaStream_t st)
 {
     const dim3 b(PROP_BX, PROP_BY);
@@ -334,10 +336,12 @@ void prop_tile_shape(int* w, int* h)
 
 int propagate_batch_launches(int counting) { return counting ? 3 : 6; }
 
-void launch_propagate_batch(const PropParams* tab, const JobList& J, int ctas_per_sm, int fused, int counting,
+void launch_propagate_batch(const PropParams* group, int n, const JobList& J, int ctas_per_sm, int fused, int counting,
                             int* next, cudaStream_t st)
 {
-    if (J.njobs <= 0) return;
+    if (J.njobs <= 0 || n < 1 || n > PROP_GROUP) return;
+    static thread_local PropGroup tab;   // 23 KB: off the stack; copied into the launch
+    for (int i = 0; i < n; i++) tab.p[i] = group[i];
     int dev = 0, sms = 1;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
