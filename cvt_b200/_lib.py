@@ -86,7 +86,7 @@ def lib():
         "pm_set_batch_branches": (i32, [vp, i32]),
         "pm_batch_schedule": (i32, [i32, i32, vp, vp, vp, vp, vp]),
         "pm_batch_partition": (i32, [i32, i32, vp, vp, vp, vp, vp, vp]),
-        "pm_set_batch_schedule": (i32, [vp, i32, i32, i32]),
+        "pm_set_batch_schedule": (i32, [vp, i32, i32, i32, i32]),
         "pm_batch_jobs": (i32, [i32, vp, vp, vp, i32, i32, i32, vp, i32, C.POINTER(C.c_int)]),
         "pm_get_counters": (i32, [vp, C.POINTER(C.c_uint64)]),
         "pm_set_profiling": (i32, [vp, i32]),

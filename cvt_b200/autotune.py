@@ -5,19 +5,19 @@ smoothing stages of all pairs as persistent launches over one tile list, the pai
 post-processing as concurrent graph branches) or branched (each pair's whole pipeline a
 branch of one graph).  The knobs trade overlap, tails and cache locality against each other:
 the schedule, the propagate CTAs per SM (the persistent grid; 0 = as many as fit), the tile
-order (pair after pair, or the pairs' tile rows interleaved) and the number of concurrent
-branches.  tune_batch times the caller's own batch, with a short iteration count, under each
+shape (32 x 4 or 16 x 8 pixels), the tile order (pair after pair, or the pairs' tile rows
+interleaved) and the number of concurrent branches.  tune_batch times the caller's own batch, with a short iteration count, under each
 candidate and keeps the fastest on the handle; results are the same bit for bit under every
 candidate, only the time differs.
 """
 import statistics
 
-# candidates tried by default: {schedule, ctas_per_sm, tile_order, branches}
+# candidates tried by default: {schedule, ctas_per_sm, tile_order, tile_w, branches}
 DEFAULT_CANDIDATES = (
-    {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 0, "branches": 16},
-    {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 1, "branches": 16},
-    {"schedule": "lockstep", "ctas_per_sm": 4, "tile_order": 0, "branches": 16},
-    {"schedule": "branched", "ctas_per_sm": 0, "tile_order": 0, "branches": 16},
+    {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 0, "tile_w": 32, "branches": 16},
+    {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 0, "tile_w": 16, "branches": 16},
+    {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 1, "tile_w": 32, "branches": 16},
+    {"schedule": "branched", "ctas_per_sm": 0, "tile_order": 0, "tile_w": 32, "branches": 16},
 )
 
 
@@ -34,7 +34,7 @@ def cuda_event_ms(fn):
 
 
 def _full(c):
-    d = {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 0, "branches": 16}
+    d = {"schedule": "lockstep", "ctas_per_sm": 0, "tile_order": 0, "tile_w": 32, "branches": 16}
     d.update(c)
     return d
 
@@ -43,13 +43,14 @@ def label(c):
     c = _full(c)
     if c["schedule"] == "branched":
         return "branched/%d" % c["branches"]
-    return "lockstep/ctas%d/order%d/%d" % (c["ctas_per_sm"], c["tile_order"], c["branches"])
+    return "lockstep/ctas%d/order%d/tile%dx%d/%d" % (c["ctas_per_sm"], c["tile_order"], c["tile_w"],
+                                                      128 // c["tile_w"], c["branches"])
 
 
 def apply(pm, c):
     """set candidate c on the handle of pm"""
     c = _full(c)
-    pm.set_batch_schedule(c["schedule"], c["ctas_per_sm"], c["tile_order"])
+    pm.set_batch_schedule(c["schedule"], c["ctas_per_sm"], c["tile_order"], c["tile_w"])
     pm.set_batch_branches(c["branches"])
 
 

@@ -54,7 +54,7 @@ struct pm_handle {
     // concurrent branches of batched calls (pm_set_batch_branches; 0: PM_BATCH_BRANCHES)
     int batch_branches = 0;
     // schedule of batched calls (pm_set_batch_schedule)
-    int batch_schedule = PM_BATCH_BRANCHED, batch_ctas = 0, batch_order = 0;
+    int batch_schedule = PM_BATCH_BRANCHED, batch_ctas = 0, batch_order = 0, batch_tile_w = 32;
     // lockstep batched calls: per-pair argument tables, job lists and work counters in one
     // device allocation, and the host bytes last uploaded into it
     void* btab = nullptr;
@@ -1312,12 +1312,14 @@ static void batch_jobs(int n, const int* width, const int* height, const int* or
     }
 }
 
-int pm_set_batch_schedule(pm_handle* h, int schedule, int ctas_per_sm, int tile_order)
+int pm_set_batch_schedule(pm_handle* h, int schedule, int ctas_per_sm, int tile_order, int tile_w)
 {
     if (!h) return fail(nullptr, PM_EINVAL_ARG, "null handle");
     if (schedule != PM_BATCH_LOCKSTEP && schedule != PM_BATCH_BRANCHED) return fail(h, PM_EINVAL_ARG, "unknown batch schedule");
     if (ctas_per_sm < 0 || ctas_per_sm > 64) return fail(h, PM_EINVAL_ARG, "CTAs per SM out of range");
     if (tile_order != 0 && tile_order != 1) return fail(h, PM_EINVAL_ARG, "unknown tile order");
+    if (tile_w != 0 && tile_w != 16 && tile_w != 32) return fail(h, PM_EINVAL_ARG, "tile width must be 16 or 32");
+    h->batch_tile_w = tile_w ? tile_w : 32;
     h->batch_schedule = schedule;
     h->batch_ctas = ctas_per_sm;
     h->batch_order = tile_order;
@@ -1404,7 +1406,7 @@ static int batch_lockstep(pm_handle* h, int n, const uint8_t* const* left, const
     // whose arguments are the launch's parameters: group g's table lists its pairs' arguments
     // in order and its job list indexes that table
     int ptw, pth;
-    prop_tile_shape(&ptw, &pth);
+    if (!prop_batch_tile_shape(h->batch_tile_w, &ptw, &pth)) return fail(h, PM_EINVAL_ARG, "unsupported tile width");
     const int ngroups = (n + PROP_GROUP - 1) / PROP_GROUP;
     std::vector<std::vector<PropParams>> gtab((size_t)ngroups * itx * views);
     std::vector<std::vector<uint32_t>> jpg(ngroups);
@@ -1494,7 +1496,8 @@ static int batch_lockstep(pm_handle* h, int n, const uint8_t* const* left, const
             for (int v = 0; v < views; v++)
                 for (int g = 0; g < ngroups; g++) {
                     const std::vector<PropParams>& t = gtab[((size_t)g * itx + it) * views + v];
-                    launch_propagate_batch(t.data(), (int)t.size(), Jp[g], h->batch_ctas, F, h->counting, next, cs);
+                    launch_propagate_batch(t.data(), (int)t.size(), Jp[g], ptw, h->batch_ctas, F, h->counting, next,
+                                           cs);
                     next += propagate_batch_launches(h->counting);
                 }
             if (it + 1 < itx) {   // as in run_level: no smoothing after the last iteration
@@ -1522,7 +1525,8 @@ static int batch_lockstep(pm_handle* h, int n, const uint8_t* const* left, const
     std::vector<uint64_t> key = {(uint64_t)n, (uint64_t)nb, (uint64_t)iterations, (uint64_t)pp, (uint64_t)o.views,
                                  (uint64_t)o.fused, fbits(o.thetamin), fbits(o.maxdispdiff), fbits(o.maxanglediff),
                                  (uint64_t)o.rof_iters, (uint64_t)h->counting, (uint64_t)PM_BATCH_LOCKSTEP,
-                                 (uint64_t)h->batch_ctas, (uint64_t)h->batch_order, (uint64_t)(uintptr_t)h->btab};
+                                 (uint64_t)h->batch_ctas, (uint64_t)h->batch_order, (uint64_t)h->batch_tile_w,
+                                 (uint64_t)(uintptr_t)h->btab};
     for (int i = 0; i < n; i++) {
         const uint64_t v[] = {(uint64_t)(uintptr_t)h->bws[i], (uint64_t)(uintptr_t)left[i], (uint64_t)(uintptr_t)right[i],
                               (uint64_t)width[i], (uint64_t)height[i], (uint64_t)stride[i], (uint64_t)patchsize[i],

@@ -59,8 +59,11 @@ __device__ __forceinline__ int grab_job(int* next)
     return s_job;
 }
 
-// propagate tile (threads per CTA = width x height pixels)
+// propagate tile of the single-pair kernels (threads per CTA = width x height pixels)
 void prop_tile_shape(int* w, int* h);
+// propagate tile of the batched kernels for tile width 32 or 16 (the same threads per CTA);
+// false for any other width
+bool prop_batch_tile_shape(int tile_w, int* w, int* h);
 // pairs per batched propagate launch: their arguments are one kernel parameter block
 // (128 x 184 bytes, within the 32,764 bytes a launch may pass)
 constexpr int PROP_GROUP = 128;
@@ -69,10 +72,10 @@ struct PropGroup {
 };
 static_assert(sizeof(PropGroup) + 64 <= 32764, "a batched propagate launch's parameters exceed the launch limit");
 // the propagate pass of a group of n <= PROP_GROUP pairs of a batch: group[k] (host memory)
-// holds pair k's arguments, J the group's tiles (prop_tile_shape) with job.x = k; at most
-// ctas_per_sm CTAs per SM (0: as many as fit); next: propagate_batch_launches(counting) work
-// counters, zero
-void launch_propagate_batch(const PropParams* group, int n, const JobList& J, int ctas_per_sm, int fused,
+// holds pair k's arguments, J the group's tiles (prop_batch_tile_shape(tile_w)) with job.x = k;
+// at most ctas_per_sm CTAs per SM (0: as many as fit); next: propagate_batch_launches(counting)
+// work counters, zero
+void launch_propagate_batch(const PropParams* group, int n, const JobList& J, int tile_w, int ctas_per_sm, int fused,
                             int counting, int* next, cudaStream_t st);
 int propagate_batch_launches(int counting);
 

@@ -93,11 +93,11 @@ __device__ __forceinline__ bool known_outcome(float4 nb, float4 self, float thet
 // [-4, 5] (:982-991), 6 a random plane (:996-1002), 7-8 cross-view planes (:1007-1016),
 // 9 the randomized refinement (:1021-1028).  One loop, so that the window evaluation has a
 // single call site.
-template <bool F, bool COUNT, bool CHK>
+template <bool F, bool COUNT, bool CHK, int BX = PROP_BX, int BY = PROP_BY>
 __device__ __forceinline__ void chain_tile(const PropParams& P, int bx, int by, Counters& cnt)
 {
     const ViewData& V = P.V;
-    const int px = bx * PROP_BX + threadIdx.x, py = by * PROP_BY + threadIdx.y;
+    const int px = bx * BX + threadIdx.x, py = by * BY + threadIdx.y;
     if (px < V.W && py < V.H) {
         const int W = V.W;
         const size_t idx = (size_t)py * W + px;
@@ -173,11 +173,11 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_CHAIN_BLOCKS) k_prop_chain(Pr
 }
 
 // Gauss-Newton plane steps (:1034-1038)
-template <bool F, bool COUNT, bool CHK>
+template <bool F, bool COUNT, bool CHK, int BX = PROP_BX, int BY = PROP_BY>
 __device__ __forceinline__ void klt_tile(const PropParams& P, int bx, int by, Counters& cnt)
 {
     const ViewData& V = P.V;
-    const int px = bx * PROP_BX + threadIdx.x, py = by * PROP_BY + threadIdx.y;
+    const int px = bx * BX + threadIdx.x, py = by * BY + threadIdx.y;
     if (px < V.W && py < V.H) {
         const size_t idx = (size_t)py * V.W + px;
         float4 nb = P.tmp_self[idx];
@@ -196,11 +196,11 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_KLT_BLOCKS) k_prop_klt(PropPa
 }
 
 // evaluation of the Gauss-Newton result (:1039-1052), view scatter (:1060-1067), output (:1070)
-template <bool F, bool COUNT, bool CHK>
+template <bool F, bool COUNT, bool CHK, int BX = PROP_BX, int BY = PROP_BY>
 __device__ __forceinline__ void final_tile(const PropParams& P, int bx, int by, Counters& cnt)
 {
     const ViewData& V = P.V;
-    const int px = bx * PROP_BX + threadIdx.x, py = by * PROP_BY + threadIdx.y;
+    const int px = bx * BX + threadIdx.x, py = by * BY + threadIdx.y;
     if (px < V.W && py < V.H) {
         const int W = V.W;
         const size_t idx = (size_t)py * W + px;
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(PROP_THREADS) k_prop_final(PropParams P)
 // parameter block (read through the constant cache, as a single-pair launch reads its own),
 // job.x indexing it.  Every pixel runs the same operations on the same fields as in a
 // single-pair launch, so the results are the same bit for bit.
-template <bool F, bool COUNT, bool CHK>
+template <bool F, bool COUNT, bool CHK, int BX>
 __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
     k_prop_chain_b(const __grid_constant__ PropGroup G, const uint2* __restrict__ jobs, int njobs, int* next)
 {
@@ -259,12 +259,12 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
         const PropParams& P = G.p[job.x];
         if (variant_skips<CHK>(P.V, P.dual)) continue;
         Counters cnt = {0, 0, 0, 0};
-        chain_tile<F, COUNT, CHK>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
+        chain_tile<F, COUNT, CHK, BX, PROP_THREADS / BX>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
         flush_counters<COUNT>(cnt, P.counters);
     }
 }
 
-template <bool F, bool COUNT, bool CHK>
+template <bool F, bool COUNT, bool CHK, int BX>
 __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
     k_prop_klt_b(const __grid_constant__ PropGroup G, const uint2* __restrict__ jobs, int njobs, int* next)
 {
@@ -275,12 +275,12 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
         const PropParams& P = G.p[job.x];
         if (variant_skips<CHK>(P.V, P.dual)) continue;
         Counters cnt = {0, 0, 0, 0};
-        klt_tile<F, COUNT, CHK>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
+        klt_tile<F, COUNT, CHK, BX, PROP_THREADS / BX>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
         flush_counters<COUNT>(cnt, P.counters);
     }
 }
 
-template <bool F, bool COUNT, bool CHK>
+template <bool F, bool COUNT, bool CHK, int BX>
 __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
     k_prop_final_b(const __grid_constant__ PropGroup G, const uint2* __restrict__ jobs, int njobs, int* next)
 {
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(PROP_THREADS, PM_BATCH_BLOCKS)
         const PropParams& P = G.p[job.x];
         if (variant_skips<CHK>(P.V, P.dual)) continue;
         Counters cnt = {0, 0, 0, 0};
-        final_tile<F, COUNT, CHK>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
+        final_tile<F, COUNT, CHK, BX, PROP_THREADS / BX>(P, (int)(job.y & 0xffffu), (int)(job.y >> 16), cnt);
         flush_counters<COUNT>(cnt, P.counters);
     }
 }
@@ -308,22 +308,31 @@ int resident_ctas(K kernel)
     return n < 1 ? 1 : n;
 }
 
-template <bool F, bool COUNT, bool CHK>
-void launch_batch_variant(const PropGroup& tab, const JobList& J, int ctas_per_sm, int sms, int* next,
-                          cudaStream_t st)
+template <bool F, bool COUNT, bool CHK, int BX>
+void launch_batch_shape(const PropGroup& tab, const JobList& J, int ctas_per_sm, int sms, int* next, cudaStream_t st)
 {
-    const dim3 b(PROP_BX, PROP_BY);
+    const dim3 b(BX, PROP_THREADS / BX);
     auto grid = [&](int resident) {
         const int per_sm = ctas_per_sm > 0 && ctas_per_sm < resident ? ctas_per_sm : resident;
         const long long g = (long long)per_sm * sms;
         return (unsigned)(g < J.njobs ? g : J.njobs);
     };
-    k_prop_chain_b<F, COUNT, CHK><<<grid(resident_ctas(k_prop_chain_b<F, COUNT, CHK>)), b, 0, st>>>(tab, J.jobs,
-                                                                                                   J.njobs, next);
-    k_prop_klt_b<F, COUNT, CHK><<<grid(resident_ctas(k_prop_klt_b<F, COUNT, CHK>)), b, 0, st>>>(tab, J.jobs, J.njobs,
-                                                                                               next + 1);
-    k_prop_final_b<F, COUNT, CHK><<<grid(resident_ctas(k_prop_final_b<F, COUNT, CHK>)), b, 0, st>>>(tab, J.jobs,
-                                                                                                   J.njobs, next + 2);
+    k_prop_chain_b<F, COUNT, CHK, BX><<<grid(resident_ctas(k_prop_chain_b<F, COUNT, CHK, BX>)), b, 0, st>>>(
+        tab, J.jobs, J.njobs, next);
+    k_prop_klt_b<F, COUNT, CHK, BX><<<grid(resident_ctas(k_prop_klt_b<F, COUNT, CHK, BX>)), b, 0, st>>>(
+        tab, J.jobs, J.njobs, next + 1);
+    k_prop_final_b<F, COUNT, CHK, BX><<<grid(resident_ctas(k_prop_final_b<F, COUNT, CHK, BX>)), b, 0, st>>>(
+        tab, J.jobs, J.njobs, next + 2);
+}
+
+// the tile shapes of the batched kernels: 32 x 4 pixels (a warp = 32 pixels of a row) or
+// 16 x 8 (a warp = two rows of 16)
+template <bool F, bool COUNT, bool CHK>
+void launch_batch_variant(const PropGroup& tab, const JobList& J, int tile_w, int ctas_per_sm, int sms, int* next,
+                          cudaStream_t st)
+{
+    if (tile_w == 16) launch_batch_shape<F, COUNT, CHK, 16>(tab, J, ctas_per_sm, sms, next, st);
+    else launch_batch_shape<F, COUNT, CHK, 32>(tab, J, ctas_per_sm, sms, next, st);
 }
 
 }  // namespace
@@ -334,10 +343,18 @@ void prop_tile_shape(int* w, int* h)
     *h = PROP_BY;
 }
 
+bool prop_batch_tile_shape(int tile_w, int* w, int* h)
+{
+    if (tile_w != 16 && tile_w != 32) return false;
+    *w = tile_w;
+    *h = PROP_THREADS / tile_w;
+    return true;
+}
+
 int propagate_batch_launches(int counting) { return counting ? 3 : 6; }
 
-void launch_propagate_batch(const PropParams* group, int n, const JobList& J, int ctas_per_sm, int fused, int counting,
-                            int* next, cudaStream_t st)
+void launch_propagate_batch(const PropParams* group, int n, const JobList& J, int tile_w, int ctas_per_sm, int fused,
+                            int counting, int* next, cudaStream_t st)
 {
     if (J.njobs <= 0 || n < 1 || n > PROP_GROUP) return;
     static thread_local PropGroup tab;   // 23 KB: off the stack; copied into the launch
@@ -351,14 +368,14 @@ void launch_propagate_batch(const PropParams* group, int n, const JobList& J, in
     // as launch_propagate: uncounted passes run both variants (each table entry has dual = 1),
     // counted ones the checked variant alone (dual = 0)
     if (counting) {
-        if (fused) launch_batch_variant<true, true, true>(tab, J, ctas_per_sm, sms, next, st);
-        else launch_batch_variant<false, true, true>(tab, J, ctas_per_sm, sms, next, st);
+        if (fused) launch_batch_variant<true, true, true>(tab, J, tile_w, ctas_per_sm, sms, next, st);
+        else launch_batch_variant<false, true, true>(tab, J, tile_w, ctas_per_sm, sms, next, st);
     } else if (fused) {
-        launch_batch_variant<true, false, false>(tab, J, ctas_per_sm, sms, next, st);
-        launch_batch_variant<true, false, true>(tab, J, ctas_per_sm, sms, next + 3, st);
+        launch_batch_variant<true, false, false>(tab, J, tile_w, ctas_per_sm, sms, next, st);
+        launch_batch_variant<true, false, true>(tab, J, tile_w, ctas_per_sm, sms, next + 3, st);
     } else {
-        launch_batch_variant<false, false, false>(tab, J, ctas_per_sm, sms, next, st);
-        launch_batch_variant<false, false, true>(tab, J, ctas_per_sm, sms, next + 3, st);
+        launch_batch_variant<false, false, false>(tab, J, tile_w, ctas_per_sm, sms, next, st);
+        launch_batch_variant<false, false, true>(tab, J, tile_w, ctas_per_sm, sms, next + 3, st);
     }
 }
 

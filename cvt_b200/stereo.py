@@ -58,14 +58,15 @@ class PMHuberStereo:
         """concurrent branches of later batched calls (0: the library's default, 16)"""
         _lib.check(_lib.lib().pm_set_batch_branches(self._h, int(n)), self._h)
 
-    def set_batch_schedule(self, schedule="branched", ctas_per_sm=0, tile_order=0):
+    def set_batch_schedule(self, schedule="branched", ctas_per_sm=0, tile_order=0, tile_w=32):
         """how later batched calls run: "branched" (the default: each pair's pipeline a graph
         branch) or "lockstep" (every iteration's propagate passes and smoothing stages of all
         pairs as persistent launches over one tile list; ctas_per_sm caps the propagate CTAs per
         SM, 0 = as many as fit; tile_order 0 = pair after pair, 1 = the pairs' tile rows
-        interleaved)"""
+        interleaved; tile_w 32 = tiles of 32 x 4 pixels, 16 = 16 x 8)"""
         mode = {"lockstep": _lib.PM_BATCH_LOCKSTEP, "branched": _lib.PM_BATCH_BRANCHED}[schedule]
-        _lib.check(_lib.lib().pm_set_batch_schedule(self._h, mode, int(ctas_per_sm), int(tile_order)), self._h)
+        _lib.check(_lib.lib().pm_set_batch_schedule(self._h, mode, int(ctas_per_sm), int(tile_order), int(tile_w)),
+                   self._h)
 
     def set_counting(self, on):
         _lib.check(_lib.lib().pm_set_counting(self._h, int(bool(on))), self._h)

@@ -174,14 +174,16 @@ int pm_set_batch_branches(pm_handle* h, int n);
  * (pm_batch_jobs; tile_order 0: pairs in decreasing window work, each pair's tiles row-major;
  * 1: the pairs' tile rows interleaved, row 0 of every pair first), so one launch spans the
  * whole batch and no pair waits on a launch tail.  ctas_per_sm caps the propagate launches'
- * CTAs per SM (0: as many as fit).  Results are the same bit for bit under every schedule;
+ * CTAs per SM (0: as many as fit); tile_w is the width of their tiles of 128 pixels, 32 (32 x 4,
+ * the single-pair kernels' shape) or 16 (16 x 8); 0 means 32.  Results are the same bit for bit
+ * under every schedule and tile shape;
  * cvt_b200.autotune picks one by timing the caller's batch.  A lockstep call uploads
  * per-pair argument tables before its launch, waiting for the handle's earlier work on
  * `stream` when they change; when the caller is capturing `stream` itself, the call runs
  * branched.  The reference runs one pair per call (PMHuberStereo.cpp:75) and has no
  * counterpart. */
 enum { PM_BATCH_LOCKSTEP = 0, PM_BATCH_BRANCHED = 1 };
-int pm_set_batch_schedule(pm_handle* h, int schedule, int ctas_per_sm, int tile_order);
+int pm_set_batch_schedule(pm_handle* h, int schedule, int ctas_per_sm, int tile_order, int tile_w);
 /* host only: the tile job list of a lockstep batch for tiles of tile_w x tile_h pixels, as the
  * batched call builds it: jobs[2k] = the pair, jobs[2k + 1] = (tile row << 16) | tile column.
  * *njobs receives the job count; jobs may be NULL to query it, else it has room for njobs_cap

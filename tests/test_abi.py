@@ -248,7 +248,7 @@ def test_batch_jobs_cover_every_tile_once(native):
         W = np.array([s[0] for s in sizes], np.int32)
         H = np.array([s[1] for s in sizes], np.int32)
         R = np.array([s[2] for s in sizes], np.int32)
-        for tw, th in ((32, 4), (32, 8), (32, 16)):
+        for tw, th in ((32, 4), (16, 8), (32, 8), (32, 16)):
             for order in (0, 1):
                 cnt = C.c_int()
                 assert native.pm_batch_jobs(n, W.ctypes.data, H.ctypes.data, R.ctypes.data, tw, th, order, None, 0,
@@ -274,7 +274,7 @@ def test_batch_jobs_cover_every_tile_once(native):
                                 C.byref(cnt)) == _lib.PM_EINVAL_ARG
     assert native.pm_batch_jobs(0, None, None, None, 32, 4, 0, None, 0, C.byref(cnt)) == _lib.PM_OK
     assert cnt.value == 0
-    assert native.pm_set_batch_schedule(None, 0, 0, 0) == _lib.PM_EINVAL_ARG
+    assert native.pm_set_batch_schedule(None, 0, 0, 0, 32) == _lib.PM_EINVAL_ARG
 
 
 def test_batch_specs_seeded_and_in_range():
@@ -416,8 +416,8 @@ def test_autotuner_keeps_the_fastest_candidate():
             self.state, self.calls, self.set_log = None, [], []
             self.sched = self.branches = None
 
-        def set_batch_schedule(self, schedule, ctas, order):
-            self.sched = (schedule, ctas, order)
+        def set_batch_schedule(self, schedule, ctas, order, tile_w):
+            self.sched = (schedule, ctas, order, tile_w)
 
         def set_batch_branches(self, n):
             self.branches = n
@@ -428,8 +428,8 @@ def test_autotuner_keeps_the_fastest_candidate():
             self.calls.append((self.state, iterations, pp))
 
     cands = [{"schedule": "branched", "branches": 4}, {"schedule": "lockstep", "ctas_per_sm": 3},
-             {"schedule": "lockstep", "tile_order": 1, "branches": 8}]
-    keys = [("branched", 0, 0, 4), ("lockstep", 3, 0, 16), ("lockstep", 0, 1, 8)]
+             {"schedule": "lockstep", "tile_order": 1, "tile_w": 16, "branches": 8}]
+    keys = [("branched", 0, 0, 32, 4), ("lockstep", 3, 0, 32, 16), ("lockstep", 0, 1, 16, 8)]
     for cost, want in (([50.0, 20.0, 30.0], 1), ([9.0, 12.0, 9.0], 0)):
         pm = FakeHandle()
         table = dict(zip(keys, cost))

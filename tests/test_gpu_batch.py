@@ -54,18 +54,20 @@ def test_batch_equals_single_pair_calls(torch_cuda):
                 assert bits_equal(_host(o[k]), _host(e[k])).all(), (rep, k)
 
 
-@pytest.mark.parametrize("schedule,ctas,order,fused", [("lockstep", 0, 0, False), ("lockstep", 2, 1, False),
-                                                        ("lockstep", 0, 1, True), ("branched", 0, 0, False)])
-def test_schedules_equal_single_pair_calls(torch_cuda, schedule, ctas, order, fused):
-    """the lockstep schedule (persistent launches over the tiles of every pair) and the branched
-    one give the single-pair results bit for bit, on capture and on replay, in both arithmetics"""
+@pytest.mark.parametrize("schedule,ctas,order,tile_w,fused", [
+    ("lockstep", 0, 0, 32, False), ("lockstep", 2, 1, 32, False), ("lockstep", 0, 1, 32, True),
+    ("lockstep", 0, 0, 16, False), ("lockstep", 3, 1, 16, True), ("branched", 0, 0, 32, False)])
+def test_schedules_equal_single_pair_calls(torch_cuda, schedule, ctas, order, tile_w, fused):
+    """the lockstep schedule (persistent launches over the tiles of every pair, tiles of 32 x 4 or
+    16 x 8 pixels) and the branched one give the single-pair results bit for bit, on capture and
+    on replay, in both arithmetics"""
     from cvt_b200 import PMHuberStereo
 
     pairs = _pairs(torch_cuda)
     eager = PMHuberStereo(views=2, fused=fused, use_graph=False)
     ref = [eager.disparity_map(a, b, r, d, 3, planes=True) for a, b, r, d in pairs]
     pm = PMHuberStereo(views=2, fused=fused)
-    pm.set_batch_schedule(schedule, ctas, order)
+    pm.set_batch_schedule(schedule, ctas, order, tile_w)
     for rep in range(2):
         out = pm.disparity_map_batch([p[0] for p in pairs], [p[1] for p in pairs], [p[2] for p in pairs],
                                      [p[3] for p in pairs], 3, planes=True)
@@ -160,3 +162,5 @@ def test_branch_counts_and_autotuner_keep_results(torch_cuda, native):
 
     with pytest.raises(_lib.StereoError):
         pm.set_batch_branches(99)
+    with pytest.raises(_lib.StereoError):
+        pm.set_batch_schedule("lockstep", 0, 0, 24)
